@@ -1,0 +1,300 @@
+/*
+ * rbgpu.h - C ABI of the B200 wavefront path-tracing core (librbgpu.so).
+ *
+ * The core is a drop-in for the unidirectional path integrator of the C++
+ * renderer LinkClinton/rainbow. The reference has no C ABI: its extension
+ * point is the C++ class `integrator` (rainbow-cpu/integrators/integrator.hpp:58-71)
+ * and `path_integrator(sampler2d, sampler1d, max_depth = 5, threshold = 1)`
+ * (rainbow-cpu/integrators/path_integrator.hpp:9-12). Each entry point below
+ * names the reference interface whose work it takes over. A C++ adapter class
+ * deriving from `integrator` exports the reference scene into these structures
+ * and writes the result back through film::set_pixel (rainbow-cpu/cameras/film.cpp:202-205).
+ *
+ * Conventions
+ *  - Every call returns rb_status; no exception crosses this boundary.
+ *  - Matrices are 4x4 float, column-major, element (row r, column c) at [c * 4 + r]
+ *    (the glm layout the reference uses, rainbow-core/math/matrix4x4.hpp:15).
+ *  - Vectors are float triples. Colours are linear RGB (the reference's
+ *    color_spectrum, rainbow-cpu/shared/spectrums/color_spectrum.cpp:58-70).
+ *  - Host pointers passed in are read during the call only and never retained.
+ *  - One host thread per context; calls on one context are serialised.
+ */
+#ifndef RBGPU_H
+#define RBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBGPU_ABI_VERSION 1
+
+/* ------------------------------------------------------------------ status */
+typedef int32_t rb_status;
+enum {
+	RB_OK = 0,
+	RB_ERR_INVALID_ARGUMENT = 1,
+	RB_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+	RB_ERR_OUT_OF_MEMORY = 3,
+	RB_ERR_NO_SCENE = 4,         /* render/trace before rb_scene_upload */
+	RB_ERR_STACK_OVERFLOW = 5,   /* device traversal stack limit reached (reported, never trapped) */
+	RB_ERR_QUEUE_OVERFLOW = 6,   /* a wavefront queue exceeded its capacity */
+	RB_ERR_UNSUPPORTED = 7,      /* scene feature outside the supported subset */
+	RB_ERR_IO = 8,               /* checkpoint file could not be read or written */
+	RB_ERR_CHECKPOINT = 9,       /* checkpoint does not match the context */
+	RB_ERR_DEVICE_TIMEOUT = 10,  /* a bounded device wait gave up */
+	RB_ERR_NO_DEVICE = 11        /* no CUDA device is visible */
+};
+
+/* Human-readable name of a status code. Never NULL. */
+const char* rb_status_string(rb_status status);
+
+/* ------------------------------------------------------------------ scene description */
+
+/* Indexed triangle mesh. Replaces rainbow-cpu/shapes/mesh.hpp:16-108
+ * (mesh(positions, tangents, normals, uvs, indices, reverse_orientation)).
+ * uvs are triples because the reference stores them as vector3. */
+typedef struct rb_mesh_desc {
+	const float* positions;     /* 3 * num_vertices, local space */
+	const float* normals;       /* 3 * num_vertices or NULL */
+	const float* tangents;      /* 3 * num_vertices or NULL */
+	const float* uvs;           /* 3 * num_vertices or NULL (defaults (0,0),(1,0),(1,1) per face) */
+	const uint32_t* indices;    /* 3 * num_triangles */
+	uint32_t num_vertices;
+	uint32_t num_triangles;
+	int32_t reverse_orientation;
+	int32_t reserved;
+} rb_mesh_desc;
+
+enum {
+	RB_MATERIAL_MATTE = 0,  /* rainbow-cpu/materials/matte_material.cpp:13-29 (Lambert when sigma == 0) */
+	RB_MATERIAL_METAL = 1,  /* rainbow-cpu/materials/metal_material.cpp:17-37 */
+	RB_MATERIAL_GLASS = 2   /* rainbow-cpu/materials/glass_material.cpp:25-64 */
+};
+
+/* Constant-texture material parameters (constant_texture_t, textures/detail/constant_texture.hpp:25-35). */
+typedef struct rb_material_desc {
+	uint32_t kind;
+	int32_t remap_roughness;    /* metal/glass: apply trowbridge_reitz_distribution::roughness_to_alpha */
+	float diffuse[3];           /* matte */
+	float sigma;                /* matte Oren-Nayar sigma; only 0 (Lambert) is supported */
+	float eta[3];               /* metal: conductor eta (RGB) */
+	float k[3];                 /* metal: conductor absorption k (RGB) */
+	float reflectance[3];       /* glass */
+	float transmission[3];      /* glass */
+	float ior;                  /* glass */
+	float roughness_u;          /* metal, glass (glass with both zero -> fresnel_specular) */
+	float roughness_v;
+} rb_material_desc;
+
+enum {
+	RB_EMITTER_SURFACE = 0,      /* rainbow-cpu/emitters/surface_light.cpp (one-sided on the geometric normal) */
+	RB_EMITTER_ENVIRONMENT = 1   /* rainbow-cpu/emitters/environment_light.cpp with a constant map of 1 */
+};
+
+typedef struct rb_emitter_desc {
+	uint32_t kind;
+	float radiance[3];          /* surface radiance, or environment intensity */
+	float radius;               /* environment: the radius passed to environment_light(intensity, radius) */
+} rb_emitter_desc;
+
+/* One scene entity: rainbow-cpu/scenes/entity.hpp:22-70,
+ * entity(material, emitter, shape, media, transform). -1 means the component is absent.
+ * An entity without a material is invisible (entity.cpp:80-83). */
+typedef struct rb_entity_desc {
+	int32_t mesh;
+	int32_t material;
+	int32_t emitter;
+	int32_t medium;             /* reserved, must be -1 */
+	float local_to_world[16];
+	float world_to_local[16];
+} rb_entity_desc;
+
+/* Flattened binary BVH over (entity, triangle) leaves, the layout of the
+ * reference's bounding_volume_hierarchy<entity_reference>
+ * (rainbow-cpu/shared/accelerators/bounding_volume_hierarchy.hpp:45-80) in preorder.
+ * Node i is 8 words: min.xyz, max.xyz (float), then w0, w1 (uint32 bit patterns):
+ *   interior: left child = i + 1, w0 = right child index, w1 = split axis (0..2)
+ *   leaf:     w0 = first prim slot, w1 = RB_BVH_LEAF_FLAG | count
+ * Prim slot s refers to triangle prim_index[s] of entity prim_entity[s]. */
+#define RB_BVH_LEAF_FLAG 0x80000000u
+typedef struct rb_bvh_desc {
+	const float* nodes;         /* 8 * num_nodes words */
+	uint32_t num_nodes;
+	uint32_t num_prims;
+	const uint32_t* prim_entity;
+	const uint32_t* prim_index;
+} rb_bvh_desc;
+
+/* Scene: rainbow-cpu/scenes/scene.hpp:24-44. Entities are kept in add order;
+ * the emitter list is the entities with an emitter, in that order
+ * (scene::add_entity, scene.cpp:16-28). */
+typedef struct rb_scene_desc {
+	const rb_mesh_desc* meshes;
+	uint32_t num_meshes;
+	uint32_t num_entities;
+	const rb_entity_desc* entities;
+	const rb_material_desc* materials;
+	uint32_t num_materials;
+	uint32_t num_emitters;
+	const rb_emitter_desc* emitters;
+	rb_bvh_desc bvh;            /* num_nodes == 0: rb_scene_upload builds it (rb_bvh_build) */
+} rb_scene_desc;
+
+/* Pinhole / thin-lens perspective camera: rainbow-cpu/cameras/perspective_camera.cpp:78-99.
+ * raster_to_camera is projective_camera::mRasterToCamera (camera.cpp:21-52),
+ * camera_to_world is camera::mCameraToWorld. The eye/target/up/fov fields
+ * record how the matrices were made; the kernels read only the matrices. */
+typedef struct rb_camera_desc {
+	float raster_to_camera[16];
+	float camera_to_world[16];
+	float eye[3];
+	float target[3];
+	float up[3];
+	float fov_degrees;
+	float lens_radius;          /* 0: pinhole */
+	float focus_distance;
+	int32_t width;
+	int32_t height;
+} rb_camera_desc;
+
+/* ------------------------------------------------------------------ rays and hits */
+
+/* A reference `ray` (rainbow-cpu/shared/ray.hpp:13-28): direction as the ray
+ * holds it (the constructor normalises it), origin, and the current length. */
+typedef struct rb_ray {
+	float origin[3];
+	float direction[3];
+	float length;
+} rb_ray;
+
+/* Closest hit: entity ordinal and triangle index within the entity's mesh
+ * (-1, -1 on a miss), world ray length after the hit (the value the reference
+ * leaves in ray.length), and the barycentrics b1, b2 of the hit triangle. */
+typedef struct rb_hit {
+	int32_t entity;
+	int32_t triangle;
+	float t;
+	float b1;
+	float b2;
+} rb_hit;
+
+/* ------------------------------------------------------------------ context */
+typedef struct rb_context rb_context;
+
+/* Create a context on CUDA device `device`. Replaces nothing in the reference
+ * (which has no device); holds device memory, streams and captured graphs. */
+rb_status rb_context_create(rb_context** out, int device);
+rb_status rb_context_destroy(rb_context* ctx);
+
+/* Upload a scene (copied; the caller keeps ownership of the description).
+ * Replaces scene::build_accelerator (rainbow-cpu/scenes/scene.cpp:30-80): when
+ * desc->bvh.num_nodes == 0 the tree is built with the reference's rules. */
+rb_status rb_scene_upload(rb_context* ctx, const rb_scene_desc* desc);
+
+/* Closest hit of each ray over all entities: scene::intersect (scene.cpp:82-95). */
+rb_status rb_trace_closest(rb_context* ctx, const rb_ray* rays, uint32_t count, rb_hit* hits);
+/* Closest hit over visible entities only: scene::intersect_with_shadow_ray (scene.cpp:97-112). */
+rb_status rb_trace_shadow(rb_context* ctx, const rb_ray* rays, uint32_t count, rb_hit* hits);
+/* Same as the two calls above on device-resident arrays, enqueued on `stream`
+ * (a cudaStream_t, NULL for the context's stream); returns once enqueued. */
+rb_status rb_trace_closest_device(rb_context* ctx, const rb_ray* d_rays, uint32_t count, rb_hit* d_hits, void* stream);
+rb_status rb_trace_shadow_device(rb_context* ctx, const rb_ray* d_rays, uint32_t count, rb_hit* d_hits, void* stream);
+
+/* ------------------------------------------------------------------ rendering */
+enum {
+	RB_RENDER_RESET = 1u << 0      /* clear the film accumulators before adding these samples */
+};
+
+/* One render call: path_integrator::trace (rainbow-cpu/integrators/path_integrator.cpp:15-47)
+ * for samples [first_sample, first_sample + spp) of every pixel, driven the way
+ * sampler_integrator::render (sampler_integrator.cpp:19-144) drives it, with one
+ * PCG32 stream per (pixel, sample) instead of one per 16x16 tile. */
+typedef struct rb_render_params {
+	rb_camera_desc camera;
+	uint32_t spp;
+	uint32_t first_sample;
+	uint32_t max_depth;         /* reference default 5 */
+	float rr_threshold;         /* reference default 1 */
+	uint32_t seed;              /* mixed into every per-sample stream (15 bits used) */
+	uint32_t flags;             /* RB_RENDER_* */
+	uint32_t paths_per_wave;    /* 0: library default */
+	uint32_t reserved;
+} rb_render_params;
+
+/* Render and write the per-pixel mean radiance (box filter, film::add_tile +
+ * pixel::spectrum, film.cpp:11-21,207-223) of everything accumulated since the
+ * last reset into rgb_out (caller-owned, width * height * 3 floats, row-major,
+ * pixel (x, y) at (y * width + x) * 3). rgb_out may be NULL. */
+rb_status rb_render(rb_context* ctx, const rb_render_params* params, float* rgb_out);
+
+/* Read back the accumulators: per-pixel sums of radiance (double, 3 per pixel),
+ * of squared radiance (double, 3 per pixel) and the sample count per pixel.
+ * Any output may be NULL. */
+rb_status rb_film_read(rb_context* ctx, double* sum_rgb, double* sum_sq_rgb, uint32_t* sample_count);
+
+/* Counters of the last rb_render call. */
+typedef struct rb_render_stats {
+	uint64_t samples;
+	uint64_t extend_rays;       /* closest-hit rays of the path (one per bounce) */
+	uint64_t shadow_rays;       /* NEE shadow rays */
+	uint64_t mis_rays;          /* BSDF-sampled emitter-search rays of the MIS step */
+	uint64_t node_visits;       /* box tests (filled only when counting is enabled) */
+	uint64_t triangle_tests;    /* (filled only when counting is enabled) */
+	uint32_t device_error;      /* rb_status raised inside a kernel, RB_OK if none */
+	uint32_t kernel_launches;
+	float elapsed_ms;           /* device time of the call, CUDA events */
+	float trace_ms;             /* device time of the traversal kernels */
+} rb_render_stats;
+rb_status rb_render_stats_get(rb_context* ctx, rb_render_stats* out);
+
+/* Enable node-visit / triangle-test counting in the traversal kernels (slower). */
+rb_status rb_set_counting(rb_context* ctx, int enabled);
+
+/* Checkpoint / resume of the film accumulators and sample counter. */
+rb_status rb_checkpoint_save(rb_context* ctx, const char* path);
+rb_status rb_checkpoint_load(rb_context* ctx, const char* path);
+
+/* ------------------------------------------------------------------ host-side helpers (no GPU) */
+
+/* Build the flattened BVH of a scene with the reference's rules: one leaf per
+ * triangle of each entity, median split on the widest centroid axis with
+ * std::nth_element (detail/bounding_volume_hierarchy.hpp:162-233). Returns
+ * RB_ERR_UNSUPPORTED for scenes that need the reference's two-level tree
+ * (a shape referenced more than once or more than 2^17 triangles, scene.cpp:41-75). */
+typedef struct rb_bvh rb_bvh;
+rb_status rb_bvh_build(const rb_scene_desc* desc, rb_bvh** out);
+rb_status rb_bvh_get(const rb_bvh* bvh, rb_bvh_desc* out);
+rb_status rb_bvh_depth(const rb_bvh* bvh, uint32_t* max_depth);
+void rb_bvh_free(rb_bvh* bvh);
+
+/* Seeded synthetic scenes of the benchmark configurations. */
+enum {
+	RB_SCENE_BOX = 0,          /* closed box room: 32 triangles, one 0.25 x 0.25 quad light */
+	RB_SCENE_SPHERES = 1,      /* displaced icospheres over a ground plane, 4 quad lights + environment */
+	RB_SCENE_SLIT_ROOM = 2     /* glossy room, light behind a wall with a slit (hard indirect) */
+};
+typedef struct rb_scene_gen_params {
+	uint32_t kind;
+	uint32_t seed;
+	uint32_t num_spheres;      /* RB_SCENE_SPHERES / RB_SCENE_SLIT_ROOM clutter count */
+	uint32_t subdivision;      /* icosphere subdivision level */
+	int32_t width;
+	int32_t height;
+} rb_scene_gen_params;
+typedef struct rb_scene rb_scene;
+rb_status rb_scene_generate(const rb_scene_gen_params* params, rb_scene** out);
+/* Pointers stay valid until rb_scene_free. bvh is left empty (num_nodes == 0). */
+rb_status rb_scene_get(const rb_scene* scene, rb_scene_desc* desc, rb_camera_desc* camera);
+void rb_scene_free(rb_scene* scene);
+
+/* Library ABI version (RBGPU_ABI_VERSION at build time). */
+int32_t rb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBGPU_H */

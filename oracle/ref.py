@@ -1,0 +1,160 @@
+"""ctypes wrapper of oracle/_ref/liboracle_ref.so (TEST INFRASTRUCTURE ONLY).
+
+The library is the reference renderer itself (rainbow-core + rainbow-cpu sources
+compiled by oracle/Makefile) plus oracle/harness/ref_harness.cpp. Entry points
+take the same rb_scene_desc / rb_camera_desc structures as the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "liboracle_ref.so")
+
+_LIB = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        from rainbow_b200._native import CameraDesc, SceneDesc
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} missing (build with `make -C oracle ref` where the reference is present)")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, f32, i32 = C.c_void_p, C.c_uint32, C.c_float, C.c_int
+        sig = {
+            "orc_scene_build": (i32, [C.POINTER(SceneDesc), C.POINTER(CameraDesc), C.POINTER(vp)]),
+            "orc_scene_free": (None, [vp]),
+            "orc_export_bvh": (i32, [vp, vp, vp, vp, C.POINTER(u32), C.POINTER(u32)]),
+            "orc_export_camera": (i32, [vp, vp, vp]),
+            "orc_export_areas": (i32, [vp, vp]),
+            "orc_trace": (i32, [vp, vp, u32, i32, vp, vp]),
+            "orc_make_rays": (i32, [vp, u32, C.c_uint64, vp]),
+            "orc_camera_rays": (i32, [vp, vp, vp, u32, u32, vp]),
+            "orc_trace_samples": (i32, [vp, vp, vp, u32, u32, f32, u32, vp]),
+            "orc_render": (i32, [vp, u32, u32, u32, f32, u32, i32, i32, i32, vp, vp, C.POINTER(C.c_double)]),
+            "orc_render_shipped": (i32, [vp, u32, u32, f32, vp, C.POINTER(C.c_double)]),
+            "orc_pcg32": (i32, [C.c_uint64, u32, vp, vp]),
+            "orc_bsdf": (i32, [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _LIB = L
+    return _LIB
+
+
+def _ok(st, where):
+    if st != 0:
+        raise RuntimeError(f"{where} returned {st}")
+
+
+class RefScene:
+    """A reference `scene` + `perspective_camera` built from a product Scene description."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self.h = C.c_void_p()
+        _ok(lib().orc_scene_build(C.byref(scene.desc), C.byref(scene.camera), C.byref(self.h)), "orc_scene_build")
+        self.width, self.height = scene.camera.width, scene.camera.height
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_scene_free(self.h)
+            self.h = None
+
+    def bvh(self):
+        nn, npr = C.c_uint32(), C.c_uint32()
+        _ok(lib().orc_export_bvh(self.h, None, None, None, C.byref(nn), C.byref(npr)), "orc_export_bvh")
+        nodes = np.zeros((nn.value, 8), dtype=np.float32)
+        pe = np.zeros(npr.value, dtype=np.uint32)
+        pi = np.zeros(npr.value, dtype=np.uint32)
+        _ok(lib().orc_export_bvh(self.h, nodes.ctypes.data, pe.ctypes.data, pi.ctypes.data, C.byref(nn), C.byref(npr)),
+            "orc_export_bvh")
+        return nodes, pe, pi
+
+    def camera_matrices(self):
+        r2c = np.zeros(16, dtype=np.float32)
+        c2w = np.zeros(16, dtype=np.float32)
+        _ok(lib().orc_export_camera(self.h, r2c.ctypes.data, c2w.ctypes.data), "orc_export_camera")
+        return r2c, c2w
+
+    def areas(self):
+        a = np.zeros(self.scene.desc.num_entities, dtype=np.float32)
+        _ok(lib().orc_export_areas(self.h, a.ctypes.data), "orc_export_areas")
+        return a
+
+    def trace(self, rays, shadow=False, points=False):
+        from rainbow_b200 import HIT_DTYPE, RAY_DTYPE
+        rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.zeros(rays.shape[0], dtype=HIT_DTYPE)
+        pts = np.zeros((rays.shape[0], 3), dtype=np.float32) if points else None
+        _ok(lib().orc_trace(self.h, rays.ctypes.data, rays.shape[0], int(shadow), hits.ctypes.data,
+                            pts.ctypes.data if points else None), "orc_trace")
+        return (hits, pts) if points else hits
+
+    def make_rays(self, n, seed):
+        from rainbow_b200 import RAY_DTYPE
+        rays = np.zeros(n, dtype=RAY_DTYPE)
+        _ok(lib().orc_make_rays(self.h, n, seed, rays.ctypes.data), "orc_make_rays")
+        return rays
+
+    def camera_rays(self, pixels, samples, seed=0):
+        from rainbow_b200 import RAY_DTYPE
+        px = np.ascontiguousarray(pixels, dtype=np.uint32)
+        sm = np.ascontiguousarray(samples, dtype=np.uint32)
+        rays = np.zeros(px.shape[0], dtype=RAY_DTYPE)
+        _ok(lib().orc_camera_rays(self.h, px.ctypes.data, sm.ctypes.data, px.shape[0], seed, rays.ctypes.data),
+            "orc_camera_rays")
+        return rays
+
+    def trace_samples(self, pixels, samples, max_depth=5, rr=1.0, seed=0):
+        px = np.ascontiguousarray(pixels, dtype=np.uint32)
+        sm = np.ascontiguousarray(samples, dtype=np.uint32)
+        out = np.zeros((px.shape[0], 3), dtype=np.float32)
+        _ok(lib().orc_trace_samples(self.h, px.ctypes.data, sm.ctypes.data, px.shape[0], max_depth, rr, seed,
+                                    out.ctypes.data), "orc_trace_samples")
+        return out
+
+    def render(self, spp, first_sample=0, max_depth=5, rr=1.0, seed=0, threads=0, rows=(0, 0)):
+        """FP64 per-pixel sums (H, W, 3) of L and L^2 and the wall seconds."""
+        s = np.zeros((self.height, self.width, 3), dtype=np.float64)
+        q = np.zeros_like(s)
+        sec = C.c_double()
+        _ok(lib().orc_render(self.h, spp, first_sample, max_depth, rr, seed, threads, rows[0], rows[1], s.ctypes.data,
+                             q.ctypes.data, C.byref(sec)), "orc_render")
+        return s, q, sec.value
+
+    def render_shipped(self, spp, max_depth=5, rr=1.0):
+        img = np.zeros((self.height, self.width, 3), dtype=np.float32)
+        sec = C.c_double()
+        _ok(lib().orc_render_shipped(self.h, spp, max_depth, rr, img.ctypes.data, C.byref(sec)), "orc_render_shipped")
+        return img, sec.value
+
+
+def pcg32(seed, n):
+    u = np.zeros(n, dtype=np.uint32)
+    r = np.zeros(n, dtype=np.float32)
+    _ok(lib().orc_pcg32(seed, n, u.ctypes.data, r.ctypes.data), "orc_pcg32")
+    return u, r
+
+
+def bsdf(material, wo, u, wi_eval, include):
+    """scattering_function_collection sample / evaluate / pdf for one material."""
+    n = wo.shape[0]
+    wo = np.ascontiguousarray(wo, dtype=np.float32)
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    wie = np.ascontiguousarray(wi_eval, dtype=np.float32)
+    out = dict(wi=np.zeros((n, 3), np.float32), f=np.zeros((n, 3), np.float32), pdf=np.zeros(n, np.float32),
+               type=np.zeros(n, np.uint32), f_eval=np.zeros((n, 3), np.float32), pdf_eval=np.zeros(n, np.float32))
+    _ok(lib().orc_bsdf(C.byref(material), n, wo.ctypes.data, u.ctypes.data, wie.ctypes.data, include,
+                       out["wi"].ctypes.data, out["f"].ctypes.data, out["pdf"].ctypes.data, out["type"].ctypes.data,
+                       out["f_eval"].ctypes.data, out["pdf_eval"].ctypes.data), "orc_bsdf")
+    return out

@@ -1,0 +1,210 @@
+"""B200 wavefront path-tracing core, a drop-in for rainbow's path_integrator.
+
+Python host layer over the C ABI of librbgpu.so (include/rbgpu.h). It mirrors
+the reference's integrator interface for scripts and tests:
+
+    scene = generate_scene(RB_SCENE_BOX, width=256, height=256)
+    integrator = PathIntegrator(spp=16, max_depth=5, threshold=1.0)
+    image = integrator.render(scene.camera, scene)   # (H, W, 3) float32 per-pixel means
+
+`PathIntegrator(spp, max_depth=5, threshold=1)` takes the arguments of
+`path_integrator(sampler2d(spp), sampler1d, max_depth, threshold)`
+(rainbow-cpu/integrators/path_integrator.hpp:9-12); render(camera, scene)
+follows integrator::render (integrator.hpp:64-66) and returns the film instead
+of writing it. Every call runs the sm_100a kernels; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._native import (  # noqa: F401  (re-exported constants)
+    HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE,
+    RB_MATERIAL_METAL, RB_RENDER_RESET, RB_SCENE_BOX, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES, BvhDesc, CameraDesc,
+    RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
+)
+
+__all__ = ["Scene", "Context", "PathIntegrator", "generate_scene", "build_bvh", "RbError", "RAY_DTYPE", "HIT_DTYPE"]
+
+
+class Scene:
+    """A scene description (rb_scene_desc) plus its camera (rb_camera_desc).
+
+    Generated scenes own their arrays inside the library; `desc` points into them.
+    """
+
+    def __init__(self, handle, desc: SceneDesc, camera: CameraDesc, keepalive=()):
+        self._handle = handle
+        self.desc = desc
+        self.camera = camera
+        self._keepalive = list(keepalive)
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            lib().rb_scene_free(self._handle)
+            self._handle = None
+
+    @property
+    def num_triangles(self) -> int:
+        return sum(self.desc.meshes[i].num_triangles for i in range(self.desc.num_meshes))
+
+    def with_bvh(self, bvh: "Bvh") -> "Scene":
+        """A view of this scene that carries a caller-supplied flattened BVH."""
+        d = SceneDesc()
+        C.pointer(d)[0] = self.desc
+        d.bvh = bvh.desc
+        return Scene(None, d, self.camera, keepalive=[self, bvh])
+
+
+def generate_scene(kind: int, seed: int = 0, width: int = 256, height: int = 256, num_spheres: int = 200,
+                   subdivision: int = 4) -> Scene:
+    """Seeded synthetic scene of one of the benchmark configurations (rb_scene_generate)."""
+    p = SceneGenParams(kind, seed, num_spheres, subdivision, width, height)
+    h = C.c_void_p()
+    check(lib().rb_scene_generate(C.byref(p), C.byref(h)), "rb_scene_generate")
+    desc, cam = SceneDesc(), CameraDesc()
+    check(lib().rb_scene_get(h, C.byref(desc), C.byref(cam)), "rb_scene_get")
+    return Scene(h, desc, cam)
+
+
+@dataclass
+class Bvh:
+    nodes: np.ndarray        # (num_nodes, 8) float32 words
+    prim_entity: np.ndarray  # uint32
+    prim_index: np.ndarray   # uint32
+    depth: int
+    desc: BvhDesc
+
+
+def build_bvh(scene: Scene) -> Bvh:
+    """The reference's median-split tree over the scene (rb_bvh_build), as arrays."""
+    h = C.c_void_p()
+    check(lib().rb_bvh_build(C.byref(scene.desc), C.byref(h)), "rb_bvh_build")
+    try:
+        d = BvhDesc()
+        check(lib().rb_bvh_get(h, C.byref(d)), "rb_bvh_get")
+        depth = C.c_uint32()
+        check(lib().rb_bvh_depth(h, C.byref(depth)), "rb_bvh_depth")
+        nodes = np.ctypeslib.as_array(d.nodes, (d.num_nodes * 8,)).reshape(-1, 8).copy()
+        pe = np.ctypeslib.as_array(d.prim_entity, (d.num_prims,)).copy()
+        pi = np.ctypeslib.as_array(d.prim_index, (d.num_prims,)).copy()
+    finally:
+        lib().rb_bvh_free(h)
+    return bvh_from_arrays(nodes, pe, pi, int(depth.value))
+
+
+def bvh_from_arrays(nodes: np.ndarray, prim_entity: np.ndarray, prim_index: np.ndarray, depth: int = 0) -> Bvh:
+    nodes = np.ascontiguousarray(nodes, dtype=np.float32).reshape(-1, 8)
+    pe = np.ascontiguousarray(prim_entity, dtype=np.uint32)
+    pi = np.ascontiguousarray(prim_index, dtype=np.uint32)
+    d = BvhDesc(nodes.ctypes.data_as(C.POINTER(C.c_float)), nodes.shape[0], pe.shape[0],
+                pe.ctypes.data_as(C.POINTER(C.c_uint32)), pi.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return Bvh(nodes, pe, pi, depth, d)
+
+
+def camera_copy(cam: CameraDesc, **overrides) -> CameraDesc:
+    c = CameraDesc()
+    C.pointer(c)[0] = cam
+    for k, v in overrides.items():
+        if k in ("raster_to_camera", "camera_to_world"):
+            getattr(c, k)[:] = [float(x) for x in np.asarray(v, dtype=np.float32).reshape(16)]
+        else:
+            setattr(c, k, v)
+    return c
+
+
+class Context:
+    """One device context (rb_context): scene upload, ray tracing, rendering."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        check(lib().rb_context_create(C.byref(self._h), device), "rb_context_create")
+        self.scene = None
+
+    def close(self):
+        if self._h:
+            lib().rb_context_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+    def upload(self, scene: Scene) -> None:
+        check(lib().rb_scene_upload(self._h, C.byref(scene.desc)), "rb_scene_upload")
+        self.scene = scene
+
+    def _trace(self, rays: np.ndarray, shadow: bool) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=RAY_DTYPE)
+        hits = np.zeros(rays.shape[0], dtype=HIT_DTYPE)
+        fn = lib().rb_trace_shadow if shadow else lib().rb_trace_closest
+        check(fn(self._h, rays.ctypes.data, rays.shape[0], hits.ctypes.data), "rb_trace")
+        return hits
+
+    def trace_closest(self, rays: np.ndarray) -> np.ndarray:
+        return self._trace(rays, False)
+
+    def trace_shadow(self, rays: np.ndarray) -> np.ndarray:
+        return self._trace(rays, True)
+
+    def render(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5, threshold: float = 1.0,
+               seed: int = 0, reset: bool = True, paths_per_wave: int = 0, want_image: bool = True):
+        p = RenderParams()
+        p.camera = camera
+        p.spp, p.first_sample, p.max_depth, p.rr_threshold = spp, first_sample, max_depth, threshold
+        p.seed, p.flags, p.paths_per_wave = seed, (RB_RENDER_RESET if reset else 0), paths_per_wave
+        img = np.zeros((camera.height, camera.width, 3), dtype=np.float32) if want_image else None
+        self._film_shape = (camera.width, camera.height)
+        check(lib().rb_render(self._h, C.byref(p), img.ctypes.data if want_image else None), "rb_render")
+        return img
+
+    def film(self):
+        """(sum, sum_sq, count) FP64 accumulators of every pixel."""
+        s = lib()
+        cam = self._last_camera_shape()
+        sum_ = np.zeros((cam[1], cam[0], 3), dtype=np.float64)
+        sq = np.zeros_like(sum_)
+        cnt = np.zeros((cam[1], cam[0]), dtype=np.uint32)
+        check(s.rb_film_read(self._h, sum_.ctypes.data, sq.ctypes.data, cnt.ctypes.data), "rb_film_read")
+        return sum_, sq, cnt
+
+    def _last_camera_shape(self):
+        if not hasattr(self, "_film_shape"):
+            raise RbError(4, "film")
+        return self._film_shape
+
+    def stats(self) -> RenderStats:
+        st = RenderStats()
+        check(lib().rb_render_stats_get(self._h, C.byref(st)), "rb_render_stats_get")
+        return st
+
+    def set_counting(self, enabled: bool) -> None:
+        check(lib().rb_set_counting(self._h, int(enabled)), "rb_set_counting")
+
+    def checkpoint_save(self, path: str) -> None:
+        check(lib().rb_checkpoint_save(self._h, path.encode()), "rb_checkpoint_save")
+
+    def checkpoint_load(self, path: str) -> None:
+        check(lib().rb_checkpoint_load(self._h, path.encode()), "rb_checkpoint_load")
+
+
+class PathIntegrator:
+    """path_integrator(sampler2d(spp), sampler1d, max_depth=5, threshold=1) on the GPU."""
+
+    def __init__(self, spp: int, max_depth: int = 5, threshold: float = 1.0, seed: int = 0, device: int = 0):
+        self.spp, self.max_depth, self.threshold, self.seed = spp, max_depth, threshold, seed
+        self.context = Context(device)
+        self._uploaded = None
+
+    def render(self, camera: CameraDesc, scene: Scene) -> np.ndarray:
+        if self._uploaded is not scene:
+            self.context.upload(scene)
+            self._uploaded = scene
+        return self.context.render(camera, self.spp, max_depth=self.max_depth, threshold=self.threshold, seed=self.seed)

@@ -1,0 +1,569 @@
+// C ABI of the wavefront path-tracing core (include/rbgpu.h).
+//
+// A context owns one device's memory: the packed scene, the wave buffers, the
+// film accumulators (FP64 sums and squared sums, sample counts) and one CUDA
+// graph per (wave capacity, depth, counting) configuration. A render call
+// splits its pixels x spp work items into waves; each wave is one replay of the
+// captured graph (camera rays plus max_depth bounces), with the wave's first
+// work item written to a device-side parameter block before the replay.
+#include "../../include/rbgpu.h"
+#include "host/scene_pack.h"
+#include "kernels.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+using namespace rb;
+
+namespace {
+
+template <typename T>
+cudaError_t dev_alloc(T** p, size_t count) {
+	*p = nullptr;
+	if (count == 0) return cudaSuccess;
+	return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+template <typename T>
+cudaError_t dev_upload(T** p, const std::vector<T>& v, cudaStream_t s) {
+	cudaError_t e = dev_alloc(p, v.size());
+	if (e != cudaSuccess || v.empty()) return e;
+	return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+template <typename T>
+void dev_free(T*& p) {
+	if (p) cudaFree(p);
+	p = nullptr;
+}
+
+rb_status from_cuda(cudaError_t e) {
+	if (e == cudaSuccess) return RB_OK;
+	if (e == cudaErrorMemoryAllocation) return RB_ERR_OUT_OF_MEMORY;
+	if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return RB_ERR_NO_DEVICE;
+	return RB_ERR_CUDA;
+}
+
+#define RB_CUDA(call)                                   \
+	do {                                                \
+		const cudaError_t rb_e_ = (call);               \
+		if (rb_e_ != cudaSuccess) return from_cuda(rb_e_); \
+	} while (0)
+
+struct device_scene {
+	float4* nodes = nullptr;
+	float4* tri_a = nullptr;
+	float4* tri_b = nullptr;
+	float2* tri_c = nullptr;
+	uint32_t* prim_index = nullptr;
+	uint32_t* prim_entity = nullptr;
+	pt::entity_rec* entities = nullptr;
+	pt::mesh_rec* meshes = nullptr;
+	float* positions = nullptr;
+	float* normals = nullptr;
+	float* tangents = nullptr;
+	float* uvs = nullptr;
+	uint32_t* indices = nullptr;
+	pt::material_rec* materials = nullptr;
+	pt::emitter_rec* emitters = nullptr;
+	int32_t* environments = nullptr;
+	void release() {
+		dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
+		dev_free(entities); dev_free(meshes); dev_free(positions); dev_free(normals); dev_free(tangents); dev_free(uvs);
+		dev_free(indices); dev_free(materials); dev_free(emitters); dev_free(environments);
+	}
+};
+
+struct graph_key {
+	uint32_t capacity = 0, max_depth = 0, stack = 0;
+	bool count = false;
+	bool operator==(const graph_key& o) const {
+		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count;
+	}
+};
+
+constexpr uint32_t kCheckpointMagic = 0x52424350u;  // "RBCP"
+
+} // namespace
+
+struct rb_context {
+	int device = 0;
+	int num_sms = 148;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+
+	bool has_scene = false;
+	bool has_invisible = false;
+	uint32_t bvh_depth = 0;
+	uint32_t num_entities = 0;
+	device_scene scene;
+	pt::scene_view view{};
+
+	gpu::wave_buffers wave{};
+	uint32_t wave_capacity = 0;
+	gpu::wave_params* params_host = nullptr;  // pinned
+	gpu::film_buffers film{};
+	int32_t film_w = 0, film_h = 0;
+	uint64_t film_samples = 0;  // samples per pixel accumulated since the last reset
+
+	cudaGraphExec_t graph = nullptr;
+	graph_key graph_cfg;
+
+	rb_ray* trace_rays = nullptr;
+	rb_hit* trace_hits = nullptr;
+	size_t trace_cap = 0;
+
+	uint32_t* counters = nullptr;
+	uint32_t* counters_host = nullptr;  // pinned
+	bool counting = false;
+	rb_render_stats stats{};
+
+	gpu::launch_cfg cfg() const {
+		gpu::launch_cfg c;
+		c.block_trace = 128;
+		c.block_shade = 128;
+		c.grid_trace = num_sms * 8;
+		c.grid_shade = num_sms * 8;
+		c.stack_depth = bvh_depth + 3 <= 32 ? 32 : 64;
+		c.count = counting;
+		return c;
+	}
+
+	void release_wave() {
+		dev_free(wave.ray_o); dev_free(wave.ray_d); dev_free(wave.beta); dev_free(wave.radiance); dev_free(wave.bounces);
+		dev_free(wave.rng); dev_free(wave.pixel); dev_free(wave.sample); dev_free(wave.hit); dev_free(wave.rec);
+		dev_free(wave.sec_o); dev_free(wave.sec_d); dev_free(wave.sec_hit); dev_free(wave.queue[0]); dev_free(wave.queue[1]);
+		dev_free(wave.sec_queue);
+		wave_capacity = 0;
+	}
+	void release_graph() {
+		if (graph) cudaGraphExecDestroy(graph);
+		graph = nullptr;
+		graph_cfg = graph_key();
+	}
+	void release_film() {
+		dev_free(film.sum); dev_free(film.sum_sq); dev_free(film.count);
+		film_w = film_h = 0;
+		film_samples = 0;
+	}
+};
+
+namespace {
+
+rb_status ensure_wave(rb_context* c, uint32_t capacity) {
+	if (c->wave_capacity >= capacity) return RB_OK;
+	c->release_graph();
+	c->release_wave();
+	gpu::wave_buffers& w = c->wave;
+	const size_t n = capacity;
+	RB_CUDA(dev_alloc(&w.ray_o, n)); RB_CUDA(dev_alloc(&w.ray_d, n)); RB_CUDA(dev_alloc(&w.beta, n));
+	RB_CUDA(dev_alloc(&w.radiance, n)); RB_CUDA(dev_alloc(&w.bounces, n)); RB_CUDA(dev_alloc(&w.rng, n));
+	RB_CUDA(dev_alloc(&w.pixel, n)); RB_CUDA(dev_alloc(&w.sample, n)); RB_CUDA(dev_alloc(&w.hit, n));
+	RB_CUDA(dev_alloc(&w.rec, n)); RB_CUDA(dev_alloc(&w.sec_o, 2 * n)); RB_CUDA(dev_alloc(&w.sec_d, 2 * n));
+	RB_CUDA(dev_alloc(&w.sec_hit, 2 * n)); RB_CUDA(dev_alloc(&w.queue[0], n)); RB_CUDA(dev_alloc(&w.queue[1], n));
+	RB_CUDA(dev_alloc(&w.sec_queue, 2 * n));
+	w.capacity = capacity;
+	w.counters = c->counters;
+	c->wave_capacity = capacity;
+	return RB_OK;
+}
+
+rb_status ensure_film(rb_context* c, int32_t width, int32_t height, bool reset) {
+	if (c->film_w != width || c->film_h != height) {
+		c->release_film();
+		const size_t px = static_cast<size_t>(width) * height;
+		RB_CUDA(dev_alloc(&c->film.sum, 3 * px));
+		RB_CUDA(dev_alloc(&c->film.sum_sq, 3 * px));
+		RB_CUDA(dev_alloc(&c->film.count, px));
+		c->film_w = width;
+		c->film_h = height;
+		reset = true;
+	}
+	if (reset) {
+		const size_t px = static_cast<size_t>(width) * height;
+		RB_CUDA(cudaMemsetAsync(c->film.sum, 0, 3 * px * sizeof(double), c->stream));
+		RB_CUDA(cudaMemsetAsync(c->film.sum_sq, 0, 3 * px * sizeof(double), c->stream));
+		RB_CUDA(cudaMemsetAsync(c->film.count, 0, px * sizeof(uint32_t), c->stream));
+		c->film_samples = 0;
+	}
+	return RB_OK;
+}
+
+// Records one wave (counter reset + camera + bounces) into a graph.
+rb_status capture_wave(rb_context* c, uint32_t max_depth) {
+	const gpu::launch_cfg cfg = c->cfg();
+	graph_key key;
+	key.capacity = c->wave_capacity;
+	key.max_depth = max_depth;
+	key.stack = static_cast<uint32_t>(cfg.stack_depth);
+	key.count = cfg.count;
+	if (c->graph && c->graph_cfg == key) return RB_OK;
+	c->release_graph();
+	cudaGraph_t g = nullptr;
+	RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+	cudaError_t e = cudaMemsetAsync(c->counters, 0, 3 * sizeof(uint32_t), c->stream);
+	if (e == cudaSuccess) e = gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream);
+	if (e == cudaSuccess) e = gpu::launch_next_wave(c->wave, c->stream);
+	const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+	if (e != cudaSuccess || e2 != cudaSuccess) {
+		if (g) cudaGraphDestroy(g);
+		return from_cuda(e != cudaSuccess ? e : e2);
+	}
+	e = cudaGraphInstantiate(&c->graph, g, 0);
+	cudaGraphDestroy(g);
+	RB_CUDA(e);
+	c->graph_cfg = key;
+	return RB_OK;
+}
+
+bool host_is_valid_camera(const rb_camera_desc& cam) {
+	return cam.width > 0 && cam.height > 0 && cam.width <= 16384 && cam.height <= 16384 &&
+		static_cast<uint64_t>(cam.width) * cam.height < (1ull << 24);
+}
+
+} // namespace
+
+extern "C" {
+
+int32_t rb_abi_version(void) { return RBGPU_ABI_VERSION; }
+
+const char* rb_status_string(rb_status s) {
+	switch (s) {
+	case RB_OK: return "ok";
+	case RB_ERR_INVALID_ARGUMENT: return "invalid argument";
+	case RB_ERR_CUDA: return "CUDA runtime error";
+	case RB_ERR_OUT_OF_MEMORY: return "out of device memory";
+	case RB_ERR_NO_SCENE: return "no scene uploaded";
+	case RB_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+	case RB_ERR_QUEUE_OVERFLOW: return "wavefront queue overflow";
+	case RB_ERR_UNSUPPORTED: return "scene feature not supported";
+	case RB_ERR_IO: return "checkpoint I/O error";
+	case RB_ERR_CHECKPOINT: return "checkpoint does not match the context";
+	case RB_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+	case RB_ERR_NO_DEVICE: return "no CUDA device";
+	default: return "unknown status";
+	}
+}
+
+rb_status rb_context_create(rb_context** out, int device) {
+	if (out == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	*out = nullptr;
+	int count = 0;
+	if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+		cudaGetLastError();
+		return RB_ERR_NO_DEVICE;
+	}
+	if (device < 0 || device >= count) return RB_ERR_INVALID_ARGUMENT;
+	rb_context* c = new (std::nothrow) rb_context();
+	if (c == nullptr) return RB_ERR_OUT_OF_MEMORY;
+	c->device = device;
+	rb_status st = RB_OK;
+	do {
+		if (cudaSetDevice(device) != cudaSuccess) { st = RB_ERR_CUDA; break; }
+		cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+		if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { st = RB_ERR_CUDA; break; }
+		if (cudaEventCreate(&c->ev_begin) != cudaSuccess || cudaEventCreate(&c->ev_end) != cudaSuccess) { st = RB_ERR_CUDA; break; }
+		if (cudaMalloc(&c->counters, gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
+		if (cudaMemset(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_CUDA; break; }
+		if (cudaMallocHost(&c->counters_host, gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
+		if (cudaMallocHost(&c->params_host, sizeof(gpu::wave_params)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
+		if (cudaMalloc(&c->wave.params, sizeof(gpu::wave_params)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
+	} while (false);
+	if (st != RB_OK) {
+		rb_context_destroy(c);
+		return st;
+	}
+	*out = c;
+	return RB_OK;
+}
+
+rb_status rb_context_destroy(rb_context* c) {
+	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	cudaSetDevice(c->device);
+	if (c->stream) cudaStreamSynchronize(c->stream);
+	c->release_graph();
+	c->release_wave();
+	c->release_film();
+	c->scene.release();
+	dev_free(c->trace_rays);
+	dev_free(c->trace_hits);
+	dev_free(c->counters);
+	dev_free(c->wave.params);
+	if (c->counters_host) cudaFreeHost(c->counters_host);
+	if (c->params_host) cudaFreeHost(c->params_host);
+	if (c->ev_begin) cudaEventDestroy(c->ev_begin);
+	if (c->ev_end) cudaEventDestroy(c->ev_end);
+	if (c->stream) cudaStreamDestroy(c->stream);
+	delete c;
+	return RB_OK;
+}
+
+rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
+	if (c == nullptr || desc == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	host::packed_scene p;
+	const rb_status st = host::pack_scene(desc, p);
+	if (st != RB_OK) return st;
+	if (p.bvh_depth + 3 > 64) return RB_ERR_UNSUPPORTED;
+	RB_CUDA(cudaSetDevice(c->device));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	c->release_graph();
+	c->scene.release();
+	c->has_scene = false;
+	device_scene& d = c->scene;
+	RB_CUDA(dev_upload(&d.nodes, p.nodes, c->stream));
+	RB_CUDA(dev_upload(&d.tri_a, p.tri_a, c->stream));
+	RB_CUDA(dev_upload(&d.tri_b, p.tri_b, c->stream));
+	RB_CUDA(dev_upload(&d.tri_c, p.tri_c, c->stream));
+	RB_CUDA(dev_upload(&d.prim_index, p.prim_index, c->stream));
+	RB_CUDA(dev_upload(&d.prim_entity, p.prim_entity, c->stream));
+	RB_CUDA(dev_upload(&d.entities, p.entities, c->stream));
+	RB_CUDA(dev_upload(&d.meshes, p.meshes, c->stream));
+	RB_CUDA(dev_upload(&d.positions, p.positions, c->stream));
+	RB_CUDA(dev_upload(&d.normals, p.normals, c->stream));
+	RB_CUDA(dev_upload(&d.tangents, p.tangents, c->stream));
+	RB_CUDA(dev_upload(&d.uvs, p.uvs, c->stream));
+	RB_CUDA(dev_upload(&d.indices, p.indices, c->stream));
+	RB_CUDA(dev_upload(&d.materials, p.materials, c->stream));
+	RB_CUDA(dev_upload(&d.emitters, p.emitters, c->stream));
+	RB_CUDA(dev_upload(&d.environments, p.environments, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	pt::scene_view v{};
+	v.nodes = d.nodes; v.tri_a = d.tri_a; v.tri_b = d.tri_b; v.tri_c = d.tri_c; v.prim_index = d.prim_index;
+	v.entities = d.entities; v.meshes = d.meshes; v.positions = d.positions; v.normals = d.normals;
+	v.tangents = d.tangents; v.uvs = d.uvs; v.indices = d.indices; v.materials = d.materials; v.emitters = d.emitters;
+	v.environments = d.environments; v.env = p.env;
+	v.num_nodes = static_cast<uint32_t>(p.nodes.size() / 2);
+	v.num_emitters = static_cast<uint32_t>(p.emitters.size());
+	v.num_environments = static_cast<uint32_t>(p.environments.size());
+	v.num_entities = static_cast<uint32_t>(p.entities.size());
+	c->view = v;
+	c->bvh_depth = p.bvh_depth;
+	c->num_entities = v.num_entities;
+	c->has_invisible = false;
+	for (const auto& e : p.entities)
+		if ((e.flags & pt::ENT_HAS_SHAPE) && !(e.flags & pt::ENT_HAS_MATERIAL)) c->has_invisible = true;
+	c->has_scene = true;
+	return RB_OK;
+}
+
+static rb_status trace_device(rb_context* c, const rb_ray* d_rays, uint32_t n, rb_hit* d_hits, bool shadow, cudaStream_t s) {
+	gpu::launch_cfg cfg = c->cfg();
+	RB_CUDA(gpu::launch_trace_rays(c->view, c->scene.prim_entity, d_rays, n, d_hits, shadow, cfg, c->counters, s));
+	return RB_OK;
+}
+
+static rb_status trace_host(rb_context* c, const rb_ray* rays, uint32_t n, rb_hit* hits, bool shadow) {
+	if (c == nullptr || (n > 0 && (rays == nullptr || hits == nullptr))) return RB_ERR_INVALID_ARGUMENT;
+	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	if (n == 0) return RB_OK;
+	RB_CUDA(cudaSetDevice(c->device));
+	if (c->trace_cap < n) {
+		dev_free(c->trace_rays);
+		dev_free(c->trace_hits);
+		c->trace_cap = 0;
+		RB_CUDA(dev_alloc(&c->trace_rays, n));
+		RB_CUDA(dev_alloc(&c->trace_hits, n));
+		c->trace_cap = n;
+	}
+	RB_CUDA(cudaMemsetAsync(c->counters + gpu::CNT_ERROR, 0, sizeof(uint32_t), c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->trace_rays, rays, n * sizeof(rb_ray), cudaMemcpyHostToDevice, c->stream));
+	const rb_status st = trace_device(c, c->trace_rays, n, c->trace_hits, shadow, c->stream);
+	if (st != RB_OK) return st;
+	RB_CUDA(cudaMemcpyAsync(hits, c->trace_hits, n * sizeof(rb_hit), cudaMemcpyDeviceToHost, c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	if (c->counters_host[gpu::CNT_ERROR] != 0) return static_cast<rb_status>(c->counters_host[gpu::CNT_ERROR]);
+	return RB_OK;
+}
+
+rb_status rb_trace_closest(rb_context* c, const rb_ray* rays, uint32_t n, rb_hit* hits) { return trace_host(c, rays, n, hits, false); }
+rb_status rb_trace_shadow(rb_context* c, const rb_ray* rays, uint32_t n, rb_hit* hits) { return trace_host(c, rays, n, hits, true); }
+
+rb_status rb_trace_closest_device(rb_context* c, const rb_ray* d_rays, uint32_t n, rb_hit* d_hits, void* stream) {
+	if (c == nullptr || (n > 0 && (d_rays == nullptr || d_hits == nullptr))) return RB_ERR_INVALID_ARGUMENT;
+	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	RB_CUDA(cudaSetDevice(c->device));
+	return trace_device(c, d_rays, n, d_hits, false, stream ? static_cast<cudaStream_t>(stream) : c->stream);
+}
+rb_status rb_trace_shadow_device(rb_context* c, const rb_ray* d_rays, uint32_t n, rb_hit* d_hits, void* stream) {
+	if (c == nullptr || (n > 0 && (d_rays == nullptr || d_hits == nullptr))) return RB_ERR_INVALID_ARGUMENT;
+	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	RB_CUDA(cudaSetDevice(c->device));
+	return trace_device(c, d_rays, n, d_hits, true, stream ? static_cast<cudaStream_t>(stream) : c->stream);
+}
+
+rb_status rb_set_counting(rb_context* c, int enabled) {
+	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (c->counting != (enabled != 0)) c->release_graph();
+	c->counting = enabled != 0;
+	return RB_OK;
+}
+
+rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) {
+	if (c == nullptr || prm == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	const rb_camera_desc& cam = prm->camera;
+	if (!host_is_valid_camera(cam) || prm->max_depth == 0 || prm->max_depth > 64) return RB_ERR_INVALID_ARGUMENT;
+	if (static_cast<uint64_t>(prm->first_sample) + prm->spp > (1u << 24)) return RB_ERR_INVALID_ARGUMENT;
+	RB_CUDA(cudaSetDevice(c->device));
+	rb_status st = ensure_film(c, cam.width, cam.height, (prm->flags & RB_RENDER_RESET) != 0);
+	if (st != RB_OK) return st;
+	const uint64_t pixels = static_cast<uint64_t>(cam.width) * cam.height;
+	const uint64_t total = pixels * prm->spp;
+	uint64_t capacity = prm->paths_per_wave ? prm->paths_per_wave : (1ull << 21);
+	if (capacity > total) capacity = total;
+	if (capacity > (1ull << 24)) return RB_ERR_INVALID_ARGUMENT;
+	if (capacity == 0) capacity = 1;
+	st = ensure_wave(c, static_cast<uint32_t>(capacity));
+	if (st != RB_OK) return st;
+
+	gpu::wave_params& hp = *c->params_host;
+	std::memcpy(hp.r2c, cam.raster_to_camera, sizeof(hp.r2c));
+	std::memcpy(hp.c2w, cam.camera_to_world, sizeof(hp.c2w));
+	hp.lens = cam.lens_radius;
+	hp.focus = cam.focus_distance;
+	hp.width = static_cast<uint32_t>(cam.width);
+	hp.height = static_cast<uint32_t>(cam.height);
+	hp.total_items = total;
+	hp.first_sample = prm->first_sample;
+	hp.seed = prm->seed;
+	hp.max_depth = prm->max_depth;
+	hp.rr_threshold = prm->rr_threshold;
+
+	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
+	const bool use_graph = !c->has_invisible;
+	if (use_graph) {
+		st = capture_wave(c, prm->max_depth);
+		if (st != RB_OK) return st;
+	}
+	const gpu::launch_cfg cfg = c->cfg();
+	uint32_t launches = 0;
+	hp.first_item = 0;
+	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
+	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
+		if (use_graph) {
+			// the graph's last node moves params->first_item to the next wave
+			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+			launches += 2 + 5 * prm->max_depth;
+		} else {
+			// invisible entities: a pass-through does not count as a bounce, so
+			// keep bouncing until the active queue drains
+			RB_CUDA(cudaMemsetAsync(c->counters, 0, 3 * sizeof(uint32_t), c->stream));
+			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, prm->max_depth, 0u, cfg, c->stream));
+			launches += 1 + 5 * prm->max_depth;
+			uint32_t q = prm->max_depth & 1u;
+			for (int guard = 0; guard < 4096; guard++) {
+				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+				RB_CUDA(cudaStreamSynchronize(c->stream));
+				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
+				RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
+				launches += 5;
+				q ^= 1u;
+			}
+			RB_CUDA(gpu::launch_next_wave(c->wave, c->stream));
+			launches += 1;
+		}
+	}
+	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	const uint32_t* h = c->counters_host;
+	auto u64 = [&](uint32_t w) { return static_cast<uint64_t>(h[w]) | (static_cast<uint64_t>(h[w + 1]) << 32); };
+	rb_render_stats& s = c->stats;
+	s.samples = total;
+	s.extend_rays = u64(gpu::CNT_EXTEND_RAYS);
+	s.shadow_rays = u64(gpu::CNT_SHADOW_RAYS);
+	s.mis_rays = u64(gpu::CNT_MIS_RAYS);
+	s.node_visits = u64(gpu::CNT_NODE_VISITS);
+	s.triangle_tests = u64(gpu::CNT_TRI_TESTS);
+	s.device_error = h[gpu::CNT_ERROR];
+	s.kernel_launches = launches;
+	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
+	s.trace_ms = 0.f;
+	c->film_samples += prm->spp;
+	if (h[gpu::CNT_ERROR] != 0) return static_cast<rb_status>(h[gpu::CNT_ERROR]);
+
+	if (rgb_out != nullptr) {
+		std::vector<double> sum(3 * pixels);
+		std::vector<uint32_t> cnt(pixels);
+		RB_CUDA(cudaMemcpy(sum.data(), c->film.sum, sum.size() * sizeof(double), cudaMemcpyDeviceToHost));
+		RB_CUDA(cudaMemcpy(cnt.data(), c->film.count, cnt.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+		for (uint64_t i = 0; i < pixels; i++)
+			for (int k = 0; k < 3; k++)
+				rgb_out[3 * i + k] = cnt[i] ? static_cast<float>(sum[3 * i + k] / cnt[i]) : 0.f;
+	}
+	return RB_OK;
+}
+
+rb_status rb_film_read(rb_context* c, double* sum_rgb, double* sum_sq_rgb, uint32_t* count) {
+	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (c->film_w == 0) return RB_ERR_NO_SCENE;
+	RB_CUDA(cudaSetDevice(c->device));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	const size_t px = static_cast<size_t>(c->film_w) * c->film_h;
+	if (sum_rgb) RB_CUDA(cudaMemcpy(sum_rgb, c->film.sum, 3 * px * sizeof(double), cudaMemcpyDeviceToHost));
+	if (sum_sq_rgb) RB_CUDA(cudaMemcpy(sum_sq_rgb, c->film.sum_sq, 3 * px * sizeof(double), cudaMemcpyDeviceToHost));
+	if (count) RB_CUDA(cudaMemcpy(count, c->film.count, px * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+	return RB_OK;
+}
+
+rb_status rb_render_stats_get(rb_context* c, rb_render_stats* out) {
+	if (c == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	*out = c->stats;
+	return RB_OK;
+}
+
+// Checkpoint layout: magic, version, width, height, samples per pixel so far,
+// then the FP64 sums, FP64 squared sums and uint32 counts.
+rb_status rb_checkpoint_save(rb_context* c, const char* path) {
+	if (c == nullptr || path == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (c->film_w == 0) return RB_ERR_NO_SCENE;
+	const size_t px = static_cast<size_t>(c->film_w) * c->film_h;
+	std::vector<double> sum(3 * px), sq(3 * px);
+	std::vector<uint32_t> cnt(px);
+	const rb_status st = rb_film_read(c, sum.data(), sq.data(), cnt.data());
+	if (st != RB_OK) return st;
+	FILE* f = std::fopen(path, "wb");
+	if (f == nullptr) return RB_ERR_IO;
+	const uint32_t head[4] = {kCheckpointMagic, 1u, static_cast<uint32_t>(c->film_w), static_cast<uint32_t>(c->film_h)};
+	const uint64_t spp = c->film_samples;
+	bool ok = std::fwrite(head, sizeof(head), 1, f) == 1 && std::fwrite(&spp, sizeof(spp), 1, f) == 1 &&
+		std::fwrite(sum.data(), sizeof(double), sum.size(), f) == sum.size() &&
+		std::fwrite(sq.data(), sizeof(double), sq.size(), f) == sq.size() &&
+		std::fwrite(cnt.data(), sizeof(uint32_t), cnt.size(), f) == cnt.size();
+	ok = (std::fclose(f) == 0) && ok;
+	return ok ? RB_OK : RB_ERR_IO;
+}
+
+rb_status rb_checkpoint_load(rb_context* c, const char* path) {
+	if (c == nullptr || path == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	FILE* f = std::fopen(path, "rb");
+	if (f == nullptr) return RB_ERR_IO;
+	uint32_t head[4];
+	uint64_t spp = 0;
+	if (std::fread(head, sizeof(head), 1, f) != 1 || std::fread(&spp, sizeof(spp), 1, f) != 1 || head[0] != kCheckpointMagic ||
+		head[1] != 1u || head[2] == 0 || head[3] == 0 || static_cast<uint64_t>(head[2]) * head[3] >= (1ull << 24)) {
+		std::fclose(f);
+		return RB_ERR_CHECKPOINT;
+	}
+	const size_t px = static_cast<size_t>(head[2]) * head[3];
+	std::vector<double> sum(3 * px), sq(3 * px);
+	std::vector<uint32_t> cnt(px);
+	const bool ok = std::fread(sum.data(), sizeof(double), sum.size(), f) == sum.size() &&
+		std::fread(sq.data(), sizeof(double), sq.size(), f) == sq.size() &&
+		std::fread(cnt.data(), sizeof(uint32_t), cnt.size(), f) == cnt.size();
+	std::fclose(f);
+	if (!ok) return RB_ERR_CHECKPOINT;
+	RB_CUDA(cudaSetDevice(c->device));
+	const rb_status st = ensure_film(c, static_cast<int32_t>(head[2]), static_cast<int32_t>(head[3]), true);
+	if (st != RB_OK) return st;
+	RB_CUDA(cudaMemcpyAsync(c->film.sum, sum.data(), sum.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->film.sum_sq, sq.data(), sq.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->film.count, cnt.data(), cnt.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	c->film_samples = spp;
+	return RB_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,37 @@
+// Host packing of an rb_scene_desc into the flat record arrays the kernels read.
+#pragma once
+
+#include "../../../include/rbgpu.h"
+#include "../pt/pt_types.h"
+
+#include <vector>
+
+namespace rb {
+namespace host {
+
+struct packed_scene {
+	std::vector<float4> nodes;            // 2 per BVH node
+	std::vector<float4> tri_a, tri_b;     // per prim slot, entity-local p0 / e1 / e2
+	std::vector<float2> tri_c;
+	std::vector<uint32_t> prim_index;
+	std::vector<uint32_t> prim_entity;
+	std::vector<pt::entity_rec> entities;
+	std::vector<pt::mesh_rec> meshes;
+	std::vector<float> positions, normals, tangents, uvs;
+	std::vector<uint32_t> indices;
+	std::vector<pt::material_rec> materials;
+	std::vector<pt::emitter_rec> emitters;
+	std::vector<int32_t> environments;
+	pt::env_distribution env{};
+	uint32_t bvh_depth = 0;
+};
+
+// Validates and packs a scene. Builds the BVH with rb_bvh_build when the
+// description carries none.
+rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out);
+
+// A scene_view whose pointers are the host vectors of `p`.
+pt::scene_view host_view(const packed_scene& p);
+
+} // namespace host
+} // namespace rb

@@ -1,0 +1,368 @@
+// Wavefront path-tracing kernels for sm_100a.
+//
+// Traversal kernels keep each thread's DFS stack in shared memory, laid out
+// [entry][thread] so a warp's pushes and pops hit 32 distinct banks. Queues
+// are compacted with one atomic per warp: __ballot_sync collects the lanes
+// that push, the lowest such lane reserves popc(mask) slots, and every lane
+// writes at base + popc(mask & lanes_below_me). All loops are grid-stride loops
+// over counts that live in device memory, so the launches can be captured in a
+// CUDA graph once and replayed for every wave.
+#include "kernels.cuh"
+
+namespace rb {
+namespace gpu {
+
+using namespace rb::pt;
+
+namespace {
+
+struct smem_stack {
+	uint32_t* base;
+	uint32_t stride;
+	uint32_t sp;
+	uint32_t cap;
+	__device__ void reset() { sp = 0; }
+	__device__ void push(uint32_t v) { base[sp * stride] = v; sp++; }
+	__device__ uint32_t pop() { sp--; return base[sp * stride]; }
+	__device__ bool empty() const { return sp == 0; }
+	__device__ bool full() const { return sp + 2 > cap; }
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+	uint32_t m;
+	asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+	return m;
+}
+
+// Warp-aggregated push of `value` into queue (when `pred`); all lanes of the
+// warp must call it together.
+__device__ __forceinline__ void warp_push(bool pred, uint32_t value, uint32_t* queue, uint32_t* counter) {
+	const uint32_t mask = __ballot_sync(0xffffffffu, pred);
+	if (mask == 0) return;
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t leader = __ffs(mask) - 1;
+	uint32_t base = 0;
+	if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+	base = __shfl_sync(0xffffffffu, base, leader);
+	if (pred) queue[base + __popc(mask & lanemask_lt())] = value;
+}
+
+__device__ __forceinline__ void add64(uint32_t* counters, uint32_t word, uint64_t v) {
+	atomicAdd(reinterpret_cast<unsigned long long*>(counters + word), static_cast<unsigned long long>(v));
+}
+
+__device__ __forceinline__ void warp_add64(uint32_t* counters, uint32_t word, uint32_t v) {
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+	if ((threadIdx.x & 31u) == 0 && v) add64(counters, word, v);
+}
+
+__device__ __forceinline__ void set_error(uint32_t* counters, uint32_t code) { atomicCAS(counters + CNT_ERROR, 0u, code); }
+
+__device__ __forceinline__ hit_t to_hit(float4 h) {
+	hit_t r;
+	r.slot = static_cast<int32_t>(__float_as_uint(h.x));
+	r.b1 = h.z;
+	r.b2 = h.w;
+	return r;
+}
+
+template <bool SHADOW, bool COUNT>
+__device__ __forceinline__ bool trace_one(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h, smem_stack& st,
+	uint32_t& nodes, uint32_t& tris) {
+	trace_counters c{0u, 0u};
+	const bool ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
+	nodes += c.nodes;
+	tris += c.tris;
+	return ok;
+}
+
+// ------------------------------------------------------------------ ray batches
+template <bool SHADOW, bool COUNT>
+__global__ void __launch_bounds__(128) k_trace_rays(scene_view s, const uint32_t* __restrict__ prim_entity,
+	const rb_ray* __restrict__ rays, uint32_t n, rb_hit* __restrict__ hits, uint32_t stack_cap, uint32_t* counters) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st{smem + threadIdx.x, blockDim.x, 0u, stack_cap};
+	uint32_t nodes = 0, tris = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t i = base + threadIdx.x;
+		if (i < n) {
+			const rb_ray r = rays[i];
+			float len = r.length;
+			hit_t h;
+			const vec3 o{r.origin[0], r.origin[1], r.origin[2]};
+			const vec3 d{r.direction[0], r.direction[1], r.direction[2]};
+			if (!trace_one<SHADOW, COUNT>(s, o, d, len, h, st, nodes, tris)) set_error(counters, RB_ERR_STACK_OVERFLOW);
+			rb_hit out;
+			if (h.slot >= 0) {
+				out.entity = static_cast<int32_t>(prim_entity[h.slot]);
+				out.triangle = static_cast<int32_t>(s.prim_index[h.slot]);
+				out.b1 = h.b1;
+				out.b2 = h.b2;
+			} else {
+				out.entity = -1;
+				out.triangle = -1;
+				out.b1 = out.b2 = 0.f;
+			}
+			out.t = len;
+			hits[i] = out;
+		}
+	}
+	if (COUNT) {
+		warp_add64(counters, CNT_NODE_VISITS, nodes);
+		warp_add64(counters, CNT_TRI_TESTS, tris);
+	}
+}
+
+// ------------------------------------------------------------------ wavefront
+__device__ __forceinline__ pcg32 load_rng(const wave_buffers& w, const wave_params& p, uint32_t i) {
+	pcg32 g;
+	g.state = w.rng[i];
+	g.inc = (stream_seed(w.pixel[i], w.sample[i], p.seed) << 1u) | 1u;
+	return g;
+}
+
+__device__ __forceinline__ path_state load_path(const wave_buffers& w, const wave_params& p, uint32_t i) {
+	path_state st;
+	const float4 o = w.ray_o[i], d = w.ray_d[i], b = w.beta[i], L = w.radiance[i];
+	st.o = vec3{o.x, o.y, o.z};
+	st.len = o.w;
+	st.d = vec3{d.x, d.y, d.z};
+	st.beta = vec3{b.x, b.y, b.z};
+	st.eta = b.w;
+	st.L = vec3{L.x, L.y, L.z};
+	st.flags = __float_as_uint(L.w);
+	st.bounces = w.bounces[i];
+	st.rng = load_rng(w, p, i);
+	return st;
+}
+
+__device__ __forceinline__ void store_path(const wave_buffers& w, uint32_t i, const path_state& st) {
+	w.ray_o[i] = make_float4(st.o.x, st.o.y, st.o.z, st.len);
+	w.ray_d[i] = make_float4(st.d.x, st.d.y, st.d.z, 0.f);
+	w.beta[i] = make_float4(st.beta.x, st.beta.y, st.beta.z, st.eta);
+	w.radiance[i] = make_float4(st.L.x, st.L.y, st.L.z, __uint_as_float(st.flags));
+	w.bounces[i] = st.bounces;
+	w.rng[i] = st.rng.state;
+}
+
+__device__ __forceinline__ void film_add(const film_buffers& f, uint32_t pixel, vec3 L) {
+	double* s = f.sum + 3ull * pixel;
+	double* q = f.sum_sq + 3ull * pixel;
+	atomicAdd(s + 0, static_cast<double>(L.x));
+	atomicAdd(s + 1, static_cast<double>(L.y));
+	atomicAdd(s + 2, static_cast<double>(L.z));
+	atomicAdd(q + 0, static_cast<double>(L.x) * L.x);
+	atomicAdd(q + 1, static_cast<double>(L.y) * L.y);
+	atomicAdd(q + 2, static_cast<double>(L.z) * L.z);
+	atomicAdd(f.count + pixel, 1u);
+}
+
+// sampler_integrator::render's per-sample set-up (sampler_integrator.cpp:102-126) for
+// every work item of the wave; all of them enter the active queue.
+__global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_out) {
+	const wave_params& p = *w.params;
+	const uint64_t pixels = static_cast<uint64_t>(p.width) * p.height;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < w.capacity; base += gridDim.x * blockDim.x) {
+		const uint32_t i = base + threadIdx.x;
+		const uint64_t item = p.first_item + i;
+		const bool valid = i < w.capacity && item < p.total_items;
+		if (valid) {
+			const uint32_t pixel = static_cast<uint32_t>(item % pixels);
+			const uint32_t sample = p.first_sample + static_cast<uint32_t>(item / pixels);
+			path_state st;
+			path_begin(st, p.r2c, p.c2w, p.lens, p.focus, pixel % p.width, pixel / p.width, pixel, sample, p.seed);
+			w.pixel[i] = pixel;
+			w.sample[i] = sample;
+			store_path(w, i, st);
+		}
+		warp_push(valid, i, w.queue[queue_out], w.counters + CNT_ACTIVE);
+	}
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st{smem + threadIdx.x, blockDim.x, 0u, stack_cap};
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	uint32_t nodes = 0, tris = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		if (k < n) {
+			const uint32_t i = q[k];
+			const float4 o = w.ray_o[i], d = w.ray_d[i];
+			float len = o.w;
+			hit_t h;
+			if (!trace_one<false, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris)) {
+				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+				h.slot = -1;
+			}
+			w.hit[i] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
+		}
+	}
+	if (COUNT) {
+		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
+		warp_add64(w.counters, CNT_TRI_TESTS, tris);
+	}
+}
+
+__global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w, film_buffers f, uint32_t queue_in) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool push_shadow = false, push_mis = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = q[k];
+			path_state st = load_path(w, p, i);
+			shade_record& rec = w.rec[i];
+			shade_record r;
+			const bool alive = shade_a(s, st, to_hit(w.hit[i]), r);
+			if (!alive) {
+				film_add(f, w.pixel[i], st.L);
+				st.flags |= 0x80000000u;  // ended in shade_a; shade_b skips it
+			} else {
+				push_shadow = r.nee_entity >= 0;
+				push_mis = r.mis_valid != 0;
+				if (push_shadow) {
+					w.sec_o[2 * i] = make_float4(r.shadow_ray.o.x, r.shadow_ray.o.y, r.shadow_ray.o.z, r.shadow_ray.len);
+					w.sec_d[2 * i] = make_float4(r.shadow_ray.d.x, r.shadow_ray.d.y, r.shadow_ray.d.z, 0.f);
+				}
+				if (push_mis) {
+					w.sec_o[2 * i + 1] = make_float4(r.mis_ray.o.x, r.mis_ray.o.y, r.mis_ray.o.z, r.mis_ray.len);
+					w.sec_d[2 * i + 1] = make_float4(r.mis_ray.d.x, r.mis_ray.d.y, r.mis_ray.d.z, 0.f);
+				}
+			}
+			rec = r;
+			store_path(w, i, st);
+		}
+		warp_push(push_shadow, 2 * i, w.sec_queue, w.counters + CNT_SECONDARY);
+		warp_push(push_mis, 2 * i + 1, w.sec_queue, w.counters + CNT_SECONDARY);
+		const uint32_t ns = __popc(__ballot_sync(0xffffffffu, push_shadow));
+		const uint32_t nm = __popc(__ballot_sync(0xffffffffu, push_mis));
+		if ((threadIdx.x & 31u) == 0) {
+			if (ns) add64(w.counters, CNT_SHADOW_RAYS, ns);
+			if (nm) add64(w.counters, CNT_MIS_RAYS, nm);
+		}
+	}
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st{smem + threadIdx.x, blockDim.x, 0u, stack_cap};
+	const uint32_t n = w.counters[CNT_SECONDARY];
+	uint32_t nodes = 0, tris = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		if (k < n) {
+			const uint32_t j = w.sec_queue[k];
+			const float4 o = w.sec_o[j], d = w.sec_d[j];
+			float len = o.w;
+			hit_t h;
+			if (!trace_one<true, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris)) {
+				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+				h.slot = -1;
+			}
+			w.sec_hit[j] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
+		}
+	}
+	if (COUNT) {
+		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
+		warp_add64(w.counters, CNT_TRI_TESTS, tris);
+	}
+}
+
+__global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, film_buffers f, uint32_t queue_in) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	uint32_t* qn = w.queue[queue_in ^ 1u];
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool alive = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = q[k];
+			path_state st = load_path(w, p, i);
+			if (!(st.flags & 0x80000000u)) {
+				const shade_record& rec = w.rec[i];
+				const hit_t sh = to_hit(w.sec_hit[2 * i]);
+				const hit_t mh = to_hit(w.sec_hit[2 * i + 1]);
+				alive = shade_b(s, st, rec, sh, mh, p.max_depth, p.rr_threshold);
+				if (!alive) film_add(f, w.pixel[i], st.L);
+				store_path(w, i, st);
+			}
+		}
+		warp_push(alive, i, qn, w.counters + CNT_NEXT);
+	}
+}
+
+// Moves the next queue's count into place and accumulates the extend-ray count.
+__global__ void k_advance(uint32_t* counters) {
+	add64(counters, CNT_EXTEND_RAYS, counters[CNT_ACTIVE]);
+	counters[CNT_ACTIVE] = counters[CNT_NEXT];
+	counters[CNT_NEXT] = 0u;
+	counters[CNT_SECONDARY] = 0u;
+}
+
+// Moves the wave window forward so the next replay of the same graph renders
+// the following work items.
+__global__ void k_next_wave(wave_params* p, uint32_t capacity) { p->first_item += capacity; }
+
+template <bool COUNT>
+cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
+	const launch_cfg& cfg, cudaStream_t stream) {
+	const size_t smem = static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	k_extend<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	k_shade_a<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, f, queue_in);
+	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	k_shade_b<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, f, queue_in);
+	k_advance<<<1, 1, 0, stream>>>(w.counters);
+	return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t launch_trace_rays(const scene_view& s, const uint32_t* prim_entity, const rb_ray* rays, uint32_t n, rb_hit* hits,
+	bool shadow, const launch_cfg& cfg, uint32_t* counters, cudaStream_t stream) {
+	if (n == 0) return cudaSuccess;
+	const size_t smem = static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	const uint32_t blocks_needed = (n + cfg.block_trace - 1) / cfg.block_trace;
+	const int grid = static_cast<int>(blocks_needed < static_cast<uint32_t>(cfg.grid_trace) ? blocks_needed : cfg.grid_trace);
+	if (shadow) {
+		if (cfg.count) k_trace_rays<true, true><<<grid, cfg.block_trace, smem, stream>>>(s, prim_entity, rays, n, hits, cfg.stack_depth, counters);
+		else k_trace_rays<true, false><<<grid, cfg.block_trace, smem, stream>>>(s, prim_entity, rays, n, hits, cfg.stack_depth, counters);
+	} else {
+		if (cfg.count) k_trace_rays<false, true><<<grid, cfg.block_trace, smem, stream>>>(s, prim_entity, rays, n, hits, cfg.stack_depth, counters);
+		else k_trace_rays<false, false><<<grid, cfg.block_trace, smem, stream>>>(s, prim_entity, rays, n, hits, cfg.stack_depth, counters);
+	}
+	return cudaGetLastError();
+}
+
+cudaError_t launch_bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
+	const launch_cfg& cfg, cudaStream_t stream) {
+	return cfg.count ? bounce<true>(s, w, f, queue_in, cfg, stream) : bounce<false>(s, w, f, queue_in, cfg, stream);
+}
+
+cudaError_t launch_wave(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t max_depth,
+	uint32_t first_queue, const launch_cfg& cfg, cudaStream_t stream) {
+	k_camera<<<cfg.grid_shade, 256, 0, stream>>>(w, first_queue);
+	cudaError_t err = cudaGetLastError();
+	uint32_t qi = first_queue;
+	for (uint32_t b = 0; b < max_depth && err == cudaSuccess; b++) {
+		err = launch_bounce(s, w, f, qi, cfg, stream);
+		qi ^= 1u;
+	}
+	return err;
+}
+
+cudaError_t launch_next_wave(const wave_buffers& w, cudaStream_t stream) {
+	k_next_wave<<<1, 1, 0, stream>>>(w.params, w.capacity);
+	return cudaGetLastError();
+}
+
+} // namespace gpu
+} // namespace rb

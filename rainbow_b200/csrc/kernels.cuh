@@ -1,0 +1,93 @@
+// Kernel launchers of the wavefront path tracer (kernels.cu).
+#pragma once
+
+#include "../../include/rbgpu.h"
+#include "pt/pt_path.h"
+
+#include <cuda_runtime.h>
+
+namespace rb {
+namespace gpu {
+
+// Device-side counters of one context. Indices into device_counters::c.
+enum : uint32_t {
+	CNT_ACTIVE = 0,      // paths in the current active queue
+	CNT_NEXT = 1,        // paths pushed to the next active queue
+	CNT_SECONDARY = 2,   // secondary rays queued this bounce
+	CNT_ERROR = 3,       // first device error (rb_status), 0 if none
+	CNT_EXTEND_RAYS = 4, // 64-bit stats, two words each (lo, hi) from here on
+	CNT_SHADOW_RAYS = 6,
+	CNT_MIS_RAYS = 8,
+	CNT_NODE_VISITS = 10,
+	CNT_TRI_TESTS = 12,
+	CNT_WORDS = 16
+};
+
+// Per-launch wave parameters, read by the kernels from device memory so a
+// captured graph can be replayed for every wave.
+struct wave_params {
+	float r2c[16];
+	float c2w[16];
+	float lens, focus;
+	uint32_t width, height;
+	uint64_t first_item;     // first work item of the wave (item = sample_offset * pixels + pixel)
+	uint64_t total_items;    // pixels * spp of this render call
+	uint32_t first_sample;
+	uint32_t seed;
+	uint32_t max_depth;
+	float rr_threshold;
+};
+
+// Path state of one wave, structure of arrays over `capacity` paths.
+struct wave_buffers {
+	uint32_t capacity;
+	float4* ray_o;           // o.xyz, length
+	float4* ray_d;           // d.xyz, unused
+	float4* beta;            // beta.xyz, eta
+	float4* radiance;        // L.xyz, flags (bits)
+	int32_t* bounces;
+	unsigned long long* rng; // PCG32 state; the increment is rebuilt from the stream seed
+	uint32_t* pixel;
+	uint32_t* sample;
+	float4* hit;             // slot (bits), t, b1, b2
+	pt::shade_record* rec;
+	float4* sec_o;           // 2 per path: shadow ray, MIS ray
+	float4* sec_d;
+	float4* sec_hit;
+	uint32_t* queue[2];      // active queues (ping-pong)
+	uint32_t* sec_queue;
+	uint32_t* counters;
+	wave_params* params;
+};
+
+struct film_buffers {
+	double* sum;             // 3 per pixel
+	double* sum_sq;          // 3 per pixel
+	uint32_t* count;         // samples per pixel
+};
+
+struct launch_cfg {
+	int grid_trace, grid_shade;
+	int block_trace, block_shade;
+	int stack_depth;         // traversal stack entries per thread (32 or 64)
+	bool count;              // node / triangle counting
+};
+
+// Ray batches for rb_trace_closest / rb_trace_shadow.
+cudaError_t launch_trace_rays(const pt::scene_view& s, const uint32_t* prim_entity, const rb_ray* rays, uint32_t n,
+	rb_hit* hits, bool shadow, const launch_cfg& cfg, uint32_t* counters, cudaStream_t stream);
+
+// One wave: camera rays then `max_depth` bounces of
+// extend -> shade_a -> secondary trace -> shade_b -> advance.
+cudaError_t launch_wave(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t max_depth,
+	uint32_t first_queue, const launch_cfg& cfg, cudaStream_t stream);
+
+// Advances params->first_item by the wave capacity (the last node of a wave).
+cudaError_t launch_next_wave(const wave_buffers& w, cudaStream_t stream);
+
+// One extra bounce (used when invisible entities make paths outlive max_depth iterations).
+cudaError_t launch_bounce(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
+	const launch_cfg& cfg, cudaStream_t stream);
+
+} // namespace gpu
+} // namespace rb

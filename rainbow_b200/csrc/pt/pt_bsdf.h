@@ -1,0 +1,418 @@
+// BSDFs of the three supported materials and the lobe-collection rules of
+// scattering_function_collection (rainbow-cpu/scatterings/scattering_function_collection.cpp:29-148).
+// All directions are in the shading frame (z = shading normal). Host- and
+// device-compilable, reference operation order throughout.
+#pragma once
+
+#include "pt_types.h"
+
+namespace rb {
+namespace pt {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTwoPi = 6.28318530717958647692f;
+constexpr float kHalfPi = 1.57079632679489661923f;
+constexpr float kQuarterPi = 0.785398163397448309616f;
+constexpr float kInvPi = 0.318309886183790671538f;
+constexpr float kInvTwoPi = 0.159154943091895335769f;
+constexpr float kOneMinusEps = 1.f - FLT_EPSILON;
+
+// scattering_type bits (rainbow-cpu/scatterings/scattering_function.hpp:26-34)
+enum : uint32_t {
+	ST_REFLECTION = 1u << 0,
+	ST_TRANSMISSION = 1u << 1,
+	ST_SPECULAR = 1u << 2,
+	ST_DIFFUSE = 1u << 3,
+	ST_GLOSSY = 1u << 4,
+	ST_ALL = 31u,
+	ST_NON_SPECULAR = ST_ALL ^ ST_SPECULAR
+};
+RB_HD bool type_match(uint32_t target, uint32_t flag) { return (target & flag) == flag; }
+
+// ------------------------------------------------------------------ shading-frame trigonometry
+// rainbow-core/shading_function.cpp:3-127
+RB_HD float cos2_theta(vec3 w) { return w.z * w.z; }
+RB_HD float sin2_theta(vec3 w) { return fmax_ref(0.f, 1.f - cos2_theta(w)); }
+RB_HD float sin_theta(vec3 w) { return sqrtf(sin2_theta(w)); }
+RB_HD float tan_theta(vec3 w) { return sin_theta(w) / w.z; }
+RB_HD float tan2_theta(vec3 w) { return sin2_theta(w) / cos2_theta(w); }
+RB_HD float cos_phi(vec3 w) {
+	const float s = sin_theta(w);
+	return s == 0.f ? 1.f : fclamp_ref(w.x / s, -1.f, 1.f);
+}
+RB_HD float sin_phi(vec3 w) {
+	const float s = sin_theta(w);
+	return s == 0.f ? 0.f : fclamp_ref(w.y / s, -1.f, 1.f);
+}
+RB_HD bool same_hemisphere(vec3 a, vec3 b) { return a.z * b.z > 0.f; }
+RB_HD vec3 face_forward(vec3 v, vec3 f) { return dot(v, f) > 0.f ? v : -v; }
+RB_HD vec3 reflect(vec3 wi, vec3 n) { return -wi + 2.f * dot(wi, n) * n; }
+RB_HD vec3 refract(vec3 wi, vec3 n, float eta) {
+	const float ci = dot(wi, n);
+	const float s2i = fmax_ref(0.f, 1.f - ci * ci);
+	const float s2o = s2i * eta * eta;
+	if (s2o >= 1.f) return vec3{0.f, 0.f, 0.f};
+	const float co = sqrtf(1.f - s2o);
+	return -wi * eta + (ci * eta - co) * n;
+}
+
+// rainbow-core/sample_function.cpp:15-44
+RB_HD vec2 concentric_disk(vec2 u) {
+	const vec2 r = 2.f * u - vec2{1.f, 1.f};
+	if (r.x == 0.f && r.y == 0.f) return vec2{0.f, 0.f};
+	float theta, rad;
+	if (fabs_ref(r.x) > fabs_ref(r.y)) {
+		rad = r.x;
+		theta = kQuarterPi * (r.y / r.x);
+	} else {
+		rad = r.y;
+		theta = kHalfPi - kQuarterPi * (r.x / r.y);
+	}
+	return rad * vec2{cosf(theta), sinf(theta)};
+}
+RB_HD vec3 cosine_hemisphere(vec2 u) {
+	const vec2 d = concentric_disk(u);
+	const float z = sqrtf(fmax_ref(0.f, 1.f - dot(d, d)));
+	return vec3{d.x, d.y, z};
+}
+RB_HD float cosine_hemisphere_pdf(float c) { return c * kInvPi; }
+
+// ------------------------------------------------------------------ Trowbridge-Reitz
+// rainbow-cpu/scatterings/distribution/trowbridge_reitz_distribution.cpp and
+// microfacet_distribution.cpp (visible-normal sampling enabled).
+RB_HD float tr_d(float ax, float ay, vec3 wh) {
+	const float t2 = tan2_theta(wh);
+	if (isinf(t2)) return 0.f;
+	const float c4 = cos2_theta(wh) * cos2_theta(wh);
+	const float cp = cos_phi(wh), sp = sin_phi(wh);
+	const float e = (cp * cp / (ax * ax) + sp * sp / (ay * ay)) * t2;
+	return 1.f / (kPi * ax * ay * c4 * (1.f + e) * (1.f + e));
+}
+RB_HD float tr_lambda(float ax, float ay, vec3 w) {
+	const float at = fabs_ref(tan_theta(w));
+	if (isinf(at)) return 0.f;
+	const float cp = cos_phi(w), sp = sin_phi(w);
+	const float alpha = sqrtf(cp * cp * ax * ax + sp * sp * ay * ay);
+	const float a2 = (alpha * at) * (alpha * at);
+	return (-1.f + sqrtf(1.f + a2)) / 2.f;
+}
+RB_HD float tr_g(float ax, float ay, vec3 wo, vec3 wi) { return 1.f / (1.f + tr_lambda(ax, ay, wo) + tr_lambda(ax, ay, wi)); }
+RB_HD float tr_g1(float ax, float ay, vec3 w) { return 1.f / (1.f + tr_lambda(ax, ay, w)); }
+RB_HD float tr_pdf(float ax, float ay, vec3 wo, vec3 wh) {
+	return tr_d(ax, ay, wh) * tr_g1(ax, ay, wo) * fabs_ref(dot(wo, wh)) / fabs_ref(wo.z);
+}
+
+// trowbridge_reitz_sample(cos_theta, u1, u2): slope sampling of the isotropic
+// distribution, including its rational approximation of the inverse CDF (:7-45).
+RB_HD vec2 tr_sample11(float cos_t, float u1, float u2) {
+	if (static_cast<double>(cos_t) > 0.9999) {
+		const float r = sqrtf(u1 / (1.f - u1));
+		const float phi = kTwoPi * u2;
+		return vec2{r * cosf(phi), r * sinf(phi)};
+	}
+	const float sin_t = sqrtf(fmax_ref(0.f, 1.f - cos_t * cos_t));
+	const float tan_t = sin_t / cos_t;
+	const float a = 1.f / tan_t;
+	const float g1 = 2.f / (1.f + sqrtf(1.f + 1.f / (a * a)));
+	const float A = 2.f * u1 / g1 - 1.f;
+	float tmp = 1.f / (A * A - 1.f);
+	if (static_cast<double>(tmp) > 1e10) tmp = 1e10f;
+	const float B = tan_t;
+	const float D = sqrtf(fmax_ref(B * B * tmp * tmp - (A * A - B * B) * tmp, 0.f));
+	const float sx1 = B * tmp - D;
+	const float sx2 = B * tmp + D;
+	vec2 slope;
+	slope.x = (A < 0.f || sx2 > 1.f / tan_t) ? sx1 : sx2;
+	float S;
+	if (u2 > 0.5f) {
+		S = 1.f;
+		u2 = 2.f * (u2 - .5f);
+	} else {
+		S = -1.f;
+		u2 = 2.f * (.5f - u2);
+	}
+	const float z = (u2 * (u2 * (u2 * 0.27385f - 0.73369f) + 0.46341f)) /
+		(u2 * (u2 * (u2 * 0.093073f + 0.309420f) - 1.000000f) + 0.597999f);
+	slope.y = S * z * sqrtf(1.f + slope.x * slope.x);
+	return slope;
+}
+RB_HD vec3 tr_sample_visible(vec3 wi, float ax, float ay, float u1, float u2) {
+	const vec3 ws = normalize(vec3{ax * wi.x, ay * wi.y, wi.z});
+	vec2 slope = tr_sample11(ws.z, u1, u2);
+	const float tmp = cos_phi(ws) * slope.x - sin_phi(ws) * slope.y;
+	slope.y = sin_phi(ws) * slope.x + cos_phi(ws) * slope.y;
+	slope.x = tmp;
+	slope.x = ax * slope.x;
+	slope.y = ay * slope.y;
+	return normalize(vec3{-slope.x, -slope.y, 1.f});
+}
+RB_HD vec3 tr_sample(float ax, float ay, vec3 wo, vec2 u) {
+	const bool flip = wo.z < 0.f;
+	const vec3 wh = tr_sample_visible(flip ? -wo : wo, ax, ay, u.x, u.y);
+	return flip ? -wh : wh;
+}
+
+// ------------------------------------------------------------------ Fresnel
+// rainbow-cpu/scatterings/fresnel_effect.cpp:5-58
+RB_HD float fresnel_dielectric(float cos_i, float eta_i, float eta_o) {
+	cos_i = fclamp_ref(cos_i, -1.f, 1.f);
+	if (cos_i < 0.f) {
+		const float t = eta_i; eta_i = eta_o; eta_o = t;
+		cos_i = fabs_ref(cos_i);
+	}
+	const float sin_i = sqrtf(fmax_ref(0.f, 1.f - cos_i * cos_i));
+	const float sin_o = sin_i * eta_i / eta_o;
+	const float cos_o = sqrtf(fmax_ref(0.f, 1.f - sin_o * sin_o));
+	if (sin_o >= 1.f) return 1.f;
+	const float r0 = (eta_o * cos_i - eta_i * cos_o) / (eta_o * cos_i + eta_i * cos_o);
+	const float r1 = (eta_i * cos_i - eta_o * cos_o) / (eta_i * cos_i + eta_o * cos_o);
+	return (r0 * r0 + r1 * r1) / 2.f;
+}
+// conductor with eta_i = 1 (metal_material.cpp:29), one channel
+RB_HD float fresnel_conductor1(float cos_i, float eta, float k) {
+	cos_i = fclamp_ref(cos_i, -1.f, 1.f);
+	const float e = eta / 1.f, ek = k / 1.f;
+	const float c2 = cos_i * cos_i;
+	const float s2 = 1.f - c2;
+	const float e2 = e * e, ek2 = ek * ek;
+	const float t0 = e2 - ek2 - s2;
+	const float ab = sqrtf(t0 * t0 + e2 * ek2 * 4.f);
+	const float t1 = ab + c2;
+	const float a = sqrtf((ab + t0) * 0.5f);
+	const float t2 = a * 2.f * cos_i;
+	const float t3 = ab * c2 + s2 * s2;
+	const float t4 = t2 * s2;
+	const float r0 = (t1 - t2) / (t1 + t2);
+	const float r1 = r0 * (t3 - t4) / (t3 + t4);
+	return (r0 + r1) * 0.5f;
+}
+RB_HD spectrum fresnel_conductor(float cos_i, spectrum eta, spectrum k) {
+	const float c = fabs_ref(cos_i);
+	return spectrum{fresnel_conductor1(c, eta.x, k.x), fresnel_conductor1(c, eta.y, k.y), fresnel_conductor1(c, eta.z, k.z)};
+}
+
+// ------------------------------------------------------------------ lobes
+struct lobe_sample {
+	uint32_t type;
+	spectrum f;
+	vec3 wi;
+	float pdf;
+};
+RB_HD lobe_sample no_sample() { return lobe_sample{0u, spectrum{0.f, 0.f, 0.f}, vec3{0.f, 0.f, 0.f}, 0.f}; }
+
+// Lobe kinds in collection order for each material.
+enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, LOBE_FRESNEL_SPECULAR = 3 };
+
+struct bsdf_t {
+	uint32_t kinds[2];
+	uint32_t types[2];
+	uint32_t count;
+	const material_rec* m;
+	float eta;  // collection eta (glass IOR, else 1)
+};
+
+RB_HD bsdf_t make_bsdf(const material_rec* m) {
+	bsdf_t b;
+	b.m = m;
+	b.count = 0;
+	b.eta = 1.f;
+	switch (m->kind) {
+	case MAT_LAMBERT:
+		b.kinds[0] = LOBE_LAMBERT; b.types[0] = ST_DIFFUSE | ST_REFLECTION; b.count = 1;
+		break;
+	case MAT_METAL:
+		b.kinds[0] = LOBE_MF_REFLECT; b.types[0] = ST_GLOSSY | ST_REFLECTION; b.count = 1;
+		break;
+	case MAT_GLASS_ROUGH:
+		b.eta = m->eta;
+		if (m->has_reflect) { b.kinds[b.count] = LOBE_MF_REFLECT; b.types[b.count] = ST_GLOSSY | ST_REFLECTION; b.count++; }
+		if (m->has_transmit) { b.kinds[b.count] = LOBE_MF_TRANSMIT; b.types[b.count] = ST_GLOSSY | ST_TRANSMISSION; b.count++; }
+		break;
+	case MAT_GLASS_SMOOTH:
+		b.eta = m->eta;
+		if (m->has_reflect || m->has_transmit) {
+			b.kinds[0] = LOBE_FRESNEL_SPECULAR; b.types[0] = ST_REFLECTION | ST_TRANSMISSION | ST_SPECULAR; b.count = 1;
+		}
+		break;
+	default: break;  // black matte: no lobes
+	}
+	return b;
+}
+
+RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi) {
+	const float co = fabs_ref(wo.z), ci = fabs_ref(wi.z);
+	vec3 wh = wi + wo;
+	if (co == 0.f || ci == 0.f) return spectrum{0.f, 0.f, 0.f};
+	if (wh.x == 0.f && wh.y == 0.f && wh.z == 0.f) return spectrum{0.f, 0.f, 0.f};
+	wh = face_forward(normalize(wh), vec3{0.f, 0.f, 1.f});
+	spectrum F, R;
+	if (m->kind == MAT_METAL) {
+		F = fresnel_conductor(dot(wi, wh), m->cond_eta, m->cond_k);
+		R = spectrum{1.f, 1.f, 1.f};
+	} else {
+		F = splat3(fresnel_dielectric(dot(wi, wh), 1.f, m->eta));
+		R = m->reflectance;
+	}
+	const float G = tr_g(m->alpha_x, m->alpha_y, wo, wi);
+	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
+	return R * (G * D) * F / (4.f * ci * co);
+}
+RB_HD float mf_reflect_pdf(const material_rec* m, vec3 wo, vec3 wi) {
+	if (!same_hemisphere(wo, wi)) return 0.f;
+	const vec3 wh = normalize(wo + wi);
+	return tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh));
+}
+RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi) {
+	if (same_hemisphere(wo, wi)) return spectrum{0.f, 0.f, 0.f};
+	const float co = wo.z, ci = wi.z;
+	if (co == 0.f || ci == 0.f) return spectrum{0.f, 0.f, 0.f};
+	const bool entering = co > 0.f;
+	const float eta = entering ? (m->eta / 1.f) : (1.f / m->eta);
+	const vec3 wh = face_forward(normalize(wo + wi * eta), vec3{0.f, 0.f, 1.f});
+	const float F = fresnel_dielectric(dot(wo, wh), 1.f, m->eta);
+	const float denom = dot(wo, wh) + eta * dot(wi, wh);
+	const float factor = 1.f / eta;
+	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
+	const float G = tr_g(m->alpha_x, m->alpha_y, wo, wi);
+	const float v = fabs_ref(D * G * eta * eta * fabs_ref(dot(wi, wh)) * fabs_ref(dot(wo, wh) * factor * factor) /
+		(ci * co * denom * denom));
+	return (splat3(1.f) - splat3(F)) * m->transmission * v;
+}
+RB_HD float mf_transmit_pdf(const material_rec* m, vec3 wo, vec3 wi) {
+	if (same_hemisphere(wo, wi)) return 0.f;
+	const bool entering = wo.z > 0.f;
+	const float eta = entering ? (m->eta / 1.f) : (1.f / m->eta);
+	const vec3 wh = normalize(wo + wi * eta);
+	const float denom = dot(wo, wh) + eta * dot(wi, wh);
+	return tr_pdf(m->alpha_x, m->alpha_y, wo, wh) * fabs_ref((eta * eta * dot(wi, wh)) / (denom * denom));
+}
+
+RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
+	switch (b.kinds[i]) {
+	case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
+	case LOBE_MF_REFLECT: return mf_reflect_f(b.m, wo, wi);
+	case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
+	default: return spectrum{0.f, 0.f, 0.f};
+	}
+}
+RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
+	switch (b.kinds[i]) {
+	case LOBE_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
+	case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
+	case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
+	default: return 0.f;
+	}
+}
+RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+	const material_rec* m = b.m;
+	switch (b.kinds[i]) {
+	case LOBE_LAMBERT: {
+		vec3 wi = cosine_hemisphere(u);
+		if (wo.z < 0.f) wi.z = -wi.z;
+		return lobe_sample{b.types[i], lobe_f(b, i, wo, wi), wi, lobe_pdf(b, i, wo, wi)};
+	}
+	case LOBE_MF_REFLECT: {
+		if (wo.z == 0.f) return no_sample();
+		const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
+		if (dot(wo, wh) < 0.f) return no_sample();
+		const vec3 wi = reflect(wo, wh);
+		if (!same_hemisphere(wo, wi)) return no_sample();
+		return lobe_sample{b.types[i], mf_reflect_f(m, wo, wi), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
+	}
+	case LOBE_MF_TRANSMIT: {
+		if (wo.z == 0.f) return no_sample();
+		const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
+		if (dot(wo, wh) < 0.f) return no_sample();
+		const bool entering = wo.z > 0.f;
+		const float eta = entering ? (1.f / m->eta) : (m->eta / 1.f);
+		const vec3 wi = refract(wo, wh, eta);
+		if (is_zero(wi)) return no_sample();
+		return lobe_sample{b.types[i], mf_transmit_f(m, wo, wi), wi, mf_transmit_pdf(m, wo, wi)};
+	}
+	case LOBE_FRESNEL_SPECULAR: {
+		// fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
+		const float F = fresnel_dielectric(wo.z, 1.f, m->eta);
+		if (u.x < F) {
+			const vec3 wi{-wo.x, -wo.y, wo.z};
+			return lobe_sample{ST_REFLECTION | ST_SPECULAR, m->reflectance * F / fabs_ref(wi.z), wi, F};
+		}
+		const bool entering = wo.z > 0.f;
+		const float ei = entering ? 1.f : m->eta;
+		const float eo = entering ? m->eta : 1.f;
+		const vec3 wi = refract(wo, face_forward(vec3{0.f, 0.f, 1.f}, wo), ei / eo);
+		if (is_zero(wi)) return no_sample();
+		const float factor = (ei * ei) / (eo * eo);
+		const spectrum v = m->transmission * (splat3(1.f) - splat3(F)) * factor / fabs_ref(wi.z);
+		return lobe_sample{ST_TRANSMISSION | ST_SPECULAR, v, wi, 1.f - F};
+	}
+	default: return no_sample();
+	}
+}
+
+// ------------------------------------------------------------------ collection
+// scattering_function_collection::evaluate (:29-46)
+RB_HD spectrum bsdf_f(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
+	if (wo.z == 0.f) return spectrum{0.f, 0.f, 0.f};
+	const uint32_t rt = same_hemisphere(wo, wi) ? ST_REFLECTION : ST_TRANSMISSION;
+	spectrum f{0.f, 0.f, 0.f};
+	for (uint32_t i = 0; i < b.count; i++)
+		if (type_match(include, b.types[i]) && type_match(b.types[i], rt)) f = f + lobe_f(b, i, wo, wi);
+	return f;
+}
+// scattering_function_collection::pdf (:131-148)
+RB_HD float bsdf_pdf(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
+	if (b.count == 0 || wo.z == 0.f) return 0.f;
+	uint32_t n = 0;
+	float pdf = 0.f;
+	for (uint32_t i = 0; i < b.count; i++)
+		if (type_match(include, b.types[i])) {
+			pdf = pdf + lobe_pdf(b, i, wo, wi);
+			n++;
+		}
+	return n != 0 ? pdf / static_cast<float>(n) : 0.f;
+}
+RB_HD uint32_t bsdf_count(const bsdf_t& b, uint32_t include) {
+	uint32_t n = 0;
+	for (uint32_t i = 0; i < b.count; i++)
+		if (type_match(include, b.types[i])) n++;
+	return n;
+}
+// scattering_function_collection::sample (:48-100) with wo already in the
+// shading frame; the returned wi is in the shading frame too.
+RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include) {
+	uint32_t idx[2];
+	uint32_t n = 0;
+	for (uint32_t i = 0; i < b.count; i++)
+		if (type_match(include, b.types[i])) idx[n++] = i;
+	if (n == 0) return no_sample();
+	const float fn = static_cast<float>(n);
+	uint32_t which = static_cast<uint32_t>(floorf(u.x * fn));
+	if (which > n - 1) which = n - 1;
+	const float rx = u.x * fn - static_cast<float>(which);
+	const vec2 ur{(kOneMinusEps < rx) ? kOneMinusEps : rx, u.y};
+	if (wo.z == 0.f) return no_sample();
+	lobe_sample s = lobe_sample_dir(b, idx[which], wo, ur);
+	if (s.pdf == 0.f) return no_sample();
+	if (!type_match(s.type, ST_SPECULAR)) {
+		const uint32_t rt = same_hemisphere(wo, s.wi) ? ST_REFLECTION : ST_TRANSMISSION;
+		s.f = spectrum{0.f, 0.f, 0.f};
+		s.pdf = 0.f;
+		for (uint32_t k = 0; k < n; k++) {
+			const uint32_t i = idx[k];
+			if (type_match(b.types[i], rt)) s.f = s.f + lobe_f(b, i, wo, s.wi);
+			s.pdf = s.pdf + lobe_pdf(b, i, wo, s.wi);
+		}
+	}
+	s.pdf = s.pdf / fn;
+	return s;
+}
+
+// trowbridge_reitz_distribution::roughness_to_alpha (:128-137); host-side use.
+RB_HD float roughness_to_alpha(float roughness) {
+	roughness = fmax_ref(roughness, 1e-3f);
+	const float x = logf(roughness);
+	return 1.62142f + 0.819955f * x + 0.1734f * x * x + 0.0171201f * x * x * x + 0.000640711f * x * x * x * x;
+}
+
+} // namespace pt
+} // namespace rb

@@ -1,0 +1,326 @@
+// Ray/scene geometry of the wavefront path tracer: world<->entity ray
+// transforms, slab and triangle tests, the closest-hit traversal in the
+// reference's visiting order, surface-interaction construction and ray spawning.
+// Host- and device-compilable; every float operation keeps the reference's order.
+#pragma once
+
+#include "pt_types.h"
+
+namespace rb {
+namespace pt {
+
+#if defined(__CUDA_ARCH__)
+#define RB_LDG(p) __ldg(p)
+#else
+#define RB_LDG(p) (*(p))
+#endif
+
+struct ray_t {
+	vec3 o, d;
+	float len;
+};
+
+// ray_epsilon / shadow_epsilon (rainbow-cpu/shared/ray.hpp:10-11)
+constexpr float kRayEpsilon = FLT_EPSILON / 2 * 1500;
+constexpr float kShadowEpsilon = kRayEpsilon * 10;
+constexpr float kInf = __builtin_huge_valf();
+
+// ------------------------------------------------------------------ entity frames
+// The ray as entity::intersect sees it (rainbow-cpu/scenes/entity.cpp:18-37 with
+// transform::operator()(ray), transform.cpp:94-105): direction normalised twice
+// (once by the transform, once by the ray constructor), local length = world
+// length * |W2L d|, and back: world length = local t * |L2W d_local|.
+struct local_ray {
+	vec3 o, d;
+	float to_local;   // |W2L d|
+	float to_world;   // |L2W d_local|
+};
+
+RB_HD local_ray make_local_ray(const float* w2l, const float* l2w, vec3 o, vec3 d) {
+	local_ray r;
+	const vec3 dl = xform_vector(w2l, d);
+	r.to_local = length(dl);
+	r.d = normalize(normalize(dl));
+	r.o = xform_point(w2l, o);
+	r.to_world = length(xform_vector(l2w, r.d));
+	return r;
+}
+
+// ------------------------------------------------------------------ tests
+// Slab test of bounding_box<T>::intersect (detail/accelerator.hpp:29-53) with
+// t1 = the ray's current length. inv = 1 / direction per axis.
+// fminf/fmaxf give the same outcome as glm's ternary min/max here: t0 and t1
+// are never NaN, and a NaN slab bound is ignored by both.
+RB_HD bool slab_hit(float4 a, float4 b, vec3 o, vec3 inv, float len) {
+	float t0 = 0.f, t1 = len;
+	float n = (a.x - o.x) * inv.x, f = (a.w - o.x) * inv.x;
+	if (n > f) { const float t = n; n = f; f = t; }
+	t0 = fmaxf(t0, n); t1 = fminf(t1, f);
+	if (t0 > t1) return false;
+	n = (a.y - o.y) * inv.y; f = (b.x - o.y) * inv.y;
+	if (n > f) { const float t = n; n = f; f = t; }
+	t0 = fmaxf(t0, n); t1 = fminf(t1, f);
+	if (t0 > t1) return false;
+	n = (a.z - o.z) * inv.z; f = (b.y - o.z) * inv.z;
+	if (n > f) { const float t = n; n = f; f = t; }
+	t0 = fmaxf(t0, n); t1 = fminf(t1, f);
+	return !(t0 > t1);
+}
+
+// Moller-Trumbore of mesh::intersect_with_triangle (rainbow-cpu/shapes/mesh.cpp:328-348).
+RB_HD bool triangle_hit(vec3 o, vec3 d, float len, vec3 p0, vec3 e1, vec3 e2, float& t, float& b1, float& b2) {
+	const vec3 pv = cross(d, e2);
+	const vec3 tv = o - p0;
+	const vec3 qv = cross(tv, e1);
+	const float inv_det = 1.f / dot(e1, pv);
+	b1 = dot(tv, pv) * inv_det;
+	b2 = dot(d, qv) * inv_det;
+	const float b0 = 1.f - b1 - b2;
+	t = dot(e2, qv) * inv_det;
+	if (t <= 0.f || t >= len) return false;
+	if (b0 < 0.f || b0 > 1.f) return false;
+	if (b1 < 0.f || b1 > 1.f) return false;
+	if (b2 < 0.f || b2 > 1.f) return false;
+	return true;
+}
+
+// ------------------------------------------------------------------ closest hit
+struct hit_t {
+	int32_t slot;  // prim slot, -1 on a miss
+	float b1, b2;
+};
+
+struct trace_counters {
+	uint32_t nodes, tris;
+};
+
+constexpr uint32_t kEntityInvisible = 0x80000000u;  // flag in the tri_c entity word
+
+RB_HD float u32_as_float(uint32_t v) {
+#if defined(__CUDA_ARCH__)
+	return __uint_as_float(v);
+#else
+	float f;
+	__builtin_memcpy(&f, &v, 4);
+	return f;
+#endif
+}
+RB_HD uint32_t float_as_u32(float f) {
+#if defined(__CUDA_ARCH__)
+	return __float_as_uint(f);
+#else
+	uint32_t v;
+	__builtin_memcpy(&v, &f, 4);
+	return v;
+#endif
+}
+
+// Closest hit in the visiting order of bounding_volume_hierarchy<T>::intersect
+// (detail/bounding_volume_hierarchy.hpp:60-108): pop a node, slab-test it
+// against the current length, test a leaf's triangles in order, otherwise push
+// the far child then the near child (near = right when the ray's direction is
+// negative on the split axis). SHADOW skips invisible entities
+// (intersect_with_shadow_ray, :110-160). `len` is updated in place like the
+// reference's mutable ray.length. Stack provides push/pop/empty/full.
+// Returns false when the stack overflowed (the hit is then incomplete).
+template <bool SHADOW, bool COUNT, typename Stack>
+RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack, trace_counters& cnt) {
+	const vec3 inv = 1.f / d;
+	const bool neg[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+	hit.slot = -1;
+	uint32_t cur_entity = 0xffffffffu;
+	local_ray lr{};
+	stack.reset();
+	stack.push(0u);
+	while (!stack.empty()) {
+		const uint32_t n = stack.pop();
+		const float4 a = RB_LDG(s.nodes + 2 * n);
+		const float4 b = RB_LDG(s.nodes + 2 * n + 1);
+		if (COUNT) cnt.nodes++;
+		if (!slab_hit(a, b, o, inv, len)) continue;
+		const uint32_t w0 = float_as_u32(b.z), w1 = float_as_u32(b.w);
+		if (w1 & RB_BVH_LEAF_FLAG) {
+			const uint32_t count = w1 & ~RB_BVH_LEAF_FLAG;
+			for (uint32_t k = 0; k < count; k++) {
+				const uint32_t slot = w0 + k;
+				const float2 tc = RB_LDG(s.tri_c + slot);
+				const uint32_t ew = float_as_u32(tc.y);
+				if (SHADOW && (ew & kEntityInvisible)) continue;
+				const uint32_t ent = ew & ~kEntityInvisible;
+				const float4 ta = RB_LDG(s.tri_a + slot);
+				const float4 tb = RB_LDG(s.tri_b + slot);
+				if (ent != cur_entity) {
+					cur_entity = ent;
+					lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
+				}
+				if (COUNT) cnt.tris++;
+				float t, b1, b2;
+				if (triangle_hit(lr.o, lr.d, len * lr.to_local, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y},
+						vec3{tb.z, tb.w, tc.x}, t, b1, b2)) {
+					len = t * lr.to_world;
+					hit.slot = static_cast<int32_t>(slot);
+					hit.b1 = b1;
+					hit.b2 = b2;
+				}
+			}
+			continue;
+		}
+		const uint32_t left = n + 1, right = w0;
+		if (stack.full()) return false;
+		if (neg[w1]) { stack.push(left); stack.push(right); }
+		else { stack.push(right); stack.push(left); }
+	}
+	return true;
+}
+
+// ------------------------------------------------------------------ surface interaction
+// World-space surface interaction of a hit: mesh::intersect_with_triangle's
+// interaction (mesh.cpp:350-441) taken to world space by
+// transform::operator()(surface_interaction) (transform.cpp:38-50).
+struct surface_t {
+	vec3 p;        // point
+	vec3 n;        // geometric normal, face-forwarded to the shading normal
+	vec3 sx, sy, sz;
+	vec3 wo;
+	int32_t entity;
+};
+
+RB_HD vec3 load3(const float* a, uint32_t i) { return vec3{a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
+
+// coordinate_system(normal) (rainbow-cpu/shared/coordinate_system.cpp:8-23)
+RB_HD void frame_from_normal(vec3 normal, vec3& x, vec3& y, vec3& z) {
+	z = normalize(normal);
+	if (fabs_ref(z.x) > fabs_ref(z.y)) x = vec3{-z.z, 0.f, z.x} / sqrtf(z.x * z.x + z.z * z.z);
+	else x = vec3{0.f, z.z, -z.y} / sqrtf(z.y * z.y + z.z * z.z);
+	y = cross(z, x);
+}
+
+// Local interaction pieces of one triangle at barycentrics (b1, b2).
+struct local_surface {
+	vec3 p, n, sx, sy, sz;
+};
+
+RB_HD local_surface triangle_surface(const scene_view& s, const mesh_rec& m, uint32_t tri, float b1, float b2) {
+	const uint32_t* idx = s.indices + m.index_offset + 3 * tri;
+	const uint32_t i0 = m.vertex_offset + idx[0], i1 = m.vertex_offset + idx[1], i2 = m.vertex_offset + idx[2];
+	const vec3 p0 = load3(s.positions, i0), p1 = load3(s.positions, i1), p2 = load3(s.positions, i2);
+	vec3 uv0{0.f, 0.f, 0.f}, uv1{1.f, 0.f, 0.f}, uv2{1.f, 1.f, 0.f};
+	if (m.flags & MESH_HAS_UVS) { uv0 = load3(s.uvs, i0); uv1 = load3(s.uvs, i1); uv2 = load3(s.uvs, i2); }
+	const bool reverse = (m.flags & MESH_REVERSE) != 0;
+	const vec3 e1 = p1 - p0, e2 = p2 - p0;
+	const float b0 = 1.f - b1 - b2;
+	local_surface out;
+	out.p = p0 * b0 + p1 * b1 + p2 * b2;
+	const vec3 normal = reverse ? -normalize(cross(e1, e2)) : normalize(cross(e1, e2));
+	const vec3 duv02 = uv0 - uv2, duv12 = uv1 - uv2;
+	const vec3 dp02 = p0 - p2, dp12 = p1 - p2;
+	const float determinant = duv02.x * duv12.y - duv02.y * duv12.x;
+	const float inv_determinant = 1.f / determinant;
+	vec3 dp_du = (duv12.y * dp02 - duv02.y * dp12) * inv_determinant;
+	vec3 dp_dv = (-duv12.x * dp02 + duv02.x * dp12) * inv_determinant;
+	// abs(determinant) < 1e-8 compares in double (a double literal in mesh.cpp:385)
+	if (static_cast<double>(fabs_ref(determinant)) < 1e-8 || length(cross(dp_du, dp_dv)) == 0.f) {
+		vec3 fx, fy, fz;
+		frame_from_normal(normal, fx, fy, fz);
+		dp_du = fx;
+		dp_dv = fy;
+	}
+	vec3 z = normal;
+	if (m.flags & MESH_HAS_NORMALS) {
+		z = b0 * load3(s.normals, i0) + b1 * load3(s.normals, i1) + b2 * load3(s.normals, i2);
+		if (reverse) z = z * -1.f;
+		if (length_squared(z) <= 0.f) z = normal;
+	}
+	vec3 x = dp_du;
+	if (m.flags & MESH_HAS_TANGENTS) {
+		x = b0 * load3(s.tangents, i0) + b1 * load3(s.tangents, i1) + b2 * load3(s.tangents, i2);
+		if (reverse) x = x * -1.f;
+		if (length_squared(x) <= 0.f) x = dp_du;
+	}
+	x = normalize(x);
+	z = normalize(z);
+	vec3 y = cross(z, x);
+	if (length_squared(y) > 0.f) {
+		y = normalize(y);
+		x = normalize(cross(y, z));
+	} else {
+		frame_from_normal(z, x, y, z);
+	}
+	out.sx = x;
+	out.sy = y;
+	out.sz = z;
+	out.n = dot(normal, z) > 0.f ? normal : -normal;  // face_forward(normal, shading z)
+	return out;
+}
+
+// World interaction of hit (slot, b1, b2) on a ray with world direction d.
+RB_HD surface_t make_surface(const scene_view& s, int32_t slot, float b1, float b2, vec3 o, vec3 d) {
+	const float2 tc = s.tri_c[slot];
+	const uint32_t ent = float_as_u32(tc.y) & ~kEntityInvisible;
+	const entity_rec& e = s.entities[ent];
+	const local_ray lr = make_local_ray(e.w2l, e.l2w, o, d);
+	const local_surface ls = triangle_surface(s, s.meshes[e.mesh], s.prim_index[slot], b1, b2);
+	surface_t out;
+	// transform::operator()(coordinate_system) (transform.cpp:62-76)
+	vec3 x = xform_vector(e.l2w, ls.sx);
+	vec3 y = xform_vector(e.l2w, ls.sy);
+	const vec3 z = normalize(cross(x, y));
+	x = normalize(x);
+	y = normalize(cross(z, x));
+	out.sx = x;
+	out.sy = y;
+	out.sz = z;
+	out.n = xform_normal(e.w2l, ls.n);
+	out.p = xform_point(e.l2w, ls.p);
+	out.wo = normalize(xform_vector(e.l2w, -lr.d));
+	out.entity = static_cast<int32_t>(ent);
+	return out;
+}
+
+// ------------------------------------------------------------------ spawning
+RB_HD float next_toward(float x, bool up) {
+	// std::nextafter(x, up ? FLT_MAX : FLT_MIN): FLT_MIN is the smallest positive
+	// normal, so a value below it moves up (interaction.cpp:40-42).
+	return nextafterf(x, up ? FLT_MAX : FLT_MIN);
+}
+
+// offset_ray_origin (rainbow-cpu/shared/interactions/interaction.cpp:25-46)
+RB_HD vec3 offset_origin(vec3 p, vec3 n, vec3 dir) {
+	const float scale = kRayEpsilon * (1.f + max_component(vabs(p)));
+	vec3 off = scale * n;
+	if (dot(n, dir) < 0.f) off = -off;
+	vec3 q = p + off;
+	q.x = next_toward(q.x, off.x > 0.f);
+	q.y = next_toward(q.y, off.y > 0.f);
+	q.z = next_toward(q.z, off.z > 0.f);
+	return q;
+}
+
+// interaction::spawn_ray: ray(direction, offset origin) -> the constructor normalises.
+RB_HD ray_t spawn_ray(vec3 p, vec3 n, vec3 dir) {
+	ray_t r;
+	r.o = offset_origin(p, n, dir);
+	r.d = normalize(dir);
+	r.len = kInf;
+	return r;
+}
+
+// interaction::spawn_ray_to (interaction.cpp:17-23)
+RB_HD ray_t spawn_ray_to(vec3 p, vec3 n, vec3 target) {
+	ray_t r;
+	r.o = offset_origin(p, n, normalize(target - p));
+	const vec3 dir = target - r.o;
+	r.d = normalize(normalize(dir));
+	r.len = length(dir) - kShadowEpsilon;
+	return r;
+}
+
+// world_to_local / local_to_world of a coordinate_system (coordinate_system.cpp:66-78)
+RB_HD vec3 to_local(const surface_t& si, vec3 v) { return vec3{dot(v, si.sx), dot(v, si.sy), dot(v, si.sz)}; }
+RB_HD vec3 to_world(const surface_t& si, vec3 l) {
+	return vec3{si.sx.x * l.x + si.sy.x * l.y + si.sz.x * l.z, si.sx.y * l.x + si.sy.y * l.y + si.sz.y * l.z,
+		si.sx.z * l.x + si.sy.z * l.y + si.sz.z * l.z};
+}
+
+} // namespace pt
+} // namespace rb

@@ -1,0 +1,227 @@
+// Per-path stages of path_integrator::trace (rainbow-cpu/integrators/path_integrator.cpp:15-47)
+// split at the two points where the reference traces a ray in the middle of
+// shading. One bounce is:
+//   extend   closest hit of the path ray                    (scene::intersect)
+//   shade_a  environment / emission / pass-through; when the BSDF has a
+//            non-specular lobe: emitter pick (1D), light sample (2D) and the
+//            MIS BSDF sample (2D) of uniform_sample_one_emitter
+//            (integrator.cpp:101-201) -> a shadow ray and an MIS ray
+//   trace    both secondary rays, visible entities only (intersect_with_shadow_ray)
+//   shade_b  resolve the shadow test and find_emitter (integrator.cpp:49-82,
+//            drawing the environment pick (1D) only when the MIS ray misses),
+//            path BSDF sample (2D), throughput/eta update, spawn, Russian
+//            roulette (1D) exactly as path_integrator::trace orders them.
+// Splitting there keeps the reference's per-sample random-number order.
+#pragma once
+
+#include "pt_light.h"
+
+namespace rb {
+namespace pt {
+
+enum : uint32_t { PATH_SPECULAR = 1u << 0 };
+
+struct path_state {
+	vec3 o, d;
+	float len;
+	spectrum beta, L;
+	float eta;
+	uint32_t flags;
+	int32_t bounces;
+	pcg32 rng;
+};
+
+// Everything shade_b needs from shade_a.
+struct shade_record {
+	surface_t si;
+	uint32_t material;
+	uint32_t pass_through;        // invisible entity: continue straight on
+	uint32_t did_nee;             // uniform_sample_one_emitter was called
+	int32_t nee_entity;           // emitter entity of the shadow ray, -1: no shadow ray
+	spectrum nee_L;               // its contribution if unoccluded
+	uint32_t mis_valid;
+	uint32_t mis_specular;
+	vec3 mis_wi;                  // world direction of the MIS BSDF sample
+	spectrum mis_f;               // f * |cos|
+	float mis_pdf;
+	ray_t shadow_ray, mis_ray;
+};
+
+// perspective_camera::sample(position, u) (rainbow-cpu/cameras/perspective_camera.cpp:78-99)
+// for pixel (x, y): position = (x, y) + film sample, then the lens sample.
+RB_HD ray_t camera_ray(const float* r2c, const float* c2w, float lens, float focus, uint32_t x, uint32_t y, pcg32& rng) {
+	const vec2 f = pcg_2d(rng);
+	const vec2 lu = pcg_2d(rng);
+	const float px = static_cast<float>(x) + f.x, py = static_cast<float>(y) + f.y;
+	const vec3 target = xform_point(r2c, vec3{px, py, 0.f});
+	vec3 o{0.f, 0.f, 0.f};
+	vec3 d = normalize(normalize(target));
+	if (lens > 0.f) {
+		const vec3 fp = o + d * (focus / d.z);
+		const vec2 l = concentric_disk(lu) * lens;
+		o = vec3{l.x, l.y, 0.f};
+		d = normalize(fp - o);
+	}
+	const vec3 dw = xform_vector(c2w, d);
+	ray_t r;
+	r.d = normalize(normalize(dw));
+	r.o = xform_point(c2w, o);
+	r.len = kInf * length(dw);
+	return r;
+}
+
+RB_HD void path_begin(path_state& p, const float* r2c, const float* c2w, float lens, float focus, uint32_t x, uint32_t y,
+	uint32_t pixel, uint32_t sample, uint32_t seed) {
+	p.rng = pcg_seed(stream_seed(pixel, sample, seed));
+	const ray_t r = camera_ray(r2c, c2w, lens, focus, x, y, p.rng);
+	p.o = r.o;
+	p.d = r.d;
+	p.len = r.len;
+	p.beta = splat3(1.f);
+	p.L = splat3(0.f);
+	p.eta = 1.f;
+	p.flags = 0u;
+	p.bounces = 0;
+}
+
+RB_HD uint32_t hit_entity(const scene_view& s, int32_t slot) {
+	return float_as_u32(s.tri_c[slot].y) & ~kEntityInvisible;
+}
+
+// Returns false when the path ends here (a miss).
+RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_record& rec) {
+	rec.pass_through = 0u;
+	rec.did_nee = 0u;
+	rec.nee_entity = -1;
+	rec.mis_valid = 0u;
+	const bool count_emission = p.bounces == 0 || (p.flags & PATH_SPECULAR);
+	if (h.slot < 0) {
+		// sample_surface_interaction, miss branch (integrator.cpp:333-346)
+		if (count_emission)
+			for (uint32_t i = 0; i < s.num_environments; i++) p.L = p.L + p.beta * s.emitters[s.environments[i]].radiance;
+		return false;
+	}
+	rec.si = make_surface(s, h.slot, h.b1, h.b2, p.o, p.d);
+	const surface_t& si = rec.si;
+	const entity_rec& ent = s.entities[si.entity];
+	if (count_emission && (ent.flags & ENT_HAS_EMITTER))
+		p.L = p.L + p.beta * surface_emission(ent, s.emitters[ent.emitter], si.n, -p.d);
+	if (!(ent.flags & ENT_HAS_MATERIAL)) {
+		const ray_t r = spawn_ray(si.p, si.n, p.d);
+		p.o = r.o;
+		p.d = r.d;
+		p.len = r.len;
+		p.bounces--;
+		rec.pass_through = 1u;
+		return true;
+	}
+	rec.material = static_cast<uint32_t>(ent.material);
+	const bsdf_t b = make_bsdf(s.materials + ent.material);
+	if (bsdf_count(b, ST_NON_SPECULAR) == 0) return true;
+	rec.did_nee = 1u;
+	const vec3 wo = to_local(si, si.wo);
+	// emitter sampling half (integrator.cpp:121-159)
+	const float n = static_cast<float>(s.num_emitters);
+	uint32_t which = static_cast<uint32_t>(floorf(pcg_real(p.rng) * n));
+	if (which > s.num_emitters - 1) which = s.num_emitters - 1;
+	const float pick_pdf = 1.f / n;
+	const emitter_rec& em = s.emitters[which];
+	light_sample ls = sample_emitter(s, em, si.p, si.n, pcg_2d(p.rng));
+	ls.pdf = ls.pdf * pick_pdf;
+	if (!is_black(ls.L) && ls.pdf > 0.f) {
+		const vec3 wi = to_local(si, ls.wi);
+		spectrum f = bsdf_f(b, wo, wi, ST_NON_SPECULAR);
+		const float fpdf = bsdf_pdf(b, wo, wi, ST_NON_SPECULAR);
+		f = f * fabs_ref(dot(ls.wi, si.sz));
+		if (!is_black(f) && fpdf > 0.f) {
+			rec.shadow_ray = spawn_ray_to(si.p, si.n, ls.p);
+			const float w = power_heuristic(ls.pdf, fpdf);
+			rec.nee_L = f * ls.L * w / ls.pdf;
+			rec.nee_entity = em.entity;
+		}
+	}
+	// BSDF sampling half (integrator.cpp:161-198)
+	const lobe_sample bs = bsdf_sample(b, wo, pcg_2d(p.rng), ST_NON_SPECULAR);
+	const vec3 wi_w = bs.pdf > 0.f ? to_world(si, bs.wi) : vec3{0.f, 0.f, 0.f};
+	const spectrum v = bs.f * fabs_ref(dot(wi_w, si.sz));
+	if (!is_black(v) && bs.pdf > 0.f) {
+		rec.mis_valid = 1u;
+		rec.mis_specular = type_match(bs.type, ST_SPECULAR) ? 1u : 0u;
+		rec.mis_wi = wi_w;
+		rec.mis_f = v;
+		rec.mis_pdf = bs.pdf;
+		rec.mis_ray = spawn_ray(si.p, si.n, wi_w);
+	}
+	return true;
+}
+
+// Returns false when the path ends (BSDF sample failed, Russian roulette, max depth).
+// shadow / mis are the closest visible hits of rec.shadow_ray / rec.mis_ray.
+RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, const hit_t& shadow, const hit_t& mis,
+	uint32_t max_depth, float rr_threshold) {
+	if (!rec.pass_through) {
+		const surface_t& si = rec.si;
+		if (rec.did_nee) {
+			spectrum Ls = splat3(0.f);
+			if (rec.nee_entity >= 0 && (shadow.slot < 0 || hit_entity(s, shadow.slot) == static_cast<uint32_t>(rec.nee_entity)))
+				Ls = Ls + rec.nee_L;
+			if (rec.mis_valid) {
+				// find_emitter (integrator.cpp:49-82) and the MIS term (:165-195)
+				bool found = false;
+				spectrum Le = splat3(0.f);
+				float epdf = 0.f;
+				const float pick_pdf = 1.f / static_cast<float>(s.num_emitters);
+				if (mis.slot >= 0) {
+					const uint32_t e = hit_entity(s, mis.slot);
+					const entity_rec& ent = s.entities[e];
+					if (ent.flags & ENT_HAS_EMITTER) {
+						const surface_t es = make_surface(s, mis.slot, mis.b1, mis.b2, rec.mis_ray.o, rec.mis_ray.d);
+						const emitter_rec& em = s.emitters[ent.emitter];
+						Le = surface_emission(ent, em, es.n, -rec.mis_wi);
+						epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
+						found = true;
+					}
+				} else if (s.num_environments > 0) {
+					const float ne = static_cast<float>(s.num_environments);
+					uint32_t which = static_cast<uint32_t>(floorf(pcg_real(p.rng) * ne));
+					if (which > s.num_environments - 1) which = s.num_environments - 1;
+					const emitter_rec& em = s.emitters[s.environments[which]];
+					Le = em.radiance;
+					epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
+					found = true;
+				}
+				if (found && !is_black(Le) && epdf > 0.f) {
+					const float w = rec.mis_specular ? 1.f : power_heuristic(rec.mis_pdf, epdf);
+					Ls = Ls + rec.mis_f * Le * w / rec.mis_pdf;
+				}
+			}
+			p.L = p.L + p.beta * Ls;
+		}
+		// path continuation (integrator.cpp:380-399)
+		const bsdf_t b = make_bsdf(s.materials + rec.material);
+		const vec3 wo = to_local(si, si.wo);
+		const lobe_sample bs = bsdf_sample(b, wo, pcg_2d(p.rng), ST_ALL);
+		if (is_black(bs.f) || bs.pdf == 0.f) return false;
+		const vec3 wi = to_world(si, bs.wi);
+		p.beta = p.beta * (bs.f * fabs_ref(dot(wi, si.sz)) / bs.pdf);
+		p.flags = type_match(bs.type, ST_SPECULAR) ? (p.flags | PATH_SPECULAR) : (p.flags & ~PATH_SPECULAR);
+		if (type_match(bs.type, ST_SPECULAR | ST_TRANSMISSION))
+			p.eta = p.eta * ((dot(si.wo, si.n) > 0.f) ? (b.eta * b.eta) : (1.f / (b.eta * b.eta)));
+		const ray_t r = spawn_ray(si.p, si.n, wi);
+		p.o = r.o;
+		p.d = r.d;
+		p.len = r.len;
+	}
+	// Russian roulette (path_integrator.cpp:35-43)
+	const float mc = spectrum_max(p.beta * p.eta);
+	if (mc < rr_threshold && p.bounces > 3) {
+		const float q = fmax_ref(0.05f, 1.f - mc);
+		if (pcg_real(p.rng) < q) return false;
+		p.beta = p.beta / (1.f - q);
+	}
+	p.bounces++;
+	return p.bounces < static_cast<int32_t>(max_depth);
+}
+
+} // namespace pt
+} // namespace rb

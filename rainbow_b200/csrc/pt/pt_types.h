@@ -1,0 +1,162 @@
+// Scene records, the PCG32 sampler stream and spectrum helpers of the
+// wavefront path tracer. Host- and device-compilable.
+#pragma once
+
+#include "../rb_math.h"
+
+#include <vector_types.h>  // float2 / float4 (CUDA headers, also usable from host C++)
+
+#include <float.h>
+#include <stdint.h>
+
+namespace rb {
+namespace pt {
+
+using spectrum = vec3;  // RGB color_spectrum (rainbow-cpu/shared/spectrums/color_spectrum.cpp:58-70)
+
+RB_HD bool is_black(spectrum s) { return s.x == 0.f && s.y == 0.f && s.z == 0.f; }
+// coefficient_spectrum::max_component: m = max(m, c) with glm's max.
+RB_HD float spectrum_max(spectrum s) { return fmax_ref(fmax_ref(s.x, s.y), s.z); }
+
+// ------------------------------------------------------------------ PCG32
+// pcg32 (rainbow-cpu/shared/random_generator.cpp:41-85): seed -> inc = seed << 1 | 1,
+// state = 0, step, state += default state, step. XSH-RR output.
+struct pcg32 {
+	uint64_t state;
+	uint64_t inc;
+};
+constexpr uint64_t kPcgDefaultState = 0x853c49e6748fea9bULL;
+constexpr uint64_t kPcgMult = 0x5851f42d4c957f2dULL;
+
+RB_HD uint32_t pcg_next(pcg32& g) {
+	const uint64_t old = g.state;
+	g.state = old * kPcgMult + g.inc;
+	const uint32_t xs = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+	const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+	return (xs >> rot) | (xs << ((~rot + 1u) & 31u));
+}
+RB_HD pcg32 pcg_seed(uint64_t seed) {
+	pcg32 g;
+	g.state = 0u;
+	g.inc = (seed << 1u) | 1u;
+	pcg_next(g);
+	g.state += kPcgDefaultState;
+	pcg_next(g);
+	return g;
+}
+// uniform_real: min(1 - eps, float(u32) * 2^-32), with std::min's (b < a) ? b : a.
+RB_HD float pcg_real(pcg32& g) {
+	const float v = static_cast<float>(pcg_next(g)) * 2.3283064365386963e-10f;
+	const float one_minus_eps = 1.f - FLT_EPSILON;
+	return (v < one_minus_eps) ? v : one_minus_eps;
+}
+RB_HD vec2 pcg_2d(pcg32& g) {
+	const float a = pcg_real(g);
+	const float b = pcg_real(g);
+	return vec2{a, b};
+}
+
+// Seed of the stream of one (pixel, sample): pixel in bits 0-23, sample in
+// bits 24-47, render seed in bits 48-62. The reference instead shares one
+// stream across a 16x16 tile (sampler_integrator.cpp:94-96); per-sample streams
+// make every sample independent of the launch order.
+RB_HD uint64_t stream_seed(uint32_t pixel, uint32_t sample, uint32_t seed) {
+	return static_cast<uint64_t>(pixel & 0xffffffu) | (static_cast<uint64_t>(sample & 0xffffffu) << 24) |
+		(static_cast<uint64_t>(seed & 0x7fffu) << 48);
+}
+
+// ------------------------------------------------------------------ scene records
+enum : uint32_t {
+	ENT_HAS_SHAPE = 1u << 0,
+	ENT_HAS_MATERIAL = 1u << 1,
+	ENT_HAS_EMITTER = 1u << 2,
+	ENT_VISIBLE = 1u << 3  // shape and material (entity::visible, entity.cpp:80-83)
+};
+
+struct entity_rec {
+	float l2w[16];
+	float w2l[16];
+	int32_t mesh;
+	int32_t material;
+	int32_t emitter;      // index into the emitter table, -1 if none
+	uint32_t flags;
+	float area;           // shape_instance_properties::area (world-space area)
+	int32_t pad[3];
+};
+
+enum : uint32_t {
+	MESH_HAS_NORMALS = 1u << 0,
+	MESH_HAS_TANGENTS = 1u << 1,
+	MESH_HAS_UVS = 1u << 2,
+	MESH_REVERSE = 1u << 3
+};
+
+struct mesh_rec {
+	uint32_t vertex_offset;   // into the vertex arrays (in vertices)
+	uint32_t index_offset;    // into the index array (in indices)
+	uint32_t num_triangles;
+	uint32_t flags;
+};
+
+enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4 };
+
+struct material_rec {
+	uint32_t kind;
+	float alpha_x, alpha_y;   // Trowbridge-Reitz alphas (roughness_to_alpha applied on the host)
+	float eta;                // glass IOR
+	spectrum diffuse;         // lambert reflectance
+	spectrum reflectance;     // glass reflectance
+	spectrum transmission;    // glass transmission
+	spectrum cond_eta;        // conductor eta
+	spectrum cond_k;          // conductor k
+	uint32_t has_reflect;     // glass: reflectance not black
+	uint32_t has_transmit;    // glass: transmission not black
+};
+
+enum : uint32_t { EMIT_SURFACE = 0, EMIT_ENVIRONMENT = 1 };
+
+struct emitter_rec {
+	uint32_t kind;
+	int32_t entity;           // owning entity ordinal
+	spectrum radiance;        // surface radiance / environment intensity
+	float radius;             // environment radius
+};
+
+// 2x2 piecewise-constant distribution of a constant environment map
+// (environment_light.cpp:20-36, distribution.hpp:48-141), precomputed on the host.
+struct env_distribution {
+	float cdf_row[2][3];      // conditional CDFs of the two rows
+	float value_row[2][2];
+	float integral_row[2];
+	float cdf_marg[3];        // marginal CDF
+	float value_marg[2];
+	float integral_marg;
+};
+
+// Flat view of an uploaded scene; pointers are device pointers in kernels and
+// host pointers in host-side use.
+struct scene_view {
+	const float4* nodes;          // 2 per node: (min.xyz, max.x), (max.y, max.z, w0, w1)
+	const float4* tri_a;          // per prim slot: (p0.xyz, e1.x)        entity-local space
+	const float4* tri_b;          // (e1.y, e1.z, e2.x, e2.y)
+	const float2* tri_c;          // (e2.z, entity as bits)
+	const uint32_t* prim_index;   // triangle index within its mesh
+	const entity_rec* entities;
+	const mesh_rec* meshes;
+	const float* positions;       // 3 per vertex
+	const float* normals;
+	const float* tangents;
+	const float* uvs;
+	const uint32_t* indices;
+	const material_rec* materials;
+	const emitter_rec* emitters;  // scene->emitters() order
+	const int32_t* environments;  // emitter indices of the environment emitters
+	env_distribution env;
+	uint32_t num_nodes;
+	uint32_t num_emitters;
+	uint32_t num_environments;
+	uint32_t num_entities;
+};
+
+} // namespace pt
+} // namespace rb

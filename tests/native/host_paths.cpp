@@ -1,0 +1,112 @@
+// Test-only host build of the kernels' per-path functions (rainbow_b200/csrc/pt/*.h).
+//
+// The device code of the path tracer is written as __host__ __device__
+// functions. This file compiles them for the CPU, with glibc's libm (the same
+// library the compiled reference uses), and drives them one sample at a time,
+// so a test can check the stage logic and its random-number order against the
+// reference bit for bit without a GPU. It is not reachable from the library:
+// librbgpu.so has no CPU path.
+#include "../../include/rbgpu.h"
+#include "../../rainbow_b200/csrc/host/scene_pack.h"
+#include "../../rainbow_b200/csrc/pt/pt_path.h"
+
+#include <new>
+
+using namespace rb;
+using namespace rb::pt;
+
+namespace {
+
+struct host_stack {
+	uint32_t data[128];
+	uint32_t sp = 0;
+	void reset() { sp = 0; }
+	void push(uint32_t v) { data[sp++] = v; }
+	uint32_t pop() { return data[--sp]; }
+	bool empty() const { return sp == 0; }
+	bool full() const { return sp + 2 > 128; }
+};
+
+struct hp_scene {
+	host::packed_scene packed;
+	scene_view view;
+};
+
+hit_t trace(const scene_view& v, vec3 o, vec3 d, float& len, bool shadow) {
+	host_stack st;
+	trace_counters c{0, 0};
+	hit_t h;
+	if (shadow) closest_hit<true, false>(v, o, d, len, h, st, c);
+	else closest_hit<false, false>(v, o, d, len, h, st, c);
+	return h;
+}
+
+} // namespace
+
+extern "C" {
+
+int hp_create(const rb_scene_desc* desc, void** out) {
+	auto* s = new (std::nothrow) hp_scene();
+	if (!s) return RB_ERR_OUT_OF_MEMORY;
+	const rb_status st = host::pack_scene(desc, s->packed);
+	if (st != RB_OK) {
+		delete s;
+		return st;
+	}
+	s->view = host::host_view(s->packed);
+	*out = s;
+	return RB_OK;
+}
+
+void hp_free(void* s) { delete static_cast<hp_scene*>(s); }
+
+int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {
+	const hp_scene& s = *static_cast<hp_scene*>(hs);
+	for (uint32_t i = 0; i < n; i++) {
+		float len = rays[i].length;
+		const hit_t h = trace(s.view, vec3{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]},
+			vec3{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]}, len, shadow != 0);
+		hits[i].entity = h.slot >= 0 ? static_cast<int32_t>(s.packed.prim_entity[h.slot]) : -1;
+		hits[i].triangle = h.slot >= 0 ? static_cast<int32_t>(s.packed.prim_index[h.slot]) : -1;
+		hits[i].t = len;
+		hits[i].b1 = h.slot >= 0 ? h.b1 : 0.f;
+		hits[i].b2 = h.slot >= 0 ? h.b2 : 0.f;
+	}
+	return RB_OK;
+}
+
+// Radiance of (pixel, sample) pairs through the same stage sequence the
+// kernels run: camera, then per bounce extend -> shade_a -> secondary rays -> shade_b.
+int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples, uint32_t n,
+	uint32_t max_depth, float rr, uint32_t seed, float* out) {
+	const hp_scene& s = *static_cast<hp_scene*>(hs);
+	for (uint32_t i = 0; i < n; i++) {
+		const uint32_t pixel = pixels[i];
+		const uint32_t x = pixel % static_cast<uint32_t>(cam->width), y = pixel / static_cast<uint32_t>(cam->width);
+		path_state p;
+		path_begin(p, cam->raster_to_camera, cam->camera_to_world, cam->lens_radius, cam->focus_distance, x, y, pixel,
+			samples[i], seed);
+		for (int guard = 0; guard < 4096; guard++) {
+			float len = p.len;
+			const hit_t h = trace(s.view, p.o, p.d, len, false);
+			shade_record rec;
+			if (!shade_a(s.view, p, h, rec)) break;
+			hit_t sh{-1, 0.f, 0.f}, mh{-1, 0.f, 0.f};
+			if (rec.nee_entity >= 0) {
+				float l = rec.shadow_ray.len;
+				sh = trace(s.view, rec.shadow_ray.o, rec.shadow_ray.d, l, true);
+			}
+			if (rec.mis_valid) {
+				float l = rec.mis_ray.len;
+				mh = trace(s.view, rec.mis_ray.o, rec.mis_ray.d, l, true);
+			}
+			if (!shade_b(s.view, p, rec, sh, mh, max_depth, rr)) break;
+		}
+		out[3 * i] = p.L.x;
+		out[3 * i + 1] = p.L.y;
+		out[3 * i + 2] = p.L.z;
+	}
+	return RB_OK;
+}
+
+} // extern "C"
