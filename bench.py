@@ -1,0 +1,296 @@
+"""Benchmark of the wavefront path tracer on one or more B200s.
+
+Workload (the metric's single-GPU configuration): the seeded sphere scene of
+1,024,010 FP32 triangles (200 displaced icospheres at subdivision 4 over a
+ground quad; 40% Lambert / 30% Trowbridge-Reitz conductor / 30% dielectric; 4
+quad lights and a constant environment of 0.5), 1024 x 1024 pixels, max depth 8,
+Russian roulette as the reference applies it. Inputs are synthetic (seeded
+generator), standing in for the configuration's procedural scene.
+
+A step is one pass of the hot path over one batch: one sample of every pixel
+(1,048,576 paths, all bounces, with NEE shadow and MIS rays). `value` is
+Msamples/s over the K timed steps measured with CUDA events on the launching
+stream (inputs resident in HBM); `e2e` is the same metric through the public C
+ABI with the step's parameters copied in and the film read back to host memory
+every step. L2 is flushed (a 256 MiB write) before every timed step.
+
+--impl reference times the reference CPU integrator (path_integrator::trace of
+the reference sources, compiled as oracle/_ref) on a bounded sample of each step
+on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(kind=1, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4, max_depth=8)
+METRIC = "time to relMSE 0.01: guided vs plain wavefront PT on 1 B200; Msamples/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference_rate(scene, rows, spp, threads, first_sample=0):
+    """Msamples/s of the reference integrator (oracle/_ref) on image rows [rows[0], rows[1])."""
+    from oracle import ref
+    R = ref.RefScene(scene)
+    _, _, sec = R.render(spp, first_sample, WORKLOAD["max_depth"], 1.0, 0, threads, rows=rows)
+    samples = (rows[1] - rows[0]) * scene.camera.width * spp
+    return samples / sec / 1e6, sec, samples
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import rainbow_b200 as rb
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liboracle_ref.so not built"}))
+        return 0
+    scene = rb.generate_scene(WORKLOAD["kind"], seed=WORKLOAD["seed"], width=WORKLOAD["width"],
+                              height=WORKLOAD["height"], num_spheres=WORKLOAD["num_spheres"],
+                              subdivision=WORKLOAD["subdivision"])
+    threads = os.cpu_count() or 1
+    rows = args.ref_rows
+    r0 = (WORKLOAD["height"] - rows) // 2
+    band = (r0, r0 + rows)
+    R = ref.RefScene(scene)
+    for k in range(args.warmup):
+        R.render(1, 10_000 + k, WORKLOAD["max_depth"], 1.0, 0, threads, rows=(r0, r0 + max(1, rows // 4)))
+    total_s, total_samples = 0.0, 0
+    for k in range(args.steps):
+        _, _, sec = R.render(1, k, WORKLOAD["max_depth"], 1.0, 0, threads, rows=band)
+        total_s += sec
+        total_samples += rows * scene.camera.width
+    value = total_samples / total_s / 1e6
+    sample = f"rows {band[0]}-{band[1] - 1} of the 1024x1024 image, 1 spp per step ({rows * 1024} paths)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_dict(world, l2="n/a (CPU)"),
+        "cpu_baseline": {"value": value, "unit": "Msamples/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def config_dict(world, l2="flushed before every timed step (256 MiB write)"):
+    return {"workload": "sphere field, 1,024,010 triangles, 1024x1024, 1 spp per step, max depth 8",
+            "triangles": 1024010, "width": WORKLOAD["width"], "height": WORKLOAD["height"],
+            "max_depth": WORKLOAD["max_depth"], "spp_per_step": 1, "parallelism": f"replicas x{world} (sample ranges)",
+            "l2": l2}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=32)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-rows", type=int, default=64, help="image rows per step timed on the CPU reference")
+    ap.add_argument("--cpu-rows", type=int, default=512, help="rows (a central band) of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import rainbow_b200 as rb
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    scene = rb.generate_scene(WORKLOAD["kind"], seed=WORKLOAD["seed"], width=WORKLOAD["width"],
+                              height=WORKLOAD["height"], num_spheres=WORKLOAD["num_spheres"],
+                              subdivision=WORKLOAD["subdivision"])
+    W, H, depth = scene.camera.width, scene.camera.height, WORKLOAD["max_depth"]
+    pixels = W * H
+    ctx = rb.Context(local)
+    ctx.upload(scene)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # each rank renders its own range of sample indices (weak scaling, no data-path collective)
+    base = rank * (args.steps + args.warmup + 8)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        ctx.render(scene.camera, spp=1, first_sample=base + args.steps + k, max_depth=depth, reset=(k == 0),
+                   want_image=False)
+
+    # ---- device-timed steps (value)
+    launches = 0
+    device_ms = 0.0
+    rays = 0
+    barrier()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ctx.render(scene.camera, spp=1, first_sample=base + k, max_depth=depth, reset=(k == 0), want_image=False)
+            st = ctx.stats()
+            device_ms += st.elapsed_ms
+            launches += st.kernel_launches
+            rays += st.extend_rays + st.shadow_rays + st.mis_rays
+        barrier()
+    t = torch.tensor([device_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps * pixels / (max_ms / 1e3) / 1e6
+    mrays = world * rays / (max_ms / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with host buffers (params in, film out every step)
+    img = np.zeros((H, W, 3), dtype=np.float32)
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        p = rb.RenderParams()
+        p.camera = scene.camera
+        p.spp, p.first_sample, p.max_depth, p.rr_threshold, p.seed = 1, base + k, depth, 1.0, 0
+        p.flags = rb.RB_RENDER_RESET if k == 0 else 0
+        rb.check(rb.lib().rb_render(ctx._h, ctypes.byref(p), img.ctypes.data), "rb_render")
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * pixels / float(tt.item()) / 1e6
+    h2d = 176  # wave parameter block copied in per call
+    d2h = pixels * (3 * 8 + 4)  # FP64 sums and counts read back per call
+
+    # ---- roofline of the traversal kernels (separate untimed passes of the same step)
+    ctx.set_counting(True)
+    ctx.render(scene.camera, spp=1, first_sample=base, max_depth=depth, reset=True, want_image=False)
+    cst = ctx.stats()
+    ctx.set_counting(False)
+    ctx.set_profiling(True)
+    ctx.render(scene.camera, spp=1, first_sample=base, max_depth=depth, reset=True, want_image=False)
+    pst = ctx.stats()
+    ctx.set_profiling(False)
+    trav_rays = cst.extend_rays + cst.shadow_rays + cst.mis_rays
+    alg_bytes = 32 * cst.node_visits + 40 * cst.triangle_tests + 48 * trav_rays
+    trav_ms = pst.extend_ms + pst.secondary_ms
+    nl = max(1, pst.extend_launches + pst.secondary_launches)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / (trav_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traversal_sphere_field.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+            if ref.available():
+                threads = os.cpu_count() or 1
+                r0 = (H - args.cpu_rows) // 2
+                v, sec, n = cpu_reference_rate(scene, (r0, r0 + args.cpu_rows), 1, threads)
+                cpu = {"value": v, "unit": "Msamples/s", "cores": threads, "kind": "reference",
+                       "sample": f"rows {r0}-{r0 + args.cpu_rows - 1} of the image at 1 spp ({n} paths, {sec:.1f} s)"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": config_dict(world), "mrays_per_s": mrays,
+            "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_extend + k_trace_secondary (BVH traversal)",
+                         "algorithmic_bytes_per_launch": alg_bytes / nl, "ms_per_launch": trav_ms / nl,
+                         "launches": nl},
+            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -246,12 +246,18 @@ typedef struct rb_render_stats {
 	uint32_t device_error;      /* rb_status raised inside a kernel, RB_OK if none */
 	uint32_t kernel_launches;
 	float elapsed_ms;           /* device time of the call, CUDA events */
-	float trace_ms;             /* device time of the traversal kernels */
+	float extend_ms;            /* device time of the extend (closest-hit) launches; profiling only */
+	float secondary_ms;         /* device time of the shadow / MIS traversal launches; profiling only */
+	uint32_t extend_launches;   /* traversal launches timed by profiling */
+	uint32_t secondary_launches;
 } rb_render_stats;
 rb_status rb_render_stats_get(rb_context* ctx, rb_render_stats* out);
 
 /* Enable node-visit / triangle-test counting in the traversal kernels (slower). */
 rb_status rb_set_counting(rb_context* ctx, int enabled);
+/* Time every traversal launch with CUDA events on the launching stream
+ * (stats extend_ms / secondary_ms). Launches then run without graph replay. */
+rb_status rb_set_profiling(rb_context* ctx, int enabled);
 
 /* Checkpoint / resume of the film accumulators and sample counter. */
 rb_status rb_checkpoint_save(rb_context* ctx, const char* path);

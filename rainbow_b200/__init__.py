@@ -188,6 +188,9 @@ class Context:
     def set_counting(self, enabled: bool) -> None:
         check(lib().rb_set_counting(self._h, int(enabled)), "rb_set_counting")
 
+    def set_profiling(self, enabled: bool) -> None:
+        check(lib().rb_set_profiling(self._h, int(enabled)), "rb_set_profiling")
+
     def checkpoint_save(self, path: str) -> None:
         check(lib().rb_checkpoint_save(self._h, path.encode()), "rb_checkpoint_save")
 

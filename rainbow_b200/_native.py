@@ -80,7 +80,8 @@ class RenderStats(C.Structure):
     _fields_ = [("samples", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("mis_rays", C.c_uint64), ("node_visits", C.c_uint64), ("triangle_tests", C.c_uint64),
                 ("device_error", C.c_uint32), ("kernel_launches", C.c_uint32), ("elapsed_ms", C.c_float),
-                ("trace_ms", C.c_float)]
+                ("extend_ms", C.c_float), ("secondary_ms", C.c_float), ("extend_launches", C.c_uint32),
+                ("secondary_launches", C.c_uint32)]
 
 
 class SceneGenParams(C.Structure):
@@ -106,6 +107,7 @@ SIGNATURES = {
     "rb_film_read": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rb_render_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(RenderStats)]),
     "rb_set_counting": (C.c_int32, [C.c_void_p, C.c_int]),
+    "rb_set_profiling": (C.c_int32, [C.c_void_p, C.c_int]),
     "rb_checkpoint_save": (C.c_int32, [C.c_void_p, C.c_char_p]),
     "rb_checkpoint_load": (C.c_int32, [C.c_void_p, C.c_char_p]),
     "rb_bvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),

@@ -116,6 +116,11 @@ struct rb_context {
 	uint32_t* counters = nullptr;
 	uint32_t* counters_host = nullptr;  // pinned
 	bool counting = false;
+	bool profiling = false;
+	static constexpr uint32_t kMaxEvents = 4096;  // event pairs per render call when profiling
+	std::vector<cudaEvent_t> events;
+	std::vector<uint8_t> event_kind;
+	uint32_t next_event = 0;
 	rb_render_stats stats{};
 
 	gpu::launch_cfg cfg() const {
@@ -126,6 +131,16 @@ struct rb_context {
 		c.grid_shade = num_sms * 8;
 		c.stack_depth = bvh_depth + 3 <= 32 ? 32 : 64;
 		c.count = counting;
+		return c;
+	}
+	gpu::launch_cfg profiled_cfg() {
+		gpu::launch_cfg c = cfg();
+		if (profiling && !events.empty()) {
+			c.events = events.data();
+			c.next_event = &next_event;
+			c.max_events = static_cast<uint32_t>(events.size() / 2);
+			c.event_kind = event_kind.data();
+		}
 		return c;
 	}
 
@@ -291,6 +306,7 @@ rb_status rb_context_destroy(rb_context* c) {
 	dev_free(c->wave.params);
 	if (c->counters_host) cudaFreeHost(c->counters_host);
 	if (c->params_host) cudaFreeHost(c->params_host);
+	for (cudaEvent_t e : c->events) cudaEventDestroy(e);
 	if (c->ev_begin) cudaEventDestroy(c->ev_begin);
 	if (c->ev_end) cudaEventDestroy(c->ev_end);
 	if (c->stream) cudaStreamDestroy(c->stream);
@@ -399,6 +415,18 @@ rb_status rb_set_counting(rb_context* c, int enabled) {
 	return RB_OK;
 }
 
+rb_status rb_set_profiling(rb_context* c, int enabled) {
+	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	c->profiling = enabled != 0;
+	if (c->profiling && c->events.empty()) {
+		RB_CUDA(cudaSetDevice(c->device));
+		c->events.resize(2 * rb_context::kMaxEvents);
+		c->event_kind.resize(rb_context::kMaxEvents);
+		for (auto& e : c->events) RB_CUDA(cudaEventCreate(&e));
+	}
+	return RB_OK;
+}
+
 rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) {
 	if (c == nullptr || prm == nullptr) return RB_ERR_INVALID_ARGUMENT;
 	if (!c->has_scene) return RB_ERR_NO_SCENE;
@@ -431,12 +459,13 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	hp.rr_threshold = prm->rr_threshold;
 
 	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
-	const bool use_graph = !c->has_invisible;
+	const bool use_graph = !c->has_invisible && !c->profiling;
+	c->next_event = 0;
 	if (use_graph) {
 		st = capture_wave(c, prm->max_depth);
 		if (st != RB_OK) return st;
 	}
-	const gpu::launch_cfg cfg = c->cfg();
+	const gpu::launch_cfg cfg = c->profiled_cfg();
 	uint32_t launches = 0;
 	hp.first_item = 0;
 	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
@@ -447,13 +476,13 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
 			launches += 2 + 5 * prm->max_depth;
 		} else {
-			// invisible entities: a pass-through does not count as a bounce, so
-			// keep bouncing until the active queue drains
+			// direct launches: profiling, or invisible entities (a pass-through
+			// does not count as a bounce, so keep bouncing until the queue drains)
 			RB_CUDA(cudaMemsetAsync(c->counters, 0, 3 * sizeof(uint32_t), c->stream));
 			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, prm->max_depth, 0u, cfg, c->stream));
 			launches += 1 + 5 * prm->max_depth;
 			uint32_t q = prm->max_depth & 1u;
-			for (int guard = 0; guard < 4096; guard++) {
+			for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
 				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 				RB_CUDA(cudaStreamSynchronize(c->stream));
 				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
@@ -480,7 +509,14 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	s.device_error = h[gpu::CNT_ERROR];
 	s.kernel_launches = launches;
 	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
-	s.trace_ms = 0.f;
+	s.extend_ms = s.secondary_ms = 0.f;
+	s.extend_launches = s.secondary_launches = 0;
+	for (uint32_t k = 0; c->profiling && k < c->next_event; k++) {
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, c->events[2 * k], c->events[2 * k + 1]);
+		if (c->event_kind[k] == 0) { s.extend_ms += ms; s.extend_launches++; }
+		else { s.secondary_ms += ms; s.secondary_launches++; }
+	}
 	c->film_samples += prm->spp;
 	if (h[gpu::CNT_ERROR] != 0) return static_cast<rb_status>(h[gpu::CNT_ERROR]);
 

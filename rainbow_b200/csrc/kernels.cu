@@ -316,9 +316,15 @@ template <bool COUNT>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
 	const size_t smem = static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	const bool timed = cfg.events != nullptr && *cfg.next_event + 2 <= cfg.max_events;
+	uint32_t ev = timed ? *cfg.next_event : 0u;
+	if (timed) { cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 0; }
 	k_extend<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
 	k_shade_a<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, f, queue_in);
+	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
 	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
 	k_shade_b<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, f, queue_in);
 	k_advance<<<1, 1, 0, stream>>>(w.counters);
 	return cudaGetLastError();

@@ -71,6 +71,12 @@ struct launch_cfg {
 	int block_trace, block_shade;
 	int stack_depth;         // traversal stack entries per thread (32 or 64)
 	bool count;              // node / triangle counting
+	// optional CUDA events recorded around every traversal launch (profiling);
+	// event pairs [2k, 2k + 1], k counted by *next_event, up to max_events pairs
+	cudaEvent_t* events = nullptr;
+	uint32_t* next_event = nullptr;
+	uint32_t max_events = 0;
+	uint8_t* event_kind = nullptr;  // 0 extend, 1 secondary
 };
 
 // Ray batches for rb_trace_closest / rb_trace_shadow.

@@ -1,0 +1,141 @@
+"""Regenerates the golden fixtures in tests/golden/ from the oracle.
+
+The reference ships no tests or known-answer vectors, so the fixtures are
+outputs of the reference renderer itself, compiled from its sources as
+oracle/_ref/liboracle_ref.so (`make -C oracle ref`), on inputs made by the
+product's seeded scene generator:
+
+  pcg32          uniform_uint32 / uniform_real streams of pcg32(seed)
+  box_rays       4096 seeded rays (camera rays and 1-2 diffuse bounces) in the box
+                 room: scene::intersect and intersect_with_shadow_ray results
+  spheres_rays   the same on a 30-sphere displaced-icosphere scene
+  box_samples    radiance of 1024 (pixel, sample) pairs, path_integrator::trace, depth 5
+  spheres_samples  the same at depth 8 (metal, glass, quad lights, environment)
+  bsdf_*         scattering_function_collection sample / evaluate / pdf per material
+  box_image      32 x 32 box room, 256 spp, FP64 per-pixel sums of L and L^2
+  bvh_c2         SHA-256 of the reference BVH of the 1,024,010-triangle sphere scene
+
+Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import rainbow_b200 as rb  # noqa: E402
+from oracle import ref  # noqa: E402
+
+BOX = dict(kind=rb.RB_SCENE_BOX, seed=0, width=64, height=64, num_spheres=0, subdivision=0)
+SPHERES = dict(kind=rb.RB_SCENE_SPHERES, seed=1, width=96, height=96, num_spheres=30, subdivision=2)
+C2 = dict(kind=rb.RB_SCENE_SPHERES, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4)
+
+
+def scene_of(p):
+    return rb.generate_scene(p["kind"], seed=p["seed"], width=p["width"], height=p["height"],
+                             num_spheres=p["num_spheres"], subdivision=p["subdivision"])
+
+
+def params_array(p):
+    return np.array([p["kind"], p["seed"], p["width"], p["height"], p["num_spheres"], p["subdivision"]], dtype=np.int64)
+
+
+def save(name, **arrays):
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays)
+    print("wrote", name, {k: v.shape for k, v in arrays.items()})
+
+
+def bvh_digest(nodes, pe, pi):
+    h = hashlib.sha256()
+    for a in (nodes.astype(np.float32).view(np.uint32), pe.astype(np.uint32), pi.astype(np.uint32)):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def main():
+    seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
+    u32 = np.zeros((len(seeds), 64), np.uint32)
+    reals = np.zeros((len(seeds), 64), np.float32)
+    for i, s in enumerate(seeds):
+        u32[i], reals[i] = ref.pcg32(int(s), 64)
+    save("pcg32", seeds=seeds, u32=u32, reals=reals)
+
+    for name, p, nrays, depth in (("box", BOX, 4096, 5), ("spheres", SPHERES, 8192, 8)):
+        s = scene_of(p)
+        R = ref.RefScene(s)
+        rays = R.make_rays(nrays, 7)
+        hc, pc = R.trace(rays, shadow=False, points=True)
+        hs = R.trace(rays, shadow=True)
+        r2c, c2w = R.camera_matrices()
+        nodes, pe, pi = R.bvh()
+        save(f"{name}_rays", params=params_array(p), rays=rays, hits_closest=hc, points_closest=pc, hits_shadow=hs,
+             raster_to_camera=r2c, camera_to_world=c2w, areas=R.areas(), bvh_nodes=nodes, bvh_prim_entity=pe,
+             bvh_prim_index=pi)
+        rng = np.random.default_rng(11)
+        W, H = p["width"], p["height"]
+        px = rng.integers(0, W * H, 1024).astype(np.uint32)
+        sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+        L = R.trace_samples(px, sm, max_depth=depth, rr=1.0, seed=0)
+        save(f"{name}_samples", params=params_array(p), pixels=px, samples=sm, radiance=L, max_depth=np.array(depth))
+
+    # BSDF known answers on the shading frame = world axes
+    rng = np.random.default_rng(5)
+    n = 512
+    wo = rng.normal(size=(n, 3)).astype(np.float32)
+    wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    wi = rng.normal(size=(n, 3)).astype(np.float32)
+    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    u = rng.random((n, 2), dtype=np.float32)
+    mats = {
+        "lambert": dict(kind=rb.RB_MATERIAL_MATTE, diffuse=(0.7, 0.4, 0.2)),
+        "metal": dict(kind=rb.RB_MATERIAL_METAL, rough=0.3),
+        "glass_rough": dict(kind=rb.RB_MATERIAL_GLASS, rough=0.2),
+        "glass_smooth": dict(kind=rb.RB_MATERIAL_GLASS, rough=0.0),
+    }
+    for key, m in mats.items():
+        md = material_desc(m)
+        for include_name, include in (("all", 31), ("nonspec", 27)):
+            out = ref.bsdf(md, wo, u, wi, include)
+            save(f"bsdf_{key}_{include_name}", wo=wo, u=u, wi_eval=wi, include=np.array(include),
+                 material=np.frombuffer(bytes(md), dtype=np.uint8), **out)
+
+    s = scene_of(dict(BOX, width=32, height=32))
+    R = ref.RefScene(s)
+    sums, sq, sec = R.render(256, 0, 5, 1.0, 0, 0)
+    save("box_image", params=params_array(dict(BOX, width=32, height=32)), spp=np.array(256), sum=sums, sum_sq=sq)
+
+    s = scene_of(C2)
+    R = ref.RefScene(s)
+    nodes, pe, pi = R.bvh()
+    save("bvh_c2", params=params_array(C2), digest=np.array(bvh_digest(nodes, pe, pi)),
+         num_nodes=np.array(nodes.shape[0]), num_prims=np.array(pe.shape[0]))
+
+
+def material_desc(m):
+    md = rb._native.MaterialDesc()
+    md.kind = m["kind"]
+    if m["kind"] == rb.RB_MATERIAL_MATTE:
+        md.diffuse[:] = m["diffuse"]
+        md.sigma = 0.0
+    elif m["kind"] == rb.RB_MATERIAL_METAL:
+        md.remap_roughness = 1
+        md.eta[:] = (0.200438, 0.924033, 1.102212)
+        md.k[:] = (3.912949, 2.452848, 2.142188)
+        md.roughness_u = md.roughness_v = m["rough"]
+    else:
+        md.remap_roughness = 1
+        md.reflectance[:] = (1.0, 1.0, 1.0)
+        md.transmission[:] = (1.0, 1.0, 1.0)
+        md.ior = 1.5
+        md.roughness_u = md.roughness_v = m["rough"]
+    return md
+
+
+if __name__ == "__main__":
+    main()
