@@ -51,6 +51,7 @@ rb_status from_cuda(cudaError_t e) {
 	} while (0)
 
 struct device_scene {
+	pt::wide_node* wnodes = nullptr;
 	float4* nodes = nullptr;
 	float4* tri_a = nullptr;
 	float4* tri_b = nullptr;
@@ -68,7 +69,7 @@ struct device_scene {
 	pt::emitter_rec* emitters = nullptr;
 	int32_t* environments = nullptr;
 	void release() {
-		dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
+		dev_free(wnodes); dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
 		dev_free(entities); dev_free(meshes); dev_free(positions); dev_free(normals); dev_free(tangents); dev_free(uvs);
 		dev_free(indices); dev_free(materials); dev_free(emitters); dev_free(environments);
 	}
@@ -146,9 +147,10 @@ struct rb_context {
 
 	void release_wave() {
 		dev_free(wave.ray_o); dev_free(wave.ray_d); dev_free(wave.beta); dev_free(wave.radiance); dev_free(wave.bounces);
-		dev_free(wave.rng); dev_free(wave.pixel); dev_free(wave.sample); dev_free(wave.hit); dev_free(wave.rec);
+		dev_free(wave.rng); dev_free(wave.pixel); dev_free(wave.sample); dev_free(wave.hit); dev_free(wave.rec); dev_free(wave.result);
 		dev_free(wave.sec_o); dev_free(wave.sec_d); dev_free(wave.sec_hit); dev_free(wave.queue[0]); dev_free(wave.queue[1]);
 		dev_free(wave.sec_queue);
+		dev_free(wave.class_queue);
 		wave_capacity = 0;
 	}
 	void release_graph() {
@@ -174,9 +176,10 @@ rb_status ensure_wave(rb_context* c, uint32_t capacity) {
 	RB_CUDA(dev_alloc(&w.ray_o, n)); RB_CUDA(dev_alloc(&w.ray_d, n)); RB_CUDA(dev_alloc(&w.beta, n));
 	RB_CUDA(dev_alloc(&w.radiance, n)); RB_CUDA(dev_alloc(&w.bounces, n)); RB_CUDA(dev_alloc(&w.rng, n));
 	RB_CUDA(dev_alloc(&w.pixel, n)); RB_CUDA(dev_alloc(&w.sample, n)); RB_CUDA(dev_alloc(&w.hit, n));
-	RB_CUDA(dev_alloc(&w.rec, n)); RB_CUDA(dev_alloc(&w.sec_o, 2 * n)); RB_CUDA(dev_alloc(&w.sec_d, 2 * n));
+	RB_CUDA(dev_alloc(&w.rec, n)); RB_CUDA(dev_alloc(&w.result, n)); RB_CUDA(dev_alloc(&w.sec_o, 2 * n)); RB_CUDA(dev_alloc(&w.sec_d, 2 * n));
 	RB_CUDA(dev_alloc(&w.sec_hit, 2 * n)); RB_CUDA(dev_alloc(&w.queue[0], n)); RB_CUDA(dev_alloc(&w.queue[1], n));
 	RB_CUDA(dev_alloc(&w.sec_queue, 2 * n));
+	RB_CUDA(dev_alloc(&w.class_queue, static_cast<size_t>(pt::NUM_CLASSES) * n));
 	w.capacity = capacity;
 	w.counters = c->counters;
 	c->wave_capacity = capacity;
@@ -216,9 +219,9 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 	c->release_graph();
 	cudaGraph_t g = nullptr;
 	RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-	cudaError_t e = cudaMemsetAsync(c->counters, 0, 3 * sizeof(uint32_t), c->stream);
+	cudaError_t e = cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream);
 	if (e == cudaSuccess) e = gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream);
-	if (e == cudaSuccess) e = gpu::launch_next_wave(c->wave, c->stream);
+	if (e == cudaSuccess) e = gpu::launch_next_wave(c->wave, c->film, c->num_sms * 4, c->stream);
 	const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
 	if (e != cudaSuccess || e2 != cudaSuccess) {
 		if (g) cudaGraphDestroy(g);
@@ -327,6 +330,7 @@ rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
 	c->has_scene = false;
 	device_scene& d = c->scene;
 	RB_CUDA(dev_upload(&d.nodes, p.nodes, c->stream));
+	if (p.wide_ok) RB_CUDA(dev_upload(&d.wnodes, p.wnodes, c->stream));
 	RB_CUDA(dev_upload(&d.tri_a, p.tri_a, c->stream));
 	RB_CUDA(dev_upload(&d.tri_b, p.tri_b, c->stream));
 	RB_CUDA(dev_upload(&d.tri_c, p.tri_c, c->stream));
@@ -344,6 +348,10 @@ rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
 	RB_CUDA(dev_upload(&d.environments, p.environments, c->stream));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
 	pt::scene_view v{};
+	v.wnodes = p.wide_ok ? d.wnodes : nullptr;
+	v.root_a = p.root_a;
+	v.root_b = p.root_b;
+	v.root_ref = p.root_ref;
 	v.nodes = d.nodes; v.tri_a = d.tri_a; v.tri_b = d.tri_b; v.tri_c = d.tri_c; v.prim_index = d.prim_index;
 	v.entities = d.entities; v.meshes = d.meshes; v.positions = d.positions; v.normals = d.normals;
 	v.tangents = d.tangents; v.uvs = d.uvs; v.indices = d.indices; v.materials = d.materials; v.emitters = d.emitters;
@@ -474,24 +482,24 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		if (use_graph) {
 			// the graph's last node moves params->first_item to the next wave
 			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
-			launches += 2 + 5 * prm->max_depth;
+			launches += 3 + 12 * prm->max_depth;
 		} else {
 			// direct launches: profiling, or invisible entities (a pass-through
 			// does not count as a bounce, so keep bouncing until the queue drains)
-			RB_CUDA(cudaMemsetAsync(c->counters, 0, 3 * sizeof(uint32_t), c->stream));
+			RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream));
 			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, prm->max_depth, 0u, cfg, c->stream));
-			launches += 1 + 5 * prm->max_depth;
+			launches += 1 + 12 * prm->max_depth;
 			uint32_t q = prm->max_depth & 1u;
 			for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
 				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 				RB_CUDA(cudaStreamSynchronize(c->stream));
 				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
 				RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
-				launches += 5;
+				launches += 12;
 				q ^= 1u;
 			}
-			RB_CUDA(gpu::launch_next_wave(c->wave, c->stream));
-			launches += 1;
+			RB_CUDA(gpu::launch_next_wave(c->wave, c->film, c->num_sms * 4, c->stream));
+			launches += 2;
 		}
 	}
 	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));

@@ -209,6 +209,43 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			}
 			out.bvh_depth = depth;
 		}
+		// ---- wide nodes: interior nodes numbered in preorder, children's boxes inline
+		{
+			const uint32_t nn = bvh.num_nodes;
+			auto word = [&](uint32_t n, int k) {
+				uint32_t v;
+				std::memcpy(&v, bvh.nodes + 8ull * n + k, 4);
+				return v;
+			};
+			std::vector<uint32_t> wid(nn, 0xffffffffu);
+			uint32_t next = 0;
+			for (uint32_t n = 0; n < nn; n++)
+				if (!(word(n, 7) & RB_BVH_LEAF_FLAG)) wid[n] = next++;
+			bool ok = bvh.num_prims < (1u << 24);
+			auto ref_of = [&](uint32_t n) -> uint32_t {
+				const uint32_t w1 = word(n, 7);
+				if (!(w1 & RB_BVH_LEAF_FLAG)) return wid[n];
+				const uint32_t count = w1 & ~RB_BVH_LEAF_FLAG, first = word(n, 6);
+				if (count == 0 || count > 127 || first >= (1u << 24)) ok = false;
+				return pt::kRefLeaf | ((count & 0x7fu) << 24) | (first & 0x00ffffffu);
+			};
+			out.wnodes.resize(next);
+			for (uint32_t n = 0; n < nn; n++) {
+				if (wid[n] == 0xffffffffu) continue;
+				const uint32_t l = n + 1, r = word(n, 6);
+				const float* bl = bvh.nodes + 8ull * l;
+				const float* br = bvh.nodes + 8ull * r;
+				pt::wide_node& w = out.wnodes[wid[n]];
+				w.a = float4{bl[0], bl[1], bl[2], bl[3]};
+				w.b = float4{bl[4], bl[5], br[0], br[1]};
+				w.c = float4{br[2], br[3], br[4], br[5]};
+				w.d = uint4{ref_of(l), ref_of(r), word(n, 7), 0u};
+			}
+			out.root_a = float4{bvh.nodes[0], bvh.nodes[1], bvh.nodes[2], bvh.nodes[3]};
+			out.root_b = float4{bvh.nodes[4], bvh.nodes[5], 0.f, 0.f};
+			out.root_ref = nn > 0 ? ref_of(0) : 0u;
+			out.wide_ok = ok && nn > 0;
+		}
 		out.tri_a.resize(bvh.num_prims);
 		out.tri_b.resize(bvh.num_prims);
 		out.tri_c.resize(bvh.num_prims);
@@ -240,6 +277,10 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 
 pt::scene_view host_view(const packed_scene& p) {
 	pt::scene_view v{};
+	v.wnodes = p.wide_ok ? p.wnodes.data() : nullptr;
+	v.root_a = p.root_a;
+	v.root_b = p.root_b;
+	v.root_ref = p.root_ref;
 	v.nodes = p.nodes.data();
 	v.tri_a = p.tri_a.data();
 	v.tri_b = p.tri_b.data();

@@ -10,7 +10,11 @@ namespace rb {
 namespace host {
 
 struct packed_scene {
-	std::vector<float4> nodes;            // 2 per BVH node
+	std::vector<float4> nodes;            // 2 per BVH node (reference layout, exact traversal)
+	std::vector<pt::wide_node> wnodes;    // interior nodes with child boxes (fast traversal)
+	float4 root_a{}, root_b{};
+	uint32_t root_ref = 0;
+	bool wide_ok = false;                 // every leaf fits the wide-node reference encoding
 	std::vector<float4> tri_a, tri_b;     // per prim slot, entity-local p0 / e1 / e2
 	std::vector<float2> tri_c;
 	std::vector<uint32_t> prim_index;

@@ -16,17 +16,26 @@ using namespace rb::pt;
 
 namespace {
 
+// Per-thread traversal stack in shared memory, [entry][thread]: node
+// references, and for the child-box traversal the entry distance of each entry.
 struct smem_stack {
 	uint32_t* base;
+	float* te;
 	uint32_t stride;
 	uint32_t sp;
 	uint32_t cap;
 	__device__ void reset() { sp = 0; }
 	__device__ void push(uint32_t v) { base[sp * stride] = v; sp++; }
 	__device__ uint32_t pop() { sp--; return base[sp * stride]; }
+	__device__ void push(uint32_t v, float t) { base[sp * stride] = v; te[sp * stride] = t; sp++; }
+	__device__ void pop(uint32_t& v, float& t) { sp--; v = base[sp * stride]; t = te[sp * stride]; }
 	__device__ bool empty() const { return sp == 0; }
 	__device__ bool full() const { return sp + 2 > cap; }
 };
+
+__device__ __forceinline__ smem_stack make_stack(uint32_t* smem, uint32_t cap) {
+	return smem_stack{smem + threadIdx.x, reinterpret_cast<float*>(smem + cap * blockDim.x) + threadIdx.x, blockDim.x, 0u, cap};
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
 	uint32_t m;
@@ -45,6 +54,20 @@ __device__ __forceinline__ void warp_push(bool pred, uint32_t value, uint32_t* q
 	if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
 	base = __shfl_sync(0xffffffffu, base, leader);
 	if (pred) queue[base + __popc(mask & lanemask_lt())] = value;
+}
+
+// Warp-aggregated push into one of several queues: lanes with the same key are
+// grouped with __match_any_sync, one lane per group reserves the group's slots.
+// key == 0xffffffff: nothing to push. All lanes of the warp must call it together.
+__device__ __forceinline__ void warp_push_keyed(uint32_t key, uint32_t value, uint32_t* queues, uint32_t stride,
+	uint32_t* counters) {
+	const uint32_t peers = __match_any_sync(0xffffffffu, key);
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t leader = __ffs(peers) - 1;
+	uint32_t base = 0;
+	if (lane == leader && key != 0xffffffffu) base = atomicAdd(counters + key, static_cast<uint32_t>(__popc(peers)));
+	base = __shfl_sync(0xffffffffu, base, leader);
+	if (key != 0xffffffffu) queues[key * stride + base + __popc(peers & lanemask_lt())] = value;
 }
 
 __device__ __forceinline__ void add64(uint32_t* counters, uint32_t word, uint64_t v) {
@@ -70,7 +93,19 @@ template <bool SHADOW, bool COUNT>
 __device__ __forceinline__ bool trace_one(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h, smem_stack& st,
 	uint32_t& nodes, uint32_t& tris) {
 	trace_counters c{0u, 0u};
-	const bool ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
+	bool ok;
+	if (s.wnodes != nullptr && !isnan(len)) {
+		const float len0 = len;
+		const int r = closest_hit_fast<SHADOW, COUNT>(s, o, d, len, h, st, c);
+		ok = r == 1;
+		if (r < 0) {  // a NaN length appeared: redo the ray in the reference's own visiting order
+			len = len0;
+			c = trace_counters{0u, 0u};
+			ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
+		}
+	} else {
+		ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
+	}
 	nodes += c.nodes;
 	tris += c.tris;
 	return ok;
@@ -81,7 +116,7 @@ template <bool SHADOW, bool COUNT>
 __global__ void __launch_bounds__(128) k_trace_rays(scene_view s, const uint32_t* __restrict__ prim_entity,
 	const rb_ray* __restrict__ rays, uint32_t n, rb_hit* __restrict__ hits, uint32_t stack_cap, uint32_t* counters) {
 	extern __shared__ uint32_t smem[];
-	smem_stack st{smem + threadIdx.x, blockDim.x, 0u, stack_cap};
+	smem_stack st = make_stack(smem, stack_cap);
 	uint32_t nodes = 0, tris = 0;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t i = base + threadIdx.x;
@@ -145,16 +180,40 @@ __device__ __forceinline__ void store_path(const wave_buffers& w, uint32_t i, co
 	w.rng[i] = st.rng.state;
 }
 
-__device__ __forceinline__ void film_add(const film_buffers& f, uint32_t pixel, vec3 L) {
-	double* s = f.sum + 3ull * pixel;
-	double* q = f.sum_sq + 3ull * pixel;
-	atomicAdd(s + 0, static_cast<double>(L.x));
-	atomicAdd(s + 1, static_cast<double>(L.y));
-	atomicAdd(s + 2, static_cast<double>(L.z));
-	atomicAdd(q + 0, static_cast<double>(L.x) * L.x);
-	atomicAdd(q + 1, static_cast<double>(L.y) * L.y);
-	atomicAdd(q + 2, static_cast<double>(L.z) * L.z);
-	atomicAdd(f.count + pixel, 1u);
+__device__ __forceinline__ void finish(const wave_buffers& w, uint32_t i, vec3 L) {
+	w.result[i] = make_float4(L.x, L.y, L.z, 1.f);
+}
+
+// Adds the finished samples of one wave to the film: one thread per pixel sums
+// that pixel's paths of the wave in path order (plain adds, no atomics, so the
+// accumulators do not depend on the launch order). Item k of the render is
+// pixel k mod (width * height); path i of a wave is item first_item + i.
+__global__ void __launch_bounds__(256) k_film_resolve(wave_buffers w, film_buffers f) {
+	const wave_params& p = *w.params;
+	const uint64_t pixels = static_cast<uint64_t>(p.width) * p.height;
+	const uint64_t left = p.total_items > p.first_item ? p.total_items - p.first_item : 0;
+	const uint32_t n = static_cast<uint32_t>(left < w.capacity ? left : w.capacity);
+	const uint64_t shift = p.first_item % pixels;
+	for (uint64_t px = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; px < pixels;
+		 px += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+		double s0 = 0, s1 = 0, s2 = 0, q0 = 0, q1 = 0, q2 = 0;
+		uint32_t c = 0;
+		for (uint64_t i = (px + pixels - shift) % pixels; i < n; i += pixels) {
+			const float4 L = w.result[i];
+			if (L.w == 0.f) continue;
+			s0 += L.x; s1 += L.y; s2 += L.z;
+			q0 += static_cast<double>(L.x) * L.x;
+			q1 += static_cast<double>(L.y) * L.y;
+			q2 += static_cast<double>(L.z) * L.z;
+			c++;
+		}
+		if (c == 0) continue;
+		double* sp = f.sum + 3 * px;
+		double* qp = f.sum_sq + 3 * px;
+		sp[0] += s0; sp[1] += s1; sp[2] += s2;
+		qp[0] += q0; qp[1] += q1; qp[2] += q2;
+		f.count[px] += c;
+	}
 }
 
 // sampler_integrator::render's per-sample set-up (sampler_integrator.cpp:102-126) for
@@ -173,6 +232,7 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 			path_begin(st, p.r2c, p.c2w, p.lens, p.focus, pixel % p.width, pixel / p.width, pixel, sample, p.seed);
 			w.pixel[i] = pixel;
 			w.sample[i] = sample;
+			w.result[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 			store_path(w, i, st);
 		}
 		warp_push(valid, i, w.queue[queue_out], w.counters + CNT_ACTIVE);
@@ -182,14 +242,15 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 template <bool COUNT>
 __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
-	smem_stack st{smem + threadIdx.x, blockDim.x, 0u, stack_cap};
+	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_ACTIVE];
 	const uint32_t* q = w.queue[queue_in];
 	uint32_t nodes = 0, tris = 0;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
+		uint32_t key = 0xffffffffu, i = 0;
 		if (k < n) {
-			const uint32_t i = q[k];
+			i = q[k];
 			const float4 o = w.ray_o[i], d = w.ray_d[i];
 			float len = o.w;
 			hit_t h;
@@ -198,7 +259,9 @@ __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, ui
 				h.slot = -1;
 			}
 			w.hit[i] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
+			key = shade_class(s, h.slot);
 		}
+		warp_push_keyed(key, i, w.class_queue, w.capacity, w.counters + CNT_CLASS);
 	}
 	if (COUNT) {
 		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
@@ -206,10 +269,11 @@ __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, ui
 	}
 }
 
-__global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w, film_buffers f, uint32_t queue_in) {
+template <uint32_t CLASS>
+__global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 	const wave_params& p = *w.params;
-	const uint32_t n = w.counters[CNT_ACTIVE];
-	const uint32_t* q = w.queue[queue_in];
+	const uint32_t n = w.counters[CNT_CLASS + CLASS];
+	const uint32_t* q = w.class_queue + CLASS * w.capacity;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
 		bool push_shadow = false, push_mis = false;
@@ -217,25 +281,31 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w, f
 		if (k < n) {
 			i = q[k];
 			path_state st = load_path(w, p, i);
-			shade_record& rec = w.rec[i];
-			shade_record r;
-			const bool alive = shade_a(s, st, to_hit(w.hit[i]), r);
-			if (!alive) {
-				film_add(f, w.pixel[i], st.L);
+			if (CLASS == CLASS_MISS) {
+				shade_miss(s, st);
+				finish(w, i, st.L);
 				st.flags |= 0x80000000u;  // ended in shade_a; shade_b skips it
 			} else {
-				push_shadow = r.nee_entity >= 0;
-				push_mis = r.mis_valid != 0;
-				if (push_shadow) {
-					w.sec_o[2 * i] = make_float4(r.shadow_ray.o.x, r.shadow_ray.o.y, r.shadow_ray.o.z, r.shadow_ray.len);
-					w.sec_d[2 * i] = make_float4(r.shadow_ray.d.x, r.shadow_ray.d.y, r.shadow_ray.d.z, 0.f);
-				}
-				if (push_mis) {
-					w.sec_o[2 * i + 1] = make_float4(r.mis_ray.o.x, r.mis_ray.o.y, r.mis_ray.o.z, r.mis_ray.len);
-					w.sec_d[2 * i + 1] = make_float4(r.mis_ray.d.x, r.mis_ray.d.y, r.mis_ray.d.z, 0.f);
+				shade_record& r = w.rec[i];
+				const bool alive = shade_a<class_material(CLASS)>(s, st, to_hit(w.hit[i]), r);
+				if (!alive) {
+					finish(w, i, st.L);
+					st.flags |= 0x80000000u;
+				} else {
+					push_shadow = r.nee_entity >= 0;
+					push_mis = r.mis_valid != 0;
+					if (push_shadow) {
+						const ray_t& sr = r.shadow_ray;
+						w.sec_o[2 * i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.len);
+						w.sec_d[2 * i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.f);
+					}
+					if (push_mis) {
+						const ray_t& mr = r.mis_ray;
+						w.sec_o[2 * i + 1] = make_float4(mr.o.x, mr.o.y, mr.o.z, mr.len);
+						w.sec_d[2 * i + 1] = make_float4(mr.d.x, mr.d.y, mr.d.z, 0.f);
+					}
 				}
 			}
-			rec = r;
 			store_path(w, i, st);
 		}
 		warp_push(push_shadow, 2 * i, w.sec_queue, w.counters + CNT_SECONDARY);
@@ -252,7 +322,7 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w, f
 template <bool COUNT>
 __global__ void __launch_bounds__(128) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
-	smem_stack st{smem + threadIdx.x, blockDim.x, 0u, stack_cap};
+	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_SECONDARY];
 	uint32_t nodes = 0, tris = 0;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -275,10 +345,11 @@ __global__ void __launch_bounds__(128) k_trace_secondary(scene_view s, wave_buff
 	}
 }
 
-__global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, film_buffers f, uint32_t queue_in) {
+template <uint32_t CLASS>
+__global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, uint32_t queue_in) {
 	const wave_params& p = *w.params;
-	const uint32_t n = w.counters[CNT_ACTIVE];
-	const uint32_t* q = w.queue[queue_in];
+	const uint32_t n = w.counters[CNT_CLASS + CLASS];
+	const uint32_t* q = w.class_queue + CLASS * w.capacity;
 	uint32_t* qn = w.queue[queue_in ^ 1u];
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
@@ -291,8 +362,9 @@ __global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, f
 				const shade_record& rec = w.rec[i];
 				const hit_t sh = to_hit(w.sec_hit[2 * i]);
 				const hit_t mh = to_hit(w.sec_hit[2 * i + 1]);
-				alive = shade_b(s, st, rec, sh, mh, p.max_depth, p.rr_threshold);
-				if (!alive) film_add(f, w.pixel[i], st.L);
+				alive = CLASS == CLASS_OTHER ? shade_b_any(s, st, rec, sh, mh, p.max_depth, p.rr_threshold)
+					: shade_b<class_material(CLASS)>(s, st, rec, sh, mh, p.max_depth, p.rr_threshold);
+				if (!alive) finish(w, i, st.L);
 				store_path(w, i, st);
 			}
 		}
@@ -306,6 +378,7 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_ACTIVE] = counters[CNT_NEXT];
 	counters[CNT_NEXT] = 0u;
 	counters[CNT_SECONDARY] = 0u;
+	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
 }
 
 // Moves the wave window forward so the next replay of the same graph renders
@@ -315,17 +388,24 @@ __global__ void k_next_wave(wave_params* p, uint32_t capacity) { p->first_item +
 template <bool COUNT>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
-	const size_t smem = static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	const bool timed = cfg.events != nullptr && *cfg.next_event + 2 <= cfg.max_events;
 	uint32_t ev = timed ? *cfg.next_event : 0u;
 	if (timed) { cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 0; }
 	k_extend<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
 	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
-	k_shade_a<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, f, queue_in);
+	k_shade_a<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_METAL><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_MISS><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
 	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
-	k_shade_b<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, f, queue_in);
+	k_shade_b<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	k_shade_b<CLASS_METAL><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	k_shade_b<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	k_shade_b<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_advance<<<1, 1, 0, stream>>>(w.counters);
 	return cudaGetLastError();
 }
@@ -335,7 +415,7 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 cudaError_t launch_trace_rays(const scene_view& s, const uint32_t* prim_entity, const rb_ray* rays, uint32_t n, rb_hit* hits,
 	bool shadow, const launch_cfg& cfg, uint32_t* counters, cudaStream_t stream) {
 	if (n == 0) return cudaSuccess;
-	const size_t smem = static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	const uint32_t blocks_needed = (n + cfg.block_trace - 1) / cfg.block_trace;
 	const int grid = static_cast<int>(blocks_needed < static_cast<uint32_t>(cfg.grid_trace) ? blocks_needed : cfg.grid_trace);
 	if (shadow) {
@@ -365,7 +445,8 @@ cudaError_t launch_wave(const scene_view& s, const wave_buffers& w, const film_b
 	return err;
 }
 
-cudaError_t launch_next_wave(const wave_buffers& w, cudaStream_t stream) {
+cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream) {
+	k_film_resolve<<<grid, 256, 0, stream>>>(w, f);
 	k_next_wave<<<1, 1, 0, stream>>>(w.params, w.capacity);
 	return cudaGetLastError();
 }

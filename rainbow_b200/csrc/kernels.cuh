@@ -15,13 +15,16 @@ enum : uint32_t {
 	CNT_NEXT = 1,        // paths pushed to the next active queue
 	CNT_SECONDARY = 2,   // secondary rays queued this bounce
 	CNT_ERROR = 3,       // first device error (rb_status), 0 if none
-	CNT_EXTEND_RAYS = 4, // 64-bit stats, two words each (lo, hi) from here on
-	CNT_SHADOW_RAYS = 6,
-	CNT_MIS_RAYS = 8,
-	CNT_NODE_VISITS = 10,
-	CNT_TRI_TESTS = 12,
-	CNT_WORDS = 16
+	CNT_CLASS = 4,       // paths per shading class this bounce (pt::NUM_CLASSES words)
+	CNT_EXTEND_RAYS = 10, // 64-bit stats, two words each (lo, hi) from here on
+	CNT_SHADOW_RAYS = 12,
+	CNT_MIS_RAYS = 14,
+	CNT_NODE_VISITS = 16,
+	CNT_TRI_TESTS = 18,
+	CNT_WORDS = 20
 };
+// words cleared at the start of a wave: everything before the 64-bit stats
+constexpr uint32_t kWaveCounterWords = CNT_EXTEND_RAYS;
 
 // Per-launch wave parameters, read by the kernels from device memory so a
 // captured graph can be replayed for every wave.
@@ -50,11 +53,13 @@ struct wave_buffers {
 	uint32_t* pixel;
 	uint32_t* sample;
 	float4* hit;             // slot (bits), t, b1, b2
+	float4* result;          // L.xyz of a finished path, w = 1 once it finished
 	pt::shade_record* rec;
 	float4* sec_o;           // 2 per path: shadow ray, MIS ray
 	float4* sec_d;
 	float4* sec_hit;
 	uint32_t* queue[2];      // active queues (ping-pong)
+	uint32_t* class_queue;   // NUM_CLASSES queues of `capacity` entries: paths by shading class
 	uint32_t* sec_queue;
 	uint32_t* counters;
 	wave_params* params;
@@ -88,8 +93,9 @@ cudaError_t launch_trace_rays(const pt::scene_view& s, const uint32_t* prim_enti
 cudaError_t launch_wave(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t max_depth,
 	uint32_t first_queue, const launch_cfg& cfg, cudaStream_t stream);
 
-// Advances params->first_item by the wave capacity (the last node of a wave).
-cudaError_t launch_next_wave(const wave_buffers& w, cudaStream_t stream);
+// Adds the wave's finished samples to the film, then advances
+// params->first_item by the wave capacity (the last nodes of a wave).
+cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream);
 
 // One extra bounce (used when invisible entities make paths outlive max_depth iterations).
 cudaError_t launch_bounce(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,

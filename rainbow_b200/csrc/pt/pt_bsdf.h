@@ -239,6 +239,11 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 	return b;
 }
 
+// Material kind known at compile time (a shading class), or MAT_ANY for a
+// run-time switch. Specialised code keeps each shading kernel small.
+constexpr int MAT_ANY = -1;
+
+template <int MAT = MAT_ANY>
 RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi) {
 	const float co = fabs_ref(wo.z), ci = fabs_ref(wi.z);
 	vec3 wh = wi + wo;
@@ -246,7 +251,8 @@ RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi) {
 	if (wh.x == 0.f && wh.y == 0.f && wh.z == 0.f) return spectrum{0.f, 0.f, 0.f};
 	wh = face_forward(normalize(wh), vec3{0.f, 0.f, 1.f});
 	spectrum F, R;
-	if (m->kind == MAT_METAL) {
+	const bool conductor = MAT == MAT_ANY ? (m->kind == MAT_METAL) : (MAT == static_cast<int>(MAT_METAL));
+	if (conductor) {
 		F = fresnel_conductor(dot(wi, wh), m->cond_eta, m->cond_k);
 		R = spectrum{1.f, 1.f, 1.f};
 	} else {
@@ -287,86 +293,119 @@ RB_HD float mf_transmit_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	return tr_pdf(m->alpha_x, m->alpha_y, wo, wh) * fabs_ref((eta * eta * dot(wi, wh)) / (denom * denom));
 }
 
+template <int MAT>
 RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
-	switch (b.kinds[i]) {
-	case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
-	case LOBE_MF_REFLECT: return mf_reflect_f(b.m, wo, wi);
-	case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
-	default: return spectrum{0.f, 0.f, 0.f};
-	}
-}
-RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
-	switch (b.kinds[i]) {
-	case LOBE_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
-	case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
-	case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
-	default: return 0.f;
-	}
-}
-RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
-	const material_rec* m = b.m;
-	switch (b.kinds[i]) {
-	case LOBE_LAMBERT: {
-		vec3 wi = cosine_hemisphere(u);
-		if (wo.z < 0.f) wi.z = -wi.z;
-		return lobe_sample{b.types[i], lobe_f(b, i, wo, wi), wi, lobe_pdf(b, i, wo, wi)};
-	}
-	case LOBE_MF_REFLECT: {
-		if (wo.z == 0.f) return no_sample();
-		const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
-		if (dot(wo, wh) < 0.f) return no_sample();
-		const vec3 wi = reflect(wo, wh);
-		if (!same_hemisphere(wo, wi)) return no_sample();
-		return lobe_sample{b.types[i], mf_reflect_f(m, wo, wi), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
-	}
-	case LOBE_MF_TRANSMIT: {
-		if (wo.z == 0.f) return no_sample();
-		const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
-		if (dot(wo, wh) < 0.f) return no_sample();
-		const bool entering = wo.z > 0.f;
-		const float eta = entering ? (1.f / m->eta) : (m->eta / 1.f);
-		const vec3 wi = refract(wo, wh, eta);
-		if (is_zero(wi)) return no_sample();
-		return lobe_sample{b.types[i], mf_transmit_f(m, wo, wi), wi, mf_transmit_pdf(m, wo, wi)};
-	}
-	case LOBE_FRESNEL_SPECULAR: {
-		// fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
-		const float F = fresnel_dielectric(wo.z, 1.f, m->eta);
-		if (u.x < F) {
-			const vec3 wi{-wo.x, -wo.y, wo.z};
-			return lobe_sample{ST_REFLECTION | ST_SPECULAR, m->reflectance * F / fabs_ref(wi.z), wi, F};
+	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return b.m->diffuse * kInvPi;
+	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_f<MAT>(b.m, wo, wi);
+	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
+		return b.kinds[i] == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi) : mf_transmit_f(b.m, wo, wi);
+	else {
+		switch (b.kinds[i]) {
+		case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
+		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi);
+		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
+		default: return spectrum{0.f, 0.f, 0.f};
 		}
-		const bool entering = wo.z > 0.f;
-		const float ei = entering ? 1.f : m->eta;
-		const float eo = entering ? m->eta : 1.f;
-		const vec3 wi = refract(wo, face_forward(vec3{0.f, 0.f, 1.f}, wo), ei / eo);
-		if (is_zero(wi)) return no_sample();
-		const float factor = (ei * ei) / (eo * eo);
-		const spectrum v = m->transmission * (splat3(1.f) - splat3(F)) * factor / fabs_ref(wi.z);
-		return lobe_sample{ST_TRANSMISSION | ST_SPECULAR, v, wi, 1.f - F};
 	}
-	default: return no_sample();
+}
+template <int MAT>
+RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
+	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
+	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_pdf(b.m, wo, wi);
+	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
+		return b.kinds[i] == LOBE_MF_REFLECT ? mf_reflect_pdf(b.m, wo, wi) : mf_transmit_pdf(b.m, wo, wi);
+	else {
+		switch (b.kinds[i]) {
+		case LOBE_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
+		case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
+		case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
+		default: return 0.f;
+		}
+	}
+}
+
+template <int MAT>
+RB_HD lobe_sample sample_lambert(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+	vec3 wi = cosine_hemisphere(u);
+	if (wo.z < 0.f) wi.z = -wi.z;
+	return lobe_sample{b.types[i], lobe_f<MAT>(b, i, wo, wi), wi, lobe_pdf<MAT>(b, i, wo, wi)};
+}
+template <int MAT>
+RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+	const material_rec* m = b.m;
+	if (wo.z == 0.f) return no_sample();
+	const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
+	if (dot(wo, wh) < 0.f) return no_sample();
+	const vec3 wi = reflect(wo, wh);
+	if (!same_hemisphere(wo, wi)) return no_sample();
+	return lobe_sample{b.types[i], mf_reflect_f<MAT>(m, wo, wi), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
+}
+RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+	const material_rec* m = b.m;
+	if (wo.z == 0.f) return no_sample();
+	const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
+	if (dot(wo, wh) < 0.f) return no_sample();
+	const bool entering = wo.z > 0.f;
+	const float eta = entering ? (1.f / m->eta) : (m->eta / 1.f);
+	const vec3 wi = refract(wo, wh, eta);
+	if (is_zero(wi)) return no_sample();
+	return lobe_sample{b.types[i], mf_transmit_f(m, wo, wi), wi, mf_transmit_pdf(m, wo, wi)};
+}
+// fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
+RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
+	const material_rec* m = b.m;
+	const float F = fresnel_dielectric(wo.z, 1.f, m->eta);
+	if (u.x < F) {
+		const vec3 wi{-wo.x, -wo.y, wo.z};
+		return lobe_sample{ST_REFLECTION | ST_SPECULAR, m->reflectance * F / fabs_ref(wi.z), wi, F};
+	}
+	const bool entering = wo.z > 0.f;
+	const float ei = entering ? 1.f : m->eta;
+	const float eo = entering ? m->eta : 1.f;
+	const vec3 wi = refract(wo, face_forward(vec3{0.f, 0.f, 1.f}, wo), ei / eo);
+	if (is_zero(wi)) return no_sample();
+	const float factor = (ei * ei) / (eo * eo);
+	const spectrum v = m->transmission * (splat3(1.f) - splat3(F)) * factor / fabs_ref(wi.z);
+	return lobe_sample{ST_TRANSMISSION | ST_SPECULAR, v, wi, 1.f - F};
+}
+
+template <int MAT>
+RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return sample_lambert<MAT>(b, i, wo, u);
+	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return sample_mf_reflect<MAT>(b, i, wo, u);
+	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
+		return b.kinds[i] == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u) : sample_mf_transmit(b, i, wo, u);
+	else {
+		switch (b.kinds[i]) {
+		case LOBE_LAMBERT: return sample_lambert<MAT_ANY>(b, i, wo, u);
+		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u);
+		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u);
+		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(b, wo, u);
+		default: return no_sample();
+		}
 	}
 }
 
 // ------------------------------------------------------------------ collection
 // scattering_function_collection::evaluate (:29-46)
+template <int MAT = MAT_ANY>
 RB_HD spectrum bsdf_f(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
 	if (wo.z == 0.f) return spectrum{0.f, 0.f, 0.f};
 	const uint32_t rt = same_hemisphere(wo, wi) ? ST_REFLECTION : ST_TRANSMISSION;
 	spectrum f{0.f, 0.f, 0.f};
 	for (uint32_t i = 0; i < b.count; i++)
-		if (type_match(include, b.types[i]) && type_match(b.types[i], rt)) f = f + lobe_f(b, i, wo, wi);
+		if (type_match(include, b.types[i]) && type_match(b.types[i], rt)) f = f + lobe_f<MAT>(b, i, wo, wi);
 	return f;
 }
 // scattering_function_collection::pdf (:131-148)
+template <int MAT = MAT_ANY>
 RB_HD float bsdf_pdf(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
 	if (b.count == 0 || wo.z == 0.f) return 0.f;
 	uint32_t n = 0;
 	float pdf = 0.f;
 	for (uint32_t i = 0; i < b.count; i++)
 		if (type_match(include, b.types[i])) {
-			pdf = pdf + lobe_pdf(b, i, wo, wi);
+			pdf = pdf + lobe_pdf<MAT>(b, i, wo, wi);
 			n++;
 		}
 	return n != 0 ? pdf / static_cast<float>(n) : 0.f;
@@ -379,6 +418,7 @@ RB_HD uint32_t bsdf_count(const bsdf_t& b, uint32_t include) {
 }
 // scattering_function_collection::sample (:48-100) with wo already in the
 // shading frame; the returned wi is in the shading frame too.
+template <int MAT = MAT_ANY>
 RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include) {
 	uint32_t idx[2];
 	uint32_t n = 0;
@@ -391,7 +431,7 @@ RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include
 	const float rx = u.x * fn - static_cast<float>(which);
 	const vec2 ur{(kOneMinusEps < rx) ? kOneMinusEps : rx, u.y};
 	if (wo.z == 0.f) return no_sample();
-	lobe_sample s = lobe_sample_dir(b, idx[which], wo, ur);
+	lobe_sample s = lobe_sample_dir<MAT>(b, idx[which], wo, ur);
 	if (s.pdf == 0.f) return no_sample();
 	if (!type_match(s.type, ST_SPECULAR)) {
 		const uint32_t rt = same_hemisphere(wo, s.wi) ? ST_REFLECTION : ST_TRANSMISSION;
@@ -399,8 +439,8 @@ RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include
 		s.pdf = 0.f;
 		for (uint32_t k = 0; k < n; k++) {
 			const uint32_t i = idx[k];
-			if (type_match(b.types[i], rt)) s.f = s.f + lobe_f(b, i, wo, s.wi);
-			s.pdf = s.pdf + lobe_pdf(b, i, wo, s.wi);
+			if (type_match(b.types[i], rt)) s.f = s.f + lobe_f<MAT>(b, i, wo, s.wi);
+			s.pdf = s.pdf + lobe_pdf<MAT>(b, i, wo, s.wi);
 		}
 	}
 	s.pdf = s.pdf / fn;

@@ -173,6 +173,122 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 	return true;
 }
 
+// ------------------------------------------------------------------ closest hit, child-box traversal
+// The same visiting decisions as closest_hit above, with each interior node
+// holding both children's boxes (wide_node) so a node is expanded with one
+// 64-byte load instead of one dependent load per popped child.
+//
+// Why the decisions are identical. The reference pushes both children (far,
+// then near), pops a node and slab-tests it against the ray length at pop time.
+// For a box, let te be the reference's t0 after the three axes (it does not
+// depend on the length) and tx the minimum of the far distances; with a
+// length that is not NaN the box passes iff te <= min(len, tx), and the early
+// exits after each axis do not change the outcome because t0 only grows and t1
+// only shrinks. Here both children are tested when their parent is expanded:
+//  - the near child is popped next by the reference with the length unchanged,
+//    so descending into it directly when it passes reproduces its pop test;
+//  - a child that fails now also fails at its later pop (the length only shrinks);
+//  - a far child that passes is pushed with te; passing now implied te <= tx,
+//    so at its pop the reference's test reduces to te <= len, checked as
+//    !(te > len).
+// Box tests are counted as the reference performs them: the root, then two per
+// expanded interior node. A NaN length (only reachable through a degenerate
+// triangle hit) returns -1 so the caller can redo the ray on the exact path.
+RB_HD bool slab_pass(float ax, float ay, float az, float bx, float by, float bz, vec3 o, vec3 inv, float len, float& te) {
+	float t0 = 0.f, t1 = len;
+	float n = (ax - o.x) * inv.x, f = (bx - o.x) * inv.x;
+	if (n > f) { const float t = n; n = f; f = t; }
+	t0 = fmaxf(t0, n); t1 = fminf(t1, f);
+	n = (ay - o.y) * inv.y; f = (by - o.y) * inv.y;
+	if (n > f) { const float t = n; n = f; f = t; }
+	t0 = fmaxf(t0, n); t1 = fminf(t1, f);
+	n = (az - o.z) * inv.z; f = (bz - o.z) * inv.z;
+	if (n > f) { const float t = n; n = f; f = t; }
+	t0 = fmaxf(t0, n); t1 = fminf(t1, f);
+	te = t0;
+	return !(t0 > t1);
+}
+
+template <bool SHADOW, bool COUNT, typename Stack>
+RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack, trace_counters& cnt) {
+	const vec3 inv = 1.f / d;
+	const bool neg[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+	hit.slot = -1;
+	uint32_t cur_entity = 0xffffffffu;
+	local_ray lr{};
+	stack.reset();
+	float te;
+	if (COUNT) cnt.nodes++;
+	if (!slab_pass(s.root_a.x, s.root_a.y, s.root_a.z, s.root_a.w, s.root_b.x, s.root_b.y, o, inv, len, te)) return 1;
+	uint32_t cur = s.root_ref;
+	for (;;) {
+		if (cur & kRefLeaf) {
+			const uint32_t first = cur & 0x00ffffffu, count = (cur >> 24) & 0x7fu;
+			for (uint32_t k = 0; k < count; k++) {
+				const uint32_t slot = first + k;
+				const float2 tc = RB_LDG(s.tri_c + slot);
+				const uint32_t ew = float_as_u32(tc.y);
+				if (SHADOW && (ew & kEntityInvisible)) continue;
+				const uint32_t ent = ew & ~kEntityInvisible;
+				const float4 ta = RB_LDG(s.tri_a + slot);
+				const float4 tb = RB_LDG(s.tri_b + slot);
+				if (ent != cur_entity) {
+					cur_entity = ent;
+					lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
+				}
+				if (COUNT) cnt.tris++;
+				float t, b1, b2;
+				if (triangle_hit(lr.o, lr.d, len * lr.to_local, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y},
+						vec3{tb.z, tb.w, tc.x}, t, b1, b2)) {
+					len = t * lr.to_world;
+					hit.slot = static_cast<int32_t>(slot);
+					hit.b1 = b1;
+					hit.b2 = b2;
+					if (isnan(len)) return -1;
+				}
+			}
+		} else {
+			const wide_node* nd = s.wnodes + cur;
+			const float4 a = RB_LDG(&nd->a), b = RB_LDG(&nd->b), c = RB_LDG(&nd->c);
+			const uint4 m = RB_LDG(&nd->d);
+			float te0, te1;
+			if (COUNT) cnt.nodes += 2;
+			const bool p0 = slab_pass(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, len, te0);
+			const bool p1 = slab_pass(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, len, te1);
+			// the reference visits the right child first when the ray is negative on the split axis
+			const bool right_first = neg[m.z];
+			const uint32_t r_first = right_first ? m.y : m.x, r_second = right_first ? m.x : m.y;
+			const bool p_first = right_first ? p1 : p0, p_second = right_first ? p0 : p1;
+			const float te_second = right_first ? te0 : te1;
+			if (p_first) {
+				if (p_second) {
+					if (stack.full()) return 0;
+					stack.push(r_second, te_second);
+				}
+				cur = r_first;
+				continue;
+			}
+			if (p_second) {
+				cur = r_second;
+				continue;
+			}
+		}
+		// pop the next far child whose box still passes at the current length
+		bool found = false;
+		while (!stack.empty()) {
+			uint32_t ref;
+			float tent;
+			stack.pop(ref, tent);
+			if (!(tent > len)) {
+				cur = ref;
+				found = true;
+				break;
+			}
+		}
+		if (!found) return 1;
+	}
+}
+
 // ------------------------------------------------------------------ surface interaction
 // World-space surface interaction of a hit: mesh::intersect_with_triangle's
 // interaction (mesh.cpp:350-441) taken to world space by

@@ -88,7 +88,34 @@ RB_HD uint32_t hit_entity(const scene_view& s, int32_t slot) {
 	return float_as_u32(s.tri_c[slot].y) & ~kEntityInvisible;
 }
 
+// Shading classes: hits are queued by the material kind of the hit entity so
+// that each shading kernel runs one BSDF's code on coherent warps.
+enum : uint32_t { CLASS_MISS = 0, CLASS_LAMBERT = 1, CLASS_METAL = 2, CLASS_GLASS_ROUGH = 3, CLASS_OTHER = 4, NUM_CLASSES = 5 };
+constexpr int class_material(uint32_t c) {
+	return c == CLASS_LAMBERT ? static_cast<int>(MAT_LAMBERT)
+		: c == CLASS_METAL ? static_cast<int>(MAT_METAL)
+		: c == CLASS_GLASS_ROUGH ? static_cast<int>(MAT_GLASS_ROUGH) : MAT_ANY;
+}
+RB_HD uint32_t class_of_material(int32_t material, const scene_view& s) {
+	if (material < 0) return CLASS_OTHER;
+	const uint32_t k = s.materials[material].kind;
+	return k == MAT_LAMBERT ? CLASS_LAMBERT : k == MAT_METAL ? CLASS_METAL : k == MAT_GLASS_ROUGH ? CLASS_GLASS_ROUGH : CLASS_OTHER;
+}
+RB_HD uint32_t shade_class(const scene_view& s, int32_t slot) {
+	if (slot < 0) return CLASS_MISS;
+	const uint32_t e = float_as_u32(s.tri_c[slot].y) & ~kEntityInvisible;
+	return class_of_material(s.entities[e].material, s);
+}
+
+// The miss branch of shade_a alone: environment radiance at bounce 0 or after
+// a specular bounce (integrator.cpp:333-346); the path always ends.
+RB_HD void shade_miss(const scene_view& s, path_state& p) {
+	if (p.bounces == 0 || (p.flags & PATH_SPECULAR))
+		for (uint32_t i = 0; i < s.num_environments; i++) p.L = p.L + p.beta * s.emitters[s.environments[i]].radiance;
+}
+
 // Returns false when the path ends here (a miss).
+template <int MAT = MAT_ANY>
 RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_record& rec) {
 	rec.pass_through = 0u;
 	rec.did_nee = 0u;
@@ -101,8 +128,8 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 			for (uint32_t i = 0; i < s.num_environments; i++) p.L = p.L + p.beta * s.emitters[s.environments[i]].radiance;
 		return false;
 	}
-	rec.si = make_surface(s, h.slot, h.b1, h.b2, p.o, p.d);
-	const surface_t& si = rec.si;
+	const surface_t si = make_surface(s, h.slot, h.b1, h.b2, p.o, p.d);
+	rec.si = si;
 	const entity_rec& ent = s.entities[si.entity];
 	if (count_emission && (ent.flags & ENT_HAS_EMITTER))
 		p.L = p.L + p.beta * surface_emission(ent, s.emitters[ent.emitter], si.n, -p.d);
@@ -130,8 +157,8 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 	ls.pdf = ls.pdf * pick_pdf;
 	if (!is_black(ls.L) && ls.pdf > 0.f) {
 		const vec3 wi = to_local(si, ls.wi);
-		spectrum f = bsdf_f(b, wo, wi, ST_NON_SPECULAR);
-		const float fpdf = bsdf_pdf(b, wo, wi, ST_NON_SPECULAR);
+		spectrum f = bsdf_f<MAT>(b, wo, wi, ST_NON_SPECULAR);
+		const float fpdf = bsdf_pdf<MAT>(b, wo, wi, ST_NON_SPECULAR);
 		f = f * fabs_ref(dot(ls.wi, si.sz));
 		if (!is_black(f) && fpdf > 0.f) {
 			rec.shadow_ray = spawn_ray_to(si.p, si.n, ls.p);
@@ -141,7 +168,7 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 		}
 	}
 	// BSDF sampling half (integrator.cpp:161-198)
-	const lobe_sample bs = bsdf_sample(b, wo, pcg_2d(p.rng), ST_NON_SPECULAR);
+	const lobe_sample bs = bsdf_sample<MAT>(b, wo, pcg_2d(p.rng), ST_NON_SPECULAR);
 	const vec3 wi_w = bs.pdf > 0.f ? to_world(si, bs.wi) : vec3{0.f, 0.f, 0.f};
 	const spectrum v = bs.f * fabs_ref(dot(wi_w, si.sz));
 	if (!is_black(v) && bs.pdf > 0.f) {
@@ -157,6 +184,7 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 
 // Returns false when the path ends (BSDF sample failed, Russian roulette, max depth).
 // shadow / mis are the closest visible hits of rec.shadow_ray / rec.mis_ray.
+template <int MAT = MAT_ANY>
 RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, const hit_t& shadow, const hit_t& mis,
 	uint32_t max_depth, float rr_threshold) {
 	if (!rec.pass_through) {
@@ -200,7 +228,7 @@ RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, 
 		// path continuation (integrator.cpp:380-399)
 		const bsdf_t b = make_bsdf(s.materials + rec.material);
 		const vec3 wo = to_local(si, si.wo);
-		const lobe_sample bs = bsdf_sample(b, wo, pcg_2d(p.rng), ST_ALL);
+		const lobe_sample bs = bsdf_sample<MAT>(b, wo, pcg_2d(p.rng), ST_ALL);
 		if (is_black(bs.f) || bs.pdf == 0.f) return false;
 		const vec3 wi = to_world(si, bs.wi);
 		p.beta = p.beta * (bs.f * fabs_ref(dot(wi, si.sz)) / bs.pdf);
@@ -221,6 +249,27 @@ RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, 
 	}
 	p.bounces++;
 	return p.bounces < static_cast<int32_t>(max_depth);
+}
+
+// Run-time dispatch to the class-specialised stages (the host build uses it;
+// the kernels launch one class at a time).
+RB_HD bool shade_a_any(const scene_view& s, path_state& p, const hit_t& h, shade_record& rec) {
+	switch (shade_class(s, h.slot)) {
+	case CLASS_LAMBERT: return shade_a<class_material(CLASS_LAMBERT)>(s, p, h, rec);
+	case CLASS_METAL: return shade_a<class_material(CLASS_METAL)>(s, p, h, rec);
+	case CLASS_GLASS_ROUGH: return shade_a<class_material(CLASS_GLASS_ROUGH)>(s, p, h, rec);
+	default: return shade_a<MAT_ANY>(s, p, h, rec);
+	}
+}
+RB_HD bool shade_b_any(const scene_view& s, path_state& p, const shade_record& rec, const hit_t& shadow, const hit_t& mis,
+	uint32_t max_depth, float rr_threshold) {
+	const uint32_t c = rec.pass_through ? CLASS_OTHER : class_of_material(static_cast<int32_t>(rec.material), s);
+	switch (c) {
+	case CLASS_LAMBERT: return shade_b<class_material(CLASS_LAMBERT)>(s, p, rec, shadow, mis, max_depth, rr_threshold);
+	case CLASS_METAL: return shade_b<class_material(CLASS_METAL)>(s, p, rec, shadow, mis, max_depth, rr_threshold);
+	case CLASS_GLASS_ROUGH: return shade_b<class_material(CLASS_GLASS_ROUGH)>(s, p, rec, shadow, mis, max_depth, rr_threshold);
+	default: return shade_b<MAT_ANY>(s, p, rec, shadow, mis, max_depth, rr_threshold);
+	}
 }
 
 } // namespace pt

@@ -10,6 +10,7 @@
 #include "../../rainbow_b200/csrc/host/scene_pack.h"
 #include "../../rainbow_b200/csrc/pt/pt_path.h"
 
+#include <cmath>
 #include <new>
 
 using namespace rb;
@@ -19,10 +20,13 @@ namespace {
 
 struct host_stack {
 	uint32_t data[128];
+	float te[128];
 	uint32_t sp = 0;
 	void reset() { sp = 0; }
 	void push(uint32_t v) { data[sp++] = v; }
 	uint32_t pop() { return data[--sp]; }
+	void push(uint32_t v, float t) { data[sp] = v; te[sp] = t; sp++; }
+	void pop(uint32_t& v, float& t) { sp--; v = data[sp]; t = te[sp]; }
 	bool empty() const { return sp == 0; }
 	bool full() const { return sp + 2 > 128; }
 };
@@ -32,10 +36,20 @@ struct hp_scene {
 	scene_view view;
 };
 
+// mode 0: the kernels' dispatch (child-box traversal, exact path on NaN);
+// mode 1: the reference-order traversal only.
+int g_mode = 0;
+
 hit_t trace(const scene_view& v, vec3 o, vec3 d, float& len, bool shadow) {
 	host_stack st;
 	trace_counters c{0, 0};
 	hit_t h;
+	if (g_mode == 0 && v.wnodes != nullptr && !std::isnan(len)) {
+		const float len0 = len;
+		const int r = shadow ? closest_hit_fast<true, false>(v, o, d, len, h, st, c) : closest_hit_fast<false, false>(v, o, d, len, h, st, c);
+		if (r >= 0) return h;
+		len = len0;
+	}
 	if (shadow) closest_hit<true, false>(v, o, d, len, h, st, c);
 	else closest_hit<false, false>(v, o, d, len, h, st, c);
 	return h;
@@ -44,6 +58,8 @@ hit_t trace(const scene_view& v, vec3 o, vec3 d, float& len, bool shadow) {
 } // namespace
 
 extern "C" {
+
+void hp_set_mode(int mode) { g_mode = mode; }
 
 int hp_create(const rb_scene_desc* desc, void** out) {
 	auto* s = new (std::nothrow) hp_scene();
@@ -90,7 +106,7 @@ int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, cons
 			float len = p.len;
 			const hit_t h = trace(s.view, p.o, p.d, len, false);
 			shade_record rec;
-			if (!shade_a(s.view, p, h, rec)) break;
+			if (!shade_a_any(s.view, p, h, rec)) break;
 			hit_t sh{-1, 0.f, 0.f}, mh{-1, 0.f, 0.f};
 			if (rec.nee_entity >= 0) {
 				float l = rec.shadow_ray.len;
@@ -100,7 +116,7 @@ int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, cons
 				float l = rec.mis_ray.len;
 				mh = trace(s.view, rec.mis_ray.o, rec.mis_ray.d, l, true);
 			}
-			if (!shade_b(s.view, p, rec, sh, mh, max_depth, rr)) break;
+			if (!shade_b_any(s.view, p, rec, sh, mh, max_depth, rr)) break;
 		}
 		out[3 * i] = p.L.x;
 		out[3 * i + 1] = p.L.y;
