@@ -1,0 +1,110 @@
+"""Pins the oracles: the compiled reference (oracle/_ref/liboracle_ref.so) and
+the plain-C restatement (oracle/restate) agree with the committed golden
+fixtures, which make_golden.py produced from the compiled reference.
+
+The reference ships no tests or known-answer vectors, so the fixtures are the
+reference's own outputs on seeded inputs; this file checks that both checkers
+still reproduce them bit for bit.
+"""
+import numpy as np
+import pytest
+
+import rainbow_b200 as rb
+from oracle import port, ref
+from tests import golden
+from tests.helpers import assert_hits_equal, scene_from_params
+
+needs_ref = pytest.mark.skipif(not ref.available(), reason="reference oracle not built (needs the reference sources)")
+
+
+def test_pcg32_port_matches_fixture():
+    fx = golden.load("pcg32")
+    for i, seed in enumerate(fx["seeds"]):
+        u, r = port.pcg32(int(seed), 64)
+        assert np.array_equal(u, fx["u32"][i])
+        assert np.array_equal(r.view(np.uint32), fx["reals"][i].view(np.uint32))
+
+
+@needs_ref
+def test_pcg32_reference_matches_fixture():
+    fx = golden.load("pcg32")
+    for i, seed in enumerate(fx["seeds"]):
+        u, r = ref.pcg32(int(seed), 64)
+        assert np.array_equal(u, fx["u32"][i])
+        assert np.array_equal(r, fx["reals"][i])
+
+
+def test_pcg32_known_stream():
+    # pcg32 with seed 0: inc = 1, two warm-up steps; first outputs are a fixed function of the constants
+    u, _ = port.pcg32(0, 4)
+    fx = golden.load("pcg32")
+    assert np.array_equal(u, fx["u32"][0][:4])
+
+
+@pytest.mark.parametrize("name", ["box_rays", "spheres_rays"])
+def test_port_trace_matches_fixture(name):
+    fx = golden.load(name)
+    scene = scene_from_params(fx["params"])
+    sb = scene.with_bvh(rb.bvh_from_arrays(fx["bvh_nodes"], fx["bvh_prim_entity"], fx["bvh_prim_index"]))
+    assert_hits_equal(port.trace(sb, fx["rays"], False), fx["hits_closest"], f"{name} closest")
+    assert_hits_equal(port.trace(sb, fx["rays"], True), fx["hits_shadow"], f"{name} shadow")
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["box_rays", "spheres_rays"])
+def test_reference_trace_matches_fixture(name):
+    fx = golden.load(name)
+    R = ref.RefScene(scene_from_params(fx["params"]))
+    assert_hits_equal(R.trace(fx["rays"], False), fx["hits_closest"], f"{name} closest")
+    assert_hits_equal(R.trace(fx["rays"], True), fx["hits_shadow"], f"{name} shadow")
+
+
+@pytest.mark.parametrize("name", ["box_samples", "spheres_samples"])
+def test_port_samples_match_fixture(name):
+    fx = golden.load(name)
+    rays_fx = golden.load(name.replace("samples", "rays"))
+    scene = scene_from_params(fx["params"])
+    sb = scene.with_bvh(rb.bvh_from_arrays(rays_fx["bvh_nodes"], rays_fx["bvh_prim_entity"], rays_fx["bvh_prim_index"]))
+    cam = rb.camera_copy(scene.camera, raster_to_camera=rays_fx["raster_to_camera"], camera_to_world=rays_fx["camera_to_world"])
+    got = port.samples(sb, cam, fx["pixels"], fx["samples"], int(fx["max_depth"]))
+    assert np.array_equal(got.view(np.uint32), fx["radiance"].view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["box_samples", "spheres_samples"])
+def test_reference_samples_match_fixture(name):
+    fx = golden.load(name)
+    R = ref.RefScene(scene_from_params(fx["params"]))
+    got = R.trace_samples(fx["pixels"], fx["samples"], max_depth=int(fx["max_depth"]))
+    assert np.array_equal(got.view(np.uint32), fx["radiance"].view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("mat", ["lambert", "metal", "glass_rough", "glass_smooth"])
+@pytest.mark.parametrize("inc", ["all", "nonspec"])
+def test_reference_bsdf_matches_fixture(mat, inc):
+    fx = golden.load(f"bsdf_{mat}_{inc}")
+    md = rb._native.MaterialDesc.from_buffer_copy(fx["material"].tobytes())
+    out = ref.bsdf(md, fx["wo"], fx["u"], fx["wi_eval"], int(fx["include"]))
+    for k in ("wi", "f", "pdf", "f_eval", "pdf_eval"):
+        assert np.array_equal(out[k].view(np.uint32), fx[k].view(np.uint32)), k
+    assert np.array_equal(out["type"], fx["type"])
+
+
+def test_port_image_statistics_match_reference_fixture():
+    """32 x 32 box room, 64 spp, independent seed: per-pixel means within 3 sigma
+    of the reference's 256-spp render (fixture)."""
+    fx = golden.load("box_image")
+    rays_fx = golden.load("box_rays")
+    scene = scene_from_params(fx["params"])
+    sb = scene.with_bvh(rb.build_bvh(scene))
+    n_ref, n = int(fx["spp"]), 64
+    s, q, _ = port.render(sb, scene.camera, n, 0, 5, 1.0, seed=5, threads=4)
+    m_ref = fx["sum"] / n_ref
+    v_ref = np.maximum(fx["sum_sq"] / n_ref - m_ref ** 2, 0)
+    m = s / n
+    v = np.maximum(q / n - m ** 2, 0)
+    se = np.sqrt(v / n + v_ref / n_ref)
+    z = np.where(se > 0, (m - m_ref) / np.where(se > 0, se, 1), 0)
+    assert (np.abs(z) > 3).mean() < 0.01
+    assert rays_fx is not None
