@@ -45,7 +45,8 @@ enum {
 	RB_ERR_IO = 8,               /* checkpoint file could not be read or written */
 	RB_ERR_CHECKPOINT = 9,       /* checkpoint does not match the context */
 	RB_ERR_DEVICE_TIMEOUT = 10,  /* a bounded device wait gave up */
-	RB_ERR_NO_DEVICE = 11        /* no CUDA device is visible */
+	RB_ERR_NO_DEVICE = 11,       /* no CUDA device is visible */
+	RB_ERR_TOO_LARGE = 12        /* more work than rb_render_noalloc's fixed scratch holds */
 };
 
 /* Human-readable name of a status code. Never NULL. */
@@ -234,6 +235,28 @@ rb_status rb_render(rb_context* ctx, const rb_render_params* params, float* rgb_
  * of squared radiance (double, 3 per pixel) and the sample count per pixel.
  * Any output may be NULL. */
 rb_status rb_film_read(rb_context* ctx, double* sum_rgb, double* sum_sq_rgb, uint32_t* sample_count);
+
+/* Render without allocating: for callers that must not call cudaMalloc at
+ * render time (code that runs inside a framework which owns the device memory
+ * pool, or a real-time loop where an allocation's implicit synchronisation is
+ * not allowed). No counterpart in the reference, which has no device.
+ * Same work as rb_render for samples [first_sample, first_sample + spp) of
+ * every pixel, but all per-path state, queues and counters live in one static
+ * device array of RB_NOALLOC_SCRATCH_BYTES that every GPU loading the library
+ * keeps until exit; at most RB_NOALLOC_MAX_PATHS = width * height * spp paths
+ * per call (larger requests return RB_ERR_TOO_LARGE). Results are ADDED to the
+ * caller's device accumulators d_sum_rgb / d_sum_sq_rgb (3 doubles per pixel)
+ * and d_count (one uint32 per pixel), which the caller zeroes before the first
+ * call. The scene must have been uploaded with rb_scene_upload beforehand. The
+ * first call on a device looks up the scratch array's device address, so make
+ * it before any stream capture. Every call shares the one scratch array: calls
+ * that overlap on the GPU (other streams, other threads) race, so serialise
+ * them. `stream` is a cudaStream_t (NULL: the context's stream); the call
+ * waits for its work to finish and returns the first device error, if any. */
+#define RB_NOALLOC_MAX_PATHS 16384u
+#define RB_NOALLOC_SCRATCH_BYTES (8u << 20)
+rb_status rb_render_noalloc(rb_context* ctx, const rb_render_params* params, double* d_sum_rgb, double* d_sum_sq_rgb,
+	uint32_t* d_count, void* stream);
 
 /* Counters of the last rb_render call. */
 typedef struct rb_render_stats {

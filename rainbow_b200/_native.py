@@ -18,6 +18,7 @@ STATUS_NAMES = {
     0: "RB_OK", 1: "RB_ERR_INVALID_ARGUMENT", 2: "RB_ERR_CUDA", 3: "RB_ERR_OUT_OF_MEMORY",
     4: "RB_ERR_NO_SCENE", 5: "RB_ERR_STACK_OVERFLOW", 6: "RB_ERR_QUEUE_OVERFLOW", 7: "RB_ERR_UNSUPPORTED",
     8: "RB_ERR_IO", 9: "RB_ERR_CHECKPOINT", 10: "RB_ERR_DEVICE_TIMEOUT", 11: "RB_ERR_NO_DEVICE",
+    12: "RB_ERR_TOO_LARGE",
 }
 
 RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS = 0, 1, 2
@@ -118,6 +119,7 @@ SIGNATURES = {
     "rb_scene_get": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(CameraDesc)]),
     "rb_scene_free": (None, [C.c_void_p]),
     "rb_abi_version": (C.c_int32, []),
+    "rb_render_noalloc": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 

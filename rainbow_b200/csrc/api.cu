@@ -241,6 +241,24 @@ bool host_is_valid_camera(const rb_camera_desc& cam) {
 
 } // namespace
 
+namespace rb {
+namespace gpu {
+// Scene view, launch configuration, stream, device and pinned counter buffer of
+// a context, for entry points defined in other files of the library.
+bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStream_t* stream, int* device,
+	uint32_t** counters_host) {
+	if (c == nullptr || !c->has_scene) return false;
+	*view = c->view;
+	*cfg = c->cfg();
+	cfg->count = false;
+	*stream = c->stream;
+	*device = c->device;
+	*counters_host = c->counters_host;
+	return true;
+}
+} // namespace gpu
+} // namespace rb
+
 extern "C" {
 
 int32_t rb_abi_version(void) { return RBGPU_ABI_VERSION; }
@@ -259,6 +277,7 @@ const char* rb_status_string(rb_status s) {
 	case RB_ERR_CHECKPOINT: return "checkpoint does not match the context";
 	case RB_ERR_DEVICE_TIMEOUT: return "device wait timed out";
 	case RB_ERR_NO_DEVICE: return "no CUDA device";
+	case RB_ERR_TOO_LARGE: return "work exceeds the fixed scratch capacity of rb_render_noalloc";
 	default: return "unknown status";
 	}
 }
