@@ -206,7 +206,9 @@ rb_status rb_trace_shadow_device(rb_context* ctx, const rb_ray* d_rays, uint32_t
 
 /* ------------------------------------------------------------------ rendering */
 enum {
-	RB_RENDER_RESET = 1u << 0      /* clear the film accumulators before adding these samples */
+	RB_RENDER_RESET = 1u << 0,     /* clear the film accumulators before adding these samples */
+	RB_RENDER_GUIDE = 1u << 1,     /* learned guiding: sample path continuations from the guide (below) */
+	RB_RENDER_TRAIN = 1u << 2      /* learned guiding: collect training samples and train after every wave */
 };
 
 /* One render call: path_integrator::trace (rainbow-cpu/integrators/path_integrator.cpp:15-47)
@@ -285,6 +287,75 @@ rb_status rb_set_profiling(rb_context* ctx, int enabled);
 /* Checkpoint / resume of the film accumulators and sample counter. */
 rb_status rb_checkpoint_save(rb_context* ctx, const char* path);
 rb_status rb_checkpoint_load(rb_context* ctx, const char* path);
+
+/* ------------------------------------------------------------------ learned path guiding
+ * No counterpart in the reference renderer, which samples path continuations
+ * from the BSDF only (integrator.cpp:380-399). A small network maps a surface
+ * vertex (position normalised to the scene box, shading normal and outgoing
+ * direction, each mapped to [0, 1]) through a 12-frequency sin/cos encoding and
+ * 4 hidden ReLU layers of width 64 (BF16 weights, FP32 accumulation on the
+ * tensor cores) to 8 von Mises-Fisher lobes (mean, concentration, weight) and a
+ * mixing fraction alpha. With RB_RENDER_GUIDE a non-specular vertex samples its
+ * continuation from the guide with probability alpha and from the BSDF
+ * otherwise, and weights it by f cos / (alpha q + (1 - alpha) p_bsdf) (one-sample
+ * MIS, unbiased for any network); until the first training step every vertex
+ * samples the BSDF alone, exactly as without the flag. With RB_RENDER_TRAIN
+ * each finished wave turns its recorded vertices into training samples
+ * (direction, BSDF pdf and weight = luminance of the radiance the continuation
+ * brought back over the throughput at the vertex) and runs steps_per_wave Adam
+ * steps of the loss -weight * (log q + log(alpha q + (1 - alpha) p_bsdf)). */
+#define RB_GUIDE_NUM_PARAMS 30000u  /* flat W1[64][224] b1[64] W2[64][64] b2 W3 b3 W4 b4 W5[48][64] b5[48] */
+#define RB_GUIDE_INPUTS 9u
+#define RB_GUIDE_OUTPUTS 48u        /* raw outputs: lobe i at 5i..5i+4 (mean xyz, log kappa, weight logit), alpha logit at 40 */
+typedef struct rb_guide_config {
+	uint32_t seed;              /* weight initialisation */
+	float learning_rate;        /* Adam step size, 0: 1e-3 */
+	uint32_t batch_size;        /* rows per training step, 0: 2^18 */
+	uint32_t steps_per_wave;    /* training steps after each wave of a RB_RENDER_TRAIN render, 0: 4 */
+	uint32_t max_samples;       /* training samples kept per wave, 0: 2^21 */
+	uint32_t min_rows;          /* steps with fewer collected samples are skipped, 0: 4096 */
+	uint32_t reserved[2];
+} rb_guide_config;
+/* One training sample (64 bytes). */
+typedef struct rb_guide_sample {
+	float inputs[9];
+	float direction[3];         /* unit world direction of the continuation */
+	float bsdf_pdf;             /* BSDF pdf of that direction (solid angle) */
+	float weight;               /* integrand over sampling pdf, >= 0 */
+	float reserved[2];
+} rb_guide_sample;
+typedef struct rb_guide_stats {
+	uint32_t steps;             /* Adam steps taken */
+	uint32_t samples_last_wave; /* training samples stored by the last wave */
+	uint32_t candidates_last_wave; /* vertices with a positive weight in the last wave */
+	uint32_t device_error;      /* rb_status of a failed bounded device wait, RB_OK if none */
+	float last_loss;
+	uint32_t rows_last_step;
+	uint32_t reserved[2];
+} rb_guide_stats;
+enum {
+	RB_GUIDE_SEQUENTIAL = 1u << 0  /* rb_guide_train: every step uses all samples in order (full batch) */
+};
+/* (Re)create the network with fresh weights and zero Adam moments; config may be NULL (defaults). */
+rb_status rb_guide_init(rb_context* ctx, const rb_guide_config* config);
+/* FP32 master weights in the flat order of RB_GUIDE_NUM_PARAMS. W1 columns
+ * 216..223 (padding features) are always zero; set ignores them. Set also
+ * clears the Adam moments and step count. */
+rb_status rb_guide_get_params(rb_context* ctx, float* params, uint32_t count);
+rb_status rb_guide_set_params(rb_context* ctx, const float* params, uint32_t count);
+/* Raw outputs (RB_GUIDE_OUTPUTS per row) of the tensor-core forward pass. */
+rb_status rb_guide_forward(rb_context* ctx, const float* inputs, uint32_t n, float* outputs);
+/* `steps` training steps on host samples (batch: config batch_size rows drawn
+ * by a hash of (step, row), or all n in order with RB_GUIDE_SEQUENTIAL).
+ * gradient (may be NULL): the batch gradient of the last step, flat order. */
+rb_status rb_guide_train(rb_context* ctx, const rb_guide_sample* samples, uint32_t n, uint32_t steps, uint32_t flags,
+	float* gradient, float* loss);
+/* Decode raw outputs (RB_GUIDE_OUTPUTS per row) and draw one direction per row
+ * from the guide density with the uniforms u (3 per row: lobe pick, two for the
+ * lobe); writes the unit direction (3 per row) and the guide pdf q at it. */
+rb_status rb_guide_sample_dirs(rb_context* ctx, const float* outputs, const float* u, uint32_t n, float* directions,
+	float* pdfs);
+rb_status rb_guide_stats_get(rb_context* ctx, rb_guide_stats* out);
 
 /* ------------------------------------------------------------------ host-side helpers (no GPU) */
 

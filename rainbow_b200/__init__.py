@@ -21,9 +21,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._native import (  # noqa: F401  (re-exported constants)
-    HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE,
-    RB_MATERIAL_METAL, RB_RENDER_RESET, RB_SCENE_BOX, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES, BvhDesc, CameraDesc,
-    RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
+    GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
+    RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_RENDER_GUIDE,
+    RB_RENDER_RESET, RB_RENDER_TRAIN, RB_SCENE_BOX, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES, BvhDesc, CameraDesc,
+    GuideConfig, GuideStats, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
 )
 
 __all__ = ["Scene", "Context", "PathIntegrator", "generate_scene", "build_bvh", "RbError", "RAY_DTYPE", "HIT_DTYPE"]
@@ -155,11 +156,14 @@ class Context:
         return self._trace(rays, True)
 
     def render(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5, threshold: float = 1.0,
-               seed: int = 0, reset: bool = True, paths_per_wave: int = 0, want_image: bool = True):
+               seed: int = 0, reset: bool = True, paths_per_wave: int = 0, want_image: bool = True,
+               guide: bool = False, train: bool = False):
+        """guide / train: learned path guiding (RB_RENDER_GUIDE / RB_RENDER_TRAIN)."""
         p = RenderParams()
         p.camera = camera
         p.spp, p.first_sample, p.max_depth, p.rr_threshold = spp, first_sample, max_depth, threshold
-        p.seed, p.flags, p.paths_per_wave = seed, (RB_RENDER_RESET if reset else 0), paths_per_wave
+        flags = (RB_RENDER_RESET if reset else 0) | (RB_RENDER_GUIDE if guide else 0) | (RB_RENDER_TRAIN if train else 0)
+        p.seed, p.flags, p.paths_per_wave = seed, flags, paths_per_wave
         img = np.zeros((camera.height, camera.width, 3), dtype=np.float32) if want_image else None
         self._film_shape = (camera.width, camera.height)
         check(lib().rb_render(self._h, C.byref(p), img.ctypes.data if want_image else None), "rb_render")
@@ -196,6 +200,52 @@ class Context:
 
     def checkpoint_load(self, path: str) -> None:
         check(lib().rb_checkpoint_load(self._h, path.encode()), "rb_checkpoint_load")
+
+    # ---- learned path guiding
+    def guide_init(self, seed: int = 0, learning_rate: float = 1e-3, batch_size: int = 1 << 18, steps_per_wave: int = 4,
+                   max_samples: int = 1 << 21, min_rows: int = 4096) -> None:
+        cfg = GuideConfig(seed, learning_rate, batch_size, steps_per_wave, max_samples, min_rows)
+        check(lib().rb_guide_init(self._h, C.byref(cfg)), "rb_guide_init")
+
+    def guide_params(self) -> np.ndarray:
+        out = np.zeros(RB_GUIDE_NUM_PARAMS, dtype=np.float32)
+        check(lib().rb_guide_get_params(self._h, out.ctypes.data, out.size), "rb_guide_get_params")
+        return out
+
+    def guide_set_params(self, params: np.ndarray) -> None:
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().rb_guide_set_params(self._h, params.ctypes.data, params.size), "rb_guide_set_params")
+
+    def guide_forward(self, inputs: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(inputs, dtype=np.float32).reshape(-1, 9)
+        out = np.zeros((x.shape[0], RB_GUIDE_OUTPUTS), dtype=np.float32)
+        check(lib().rb_guide_forward(self._h, x.ctypes.data, x.shape[0], out.ctypes.data), "rb_guide_forward")
+        return out
+
+    def guide_train(self, samples: np.ndarray, steps: int = 1, sequential: bool = False):
+        """Training steps on host samples (GUIDE_SAMPLE_DTYPE); returns (gradient of the last step, its loss)."""
+        samples = np.ascontiguousarray(samples, dtype=GUIDE_SAMPLE_DTYPE)
+        grad = np.zeros(RB_GUIDE_NUM_PARAMS, dtype=np.float32)
+        loss = C.c_float()
+        check(lib().rb_guide_train(self._h, samples.ctypes.data, samples.shape[0], steps,
+                                   RB_GUIDE_SEQUENTIAL if sequential else 0, grad.ctypes.data, C.byref(loss)),
+              "rb_guide_train")
+        return grad, loss.value
+
+    def guide_sample(self, outputs: np.ndarray, u: np.ndarray):
+        """Decode raw outputs and draw one direction per row; returns (directions, guide pdf)."""
+        raw = np.ascontiguousarray(outputs, dtype=np.float32).reshape(-1, RB_GUIDE_OUTPUTS)
+        uu = np.ascontiguousarray(u, dtype=np.float32).reshape(-1, 3)
+        d = np.zeros((raw.shape[0], 3), dtype=np.float32)
+        pdf = np.zeros(raw.shape[0], dtype=np.float32)
+        check(lib().rb_guide_sample_dirs(self._h, raw.ctypes.data, uu.ctypes.data, raw.shape[0], d.ctypes.data,
+                                         pdf.ctypes.data), "rb_guide_sample_dirs")
+        return d, pdf
+
+    def guide_stats(self) -> GuideStats:
+        st = GuideStats()
+        check(lib().rb_guide_stats_get(self._h, C.byref(st)), "rb_guide_stats_get")
+        return st
 
 
 class PathIntegrator:

@@ -25,6 +25,12 @@ RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS = 0, 1, 2
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
 RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM = 0, 1, 2
 RB_RENDER_RESET = 1
+RB_RENDER_GUIDE = 2
+RB_RENDER_TRAIN = 4
+RB_GUIDE_SEQUENTIAL = 1
+RB_GUIDE_NUM_PARAMS = 30000
+RB_GUIDE_INPUTS = 9
+RB_GUIDE_OUTPUTS = 48
 RB_BVH_LEAF_FLAG = 0x80000000
 
 F16 = C.c_float * 16
@@ -90,6 +96,23 @@ class SceneGenParams(C.Structure):
                 ("subdivision", C.c_uint32), ("width", C.c_int32), ("height", C.c_int32)]
 
 
+class GuideConfig(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("learning_rate", C.c_float), ("batch_size", C.c_uint32),
+                ("steps_per_wave", C.c_uint32), ("max_samples", C.c_uint32), ("min_rows", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+
+class GuideStats(C.Structure):
+    _fields_ = [("steps", C.c_uint32), ("samples_last_wave", C.c_uint32), ("candidates_last_wave", C.c_uint32),
+                ("device_error", C.c_uint32), ("last_loss", C.c_float), ("rows_last_step", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+
+# rb_guide_sample: inputs[9], direction[3], bsdf_pdf, weight, reserved[2] (64 bytes)
+GUIDE_SAMPLE_DTYPE = np.dtype([("inputs", "<f4", 9), ("direction", "<f4", 3), ("bsdf_pdf", "<f4"),
+                               ("weight", "<f4"), ("reserved", "<f4", 2)])
+assert GUIDE_SAMPLE_DTYPE.itemsize == 64
+
 RAY_DTYPE = np.dtype([("origin", "<f4", 3), ("direction", "<f4", 3), ("length", "<f4")])
 HIT_DTYPE = np.dtype([("entity", "<i4"), ("triangle", "<i4"), ("t", "<f4"), ("b1", "<f4"), ("b2", "<f4")])
 assert RAY_DTYPE.itemsize == 28 and HIT_DTYPE.itemsize == 20
@@ -120,6 +143,13 @@ SIGNATURES = {
     "rb_scene_free": (None, [C.c_void_p]),
     "rb_abi_version": (C.c_int32, []),
     "rb_render_noalloc": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rb_guide_init": (C.c_int32, [C.c_void_p, C.POINTER(GuideConfig)]),
+    "rb_guide_get_params": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    "rb_guide_set_params": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    "rb_guide_forward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "rb_guide_train": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "rb_guide_sample_dirs": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "rb_guide_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GuideStats)]),
 }
 
 

@@ -78,8 +78,10 @@ struct device_scene {
 struct graph_key {
 	uint32_t capacity = 0, max_depth = 0, stack = 0;
 	bool count = false;
+	uint32_t guide_mode = 0, guide_steps = 0, guide_batch = 0;
 	bool operator==(const graph_key& o) const {
-		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count;
+		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
+			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch;
 	}
 };
 
@@ -101,7 +103,8 @@ struct rb_context {
 	pt::scene_view view{};
 
 	gpu::wave_buffers wave{};
-	uint32_t wave_capacity = 0;
+	uint32_t wave_capacity = 0;  // paths per wave of the current render call (<= wave_alloc)
+	uint32_t wave_alloc = 0;     // paths the wave buffers hold
 	gpu::wave_params* params_host = nullptr;  // pinned
 	gpu::film_buffers film{};
 	int32_t film_w = 0, film_h = 0;
@@ -123,6 +126,8 @@ struct rb_context {
 	std::vector<uint8_t> event_kind;
 	uint32_t next_event = 0;
 	rb_render_stats stats{};
+	guide::guide_state guide;        // learned path guide (allocated on first use)
+	uint32_t guide_mode = 0;         // gpu::GUIDE_* of the current render call
 
 	gpu::launch_cfg cfg() const {
 		gpu::launch_cfg c;
@@ -132,6 +137,10 @@ struct rb_context {
 		c.grid_shade = num_sms * 8;
 		c.stack_depth = bvh_depth + 3 <= 32 ? 32 : 64;
 		c.count = counting;
+		if (guide_mode != 0u && guide.ready) {
+			c.guide = &guide;
+			c.guide_mode = guide_mode;
+		}
 		return c;
 	}
 	gpu::launch_cfg profiled_cfg() {
@@ -152,6 +161,7 @@ struct rb_context {
 		dev_free(wave.sec_queue);
 		dev_free(wave.class_queue);
 		wave_capacity = 0;
+		wave_alloc = 0;
 	}
 	void release_graph() {
 		if (graph) cudaGraphExecDestroy(graph);
@@ -168,7 +178,13 @@ struct rb_context {
 namespace {
 
 rb_status ensure_wave(rb_context* c, uint32_t capacity) {
-	if (c->wave_capacity >= capacity) return RB_OK;
+	if (c->wave_alloc >= capacity) {
+		// same buffers, smaller waves: the kernels read the wave size from wave.capacity
+		if (c->wave_capacity != capacity) c->release_graph();
+		c->wave.capacity = capacity;
+		c->wave_capacity = capacity;
+		return RB_OK;
+	}
 	c->release_graph();
 	c->release_wave();
 	gpu::wave_buffers& w = c->wave;
@@ -183,6 +199,7 @@ rb_status ensure_wave(rb_context* c, uint32_t capacity) {
 	w.capacity = capacity;
 	w.counters = c->counters;
 	c->wave_capacity = capacity;
+	c->wave_alloc = capacity;
 	return RB_OK;
 }
 
@@ -215,13 +232,18 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 	key.max_depth = max_depth;
 	key.stack = static_cast<uint32_t>(cfg.stack_depth);
 	key.count = cfg.count;
+	key.guide_mode = cfg.guide_mode;
+	if (cfg.guide) {
+		key.guide_steps = cfg.guide->cfg.steps_per_wave;
+		key.guide_batch = cfg.guide->cfg.batch_size;
+	}
 	if (c->graph && c->graph_cfg == key) return RB_OK;
 	c->release_graph();
 	cudaGraph_t g = nullptr;
 	RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
 	cudaError_t e = cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream);
 	if (e == cudaSuccess) e = gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream);
-	if (e == cudaSuccess) e = gpu::launch_next_wave(c->wave, c->film, c->num_sms * 4, c->stream);
+	if (e == cudaSuccess) e = gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream);
 	const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
 	if (e != cudaSuccess || e2 != cudaSuccess) {
 		if (g) cudaGraphDestroy(g);
@@ -231,6 +253,26 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 	cudaGraphDestroy(g);
 	RB_CUDA(e);
 	c->graph_cfg = key;
+	return RB_OK;
+}
+
+// Learned guiding for one render call: the guide (default configuration on
+// first use), its per-path buffers for this wave size and depth, and the
+// pointers the kernels read. A plain render leaves the guide untouched.
+rb_status prepare_guide(rb_context* c, const rb_render_params* prm) {
+	c->guide_mode = 0u;
+	c->wave.guide = guide::wave_guide{};
+	if (!(prm->flags & (RB_RENDER_GUIDE | RB_RENDER_TRAIN))) return RB_OK;
+	if (!c->guide.ready) {
+		const rb_status st = rb_guide_init(c, nullptr);
+		if (st != RB_OK) return st;
+	}
+	guide::guide_state& g = c->guide;
+	const float4* before = g.query_in;
+	RB_CUDA(guide::allocate_wave(g, c->wave_capacity, prm->max_depth));
+	if (g.query_in != before) c->release_graph();
+	c->guide_mode = ((prm->flags & RB_RENDER_GUIDE) ? gpu::GUIDE_SAMPLE : 0u) | ((prm->flags & RB_RENDER_TRAIN) ? gpu::GUIDE_TRAIN : 0u);
+	c->wave.guide = guide::wave_guide{g.dstate, g.query_in, g.query_out, g.queue, g.vertices, g.vertex_count, g.depth};
 	return RB_OK;
 }
 
@@ -251,11 +293,26 @@ bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStre
 	*view = c->view;
 	*cfg = c->cfg();
 	cfg->count = false;
+	cfg->guide = nullptr;
+	cfg->guide_mode = 0u;
 	*stream = c->stream;
 	*device = c->device;
 	*counters_host = c->counters_host;
 	return true;
 }
+
+// The guide of a context with its stream, device and SM count, for the
+// rb_guide_* entry points (guide_api.cu).
+guide::guide_state* context_guide(rb_context* c, cudaStream_t* stream, int* device, int* num_sms) {
+	if (c == nullptr) return nullptr;
+	*stream = c->stream;
+	*device = c->device;
+	*num_sms = c->num_sms;
+	return &c->guide;
+}
+
+// Drops the captured wave graph (its launches bake in guide buffer addresses).
+void context_drop_graph(rb_context* c) { c->release_graph(); }
 } // namespace gpu
 } // namespace rb
 
@@ -322,6 +379,7 @@ rb_status rb_context_destroy(rb_context* c) {
 	c->release_wave();
 	c->release_film();
 	c->scene.release();
+	guide::release(c->guide);
 	dev_free(c->trace_rays);
 	dev_free(c->trace_hits);
 	dev_free(c->counters);
@@ -471,6 +529,8 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	if (capacity == 0) capacity = 1;
 	st = ensure_wave(c, static_cast<uint32_t>(capacity));
 	if (st != RB_OK) return st;
+	st = prepare_guide(c, prm);
+	if (st != RB_OK) return st;
 
 	gpu::wave_params& hp = *c->params_host;
 	std::memcpy(hp.r2c, cam.raster_to_camera, sizeof(hp.r2c));
@@ -484,6 +544,17 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	hp.seed = prm->seed;
 	hp.max_depth = prm->max_depth;
 	hp.rr_threshold = prm->rr_threshold;
+	hp.guide_flags = c->guide_mode;
+	{
+		// scene box of the guide inputs: the root box of the BVH
+		const float lo[3] = {c->view.root_a.x, c->view.root_a.y, c->view.root_a.z};
+		const float hi[3] = {c->view.root_a.w, c->view.root_b.x, c->view.root_b.y};
+		for (int k = 0; k < 3; k++) {
+			const float ext = hi[k] - lo[k];
+			hp.box_min[k] = lo[k];
+			hp.box_inv[k] = ext > 0.f ? 1.f / ext : 0.f;
+		}
+	}
 
 	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
 	const bool use_graph = !c->has_invisible && !c->profiling;
@@ -501,24 +572,23 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		if (use_graph) {
 			// the graph's last node moves params->first_item to the next wave
 			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
-			launches += 3 + 12 * prm->max_depth;
+			launches += gpu::wave_launches(prm->max_depth, cfg);
 		} else {
 			// direct launches: profiling, or invisible entities (a pass-through
 			// does not count as a bounce, so keep bouncing until the queue drains)
 			RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream));
 			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, prm->max_depth, 0u, cfg, c->stream));
-			launches += 1 + 12 * prm->max_depth;
+			launches += gpu::wave_launches(prm->max_depth, cfg) - 2u;
 			uint32_t q = prm->max_depth & 1u;
 			for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
 				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 				RB_CUDA(cudaStreamSynchronize(c->stream));
 				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
 				RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
-				launches += 12;
+				launches += 12 + ((cfg.guide_mode & gpu::GUIDE_SAMPLE) ? 1u : 0u);
 				q ^= 1u;
 			}
-			RB_CUDA(gpu::launch_next_wave(c->wave, c->film, c->num_sms * 4, c->stream));
-			launches += 2;
+			RB_CUDA(gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream));
 		}
 	}
 	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));

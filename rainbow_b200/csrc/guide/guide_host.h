@@ -1,0 +1,91 @@
+// Host-side state and kernel launchers of the learned path guide.
+#pragma once
+
+#include "../../../include/rbgpu.h"
+#include "guide_net.h"
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rb {
+namespace guide {
+
+// Device-resident counters of the guide (one per context).
+struct device_state {
+	uint32_t step;             // Adam steps taken
+	uint32_t ticket;           // blocks of the running Adam launch that finished
+	uint32_t sample_count;     // training samples stored this wave
+	uint32_t candidates;       // vertices with a positive training weight this wave
+	uint32_t candidates_last;  // the same for the previous wave (sets the keep probability)
+	uint32_t error;            // rb_status of a failed bounded wait, RB_OK if none
+	float last_loss;           // loss of the last step
+	uint32_t rows_last;        // rows of the last step
+	uint32_t usable;           // weights trained or loaded: the renderer may sample the guide
+	uint32_t pad[3];
+};
+
+// One recorded path vertex (5 float4): inputs x0..x8, the continuation
+// direction, the BSDF pdf of that direction, the throughput at the vertex and
+// the path radiance after the vertex's direct lighting.
+constexpr int kVertexFloat4 = 5;
+// One training sample (4 float4): x0..x8, direction, bsdf_pdf, weight.
+constexpr int kSampleFloat4 = 4;
+
+struct guide_state {
+	bool ready = false;              // buffers allocated
+	rb_guide_config cfg{};
+	device_state* dstate = nullptr;
+	float* master = nullptr;         // FP32 weights, device layout (kAugParams)
+	float* adam_m = nullptr;
+	float* adam_v = nullptr;
+	uint8_t* image = nullptr;        // bf16 image of the weights (kImageBytes)
+	float* grad = nullptr;           // summed gradient of the last step (kAugParams), device layout
+	float* partial = nullptr;        // per-CTA gradient partials [ctas][kAugParams]
+	float* partial_loss = nullptr;   // [ctas]
+	int ctas = 0;
+	float4* samples = nullptr;       // training samples of the current wave
+	uint32_t sample_cap = 0;
+	float4* host_samples = nullptr;  // rb_guide_train upload buffer (device)
+	uint32_t host_sample_cap = 0;
+	uint32_t* host_count = nullptr;  // its sample count (device)
+	// per-wave path buffers (sized with the wave)
+	float4* query_in = nullptr;      // 3 per path: the 9 inputs
+	float4* query_out = nullptr;     // 12 per path: decoded guide
+	uint32_t* queue = nullptr;       // paths that need a guide this bounce
+	float4* vertices = nullptr;      // kVertexFloat4 per record, `depth` records per path
+	uint32_t* vertex_count = nullptr;
+	uint32_t wave_capacity = 0;
+	uint32_t depth = 0;
+};
+
+// Pointers the wavefront kernels use (a plain copy inside wave_buffers).
+struct wave_guide {
+	const device_state* dstate;
+	float4* query_in;
+	float4* query_out;
+	uint32_t* queue;
+	float4* vertices;
+	uint32_t* vertex_count;
+	uint32_t depth;
+};
+
+void release(guide_state& g);
+cudaError_t allocate(guide_state& g, int ctas);
+cudaError_t allocate_wave(guide_state& g, uint32_t capacity, uint32_t depth);
+
+// Launchers (guide.cu).
+cudaError_t launch_init_image(const guide_state& g, cudaStream_t s);
+cudaError_t launch_forward_raw(const guide_state& g, const float* x, uint32_t n, float* out, cudaStream_t s);
+cudaError_t launch_forward_queue(const guide_state& g, const uint32_t* count, cudaStream_t s);
+// One training step over min(batch, *count, count_cap) samples: the gradient kernel then
+// the reduction + Adam kernel. sequential: row r uses sample r, else rows draw
+// samples by a hash of (step, row).
+cudaError_t launch_train_step(const guide_state& g, const float4* samples, const uint32_t* count, uint32_t count_cap,
+	uint32_t batch, uint32_t min_rows, bool sequential, cudaStream_t s);
+cudaError_t launch_decode_sample(const float* raw, const float* u, uint32_t n, float* dirs, float* pdfs, cudaStream_t s);
+// Wave end: training samples from the recorded vertices of `paths` paths.
+cudaError_t launch_collect(const guide_state& g, const float4* result, const uint64_t* first_item,
+	const uint64_t* total_items, uint32_t capacity, cudaStream_t s);
+
+} // namespace guide
+} // namespace rb

@@ -148,6 +148,107 @@ __global__ void __launch_bounds__(128) k_trace_rays(scene_view s, const uint32_t
 	}
 }
 
+// ------------------------------------------------------------------ learned guiding
+// The guide's 9 inputs of a surface vertex: position in the scene box, shading
+// normal and outgoing direction, each mapped to [0, 1].
+__device__ __forceinline__ void write_guide_query(const wave_params& p, const surface_t& si, float4* out) {
+	float x[9] = {(si.p.x - p.box_min[0]) * p.box_inv[0], (si.p.y - p.box_min[1]) * p.box_inv[1],
+		(si.p.z - p.box_min[2]) * p.box_inv[2], 0.5f * (si.sz.x + 1.f), 0.5f * (si.sz.y + 1.f), 0.5f * (si.sz.z + 1.f),
+		0.5f * (si.wo.x + 1.f), 0.5f * (si.wo.y + 1.f), 0.5f * (si.wo.z + 1.f)};
+	for (int j = 0; j < 9; j++) x[j] = fminf(1.f, fmaxf(0.f, x[j]));
+	out[0] = make_float4(x[0], x[1], x[2], x[3]);
+	out[1] = make_float4(x[4], x[5], x[6], x[7]);
+	out[2] = make_float4(x[8], 0.f, 0.f, 0.f);
+}
+
+// Path continuation by one-sample MIS of the guide q (probability alpha) and
+// the BSDF: the direction comes from either, and beta is multiplied by
+// f cos / (alpha q + (1 - alpha) p_bsdf), which is unbiased for any guide.
+// g: the decoded guide of this vertex (48 floats in device memory).
+template <int MAT>
+__device__ bool continue_guided(const scene_view& s, path_state& p, const shade_record& rec, const float* g, vec3& wi_out,
+	float& pb_out) {
+	const surface_t& si = rec.si;
+	const bsdf_t b = make_bsdf(s.materials + rec.material);
+	const vec3 wo = to_local(si, si.wo);
+	const float alpha = g[guide::kAlphaOff];
+	const float u_sel = pcg_real(p.rng);
+	const vec2 u = pcg_2d(p.rng);
+	vec3 wi;
+	spectrum f;
+	float pb;
+	if (u_sel < alpha) {
+		float d[3];
+		guide::guide_sample(g, u_sel / alpha, u.x, u.y, d);
+		wi = vec3{d[0], d[1], d[2]};
+		const vec3 wl = to_local(si, wi);
+		f = bsdf_f<MAT>(b, wo, wl, ST_ALL);
+		pb = bsdf_pdf<MAT>(b, wo, wl, ST_ALL);
+	} else {
+		const lobe_sample bs = bsdf_sample<MAT>(b, wo, u, ST_ALL);
+		if (bs.pdf == 0.f) return false;
+		wi = to_world(si, bs.wi);
+		f = bs.f;
+		pb = bs.pdf;
+	}
+	const float pdf = alpha * guide::guide_pdf(g, wi.x, wi.y, wi.z) + (1.f - alpha) * pb;
+	if (is_black(f) || !(pdf > 0.f)) return false;
+	p.beta = p.beta * (f * fabs_ref(dot(wi, si.sz)) / pdf);
+	p.flags &= ~PATH_SPECULAR;
+	const ray_t r = spawn_ray(si.p, si.n, wi);
+	p.o = r.o;
+	p.d = r.d;
+	p.len = r.len;
+	wi_out = wi;
+	pb_out = pb;
+	return true;
+}
+
+// shade_b of a guided or training render: direct lighting as always, the
+// continuation from the guide where it applies (else from the BSDF, with the
+// same random numbers as plain path tracing), and one recorded training vertex
+// per guidable continuation.
+template <int MAT>
+__device__ bool shade_b_guided(const scene_view& s, const wave_buffers& w, const wave_params& p, uint32_t i, path_state& st,
+	const shade_record& rec, const hit_t& sh, const hit_t& mh) {
+	if (!rec.pass_through) {
+		if (rec.did_nee) shade_b_direct<MAT>(s, st, rec, sh, mh);
+		const spectrum beta0 = st.beta, L0 = st.L;
+		vec3 wi;
+		float pb;
+		const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && rec.guidable && w.guide.dstate->usable != 0u;
+		const bool ok = use_guide
+			? continue_guided<MAT>(s, st, rec, reinterpret_cast<const float*>(w.guide.query_out + 12 * i), wi, pb)
+			: continue_bsdf<MAT>(s, st, rec, wi, pb);
+		if (!ok) return false;
+		if ((p.guide_flags & GUIDE_TRAIN) && rec.guidable && st.bounces + 1 < static_cast<int32_t>(p.max_depth)) {
+			const uint32_t nv = w.guide.vertex_count[i];
+			if (nv < w.guide.depth) {
+				float4* r = w.guide.vertices + (static_cast<size_t>(i) * w.guide.depth + nv) * guide::kVertexFloat4;
+				const float4* x = w.guide.query_in + 3 * i;
+				r[0] = x[0];
+				r[1] = x[1];
+				r[2] = make_float4(x[2].x, wi.x, wi.y, wi.z);
+				r[3] = make_float4(pb, beta0.x, beta0.y, beta0.z);
+				r[4] = make_float4(L0.x, L0.y, L0.z, 0.f);
+				w.guide.vertex_count[i] = nv + 1u;
+			}
+		}
+	}
+	return roulette(st, p.max_depth, p.rr_threshold);
+}
+
+__device__ bool shade_b_guided_any(const scene_view& s, const wave_buffers& w, const wave_params& p, uint32_t i,
+	path_state& st, const shade_record& rec, const hit_t& sh, const hit_t& mh) {
+	const uint32_t c = rec.pass_through ? CLASS_OTHER : class_of_material(static_cast<int32_t>(rec.material), s);
+	switch (c) {
+	case CLASS_LAMBERT: return shade_b_guided<class_material(CLASS_LAMBERT)>(s, w, p, i, st, rec, sh, mh);
+	case CLASS_METAL: return shade_b_guided<class_material(CLASS_METAL)>(s, w, p, i, st, rec, sh, mh);
+	case CLASS_GLASS_ROUGH: return shade_b_guided<class_material(CLASS_GLASS_ROUGH)>(s, w, p, i, st, rec, sh, mh);
+	default: return shade_b_guided<MAT_ANY>(s, w, p, i, st, rec, sh, mh);
+	}
+}
+
 // ------------------------------------------------------------------ wavefront
 __device__ __forceinline__ pcg32 load_rng(const wave_buffers& w, const wave_params& p, uint32_t i) {
 	pcg32 g;
@@ -233,6 +334,7 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 			w.pixel[i] = pixel;
 			w.sample[i] = sample;
 			w.result[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+			if (p.guide_flags & GUIDE_TRAIN) w.guide.vertex_count[i] = 0u;
 			store_path(w, i, st);
 		}
 		warp_push(valid, i, w.queue[queue_out], w.counters + CNT_ACTIVE);
@@ -276,7 +378,7 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 	const uint32_t* q = w.class_queue + CLASS * w.capacity;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
-		bool push_shadow = false, push_mis = false;
+		bool push_shadow = false, push_mis = false, push_guide = false;
 		uint32_t i = 0;
 		if (k < n) {
 			i = q[k];
@@ -304,12 +406,17 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 						w.sec_o[2 * i + 1] = make_float4(mr.o.x, mr.o.y, mr.o.z, mr.len);
 						w.sec_d[2 * i + 1] = make_float4(mr.d.x, mr.d.y, mr.d.z, 0.f);
 					}
+					if (p.guide_flags != 0u && r.guidable && !r.pass_through) {
+						write_guide_query(p, r.si, w.guide.query_in + 3 * i);
+						push_guide = (p.guide_flags & GUIDE_SAMPLE) && w.guide.dstate->usable != 0u;
+					}
 				}
 			}
 			store_path(w, i, st);
 		}
 		warp_push(push_shadow, 2 * i, w.sec_queue, w.counters + CNT_SECONDARY);
 		warp_push(push_mis, 2 * i + 1, w.sec_queue, w.counters + CNT_SECONDARY);
+		if (CLASS != CLASS_MISS && p.guide_flags != 0u) warp_push(push_guide, i, w.guide.queue, w.counters + CNT_GUIDE);
 		const uint32_t ns = __popc(__ballot_sync(0xffffffffu, push_shadow));
 		const uint32_t nm = __popc(__ballot_sync(0xffffffffu, push_mis));
 		if ((threadIdx.x & 31u) == 0) {
@@ -362,8 +469,12 @@ __global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, u
 				const shade_record& rec = w.rec[i];
 				const hit_t sh = to_hit(w.sec_hit[2 * i]);
 				const hit_t mh = to_hit(w.sec_hit[2 * i + 1]);
-				alive = CLASS == CLASS_OTHER ? shade_b_any(s, st, rec, sh, mh, p.max_depth, p.rr_threshold)
-					: shade_b<class_material(CLASS)>(s, st, rec, sh, mh, p.max_depth, p.rr_threshold);
+				if (p.guide_flags != 0u)
+					alive = CLASS == CLASS_OTHER ? shade_b_guided_any(s, w, p, i, st, rec, sh, mh)
+						: shade_b_guided<class_material(CLASS)>(s, w, p, i, st, rec, sh, mh);
+				else
+					alive = CLASS == CLASS_OTHER ? shade_b_any(s, st, rec, sh, mh, p.max_depth, p.rr_threshold)
+						: shade_b<class_material(CLASS)>(s, st, rec, sh, mh, p.max_depth, p.rr_threshold);
 				if (!alive) finish(w, i, st.L);
 				store_path(w, i, st);
 			}
@@ -378,6 +489,7 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_ACTIVE] = counters[CNT_NEXT];
 	counters[CNT_NEXT] = 0u;
 	counters[CNT_SECONDARY] = 0u;
+	counters[CNT_GUIDE] = 0u;
 	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
 }
 
@@ -399,6 +511,10 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	k_shade_a<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_MISS><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	if (cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
+		const cudaError_t e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
+		if (e != cudaSuccess) return e;
+	}
 	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
 	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
@@ -449,6 +565,27 @@ cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int g
 	k_film_resolve<<<grid, 256, 0, stream>>>(w, f);
 	k_next_wave<<<1, 1, 0, stream>>>(w.params, w.capacity);
 	return cudaGetLastError();
+}
+
+cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int grid, const launch_cfg& cfg,
+	cudaStream_t stream) {
+	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
+	cudaError_t e = cudaSuccess;
+	if (train) e = guide::launch_collect(*cfg.guide, w.result, &w.params->first_item, &w.params->total_items, w.capacity, stream);
+	if (e == cudaSuccess) e = launch_next_wave(w, f, grid, stream);
+	if (train)
+		for (uint32_t k = 0; k < cfg.guide->cfg.steps_per_wave && e == cudaSuccess; k++)
+			e = guide::launch_train_step(*cfg.guide, cfg.guide->samples, &cfg.guide->dstate->sample_count,
+				cfg.guide->sample_cap, cfg.guide->cfg.batch_size, cfg.guide->cfg.min_rows, false, stream);
+	return e;
+}
+
+uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
+	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
+	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
+	uint32_t n = 3u + (12u + (sample ? 1u : 0u)) * max_depth;
+	if (train) n += 2u + 2u * cfg.guide->cfg.steps_per_wave;
+	return n;
 }
 
 } // namespace gpu

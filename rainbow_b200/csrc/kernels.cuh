@@ -2,6 +2,7 @@
 #pragma once
 
 #include "../../include/rbgpu.h"
+#include "guide/guide_host.h"
 #include "pt/pt_path.h"
 
 #include <cuda_runtime.h>
@@ -16,6 +17,7 @@ enum : uint32_t {
 	CNT_SECONDARY = 2,   // secondary rays queued this bounce
 	CNT_ERROR = 3,       // first device error (rb_status), 0 if none
 	CNT_CLASS = 4,       // paths per shading class this bounce (pt::NUM_CLASSES words)
+	CNT_GUIDE = 9,       // paths queued for a guide evaluation this bounce
 	CNT_EXTEND_RAYS = 10, // 64-bit stats, two words each (lo, hi) from here on
 	CNT_SHADOW_RAYS = 12,
 	CNT_MIS_RAYS = 14,
@@ -39,6 +41,15 @@ struct wave_params {
 	uint32_t seed;
 	uint32_t max_depth;
 	float rr_threshold;
+	uint32_t guide_flags;    // GUIDE_SAMPLE | GUIDE_TRAIN, 0 for plain path tracing
+	float box_min[3];        // scene box, maps vertex positions to the guide's [0, 1] inputs
+	float box_inv[3];
+};
+
+// wave_params::guide_flags
+enum : uint32_t {
+	GUIDE_SAMPLE = 1u,       // continuations sample the guide once it has been trained (one-sample MIS)
+	GUIDE_TRAIN = 2u         // record vertices for training
 };
 
 // Path state of one wave, structure of arrays over `capacity` paths.
@@ -63,6 +74,7 @@ struct wave_buffers {
 	uint32_t* sec_queue;
 	uint32_t* counters;
 	wave_params* params;
+	guide::wave_guide guide;  // null pointers unless a guided render allocated them
 };
 
 struct film_buffers {
@@ -82,6 +94,10 @@ struct launch_cfg {
 	uint32_t* next_event = nullptr;
 	uint32_t max_events = 0;
 	uint8_t* event_kind = nullptr;  // 0 extend, 1 secondary
+	// learned guiding: the guide state and the host-side mode (GUIDE_SAMPLE |
+	// GUIDE_TRAIN) deciding which guide kernels are launched
+	const guide::guide_state* guide = nullptr;
+	uint32_t guide_mode = 0;
 };
 
 // Ray batches for rb_trace_closest / rb_trace_shadow.
@@ -96,6 +112,14 @@ cudaError_t launch_wave(const pt::scene_view& s, const wave_buffers& w, const fi
 // Adds the wave's finished samples to the film, then advances
 // params->first_item by the wave capacity (the last nodes of a wave).
 cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream);
+
+// Wave end with learned guiding: training-sample collection, film resolve,
+// next-wave advance, then the training steps (cfg.guide_mode & GUIDE_TRAIN).
+cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int grid, const launch_cfg& cfg,
+	cudaStream_t stream);
+
+// Kernel launches of one wave for a given configuration (for the stats).
+uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg);
 
 // One extra bounce (used when invisible entities make paths outlive max_depth iterations).
 cudaError_t launch_bounce(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,

@@ -37,6 +37,7 @@ struct shade_record {
 	uint32_t material;
 	uint32_t pass_through;        // invisible entity: continue straight on
 	uint32_t did_nee;             // uniform_sample_one_emitter was called
+	uint32_t guidable;            // BSDF without specular lobes: a learned guide may sample here
 	int32_t nee_entity;           // emitter entity of the shadow ray, -1: no shadow ray
 	spectrum nee_L;               // its contribution if unoccluded
 	uint32_t mis_valid;
@@ -119,6 +120,7 @@ template <int MAT = MAT_ANY>
 RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_record& rec) {
 	rec.pass_through = 0u;
 	rec.did_nee = 0u;
+	rec.guidable = 0u;
 	rec.nee_entity = -1;
 	rec.mis_valid = 0u;
 	const bool count_emission = p.bounces == 0 || (p.flags & PATH_SPECULAR);
@@ -146,6 +148,7 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 	const bsdf_t b = make_bsdf(s.materials + ent.material);
 	if (bsdf_count(b, ST_NON_SPECULAR) == 0) return true;
 	rec.did_nee = 1u;
+	rec.guidable = bsdf_count(b, ST_SPECULAR) == 0 ? 1u : 0u;
 	const vec3 wo = to_local(si, si.wo);
 	// emitter sampling half (integrator.cpp:121-159)
 	const float n = static_cast<float>(s.num_emitters);
@@ -182,65 +185,75 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 	return true;
 }
 
-// Returns false when the path ends (BSDF sample failed, Russian roulette, max depth).
+// Direct lighting half of shade_b: the unoccluded NEE sample and the MIS
+// BSDF sample that found an emitter (integrator.cpp:121-198), added to the path.
 // shadow / mis are the closest visible hits of rec.shadow_ray / rec.mis_ray.
 template <int MAT = MAT_ANY>
-RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, const hit_t& shadow, const hit_t& mis,
-	uint32_t max_depth, float rr_threshold) {
-	if (!rec.pass_through) {
-		const surface_t& si = rec.si;
-		if (rec.did_nee) {
-			spectrum Ls = splat3(0.f);
-			if (rec.nee_entity >= 0 && (shadow.slot < 0 || hit_entity(s, shadow.slot) == static_cast<uint32_t>(rec.nee_entity)))
-				Ls = Ls + rec.nee_L;
-			if (rec.mis_valid) {
-				// find_emitter (integrator.cpp:49-82) and the MIS term (:165-195)
-				bool found = false;
-				spectrum Le = splat3(0.f);
-				float epdf = 0.f;
-				const float pick_pdf = 1.f / static_cast<float>(s.num_emitters);
-				if (mis.slot >= 0) {
-					const uint32_t e = hit_entity(s, mis.slot);
-					const entity_rec& ent = s.entities[e];
-					if (ent.flags & ENT_HAS_EMITTER) {
-						const surface_t es = make_surface(s, mis.slot, mis.b1, mis.b2, rec.mis_ray.o, rec.mis_ray.d);
-						const emitter_rec& em = s.emitters[ent.emitter];
-						Le = surface_emission(ent, em, es.n, -rec.mis_wi);
-						epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
-						found = true;
-					}
-				} else if (s.num_environments > 0) {
-					const float ne = static_cast<float>(s.num_environments);
-					uint32_t which = static_cast<uint32_t>(floorf(pcg_real(p.rng) * ne));
-					if (which > s.num_environments - 1) which = s.num_environments - 1;
-					const emitter_rec& em = s.emitters[s.environments[which]];
-					Le = em.radiance;
-					epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
-					found = true;
-				}
-				if (found && !is_black(Le) && epdf > 0.f) {
-					const float w = rec.mis_specular ? 1.f : power_heuristic(rec.mis_pdf, epdf);
-					Ls = Ls + rec.mis_f * Le * w / rec.mis_pdf;
-				}
+RB_HD void shade_b_direct(const scene_view& s, path_state& p, const shade_record& rec, const hit_t& shadow, const hit_t& mis) {
+	const surface_t& si = rec.si;
+	spectrum Ls = splat3(0.f);
+	if (rec.nee_entity >= 0 && (shadow.slot < 0 || hit_entity(s, shadow.slot) == static_cast<uint32_t>(rec.nee_entity)))
+		Ls = Ls + rec.nee_L;
+	if (rec.mis_valid) {
+		// find_emitter (integrator.cpp:49-82) and the MIS term (:165-195)
+		bool found = false;
+		spectrum Le = splat3(0.f);
+		float epdf = 0.f;
+		const float pick_pdf = 1.f / static_cast<float>(s.num_emitters);
+		if (mis.slot >= 0) {
+			const uint32_t e = hit_entity(s, mis.slot);
+			const entity_rec& ent = s.entities[e];
+			if (ent.flags & ENT_HAS_EMITTER) {
+				const surface_t es = make_surface(s, mis.slot, mis.b1, mis.b2, rec.mis_ray.o, rec.mis_ray.d);
+				const emitter_rec& em = s.emitters[ent.emitter];
+				Le = surface_emission(ent, em, es.n, -rec.mis_wi);
+				epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
+				found = true;
 			}
-			p.L = p.L + p.beta * Ls;
+		} else if (s.num_environments > 0) {
+			const float ne = static_cast<float>(s.num_environments);
+			uint32_t which = static_cast<uint32_t>(floorf(pcg_real(p.rng) * ne));
+			if (which > s.num_environments - 1) which = s.num_environments - 1;
+			const emitter_rec& em = s.emitters[s.environments[which]];
+			Le = em.radiance;
+			epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
+			found = true;
 		}
-		// path continuation (integrator.cpp:380-399)
-		const bsdf_t b = make_bsdf(s.materials + rec.material);
-		const vec3 wo = to_local(si, si.wo);
-		const lobe_sample bs = bsdf_sample<MAT>(b, wo, pcg_2d(p.rng), ST_ALL);
-		if (is_black(bs.f) || bs.pdf == 0.f) return false;
-		const vec3 wi = to_world(si, bs.wi);
-		p.beta = p.beta * (bs.f * fabs_ref(dot(wi, si.sz)) / bs.pdf);
-		p.flags = type_match(bs.type, ST_SPECULAR) ? (p.flags | PATH_SPECULAR) : (p.flags & ~PATH_SPECULAR);
-		if (type_match(bs.type, ST_SPECULAR | ST_TRANSMISSION))
-			p.eta = p.eta * ((dot(si.wo, si.n) > 0.f) ? (b.eta * b.eta) : (1.f / (b.eta * b.eta)));
-		const ray_t r = spawn_ray(si.p, si.n, wi);
-		p.o = r.o;
-		p.d = r.d;
-		p.len = r.len;
+		if (found && !is_black(Le) && epdf > 0.f) {
+			const float w = rec.mis_specular ? 1.f : power_heuristic(rec.mis_pdf, epdf);
+			Ls = Ls + rec.mis_f * Le * w / rec.mis_pdf;
+		}
 	}
-	// Russian roulette (path_integrator.cpp:35-43)
+	p.L = p.L + p.beta * Ls;
+}
+
+// Path continuation by BSDF sampling (integrator.cpp:380-399). Returns false
+// when the BSDF sample fails; otherwise updates beta, the specular flag, eta
+// and the ray, and reports the world direction and its pdf.
+template <int MAT = MAT_ANY>
+RB_HD bool continue_bsdf(const scene_view& s, path_state& p, const shade_record& rec, vec3& wi_out, float& pdf_out) {
+	const surface_t& si = rec.si;
+	const bsdf_t b = make_bsdf(s.materials + rec.material);
+	const vec3 wo = to_local(si, si.wo);
+	const lobe_sample bs = bsdf_sample<MAT>(b, wo, pcg_2d(p.rng), ST_ALL);
+	if (is_black(bs.f) || bs.pdf == 0.f) return false;
+	const vec3 wi = to_world(si, bs.wi);
+	p.beta = p.beta * (bs.f * fabs_ref(dot(wi, si.sz)) / bs.pdf);
+	p.flags = type_match(bs.type, ST_SPECULAR) ? (p.flags | PATH_SPECULAR) : (p.flags & ~PATH_SPECULAR);
+	if (type_match(bs.type, ST_SPECULAR | ST_TRANSMISSION))
+		p.eta = p.eta * ((dot(si.wo, si.n) > 0.f) ? (b.eta * b.eta) : (1.f / (b.eta * b.eta)));
+	const ray_t r = spawn_ray(si.p, si.n, wi);
+	p.o = r.o;
+	p.d = r.d;
+	p.len = r.len;
+	wi_out = wi;
+	pdf_out = bs.pdf;
+	return true;
+}
+
+// Russian roulette (path_integrator.cpp:35-43) and the bounce count; false
+// when the path ends.
+RB_HD bool roulette(path_state& p, uint32_t max_depth, float rr_threshold) {
 	const float mc = spectrum_max(p.beta * p.eta);
 	if (mc < rr_threshold && p.bounces > 3) {
 		const float q = fmax_ref(0.05f, 1.f - mc);
@@ -249,6 +262,20 @@ RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, 
 	}
 	p.bounces++;
 	return p.bounces < static_cast<int32_t>(max_depth);
+}
+
+// Returns false when the path ends (BSDF sample failed, Russian roulette, max depth).
+// shadow / mis are the closest visible hits of rec.shadow_ray / rec.mis_ray.
+template <int MAT = MAT_ANY>
+RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, const hit_t& shadow, const hit_t& mis,
+	uint32_t max_depth, float rr_threshold) {
+	if (!rec.pass_through) {
+		if (rec.did_nee) shade_b_direct<MAT>(s, p, rec, shadow, mis);
+		vec3 wi;
+		float pdf;
+		if (!continue_bsdf<MAT>(s, p, rec, wi, pdf)) return false;
+	}
+	return roulette(p, max_depth, rr_threshold);
 }
 
 // Run-time dispatch to the class-specialised stages (the host build uses it;
