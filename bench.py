@@ -14,6 +14,17 @@ stream (inputs resident in HBM); `e2e` is the same metric through the public C
 ABI with the step's parameters copied in and the film read back to host memory
 every step. L2 is flushed (a 256 MiB write) before every timed step.
 
+The `guided` object is the metric's comparison itself: on the hard-indirect
+room (2,048,000 clutter triangles of 100 displaced icospheres at subdivision 5,
+a 0.5 x 0.5 emitter of radiance 50 facing away from a 0.3-wide slit, glossy
+Trowbridge-Reitz floor and walls), the device time plain path tracing and
+guided path tracing (the learned guide trained online from scratch inside the
+same run, training time included) need until the relMSE against a converged
+plain render falls to each target. The resolution (256 x 256 by default instead
+of 1024 x 1024) and the reference's spp (16,384 instead of 65,536) are reduced
+so that the default run takes minutes; relMSE is a per-pixel mean, so the spp
+each form needs does not depend on the resolution to first order.
+
 --impl reference times the reference CPU integrator (path_integrator::trace of
 the reference sources, compiled as oracle/_ref) on a bounded sample of each step
 on all host cores.
@@ -36,6 +47,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(kind=1, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4, max_depth=8)
+GUIDED = dict(kind=2, seed=3, num_spheres=100, subdivision=5, max_depth=8)
 METRIC = "time to relMSE 0.01: guided vs plain wavefront PT on 1 B200; Msamples/s"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -152,6 +164,54 @@ def config_dict(world, l2="flushed before every timed step (256 MiB write)"):
             "l2": l2}
 
 
+def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp):
+    """Device time to each relMSE target: plain vs guided (online training)."""
+    scene = rb.generate_scene(GUIDED["kind"], seed=GUIDED["seed"], width=res, height=res,
+                              num_spheres=GUIDED["num_spheres"], subdivision=GUIDED["subdivision"])
+    depth = GUIDED["max_depth"]
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    t0 = time.perf_counter()
+    ctx.render(scene.camera, ref_spp, max_depth=depth, seed=1000, want_image=False)
+    s, _, c = ctx.film()
+    ref = s / c[..., None]
+    ref_s = time.perf_counter() - t0
+
+    def relmse():
+        s, _, c = ctx.film()
+        m = s / c[..., None]
+        return float(np.mean((m - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    out = {}
+    for mode in ("plain", "guided"):
+        guided = mode == "guided"
+        if guided:
+            ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=1 << 18, steps_per_wave=8, min_rows=4096)
+        ms, spp, left, hit = 0.0, 0, sorted(targets, reverse=True), {}
+        while left and spp < max_spp:
+            ctx.render(scene.camera, chunk, first_sample=spp, max_depth=depth, seed=7, reset=(spp == 0), guide=guided,
+                       train=guided, paths_per_wave=res * res * chunk, want_image=False)
+            ms += ctx.stats().elapsed_ms
+            spp += chunk
+            e = relmse()
+            while left and e <= left[0]:
+                hit[left.pop(0)] = {"s": ms / 1e3, "spp": spp, "relmse": e}
+        out[mode] = hit
+        if guided:
+            st = ctx.guide_stats()
+            out["guide"] = {"adam_steps": st.steps, "last_loss": st.last_loss, "device_error": st.device_error}
+    ctx.close()
+    res_t = {}
+    for t in targets:
+        p, g = out["plain"].get(t), out["guided"].get(t)
+        res_t[str(t)] = {"plain_s": p and p["s"], "plain_spp": p and p["spp"], "guided_s": g and g["s"],
+                         "guided_spp": g and g["spp"], "speedup": (p["s"] / g["s"]) if (p and g) else None}
+    return {"workload": f"slit room, {GUIDED['num_spheres'] * 20480 + 18} triangles, {res}x{res}, max depth {depth}, "
+                        f"chunks of {chunk} spp (one wave each, 8 Adam steps of up to 2^18 samples after each guided wave)",
+            "reference": f"plain, {ref_spp} spp, FP64 accumulation ({ref_s:.1f} s)", "targets": res_t,
+            "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,6 +221,10 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=64, help="image rows per step timed on the CPU reference")
     ap.add_argument("--cpu-rows", type=int, default=512, help="rows (a central band) of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-guided", action="store_true")
+    ap.add_argument("--guided-res", type=int, default=256)
+    ap.add_argument("--guided-ref-spp", type=int, default=16384)
+    ap.add_argument("--guided-chunk", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -271,6 +335,13 @@ def main():
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
+    guided = None
+    if rank == 0 and world == 1 and not args.no_guided:
+        try:
+            guided = guided_leg(rb, local, args.guided_res, args.guided_ref_spp, (0.01, 0.001), args.guided_chunk, 8192)
+        except Exception as e:  # reported, never required for the throughput line
+            guided = {"error": str(e)}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
@@ -283,7 +354,7 @@ def main():
                          "kernel": "k_extend + k_trace_secondary (BVH traversal)",
                          "algorithmic_bytes_per_launch": alg_bytes / nl, "ms_per_launch": trav_ms / nl,
                          "launches": nl},
-            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches, "guided": guided,
         }
         print(json.dumps(line))
     ctx.close()

@@ -302,8 +302,10 @@ rb_status rb_checkpoint_load(rb_context* ctx, const char* path);
  * samples the BSDF alone, exactly as without the flag. With RB_RENDER_TRAIN
  * each finished wave turns its recorded vertices into training samples
  * (direction, BSDF pdf and weight = luminance of the radiance the continuation
- * brought back over the throughput at the vertex) and runs steps_per_wave Adam
- * steps of the loss -weight * (log q + log(alpha q + (1 - alpha) p_bsdf)). */
+ * brought back over the throughput at the vertex), appends them to a replay
+ * ring that keeps the samples of earlier waves, and runs steps_per_wave Adam
+ * steps on batches drawn from the whole ring, of the loss
+ * -weight * (log q + log(alpha q + (1 - alpha) p_bsdf)). */
 #define RB_GUIDE_NUM_PARAMS 30000u  /* flat W1[64][224] b1[64] W2[64][64] b2 W3 b3 W4 b4 W5[48][64] b5[48] */
 #define RB_GUIDE_INPUTS 9u
 #define RB_GUIDE_OUTPUTS 48u        /* raw outputs: lobe i at 5i..5i+4 (mean xyz, log kappa, weight logit), alpha logit at 40 */
@@ -311,10 +313,13 @@ typedef struct rb_guide_config {
 	uint32_t seed;              /* weight initialisation */
 	float learning_rate;        /* Adam step size, 0: 1e-3 */
 	uint32_t batch_size;        /* rows per training step, 0: 2^18 */
-	uint32_t steps_per_wave;    /* training steps after each wave of a RB_RENDER_TRAIN render, 0: 4 */
-	uint32_t max_samples;       /* training samples kept per wave, 0: 2^21 */
+	uint32_t steps_per_wave;    /* training steps after each wave of a RB_RENDER_TRAIN render, 0: 8 */
+	uint32_t max_samples;       /* replay ring of training samples (rounded up to a power of two), 0: 2^21 */
 	uint32_t min_rows;          /* steps with fewer collected samples are skipped, 0: 4096 */
-	uint32_t reserved[2];
+	float weight_clip;          /* rendering-time training clips each weight at this multiple of the
+	                               running mean weight (fewer steps dominated by rare paths), 0: 16,
+	                               < 0: no clipping */
+	uint32_t reserved;
 } rb_guide_config;
 /* One training sample (64 bytes). */
 typedef struct rb_guide_sample {

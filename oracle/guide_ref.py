@@ -32,7 +32,7 @@ N_OUT = 48
 N_LOBES = 8
 LAYERS = [(K1, HID), (HID, HID), (HID, HID), (HID, HID), (HID, N_OUT)]
 NUM_PARAMS = sum(i * o + o for i, o in LAYERS)  # 30000
-KAPPA_MIN, KAPPA_MAX = -4.0, 6.0  # clamp of the log-concentration
+KAPPA_MIN, KAPPA_MAX = -4.0, 8.0  # clamp of the log-concentration
 ALPHA_LO, ALPHA_HI = 0.1, 0.9      # range of the guide selection probability
 EPS_UNIFORM = 0.02                 # share of the uniform sphere density in q
 NORM_FLOOR = 1e-6                  # |m| floor in the mean-direction gradient

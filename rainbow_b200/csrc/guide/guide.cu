@@ -348,6 +348,8 @@ struct train_args {
 	uint32_t batch;
 	uint32_t min_rows;
 	uint32_t sequential;
+	uint32_t budgeted;
+	float weight_clip;          // > 0: weights clipped at weight_clip * state->weight_mean
 	const device_state* state;
 	float* partial;             // [gridDim.x][kAugParams]
 	float* partial_loss;        // [gridDim.x]
@@ -359,6 +361,7 @@ __device__ __forceinline__ uint32_t step_rows(uint32_t count, uint32_t batch, ui
 }
 
 __global__ void __launch_bounds__(128, 1) k_train(train_args a) {
+	if (a.budgeted && a.state->wave_step >= a.state->wave_budget) return;
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = align128(smem_raw);
 	const uint32_t t = threadIdx.x, warp = t >> 5;
@@ -382,6 +385,7 @@ __global__ void __launch_bounds__(128, 1) k_train(train_args a) {
 	const float inv_n = rows ? 1.f / static_cast<float>(rows) : 0.f;
 	const uint32_t tiles = (rows + kTileRows - 1) / kTileRows;
 	const uint32_t step = a.state->step;
+	const float wmax = a.weight_clip > 0.f && a.state->weight_mean > 0.f ? a.weight_clip * a.state->weight_mean : INFINITY;
 	uint64_t* bar = &bars[1];
 	uint32_t phase = 0;
 	bool first = true, failed = !loaded;
@@ -399,7 +403,7 @@ __global__ void __launch_bounds__(128, 1) k_train(train_args a) {
 			x[0] = s0.x; x[1] = s0.y; x[2] = s0.z; x[3] = s0.w;
 			x[4] = s1.x; x[5] = s1.y; x[6] = s1.z; x[7] = s1.w; x[8] = s2.x;
 			dx = s2.y; dy = s2.z; dz = s2.w;
-			pb = s3.x; wgt = s3.y;
+			pb = s3.x; wgt = fminf(s3.y, wmax);
 		}
 		encode_row(x, X0, t);
 		// forward
@@ -505,6 +509,7 @@ struct adam_args {
 	uint32_t count_cap;
 	uint32_t batch;
 	uint32_t min_rows;
+	uint32_t budgeted;
 	float lr;
 };
 
@@ -512,6 +517,7 @@ struct adam_args {
 // beta2 0.999, eps 1e-8, bias-corrected) on the FP32 master weights and a
 // fresh BF16 image. The last block to finish advances the step counter.
 __global__ void __launch_bounds__(256) k_adam(adam_args a) {
+	if (a.budgeted && a.state->wave_step >= a.state->wave_budget) return;
 	const uint32_t rows = step_rows(min(*a.count, a.count_cap), a.batch, a.min_rows);
 	if (rows == 0u) return;
 	const uint32_t t_step = a.state->step + 1u;
@@ -546,6 +552,7 @@ __global__ void __launch_bounds__(256) k_adam(adam_args a) {
 		if (atomicAdd(&a.state->ticket, 1u) == gridDim.x - 1u) {
 			a.state->step = t_step;
 			a.state->usable = 1u;
+			a.state->wave_step += 1u;
 			a.state->ticket = 0u;
 			__threadfence();
 		}
@@ -590,13 +597,29 @@ struct collect_args {
 __global__ void k_collect_begin(device_state* s) {
 	s->candidates_last = s->candidates;
 	s->candidates = 0u;
-	s->sample_count = 0u;
+	s->wave_written = 0u;
+	s->wave_weight = 0.f;
+}
+
+// Ring fill, running mean of the weights (an exponential average over waves,
+// weight 1/4 for the newest), and this wave's training budget (steps_per_wave steps).
+__global__ void k_collect_end(device_state* s, uint32_t cap, uint32_t steps) {
+	const uint32_t f = s->ring_filled + s->wave_written;
+	s->ring_filled = f < cap ? f : cap;
+	if (s->wave_written > 0u) {
+		const float m = s->wave_weight / static_cast<float>(s->wave_written);
+		s->weight_mean = s->weight_mean > 0.f ? 0.75f * s->weight_mean + 0.25f * m : m;
+	}
+	s->wave_budget = steps;
+	s->wave_step = 0u;
 }
 
 // One thread per path of the wave: every recorded vertex with a positive
 // weight is a candidate; candidates are kept with probability
-// min(1, 0.9 cap / candidates of the previous wave) so that the kept set
-// spreads over the whole image, and stored while there is room.
+// min(1, 0.9 cap / candidates of the previous wave), so that one wave never
+// fills the ring with the first part of the image only, and written into the
+// replay ring over its oldest samples. Every sample carries the pdf its
+// direction was drawn with, so samples of older guides stay valid.
 __global__ void __launch_bounds__(256) k_collect(collect_args a) {
 	const uint64_t first = *a.first_item, total = *a.total_items;
 	const uint64_t left = total > first ? total - first : 0;
@@ -634,18 +657,23 @@ __global__ void __launch_bounds__(256) k_collect(collect_args a) {
 			uint32_t slot0 = 0;
 			if (lane == 0) {
 				if (cmask) atomicAdd(&a.state->candidates, static_cast<uint32_t>(__popc(cmask)));
-				if (kmask) slot0 = atomicAdd(&a.state->sample_count, static_cast<uint32_t>(__popc(kmask)));
+				if (kmask) {
+					slot0 = atomicAdd(&a.state->ring_head, static_cast<uint32_t>(__popc(kmask)));
+					atomicAdd(&a.state->wave_written, static_cast<uint32_t>(__popc(kmask)));
+				}
 			}
 			slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+			float wsum = kept ? wgt : 0.f;
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+			if (lane == 0 && kmask) atomicAdd(&a.state->wave_weight, wsum);
 			if (kept) {
-				const uint32_t slot = slot0 + __popc(kmask & ((1u << lane) - 1u));
-				if (slot < a.cap) {
-					float4* s = a.samples + static_cast<size_t>(kSampleFloat4) * slot;
-					s[0] = r0;
-					s[1] = r1;
-					s[2] = r2;                                      // x8, direction
-					s[3] = make_float4(r3.x, wgt, 0.f, 0.f);        // bsdf pdf, weight
-				}
+				const uint32_t slot = (slot0 + __popc(kmask & ((1u << lane) - 1u))) & (a.cap - 1u);
+				float4* s = a.samples + static_cast<size_t>(kSampleFloat4) * slot;
+				s[0] = r0;
+				s[1] = r1;
+				s[2] = r2;                                      // x8, direction
+				s[3] = make_float4(r3.x, wgt, 0.f, 0.f);        // bsdf pdf, weight
 			}
 		}
 	}
@@ -740,7 +768,7 @@ cudaError_t launch_forward_queue(const guide_state& g, const uint32_t* count, cu
 }
 
 cudaError_t launch_train_step(const guide_state& g, const float4* samples, const uint32_t* count, uint32_t count_cap,
-	uint32_t batch, uint32_t min_rows, bool sequential, cudaStream_t s) {
+	uint32_t batch, uint32_t min_rows, bool sequential, bool budgeted, cudaStream_t s) {
 	train_args t{};
 	t.image = g.image;
 	t.samples = samples;
@@ -749,6 +777,8 @@ cudaError_t launch_train_step(const guide_state& g, const float4* samples, const
 	t.batch = batch;
 	t.min_rows = min_rows;
 	t.sequential = sequential ? 1u : 0u;
+	t.budgeted = budgeted ? 1u : 0u;
+	t.weight_clip = budgeted ? g.weight_clip : 0.f;
 	t.state = g.dstate;
 	t.partial = g.partial;
 	t.partial_loss = g.partial_loss;
@@ -768,6 +798,7 @@ cudaError_t launch_train_step(const guide_state& g, const float4* samples, const
 	a.count_cap = count_cap;
 	a.batch = batch;
 	a.min_rows = min_rows;
+	a.budgeted = budgeted ? 1u : 0u;
 	a.lr = g.cfg.learning_rate;
 	k_adam<<<(kAugParams + 255) / 256, 256, 0, s>>>(a);
 	return cudaGetLastError();
@@ -794,6 +825,7 @@ cudaError_t launch_collect(const guide_state& g, const float4* result, const uin
 	a.cap = g.sample_cap;
 	a.state = g.dstate;
 	k_collect<<<g.ctas * 8, 256, 0, s>>>(a);
+	k_collect_end<<<1, 1, 0, s>>>(g.dstate, g.sample_cap, g.cfg.steps_per_wave);
 	return cudaGetLastError();
 }
 

@@ -47,7 +47,11 @@ struct splitmix {
 };
 
 // He-uniform weights over the live inputs, zero biases; the output layer is
-// scaled by 0.1 (an almost uniform untrained guide) and its unused rows are zero.
+// scaled by 0.1 (an almost uniform untrained guide) and its unused rows are
+// zero. First-layer weights of encoding octave k > 3 start 2^-(k-3) smaller:
+// at 2^k pi with k near 11 a feature changes sign every few millimetres of the
+// scene, so the untrained network starts smooth and sharpens where the
+// training data asks for it.
 std::vector<float> default_params(uint32_t seed) {
 	std::vector<float> p(kNumParams, 0.f);
 	splitmix rng{0x5EEDull ^ (static_cast<uint64_t>(seed) << 20)};
@@ -58,7 +62,9 @@ std::vector<float> default_params(uint32_t seed) {
 		for (int o = 0; o < out; o++)
 			for (int i = 0; i < in; i++) {
 				const float u = rng.uniform();
-				w[o * in + i] = (i < live && !(l == kLayers - 1 && o > 40)) ? (2.f * u - 1.f) * lim : 0.f;
+				const int octave = (i % 24) / 2;  // feature 24 j + 2 k + s
+				const float scale = (l == 0 && octave > 3) ? std::ldexp(1.f, 3 - octave) : 1.f;
+				w[o * in + i] = (i < live && !(l == kLayers - 1 && o > 40)) ? (2.f * u - 1.f) * lim * scale : 0.f;
 			}
 	}
 	return p;
@@ -144,13 +150,17 @@ rb_status rb_guide_init(rb_context* ctx, const rb_guide_config* config) {
 	if (config) cfg = *config;
 	if (!(cfg.learning_rate > 0.f)) cfg.learning_rate = 1e-3f;
 	if (cfg.batch_size == 0) cfg.batch_size = 1u << 18;
-	if (cfg.steps_per_wave == 0) cfg.steps_per_wave = 4;
+	if (cfg.steps_per_wave == 0) cfg.steps_per_wave = 8;
 	if (cfg.max_samples == 0) cfg.max_samples = 1u << 21;
 	if (cfg.min_rows == 0) cfg.min_rows = 4096;
 	if (cfg.batch_size > (1u << 24) || cfg.max_samples > (1u << 26) || cfg.steps_per_wave > 64) return RB_ERR_INVALID_ARGUMENT;
+	uint32_t ring = 1024u;
+	while (ring < cfg.max_samples) ring <<= 1;  // the replay ring holds a power of two
+	cfg.max_samples = ring;
 	guide_state& g = *gc.g;
 	g.cfg = cfg;
 	g.sample_cap = cfg.max_samples;
+	g.weight_clip = cfg.weight_clip == 0.f ? 16.f : (cfg.weight_clip < 0.f ? 0.f : cfg.weight_clip);
 	const cudaError_t e = allocate(g, gc.sms);
 	if (e != cudaSuccess) {
 		release(g);
@@ -232,7 +242,7 @@ rb_status rb_guide_train(rb_context* ctx, const rb_guide_sample* samples, uint32
 	const bool sequential = (flags & RB_GUIDE_SEQUENTIAL) != 0;
 	const uint32_t batch = sequential ? (n > 0 ? n : 1u) : g.cfg.batch_size;
 	for (uint32_t k = 0; k < steps; k++)
-		RB_CUDA(launch_train_step(g, g.host_samples, g.host_count, n, batch, 1u, sequential, gc.stream));
+		RB_CUDA(launch_train_step(g, g.host_samples, g.host_count, n, batch, 1u, sequential, false, gc.stream));
 	RB_CUDA(cudaStreamSynchronize(gc.stream));
 	if (gradient) {
 		std::vector<float> a(kAugParams);
@@ -277,7 +287,7 @@ rb_status rb_guide_stats_get(rb_context* ctx, rb_guide_stats* out) {
 	device_state s{};
 	RB_CUDA(cudaMemcpy(&s, gc.g->dstate, sizeof(s), cudaMemcpyDeviceToHost));
 	out->steps = s.step;
-	out->samples_last_wave = s.sample_count < gc.g->sample_cap ? s.sample_count : gc.g->sample_cap;
+	out->samples_last_wave = s.wave_written;
 	out->candidates_last_wave = s.candidates;
 	out->device_error = s.error;
 	out->last_loss = s.last_loss;

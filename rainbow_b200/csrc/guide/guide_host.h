@@ -14,14 +14,20 @@ namespace guide {
 struct device_state {
 	uint32_t step;             // Adam steps taken
 	uint32_t ticket;           // blocks of the running Adam launch that finished
-	uint32_t sample_count;     // training samples stored this wave
+	uint32_t ring_head;        // training samples written since the guide was created (ring index, mod 2^32)
 	uint32_t candidates;       // vertices with a positive training weight this wave
 	uint32_t candidates_last;  // the same for the previous wave (sets the keep probability)
 	uint32_t error;            // rb_status of a failed bounded wait, RB_OK if none
 	float last_loss;           // loss of the last step
 	uint32_t rows_last;        // rows of the last step
 	uint32_t usable;           // weights trained or loaded: the renderer may sample the guide
-	uint32_t pad[3];
+	uint32_t wave_written;     // training samples written by the current wave
+	uint32_t ring_filled;      // samples in the ring (<= capacity); the training steps draw from all of them
+	uint32_t wave_budget;      // training steps to run after this wave (the launches beyond it return at once)
+	uint32_t wave_step;        // training steps run after this wave so far
+	float wave_weight;         // sum of the weights written by this wave
+	float weight_mean;         // running mean of the training weights (exponential over waves)
+	uint32_t pad;
 };
 
 // One recorded path vertex (5 float4): inputs x0..x8, the continuation
@@ -34,6 +40,7 @@ constexpr int kSampleFloat4 = 4;
 struct guide_state {
 	bool ready = false;              // buffers allocated
 	rb_guide_config cfg{};
+	float weight_clip = 16.f;        // training weights clipped at this multiple of their running mean
 	device_state* dstate = nullptr;
 	float* master = nullptr;         // FP32 weights, device layout (kAugParams)
 	float* adam_m = nullptr;
@@ -43,8 +50,8 @@ struct guide_state {
 	float* partial = nullptr;        // per-CTA gradient partials [ctas][kAugParams]
 	float* partial_loss = nullptr;   // [ctas]
 	int ctas = 0;
-	float4* samples = nullptr;       // training samples of the current wave
-	uint32_t sample_cap = 0;
+	float4* samples = nullptr;       // replay ring of training samples, filled by every training wave
+	uint32_t sample_cap = 0;         // ring capacity, a power of two
 	float4* host_samples = nullptr;  // rb_guide_train upload buffer (device)
 	uint32_t host_sample_cap = 0;
 	uint32_t* host_count = nullptr;  // its sample count (device)
@@ -79,9 +86,10 @@ cudaError_t launch_forward_raw(const guide_state& g, const float* x, uint32_t n,
 cudaError_t launch_forward_queue(const guide_state& g, const uint32_t* count, cudaStream_t s);
 // One training step over min(batch, *count, count_cap) samples: the gradient kernel then
 // the reduction + Adam kernel. sequential: row r uses sample r, else rows draw
-// samples by a hash of (step, row).
+// samples by a hash of (step, row). budgeted: the step runs only while the
+// wave's step budget (device_state::wave_budget) is not used up.
 cudaError_t launch_train_step(const guide_state& g, const float4* samples, const uint32_t* count, uint32_t count_cap,
-	uint32_t batch, uint32_t min_rows, bool sequential, cudaStream_t s);
+	uint32_t batch, uint32_t min_rows, bool sequential, bool budgeted, cudaStream_t s);
 cudaError_t launch_decode_sample(const float* raw, const float* u, uint32_t n, float* dirs, float* pdfs, cudaStream_t s);
 // Wave end: training samples from the recorded vertices of `paths` paths.
 cudaError_t launch_collect(const guide_state& g, const float4* result, const uint64_t* first_item,

@@ -43,7 +43,7 @@ constexpr int kAugParams = 33536;     // device parameters, per layer [out][K] w
 constexpr uint32_t kImageBytes = 2u * kAugParams;  // bf16 image of all layers (67,072 bytes)
 constexpr int kTileRows = 128;        // rows per tensor-core tile (MMA M)
 
-constexpr float kKappaMin = -4.f, kKappaMax = 6.f;   // clamp of the log-concentration
+constexpr float kKappaMin = -4.f, kKappaMax = 8.f;   // clamp of the log-concentration
 constexpr float kAlphaLo = 0.1f, kAlphaHi = 0.9f;    // range of the guide selection probability
 constexpr float kEpsUniform = 0.02f;                 // uniform share of the guide density
 constexpr float kNormFloor = 1e-6f;

@@ -393,9 +393,11 @@ void build_slit_room(rb_scene& s, uint32_t seed, uint32_t count, int level, int 
 	mesh_data back;
 	back.add_quad(vec3{0, 0, 0}, vec3{10, 0, 0}, vec3{10, 5, 0}, vec3{0, 5, 0});
 	s.add_entity(std::move(back), white, -1, identity_xf());
-	// 0.5 x 0.5 light facing the slit (+z), radiance 50
+	// 0.5 x 0.5 light, radiance 50, facing the back wall of its chamber (-z):
+	// no point of the room sees it, all light enters the room through the slit
+	// after at least one bounce in the chamber (hard indirect lighting)
 	mesh_data lq;
-	lq.add_quad(vec3{4.75f, 2.25f, 0.5f}, vec3{5.25f, 2.25f, 0.5f}, vec3{5.25f, 2.75f, 0.5f}, vec3{4.75f, 2.75f, 0.5f});
+	lq.add_quad(vec3{4.75f, 2.25f, 0.5f}, vec3{4.75f, 2.75f, 0.5f}, vec3{5.25f, 2.75f, 0.5f}, vec3{5.25f, 2.25f, 0.5f});
 	s.add_entity(std::move(lq), black, s.add_emitter(RB_EMITTER_SURFACE, 50.f, 50.f, 50.f), identity_xf());
 	// clutter
 	for (uint32_t i = 0; i < count; i++) {

@@ -575,8 +575,8 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 	if (e == cudaSuccess) e = launch_next_wave(w, f, grid, stream);
 	if (train)
 		for (uint32_t k = 0; k < cfg.guide->cfg.steps_per_wave && e == cudaSuccess; k++)
-			e = guide::launch_train_step(*cfg.guide, cfg.guide->samples, &cfg.guide->dstate->sample_count,
-				cfg.guide->sample_cap, cfg.guide->cfg.batch_size, cfg.guide->cfg.min_rows, false, stream);
+			e = guide::launch_train_step(*cfg.guide, cfg.guide->samples, &cfg.guide->dstate->ring_filled,
+				cfg.guide->sample_cap, cfg.guide->cfg.batch_size, cfg.guide->cfg.min_rows, false, true, stream);
 	return e;
 }
 
@@ -584,7 +584,7 @@ uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
 	uint32_t n = 3u + (12u + (sample ? 1u : 0u)) * max_depth;
-	if (train) n += 2u + 2u * cfg.guide->cfg.steps_per_wave;
+	if (train) n += 3u + 2u * cfg.guide->cfg.steps_per_wave;
 	return n;
 }
 
