@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 1
+#define RBGPU_ABI_VERSION 2
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -95,6 +95,24 @@ enum {
 	RB_EMITTER_ENVIRONMENT = 1   /* rainbow-cpu/emitters/environment_light.cpp with a constant map of 1 */
 };
 
+/* Homogeneous participating medium: rainbow-cpu/media/homogeneous_medium.cpp:7-58
+ * (homogeneous_medium(sigma_a, sigma_s, g)) with the Henyey-Greenstein phase
+ * function of asymmetry g (shared/phases/henyey_greenstein.cpp). */
+typedef struct rb_medium_desc {
+	float sigma_a[3];
+	float sigma_s[3];
+	float g;
+	uint32_t reserved;
+} rb_medium_desc;
+
+/* The media component of an entity: media(outside, inside) (media/medium.hpp:82-101),
+ * indices into rb_scene_desc.mediums, -1 for vacuum. A ray leaving a surface
+ * of the entity along +normal continues in `outside`, otherwise in `inside`. */
+typedef struct rb_media_desc {
+	int32_t inside;
+	int32_t outside;
+} rb_media_desc;
+
 typedef struct rb_emitter_desc {
 	uint32_t kind;
 	float radiance[3];          /* surface radiance, or environment intensity */
@@ -108,7 +126,7 @@ typedef struct rb_entity_desc {
 	int32_t mesh;
 	int32_t material;
 	int32_t emitter;
-	int32_t medium;             /* reserved, must be -1 */
+	int32_t medium;             /* index of the entity's media component (rb_media_desc), -1: none */
 	float local_to_world[16];
 	float world_to_local[16];
 } rb_entity_desc;
@@ -142,6 +160,10 @@ typedef struct rb_scene_desc {
 	uint32_t num_emitters;
 	const rb_emitter_desc* emitters;
 	rb_bvh_desc bvh;            /* num_nodes == 0: rb_scene_upload builds it (rb_bvh_build) */
+	const rb_medium_desc* mediums;
+	uint32_t num_mediums;
+	uint32_t num_media;
+	const rb_media_desc* media;
 } rb_scene_desc;
 
 /* Pinhole / thin-lens perspective camera: rainbow-cpu/cameras/perspective_camera.cpp:78-99.
@@ -208,7 +230,11 @@ rb_status rb_trace_shadow_device(rb_context* ctx, const rb_ray* d_rays, uint32_t
 enum {
 	RB_RENDER_RESET = 1u << 0,     /* clear the film accumulators before adding these samples */
 	RB_RENDER_GUIDE = 1u << 1,     /* learned guiding: sample path continuations from the guide (below) */
-	RB_RENDER_TRAIN = 1u << 2      /* learned guiding: collect training samples and train after every wave */
+	RB_RENDER_TRAIN = 1u << 2,     /* learned guiding: collect training samples and train after every wave */
+	RB_RENDER_VOLUME = 1u << 3     /* volume_path_integrator::trace (volume_path_integrator.cpp:13-79) instead
+	                                  of path_integrator::trace: free-flight sampling in the media of the
+	                                  path, Henyey-Greenstein scattering, transmittance on every light
+	                                  connection; cannot be combined with learned guiding */
 };
 
 /* One render call: path_integrator::trace (rainbow-cpu/integrators/path_integrator.cpp:15-47)
@@ -379,7 +405,8 @@ void rb_bvh_free(rb_bvh* bvh);
 enum {
 	RB_SCENE_BOX = 0,          /* closed box room: 32 triangles, one 0.25 x 0.25 quad light */
 	RB_SCENE_SPHERES = 1,      /* displaced icospheres over a ground plane, 4 quad lights + environment */
-	RB_SCENE_SLIT_ROOM = 2     /* glossy room, light behind a wall with a slit (hard indirect) */
+	RB_SCENE_SLIT_ROOM = 2,    /* glossy room, light behind a wall with a slit (hard indirect) */
+	RB_SCENE_FOG = 3           /* displaced icospheres in a homogeneous medium box, 16 quad lights */
 };
 typedef struct rb_scene_gen_params {
 	uint32_t kind;

@@ -18,6 +18,8 @@
 #include "../../include/rbgpu.h"
 
 #include "rainbow-cpu/integrators/path_integrator.hpp"
+#include "rainbow-cpu/integrators/volume_path_integrator.hpp"
+#include "rainbow-cpu/media/homogeneous_medium.hpp"
 #include "rainbow-cpu/cameras/perspective_camera.hpp"
 #include "rainbow-cpu/filters/box_filter.hpp"
 #include "rainbow-cpu/samplers/random_sampler.hpp"
@@ -85,6 +87,7 @@ struct orc_scene_impl {
 	int width = 0, height = 0;
 	rb_camera_desc desc{};
 	std::unordered_map<const entity*, int32_t> ordinal;
+	bool volume = false;  // trace with volume_path_integrator instead of path_integrator
 
 	std::shared_ptr<perspective_camera> make_camera(const std::shared_ptr<film>& f) const {
 		const vector3 eye(desc.eye[0], desc.eye[1], desc.eye[2]);
@@ -148,13 +151,14 @@ uint64_t stream_seed(uint32_t pixel, uint32_t sample, uint32_t seed) {
 }
 
 struct sample_driver {
-	std::shared_ptr<path_integrator> integrator;
+	std::shared_ptr<sampler_integrator> integrator;
 	std::shared_ptr<sampler1d> proto1;
 	std::shared_ptr<sampler2d> proto2;
-	sample_driver(uint32_t max_depth, float rr) {
+	sample_driver(uint32_t max_depth, float rr, bool volume) {
 		proto1 = std::make_shared<random_sampler1d>(1);
 		proto2 = std::make_shared<random_sampler2d>(1);
-		integrator = std::make_shared<path_integrator>(proto2, proto1, max_depth, rr);
+		if (volume) integrator = std::make_shared<volume_path_integrator>(proto2, proto1, max_depth, rr);
+		else integrator = std::make_shared<path_integrator>(proto2, proto1, max_depth, rr);
 	}
 	// One sample of the body of sampler_integrator::render (sampler_integrator.cpp:102-130),
 	// with samplers seeded per (pixel, sample).
@@ -193,12 +197,25 @@ int orc_scene_build(const rb_scene_desc* desc, const rb_camera_desc* cam, orc_sc
 		if (e.kind == RB_EMITTER_SURFACE) emitter_list.push_back(std::make_shared<surface_light>(L));
 		else emitter_list.push_back(std::make_shared<environment_light>(L, e.radius));
 	}
+	std::vector<std::shared_ptr<rainbow::cpus::media::medium>> mediums;
+	for (uint32_t i = 0; i < desc->num_mediums; i++) {
+		const rb_medium_desc& m = desc->mediums[i];
+		mediums.push_back(std::make_shared<rainbow::cpus::media::homogeneous_medium>(spectrum(m.sigma_a[0], m.sigma_a[1], m.sigma_a[2]),
+			spectrum(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2]), m.g));
+	}
+	std::vector<std::shared_ptr<rainbow::cpus::media::media>> media_list;
+	for (uint32_t i = 0; i < desc->num_media; i++) {
+		const rb_media_desc& m = desc->media[i];
+		media_list.push_back(std::make_shared<rainbow::cpus::media::media>(m.outside >= 0 ? mediums[m.outside] : nullptr,
+			m.inside >= 0 ? mediums[m.inside] : nullptr));
+	}
 	s->world = std::make_shared<scene>();
 	for (uint32_t i = 0; i < desc->num_entities; i++) {
 		const rb_entity_desc& e = desc->entities[i];
 		const transform xf(to_matrix(e.local_to_world), to_matrix(e.world_to_local));
 		auto ent = std::make_shared<entity>(e.material >= 0 ? materials[e.material] : nullptr,
-			e.emitter >= 0 ? emitter_list[e.emitter] : nullptr, e.mesh >= 0 ? meshes[e.mesh] : nullptr, nullptr, xf);
+			e.emitter >= 0 ? emitter_list[e.emitter] : nullptr, e.mesh >= 0 ? meshes[e.mesh] : nullptr,
+			e.medium >= 0 ? media_list[e.medium] : nullptr, xf);
 		s->ordinal[ent.get()] = static_cast<int32_t>(i);
 		s->entities.push_back(ent);
 		s->world->add_entity(ent);
@@ -215,6 +232,10 @@ int orc_scene_build(const rb_scene_desc* desc, const rb_camera_desc* cam, orc_sc
 }
 
 void orc_scene_free(orc_scene* s) { delete s; }
+
+// Selects the integrator of the tracing entry points: path_integrator (0) or
+// volume_path_integrator (1).
+void orc_set_volume(orc_scene* s, int volume) { s->volume = volume != 0; }
 
 
 
@@ -286,8 +307,6 @@ void walk(const accelerator<T>& acc, const ray& r, bool shadow, const orc_scene*
 		else { stack.push_back(n->right); stack.push_back(n->left); }
 	}
 }
-
-sample_driver* driver_for(uint32_t max_depth, float rr) { return new sample_driver(max_depth, rr); }
 
 } // namespace
 
@@ -405,7 +424,7 @@ int orc_camera_rays(orc_scene* s, const uint32_t* pixels, const uint32_t* sample
 // Radiance of individual (pixel, sample) pairs through path_integrator::trace.
 int orc_trace_samples(orc_scene* s, const uint32_t* pixels, const uint32_t* samples, uint32_t n, uint32_t max_depth, float rr,
 	uint32_t seed, float* radiance) {
-	sample_driver d(max_depth, rr);
+	sample_driver d(max_depth, rr, s->volume);
 	for (uint32_t i = 0; i < n; i++) {
 		const int x = static_cast<int>(pixels[i] % static_cast<uint32_t>(s->width));
 		const int y = static_cast<int>(pixels[i] / static_cast<uint32_t>(s->width));
@@ -425,7 +444,7 @@ int orc_render(orc_scene* s, uint32_t spp, uint32_t first_sample, uint32_t max_d
 	std::atomic<int> next_row(row_begin);
 	const auto t0 = std::chrono::steady_clock::now();
 	auto work = [&]() {
-		sample_driver d(max_depth, rr);
+		sample_driver d(max_depth, rr, s->volume);
 		for (int y = next_row++; y < row_end; y = next_row++) {
 			for (int x = 0; x < s->width; x++) {
 				const size_t p = static_cast<size_t>(y) * s->width + x;

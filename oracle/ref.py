@@ -43,6 +43,7 @@ def lib():
             "orc_render_shipped": (i32, [vp, u32, u32, f32, vp, C.POINTER(C.c_double)]),
             "orc_pcg32": (i32, [C.c_uint64, u32, vp, vp]),
             "orc_bsdf": (i32, [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
+            "orc_set_volume": (None, [vp, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -114,6 +115,10 @@ class RefScene:
         _ok(lib().orc_camera_rays(self.h, px.ctypes.data, sm.ctypes.data, px.shape[0], seed, rays.ctypes.data),
             "orc_camera_rays")
         return rays
+
+    def set_volume(self, volume: bool):
+        """Trace with volume_path_integrator (True) or path_integrator (False)."""
+        lib().orc_set_volume(self.h, 1 if volume else 0)
 
     def trace_samples(self, pixels, samples, max_depth=5, rr=1.0, seed=0):
         px = np.ascontiguousarray(pixels, dtype=np.uint32)

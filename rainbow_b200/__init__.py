@@ -23,7 +23,8 @@ import numpy as np
 from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_RENDER_GUIDE,
-    RB_RENDER_RESET, RB_RENDER_TRAIN, RB_SCENE_BOX, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES, BvhDesc, CameraDesc,
+    RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
+    BvhDesc, CameraDesc, MediaDesc, MediumDesc,
     GuideConfig, GuideStats, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
 )
 
@@ -157,12 +158,14 @@ class Context:
 
     def render(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5, threshold: float = 1.0,
                seed: int = 0, reset: bool = True, paths_per_wave: int = 0, want_image: bool = True,
-               guide: bool = False, train: bool = False):
-        """guide / train: learned path guiding (RB_RENDER_GUIDE / RB_RENDER_TRAIN)."""
+               guide: bool = False, train: bool = False, volume: bool = False):
+        """guide / train: learned path guiding (RB_RENDER_GUIDE / RB_RENDER_TRAIN); volume:
+        volume_path_integrator instead of path_integrator (RB_RENDER_VOLUME)."""
         p = RenderParams()
         p.camera = camera
         p.spp, p.first_sample, p.max_depth, p.rr_threshold = spp, first_sample, max_depth, threshold
         flags = (RB_RENDER_RESET if reset else 0) | (RB_RENDER_GUIDE if guide else 0) | (RB_RENDER_TRAIN if train else 0)
+        flags |= RB_RENDER_VOLUME if volume else 0
         p.seed, p.flags, p.paths_per_wave = seed, flags, paths_per_wave
         img = np.zeros((camera.height, camera.width, 3), dtype=np.float32) if want_image else None
         self._film_shape = (camera.width, camera.height)

@@ -23,10 +23,11 @@ STATUS_NAMES = {
 
 RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS = 0, 1, 2
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
-RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM = 0, 1, 2
+RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM, RB_SCENE_FOG = 0, 1, 2, 3
 RB_RENDER_RESET = 1
 RB_RENDER_GUIDE = 2
 RB_RENDER_TRAIN = 4
+RB_RENDER_VOLUME = 8
 RB_GUIDE_SEQUENTIAL = 1
 RB_GUIDE_NUM_PARAMS = 30000
 RB_GUIDE_INPUTS = 9
@@ -50,6 +51,14 @@ class MaterialDesc(C.Structure):
                 ("roughness_u", C.c_float), ("roughness_v", C.c_float)]
 
 
+class MediumDesc(C.Structure):
+    _fields_ = [("sigma_a", F3), ("sigma_s", F3), ("g", C.c_float), ("reserved", C.c_uint32)]
+
+
+class MediaDesc(C.Structure):
+    _fields_ = [("inside", C.c_int32), ("outside", C.c_int32)]
+
+
 class EmitterDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("radiance", F3), ("radius", C.c_float)]
 
@@ -68,7 +77,8 @@ class SceneDesc(C.Structure):
     _fields_ = [("meshes", C.POINTER(MeshDesc)), ("num_meshes", C.c_uint32), ("num_entities", C.c_uint32),
                 ("entities", C.POINTER(EntityDesc)), ("materials", C.POINTER(MaterialDesc)),
                 ("num_materials", C.c_uint32), ("num_emitters", C.c_uint32), ("emitters", C.POINTER(EmitterDesc)),
-                ("bvh", BvhDesc)]
+                ("bvh", BvhDesc), ("mediums", C.POINTER(MediumDesc)), ("num_mediums", C.c_uint32),
+                ("num_media", C.c_uint32), ("media", C.POINTER(MediaDesc))]
 
 
 class CameraDesc(C.Structure):

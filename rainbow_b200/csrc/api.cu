@@ -68,10 +68,13 @@ struct device_scene {
 	pt::material_rec* materials = nullptr;
 	pt::emitter_rec* emitters = nullptr;
 	int32_t* environments = nullptr;
+	pt::medium_rec* mediums = nullptr;
+	pt::media_rec* media = nullptr;
 	void release() {
 		dev_free(wnodes); dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
 		dev_free(entities); dev_free(meshes); dev_free(positions); dev_free(normals); dev_free(tangents); dev_free(uvs);
 		dev_free(indices); dev_free(materials); dev_free(emitters); dev_free(environments);
+		dev_free(mediums); dev_free(media);
 	}
 };
 
@@ -79,9 +82,11 @@ struct graph_key {
 	uint32_t capacity = 0, max_depth = 0, stack = 0;
 	bool count = false;
 	uint32_t guide_mode = 0, guide_steps = 0, guide_batch = 0;
+	bool volume = false;
 	bool operator==(const graph_key& o) const {
 		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
-			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch;
+			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch &&
+			volume == o.volume;
 	}
 };
 
@@ -128,6 +133,9 @@ struct rb_context {
 	rb_render_stats stats{};
 	guide::guide_state guide;        // learned path guide (allocated on first use)
 	uint32_t guide_mode = 0;         // gpu::GUIDE_* of the current render call
+	bool volume = false;             // the current render call uses the volume path integrator
+	int32_t* vol_medium = nullptr;   // per-path medium buffer (wave.medium points here in volume renders)
+	uint32_t vol_alloc = 0;          // paths the volume buffers hold
 
 	gpu::launch_cfg cfg() const {
 		gpu::launch_cfg c;
@@ -141,6 +149,7 @@ struct rb_context {
 			c.guide = &guide;
 			c.guide_mode = guide_mode;
 		}
+		c.volume = volume;
 		return c;
 	}
 	gpu::launch_cfg profiled_cfg() {
@@ -160,6 +169,9 @@ struct rb_context {
 		dev_free(wave.sec_o); dev_free(wave.sec_d); dev_free(wave.sec_hit); dev_free(wave.queue[0]); dev_free(wave.queue[1]);
 		dev_free(wave.sec_queue);
 		dev_free(wave.class_queue);
+		dev_free(vol_medium); dev_free(wave.vrec); dev_free(wave.beam); dev_free(wave.beam_queue);
+		wave.medium = nullptr;
+		vol_alloc = 0;
 		wave_capacity = 0;
 		wave_alloc = 0;
 	}
@@ -233,6 +245,7 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 	key.stack = static_cast<uint32_t>(cfg.stack_depth);
 	key.count = cfg.count;
 	key.guide_mode = cfg.guide_mode;
+	key.volume = cfg.volume;
 	if (cfg.guide) {
 		key.guide_steps = cfg.guide->cfg.steps_per_wave;
 		key.guide_batch = cfg.guide->cfg.batch_size;
@@ -273,6 +286,30 @@ rb_status prepare_guide(rb_context* c, const rb_render_params* prm) {
 	if (g.query_in != before) c->release_graph();
 	c->guide_mode = ((prm->flags & RB_RENDER_GUIDE) ? gpu::GUIDE_SAMPLE : 0u) | ((prm->flags & RB_RENDER_TRAIN) ? gpu::GUIDE_TRAIN : 0u);
 	c->wave.guide = guide::wave_guide{g.dstate, g.query_in, g.query_out, g.queue, g.vertices, g.vertex_count, g.depth};
+	return RB_OK;
+}
+
+// Volume path tracing: per-path medium, light-connection records and
+// transmittance buffers, allocated with the wave on first use.
+rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
+	c->volume = (prm->flags & RB_RENDER_VOLUME) != 0;
+	if (!c->volume) {
+		c->wave.medium = nullptr;  // plain kernels see no media
+		return RB_OK;
+	}
+	if (prm->flags & (RB_RENDER_GUIDE | RB_RENDER_TRAIN)) return RB_ERR_INVALID_ARGUMENT;
+	if (c->vol_alloc < c->wave_alloc) {
+		c->release_graph();
+		dev_free(c->vol_medium); dev_free(c->wave.vrec); dev_free(c->wave.beam); dev_free(c->wave.beam_queue);
+		c->vol_alloc = 0;
+		const size_t n = c->wave_alloc;
+		RB_CUDA(dev_alloc(&c->vol_medium, n));
+		RB_CUDA(dev_alloc(&c->wave.vrec, n));
+		RB_CUDA(dev_alloc(&c->wave.beam, 2 * n));
+		RB_CUDA(dev_alloc(&c->wave.beam_queue, 2 * n));
+		c->vol_alloc = c->wave_alloc;
+	}
+	c->wave.medium = c->vol_medium;
 	return RB_OK;
 }
 
@@ -423,6 +460,8 @@ rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
 	RB_CUDA(dev_upload(&d.materials, p.materials, c->stream));
 	RB_CUDA(dev_upload(&d.emitters, p.emitters, c->stream));
 	RB_CUDA(dev_upload(&d.environments, p.environments, c->stream));
+	RB_CUDA(dev_upload(&d.mediums, p.mediums, c->stream));
+	RB_CUDA(dev_upload(&d.media, p.media, c->stream));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
 	pt::scene_view v{};
 	v.wnodes = p.wide_ok ? d.wnodes : nullptr;
@@ -437,6 +476,9 @@ rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
 	v.num_emitters = static_cast<uint32_t>(p.emitters.size());
 	v.num_environments = static_cast<uint32_t>(p.environments.size());
 	v.num_entities = static_cast<uint32_t>(p.entities.size());
+	v.mediums = d.mediums;
+	v.media = d.media;
+	v.num_media = static_cast<uint32_t>(p.media.size());
 	c->view = v;
 	c->bvh_depth = p.bvh_depth;
 	c->num_entities = v.num_entities;
@@ -530,6 +572,8 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	st = ensure_wave(c, static_cast<uint32_t>(capacity));
 	if (st != RB_OK) return st;
 	st = prepare_guide(c, prm);
+	if (st != RB_OK) return st;
+	st = prepare_volume(c, prm);
 	if (st != RB_OK) return st;
 
 	gpu::wave_params& hp = *c->params_host;

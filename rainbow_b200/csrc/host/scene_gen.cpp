@@ -141,6 +141,8 @@ struct rb_scene {
 	std::vector<rb_entity_desc> entities;
 	std::vector<rb_material_desc> materials;
 	std::vector<rb_emitter_desc> emitters;
+	std::vector<rb_medium_desc> mediums;
+	std::vector<rb_media_desc> media;
 	rb_camera_desc camera{};
 
 	int32_t add_material(const rb_material_desc& m) {
@@ -367,6 +369,63 @@ void build_sphere_scene(rb_scene& s, uint32_t seed, uint32_t count, int level, i
 	c.height = height;
 }
 
+// Sphere field inside a homogeneous medium (sigma_a 0.02, sigma_s 0.1,
+// Henyey-Greenstein g = 0.6): the medium is the inside of an invisible box
+// entity (no material) around the spheres, the ground and 16 quad lights of
+// seeded radiance U[5, 40]; the camera looks in from outside the box, where
+// rays travel in vacuum.
+void build_fog_scene(rb_scene& s, uint32_t seed, uint32_t count, int level, int width, int height) {
+	gen_rng rng(0xf09f09ull + seed);
+	const gradient_noise noise(seed * 6151ull + 29ull);
+	std::vector<vec3> unit;
+	std::vector<uint32_t> faces;
+	icosphere(level, unit, faces);
+	const int32_t black = s.add_material(matte(0.f, 0.f, 0.f));
+	for (uint32_t i = 0; i < count; i++) {
+		const float r = rng.range(0.05f, 0.5f);
+		const vec3 c{rng.range(0.f, 10.f), rng.range(0.f, 10.f), rng.range(0.f, 10.f)};
+		const vec3 off{rng.range(0.f, 100.f), rng.range(0.f, 100.f), rng.range(0.f, 100.f)};
+		const int32_t mat = random_material(s, rng);
+		s.add_entity(displaced_sphere(unit, faces, noise, off, 0.1f, 2.5f), mat, -1, translate_scale(c, r));
+	}
+	mesh_data ground;
+	ground.add_quad(vec3{-20, -0.5f, -20}, vec3{-20, -0.5f, 30}, vec3{30, -0.5f, 30}, vec3{30, -0.5f, -20});
+	s.add_entity(std::move(ground), s.add_material(matte(0.5f, 0.5f, 0.5f)), -1, identity_xf());
+	// 16 quad lights of 0.6 x 0.6 on a 4 x 4 grid at y = 11.5, facing down
+	for (int i = 0; i < 16; i++) {
+		const float cx = 1.25f + 2.5f * static_cast<float>(i & 3), cz = 1.25f + 2.5f * static_cast<float>(i >> 2);
+		mesh_data q;
+		q.add_quad(vec3{cx - 0.3f, 11.5f, cz - 0.3f}, vec3{cx + 0.3f, 11.5f, cz - 0.3f}, vec3{cx + 0.3f, 11.5f, cz + 0.3f},
+			vec3{cx - 0.3f, 11.5f, cz + 0.3f});
+		const float L = rng.range(5.f, 40.f);
+		s.add_entity(std::move(q), black, s.add_emitter(RB_EMITTER_SURFACE, L, L, L), identity_xf());
+	}
+	// the medium box [-1, 11] x [-1, 12.5] x [-1, 11], faces wound outwards
+	rb_medium_desc fog{};
+	for (int c = 0; c < 3; c++) { fog.sigma_a[c] = 0.02f; fog.sigma_s[c] = 0.1f; }
+	fog.g = 0.6f;
+	s.mediums.push_back(fog);
+	s.media.push_back(rb_media_desc{0, -1});
+	const float x0 = -1.f, x1 = 11.f, y0 = -1.f, y1 = 12.5f, z0 = -1.f, z1 = 11.f;
+	mesh_data box;
+	box.add_quad(vec3{x0, y0, z0}, vec3{x1, y0, z0}, vec3{x1, y0, z1}, vec3{x0, y0, z1});  // -y
+	box.add_quad(vec3{x0, y1, z0}, vec3{x0, y1, z1}, vec3{x1, y1, z1}, vec3{x1, y1, z0});  // +y
+	box.add_quad(vec3{x0, y0, z0}, vec3{x0, y0, z1}, vec3{x0, y1, z1}, vec3{x0, y1, z0});  // -x
+	box.add_quad(vec3{x1, y0, z0}, vec3{x1, y1, z0}, vec3{x1, y1, z1}, vec3{x1, y0, z1});  // +x
+	box.add_quad(vec3{x0, y0, z0}, vec3{x0, y1, z0}, vec3{x1, y1, z0}, vec3{x1, y0, z0});  // -z
+	box.add_quad(vec3{x0, y0, z1}, vec3{x1, y0, z1}, vec3{x1, y1, z1}, vec3{x0, y1, z1});  // +z
+	s.add_entity(std::move(box), -1, -1, identity_xf());
+	s.entities.back().medium = 0;
+
+	rb_camera_desc& c = s.camera;
+	c.eye[0] = 5.f; c.eye[1] = 8.f; c.eye[2] = 26.f;
+	c.target[0] = 5.f; c.target[1] = 3.5f; c.target[2] = 5.f;
+	c.up[0] = 0.f; c.up[1] = 1.f; c.up[2] = 0.f;
+	c.fov_degrees = 45.f;
+	c.width = width;
+	c.height = height;
+}
+
 void build_slit_room(rb_scene& s, uint32_t seed, uint32_t count, int level, int width, int height) {
 	gen_rng rng(0xabcdefull + seed);
 	const gradient_noise noise(seed * 104729ull + 7ull);
@@ -432,6 +491,9 @@ extern "C" rb_status rb_scene_generate(const rb_scene_gen_params* params, rb_sce
 		case RB_SCENE_SLIT_ROOM:
 			build_slit_room(*s, params->seed, params->num_spheres, static_cast<int>(params->subdivision), params->width, params->height);
 			break;
+		case RB_SCENE_FOG:
+			build_fog_scene(*s, params->seed, params->num_spheres, static_cast<int>(params->subdivision), params->width, params->height);
+			break;
 		default: delete s; return RB_ERR_INVALID_ARGUMENT;
 		}
 		s->finalize();
@@ -455,6 +517,10 @@ extern "C" rb_status rb_scene_get(const rb_scene* s, rb_scene_desc* desc, rb_cam
 		desc->num_materials = static_cast<uint32_t>(s->materials.size());
 		desc->emitters = s->emitters.data();
 		desc->num_emitters = static_cast<uint32_t>(s->emitters.size());
+		desc->mediums = s->mediums.data();
+		desc->num_mediums = static_cast<uint32_t>(s->mediums.size());
+		desc->media = s->media.data();
+		desc->num_media = static_cast<uint32_t>(s->media.size());
 	}
 	if (camera != nullptr) *camera = s->camera;
 	return RB_OK;

@@ -121,10 +121,27 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			}
 			out.materials.push_back(r);
 		}
+		// ---- homogeneous media and media components
+		if ((desc->num_mediums > 0 && desc->mediums == nullptr) || (desc->num_media > 0 && desc->media == nullptr))
+			return RB_ERR_INVALID_ARGUMENT;
+		for (uint32_t i = 0; i < desc->num_mediums; i++) {
+			const rb_medium_desc& md = desc->mediums[i];
+			pt::medium_rec r{};
+			r.sigma_s = vec3{md.sigma_s[0], md.sigma_s[1], md.sigma_s[2]};
+			r.sigma_t = vec3{md.sigma_a[0] + md.sigma_s[0], md.sigma_a[1] + md.sigma_s[1], md.sigma_a[2] + md.sigma_s[2]};
+			r.g = md.g;
+			out.mediums.push_back(r);
+		}
+		for (uint32_t i = 0; i < desc->num_media; i++) {
+			const rb_media_desc& md = desc->media[i];
+			const int32_t n = static_cast<int32_t>(desc->num_mediums);
+			if (md.inside < -1 || md.inside >= n || md.outside < -1 || md.outside >= n) return RB_ERR_INVALID_ARGUMENT;
+			out.media.push_back(pt::media_rec{md.inside, md.outside});
+		}
 		// ---- entities and the emitter list (scene::add_entity order, scene.cpp:16-28)
 		for (uint32_t e = 0; e < desc->num_entities; e++) {
 			const rb_entity_desc& ed = desc->entities[e];
-			if (ed.medium != -1) return RB_ERR_UNSUPPORTED;
+			if (ed.medium < -1 || ed.medium >= static_cast<int32_t>(desc->num_media)) return RB_ERR_INVALID_ARGUMENT;
 			if (ed.mesh >= static_cast<int32_t>(desc->num_meshes) || ed.material >= static_cast<int32_t>(desc->num_materials) ||
 				ed.emitter >= static_cast<int32_t>(desc->num_emitters))
 				return RB_ERR_INVALID_ARGUMENT;
@@ -134,8 +151,9 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			r.mesh = ed.mesh;
 			r.material = ed.material;
 			r.emitter = -1;
+			r.media = ed.medium;
 			r.flags = (ed.mesh >= 0 ? pt::ENT_HAS_SHAPE : 0u) | (ed.material >= 0 ? pt::ENT_HAS_MATERIAL : 0u) |
-				(ed.emitter >= 0 ? pt::ENT_HAS_EMITTER : 0u);
+				(ed.emitter >= 0 ? pt::ENT_HAS_EMITTER : 0u) | (ed.medium >= 0 ? pt::ENT_HAS_MEDIA : 0u);
 			if (ed.mesh >= 0 && ed.material >= 0) r.flags |= pt::ENT_VISIBLE;
 			if (ed.mesh >= 0) {
 				// mesh::area(transform): sum of 0.5 |(p2 - p0) x (p2 - p1)| over world-space triangles
@@ -301,6 +319,9 @@ pt::scene_view host_view(const packed_scene& p) {
 	v.num_emitters = static_cast<uint32_t>(p.emitters.size());
 	v.num_environments = static_cast<uint32_t>(p.environments.size());
 	v.num_entities = static_cast<uint32_t>(p.entities.size());
+	v.mediums = p.mediums.data();
+	v.media = p.media.data();
+	v.num_media = static_cast<uint32_t>(p.media.size());
 	return v;
 }
 

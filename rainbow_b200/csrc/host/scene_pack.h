@@ -25,6 +25,8 @@ struct packed_scene {
 	std::vector<uint32_t> indices;
 	std::vector<pt::material_rec> materials;
 	std::vector<pt::emitter_rec> emitters;
+	std::vector<pt::medium_rec> mediums;
+	std::vector<pt::media_rec> media;
 	std::vector<int32_t> environments;
 	pt::env_distribution env{};
 	uint32_t bvh_depth = 0;

@@ -8,6 +8,7 @@
 // over counts that live in device memory, so the launches can be captured in a
 // CUDA graph once and replayed for every wave.
 #include "kernels.cuh"
+#include "pt/pt_volume.h"
 
 namespace rb {
 namespace gpu {
@@ -269,6 +270,7 @@ __device__ __forceinline__ path_state load_path(const wave_buffers& w, const wav
 	st.flags = __float_as_uint(L.w);
 	st.bounces = w.bounces[i];
 	st.rng = load_rng(w, p, i);
+	st.medium = w.medium != nullptr ? w.medium[i] : -1;
 	return st;
 }
 
@@ -279,6 +281,7 @@ __device__ __forceinline__ void store_path(const wave_buffers& w, uint32_t i, co
 	w.radiance[i] = make_float4(st.L.x, st.L.y, st.L.z, __uint_as_float(st.flags));
 	w.bounces[i] = st.bounces;
 	w.rng[i] = st.rng.state;
+	if (w.medium != nullptr) w.medium[i] = st.medium;
 }
 
 __device__ __forceinline__ void finish(const wave_buffers& w, uint32_t i, vec3 L) {
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 	}
 }
 
-template <bool COUNT>
+template <bool COUNT, bool VOL>
 __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
 	smem_stack st = make_stack(smem, stack_cap);
@@ -361,7 +364,7 @@ __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, ui
 				h.slot = -1;
 			}
 			w.hit[i] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
-			key = shade_class(s, h.slot);
+			key = (VOL && w.medium[i] >= 0) ? static_cast<uint32_t>(CLASS_MEDIUM) : shade_class(s, h.slot);
 		}
 		warp_push_keyed(key, i, w.class_queue, w.capacity, w.counters + CNT_CLASS);
 	}
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, ui
 	}
 }
 
-template <uint32_t CLASS>
+template <uint32_t CLASS, bool VOL>
 __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 	const wave_params& p = *w.params;
 	const uint32_t n = w.counters[CNT_CLASS + CLASS];
@@ -389,7 +392,13 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 				st.flags |= 0x80000000u;  // ended in shade_a; shade_b skips it
 			} else {
 				shade_record& r = w.rec[i];
-				const bool alive = shade_a<class_material(CLASS)>(s, st, to_hit(w.hit[i]), r);
+				vol_rec* vr = nullptr;
+				if (VOL) {
+					vr = w.vrec + i;
+					vr->flags = 0u;
+					vr->medium = st.medium;
+				}
+				const bool alive = shade_a<class_material(CLASS)>(s, st, to_hit(w.hit[i]), r, vr);
 				if (!alive) {
 					finish(w, i, st.L);
 					st.flags |= 0x80000000u;
@@ -483,6 +492,352 @@ __global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, u
 	}
 }
 
+// ------------------------------------------------------------------ volume path tracing
+// volume_path_integrator::trace (volume_path_integrator.cpp:13-79) per bounce:
+// extend -> shade_a (surface classes, and CLASS_MEDIUM: free-flight sampling,
+// then a medium vertex or the surface reached) -> shadow / MIS rays ->
+// k_vol_direct (what each light connection found) -> k_beam (transmittance of
+// each connection through invisible medium boundaries) -> k_vol_continue
+// (accumulate, continue by BSDF or phase function, switch media, roulette).
+// The random numbers are drawn in the reference's order; the transmittance
+// walks draw none.
+
+// Emitter sampling and phase sampling at a medium vertex, the first half of
+// uniform_sample_one_emitter for a medium_interaction (integrator.cpp:203-288).
+__device__ void medium_vertex_a(const scene_view& s, path_state& p, shade_record& rec, vol_rec& vr, const medium_rec& m,
+	float t) {
+	const vec3 point = p.o + p.d * t;
+	const vec3 wo = -p.d;
+	const vec3 zero{0.f, 0.f, 0.f};
+	vr.flags = VOL_MEDIUM_VERTEX;
+	vr.g = m.g;
+	rec.pass_through = 0u;
+	rec.did_nee = 1u;
+	rec.guidable = 0u;
+	rec.nee_entity = -1;
+	rec.mis_valid = 0u;
+	rec.si.p = point;
+	rec.si.n = zero;
+	rec.si.wo = wo;
+	rec.si.entity = -1;
+	const float n = static_cast<float>(s.num_emitters);
+	uint32_t which = static_cast<uint32_t>(floorf(pcg_real(p.rng) * n));
+	if (which > s.num_emitters - 1) which = s.num_emitters - 1;
+	const emitter_rec& em = s.emitters[which];
+	light_sample ls = sample_emitter(s, em, point, zero, pcg_2d(p.rng));
+	ls.pdf = ls.pdf * (1.f / n);
+	if (!is_black(ls.L) && ls.pdf > 0.f) {
+		const float ph = hg_phase(dot(wo, ls.wi), m.g);
+		const spectrum fv = splat3(ph);
+		if (!is_black(fv) && ph > 0.f) {
+			rec.shadow_ray = spawn_ray_to(point, zero, ls.p);
+			rec.nee_entity = em.entity;
+			vr.nee_f = fv;
+			vr.nee_Le = ls.L;
+			vr.nee_w = power_heuristic(ls.pdf, ph);
+			vr.nee_pdf = ls.pdf;
+			vr.nee_to = ls.p;
+		}
+	}
+	vec3 wi;
+	const float ph = hg_sample(wo, m.g, pcg_2d(p.rng), wi);
+	const spectrum fv = splat3(ph);
+	if (!is_black(fv) && ph > 0.f) {
+		rec.mis_valid = 1u;
+		rec.mis_specular = 0u;
+		rec.mis_wi = wi;
+		rec.mis_f = fv;
+		rec.mis_pdf = ph;
+		rec.mis_ray = spawn_ray(point, zero, wi);
+	}
+}
+
+// Paths inside a medium: homogeneous_medium::sample over the segment to the
+// closest hit (or to infinity on a miss), then a medium vertex or the surface.
+__global__ void __launch_bounds__(128) k_shade_a_medium(scene_view s, wave_buffers w) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_CLASS + CLASS_MEDIUM];
+	const uint32_t* q = w.class_queue + CLASS_MEDIUM * w.capacity;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool push_shadow = false, push_mis = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = q[k];
+			path_state st = load_path(w, p, i);
+			shade_record& r = w.rec[i];
+			vol_rec& vr = w.vrec[i];
+			vr.flags = 0u;
+			vr.medium = st.medium;
+			const float4 hv = w.hit[i];
+			const medium_rec& m = s.mediums[st.medium];
+			const float u_channel = pcg_real(st.rng);
+			const float u_distance = pcg_real(st.rng);
+			const medium_event ev = sample_medium(m, hv.y, u_channel, u_distance);
+			st.beta = st.beta * ev.weight;
+			bool alive;
+			if (is_black(st.beta)) {
+				alive = false;
+			} else if (ev.scattered) {
+				medium_vertex_a(s, st, r, vr, m, ev.t);
+				alive = true;
+			} else {
+				alive = shade_a<MAT_ANY>(s, st, to_hit(hv), r, &vr);
+			}
+			if (!alive) {
+				finish(w, i, st.L);
+				st.flags |= 0x80000000u;
+			} else {
+				push_shadow = r.nee_entity >= 0;
+				push_mis = r.mis_valid != 0;
+				if (push_shadow) {
+					const ray_t& sr = r.shadow_ray;
+					w.sec_o[2 * i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.len);
+					w.sec_d[2 * i] = make_float4(sr.d.x, sr.d.y, sr.d.z, 0.f);
+				}
+				if (push_mis) {
+					const ray_t& mr = r.mis_ray;
+					w.sec_o[2 * i + 1] = make_float4(mr.o.x, mr.o.y, mr.o.z, mr.len);
+					w.sec_d[2 * i + 1] = make_float4(mr.d.x, mr.d.y, mr.d.z, 0.f);
+				}
+			}
+			store_path(w, i, st);
+		}
+		warp_push(push_shadow, 2 * i, w.sec_queue, w.counters + CNT_SECONDARY);
+		warp_push(push_mis, 2 * i + 1, w.sec_queue, w.counters + CNT_SECONDARY);
+		const uint32_t ns = __popc(__ballot_sync(0xffffffffu, push_shadow));
+		const uint32_t nm = __popc(__ballot_sync(0xffffffffu, push_mis));
+		if ((threadIdx.x & 31u) == 0) {
+			if (ns) add64(w.counters, CNT_SHADOW_RAYS, ns);
+			if (nm) add64(w.counters, CNT_MIS_RAYS, nm);
+		}
+	}
+}
+
+// What the two light connections found (integrator.cpp:136-160,166-197 for a
+// surface, :218-241,249-284 for a medium vertex): the unoccluded emitter sample,
+// the emitter or environment found by the MIS sample (with find_emitter's
+// environment pick, :49-82), and the point each connection ends at. Scenes
+// without media skip the transmittance walks.
+__global__ void __launch_bounds__(128) k_vol_direct(scene_view s, wave_buffers w, uint32_t queue_in) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool push_nee = false, push_mis = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = q[k];
+			const uint32_t flags = __float_as_uint(w.radiance[i].w);
+			const shade_record& rec = w.rec[i];
+			if (!(flags & 0x80000000u) && !rec.pass_through && rec.did_nee) {
+				vol_rec& vr = w.vrec[i];
+				pcg32 rng = load_rng(w, p, i);
+				const surface_t& si = rec.si;
+				const hit_t sh = to_hit(w.sec_hit[2 * i]);
+				if (rec.nee_entity >= 0 && (sh.slot < 0 || hit_entity(s, sh.slot) == static_cast<uint32_t>(rec.nee_entity)))
+					vr.flags |= VOL_NEE;
+				if (rec.mis_valid) {
+					const hit_t mh = to_hit(w.sec_hit[2 * i + 1]);
+					bool found = false;
+					spectrum Le = splat3(0.f);
+					float epdf = 0.f;
+					vec3 to{0.f, 0.f, 0.f};
+					const float pick_pdf = 1.f / static_cast<float>(s.num_emitters);
+					if (mh.slot >= 0) {
+						const entity_rec& ent = s.entities[hit_entity(s, mh.slot)];
+						if (ent.flags & ENT_HAS_EMITTER) {
+							const surface_t es = make_surface(s, mh.slot, mh.b1, mh.b2, rec.mis_ray.o, rec.mis_ray.d);
+							const emitter_rec& em = s.emitters[ent.emitter];
+							Le = surface_emission(ent, em, es.n, -rec.mis_wi);
+							epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
+							to = es.p;
+							found = true;
+						}
+					} else if (s.num_environments > 0) {
+						const float ne = static_cast<float>(s.num_environments);
+						uint32_t which = static_cast<uint32_t>(floorf(pcg_real(rng) * ne));
+						if (which > s.num_environments - 1) which = s.num_environments - 1;
+						const emitter_rec& em = s.emitters[s.environments[which]];
+						Le = em.radiance;
+						epdf = emitter_pdf(s, em, si.p, si.n, rec.mis_wi) * pick_pdf;
+						to = si.p + (2.f * rec.mis_wi) * em.radius;
+						found = true;
+					}
+					if (found && !is_black(Le) && epdf > 0.f) {
+						vr.flags |= VOL_MIS;
+						vr.mis_Le = Le;
+						vr.mis_w = rec.mis_specular ? 1.f : power_heuristic(rec.mis_pdf, epdf);
+						vr.mis_to = to;
+					}
+				}
+				w.rng[i] = rng.state;
+				if (s.num_media == 0) {
+					w.beam[2 * i] = make_float4(1.f, 1.f, 1.f, 0.f);
+					w.beam[2 * i + 1] = make_float4(1.f, 1.f, 1.f, 0.f);
+				} else {
+					push_nee = (vr.flags & VOL_NEE) != 0u;
+					push_mis = (vr.flags & VOL_MIS) != 0u;
+				}
+			}
+		}
+		warp_push(push_nee, 2 * i, w.beam_queue, w.counters + CNT_BEAM);
+		warp_push(push_mis, 2 * i + 1, w.beam_queue, w.counters + CNT_BEAM);
+	}
+}
+
+// scene::evaluate_media_beam (scenes/scene.cpp:114-148): from the vertex to the
+// connection's end point, closest hits over all entities; every segment
+// multiplies the transmittance of the medium it runs in, an invisible entity
+// with media switches the medium, a visible one blocks the connection.
+constexpr uint32_t kMaxBeamSegments = 256;
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_beam(scene_view s, wave_buffers w, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack stk = make_stack(smem, stack_cap);
+	const uint32_t n = w.counters[CNT_BEAM];
+	uint32_t nodes = 0, tris = 0, queries = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		if (k >= n) continue;
+		const uint32_t j = w.beam_queue[k];
+		const uint32_t i = j >> 1;
+		const shade_record& rec = w.rec[i];
+		const vol_rec& vr = w.vrec[i];
+		const vec3 target = (j & 1u) ? vr.mis_to : vr.nee_to;
+		int32_t medium = vr.medium;
+		spectrum L = splat3(1.f);
+		ray_t r = spawn_ray_to(rec.si.p, rec.si.n, target);
+		bool blocked = false, done = false;
+		for (uint32_t seg = 0; seg < kMaxBeamSegments; seg++) {
+			float len = r.len;
+			hit_t h;
+			queries++;
+			if (!trace_one<false, COUNT>(s, r.o, r.d, len, h, stk, nodes, tris)) {
+				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+				blocked = true;
+				break;
+			}
+			if (h.slot < 0) {
+				done = true;
+				break;
+			}
+			L = L * transmittance(s, medium, len);
+			const entity_rec& ent = s.entities[hit_entity(s, h.slot)];
+			if (ent.flags & ENT_VISIBLE) {
+				blocked = true;
+				break;
+			}
+			const surface_t si = make_surface(s, h.slot, h.b1, h.b2, r.o, r.d);
+			r = spawn_ray_to(si.p, si.n, target);
+			if (ent.flags & ENT_HAS_MEDIA) medium = medium_after(s, ent, si.n, r.d);
+		}
+		if (!done && !blocked) {
+			set_error(w.counters, RB_ERR_STACK_OVERFLOW);  // more boundary crossings than the walk allows
+			blocked = true;
+		}
+		if (!blocked) L = L * transmittance(s, medium, r.len);
+		else L = splat3(0.f);
+		w.beam[j] = make_float4(L.x, L.y, L.z, 0.f);
+	}
+	if (COUNT) {
+		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
+		warp_add64(w.counters, CNT_TRI_TESTS, tris);
+	}
+	warp_add64(w.counters, CNT_BEAM_RAYS, queries);
+}
+
+// The rest of the bounce: the light connections with their transmittance
+// (the reference's association of each product), then the continuation by the
+// BSDF (surface) or the phase function (medium vertex), the medium switch when
+// the entity carries media (volume_path_integrator.cpp:50-64), and roulette.
+__device__ bool vol_continue(const scene_view& s, const wave_buffers& w, const wave_params& p, uint32_t i, path_state& st) {
+	const shade_record& rec = w.rec[i];
+	const vol_rec& vr = w.vrec[i];
+	const bool medium_vertex = (vr.flags & VOL_MEDIUM_VERTEX) != 0u;
+	if (!rec.pass_through) {
+		if (rec.did_nee) {
+			spectrum L = splat3(0.f);
+			if (vr.flags & VOL_NEE) {
+				const float4 b4 = w.beam[2 * i];
+				const spectrum b{b4.x, b4.y, b4.z};
+				if (medium_vertex) L = L + vr.nee_f * vr.nee_Le * b * vr.nee_w / vr.nee_pdf;
+				else L = L + (vr.nee_f * b) * vr.nee_Le * vr.nee_w / vr.nee_pdf;
+			}
+			if (vr.flags & VOL_MIS) {
+				const float4 b4 = w.beam[2 * i + 1];
+				const spectrum b{b4.x, b4.y, b4.z};
+				if (medium_vertex) L = L + rec.mis_f * vr.mis_Le * b * vr.mis_w / rec.mis_pdf;
+				else L = L + (rec.mis_f * b) * vr.mis_Le * vr.mis_w / rec.mis_pdf;
+			}
+			st.L = st.L + st.beta * L;
+		}
+		if (medium_vertex) {
+			// sample_medium_interaction (integrator.cpp:408-421): the phase value is its pdf, beta stays
+			vec3 wi;
+			hg_sample(rec.si.wo, vr.g, pcg_2d(st.rng), wi);
+			st.flags &= ~PATH_SPECULAR;
+			const ray_t r = spawn_ray(rec.si.p, vec3{0.f, 0.f, 0.f}, wi);
+			st.o = r.o;
+			st.d = r.d;
+			st.len = r.len;
+		} else {
+			vec3 wi;
+			float pdf;
+			if (!continue_bsdf<MAT_ANY>(s, st, rec, wi, pdf)) return false;
+		}
+	}
+	if (!medium_vertex) {
+		const entity_rec& ent = s.entities[rec.si.entity];
+		if (ent.flags & ENT_HAS_MEDIA) st.medium = medium_after(s, ent, rec.si.n, st.d);
+	}
+	return roulette(st, p.max_depth, p.rr_threshold);
+}
+
+__global__ void __launch_bounds__(128) k_vol_continue(scene_view s, wave_buffers w, uint32_t queue_in) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	uint32_t* qn = w.queue[queue_in ^ 1u];
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool alive = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = q[k];
+			path_state st = load_path(w, p, i);
+			if (!(st.flags & 0x80000000u)) {
+				alive = vol_continue(s, w, p, i, st);
+				if (!alive) finish(w, i, st.L);
+				store_path(w, i, st);
+			}
+		}
+		warp_push(alive, i, qn, w.counters + CNT_NEXT);
+	}
+}
+
+__global__ void k_advance(uint32_t* counters);
+
+template <bool COUNT>
+cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t queue_in, const launch_cfg& cfg,
+	cudaStream_t stream) {
+	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	k_extend<COUNT, true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	k_shade_a<CLASS_LAMBERT, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_METAL, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_GLASS_ROUGH, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_OTHER, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_MISS, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a_medium<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	k_vol_direct<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	k_beam<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	k_vol_continue<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	k_advance<<<1, 1, 0, stream>>>(w.counters);
+	return cudaGetLastError();
+}
+
 // Moves the next queue's count into place and accumulates the extend-ray count.
 __global__ void k_advance(uint32_t* counters) {
 	add64(counters, CNT_EXTEND_RAYS, counters[CNT_ACTIVE]);
@@ -490,6 +845,7 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_NEXT] = 0u;
 	counters[CNT_SECONDARY] = 0u;
 	counters[CNT_GUIDE] = 0u;
+	counters[CNT_BEAM] = 0u;
 	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
 }
 
@@ -500,17 +856,18 @@ __global__ void k_next_wave(wave_params* p, uint32_t capacity) { p->first_item +
 template <bool COUNT>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
+	if (cfg.volume) return volume_bounce<COUNT>(s, w, queue_in, cfg, stream);
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	const bool timed = cfg.events != nullptr && *cfg.next_event + 2 <= cfg.max_events;
 	uint32_t ev = timed ? *cfg.next_event : 0u;
 	if (timed) { cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 0; }
-	k_extend<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	k_extend<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
 	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
-	k_shade_a<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_METAL><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_MISS><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_LAMBERT, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_METAL, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_GLASS_ROUGH, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_OTHER, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_MISS, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	if (cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
 		const cudaError_t e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
 		if (e != cudaSuccess) return e;
@@ -581,6 +938,7 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 }
 
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
+	if (cfg.volume) return 3u + 12u * max_depth;
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
 	uint32_t n = 3u + (12u + (sample ? 1u : 0u)) * max_depth;

@@ -17,14 +17,17 @@ enum : uint32_t {
 	CNT_SECONDARY = 2,   // secondary rays queued this bounce
 	CNT_ERROR = 3,       // first device error (rb_status), 0 if none
 	CNT_CLASS = 4,       // paths per shading class this bounce (pt::NUM_CLASSES words)
-	CNT_GUIDE = 9,       // paths queued for a guide evaluation this bounce
-	CNT_EXTEND_RAYS = 10, // 64-bit stats, two words each (lo, hi) from here on
-	CNT_SHADOW_RAYS = 12,
-	CNT_MIS_RAYS = 14,
-	CNT_NODE_VISITS = 16,
-	CNT_TRI_TESTS = 18,
-	CNT_WORDS = 20
+	CNT_GUIDE = 10,      // paths queued for a guide evaluation this bounce
+	CNT_BEAM = 11,       // light connections queued for a transmittance walk this bounce
+	CNT_EXTEND_RAYS = 12, // 64-bit stats, two words each (lo, hi) from here on
+	CNT_SHADOW_RAYS = 14,
+	CNT_MIS_RAYS = 16,
+	CNT_NODE_VISITS = 18,
+	CNT_TRI_TESTS = 20,
+	CNT_BEAM_RAYS = 22,  // closest-hit queries of the transmittance walks
+	CNT_WORDS = 24
 };
+static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
 // words cleared at the start of a wave: everything before the 64-bit stats
 constexpr uint32_t kWaveCounterWords = CNT_EXTEND_RAYS;
 
@@ -75,6 +78,11 @@ struct wave_buffers {
 	uint32_t* counters;
 	wave_params* params;
 	guide::wave_guide guide;  // null pointers unless a guided render allocated them
+	// volume path tracing (null unless a volume render allocated them)
+	int32_t* medium;         // medium of each path, -1: vacuum
+	pt::vol_rec* vrec;       // light-connection factors of the current vertex
+	float4* beam;            // 2 per path: transmittance of the NEE and MIS connections
+	uint32_t* beam_queue;    // connections (2 i, 2 i + 1) waiting for their transmittance
 };
 
 struct film_buffers {
@@ -98,6 +106,7 @@ struct launch_cfg {
 	// GUIDE_TRAIN) deciding which guide kernels are launched
 	const guide::guide_state* guide = nullptr;
 	uint32_t guide_mode = 0;
+	bool volume = false;     // volume_path_integrator instead of path_integrator
 };
 
 // Ray batches for rb_trace_closest / rb_trace_shadow.

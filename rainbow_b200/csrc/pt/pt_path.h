@@ -29,6 +29,7 @@ struct path_state {
 	uint32_t flags;
 	int32_t bounces;
 	pcg32 rng;
+	int32_t medium;               // medium the path travels in (volume path tracing), -1: vacuum
 };
 
 // Everything shade_b needs from shade_a.
@@ -46,6 +47,23 @@ struct shade_record {
 	spectrum mis_f;               // f * |cos|
 	float mis_pdf;
 	ray_t shadow_ray, mis_ray;
+};
+
+// Volume path tracing keeps the factors of each light connection apart until
+// the connection's transmittance is known, so that it enters the sum at the
+// place the reference multiplies it in (integrator.cpp:139-146,180-191,226-232,263-271).
+enum : uint32_t { VOL_MEDIUM_VERTEX = 1u, VOL_NEE = 2u, VOL_MIS = 4u };
+struct vol_rec {
+	spectrum nee_f;      // f * |cos| (surface) or the phase value (medium vertex)
+	spectrum nee_Le;     // emitter_sample.intensity
+	float nee_w, nee_pdf;
+	vec3 nee_to;         // the sampled point on the emitter
+	spectrum mis_Le;     // radiance found by the MIS sample
+	float mis_w;
+	vec3 mis_to;         // the point it was found at
+	int32_t medium;      // medium of the path at this vertex
+	uint32_t flags;      // VOL_*
+	float g;             // phase asymmetry of a medium vertex
 };
 
 // perspective_camera::sample(position, u) (rainbow-cpu/cameras/perspective_camera.cpp:78-99)
@@ -83,6 +101,7 @@ RB_HD void path_begin(path_state& p, const float* r2c, const float* c2w, float l
 	p.eta = 1.f;
 	p.flags = 0u;
 	p.bounces = 0;
+	p.medium = -1;
 }
 
 RB_HD uint32_t hit_entity(const scene_view& s, int32_t slot) {
@@ -91,7 +110,10 @@ RB_HD uint32_t hit_entity(const scene_view& s, int32_t slot) {
 
 // Shading classes: hits are queued by the material kind of the hit entity so
 // that each shading kernel runs one BSDF's code on coherent warps.
-enum : uint32_t { CLASS_MISS = 0, CLASS_LAMBERT = 1, CLASS_METAL = 2, CLASS_GLASS_ROUGH = 3, CLASS_OTHER = 4, NUM_CLASSES = 5 };
+// CLASS_MEDIUM: paths inside a medium (volume path tracing), whose next vertex
+// is decided by free-flight sampling before any surface is shaded.
+enum : uint32_t { CLASS_MISS = 0, CLASS_LAMBERT = 1, CLASS_METAL = 2, CLASS_GLASS_ROUGH = 3, CLASS_OTHER = 4, CLASS_MEDIUM = 5,
+	NUM_CLASSES = 6 };
 constexpr int class_material(uint32_t c) {
 	return c == CLASS_LAMBERT ? static_cast<int>(MAT_LAMBERT)
 		: c == CLASS_METAL ? static_cast<int>(MAT_METAL)
@@ -115,9 +137,10 @@ RB_HD void shade_miss(const scene_view& s, path_state& p) {
 		for (uint32_t i = 0; i < s.num_environments; i++) p.L = p.L + p.beta * s.emitters[s.environments[i]].radiance;
 }
 
-// Returns false when the path ends here (a miss).
+// Returns false when the path ends here (a miss). vr (volume path tracing
+// only): receives the factors of the emitter-sampling connection.
 template <int MAT = MAT_ANY>
-RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_record& rec) {
+RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_record& rec, vol_rec* vr = nullptr) {
 	rec.pass_through = 0u;
 	rec.did_nee = 0u;
 	rec.guidable = 0u;
@@ -168,6 +191,13 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 			const float w = power_heuristic(ls.pdf, fpdf);
 			rec.nee_L = f * ls.L * w / ls.pdf;
 			rec.nee_entity = em.entity;
+			if (vr != nullptr) {
+				vr->nee_f = f;
+				vr->nee_Le = ls.L;
+				vr->nee_w = w;
+				vr->nee_pdf = ls.pdf;
+				vr->nee_to = ls.p;
+			}
 		}
 	}
 	// BSDF sampling half (integrator.cpp:161-198)

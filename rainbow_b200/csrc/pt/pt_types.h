@@ -70,7 +70,8 @@ enum : uint32_t {
 	ENT_HAS_SHAPE = 1u << 0,
 	ENT_HAS_MATERIAL = 1u << 1,
 	ENT_HAS_EMITTER = 1u << 2,
-	ENT_VISIBLE = 1u << 3  // shape and material (entity::visible, entity.cpp:80-83)
+	ENT_VISIBLE = 1u << 3, // shape and material (entity::visible, entity.cpp:80-83)
+	ENT_HAS_MEDIA = 1u << 4
 };
 
 struct entity_rec {
@@ -81,7 +82,23 @@ struct entity_rec {
 	int32_t emitter;      // index into the emitter table, -1 if none
 	uint32_t flags;
 	float area;           // shape_instance_properties::area (world-space area)
-	int32_t pad[3];
+	int32_t media;        // index into the media table, -1 if none
+	int32_t pad[2];
+};
+
+// homogeneous_medium (media/homogeneous_medium.cpp:7-11): sigma_t = sigma_a + sigma_s,
+// Henyey-Greenstein asymmetry g.
+struct medium_rec {
+	vec3 sigma_s;
+	vec3 sigma_t;
+	float g;
+	float pad;
+};
+
+// media(outside, inside) (media/medium.hpp:82-101): medium indices, -1 for vacuum.
+struct media_rec {
+	int32_t inside;
+	int32_t outside;
 };
 
 enum : uint32_t {
@@ -171,6 +188,10 @@ struct scene_view {
 	uint32_t num_emitters;
 	uint32_t num_environments;
 	uint32_t num_entities;
+	const medium_rec* mediums;
+	const media_rec* media;
+	uint32_t num_media;
+	uint32_t pad1;
 };
 
 } // namespace pt

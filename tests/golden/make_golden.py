@@ -14,8 +14,11 @@ product's seeded scene generator:
   bsdf_*         scattering_function_collection sample / evaluate / pdf per material
   box_image      32 x 32 box room, 256 spp, FP64 per-pixel sums of L and L^2
   bvh_c2         SHA-256 of the reference BVH of the 1,024,010-triangle sphere scene
+  fog_samples    radiance of 1024 (pixel, sample) pairs, volume_path_integrator::trace,
+                 depth 12, displaced spheres inside a homogeneous medium box
+  fog_image      32 x 32 fog scene, 256 spp, volume_path_integrator, FP64 sums of L and L^2
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [--only fog]
 """
 from __future__ import annotations
 
@@ -35,6 +38,7 @@ from oracle import ref  # noqa: E402
 BOX = dict(kind=rb.RB_SCENE_BOX, seed=0, width=64, height=64, num_spheres=0, subdivision=0)
 SPHERES = dict(kind=rb.RB_SCENE_SPHERES, seed=1, width=96, height=96, num_spheres=30, subdivision=2)
 C2 = dict(kind=rb.RB_SCENE_SPHERES, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4)
+FOG = dict(kind=rb.RB_SCENE_FOG, seed=4, width=48, height=48, num_spheres=24, subdivision=2)
 
 
 def scene_of(p):
@@ -58,7 +62,25 @@ def bvh_digest(nodes, pe, pi):
     return h.hexdigest()
 
 
+def fog_fixtures():
+    s = scene_of(FOG)
+    R = ref.RefScene(s)
+    R.set_volume(True)
+    rng = np.random.default_rng(13)
+    px = rng.integers(0, FOG["width"] * FOG["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=12, rr=1.0, seed=0)
+    save("fog_samples", params=params_array(FOG), pixels=px, samples=sm, radiance=L, max_depth=np.array(12))
+    small = dict(FOG, width=32, height=32)
+    R = ref.RefScene(scene_of(small))
+    R.set_volume(True)
+    sums, sq, _ = R.render(256, 0, 12, 1.0, 0, 0)
+    save("fog_image", params=params_array(small), spp=np.array(256), max_depth=np.array(12), sum=sums, sum_sq=sq)
+
+
 def main():
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "fog":
+        return fog_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -115,6 +137,7 @@ def main():
     nodes, pe, pi = R.bvh()
     save("bvh_c2", params=params_array(C2), digest=np.array(bvh_digest(nodes, pe, pi)),
          num_nodes=np.array(nodes.shape[0]), num_prims=np.array(pe.shape[0]))
+    fog_fixtures()
 
 
 def material_desc(m):

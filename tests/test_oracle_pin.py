@@ -108,3 +108,22 @@ def test_port_image_statistics_match_reference_fixture():
     z = np.where(se > 0, (m - m_ref) / np.where(se > 0, se, 1), 0)
     assert (np.abs(z) > 3).mean() < 0.01
     assert rays_fx is not None
+
+
+def test_reference_volume_integrator_runs_on_fog_scene():
+    """The compiled reference's volume_path_integrator renders the fog scene
+    with the product's media description, and the committed fixture is its
+    output."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference not compiled here")
+    fx = golden.load("fog_image")
+    scene = scene_from_params(fx["params"])
+    R = ref.RefScene(scene)
+    R.set_volume(True)
+    sums, sq, _ = R.render(8, 0, int(fx["max_depth"]), 1.0, 0, 1)
+    assert np.isfinite(sums).all() and sums.sum() > 0
+    # path_integrator ignores media: the two integrators differ on this scene
+    R.set_volume(False)
+    plain, _, _ = R.render(8, 0, int(fx["max_depth"]), 1.0, 0, 1)
+    assert not np.array_equal(plain, sums)
