@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 2
+#define RBGPU_ABI_VERSION 3
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -313,6 +313,76 @@ rb_status rb_set_profiling(rb_context* ctx, int enabled);
 /* Checkpoint / resume of the film accumulators and sample counter. */
 rb_status rb_checkpoint_save(rb_context* ctx, const char* path);
 rb_status rb_checkpoint_load(rb_context* ctx, const char* path);
+
+/* ------------------------------------------------------------------ launch tuning and autotuner
+ * No counterpart in the reference (its only knob is the 16x16 tile of
+ * sampler_integrator.cpp:30). The wavefront's launch shapes: paths per wave
+ * (queue capacity), threads per block of the traversal and shading kernels,
+ * blocks per SM of the grid-stride launches, and the sort key of the hit
+ * queues. Every setting gives the same image; only the speed changes. */
+enum {
+	RB_SORT_MATERIAL = 0,       /* one hit queue per material class (coherent shading warps) */
+	RB_SORT_NONE = 1            /* one hit queue for every surface hit (no sorting) */
+};
+typedef struct rb_tuning {
+	uint32_t paths_per_wave;    /* queue capacity, 0: library default (2^21); a render's own
+	                               rb_render_params.paths_per_wave takes precedence */
+	uint32_t block_trace;       /* 32..256, a multiple of 32; 0: 128 */
+	uint32_t block_shade;       /* 32..256, a multiple of 32; 0: 128 */
+	uint32_t grid_per_sm;       /* 1..64; 0: 8 */
+	uint32_t sort;              /* RB_SORT_* */
+	uint32_t reserved[3];
+} rb_tuning;
+/* Use `tuning` (NULL: defaults) for the context's later render calls. */
+rb_status rb_set_tuning(rb_context* ctx, const rb_tuning* tuning);
+rb_status rb_get_tuning(rb_context* ctx, rb_tuning* tuning);
+/* Autotuner: times renders of `probe_spp` samples per pixel of `params`
+ * (its camera, depth and seed; the film is left cleared) under candidate
+ * tunings by coordinate descent over the settings above (CUDA events, best of
+ * repeats), keeps the fastest for the context and returns it with its time. */
+rb_status rb_tune_render(rb_context* ctx, const rb_render_params* params, uint32_t probe_spp, rb_tuning* best,
+	float* best_ms);
+
+/* ------------------------------------------------------------------ batched rendering
+ * No counterpart in the reference, which renders one scene per
+ * integrator::render call (integrator.hpp:64-66). Many scenes of uneven size
+ * are uploaded together and rendered by one sequence of wavefront launches:
+ * their samples share waves and queues, every path carries its scene, and each
+ * scene's film is its own range of one merged film. Scene k's samples are the
+ * ones rb_render would make for it with the same camera, spp, first_sample and
+ * seed (same per-sample streams), so a batch and the scenes' separate renders
+ * give the same films up to the order of FP64 additions. Learned guiding and
+ * volumes are not available in batches. */
+typedef struct rb_batch_view {
+	rb_camera_desc camera;
+	uint32_t spp;
+	uint32_t first_sample;
+	uint32_t seed;
+	uint32_t reserved;
+} rb_batch_view;
+typedef struct rb_batch_params {
+	const rb_batch_view* views; /* one per uploaded scene, in upload order */
+	uint32_t count;             /* number of uploaded scenes */
+	uint32_t max_depth;         /* shared by every scene */
+	float rr_threshold;
+	uint32_t flags;             /* RB_RENDER_RESET only */
+	const uint32_t* order;      /* order in which scenes are started (a permutation), NULL: upload order */
+} rb_batch_params;
+/* Upload `count` scenes into the context, replacing any scene or batch there.
+ * Afterwards rb_render, rb_trace_* and rb_render_noalloc refuse the context
+ * until an rb_scene_upload. */
+rb_status rb_batch_upload(rb_context* ctx, const rb_scene_desc* scenes, uint32_t count);
+/* Render every scene of the batch. scene_ms (may be NULL, `count` floats):
+ * device time from the start of the call until the wave that completed each
+ * scene had finished (the scene's latency within the batch). */
+rb_status rb_batch_render(rb_context* ctx, const rb_batch_params* params, float* scene_ms);
+/* Film of scene `scene` of the last batch render (layout as rb_film_read / rb_render). */
+rb_status rb_batch_film_read(rb_context* ctx, uint32_t scene, double* sum_rgb, double* sum_sq_rgb, uint32_t* sample_count);
+rb_status rb_batch_image(rb_context* ctx, uint32_t scene, float* rgb_out);
+/* The autotuner on a batch: probes render the batch's first `probe_items`
+ * work items (scene order as in params). */
+rb_status rb_tune_batch(rb_context* ctx, const rb_batch_params* params, uint64_t probe_items, rb_tuning* best,
+	float* best_ms);
 
 /* ------------------------------------------------------------------ learned path guiding
  * No counterpart in the reference renderer, which samples path continuations

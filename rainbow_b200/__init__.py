@@ -24,6 +24,7 @@ from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_RENDER_GUIDE,
     RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
+    RB_SORT_MATERIAL, RB_SORT_NONE, BatchParams, BatchView, Tuning,
     BvhDesc, CameraDesc, MediaDesc, MediumDesc,
     GuideConfig, GuideStats, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
 )
@@ -249,6 +250,93 @@ class Context:
         st = GuideStats()
         check(lib().rb_guide_stats_get(self._h, C.byref(st)), "rb_guide_stats_get")
         return st
+
+
+    # ---- launch tuning (rb_set_tuning / rb_tune_render)
+    def set_tuning(self, tuning: Tuning | None = None, **fields) -> None:
+        t = Tuning()
+        if tuning is not None:
+            C.pointer(t)[0] = tuning
+        for k, v in fields.items():
+            setattr(t, k, v)
+        check(lib().rb_set_tuning(self._h, C.byref(t)), "rb_set_tuning")
+
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        check(lib().rb_get_tuning(self._h, C.byref(t)), "rb_get_tuning")
+        return t
+
+    def tune_render(self, camera: CameraDesc, probe_spp: int = 1, max_depth: int = 5, threshold: float = 1.0,
+                    seed: int = 0, volume: bool = False):
+        """Autotune the launch shapes on `probe_spp` samples per pixel; returns (Tuning, ms)."""
+        p = RenderParams()
+        p.camera = camera
+        p.spp, p.max_depth, p.rr_threshold, p.seed = probe_spp, max_depth, threshold, seed
+        p.flags = RB_RENDER_VOLUME if volume else 0
+        t, ms = Tuning(), C.c_float()
+        check(lib().rb_tune_render(self._h, C.byref(p), probe_spp, C.byref(t), C.byref(ms)), "rb_tune_render")
+        self._film_shape = (camera.width, camera.height)
+        return t, float(ms.value)
+
+    # ---- batched rendering (rb_batch_*)
+    def batch_upload(self, scenes) -> None:
+        """Upload many scenes at once (rb_batch_upload); replaces any scene."""
+        scenes = list(scenes)
+        arr = (SceneDesc * len(scenes))()
+        for k, sc in enumerate(scenes):
+            arr[k] = sc.desc
+        check(lib().rb_batch_upload(self._h, arr, len(scenes)), "rb_batch_upload")
+        self.batch_scenes = scenes
+        self.scene = None
+
+    def _batch_params(self, views, max_depth, threshold, reset, order):
+        arr = (BatchView * len(views))()
+        for k, v in enumerate(views):
+            arr[k].camera = v["camera"]
+            arr[k].spp = v["spp"]
+            arr[k].first_sample = v.get("first_sample", 0)
+            arr[k].seed = v.get("seed", 0)
+        p = BatchParams()
+        p.views = arr
+        p.count = len(views)
+        p.max_depth, p.rr_threshold, p.flags = max_depth, threshold, RB_RENDER_RESET if reset else 0
+        keep = [arr]
+        if order is not None:
+            o = (C.c_uint32 * len(order))(*[int(x) for x in order])
+            p.order = o
+            keep.append(o)
+        return p, keep
+
+    def batch_render(self, views, max_depth: int = 5, threshold: float = 1.0, reset: bool = True, order=None):
+        """Render every uploaded scene (views: dicts of camera, spp, first_sample, seed);
+        returns each scene's completion time in ms from the call's start."""
+        p, keep = self._batch_params(views, max_depth, threshold, reset, order)
+        ms = np.zeros(len(views), dtype=np.float32)
+        check(lib().rb_batch_render(self._h, C.byref(p), ms.ctypes.data), "rb_batch_render")
+        self._batch_shapes = [(v["camera"].width, v["camera"].height) for v in views]
+        return ms
+
+    def tune_batch(self, views, probe_items: int, max_depth: int = 5, threshold: float = 1.0, order=None):
+        p, keep = self._batch_params(views, max_depth, threshold, True, order)
+        t, ms = Tuning(), C.c_float()
+        check(lib().rb_tune_batch(self._h, C.byref(p), int(probe_items), C.byref(t), C.byref(ms)), "rb_tune_batch")
+        self._batch_shapes = [(v["camera"].width, v["camera"].height) for v in views]
+        return t, float(ms.value)
+
+    def batch_film(self, scene: int):
+        w, h = self._batch_shapes[scene]
+        sum_ = np.zeros((h, w, 3), dtype=np.float64)
+        sq = np.zeros_like(sum_)
+        cnt = np.zeros((h, w), dtype=np.uint32)
+        check(lib().rb_batch_film_read(self._h, scene, sum_.ctypes.data, sq.ctypes.data, cnt.ctypes.data),
+              "rb_batch_film_read")
+        return sum_, sq, cnt
+
+    def batch_image(self, scene: int) -> np.ndarray:
+        w, h = self._batch_shapes[scene]
+        img = np.zeros((h, w, 3), dtype=np.float32)
+        check(lib().rb_batch_image(self._h, scene, img.ctypes.data), "rb_batch_image")
+        return img
 
 
 class PathIntegrator:

@@ -33,6 +33,7 @@ RB_GUIDE_NUM_PARAMS = 30000
 RB_GUIDE_INPUTS = 9
 RB_GUIDE_OUTPUTS = 48
 RB_BVH_LEAF_FLAG = 0x80000000
+RB_SORT_MATERIAL, RB_SORT_NONE = 0, 1
 
 F16 = C.c_float * 16
 F3 = C.c_float * 3
@@ -91,6 +92,24 @@ class RenderParams(C.Structure):
     _fields_ = [("camera", CameraDesc), ("spp", C.c_uint32), ("first_sample", C.c_uint32),
                 ("max_depth", C.c_uint32), ("rr_threshold", C.c_float), ("seed", C.c_uint32),
                 ("flags", C.c_uint32), ("paths_per_wave", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("paths_per_wave", C.c_uint32), ("block_trace", C.c_uint32), ("block_shade", C.c_uint32),
+                ("grid_per_sm", C.c_uint32), ("sort", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in ("paths_per_wave", "block_trace", "block_shade", "grid_per_sm", "sort")}
+
+
+class BatchView(C.Structure):
+    _fields_ = [("camera", CameraDesc), ("spp", C.c_uint32), ("first_sample", C.c_uint32), ("seed", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class BatchParams(C.Structure):
+    _fields_ = [("views", C.POINTER(BatchView)), ("count", C.c_uint32), ("max_depth", C.c_uint32),
+                ("rr_threshold", C.c_float), ("flags", C.c_uint32), ("order", C.POINTER(C.c_uint32))]
 
 
 class RenderStats(C.Structure):
@@ -160,6 +179,16 @@ SIGNATURES = {
     "rb_guide_train": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     "rb_guide_sample_dirs": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "rb_guide_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GuideStats)]),
+    "rb_set_tuning": (C.c_int32, [C.c_void_p, C.POINTER(Tuning)]),
+    "rb_get_tuning": (C.c_int32, [C.c_void_p, C.POINTER(Tuning)]),
+    "rb_tune_render": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.POINTER(Tuning),
+                                   C.POINTER(C.c_float)]),
+    "rb_batch_upload": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.c_uint32]),
+    "rb_batch_render": (C.c_int32, [C.c_void_p, C.POINTER(BatchParams), C.c_void_p]),
+    "rb_batch_film_read": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rb_batch_image": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "rb_tune_batch": (C.c_int32, [C.c_void_p, C.POINTER(BatchParams), C.c_uint64, C.POINTER(Tuning),
+                                  C.POINTER(C.c_float)]),
 }
 
 

@@ -6,9 +6,7 @@
 // splits its pixels x spp work items into waves; each wave is one replay of the
 // captured graph (camera rays plus max_depth bounces), with the wave's first
 // work item written to a device-side parameter block before the replay.
-#include "../../include/rbgpu.h"
-#include "host/scene_pack.h"
-#include "kernels.cuh"
+#include "context.h"
 
 #include <cstdio>
 #include <cstring>
@@ -17,177 +15,14 @@
 
 using namespace rb;
 
+using namespace rb::ctx;
+
 namespace {
-
-template <typename T>
-cudaError_t dev_alloc(T** p, size_t count) {
-	*p = nullptr;
-	if (count == 0) return cudaSuccess;
-	return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
-}
-template <typename T>
-cudaError_t dev_upload(T** p, const std::vector<T>& v, cudaStream_t s) {
-	cudaError_t e = dev_alloc(p, v.size());
-	if (e != cudaSuccess || v.empty()) return e;
-	return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
-}
-template <typename T>
-void dev_free(T*& p) {
-	if (p) cudaFree(p);
-	p = nullptr;
-}
-
-rb_status from_cuda(cudaError_t e) {
-	if (e == cudaSuccess) return RB_OK;
-	if (e == cudaErrorMemoryAllocation) return RB_ERR_OUT_OF_MEMORY;
-	if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return RB_ERR_NO_DEVICE;
-	return RB_ERR_CUDA;
-}
-
-#define RB_CUDA(call)                                   \
-	do {                                                \
-		const cudaError_t rb_e_ = (call);               \
-		if (rb_e_ != cudaSuccess) return from_cuda(rb_e_); \
-	} while (0)
-
-struct device_scene {
-	pt::wide_node* wnodes = nullptr;
-	float4* nodes = nullptr;
-	float4* tri_a = nullptr;
-	float4* tri_b = nullptr;
-	float2* tri_c = nullptr;
-	uint32_t* prim_index = nullptr;
-	uint32_t* prim_entity = nullptr;
-	pt::entity_rec* entities = nullptr;
-	pt::mesh_rec* meshes = nullptr;
-	float* positions = nullptr;
-	float* normals = nullptr;
-	float* tangents = nullptr;
-	float* uvs = nullptr;
-	uint32_t* indices = nullptr;
-	pt::material_rec* materials = nullptr;
-	pt::emitter_rec* emitters = nullptr;
-	int32_t* environments = nullptr;
-	pt::medium_rec* mediums = nullptr;
-	pt::media_rec* media = nullptr;
-	void release() {
-		dev_free(wnodes); dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
-		dev_free(entities); dev_free(meshes); dev_free(positions); dev_free(normals); dev_free(tangents); dev_free(uvs);
-		dev_free(indices); dev_free(materials); dev_free(emitters); dev_free(environments);
-		dev_free(mediums); dev_free(media);
-	}
-};
-
-struct graph_key {
-	uint32_t capacity = 0, max_depth = 0, stack = 0;
-	bool count = false;
-	uint32_t guide_mode = 0, guide_steps = 0, guide_batch = 0;
-	bool volume = false;
-	bool operator==(const graph_key& o) const {
-		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
-			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch &&
-			volume == o.volume;
-	}
-};
-
 constexpr uint32_t kCheckpointMagic = 0x52424350u;  // "RBCP"
-
 } // namespace
 
-struct rb_context {
-	int device = 0;
-	int num_sms = 148;
-	cudaStream_t stream = nullptr;
-	cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
-
-	bool has_scene = false;
-	bool has_invisible = false;
-	uint32_t bvh_depth = 0;
-	uint32_t num_entities = 0;
-	device_scene scene;
-	pt::scene_view view{};
-
-	gpu::wave_buffers wave{};
-	uint32_t wave_capacity = 0;  // paths per wave of the current render call (<= wave_alloc)
-	uint32_t wave_alloc = 0;     // paths the wave buffers hold
-	gpu::wave_params* params_host = nullptr;  // pinned
-	gpu::film_buffers film{};
-	int32_t film_w = 0, film_h = 0;
-	uint64_t film_samples = 0;  // samples per pixel accumulated since the last reset
-
-	cudaGraphExec_t graph = nullptr;
-	graph_key graph_cfg;
-
-	rb_ray* trace_rays = nullptr;
-	rb_hit* trace_hits = nullptr;
-	size_t trace_cap = 0;
-
-	uint32_t* counters = nullptr;
-	uint32_t* counters_host = nullptr;  // pinned
-	bool counting = false;
-	bool profiling = false;
-	static constexpr uint32_t kMaxEvents = 4096;  // event pairs per render call when profiling
-	std::vector<cudaEvent_t> events;
-	std::vector<uint8_t> event_kind;
-	uint32_t next_event = 0;
-	rb_render_stats stats{};
-	guide::guide_state guide;        // learned path guide (allocated on first use)
-	uint32_t guide_mode = 0;         // gpu::GUIDE_* of the current render call
-	bool volume = false;             // the current render call uses the volume path integrator
-	int32_t* vol_medium = nullptr;   // per-path medium buffer (wave.medium points here in volume renders)
-	uint32_t vol_alloc = 0;          // paths the volume buffers hold
-
-	gpu::launch_cfg cfg() const {
-		gpu::launch_cfg c;
-		c.block_trace = 128;
-		c.block_shade = 128;
-		c.grid_trace = num_sms * 8;
-		c.grid_shade = num_sms * 8;
-		c.stack_depth = bvh_depth + 3 <= 32 ? 32 : 64;
-		c.count = counting;
-		if (guide_mode != 0u && guide.ready) {
-			c.guide = &guide;
-			c.guide_mode = guide_mode;
-		}
-		c.volume = volume;
-		return c;
-	}
-	gpu::launch_cfg profiled_cfg() {
-		gpu::launch_cfg c = cfg();
-		if (profiling && !events.empty()) {
-			c.events = events.data();
-			c.next_event = &next_event;
-			c.max_events = static_cast<uint32_t>(events.size() / 2);
-			c.event_kind = event_kind.data();
-		}
-		return c;
-	}
-
-	void release_wave() {
-		dev_free(wave.ray_o); dev_free(wave.ray_d); dev_free(wave.beta); dev_free(wave.radiance); dev_free(wave.bounces);
-		dev_free(wave.rng); dev_free(wave.pixel); dev_free(wave.sample); dev_free(wave.hit); dev_free(wave.rec); dev_free(wave.result);
-		dev_free(wave.sec_o); dev_free(wave.sec_d); dev_free(wave.sec_hit); dev_free(wave.queue[0]); dev_free(wave.queue[1]);
-		dev_free(wave.sec_queue);
-		dev_free(wave.class_queue);
-		dev_free(vol_medium); dev_free(wave.vrec); dev_free(wave.beam); dev_free(wave.beam_queue);
-		wave.medium = nullptr;
-		vol_alloc = 0;
-		wave_capacity = 0;
-		wave_alloc = 0;
-	}
-	void release_graph() {
-		if (graph) cudaGraphExecDestroy(graph);
-		graph = nullptr;
-		graph_cfg = graph_key();
-	}
-	void release_film() {
-		dev_free(film.sum); dev_free(film.sum_sq); dev_free(film.count);
-		film_w = film_h = 0;
-		film_samples = 0;
-	}
-};
-
-namespace {
+namespace rb {
+namespace ctx {
 
 rb_status ensure_wave(rb_context* c, uint32_t capacity) {
 	if (c->wave_alloc >= capacity) {
@@ -222,6 +57,7 @@ rb_status ensure_film(rb_context* c, int32_t width, int32_t height, bool reset) 
 		RB_CUDA(dev_alloc(&c->film.sum, 3 * px));
 		RB_CUDA(dev_alloc(&c->film.sum_sq, 3 * px));
 		RB_CUDA(dev_alloc(&c->film.count, px));
+		RB_CUDA(dev_alloc(&c->film_mean, 3 * px));
 		c->film_w = width;
 		c->film_h = height;
 		reset = true;
@@ -246,6 +82,12 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 	key.count = cfg.count;
 	key.guide_mode = cfg.guide_mode;
 	key.volume = cfg.volume;
+	key.batch = cfg.batch;
+	key.block_trace = static_cast<uint32_t>(cfg.block_trace);
+	key.block_shade = static_cast<uint32_t>(cfg.block_shade);
+	key.grid_trace = static_cast<uint32_t>(cfg.grid_trace);
+	key.grid_shade = static_cast<uint32_t>(cfg.grid_shade);
+	key.sort = cfg.sort;
 	if (cfg.guide) {
 		key.guide_steps = cfg.guide->cfg.steps_per_wave;
 		key.guide_batch = cfg.guide->cfg.batch_size;
@@ -313,12 +155,140 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 	return RB_OK;
 }
 
+// Runs the waves of one render call, whose parameters are in c->params_host
+// (first_item is set here): one graph replay per wave, or direct launches when
+// profiling or when invisible entities make paths outlive max_depth
+// iterations. Records wave_events[k] (when given) after wave k and fills the
+// call's statistics.
+rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, cudaEvent_t* wave_events) {
+	gpu::wave_params& hp = *c->params_host;
+	rb_status st = RB_OK;
+	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
+	const bool use_graph = !c->has_invisible && !c->profiling;
+	c->next_event = 0;
+	if (use_graph) {
+		st = capture_wave(c, max_depth);
+		if (st != RB_OK) return st;
+	}
+	const gpu::launch_cfg cfg = c->profiled_cfg();
+	uint32_t launches = 0;
+	hp.first_item = 0;
+	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
+	uint64_t wave = 0;
+	for (uint64_t first = 0; first < total; first += c->wave_capacity, wave++) {
+		if (use_graph) {
+			// the graph's last node moves params->first_item to the next wave
+			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+			launches += gpu::wave_launches(max_depth, cfg);
+		} else {
+			// direct launches: profiling, or invisible entities (a pass-through
+			// does not count as a bounce, so keep bouncing until the queue drains)
+			RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream));
+			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream));
+			launches += gpu::wave_launches(max_depth, cfg) - 2u;
+			uint32_t q = max_depth & 1u;
+			for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
+				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+				RB_CUDA(cudaStreamSynchronize(c->stream));
+				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
+				RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
+				launches += (cfg.sort == RB_SORT_NONE ? 7u : 12u) + ((cfg.guide_mode & gpu::GUIDE_SAMPLE) ? 1u : 0u);
+				q ^= 1u;
+			}
+			RB_CUDA(gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream));
+		}
+		if (wave_events != nullptr) RB_CUDA(cudaEventRecord(wave_events[wave], c->stream));
+	}
+	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	const uint32_t* h = c->counters_host;
+	auto u64 = [&](uint32_t w) { return static_cast<uint64_t>(h[w]) | (static_cast<uint64_t>(h[w + 1]) << 32); };
+	rb_render_stats& s = c->stats;
+	s.samples = total;
+	s.extend_rays = u64(gpu::CNT_EXTEND_RAYS);
+	s.shadow_rays = u64(gpu::CNT_SHADOW_RAYS);
+	s.mis_rays = u64(gpu::CNT_MIS_RAYS);
+	s.node_visits = u64(gpu::CNT_NODE_VISITS);
+	s.triangle_tests = u64(gpu::CNT_TRI_TESTS);
+	s.device_error = h[gpu::CNT_ERROR];
+	s.kernel_launches = launches;
+	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
+	s.extend_ms = s.secondary_ms = 0.f;
+	s.extend_launches = s.secondary_launches = 0;
+	for (uint32_t k = 0; c->profiling && k < c->next_event; k++) {
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, c->events[2 * k], c->events[2 * k + 1]);
+		if (c->event_kind[k] == 0) { s.extend_ms += ms; s.extend_launches++; }
+		else { s.secondary_ms += ms; s.secondary_launches++; }
+	}
+	return RB_OK;
+}
+
+// Replaces the context's scene (or batch) with the packed arrays of `p`.
+rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
+	if (p.bvh_depth + 3 > 64) return RB_ERR_UNSUPPORTED;
+	RB_CUDA(cudaSetDevice(c->device));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	c->release_graph();
+	c->scene.release();
+	c->release_batch();
+	c->has_scene = false;
+	device_scene& d = c->scene;
+	RB_CUDA(dev_upload(&d.nodes, p.nodes, c->stream));
+	if (p.wide_ok) RB_CUDA(dev_upload(&d.wnodes, p.wnodes, c->stream));
+	RB_CUDA(dev_upload(&d.tri_a, p.tri_a, c->stream));
+	RB_CUDA(dev_upload(&d.tri_b, p.tri_b, c->stream));
+	RB_CUDA(dev_upload(&d.tri_c, p.tri_c, c->stream));
+	RB_CUDA(dev_upload(&d.prim_index, p.prim_index, c->stream));
+	RB_CUDA(dev_upload(&d.prim_entity, p.prim_entity, c->stream));
+	RB_CUDA(dev_upload(&d.entities, p.entities, c->stream));
+	RB_CUDA(dev_upload(&d.meshes, p.meshes, c->stream));
+	RB_CUDA(dev_upload(&d.positions, p.positions, c->stream));
+	RB_CUDA(dev_upload(&d.normals, p.normals, c->stream));
+	RB_CUDA(dev_upload(&d.tangents, p.tangents, c->stream));
+	RB_CUDA(dev_upload(&d.uvs, p.uvs, c->stream));
+	RB_CUDA(dev_upload(&d.indices, p.indices, c->stream));
+	RB_CUDA(dev_upload(&d.materials, p.materials, c->stream));
+	RB_CUDA(dev_upload(&d.emitters, p.emitters, c->stream));
+	RB_CUDA(dev_upload(&d.environments, p.environments, c->stream));
+	RB_CUDA(dev_upload(&d.mediums, p.mediums, c->stream));
+	RB_CUDA(dev_upload(&d.media, p.media, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	pt::scene_view v{};
+	v.wnodes = p.wide_ok ? d.wnodes : nullptr;
+	v.root_a = p.root_a;
+	v.root_b = p.root_b;
+	v.root_ref = p.root_ref;
+	v.nodes = d.nodes; v.tri_a = d.tri_a; v.tri_b = d.tri_b; v.tri_c = d.tri_c; v.prim_index = d.prim_index;
+	v.entities = d.entities; v.meshes = d.meshes; v.positions = d.positions; v.normals = d.normals;
+	v.tangents = d.tangents; v.uvs = d.uvs; v.indices = d.indices; v.materials = d.materials; v.emitters = d.emitters;
+	v.environments = d.environments; v.env = p.env;
+	v.num_nodes = static_cast<uint32_t>(p.nodes.size() / 2);
+	v.num_emitters = static_cast<uint32_t>(p.emitters.size());
+	v.num_environments = static_cast<uint32_t>(p.environments.size());
+	v.num_entities = static_cast<uint32_t>(p.entities.size());
+	v.mediums = d.mediums;
+	v.media = d.media;
+	v.num_media = static_cast<uint32_t>(p.media.size());
+	c->view = v;
+	c->bvh_depth = p.bvh_depth;
+	c->num_entities = v.num_entities;
+	c->has_invisible = false;
+	for (const auto& e : p.entities)
+		if ((e.flags & pt::ENT_HAS_SHAPE) && !(e.flags & pt::ENT_HAS_MATERIAL)) c->has_invisible = true;
+	c->has_scene = true;
+	return RB_OK;
+}
+
 bool host_is_valid_camera(const rb_camera_desc& cam) {
 	return cam.width > 0 && cam.height > 0 && cam.width <= 16384 && cam.height <= 16384 &&
 		static_cast<uint64_t>(cam.width) * cam.height < (1ull << 24);
 }
 
-} // namespace
+} // namespace ctx
+} // namespace rb
 
 namespace rb {
 namespace gpu {
@@ -326,7 +296,7 @@ namespace gpu {
 // a context, for entry points defined in other files of the library.
 bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStream_t* stream, int* device,
 	uint32_t** counters_host) {
-	if (c == nullptr || !c->has_scene) return false;
+	if (c == nullptr || !c->has_scene || c->is_batch) return false;
 	*view = c->view;
 	*cfg = c->cfg();
 	cfg->count = false;
@@ -416,6 +386,8 @@ rb_status rb_context_destroy(rb_context* c) {
 	c->release_wave();
 	c->release_film();
 	c->scene.release();
+	c->release_batch();
+	for (cudaEvent_t e : c->wave_events) cudaEventDestroy(e);
 	guide::release(c->guide);
 	dev_free(c->trace_rays);
 	dev_free(c->trace_hits);
@@ -436,57 +408,7 @@ rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
 	host::packed_scene p;
 	const rb_status st = host::pack_scene(desc, p);
 	if (st != RB_OK) return st;
-	if (p.bvh_depth + 3 > 64) return RB_ERR_UNSUPPORTED;
-	RB_CUDA(cudaSetDevice(c->device));
-	RB_CUDA(cudaStreamSynchronize(c->stream));
-	c->release_graph();
-	c->scene.release();
-	c->has_scene = false;
-	device_scene& d = c->scene;
-	RB_CUDA(dev_upload(&d.nodes, p.nodes, c->stream));
-	if (p.wide_ok) RB_CUDA(dev_upload(&d.wnodes, p.wnodes, c->stream));
-	RB_CUDA(dev_upload(&d.tri_a, p.tri_a, c->stream));
-	RB_CUDA(dev_upload(&d.tri_b, p.tri_b, c->stream));
-	RB_CUDA(dev_upload(&d.tri_c, p.tri_c, c->stream));
-	RB_CUDA(dev_upload(&d.prim_index, p.prim_index, c->stream));
-	RB_CUDA(dev_upload(&d.prim_entity, p.prim_entity, c->stream));
-	RB_CUDA(dev_upload(&d.entities, p.entities, c->stream));
-	RB_CUDA(dev_upload(&d.meshes, p.meshes, c->stream));
-	RB_CUDA(dev_upload(&d.positions, p.positions, c->stream));
-	RB_CUDA(dev_upload(&d.normals, p.normals, c->stream));
-	RB_CUDA(dev_upload(&d.tangents, p.tangents, c->stream));
-	RB_CUDA(dev_upload(&d.uvs, p.uvs, c->stream));
-	RB_CUDA(dev_upload(&d.indices, p.indices, c->stream));
-	RB_CUDA(dev_upload(&d.materials, p.materials, c->stream));
-	RB_CUDA(dev_upload(&d.emitters, p.emitters, c->stream));
-	RB_CUDA(dev_upload(&d.environments, p.environments, c->stream));
-	RB_CUDA(dev_upload(&d.mediums, p.mediums, c->stream));
-	RB_CUDA(dev_upload(&d.media, p.media, c->stream));
-	RB_CUDA(cudaStreamSynchronize(c->stream));
-	pt::scene_view v{};
-	v.wnodes = p.wide_ok ? d.wnodes : nullptr;
-	v.root_a = p.root_a;
-	v.root_b = p.root_b;
-	v.root_ref = p.root_ref;
-	v.nodes = d.nodes; v.tri_a = d.tri_a; v.tri_b = d.tri_b; v.tri_c = d.tri_c; v.prim_index = d.prim_index;
-	v.entities = d.entities; v.meshes = d.meshes; v.positions = d.positions; v.normals = d.normals;
-	v.tangents = d.tangents; v.uvs = d.uvs; v.indices = d.indices; v.materials = d.materials; v.emitters = d.emitters;
-	v.environments = d.environments; v.env = p.env;
-	v.num_nodes = static_cast<uint32_t>(p.nodes.size() / 2);
-	v.num_emitters = static_cast<uint32_t>(p.emitters.size());
-	v.num_environments = static_cast<uint32_t>(p.environments.size());
-	v.num_entities = static_cast<uint32_t>(p.entities.size());
-	v.mediums = d.mediums;
-	v.media = d.media;
-	v.num_media = static_cast<uint32_t>(p.media.size());
-	c->view = v;
-	c->bvh_depth = p.bvh_depth;
-	c->num_entities = v.num_entities;
-	c->has_invisible = false;
-	for (const auto& e : p.entities)
-		if ((e.flags & pt::ENT_HAS_SHAPE) && !(e.flags & pt::ENT_HAS_MATERIAL)) c->has_invisible = true;
-	c->has_scene = true;
-	return RB_OK;
+	return upload_packed(c, p);
 }
 
 static rb_status trace_device(rb_context* c, const rb_ray* d_rays, uint32_t n, rb_hit* d_hits, bool shadow, cudaStream_t s) {
@@ -498,6 +420,7 @@ static rb_status trace_device(rb_context* c, const rb_ray* d_rays, uint32_t n, r
 static rb_status trace_host(rb_context* c, const rb_ray* rays, uint32_t n, rb_hit* hits, bool shadow) {
 	if (c == nullptr || (n > 0 && (rays == nullptr || hits == nullptr))) return RB_ERR_INVALID_ARGUMENT;
 	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	if (c->is_batch) return RB_ERR_INVALID_ARGUMENT;
 	if (n == 0) return RB_OK;
 	RB_CUDA(cudaSetDevice(c->device));
 	if (c->trace_cap < n) {
@@ -525,12 +448,14 @@ rb_status rb_trace_shadow(rb_context* c, const rb_ray* rays, uint32_t n, rb_hit*
 rb_status rb_trace_closest_device(rb_context* c, const rb_ray* d_rays, uint32_t n, rb_hit* d_hits, void* stream) {
 	if (c == nullptr || (n > 0 && (d_rays == nullptr || d_hits == nullptr))) return RB_ERR_INVALID_ARGUMENT;
 	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	if (c->is_batch) return RB_ERR_INVALID_ARGUMENT;
 	RB_CUDA(cudaSetDevice(c->device));
 	return trace_device(c, d_rays, n, d_hits, false, stream ? static_cast<cudaStream_t>(stream) : c->stream);
 }
 rb_status rb_trace_shadow_device(rb_context* c, const rb_ray* d_rays, uint32_t n, rb_hit* d_hits, void* stream) {
 	if (c == nullptr || (n > 0 && (d_rays == nullptr || d_hits == nullptr))) return RB_ERR_INVALID_ARGUMENT;
 	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	if (c->is_batch) return RB_ERR_INVALID_ARGUMENT;
 	RB_CUDA(cudaSetDevice(c->device));
 	return trace_device(c, d_rays, n, d_hits, true, stream ? static_cast<cudaStream_t>(stream) : c->stream);
 }
@@ -557,6 +482,7 @@ rb_status rb_set_profiling(rb_context* c, int enabled) {
 rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) {
 	if (c == nullptr || prm == nullptr) return RB_ERR_INVALID_ARGUMENT;
 	if (!c->has_scene) return RB_ERR_NO_SCENE;
+	if (c->is_batch) return RB_ERR_INVALID_ARGUMENT;
 	const rb_camera_desc& cam = prm->camera;
 	if (!host_is_valid_camera(cam) || prm->max_depth == 0 || prm->max_depth > 64) return RB_ERR_INVALID_ARGUMENT;
 	if (static_cast<uint64_t>(prm->first_sample) + prm->spp > (1u << 24)) return RB_ERR_INVALID_ARGUMENT;
@@ -565,7 +491,7 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	if (st != RB_OK) return st;
 	const uint64_t pixels = static_cast<uint64_t>(cam.width) * cam.height;
 	const uint64_t total = pixels * prm->spp;
-	uint64_t capacity = prm->paths_per_wave ? prm->paths_per_wave : (1ull << 21);
+	uint64_t capacity = prm->paths_per_wave ? prm->paths_per_wave : c->tuning.paths_per_wave ? c->tuning.paths_per_wave : (1ull << 21);
 	if (capacity > total) capacity = total;
 	if (capacity > (1ull << 24)) return RB_ERR_INVALID_ARGUMENT;
 	if (capacity == 0) capacity = 1;
@@ -600,75 +526,18 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		}
 	}
 
-	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
-	const bool use_graph = !c->has_invisible && !c->profiling;
-	c->next_event = 0;
-	if (use_graph) {
-		st = capture_wave(c, prm->max_depth);
-		if (st != RB_OK) return st;
-	}
-	const gpu::launch_cfg cfg = c->profiled_cfg();
-	uint32_t launches = 0;
-	hp.first_item = 0;
-	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
-	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
-	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
-		if (use_graph) {
-			// the graph's last node moves params->first_item to the next wave
-			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
-			launches += gpu::wave_launches(prm->max_depth, cfg);
-		} else {
-			// direct launches: profiling, or invisible entities (a pass-through
-			// does not count as a bounce, so keep bouncing until the queue drains)
-			RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream));
-			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, prm->max_depth, 0u, cfg, c->stream));
-			launches += gpu::wave_launches(prm->max_depth, cfg) - 2u;
-			uint32_t q = prm->max_depth & 1u;
-			for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
-				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-				RB_CUDA(cudaStreamSynchronize(c->stream));
-				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
-				RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
-				launches += 12 + ((cfg.guide_mode & gpu::GUIDE_SAMPLE) ? 1u : 0u);
-				q ^= 1u;
-			}
-			RB_CUDA(gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream));
-		}
-	}
-	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
-	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-	RB_CUDA(cudaStreamSynchronize(c->stream));
+	st = run_waves(c, total, prm->max_depth, nullptr);
+	if (st != RB_OK) return st;
 	const uint32_t* h = c->counters_host;
-	auto u64 = [&](uint32_t w) { return static_cast<uint64_t>(h[w]) | (static_cast<uint64_t>(h[w + 1]) << 32); };
-	rb_render_stats& s = c->stats;
-	s.samples = total;
-	s.extend_rays = u64(gpu::CNT_EXTEND_RAYS);
-	s.shadow_rays = u64(gpu::CNT_SHADOW_RAYS);
-	s.mis_rays = u64(gpu::CNT_MIS_RAYS);
-	s.node_visits = u64(gpu::CNT_NODE_VISITS);
-	s.triangle_tests = u64(gpu::CNT_TRI_TESTS);
-	s.device_error = h[gpu::CNT_ERROR];
-	s.kernel_launches = launches;
-	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
-	s.extend_ms = s.secondary_ms = 0.f;
-	s.extend_launches = s.secondary_launches = 0;
-	for (uint32_t k = 0; c->profiling && k < c->next_event; k++) {
-		float ms = 0.f;
-		cudaEventElapsedTime(&ms, c->events[2 * k], c->events[2 * k + 1]);
-		if (c->event_kind[k] == 0) { s.extend_ms += ms; s.extend_launches++; }
-		else { s.secondary_ms += ms; s.secondary_launches++; }
-	}
 	c->film_samples += prm->spp;
 	if (h[gpu::CNT_ERROR] != 0) return static_cast<rb_status>(h[gpu::CNT_ERROR]);
 
 	if (rgb_out != nullptr) {
-		std::vector<double> sum(3 * pixels);
-		std::vector<uint32_t> cnt(pixels);
-		RB_CUDA(cudaMemcpy(sum.data(), c->film.sum, sum.size() * sizeof(double), cudaMemcpyDeviceToHost));
-		RB_CUDA(cudaMemcpy(cnt.data(), c->film.count, cnt.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-		for (uint64_t i = 0; i < pixels; i++)
-			for (int k = 0; k < 3; k++)
-				rgb_out[3 * i + k] = cnt[i] ? static_cast<float>(sum[3 * i + k] / cnt[i]) : 0.f;
+		// means on the device, then one copy of 3 floats per pixel (at full speed
+		// when the caller's buffer is page-locked)
+		RB_CUDA(gpu::launch_film_mean(c->film, static_cast<uint32_t>(pixels), c->film_mean, c->num_sms * 4, c->stream));
+		RB_CUDA(cudaMemcpyAsync(rgb_out, c->film_mean, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+		RB_CUDA(cudaStreamSynchronize(c->stream));
 	}
 	return RB_OK;
 }

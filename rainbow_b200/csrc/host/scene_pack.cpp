@@ -9,6 +9,7 @@
 #include "scene_pack.h"
 
 #include "../pt/pt_bsdf.h"
+#include "../pt/pt_geom.h"
 
 #include <cmath>
 #include <cstring>
@@ -227,7 +228,8 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			}
 			out.bvh_depth = depth;
 		}
-		// ---- wide nodes: interior nodes numbered in preorder, children's boxes inline
+		// ---- 4-wide nodes: every binary node at an even depth with its
+		// grandchildren as slots, numbered in preorder
 		{
 			const uint32_t nn = bvh.num_nodes;
 			auto word = [&](uint32_t n, int k) {
@@ -235,34 +237,67 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 				std::memcpy(&v, bvh.nodes + 8ull * n + k, 4);
 				return v;
 			};
-			std::vector<uint32_t> wid(nn, 0xffffffffu);
-			uint32_t next = 0;
-			for (uint32_t n = 0; n < nn; n++)
-				if (!(word(n, 7) & RB_BVH_LEAF_FLAG)) wid[n] = next++;
-			bool ok = bvh.num_prims < (1u << 24);
-			auto ref_of = [&](uint32_t n) -> uint32_t {
-				const uint32_t w1 = word(n, 7);
-				if (!(w1 & RB_BVH_LEAF_FLAG)) return wid[n];
-				const uint32_t count = w1 & ~RB_BVH_LEAF_FLAG, first = word(n, 6);
+			auto is_leaf = [&](uint32_t n) { return (word(n, 7) & RB_BVH_LEAF_FLAG) != 0; };
+			bool ok = bvh.num_prims < (1u << 24) && nn > 0;
+			auto leaf_ref = [&](uint32_t n) -> uint32_t {
+				const uint32_t count = word(n, 7) & ~RB_BVH_LEAF_FLAG, first = word(n, 6);
 				if (count == 0 || count > 127 || first >= (1u << 24)) ok = false;
 				return pt::kRefLeaf | ((count & 0x7fu) << 24) | (first & 0x00ffffffu);
 			};
-			out.wnodes.resize(next);
-			for (uint32_t n = 0; n < nn; n++) {
-				if (wid[n] == 0xffffffffu) continue;
-				const uint32_t l = n + 1, r = word(n, 6);
-				const float* bl = bvh.nodes + 8ull * l;
-				const float* br = bvh.nodes + 8ull * r;
-				pt::wide_node& w = out.wnodes[wid[n]];
-				w.a = float4{bl[0], bl[1], bl[2], bl[3]};
-				w.b = float4{bl[4], bl[5], br[0], br[1]};
-				w.c = float4{br[2], br[3], br[4], br[5]};
-				w.d = uint4{ref_of(l), ref_of(r), word(n, 7), 0u};
+			auto set_slot = [&](pt::node4& q, int k, uint32_t n, uint32_t ref) {
+				const float* b = bvh.nodes + 8ull * n;
+				reinterpret_cast<float*>(&q.lo_x)[k] = b[0];
+				reinterpret_cast<float*>(&q.lo_y)[k] = b[1];
+				reinterpret_cast<float*>(&q.lo_z)[k] = b[2];
+				reinterpret_cast<float*>(&q.hi_x)[k] = b[3];
+				reinterpret_cast<float*>(&q.hi_y)[k] = b[4];
+				reinterpret_cast<float*>(&q.hi_z)[k] = b[5];
+				reinterpret_cast<uint32_t*>(&q.ref)[k] = ref;
+				q.meta.x |= 1u << (8 + k);
+			};
+			// depth-first with an explicit work list: (binary node, node4 index)
+			std::vector<std::pair<uint32_t, uint32_t>> todo;
+			if (ok && !is_leaf(0)) {
+				out.wnodes.push_back(pt::node4{});
+				todo.push_back({0u, 0u});
+			}
+			while (ok && !todo.empty()) {
+				const auto [n, id] = todo.back();
+				todo.pop_back();
+				pt::node4 q{};
+				q.meta.x = word(n, 7) & 3u;
+				const uint32_t child[2] = {n + 1, word(n, 6)};
+				std::vector<std::pair<uint32_t, uint32_t>> later;
+				for (int p = 0; p < 2; p++) {
+					const uint32_t x = child[p];
+					if (x >= nn) { ok = false; break; }
+					if (is_leaf(x)) {
+						set_slot(q, 2 * p, x, leaf_ref(x));
+						continue;
+					}
+					q.meta.x |= (word(x, 7) & 3u) << (2 + 2 * p);
+					const uint32_t grand[2] = {x + 1, word(x, 6)};
+					for (int g = 0; g < 2; g++) {
+						const uint32_t y = grand[g];
+						if (y >= nn) { ok = false; break; }
+						if (is_leaf(y)) {
+							set_slot(q, 2 * p + g, y, leaf_ref(y));
+						} else {
+							const uint32_t yid = static_cast<uint32_t>(out.wnodes.size());
+							out.wnodes.push_back(pt::node4{});
+							set_slot(q, 2 * p + g, y, yid);
+							later.push_back({y, yid});
+						}
+					}
+				}
+				out.wnodes[id] = q;
+				for (auto it = later.rbegin(); it != later.rend(); ++it) todo.push_back(*it);
 			}
 			out.root_a = float4{bvh.nodes[0], bvh.nodes[1], bvh.nodes[2], bvh.nodes[3]};
 			out.root_b = float4{bvh.nodes[4], bvh.nodes[5], 0.f, 0.f};
-			out.root_ref = nn > 0 ? ref_of(0) : 0u;
-			out.wide_ok = ok && nn > 0;
+			out.root_ref = nn > 0 ? (is_leaf(0) ? leaf_ref(0) : 0u) : 0u;
+			out.wide_ok = ok;
+			if (!ok) out.wnodes.clear();
 		}
 		out.tri_a.resize(bvh.num_prims);
 		out.tri_b.resize(bvh.num_prims);
@@ -287,6 +322,123 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			out.tri_c[s] = float2{e2.z, wf};
 		}
 		rb_bvh_free(built);
+	} catch (const std::bad_alloc&) {
+		return RB_ERR_OUT_OF_MEMORY;
+	}
+	return RB_OK;
+}
+
+namespace {
+uint32_t bits(float f) { uint32_t v; std::memcpy(&v, &f, 4); return v; }
+float from_bits(uint32_t v) { float f; std::memcpy(&f, &v, 4); return f; }
+template <typename T>
+void append_vec(std::vector<T>& dst, const std::vector<T>& src) { dst.insert(dst.end(), src.begin(), src.end()); }
+} // namespace
+
+rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out, std::vector<scene_place>& places) {
+	try {
+		out = packed_scene();
+		places.clear();
+		bool wide_ok = true;
+		uint64_t slots = 0;
+		for (const packed_scene& p : parts) {
+			wide_ok = wide_ok && p.wide_ok;
+			slots += p.tri_a.size();
+		}
+		if (slots >= (1ull << 31) || parts.empty()) return RB_ERR_UNSUPPORTED;
+		wide_ok = wide_ok && slots < (1ull << 24);
+		for (const packed_scene& p : parts) {
+			const uint32_t node_base = static_cast<uint32_t>(out.nodes.size() / 2);
+			const uint32_t wnode_base = static_cast<uint32_t>(out.wnodes.size());
+			const uint32_t slot_base = static_cast<uint32_t>(out.tri_a.size());
+			const uint32_t entity_base = static_cast<uint32_t>(out.entities.size());
+			const uint32_t mesh_base = static_cast<uint32_t>(out.meshes.size());
+			const uint32_t vertex_base = static_cast<uint32_t>(out.positions.size() / 3);
+			const uint32_t index_base = static_cast<uint32_t>(out.indices.size());
+			const uint32_t material_base = static_cast<uint32_t>(out.materials.size());
+			const uint32_t emitter_base = static_cast<uint32_t>(out.emitters.size());
+			const uint32_t env_base = static_cast<uint32_t>(out.environments.size());
+			const int32_t medium_base = static_cast<int32_t>(out.mediums.size());
+			const int32_t media_base = static_cast<int32_t>(out.media.size());
+			// reference-layout nodes: interior w0 = right child, leaf w0 = first slot
+			for (size_t n = 0; n < p.nodes.size() / 2; n++) {
+				float4 a = p.nodes[2 * n], b = p.nodes[2 * n + 1];
+				const uint32_t w1 = bits(b.w);
+				b.z = from_bits(bits(b.z) + ((w1 & RB_BVH_LEAF_FLAG) ? slot_base : node_base));
+				out.nodes.push_back(a);
+				out.nodes.push_back(b);
+			}
+			auto reloc_ref = [&](uint32_t r) {
+				if (!(r & pt::kRefLeaf)) return r + wnode_base;
+				const uint32_t first = (r & 0x00ffffffu) + slot_base;
+				return (r & 0xff000000u) | (first & 0x00ffffffu);
+			};
+			if (wide_ok) {
+				for (pt::node4 w : p.wnodes) {
+					uint32_t* ref = reinterpret_cast<uint32_t*>(&w.ref);
+					for (int k = 0; k < 4; k++)
+						if (w.meta.x & (1u << (8 + k))) ref[k] = reloc_ref(ref[k]);
+					out.wnodes.push_back(w);
+				}
+			}
+			for (size_t k = 0; k < p.tri_a.size(); k++) {
+				float2 c = p.tri_c[k];
+				const uint32_t w = bits(c.y);
+				c.y = from_bits(((w & ~pt::kEntityInvisible) + entity_base) | (w & pt::kEntityInvisible));
+				out.tri_c.push_back(c);
+				out.prim_entity.push_back(p.prim_entity[k] + entity_base);
+			}
+			append_vec(out.tri_a, p.tri_a);
+			append_vec(out.tri_b, p.tri_b);
+			append_vec(out.prim_index, p.prim_index);
+			for (pt::entity_rec e : p.entities) {
+				if (e.mesh >= 0) e.mesh += static_cast<int32_t>(mesh_base);
+				if (e.material >= 0) e.material += static_cast<int32_t>(material_base);
+				// e.emitter stays scene-relative: a scene's view offsets the emitter array
+				if (e.media >= 0) e.media += media_base;
+				out.entities.push_back(e);
+			}
+			for (pt::mesh_rec m : p.meshes) {
+				m.vertex_offset += vertex_base;
+				m.index_offset += index_base;
+				out.meshes.push_back(m);
+			}
+			append_vec(out.positions, p.positions);
+			append_vec(out.normals, p.normals);
+			append_vec(out.tangents, p.tangents);
+			append_vec(out.uvs, p.uvs);
+			append_vec(out.indices, p.indices);
+			append_vec(out.materials, p.materials);
+			for (pt::emitter_rec e : p.emitters) {
+				e.entity += static_cast<int32_t>(entity_base);
+				out.emitters.push_back(e);
+			}
+			append_vec(out.environments, p.environments);  // scene-relative emitter indices
+			append_vec(out.mediums, p.mediums);
+			for (pt::media_rec m : p.media) {
+				if (m.inside >= 0) m.inside += medium_base;
+				if (m.outside >= 0) m.outside += medium_base;
+				out.media.push_back(m);
+			}
+			scene_place pl{};
+			pl.root_a = p.root_a;
+			pl.root_b = p.root_b;
+			pl.root_ref = wide_ok ? reloc_ref(p.root_ref) : 0u;
+			pl.root_node = node_base;
+			pl.emitter_base = emitter_base;
+			pl.num_emitters = static_cast<uint32_t>(p.emitters.size());
+			pl.env_base = env_base;
+			pl.num_environments = static_cast<uint32_t>(p.environments.size());
+			pl.env = p.env;
+			places.push_back(pl);
+			out.bvh_depth = p.bvh_depth > out.bvh_depth ? p.bvh_depth : out.bvh_depth;
+		}
+		out.wide_ok = wide_ok;
+		if (!wide_ok) out.wnodes.clear();
+		out.root_a = places[0].root_a;
+		out.root_b = places[0].root_b;
+		out.root_ref = places[0].root_ref;
+		out.env = places[0].env;
 	} catch (const std::bad_alloc&) {
 		return RB_ERR_OUT_OF_MEMORY;
 	}

@@ -95,16 +95,16 @@ __device__ __forceinline__ bool trace_one(const scene_view& s, vec3 o, vec3 d, f
 	uint32_t& nodes, uint32_t& tris) {
 	trace_counters c{0u, 0u};
 	bool ok;
-	if (s.wnodes != nullptr && !isnan(len)) {
+	if (!COUNT && s.wnodes != nullptr && !isnan(len)) {
 		const float len0 = len;
-		const int r = closest_hit_fast<SHADOW, COUNT>(s, o, d, len, h, st, c);
+		const int r = closest_hit_fast<SHADOW>(s, o, d, len, h, st);
 		ok = r == 1;
-		if (r < 0) {  // a NaN length appeared: redo the ray in the reference's own visiting order
+		if (r < 0) {  // a NaN length or a full stack: redo the ray in the reference's own visiting order
 			len = len0;
-			c = trace_counters{0u, 0u};
 			ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
 		}
 	} else {
+		// counting passes count the box and triangle tests of the reference's traversal
 		ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
 	}
 	nodes += c.nodes;
@@ -114,7 +114,7 @@ __device__ __forceinline__ bool trace_one(const scene_view& s, vec3 o, vec3 d, f
 
 // ------------------------------------------------------------------ ray batches
 template <bool SHADOW, bool COUNT>
-__global__ void __launch_bounds__(128) k_trace_rays(scene_view s, const uint32_t* __restrict__ prim_entity,
+__global__ void __launch_bounds__(256) k_trace_rays(scene_view s, const uint32_t* __restrict__ prim_entity,
 	const rb_ray* __restrict__ rays, uint32_t n, rb_hit* __restrict__ hits, uint32_t stack_cap, uint32_t* counters) {
 	extern __shared__ uint32_t smem[];
 	smem_stack st = make_stack(smem, stack_cap);
@@ -251,13 +251,38 @@ __device__ bool shade_b_guided_any(const scene_view& s, const wave_buffers& w, c
 }
 
 // ------------------------------------------------------------------ wavefront
+template <bool BATCH = false>
 __device__ __forceinline__ pcg32 load_rng(const wave_buffers& w, const wave_params& p, uint32_t i) {
 	pcg32 g;
 	g.state = w.rng[i];
-	g.inc = (stream_seed(w.pixel[i], w.sample[i], p.seed) << 1u) | 1u;
+	const uint32_t seed = BATCH ? w.batch[w.scene[i]].seed : p.seed;
+	g.inc = (stream_seed(w.pixel[i], w.sample[i], seed) << 1u) | 1u;
 	return g;
 }
 
+// Scene of work item `item` of a batch: the last scene whose first item is <= item.
+__device__ __forceinline__ uint32_t batch_scene_of_item(const wave_buffers& w, uint64_t item) {
+	uint32_t lo = 0, hi = w.num_scenes;
+	while (hi - lo > 1) {
+		const uint32_t mid = (lo + hi) >> 1;
+		if (w.batch[mid].item_base <= item) lo = mid;
+		else hi = mid;
+	}
+	return lo;
+}
+
+// Scene of merged-film pixel g of a batch.
+__device__ __forceinline__ uint32_t batch_scene_of_pixel(const wave_buffers& w, uint32_t g) {
+	uint32_t lo = 0, hi = w.num_scenes;
+	while (hi - lo > 1) {
+		const uint32_t mid = (lo + hi) >> 1;
+		if (w.batch[mid].pixel_base <= g) lo = mid;
+		else hi = mid;
+	}
+	return lo;
+}
+
+template <bool BATCH = false>
 __device__ __forceinline__ path_state load_path(const wave_buffers& w, const wave_params& p, uint32_t i) {
 	path_state st;
 	const float4 o = w.ray_o[i], d = w.ray_d[i], b = w.beta[i], L = w.radiance[i];
@@ -269,7 +294,7 @@ __device__ __forceinline__ path_state load_path(const wave_buffers& w, const wav
 	st.L = vec3{L.x, L.y, L.z};
 	st.flags = __float_as_uint(L.w);
 	st.bounces = w.bounces[i];
-	st.rng = load_rng(w, p, i);
+	st.rng = load_rng<BATCH>(w, p, i);
 	st.medium = w.medium != nullptr ? w.medium[i] : -1;
 	return st;
 }
@@ -320,8 +345,64 @@ __global__ void __launch_bounds__(256) k_film_resolve(wave_buffers w, film_buffe
 	}
 }
 
+// k_film_resolve for a batch: merged-film pixel g of scene k has the items
+// item_base + s * pixels + (g - pixel_base), s = 0 .. spp - 1; one thread per
+// pixel of the scenes the wave overlaps sums that pixel's paths of the wave in
+// path order (no atomics, as above).
+__global__ void __launch_bounds__(256) k_film_resolve_batch(wave_buffers w, film_buffers f) {
+	const wave_params& p = *w.params;
+	const uint64_t first = p.first_item;
+	const uint64_t left = p.total_items > first ? p.total_items - first : 0;
+	const uint64_t n = left < w.capacity ? left : w.capacity;
+	if (n == 0) return;
+	const batch_scene& b0 = w.batch[batch_scene_of_item(w, first)];
+	const batch_scene& b1 = w.batch[batch_scene_of_item(w, first + n - 1)];
+	const uint32_t g0 = b0.pixel_base, g1 = b1.pixel_base + b1.width * b1.height;
+	for (uint32_t g = g0 + blockIdx.x * blockDim.x + threadIdx.x; g < g1; g += gridDim.x * blockDim.x) {
+		const batch_scene& b = w.batch[batch_scene_of_pixel(w, g)];
+		const uint64_t px = static_cast<uint64_t>(b.width) * b.height;
+		const uint64_t base = b.item_base + (g - b.pixel_base);  // the pixel's item of sample 0
+		uint64_t s = base >= first ? 0 : (first - base + px - 1) / px;
+		double s0 = 0, s1 = 0, s2 = 0, q0 = 0, q1 = 0, q2 = 0;
+		uint32_t c = 0;
+		for (; s < b.spp; s++) {
+			const uint64_t item = base + s * px;
+			if (item >= first + n) break;
+			const float4 L = w.result[item - first];
+			if (L.w == 0.f) continue;
+			s0 += L.x; s1 += L.y; s2 += L.z;
+			q0 += static_cast<double>(L.x) * L.x;
+			q1 += static_cast<double>(L.y) * L.y;
+			q2 += static_cast<double>(L.z) * L.z;
+			c++;
+		}
+		if (c == 0) continue;
+		double* sp = f.sum + 3 * static_cast<size_t>(g);
+		double* qp = f.sum_sq + 3 * static_cast<size_t>(g);
+		sp[0] += s0; sp[1] += s1; sp[2] += s2;
+		qp[0] += q0; qp[1] += q1; qp[2] += q2;
+		f.count[g] += c;
+	}
+}
+
+// Per-pixel mean of the film (film::set_pixel's value after film::add_tile):
+// rgb = sum / count in FP64, rounded once to float; 0 for a pixel without samples.
+__global__ void __launch_bounds__(256) k_film_mean(film_buffers f, uint32_t pixels, float* __restrict__ rgb) {
+	for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < pixels; px += gridDim.x * blockDim.x) {
+		const uint32_t c = f.count[px];
+		const double* sp = f.sum + 3 * static_cast<size_t>(px);
+		float* o = rgb + 3 * static_cast<size_t>(px);
+		o[0] = c ? static_cast<float>(sp[0] / c) : 0.f;
+		o[1] = c ? static_cast<float>(sp[1] / c) : 0.f;
+		o[2] = c ? static_cast<float>(sp[2] / c) : 0.f;
+	}
+}
+
 // sampler_integrator::render's per-sample set-up (sampler_integrator.cpp:102-126) for
 // every work item of the wave; all of them enter the active queue.
+// Batch: item -> (scene, sample, pixel) through the scene records, and the
+// path remembers its scene.
+template <bool BATCH>
 __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_out) {
 	const wave_params& p = *w.params;
 	const uint64_t pixels = static_cast<uint64_t>(p.width) * p.height;
@@ -330,10 +411,22 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 		const uint64_t item = p.first_item + i;
 		const bool valid = i < w.capacity && item < p.total_items;
 		if (valid) {
-			const uint32_t pixel = static_cast<uint32_t>(item % pixels);
-			const uint32_t sample = p.first_sample + static_cast<uint32_t>(item / pixels);
 			path_state st;
-			path_begin(st, p.r2c, p.c2w, p.lens, p.focus, pixel % p.width, pixel / p.width, pixel, sample, p.seed);
+			uint32_t pixel, sample;
+			if (BATCH) {
+				const uint32_t k = batch_scene_of_item(w, item);
+				const batch_scene& b = w.batch[k];
+				const uint64_t local = item - b.item_base;
+				const uint64_t px = static_cast<uint64_t>(b.width) * b.height;
+				pixel = static_cast<uint32_t>(local % px);
+				sample = b.first_sample + static_cast<uint32_t>(local / px);
+				path_begin(st, b.r2c, b.c2w, b.lens, b.focus, pixel % b.width, pixel / b.width, pixel, sample, b.seed);
+				w.scene[i] = k;
+			} else {
+				pixel = static_cast<uint32_t>(item % pixels);
+				sample = p.first_sample + static_cast<uint32_t>(item / pixels);
+				path_begin(st, p.r2c, p.c2w, p.lens, p.focus, pixel % p.width, pixel / p.width, pixel, sample, p.seed);
+			}
 			w.pixel[i] = pixel;
 			w.sample[i] = sample;
 			w.result[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -344,8 +437,9 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 	}
 }
 
-template <bool COUNT, bool VOL>
-__global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap) {
+template <bool COUNT, bool VOL, bool BATCH>
+__global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
+	uint32_t sort) {
 	extern __shared__ uint32_t smem[];
 	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_ACTIVE];
@@ -359,12 +453,20 @@ __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, ui
 			const float4 o = w.ray_o[i], d = w.ray_d[i];
 			float len = o.w;
 			hit_t h;
-			if (!trace_one<false, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris)) {
+			bool ok;
+			if (BATCH) {
+				const scene_view sv = batch_view(s, w.batch[w.scene[i]]);
+				ok = trace_one<false, COUNT>(sv, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+			} else {
+				ok = trace_one<false, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+			}
+			if (!ok) {
 				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
 				h.slot = -1;
 			}
 			w.hit[i] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
 			key = (VOL && w.medium[i] >= 0) ? static_cast<uint32_t>(CLASS_MEDIUM) : shade_class(s, h.slot);
+			if (sort == RB_SORT_NONE && key != CLASS_MISS && key != CLASS_MEDIUM) key = CLASS_OTHER;
 		}
 		warp_push_keyed(key, i, w.class_queue, w.capacity, w.counters + CNT_CLASS);
 	}
@@ -374,8 +476,8 @@ __global__ void __launch_bounds__(128) k_extend(scene_view s, wave_buffers w, ui
 	}
 }
 
-template <uint32_t CLASS, bool VOL>
-__global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
+template <uint32_t CLASS, bool VOL, bool BATCH>
+__global__ void __launch_bounds__(256) k_shade_a(scene_view s_all, wave_buffers w) {
 	const wave_params& p = *w.params;
 	const uint32_t n = w.counters[CNT_CLASS + CLASS];
 	const uint32_t* q = w.class_queue + CLASS * w.capacity;
@@ -385,7 +487,8 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 		uint32_t i = 0;
 		if (k < n) {
 			i = q[k];
-			path_state st = load_path(w, p, i);
+			path_state st = load_path<BATCH>(w, p, i);
+			const scene_view s = BATCH ? batch_view(s_all, w.batch[w.scene[i]]) : s_all;
 			if (CLASS == CLASS_MISS) {
 				shade_miss(s, st);
 				finish(w, i, st.L);
@@ -435,8 +538,8 @@ __global__ void __launch_bounds__(128) k_shade_a(scene_view s, wave_buffers w) {
 	}
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(128) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap) {
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
 	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_SECONDARY];
@@ -448,7 +551,14 @@ __global__ void __launch_bounds__(128) k_trace_secondary(scene_view s, wave_buff
 			const float4 o = w.sec_o[j], d = w.sec_d[j];
 			float len = o.w;
 			hit_t h;
-			if (!trace_one<true, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris)) {
+			bool ok;
+			if (BATCH) {
+				const scene_view sv = batch_view(s, w.batch[w.scene[j >> 1]]);
+				ok = trace_one<true, COUNT>(sv, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+			} else {
+				ok = trace_one<true, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+			}
+			if (!ok) {
 				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
 				h.slot = -1;
 			}
@@ -461,8 +571,8 @@ __global__ void __launch_bounds__(128) k_trace_secondary(scene_view s, wave_buff
 	}
 }
 
-template <uint32_t CLASS>
-__global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, uint32_t queue_in) {
+template <uint32_t CLASS, bool BATCH>
+__global__ void __launch_bounds__(256) k_shade_b(scene_view s_all, wave_buffers w, uint32_t queue_in) {
 	const wave_params& p = *w.params;
 	const uint32_t n = w.counters[CNT_CLASS + CLASS];
 	const uint32_t* q = w.class_queue + CLASS * w.capacity;
@@ -473,12 +583,13 @@ __global__ void __launch_bounds__(128) k_shade_b(scene_view s, wave_buffers w, u
 		uint32_t i = 0;
 		if (k < n) {
 			i = q[k];
-			path_state st = load_path(w, p, i);
+			path_state st = load_path<BATCH>(w, p, i);
 			if (!(st.flags & 0x80000000u)) {
+				const scene_view s = BATCH ? batch_view(s_all, w.batch[w.scene[i]]) : s_all;
 				const shade_record& rec = w.rec[i];
 				const hit_t sh = to_hit(w.sec_hit[2 * i]);
 				const hit_t mh = to_hit(w.sec_hit[2 * i + 1]);
-				if (p.guide_flags != 0u)
+				if (!BATCH && p.guide_flags != 0u)
 					alive = CLASS == CLASS_OTHER ? shade_b_guided_any(s, w, p, i, st, rec, sh, mh)
 						: shade_b_guided<class_material(CLASS)>(s, w, p, i, st, rec, sh, mh);
 				else
@@ -554,7 +665,7 @@ __device__ void medium_vertex_a(const scene_view& s, path_state& p, shade_record
 
 // Paths inside a medium: homogeneous_medium::sample over the segment to the
 // closest hit (or to infinity on a miss), then a medium vertex or the surface.
-__global__ void __launch_bounds__(128) k_shade_a_medium(scene_view s, wave_buffers w) {
+__global__ void __launch_bounds__(256) k_shade_a_medium(scene_view s, wave_buffers w) {
 	const wave_params& p = *w.params;
 	const uint32_t n = w.counters[CNT_CLASS + CLASS_MEDIUM];
 	const uint32_t* q = w.class_queue + CLASS_MEDIUM * w.capacity;
@@ -619,7 +730,7 @@ __global__ void __launch_bounds__(128) k_shade_a_medium(scene_view s, wave_buffe
 // the emitter or environment found by the MIS sample (with find_emitter's
 // environment pick, :49-82), and the point each connection ends at. Scenes
 // without media skip the transmittance walks.
-__global__ void __launch_bounds__(128) k_vol_direct(scene_view s, wave_buffers w, uint32_t queue_in) {
+__global__ void __launch_bounds__(256) k_vol_direct(scene_view s, wave_buffers w, uint32_t queue_in) {
 	const wave_params& p = *w.params;
 	const uint32_t n = w.counters[CNT_ACTIVE];
 	const uint32_t* q = w.queue[queue_in];
@@ -693,7 +804,7 @@ __global__ void __launch_bounds__(128) k_vol_direct(scene_view s, wave_buffers w
 // with media switches the medium, a visible one blocks the connection.
 constexpr uint32_t kMaxBeamSegments = 256;
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_beam(scene_view s, wave_buffers w, uint32_t stack_cap) {
+__global__ void __launch_bounds__(256) k_beam(scene_view s, wave_buffers w, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
 	smem_stack stk = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_BEAM];
@@ -795,7 +906,7 @@ __device__ bool vol_continue(const scene_view& s, const wave_buffers& w, const w
 	return roulette(st, p.max_depth, p.rr_threshold);
 }
 
-__global__ void __launch_bounds__(128) k_vol_continue(scene_view s, wave_buffers w, uint32_t queue_in) {
+__global__ void __launch_bounds__(256) k_vol_continue(scene_view s, wave_buffers w, uint32_t queue_in) {
 	const wave_params& p = *w.params;
 	const uint32_t n = w.counters[CNT_ACTIVE];
 	const uint32_t* q = w.queue[queue_in];
@@ -819,18 +930,30 @@ __global__ void __launch_bounds__(128) k_vol_continue(scene_view s, wave_buffers
 
 __global__ void k_advance(uint32_t* counters);
 
+// Traversal kernels keep their stacks in dynamic shared memory; above 48 KB a
+// block needs the kernel's opt-in.
+template <typename Kernel>
+cudaError_t allow_smem(Kernel kernel, size_t bytes) {
+	if (bytes <= 48u * 1024u) return cudaSuccess;
+	return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
 template <bool COUNT>
 cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t queue_in, const launch_cfg& cfg,
 	cudaStream_t stream) {
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
-	k_extend<COUNT, true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
-	k_shade_a<CLASS_LAMBERT, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_METAL, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_GLASS_ROUGH, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_OTHER, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_MISS, true><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	cudaError_t e = allow_smem(k_extend<COUNT, true, false>, smem);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, false>, smem);
+	if (e == cudaSuccess) e = allow_smem(k_beam<COUNT>, smem);
+	if (e != cudaSuccess) return e;
+	k_extend<COUNT, true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	k_shade_a<CLASS_LAMBERT, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_METAL, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_GLASS_ROUGH, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_OTHER, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_MISS, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a_medium<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_direct<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_beam<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_continue<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -853,32 +976,39 @@ __global__ void k_advance(uint32_t* counters) {
 // the following work items.
 __global__ void k_next_wave(wave_params* p, uint32_t capacity) { p->first_item += capacity; }
 
-template <bool COUNT>
+template <bool COUNT, bool BATCH>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
-	if (cfg.volume) return volume_bounce<COUNT>(s, w, queue_in, cfg, stream);
+	if (!BATCH && cfg.volume) return volume_bounce<COUNT>(s, w, queue_in, cfg, stream);
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	cudaError_t e = allow_smem(k_extend<COUNT, false, BATCH>, smem);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, BATCH>, smem);
+	if (e != cudaSuccess) return e;
 	const bool timed = cfg.events != nullptr && *cfg.next_event + 2 <= cfg.max_events;
 	uint32_t ev = timed ? *cfg.next_event : 0u;
 	if (timed) { cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 0; }
-	k_extend<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	k_extend<COUNT, false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
-	k_shade_a<CLASS_LAMBERT, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_METAL, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_GLASS_ROUGH, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_OTHER, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	k_shade_a<CLASS_MISS, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
-	if (cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
-		const cudaError_t e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
+	if (cfg.sort == RB_SORT_MATERIAL) {
+		k_shade_a<CLASS_LAMBERT, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+		k_shade_a<CLASS_METAL, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+		k_shade_a<CLASS_GLASS_ROUGH, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	}
+	k_shade_a<CLASS_OTHER, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	k_shade_a<CLASS_MISS, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	if (!BATCH && cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
+		e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
 		if (e != cudaSuccess) return e;
 	}
 	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
-	k_trace_secondary<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
-	k_shade_b<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
-	k_shade_b<CLASS_METAL><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
-	k_shade_b<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
-	k_shade_b<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	if (cfg.sort == RB_SORT_MATERIAL) {
+		k_shade_b<CLASS_LAMBERT, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+		k_shade_b<CLASS_METAL, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+		k_shade_b<CLASS_GLASS_ROUGH, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	}
+	k_shade_b<CLASS_OTHER, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_advance<<<1, 1, 0, stream>>>(w.counters);
 	return cudaGetLastError();
 }
@@ -891,6 +1021,11 @@ cudaError_t launch_trace_rays(const scene_view& s, const uint32_t* prim_entity, 
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	const uint32_t blocks_needed = (n + cfg.block_trace - 1) / cfg.block_trace;
 	const int grid = static_cast<int>(blocks_needed < static_cast<uint32_t>(cfg.grid_trace) ? blocks_needed : cfg.grid_trace);
+	cudaError_t e = allow_smem(k_trace_rays<true, true>, smem);
+	if (e == cudaSuccess) e = allow_smem(k_trace_rays<true, false>, smem);
+	if (e == cudaSuccess) e = allow_smem(k_trace_rays<false, true>, smem);
+	if (e == cudaSuccess) e = allow_smem(k_trace_rays<false, false>, smem);
+	if (e != cudaSuccess) return e;
 	if (shadow) {
 		if (cfg.count) k_trace_rays<true, true><<<grid, cfg.block_trace, smem, stream>>>(s, prim_entity, rays, n, hits, cfg.stack_depth, counters);
 		else k_trace_rays<true, false><<<grid, cfg.block_trace, smem, stream>>>(s, prim_entity, rays, n, hits, cfg.stack_depth, counters);
@@ -903,12 +1038,15 @@ cudaError_t launch_trace_rays(const scene_view& s, const uint32_t* prim_entity, 
 
 cudaError_t launch_bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
-	return cfg.count ? bounce<true>(s, w, f, queue_in, cfg, stream) : bounce<false>(s, w, f, queue_in, cfg, stream);
+	if (cfg.batch)
+		return cfg.count ? bounce<true, true>(s, w, f, queue_in, cfg, stream) : bounce<false, true>(s, w, f, queue_in, cfg, stream);
+	return cfg.count ? bounce<true, false>(s, w, f, queue_in, cfg, stream) : bounce<false, false>(s, w, f, queue_in, cfg, stream);
 }
 
 cudaError_t launch_wave(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t max_depth,
 	uint32_t first_queue, const launch_cfg& cfg, cudaStream_t stream) {
-	k_camera<<<cfg.grid_shade, 256, 0, stream>>>(w, first_queue);
+	if (cfg.batch) k_camera<true><<<cfg.grid_shade, 256, 0, stream>>>(w, first_queue);
+	else k_camera<false><<<cfg.grid_shade, 256, 0, stream>>>(w, first_queue);
 	cudaError_t err = cudaGetLastError();
 	uint32_t qi = first_queue;
 	for (uint32_t b = 0; b < max_depth && err == cudaSuccess; b++) {
@@ -919,8 +1057,15 @@ cudaError_t launch_wave(const scene_view& s, const wave_buffers& w, const film_b
 }
 
 cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream) {
-	k_film_resolve<<<grid, 256, 0, stream>>>(w, f);
+	if (w.batch != nullptr) k_film_resolve_batch<<<grid, 256, 0, stream>>>(w, f);
+	else k_film_resolve<<<grid, 256, 0, stream>>>(w, f);
 	k_next_wave<<<1, 1, 0, stream>>>(w.params, w.capacity);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_film_mean(const film_buffers& f, uint32_t pixels, float* rgb, int grid, cudaStream_t stream) {
+	if (pixels == 0) return cudaSuccess;
+	k_film_mean<<<grid, 256, 0, stream>>>(f, pixels, rgb);
 	return cudaGetLastError();
 }
 
@@ -939,6 +1084,7 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
 	if (cfg.volume) return 3u + 12u * max_depth;
+	if (cfg.sort == RB_SORT_NONE && cfg.guide == nullptr) return 3u + 7u * max_depth;
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
 	uint32_t n = 3u + (12u + (sample ? 1u : 0u)) * max_depth;

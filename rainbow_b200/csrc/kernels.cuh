@@ -55,6 +55,44 @@ enum : uint32_t {
 	GUIDE_TRAIN = 2u         // record vertices for training
 };
 
+// One scene of a batched render (rb_batch_render): where its records sit in
+// the merged scene arrays, and its view for this render call. Item k of the
+// batch belongs to the scene with item_base <= k < the next scene's item_base;
+// within it, local item j is sample first_sample + j / pixels of pixel j % pixels.
+struct batch_scene {
+	float4 root_a, root_b;   // the scene's root box (scene_view::root_a / root_b)
+	uint32_t root_ref;       // its root in the wide-node array
+	uint32_t root_node;      // its root in the reference-layout node array
+	uint32_t emitter_base, num_emitters;
+	uint32_t env_base, num_environments;
+	uint32_t pixel_base;     // first film pixel of the scene in the merged film
+	uint32_t spp;
+	uint64_t item_base;      // first work item of the scene in this render call
+	pt::env_distribution env;
+	float r2c[16];
+	float c2w[16];
+	float lens, focus;
+	uint32_t width, height;
+	uint32_t first_sample;
+	uint32_t seed;
+};
+
+// The scene_view of one scene of a batch: the merged arrays with the scene's
+// root, emitter list and environments.
+RB_HD pt::scene_view batch_view(const pt::scene_view& merged, const batch_scene& b) {
+	pt::scene_view v = merged;
+	v.root_a = b.root_a;
+	v.root_b = b.root_b;
+	v.root_ref = b.root_ref;
+	v.root_node = b.root_node;
+	v.emitters = merged.emitters + b.emitter_base;
+	v.num_emitters = b.num_emitters;
+	v.environments = merged.environments + b.env_base;
+	v.num_environments = b.num_environments;
+	v.env = b.env;
+	return v;
+}
+
 // Path state of one wave, structure of arrays over `capacity` paths.
 struct wave_buffers {
 	uint32_t capacity;
@@ -83,6 +121,10 @@ struct wave_buffers {
 	pt::vol_rec* vrec;       // light-connection factors of the current vertex
 	float4* beam;            // 2 per path: transmittance of the NEE and MIS connections
 	uint32_t* beam_queue;    // connections (2 i, 2 i + 1) waiting for their transmittance
+	// batched rendering (null unless a batch render allocated them)
+	uint32_t* scene;         // scene of each path
+	const batch_scene* batch;  // num_scenes records
+	uint32_t num_scenes;
 };
 
 struct film_buffers {
@@ -107,6 +149,8 @@ struct launch_cfg {
 	const guide::guide_state* guide = nullptr;
 	uint32_t guide_mode = 0;
 	bool volume = false;     // volume_path_integrator instead of path_integrator
+	bool batch = false;      // many scenes per wave (wave_buffers::batch)
+	uint32_t sort = 0;       // hit queues: 0 one per material class, 1 a single queue (no sorting)
 };
 
 // Ray batches for rb_trace_closest / rb_trace_shadow.
@@ -121,6 +165,9 @@ cudaError_t launch_wave(const pt::scene_view& s, const wave_buffers& w, const fi
 // Adds the wave's finished samples to the film, then advances
 // params->first_item by the wave capacity (the last nodes of a wave).
 cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream);
+
+// Per-pixel means of the film into `rgb` (3 floats per pixel, device memory).
+cudaError_t launch_film_mean(const film_buffers& f, uint32_t pixels, float* rgb, int grid, cudaStream_t stream);
 
 // Wave end with learned guiding: training-sample collection, film resolve,
 // next-wave advance, then the training steps (cfg.guide_mode & GUIDE_TRAIN).

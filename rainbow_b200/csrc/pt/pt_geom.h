@@ -131,7 +131,7 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 	uint32_t cur_entity = 0xffffffffu;
 	local_ray lr{};
 	stack.reset();
-	stack.push(0u);
+	stack.push(s.root_node);
 	while (!stack.empty()) {
 		const uint32_t n = stack.pop();
 		const float4 a = RB_LDG(s.nodes + 2 * n);
@@ -173,10 +173,11 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 	return true;
 }
 
-// ------------------------------------------------------------------ closest hit, child-box traversal
-// The same visiting decisions as closest_hit above, with each interior node
-// holding both children's boxes (wide_node) so a node is expanded with one
-// 64-byte load instead of one dependent load per popped child.
+// ------------------------------------------------------------------ closest hit, 4-wide traversal
+// The same visiting decisions as closest_hit above, over the 4-wide collapse
+// of the same tree (node4): expanding binary node N tests the boxes of its
+// grandchildren directly (a child that is a leaf is tested itself), with one
+// 128-byte node load instead of three dependent levels of pops.
 //
 // Why the decisions are identical. The reference pushes both children (far,
 // then near), pops a node and slab-tests it against the ray length at pop time.
@@ -184,16 +185,24 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 // depend on the length) and tx the minimum of the far distances; with a
 // length that is not NaN the box passes iff te <= min(len, tx), and the early
 // exits after each axis do not change the outcome because t0 only grows and t1
-// only shrinks. Here both children are tested when their parent is expanded:
-//  - the near child is popped next by the reference with the length unchanged,
-//    so descending into it directly when it passes reproduces its pop test;
-//  - a child that fails now also fails at its later pop (the length only shrinks);
-//  - a far child that passes is pushed with te; passing now implied te <= tx,
-//    so at its pop the reference's test reduces to te <= len, checked as
-//    !(te > len).
-// Box tests are counted as the reference performs them: the root, then two per
-// expanded interior node. A NaN length (only reachable through a degenerate
-// triangle hit) returns -1 so the caller can redo the ray on the exact path.
+// only shrinks. Float subtraction and multiplication are monotonic and a
+// parent's box contains its children's, so a child that passes implies that its
+// parent passes at the same length (te_parent <= te_child, tx_parent >= tx_child).
+// Hence, at the length of N's expansion:
+//  - the near child X of N is expanded by the reference at once, at the same
+//    length: its children pass there iff they pass now, and they can be tested
+//    without testing X (a passing child implies X passes);
+//  - every other slot that fails now also fails when the reference reaches it
+//    (the length only shrinks);
+//  - a slot that passes now is pushed with te; when the reference reaches it
+//    (popping it, or popping and expanding its parent first) its test, and its
+//    parent's, reduce to te <= len, checked as !(te > len) at the pop.
+// Slots are visited in the reference's order: the pair of N's near child
+// first, each pair near child first (near = the right one when the ray's
+// direction is negative on the split axis). Box tests are not counted here;
+// counting passes use closest_hit. A NaN length (only reachable through a
+// degenerate triangle hit) or a full stack returns -1 so the caller can redo
+// the ray on the reference-order path.
 RB_HD bool slab_pass(float ax, float ay, float az, float bx, float by, float bz, vec3 o, vec3 inv, float len, float& te) {
 	float t0 = 0.f, t1 = len;
 	float n = (ax - o.x) * inv.x, f = (bx - o.x) * inv.x;
@@ -209,16 +218,18 @@ RB_HD bool slab_pass(float ax, float ay, float az, float bx, float by, float bz,
 	return !(t0 > t1);
 }
 
-template <bool SHADOW, bool COUNT, typename Stack>
-RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack, trace_counters& cnt) {
+template <typename T>
+RB_HD T pick4(T a, T b, T c, T d, uint32_t i) { return i == 0 ? a : i == 1 ? b : i == 2 ? c : d; }
+
+template <bool SHADOW, typename Stack>
+RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack) {
 	const vec3 inv = 1.f / d;
-	const bool neg[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+	const uint32_t neg = (inv.x < 0.f ? 1u : 0u) | (inv.y < 0.f ? 2u : 0u) | (inv.z < 0.f ? 4u : 0u);
 	hit.slot = -1;
 	uint32_t cur_entity = 0xffffffffu;
 	local_ray lr{};
 	stack.reset();
 	float te;
-	if (COUNT) cnt.nodes++;
 	if (!slab_pass(s.root_a.x, s.root_a.y, s.root_a.z, s.root_a.w, s.root_b.x, s.root_b.y, o, inv, len, te)) return 1;
 	uint32_t cur = s.root_ref;
 	for (;;) {
@@ -236,7 +247,6 @@ RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_
 					cur_entity = ent;
 					lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
 				}
-				if (COUNT) cnt.tris++;
 				float t, b1, b2;
 				if (triangle_hit(lr.o, lr.d, len * lr.to_local, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y},
 						vec3{tb.z, tb.w, tc.x}, t, b1, b2)) {
@@ -248,32 +258,44 @@ RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_
 				}
 			}
 		} else {
-			const wide_node* nd = s.wnodes + cur;
-			const float4 a = RB_LDG(&nd->a), b = RB_LDG(&nd->b), c = RB_LDG(&nd->c);
-			const uint4 m = RB_LDG(&nd->d);
-			float te0, te1;
-			if (COUNT) cnt.nodes += 2;
-			const bool p0 = slab_pass(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, len, te0);
-			const bool p1 = slab_pass(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, len, te1);
-			// the reference visits the right child first when the ray is negative on the split axis
-			const bool right_first = neg[m.z];
-			const uint32_t r_first = right_first ? m.y : m.x, r_second = right_first ? m.x : m.y;
-			const bool p_first = right_first ? p1 : p0, p_second = right_first ? p0 : p1;
-			const float te_second = right_first ? te0 : te1;
-			if (p_first) {
-				if (p_second) {
-					if (stack.full()) return 0;
-					stack.push(r_second, te_second);
+			const node4* nd = s.wnodes + cur;
+			const float4 lx = RB_LDG(&nd->lo_x), ly = RB_LDG(&nd->lo_y), lz = RB_LDG(&nd->lo_z);
+			const float4 hx = RB_LDG(&nd->hi_x), hy = RB_LDG(&nd->hi_y), hz = RB_LDG(&nd->hi_z);
+			const uint4 rf = RB_LDG(&nd->ref);
+			const uint32_t meta = RB_LDG(&nd->meta.x);
+			float t0, t1, t2, t3;
+			uint32_t pass = 0;
+			if ((meta & 0x100u) && slab_pass(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, len, t0)) pass |= 1u;
+			if ((meta & 0x200u) && slab_pass(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, len, t1)) pass |= 2u;
+			if ((meta & 0x400u) && slab_pass(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, len, t2)) pass |= 4u;
+			if ((meta & 0x800u) && slab_pass(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, len, t3)) pass |= 8u;
+			if (pass != 0u) {
+				// the reference's order: near pair first, near slot first within each pair
+				const uint32_t pf = (neg >> (meta & 3u)) & 1u;
+				const uint32_t ax_first = (meta >> (2u + 2u * pf)) & 3u, ax_second = (meta >> (2u + 2u * (pf ^ 1u))) & 3u;
+				const uint32_t o0 = 2u * pf + ((neg >> ax_first) & 1u);
+				const uint32_t o2 = 2u * (pf ^ 1u) + ((neg >> ax_second) & 1u);
+				const uint32_t order = o0 | ((o0 ^ 1u) << 2) | (o2 << 4) | ((o2 ^ 1u) << 6);
+				// walk the order backwards: every passing slot but the first is pushed,
+				// later ones first, so they pop in order
+				uint32_t next = 0xffffffffu;
+				float next_te = 0.f;
+#pragma unroll
+				for (int k = 3; k >= 0; k--) {
+					const uint32_t sl = (order >> (2 * k)) & 3u;
+					if (!((pass >> sl) & 1u)) continue;
+					if (next != 0xffffffffu) {
+						if (stack.full()) return -1;
+						stack.push(next, next_te);
+					}
+					next = pick4(rf.x, rf.y, rf.z, rf.w, sl);
+					next_te = pick4(t0, t1, t2, t3, sl);
 				}
-				cur = r_first;
-				continue;
-			}
-			if (p_second) {
-				cur = r_second;
+				cur = next;
 				continue;
 			}
 		}
-		// pop the next far child whose box still passes at the current length
+		// pop the next slot whose box still passes at the current length
 		bool found = false;
 		while (!stack.empty()) {
 			uint32_t ref;

@@ -150,24 +150,28 @@ struct env_distribution {
 	float integral_marg;
 };
 
-// Interior node of the traversal tree with both children's boxes (64 bytes).
-// Child reference: interior -> its index in this array; leaf ->
+// Interior node of the 4-wide traversal tree (128 bytes): binary node N of the
+// reference's tree with its grandchildren as slots [L0, L1, R0, R1] (L, R: N's
+// left and right child; X0, X1: X's left and right child). A child that is a
+// leaf takes its pair's first slot itself and leaves the second one empty.
+// Boxes are stored per coordinate, one float4 across the four slots.
+// Slot reference: interior -> its index in this array; leaf ->
 // kRefLeaf | count << 24 | first prim slot (count 1..127, slot < 2^24).
-struct wide_node {
-	float4 a;  // c0.min.xyz, c0.max.x
-	float4 b;  // c0.max.yz, c1.min.xy
-	float4 c;  // c1.min.z, c1.max.xyz
-	uint4 d;   // ref0 (left), ref1 (right), split axis, unused
+struct node4 {
+	float4 lo_x, lo_y, lo_z;
+	float4 hi_x, hi_y, hi_z;
+	uint4 ref;
+	uint4 meta;  // x: split axis of N (bits 0-1), of L (bits 2-3), of R (bits 4-5); valid slots (bits 8-11)
 };
 constexpr uint32_t kRefLeaf = 0x80000000u;
 
 // Flat view of an uploaded scene; pointers are device pointers in kernels and
 // host pointers in host-side use.
 struct scene_view {
-	const wide_node* wnodes;      // interior nodes with child boxes (fast traversal); null: exact path only
+	const node4* wnodes;          // 4-wide nodes (fast traversal); null: the reference-order traversal only
 	float4 root_a, root_b;        // root box, (min.xyz, max.x), (max.y, max.z, -, -)
 	uint32_t root_ref;
-	uint32_t pad0;
+	uint32_t root_node;           // index of the root in `nodes` (non-zero for a scene of a merged batch)
 	const float4* nodes;          // 2 per node: (min.xyz, max.x), (max.y, max.z, w0, w1)
 	const float4* tri_a;          // per prim slot: (p0.xyz, e1.x)        entity-local space
 	const float4* tri_b;          // (e1.y, e1.z, e2.x, e2.y)

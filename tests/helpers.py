@@ -58,3 +58,75 @@ def assert_hits_equal(got, want, what=""):
     assert np.array_equal(got["triangle"], want["triangle"]), f"{what}: triangle ids differ"
     bad = got["t"].view(np.uint32) != want["t"].view(np.uint32)
     assert not bad.any(), f"{what}: {bad.sum()} hit distances differ in their bits"
+
+
+class HostBatch:
+    """Several scenes merged as rb_batch_upload merges them, on the host build of the stages."""
+
+    def __init__(self, scenes):
+        L = C.CDLL(HOSTPATHS)
+        L.hp_batch_create.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]
+        L.hp_batch_free.argtypes = [C.c_void_p]
+        L.hp_batch_trace.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+        L.hp_batch_samples.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                       C.c_uint32, C.c_float, C.c_uint32, C.c_void_p]
+        self.L, self.scenes = L, list(scenes)
+        arr = (rb.SceneDesc * len(self.scenes))()
+        for k, sc in enumerate(self.scenes):
+            arr[k] = sc.desc
+        self.h = C.c_void_p()
+        assert L.hp_batch_create(arr, len(self.scenes), C.byref(self.h)) == 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.hp_batch_free(self.h)
+            self.h = None
+
+    def trace(self, scene, rays, shadow=False):
+        rays = np.ascontiguousarray(rays, dtype=rb.RAY_DTYPE)
+        hits = np.zeros(rays.shape[0], dtype=rb.HIT_DTYPE)
+        assert self.L.hp_batch_trace(self.h, scene, rays.ctypes.data, rays.shape[0], int(shadow), hits.ctypes.data) == 0
+        return hits
+
+    def samples(self, scene, camera, pixels, samples, max_depth, rr=1.0, seed=0):
+        px = np.ascontiguousarray(pixels, dtype=np.uint32)
+        sm = np.ascontiguousarray(samples, dtype=np.uint32)
+        out = np.zeros((px.shape[0], 3), dtype=np.float32)
+        assert self.L.hp_batch_samples(self.h, scene, C.byref(camera), px.ctypes.data, sm.ctypes.data, px.shape[0],
+                                       max_depth, rr, seed, out.ctypes.data) == 0
+        return out
+
+
+def random_rays(scene, n, seed):
+    """Rays toward random surface points of the scene: half from the camera eye,
+    half from other surface points (as bounce rays leave surfaces); length +inf."""
+    rng = np.random.default_rng(seed)
+    d = scene.desc
+    pts = []
+    for e in range(d.num_entities):
+        ent = d.entities[e]
+        if ent.mesh < 0:
+            continue
+        md = d.meshes[ent.mesh]
+        P = np.ctypeslib.as_array(md.positions, (md.num_vertices * 3,)).reshape(-1, 3).astype(np.float64)
+        I = np.ctypeslib.as_array(md.indices, (md.num_triangles * 3,)).reshape(-1, 3)
+        t = rng.integers(0, md.num_triangles, 64)
+        u, v = rng.random(64), rng.random(64)
+        flip = u + v > 1
+        u[flip], v[flip] = 1 - u[flip], 1 - v[flip]
+        local = P[I[t, 0]] * (1 - u - v)[:, None] + P[I[t, 1]] * u[:, None] + P[I[t, 2]] * v[:, None]
+        M = np.array(ent.local_to_world[:], dtype=np.float64).reshape(4, 4).T  # column-major storage
+        pts.append(local @ M[:3, :3].T + M[:3, 3])
+    pts = np.concatenate(pts)
+    targets = pts[rng.integers(0, len(pts), n)]
+    eye = np.array(scene.camera.eye[:], dtype=np.float64)
+    origins = np.repeat(eye[None], n, axis=0)
+    half = n // 2
+    origins[half:] = pts[rng.integers(0, len(pts), n - half)] + rng.normal(scale=1e-2, size=(n - half, 3))
+    dirs = targets - origins
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    rays = np.zeros(n, dtype=rb.RAY_DTYPE)
+    rays["origin"] = origins.astype(np.float32)
+    rays["direction"] = dirs.astype(np.float32)
+    rays["length"] = np.inf
+    return rays

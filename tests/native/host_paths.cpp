@@ -8,10 +8,12 @@
 // librbgpu.so has no CPU path.
 #include "../../include/rbgpu.h"
 #include "../../rainbow_b200/csrc/host/scene_pack.h"
+#include "../../rainbow_b200/csrc/kernels.cuh"
 #include "../../rainbow_b200/csrc/pt/pt_path.h"
 
 #include <cmath>
 #include <new>
+#include <vector>
 
 using namespace rb;
 using namespace rb::pt;
@@ -46,7 +48,7 @@ hit_t trace(const scene_view& v, vec3 o, vec3 d, float& len, bool shadow) {
 	hit_t h;
 	if (g_mode == 0 && v.wnodes != nullptr && !std::isnan(len)) {
 		const float len0 = len;
-		const int r = shadow ? closest_hit_fast<true, false>(v, o, d, len, h, st, c) : closest_hit_fast<false, false>(v, o, d, len, h, st, c);
+		const int r = shadow ? closest_hit_fast<true>(v, o, d, len, h, st) : closest_hit_fast<false>(v, o, d, len, h, st);
 		if (r >= 0) return h;
 		len = len0;
 	}
@@ -76,26 +78,29 @@ int hp_create(const rb_scene_desc* desc, void** out) {
 
 void hp_free(void* s) { delete static_cast<hp_scene*>(s); }
 
-int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {
-	const hp_scene& s = *static_cast<hp_scene*>(hs);
+} // extern "C"
+
+namespace {
+
+// entity_base: subtracted from reported entity ordinals (a scene of a merged batch).
+void trace_batch(const host::packed_scene& packed, const scene_view& view, uint32_t entity_base, const rb_ray* rays,
+	uint32_t n, int shadow, rb_hit* hits) {
 	for (uint32_t i = 0; i < n; i++) {
 		float len = rays[i].length;
-		const hit_t h = trace(s.view, vec3{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]},
+		const hit_t h = trace(view, vec3{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]},
 			vec3{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]}, len, shadow != 0);
-		hits[i].entity = h.slot >= 0 ? static_cast<int32_t>(s.packed.prim_entity[h.slot]) : -1;
-		hits[i].triangle = h.slot >= 0 ? static_cast<int32_t>(s.packed.prim_index[h.slot]) : -1;
+		hits[i].entity = h.slot >= 0 ? static_cast<int32_t>(packed.prim_entity[h.slot] - entity_base) : -1;
+		hits[i].triangle = h.slot >= 0 ? static_cast<int32_t>(packed.prim_index[h.slot]) : -1;
 		hits[i].t = len;
 		hits[i].b1 = h.slot >= 0 ? h.b1 : 0.f;
 		hits[i].b2 = h.slot >= 0 ? h.b2 : 0.f;
 	}
-	return RB_OK;
 }
 
 // Radiance of (pixel, sample) pairs through the same stage sequence the
 // kernels run: camera, then per bounce extend -> shade_a -> secondary rays -> shade_b.
-int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples, uint32_t n,
-	uint32_t max_depth, float rr, uint32_t seed, float* out) {
-	const hp_scene& s = *static_cast<hp_scene*>(hs);
+void samples_view(const scene_view& view, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples,
+	uint32_t n, uint32_t max_depth, float rr, uint32_t seed, float* out) {
 	for (uint32_t i = 0; i < n; i++) {
 		const uint32_t pixel = pixels[i];
 		const uint32_t x = pixel % static_cast<uint32_t>(cam->width), y = pixel / static_cast<uint32_t>(cam->width);
@@ -104,24 +109,96 @@ int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, cons
 			samples[i], seed);
 		for (int guard = 0; guard < 4096; guard++) {
 			float len = p.len;
-			const hit_t h = trace(s.view, p.o, p.d, len, false);
+			const hit_t h = trace(view, p.o, p.d, len, false);
 			shade_record rec;
-			if (!shade_a_any(s.view, p, h, rec)) break;
+			if (!shade_a_any(view, p, h, rec)) break;
 			hit_t sh{-1, 0.f, 0.f}, mh{-1, 0.f, 0.f};
 			if (rec.nee_entity >= 0) {
 				float l = rec.shadow_ray.len;
-				sh = trace(s.view, rec.shadow_ray.o, rec.shadow_ray.d, l, true);
+				sh = trace(view, rec.shadow_ray.o, rec.shadow_ray.d, l, true);
 			}
 			if (rec.mis_valid) {
 				float l = rec.mis_ray.len;
-				mh = trace(s.view, rec.mis_ray.o, rec.mis_ray.d, l, true);
+				mh = trace(view, rec.mis_ray.o, rec.mis_ray.d, l, true);
 			}
-			if (!shade_b_any(s.view, p, rec, sh, mh, max_depth, rr)) break;
+			if (!shade_b_any(view, p, rec, sh, mh, max_depth, rr)) break;
 		}
 		out[3 * i] = p.L.x;
 		out[3 * i + 1] = p.L.y;
 		out[3 * i + 2] = p.L.z;
 	}
+}
+
+// A merged batch (host::merge_scenes) with the per-scene views the kernels
+// build from their batch_scene records (gpu::batch_view).
+struct hp_batch {
+	host::packed_scene packed;
+	std::vector<scene_view> views;
+	std::vector<uint32_t> entity_base;
+};
+
+} // namespace
+
+extern "C" {
+
+int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {
+	const hp_scene& s = *static_cast<hp_scene*>(hs);
+	trace_batch(s.packed, s.view, 0u, rays, n, shadow, hits);
+	return RB_OK;
+}
+
+int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples, uint32_t n,
+	uint32_t max_depth, float rr, uint32_t seed, float* out) {
+	samples_view(static_cast<hp_scene*>(hs)->view, cam, pixels, samples, n, max_depth, rr, seed, out);
+	return RB_OK;
+}
+
+int hp_batch_create(const rb_scene_desc* descs, uint32_t count, void** out) {
+	auto* b = new (std::nothrow) hp_batch();
+	if (!b) return RB_ERR_OUT_OF_MEMORY;
+	std::vector<host::packed_scene> parts(count);
+	uint32_t ent = 0;
+	for (uint32_t k = 0; k < count; k++) {
+		const rb_status st = host::pack_scene(descs + k, parts[k]);
+		if (st != RB_OK) { delete b; return st; }
+		b->entity_base.push_back(ent);
+		ent += static_cast<uint32_t>(parts[k].entities.size());
+	}
+	std::vector<host::scene_place> places;
+	const rb_status st = host::merge_scenes(parts, b->packed, places);
+	if (st != RB_OK) { delete b; return st; }
+	const scene_view merged = host::host_view(b->packed);
+	for (const host::scene_place& pl : places) {
+		gpu::batch_scene r{};
+		r.root_a = pl.root_a;
+		r.root_b = pl.root_b;
+		r.root_ref = pl.root_ref;
+		r.root_node = pl.root_node;
+		r.emitter_base = pl.emitter_base;
+		r.num_emitters = pl.num_emitters;
+		r.env_base = pl.env_base;
+		r.num_environments = pl.num_environments;
+		r.env = pl.env;
+		b->views.push_back(gpu::batch_view(merged, r));
+	}
+	*out = b;
+	return RB_OK;
+}
+
+void hp_batch_free(void* b) { delete static_cast<hp_batch*>(b); }
+
+int hp_batch_trace(void* hb, uint32_t scene, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {
+	const hp_batch& b = *static_cast<hp_batch*>(hb);
+	if (scene >= b.views.size()) return RB_ERR_INVALID_ARGUMENT;
+	trace_batch(b.packed, b.views[scene], b.entity_base[scene], rays, n, shadow, hits);
+	return RB_OK;
+}
+
+int hp_batch_samples(void* hb, uint32_t scene, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples,
+	uint32_t n, uint32_t max_depth, float rr, uint32_t seed, float* out) {
+	const hp_batch& b = *static_cast<hp_batch*>(hb);
+	if (scene >= b.views.size()) return RB_ERR_INVALID_ARGUMENT;
+	samples_view(b.views[scene], cam, pixels, samples, n, max_depth, rr, seed, out);
 	return RB_OK;
 }
 
