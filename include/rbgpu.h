@@ -331,7 +331,14 @@ typedef struct rb_tuning {
 	uint32_t block_shade;       /* 32..256, a multiple of 32; 0: 128 */
 	uint32_t grid_per_sm;       /* 1..64; 0: 8 */
 	uint32_t sort;              /* RB_SORT_* */
-	uint32_t reserved[3];
+	uint32_t tail_bounce;       /* bounces run as separate wavefront stages before one kernel carries
+	                               every surviving path to its end (one thread per path, the same
+	                               stage code); 0: library default (64: none), >= max_depth: none */
+	uint32_t lanes;             /* wave lanes (1..4, 0: 1): each lane has its own path buffers, stream and
+	                               graph, so the late bounces of one wave overlap the next wave's early
+	                               ones; the film still adds the waves in order (plain and batched
+	                               renders; guided and volume renders use one lane) */
+	uint32_t reserved[1];
 } rb_tuning;
 /* Use `tuning` (NULL: defaults) for the context's later render calls. */
 rb_status rb_set_tuning(rb_context* ctx, const rb_tuning* tuning);

@@ -96,10 +96,12 @@ class RenderParams(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("paths_per_wave", C.c_uint32), ("block_trace", C.c_uint32), ("block_shade", C.c_uint32),
-                ("grid_per_sm", C.c_uint32), ("sort", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("grid_per_sm", C.c_uint32), ("sort", C.c_uint32), ("tail_bounce", C.c_uint32),
+                ("lanes", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k in ("paths_per_wave", "block_trace", "block_shade", "grid_per_sm", "sort")}
+        return {k: getattr(self, k) for k in ("paths_per_wave", "block_trace", "block_shade", "grid_per_sm", "sort",
+                                              "tail_bounce", "lanes")}
 
 
 class BatchView(C.Structure):

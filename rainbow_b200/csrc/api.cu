@@ -24,6 +24,27 @@ constexpr uint32_t kCheckpointMagic = 0x52424350u;  // "RBCP"
 namespace rb {
 namespace ctx {
 
+cudaError_t alloc_wave_buffers(gpu::wave_buffers& w, size_t n) {
+	cudaError_t e = cudaSuccess;
+	auto take = [&](auto** p, size_t count) {
+		if (e == cudaSuccess) e = dev_alloc(p, count);
+	};
+	take(&w.ray_o, n); take(&w.ray_d, n); take(&w.beta, n); take(&w.radiance, n); take(&w.bounces, n);
+	take(&w.rng, n); take(&w.pixel, n); take(&w.sample, n); take(&w.hit, n); take(&w.rec, n); take(&w.result, n);
+	take(&w.sec_o, 2 * n); take(&w.sec_d, 2 * n); take(&w.sec_hit, 2 * n); take(&w.queue[0], n); take(&w.queue[1], n);
+	take(&w.sec_queue, 2 * n);
+	take(&w.class_queue, static_cast<size_t>(pt::NUM_CLASSES) * n);
+	return e;
+}
+
+void free_wave_buffers(gpu::wave_buffers& w) {
+	dev_free(w.ray_o); dev_free(w.ray_d); dev_free(w.beta); dev_free(w.radiance); dev_free(w.bounces);
+	dev_free(w.rng); dev_free(w.pixel); dev_free(w.sample); dev_free(w.hit); dev_free(w.rec); dev_free(w.result);
+	dev_free(w.sec_o); dev_free(w.sec_d); dev_free(w.sec_hit); dev_free(w.queue[0]); dev_free(w.queue[1]);
+	dev_free(w.sec_queue);
+	dev_free(w.class_queue);
+}
+
 rb_status ensure_wave(rb_context* c, uint32_t capacity) {
 	if (c->wave_alloc >= capacity) {
 		// same buffers, smaller waves: the kernels read the wave size from wave.capacity
@@ -34,19 +55,47 @@ rb_status ensure_wave(rb_context* c, uint32_t capacity) {
 	}
 	c->release_graph();
 	c->release_wave();
+	RB_CUDA(alloc_wave_buffers(c->wave, capacity));
 	gpu::wave_buffers& w = c->wave;
-	const size_t n = capacity;
-	RB_CUDA(dev_alloc(&w.ray_o, n)); RB_CUDA(dev_alloc(&w.ray_d, n)); RB_CUDA(dev_alloc(&w.beta, n));
-	RB_CUDA(dev_alloc(&w.radiance, n)); RB_CUDA(dev_alloc(&w.bounces, n)); RB_CUDA(dev_alloc(&w.rng, n));
-	RB_CUDA(dev_alloc(&w.pixel, n)); RB_CUDA(dev_alloc(&w.sample, n)); RB_CUDA(dev_alloc(&w.hit, n));
-	RB_CUDA(dev_alloc(&w.rec, n)); RB_CUDA(dev_alloc(&w.result, n)); RB_CUDA(dev_alloc(&w.sec_o, 2 * n)); RB_CUDA(dev_alloc(&w.sec_d, 2 * n));
-	RB_CUDA(dev_alloc(&w.sec_hit, 2 * n)); RB_CUDA(dev_alloc(&w.queue[0], n)); RB_CUDA(dev_alloc(&w.queue[1], n));
-	RB_CUDA(dev_alloc(&w.sec_queue, 2 * n));
-	RB_CUDA(dev_alloc(&w.class_queue, static_cast<size_t>(pt::NUM_CLASSES) * n));
 	w.capacity = capacity;
 	w.counters = c->counters;
 	c->wave_capacity = capacity;
 	c->wave_alloc = capacity;
+	return RB_OK;
+}
+
+rb_status ensure_lanes(rb_context* c, uint32_t count) {
+	if (count > kMaxLanes) return RB_ERR_INVALID_ARGUMENT;
+	while (c->lanes.size() + 1 < count) c->lanes.emplace_back();
+	for (uint32_t k = 0; k + 1 < count; k++) {
+		wave_lane& l = c->lanes[k];
+		if (l.stream == nullptr) {
+			RB_CUDA(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking));
+			RB_CUDA(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming));
+			RB_CUDA(dev_alloc(&l.counters, gpu::CNT_WORDS));
+			RB_CUDA(dev_alloc(&l.params, 1));
+		}
+		if (l.alloc < c->wave_capacity) {
+			l.release_graph();
+			free_wave_buffers(l.wave);
+			dev_free(l.path_scene);
+			l.alloc = 0;
+			RB_CUDA(alloc_wave_buffers(l.wave, c->wave_capacity));
+			RB_CUDA(dev_alloc(&l.path_scene, c->wave_capacity));
+			l.alloc = c->wave_capacity;
+		}
+		l.wave.capacity = c->wave_capacity;
+		l.wave.counters = l.counters;
+		l.wave.params = l.params;
+		l.wave.guide = guide::wave_guide{};
+		l.wave.medium = nullptr;
+		l.wave.vrec = nullptr;
+		l.wave.beam = nullptr;
+		l.wave.beam_queue = nullptr;
+		l.wave.batch = c->wave.batch;
+		l.wave.num_scenes = c->wave.num_scenes;
+		l.wave.scene = l.path_scene;
+	}
 	return RB_OK;
 }
 
@@ -72,8 +121,11 @@ rb_status ensure_film(rb_context* c, int32_t width, int32_t height, bool reset) 
 	return RB_OK;
 }
 
-// Records one wave (counter reset + camera + bounces) into a graph.
-rb_status capture_wave(rb_context* c, uint32_t max_depth) {
+// Records one wave of buffers `w` on stream `s` into a graph: counter reset,
+// camera rays and bounces, and with_end the film resolve / guide training that
+// close the wave. Kept while the configuration is unchanged.
+rb_status capture_into(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s, uint32_t* counters, uint32_t max_depth,
+	bool with_end, cudaGraphExec_t& graph, graph_key& current) {
 	const gpu::launch_cfg cfg = c->cfg();
 	graph_key key;
 	key.capacity = c->wave_capacity;
@@ -83,32 +135,40 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 	key.guide_mode = cfg.guide_mode;
 	key.volume = cfg.volume;
 	key.batch = cfg.batch;
+	key.with_end = with_end;
 	key.block_trace = static_cast<uint32_t>(cfg.block_trace);
 	key.block_shade = static_cast<uint32_t>(cfg.block_shade);
 	key.grid_trace = static_cast<uint32_t>(cfg.grid_trace);
 	key.grid_shade = static_cast<uint32_t>(cfg.grid_shade);
 	key.sort = cfg.sort;
+	key.tail = cfg.tail;
 	if (cfg.guide) {
 		key.guide_steps = cfg.guide->cfg.steps_per_wave;
 		key.guide_batch = cfg.guide->cfg.batch_size;
 	}
-	if (c->graph && c->graph_cfg == key) return RB_OK;
-	c->release_graph();
+	if (graph && current == key) return RB_OK;
+	if (graph) cudaGraphExecDestroy(graph);
+	graph = nullptr;
+	current = graph_key();
 	cudaGraph_t g = nullptr;
-	RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-	cudaError_t e = cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream);
-	if (e == cudaSuccess) e = gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream);
-	if (e == cudaSuccess) e = gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream);
-	const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+	RB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+	cudaError_t e = cudaMemsetAsync(counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), s);
+	if (e == cudaSuccess) e = gpu::launch_wave(c->view, w, c->film, max_depth, 0u, cfg, s);
+	if (e == cudaSuccess && with_end) e = gpu::launch_wave_end(w, c->film, c->num_sms * 4, cfg, s);
+	const cudaError_t e2 = cudaStreamEndCapture(s, &g);
 	if (e != cudaSuccess || e2 != cudaSuccess) {
 		if (g) cudaGraphDestroy(g);
 		return from_cuda(e != cudaSuccess ? e : e2);
 	}
-	e = cudaGraphInstantiate(&c->graph, g, 0);
+	e = cudaGraphInstantiate(&graph, g, 0);
 	cudaGraphDestroy(g);
 	RB_CUDA(e);
-	c->graph_cfg = key;
+	current = key;
 	return RB_OK;
+}
+
+rb_status capture_wave(rb_context* c, uint32_t max_depth) {
+	return capture_into(c, c->wave, c->stream, c->counters, max_depth, true, c->graph, c->graph_cfg);
 }
 
 // Learned guiding for one render call: the guide (default configuration on
@@ -155,64 +215,126 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 	return RB_OK;
 }
 
+// Wave lanes a render call can use: more than one only for plain and batched
+// path tracing replayed from graphs, with at least two waves.
+uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& cfg) {
+	const uint32_t want = resolved_tuning(c->tuning).lanes;
+	if (want <= 1 || cfg.guide != nullptr || cfg.volume || c->profiling || c->has_invisible) return 1;
+	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
+	return static_cast<uint32_t>(waves < want ? waves : want);
+}
+
 // Runs the waves of one render call, whose parameters are in c->params_host
 // (first_item is set here): one graph replay per wave, or direct launches when
 // profiling or when invisible entities make paths outlive max_depth
-// iterations. Records wave_events[k] (when given) after wave k and fills the
-// call's statistics.
-rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, cudaEvent_t* wave_events) {
+// iterations. With several lanes, wave j runs on lane j mod lanes (own buffers
+// and stream) and its film resolve waits for wave j - 1's, so the waves'
+// bounces overlap while the film adds them in order. record_waves: event
+// c->wave_events[j] after wave j's resolve. Fills the call's statistics.
+rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves) {
 	gpu::wave_params& hp = *c->params_host;
 	rb_status st = RB_OK;
+	const gpu::launch_cfg cfg = c->profiled_cfg();
+	const uint32_t nlanes = lanes_for(c, total, cfg);
+	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
+	if (record_waves || nlanes > 1) {
+		while (c->wave_events.size() < waves) {
+			cudaEvent_t e;
+			RB_CUDA(cudaEventCreate(&e));
+			c->wave_events.push_back(e);
+		}
+	}
 	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
 	const bool use_graph = !c->has_invisible && !c->profiling;
 	c->next_event = 0;
-	if (use_graph) {
+	if (nlanes > 1) {
+		st = ensure_lanes(c, nlanes);
+		if (st == RB_OK) st = capture_into(c, c->wave, c->stream, c->counters, max_depth, false, c->graph, c->graph_cfg);
+		for (uint32_t k = 0; k + 1 < nlanes && st == RB_OK; k++) {
+			wave_lane& l = c->lanes[k];
+			st = capture_into(c, l.wave, l.stream, l.counters, max_depth, false, l.graph, l.key);
+		}
+		if (st != RB_OK) return st;
+	} else if (use_graph) {
 		st = capture_wave(c, max_depth);
 		if (st != RB_OK) return st;
 	}
-	const gpu::launch_cfg cfg = c->profiled_cfg();
 	uint32_t launches = 0;
 	hp.first_item = 0;
 	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
 	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
-	uint64_t wave = 0;
-	for (uint64_t first = 0; first < total; first += c->wave_capacity, wave++) {
-		if (use_graph) {
-			// the graph's last node moves params->first_item to the next wave
-			RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
-			launches += gpu::wave_launches(max_depth, cfg);
-		} else {
-			// direct launches: profiling, or invisible entities (a pass-through
-			// does not count as a bounce, so keep bouncing until the queue drains)
-			RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream));
-			RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream));
-			launches += gpu::wave_launches(max_depth, cfg) - 2u;
-			uint32_t q = max_depth & 1u;
-			for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
-				RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-				RB_CUDA(cudaStreamSynchronize(c->stream));
-				if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
-				RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
-				launches += (cfg.sort == RB_SORT_NONE ? 7u : 12u) + ((cfg.guide_mode & gpu::GUIDE_SAMPLE) ? 1u : 0u);
-				q ^= 1u;
-			}
-			RB_CUDA(gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream));
+	if (nlanes > 1) {
+		for (uint32_t k = 0; k + 1 < nlanes; k++) {
+			wave_lane& l = c->lanes[k];
+			RB_CUDA(cudaStreamWaitEvent(l.stream, c->ev_begin, 0));
+			RB_CUDA(cudaMemsetAsync(l.counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), l.stream));
+			RB_CUDA(cudaMemcpyAsync(l.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, l.stream));
 		}
-		if (wave_events != nullptr) RB_CUDA(cudaEventRecord(wave_events[wave], c->stream));
+		for (uint64_t j = 0; j < waves; j++) {
+			const uint32_t lane = static_cast<uint32_t>(j % nlanes);
+			const cudaStream_t s = lane == 0 ? c->stream : c->lanes[lane - 1].stream;
+			const gpu::wave_buffers& w = lane == 0 ? c->wave : c->lanes[lane - 1].wave;
+			const cudaGraphExec_t g = lane == 0 ? c->graph : c->lanes[lane - 1].graph;
+			RB_CUDA(gpu::launch_set_first(w.params, j * c->wave_capacity, s));
+			RB_CUDA(cudaGraphLaunch(g, s));
+			if (j > 0) RB_CUDA(cudaStreamWaitEvent(s, c->wave_events[j - 1], 0));
+			RB_CUDA(gpu::launch_next_wave(w, c->film, c->num_sms * 4, s));
+			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
+			launches += gpu::wave_launches(max_depth, cfg) + 1u;
+		}
+		for (uint32_t k = 0; k + 1 < nlanes; k++) {
+			wave_lane& l = c->lanes[k];
+			RB_CUDA(cudaMemcpyAsync(c->counters_host + (k + 1) * gpu::CNT_WORDS, l.counters, gpu::CNT_WORDS * sizeof(uint32_t),
+				cudaMemcpyDeviceToHost, l.stream));
+			RB_CUDA(cudaEventRecord(l.done, l.stream));
+			RB_CUDA(cudaStreamWaitEvent(c->stream, l.done, 0));
+		}
+	} else {
+		uint64_t wave = 0;
+		for (uint64_t first = 0; first < total; first += c->wave_capacity, wave++) {
+			if (use_graph) {
+				// the graph's last node moves params->first_item to the next wave
+				RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+				launches += gpu::wave_launches(max_depth, cfg);
+			} else {
+				// direct launches: profiling, or invisible entities (a pass-through
+				// does not count as a bounce, so keep bouncing until the queue drains)
+				RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), c->stream));
+				RB_CUDA(gpu::launch_wave(c->view, c->wave, c->film, max_depth, 0u, cfg, c->stream));
+				launches += gpu::wave_launches(max_depth, cfg) - 2u;
+				uint32_t q = max_depth & 1u;
+				for (int guard = 0; guard < 4096 && c->has_invisible; guard++) {
+					RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+					RB_CUDA(cudaStreamSynchronize(c->stream));
+					if (c->counters_host[gpu::CNT_ACTIVE] == 0) break;
+					RB_CUDA(gpu::launch_bounce(c->view, c->wave, c->film, q, cfg, c->stream));
+					launches += (cfg.sort == RB_SORT_NONE ? 7u : 12u) + ((cfg.guide_mode & gpu::GUIDE_SAMPLE) ? 1u : 0u);
+					q ^= 1u;
+				}
+				RB_CUDA(gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream));
+			}
+			if (record_waves) RB_CUDA(cudaEventRecord(c->wave_events[wave], c->stream));
+		}
 	}
 	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
 	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
-	const uint32_t* h = c->counters_host;
-	auto u64 = [&](uint32_t w) { return static_cast<uint64_t>(h[w]) | (static_cast<uint64_t>(h[w + 1]) << 32); };
+	// lane 0's counters, with the other lanes' statistics and first error added
+	uint32_t* h = c->counters_host;
+	auto u64 = [&](const uint32_t* a, uint32_t w) { return static_cast<uint64_t>(a[w]) | (static_cast<uint64_t>(a[w + 1]) << 32); };
 	rb_render_stats& s = c->stats;
+	s = rb_render_stats{};
+	for (uint32_t k = 0; k < nlanes; k++) {
+		const uint32_t* a = h + k * gpu::CNT_WORDS;
+		s.extend_rays += u64(a, gpu::CNT_EXTEND_RAYS);
+		s.shadow_rays += u64(a, gpu::CNT_SHADOW_RAYS);
+		s.mis_rays += u64(a, gpu::CNT_MIS_RAYS);
+		s.node_visits += u64(a, gpu::CNT_NODE_VISITS);
+		s.triangle_tests += u64(a, gpu::CNT_TRI_TESTS);
+		if (s.device_error == 0) s.device_error = a[gpu::CNT_ERROR];
+	}
+	h[gpu::CNT_ERROR] = s.device_error;
 	s.samples = total;
-	s.extend_rays = u64(gpu::CNT_EXTEND_RAYS);
-	s.shadow_rays = u64(gpu::CNT_SHADOW_RAYS);
-	s.mis_rays = u64(gpu::CNT_MIS_RAYS);
-	s.node_visits = u64(gpu::CNT_NODE_VISITS);
-	s.triangle_tests = u64(gpu::CNT_TRI_TESTS);
-	s.device_error = h[gpu::CNT_ERROR];
 	s.kernel_launches = launches;
 	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
 	s.extend_ms = s.secondary_ms = 0.f;
@@ -366,7 +488,7 @@ rb_status rb_context_create(rb_context** out, int device) {
 		if (cudaEventCreate(&c->ev_begin) != cudaSuccess || cudaEventCreate(&c->ev_end) != cudaSuccess) { st = RB_ERR_CUDA; break; }
 		if (cudaMalloc(&c->counters, gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
 		if (cudaMemset(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_CUDA; break; }
-		if (cudaMallocHost(&c->counters_host, gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
+		if (cudaMallocHost(&c->counters_host, kMaxLanes * gpu::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
 		if (cudaMallocHost(&c->params_host, sizeof(gpu::wave_params)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
 		if (cudaMalloc(&c->wave.params, sizeof(gpu::wave_params)) != cudaSuccess) { st = RB_ERR_OUT_OF_MEMORY; break; }
 	} while (false);
@@ -383,6 +505,7 @@ rb_status rb_context_destroy(rb_context* c) {
 	cudaSetDevice(c->device);
 	if (c->stream) cudaStreamSynchronize(c->stream);
 	c->release_graph();
+	c->release_lanes();
 	c->release_wave();
 	c->release_film();
 	c->scene.release();
@@ -526,7 +649,7 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		}
 	}
 
-	st = run_waves(c, total, prm->max_depth, nullptr);
+	st = run_waves(c, total, prm->max_depth, false);
 	if (st != RB_OK) return st;
 	const uint32_t* h = c->counters_host;
 	c->film_samples += prm->spp;

@@ -109,13 +109,7 @@ rb_status batch_render(rb_context* c, const rb_batch_params* prm, float* scene_m
 	hp.rr_threshold = prm->rr_threshold;
 	hp.guide_flags = 0u;
 
-	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
-	while (c->wave_events.size() < waves) {
-		cudaEvent_t e;
-		RB_CUDA(cudaEventCreate(&e));
-		c->wave_events.push_back(e);
-	}
-	st = run_waves(c, total, prm->max_depth, c->wave_events.data());
+	st = run_waves(c, total, prm->max_depth, true);
 	if (st != RB_OK) return st;
 	if (c->stats.device_error != 0) return static_cast<rb_status>(c->stats.device_error);
 	if (scene_ms != nullptr) {
@@ -146,20 +140,24 @@ rb_status time_probe(rb_context* c, const rb_tuning& t, Probe&& probe, float* ms
 	return RB_OK;
 }
 
-// Coordinate descent over the launch shapes, two passes, starting from the
-// context's current tuning. A change is kept when it is at least 1% faster.
+// Coordinate descent over the launch shapes (paths per wave with lanes,
+// block sizes, grid size, sort key, tail bounce), two passes, starting from
+// the context's current tuning. A change is kept when it is at least 1% faster.
 template <typename Probe>
 rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning* best_out, float* best_ms_out) {
 	const rb_tuning start = c->tuning;
 	rb_tuning best = resolved_tuning(c->tuning);
 	if (best.paths_per_wave == 0) best.paths_per_wave = 1u << 21;
+	best.lanes = resolved_tuning(best).lanes;
 	float best_ms = 0.f;
 	rb_status st = time_probe(c, best, probe, &best_ms);
 	if (st != RB_OK) { c->tuning = start; return st; }
-	const uint32_t waves[] = {1u << 19, 1u << 20, 1u << 21, 1u << 22};
+	const uint32_t waves[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
 	const uint32_t blocks[] = {64u, 128u, 256u};
 	const uint32_t grids[] = {2u, 4u, 8u, 16u};
 	const uint32_t sorts[] = {RB_SORT_MATERIAL, RB_SORT_NONE};
+	const uint32_t tails[] = {1u, 2u, 3u, 4u, 6u, 64u};
+	const uint32_t lane_counts[] = {1u, 2u, 3u, 4u};
 	auto try_value = [&](uint32_t rb_tuning::*field, uint32_t value) -> rb_status {
 		if (best.*field == value) return RB_OK;
 		rb_tuning t = best;
@@ -173,16 +171,37 @@ rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning*
 		}
 		return RB_OK;
 	};
-	for (int pass = 0; pass < 2 && st == RB_OK; pass++) {
+	// wave size and lanes interact (lanes only help with several waves), so
+	// they are searched together
+	auto try_waves_lanes = [&]() -> rb_status {
+		const rb_tuning base = best;
 		for (uint32_t v : waves) {
 			// capacities above the work of a probe all run as one wave of that size
 			if (v > work_items && v != waves[0] && (v >> 1) >= work_items) continue;
-			if (st == RB_OK) st = try_value(&rb_tuning::paths_per_wave, v);
+			for (uint32_t l : lane_counts) {
+				if (l > 1 && v >= work_items) continue;  // a single wave has nothing to overlap
+				rb_tuning t = base;
+				t.paths_per_wave = v;
+				t.lanes = l;
+				if (std::memcmp(&t, &best, sizeof(t)) == 0) continue;
+				float ms = 0.f;
+				const rb_status s = time_probe(c, t, probe, &ms);
+				if (s != RB_OK) return s;
+				if (ms < 0.99f * best_ms) {
+					best = t;
+					best_ms = ms;
+				}
+			}
 		}
+		return RB_OK;
+	};
+	for (int pass = 0; pass < 2 && st == RB_OK; pass++) {
+		st = try_waves_lanes();
 		for (uint32_t v : blocks) if (st == RB_OK) st = try_value(&rb_tuning::block_trace, v);
 		for (uint32_t v : blocks) if (st == RB_OK) st = try_value(&rb_tuning::block_shade, v);
 		for (uint32_t v : grids) if (st == RB_OK) st = try_value(&rb_tuning::grid_per_sm, v);
 		for (uint32_t v : sorts) if (st == RB_OK) st = try_value(&rb_tuning::sort, v);
+		for (uint32_t v : tails) if (st == RB_OK) st = try_value(&rb_tuning::tail_bounce, v);
 	}
 	if (st != RB_OK) {
 		c->release_graph();

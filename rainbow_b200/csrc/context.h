@@ -79,12 +79,14 @@ struct graph_key {
 	uint32_t guide_mode = 0, guide_steps = 0, guide_batch = 0;
 	bool volume = false;
 	bool batch = false;
-	uint32_t block_trace = 0, block_shade = 0, grid_trace = 0, grid_shade = 0, sort = 0;
+	bool with_end = true;  // the graph ends with the film resolve (one lane) or stops after the bounces
+	uint32_t block_trace = 0, block_shade = 0, grid_trace = 0, grid_shade = 0, sort = 0, tail = 0;
 	bool operator==(const graph_key& o) const {
 		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
 			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch &&
 			volume == o.volume && batch == o.batch && block_trace == o.block_trace && block_shade == o.block_shade &&
-			grid_trace == o.grid_trace && grid_shade == o.grid_shade && sort == o.sort;
+			grid_trace == o.grid_trace && grid_shade == o.grid_shade && sort == o.sort && tail == o.tail &&
+			with_end == o.with_end;
 	}
 };
 
@@ -94,13 +96,52 @@ inline rb_tuning resolved_tuning(const rb_tuning& t) {
 	if (r.block_trace == 0) r.block_trace = 128;
 	if (r.block_shade == 0) r.block_shade = 128;
 	if (r.grid_per_sm == 0) r.grid_per_sm = 8;
+	if (r.tail_bounce == 0) r.tail_bounce = 64;
+	if (r.lanes == 0) r.lanes = 1;
 	return r;
 }
 inline bool valid_tuning(const rb_tuning& t) {
 	auto block_ok = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 256 && b % 32 == 0); };
 	return block_ok(t.block_trace) && block_ok(t.block_shade) && t.grid_per_sm <= 64 && t.sort <= RB_SORT_NONE &&
-		t.paths_per_wave <= (1u << 24);
+		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= 4;
 }
+
+constexpr uint32_t kMaxLanes = 4;
+
+// Path state of one wave: the buffers of wave_buffers for `n` paths.
+cudaError_t alloc_wave_buffers(gpu::wave_buffers& w, size_t n);
+void free_wave_buffers(gpu::wave_buffers& w);
+
+// A further wave lane of a context: its own path buffers, counters, parameter
+// block, stream and wave graph, so that the waves of one render call overlap.
+struct wave_lane {
+	gpu::wave_buffers wave{};
+	uint32_t alloc = 0;              // paths its buffers hold
+	uint32_t* counters = nullptr;    // device
+	gpu::wave_params* params = nullptr;  // device
+	uint32_t* path_scene = nullptr;  // batch renders: scene of each path
+	cudaStream_t stream = nullptr;
+	cudaGraphExec_t graph = nullptr;
+	graph_key key;
+	cudaEvent_t done = nullptr;
+	void release_graph() {
+		if (graph) cudaGraphExecDestroy(graph);
+		graph = nullptr;
+		key = graph_key();
+	}
+	void release() {
+		release_graph();
+		free_wave_buffers(wave);
+		dev_free(counters);
+		dev_free(params);
+		dev_free(path_scene);
+		if (done) cudaEventDestroy(done);
+		if (stream) cudaStreamDestroy(stream);
+		done = nullptr;
+		stream = nullptr;
+		alloc = 0;
+	}
+};
 
 
 } // namespace ctx
@@ -139,7 +180,7 @@ struct rb_context {
 	size_t trace_cap = 0;
 
 	uint32_t* counters = nullptr;
-	uint32_t* counters_host = nullptr;  // pinned
+	uint32_t* counters_host = nullptr;  // pinned, kMaxLanes * CNT_WORDS (lane k's at k * CNT_WORDS)
 	bool counting = false;
 	bool profiling = false;
 	static constexpr uint32_t kMaxEvents = 4096;  // event pairs per render call when profiling
@@ -159,7 +200,8 @@ struct rb_context {
 	uint32_t* batch_path_scene = nullptr;
 	uint32_t batch_path_alloc = 0;
 	std::vector<std::pair<uint32_t, uint32_t>> batch_range;  // film (first pixel, pixels) of each scene, upload order
-	std::vector<cudaEvent_t> wave_events;
+	std::vector<cudaEvent_t> wave_events;  // recorded after each wave's film resolve
+	std::vector<wave_lane> lanes;    // wave lanes beyond the context's own (lane 0: wave, stream, graph above)
 	bool volume = false;             // the current render call uses the volume path integrator
 	int32_t* vol_medium = nullptr;   // per-path medium buffer (wave.medium points here in volume renders)
 	uint32_t vol_alloc = 0;          // paths the volume buffers hold
@@ -172,6 +214,7 @@ struct rb_context {
 		c.grid_trace = num_sms * static_cast<int>(t.grid_per_sm);
 		c.grid_shade = num_sms * static_cast<int>(t.grid_per_sm);
 		c.sort = t.sort;
+		c.tail = t.tail_bounce;
 		c.batch = is_batch;
 		// the reference-order traversal holds at most depth + 2 entries; the
 		// 4-wide one falls back to it when its stack is full
@@ -187,6 +230,7 @@ struct rb_context {
 	}
 	gpu::launch_cfg profiled_cfg() {
 		gpu::launch_cfg c = cfg();
+		if (profiling) c.tail = 0xffffffffu;  // every bounce as separate stages, each traversal launch timed
 		if (profiling && !events.empty()) {
 			c.events = events.data();
 			c.next_event = &next_event;
@@ -197,11 +241,7 @@ struct rb_context {
 	}
 
 	void release_wave() {
-		dev_free(wave.ray_o); dev_free(wave.ray_d); dev_free(wave.beta); dev_free(wave.radiance); dev_free(wave.bounces);
-		dev_free(wave.rng); dev_free(wave.pixel); dev_free(wave.sample); dev_free(wave.hit); dev_free(wave.rec); dev_free(wave.result);
-		dev_free(wave.sec_o); dev_free(wave.sec_d); dev_free(wave.sec_hit); dev_free(wave.queue[0]); dev_free(wave.queue[1]);
-		dev_free(wave.sec_queue);
-		dev_free(wave.class_queue);
+		free_wave_buffers(wave);
 		dev_free(vol_medium); dev_free(wave.vrec); dev_free(wave.beam); dev_free(wave.beam_queue);
 		wave.medium = nullptr;
 		vol_alloc = 0;
@@ -222,6 +262,11 @@ struct rb_context {
 		if (graph) cudaGraphExecDestroy(graph);
 		graph = nullptr;
 		graph_cfg = graph_key();
+		for (wave_lane& l : lanes) l.release_graph();
+	}
+	void release_lanes() {
+		for (wave_lane& l : lanes) l.release();
+		lanes.clear();
 	}
 	void release_film() {
 		dev_free(film.sum); dev_free(film.sum_sq); dev_free(film.count); dev_free(film_mean);
@@ -239,10 +284,12 @@ rb_status ensure_wave(rb_context* c, uint32_t capacity);
 rb_status ensure_film(rb_context* c, int32_t width, int32_t height, bool reset);
 // The wave graph of the current configuration (recorded when it changed).
 rb_status capture_wave(rb_context* c, uint32_t max_depth);
+// Extra lanes 1..count-1, each with buffers for c->wave_capacity paths.
+rb_status ensure_lanes(rb_context* c, uint32_t count);
 rb_status prepare_guide(rb_context* c, const rb_render_params* prm);
 rb_status prepare_volume(rb_context* c, const rb_render_params* prm);
 bool host_is_valid_camera(const rb_camera_desc& cam);
-rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, cudaEvent_t* wave_events);
+rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves);
 // Replaces the context's scene arrays with a packed scene (single or merged).
 rb_status upload_packed(rb_context* c, const host::packed_scene& p);
 

@@ -603,6 +603,91 @@ __global__ void __launch_bounds__(256) k_shade_b(scene_view s_all, wave_buffers 
 	}
 }
 
+// ------------------------------------------------------------------ tail
+// The rest of every active path in one launch. Late bounces hold few paths,
+// and their per-bounce launches cost more than their work, so from bounce
+// `tail` on one thread carries each surviving path through all its remaining
+// bounces with the same stage functions as the wavefront (extend -> shade_a ->
+// shadow and MIS rays -> shade_b) and the same random-number order, so every
+// sample's radiance is the same as without the tail. Lanes whose path ends
+// take the next path from the active queue (one atomic per warp for all lanes
+// that need one), so long paths do not idle the rest of their warp.
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_tail(scene_view s_all, wave_buffers w, uint32_t queue_in, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack stk = make_stack(smem, stack_cap);
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	const uint32_t lane = threadIdx.x & 31u;
+	uint32_t nodes = 0, tris = 0, ext = 0, nshadow = 0, nmis = 0;
+	bool have = false, exhausted = false, first = false;
+	uint32_t i = 0;
+	int guard = 0;
+	path_state st;
+	for (;;) {
+		const uint32_t need = __ballot_sync(0xffffffffu, !have);
+		if (need != 0u && !exhausted) {
+			const uint32_t leader = __ffs(need) - 1;
+			uint32_t base = 0;
+			if (lane == leader) base = atomicAdd(w.counters + CNT_TAIL, static_cast<uint32_t>(__popc(need)));
+			base = __shfl_sync(0xffffffffu, base, leader);
+			if (base + static_cast<uint32_t>(__popc(need)) >= n) exhausted = true;
+			if (!have) {
+				const uint32_t k = base + __popc(need & lanemask_lt());
+				if (k < n) {
+					i = q[k];
+					st = load_path<BATCH>(w, p, i);
+					have = true;
+					first = true;
+					guard = 0;
+				}
+			}
+		}
+		if (!__any_sync(0xffffffffu, have)) break;
+		if (have) {
+			const scene_view s = BATCH ? batch_view(s_all, w.batch[w.scene[i]]) : s_all;
+			bool alive = false;
+			float len = st.len;
+			hit_t h;
+			if (!first) ext++;  // the first extend ray of each path is counted with the queue (k_advance)
+			first = false;
+			if (!trace_one<false, COUNT>(s, st.o, st.d, len, h, stk, nodes, tris)) {
+				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+			} else {
+				shade_record rec;
+				if (shade_a_any(s, st, h, rec)) {
+					hit_t sh{-1, 0.f, 0.f}, mh{-1, 0.f, 0.f};
+					bool ok = true;
+					if (rec.nee_entity >= 0) {
+						float l = rec.shadow_ray.len;
+						nshadow++;
+						ok = trace_one<true, COUNT>(s, rec.shadow_ray.o, rec.shadow_ray.d, l, sh, stk, nodes, tris);
+					}
+					if (ok && rec.mis_valid) {
+						float l = rec.mis_ray.len;
+						nmis++;
+						ok = trace_one<true, COUNT>(s, rec.mis_ray.o, rec.mis_ray.d, l, mh, stk, nodes, tris);
+					}
+					if (!ok) set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+					else alive = shade_b_any(s, st, rec, sh, mh, p.max_depth, p.rr_threshold) && ++guard < 4096;
+				}
+			}
+			if (!alive) {
+				finish(w, i, st.L);
+				have = false;
+			}
+		}
+	}
+	warp_add64(w.counters, CNT_EXTEND_RAYS, ext);
+	warp_add64(w.counters, CNT_SHADOW_RAYS, nshadow);
+	warp_add64(w.counters, CNT_MIS_RAYS, nmis);
+	if (COUNT) {
+		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
+		warp_add64(w.counters, CNT_TRI_TESTS, tris);
+	}
+}
+
 // ------------------------------------------------------------------ volume path tracing
 // volume_path_integrator::trace (volume_path_integrator.cpp:13-79) per bounce:
 // extend -> shade_a (surface classes, and CLASS_MEDIUM: free-flight sampling,
@@ -932,9 +1017,12 @@ __global__ void k_advance(uint32_t* counters);
 
 // Traversal kernels keep their stacks in dynamic shared memory; above 48 KB a
 // block needs the kernel's opt-in.
+// They also ask for the largest shared-memory carve-out, so that four blocks
+// of 256 threads with their stacks fit on one SM.
 template <typename Kernel>
 cudaError_t allow_smem(Kernel kernel, size_t bytes) {
-	if (bytes <= 48u * 1024u) return cudaSuccess;
+	cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+	if (e != cudaSuccess || bytes <= 48u * 1024u) return e;
 	return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
 
@@ -970,11 +1058,15 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_GUIDE] = 0u;
 	counters[CNT_BEAM] = 0u;
 	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
+	counters[CNT_TAIL] = 0u;
 }
 
 // Moves the wave window forward so the next replay of the same graph renders
 // the following work items.
 __global__ void k_next_wave(wave_params* p, uint32_t capacity) { p->first_item += capacity; }
+
+// The first work item of the next wave of a lane (several lanes take turns).
+__global__ void k_set_first(wave_params* p, uint64_t first) { p->first_item = first; }
 
 template <bool COUNT, bool BATCH>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
@@ -1043,16 +1135,42 @@ cudaError_t launch_bounce(const scene_view& s, const wave_buffers& w, const film
 	return cfg.count ? bounce<true, false>(s, w, f, queue_in, cfg, stream) : bounce<false, false>(s, w, f, queue_in, cfg, stream);
 }
 
+// Whether a wave ends with the tail kernel after cfg.tail bounces (plain
+// surface path tracing only: guided and volume paths keep their stages).
+bool uses_tail(uint32_t max_depth, const launch_cfg& cfg) {
+	return cfg.tail < max_depth && !cfg.volume && cfg.guide == nullptr;
+}
+
+template <bool BATCH>
+cudaError_t launch_tail(const scene_view& s, const wave_buffers& w, uint32_t queue_in, const launch_cfg& cfg,
+	cudaStream_t stream) {
+	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	cudaError_t e;
+	if (cfg.count) {
+		e = allow_smem(k_tail<true, BATCH>, smem);
+		if (e == cudaSuccess) k_tail<true, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	} else {
+		e = allow_smem(k_tail<false, BATCH>, smem);
+		if (e == cudaSuccess) k_tail<false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	}
+	if (e != cudaSuccess) return e;
+	k_advance<<<1, 1, 0, stream>>>(w.counters);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_wave(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t max_depth,
 	uint32_t first_queue, const launch_cfg& cfg, cudaStream_t stream) {
 	if (cfg.batch) k_camera<true><<<cfg.grid_shade, 256, 0, stream>>>(w, first_queue);
 	else k_camera<false><<<cfg.grid_shade, 256, 0, stream>>>(w, first_queue);
 	cudaError_t err = cudaGetLastError();
 	uint32_t qi = first_queue;
-	for (uint32_t b = 0; b < max_depth && err == cudaSuccess; b++) {
+	const bool tail = uses_tail(max_depth, cfg);
+	const uint32_t staged = tail ? cfg.tail : max_depth;
+	for (uint32_t b = 0; b < staged && err == cudaSuccess; b++) {
 		err = launch_bounce(s, w, f, qi, cfg, stream);
 		qi ^= 1u;
 	}
+	if (tail && err == cudaSuccess) err = cfg.batch ? launch_tail<true>(s, w, qi, cfg, stream) : launch_tail<false>(s, w, qi, cfg, stream);
 	return err;
 }
 
@@ -1060,6 +1178,11 @@ cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int g
 	if (w.batch != nullptr) k_film_resolve_batch<<<grid, 256, 0, stream>>>(w, f);
 	else k_film_resolve<<<grid, 256, 0, stream>>>(w, f);
 	k_next_wave<<<1, 1, 0, stream>>>(w.params, w.capacity);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_set_first(wave_params* params, uint64_t first, cudaStream_t stream) {
+	k_set_first<<<1, 1, 0, stream>>>(params, first);
 	return cudaGetLastError();
 }
 
@@ -1084,6 +1207,7 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
 	if (cfg.volume) return 3u + 12u * max_depth;
+	if (uses_tail(max_depth, cfg)) return 3u + (cfg.sort == RB_SORT_NONE ? 7u : 12u) * cfg.tail + 2u;
 	if (cfg.sort == RB_SORT_NONE && cfg.guide == nullptr) return 3u + 7u * max_depth;
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);

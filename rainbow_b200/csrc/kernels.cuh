@@ -25,7 +25,8 @@ enum : uint32_t {
 	CNT_NODE_VISITS = 18,
 	CNT_TRI_TESTS = 20,
 	CNT_BEAM_RAYS = 22,  // closest-hit queries of the transmittance walks
-	CNT_WORDS = 24
+	CNT_TAIL = 24,       // paths taken from the active queue by the tail kernel (reset after it)
+	CNT_WORDS = 26
 };
 static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
 // words cleared at the start of a wave: everything before the 64-bit stats
@@ -151,6 +152,7 @@ struct launch_cfg {
 	bool volume = false;     // volume_path_integrator instead of path_integrator
 	bool batch = false;      // many scenes per wave (wave_buffers::batch)
 	uint32_t sort = 0;       // hit queues: 0 one per material class, 1 a single queue (no sorting)
+	uint32_t tail = 0xffffffffu;  // bounces of separate stages before the tail kernel (>= max_depth: none)
 };
 
 // Ray batches for rb_trace_closest / rb_trace_shadow.
@@ -165,6 +167,9 @@ cudaError_t launch_wave(const pt::scene_view& s, const wave_buffers& w, const fi
 // Adds the wave's finished samples to the film, then advances
 // params->first_item by the wave capacity (the last nodes of a wave).
 cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream);
+
+// Sets params->first_item (the wave window of a lane).
+cudaError_t launch_set_first(wave_params* params, uint64_t first, cudaStream_t stream);
 
 // Per-pixel means of the film into `rgb` (3 floats per pixel, device memory).
 cudaError_t launch_film_mean(const film_buffers& f, uint32_t pixels, float* rgb, int grid, cudaStream_t stream);
