@@ -234,7 +234,8 @@ enum {
 	RB_RENDER_VOLUME = 1u << 3     /* volume_path_integrator::trace (volume_path_integrator.cpp:13-79) instead
 	                                  of path_integrator::trace: free-flight sampling in the media of the
 	                                  path, Henyey-Greenstein scattering, transmittance on every light
-	                                  connection; cannot be combined with learned guiding */
+	                                  connection; with learned guiding, medium vertices use a second
+	                                  guide network (rb_guide_medium_stats_get) */
 };
 
 /* One render call: path_integrator::trace (rainbow-cpu/integrators/path_integrator.cpp:15-47)
@@ -464,6 +465,12 @@ rb_status rb_guide_train(rb_context* ctx, const rb_guide_sample* samples, uint32
 rb_status rb_guide_sample_dirs(rb_context* ctx, const float* outputs, const float* u, uint32_t n, float* directions,
 	float* pdfs);
 rb_status rb_guide_stats_get(rb_context* ctx, rb_guide_stats* out);
+/* Guided volume renders (RB_RENDER_VOLUME with RB_RENDER_GUIDE / RB_RENDER_TRAIN)
+ * guide medium vertices with a second network of the same shape (its own
+ * weights, Adam moments and replay ring), fed the vertex position, a zero
+ * normal and the outgoing direction, and mixed with the Henyey-Greenstein
+ * phase function by the same one-sample MIS; its counters: */
+rb_status rb_guide_medium_stats_get(rb_context* ctx, rb_guide_stats* out);
 
 /* ------------------------------------------------------------------ host-side helpers (no GPU) */
 

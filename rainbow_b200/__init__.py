@@ -251,6 +251,12 @@ class Context:
         check(lib().rb_guide_stats_get(self._h, C.byref(st)), "rb_guide_stats_get")
         return st
 
+    def guide_medium_stats(self) -> GuideStats:
+        """Counters of the medium guide of guided volume renders."""
+        st = GuideStats()
+        check(lib().rb_guide_medium_stats_get(self._h, C.byref(st)), "rb_guide_medium_stats_get")
+        return st
+
 
     # ---- launch tuning (rb_set_tuning / rb_tune_render)
     def set_tuning(self, tuning: Tuning | None = None, **fields) -> None:

@@ -181,6 +181,7 @@ SIGNATURES = {
     "rb_guide_train": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     "rb_guide_sample_dirs": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "rb_guide_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GuideStats)]),
+    "rb_guide_medium_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GuideStats)]),
     "rb_set_tuning": (C.c_int32, [C.c_void_p, C.POINTER(Tuning)]),
     "rb_get_tuning": (C.c_int32, [C.c_void_p, C.POINTER(Tuning)]),
     "rb_tune_render": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.POINTER(Tuning),

@@ -174,20 +174,38 @@ rb_status capture_wave(rb_context* c, uint32_t max_depth) {
 // Learned guiding for one render call: the guide (default configuration on
 // first use), its per-path buffers for this wave size and depth, and the
 // pointers the kernels read. A plain render leaves the guide untouched.
+// A guided volume render also prepares the medium guide (created from the
+// surface guide's configuration with seed + 1 on first use).
 rb_status prepare_guide(rb_context* c, const rb_render_params* prm) {
 	c->guide_mode = 0u;
 	c->wave.guide = guide::wave_guide{};
+	c->wave.guide_medium = guide::wave_guide{};
 	if (!(prm->flags & (RB_RENDER_GUIDE | RB_RENDER_TRAIN))) return RB_OK;
 	if (!c->guide.ready) {
 		const rb_status st = rb_guide_init(c, nullptr);
 		if (st != RB_OK) return st;
 	}
-	guide::guide_state& g = c->guide;
-	const float4* before = g.query_in;
-	RB_CUDA(guide::allocate_wave(g, c->wave_capacity, prm->max_depth));
-	if (g.query_in != before) c->release_graph();
+	auto attach = [&](guide::guide_state& g, guide::wave_guide& w) -> rb_status {
+		const float4* before = g.query_in;
+		RB_CUDA(guide::allocate_wave(g, c->wave_capacity, prm->max_depth));
+		if (g.query_in != before) c->release_graph();
+		w = guide::wave_guide{g.dstate, g.query_in, g.query_out, g.queue, g.vertices, g.vertex_count, g.depth};
+		return RB_OK;
+	};
+	rb_status st = attach(c->guide, c->wave.guide);
+	if (st != RB_OK) return st;
+	if (prm->flags & RB_RENDER_VOLUME) {
+		if (!c->guide_medium.ready) {
+			c->release_graph();
+			rb_guide_config mc = c->guide.cfg;
+			mc.seed += 1u;
+			st = guide::init_state(c->guide_medium, &mc, c->num_sms, c->stream);
+			if (st != RB_OK) return st;
+		}
+		st = attach(c->guide_medium, c->wave.guide_medium);
+		if (st != RB_OK) return st;
+	}
 	c->guide_mode = ((prm->flags & RB_RENDER_GUIDE) ? gpu::GUIDE_SAMPLE : 0u) | ((prm->flags & RB_RENDER_TRAIN) ? gpu::GUIDE_TRAIN : 0u);
-	c->wave.guide = guide::wave_guide{g.dstate, g.query_in, g.query_out, g.queue, g.vertices, g.vertex_count, g.depth};
 	return RB_OK;
 }
 
@@ -199,7 +217,6 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 		c->wave.medium = nullptr;  // plain kernels see no media
 		return RB_OK;
 	}
-	if (prm->flags & (RB_RENDER_GUIDE | RB_RENDER_TRAIN)) return RB_ERR_INVALID_ARGUMENT;
 	if (c->vol_alloc < c->wave_alloc) {
 		c->release_graph();
 		dev_free(c->vol_medium); dev_free(c->wave.vrec); dev_free(c->wave.beam); dev_free(c->wave.beam_queue);
@@ -442,6 +459,9 @@ guide::guide_state* context_guide(rb_context* c, cudaStream_t* stream, int* devi
 
 // Drops the captured wave graph (its launches bake in guide buffer addresses).
 void context_drop_graph(rb_context* c) { c->release_graph(); }
+
+// The medium guide of guided volume renders.
+guide::guide_state* context_guide_medium(rb_context* c) { return &c->guide_medium; }
 } // namespace gpu
 } // namespace rb
 
@@ -512,6 +532,7 @@ rb_status rb_context_destroy(rb_context* c) {
 	c->release_batch();
 	for (cudaEvent_t e : c->wave_events) cudaEventDestroy(e);
 	guide::release(c->guide);
+	guide::release(c->guide_medium);
 	dev_free(c->trace_rays);
 	dev_free(c->trace_hits);
 	dev_free(c->counters);

@@ -189,6 +189,7 @@ struct rb_context {
 	uint32_t next_event = 0;
 	rb_render_stats stats{};
 	guide::guide_state guide;        // learned path guide (allocated on first use)
+	guide::guide_state guide_medium; // guide of medium vertices in guided volume renders
 	uint32_t guide_mode = 0;         // gpu::GUIDE_* of the current render call
 	rb_tuning tuning{};              // launch shapes of render calls (zeros: defaults)
 	// batched rendering: the uploaded scenes (geometry part of their records;
@@ -224,6 +225,7 @@ struct rb_context {
 		if (guide_mode != 0u && guide.ready) {
 			c.guide = &guide;
 			c.guide_mode = guide_mode;
+			if (volume && guide_medium.ready) c.guide_medium = &guide_medium;
 		}
 		c.volume = volume;
 		return c;

@@ -13,6 +13,7 @@
 namespace rb {
 namespace gpu {
 guide::guide_state* context_guide(rb_context* c, cudaStream_t* stream, int* device, int* num_sms);
+guide::guide_state* context_guide_medium(rb_context* c);
 void context_drop_graph(rb_context* c);
 } // namespace gpu
 } // namespace rb
@@ -137,15 +138,13 @@ struct scratch {
 
 } // namespace
 
-extern "C" {
+namespace rb {
+namespace guide {
 
-rb_status rb_guide_init(rb_context* ctx, const rb_guide_config* config) {
-	guide_ctx gc;
-	rb_status st = open_guide(ctx, gc, false);
-	if (st != RB_OK) return st;
-	RB_CUDA(cudaStreamSynchronize(gc.stream));
-	gpu::context_drop_graph(ctx);
-	release(*gc.g);
+// (Re)creates guide `g` with fresh weights and zero Adam moments for `config`
+// (defaults filled in for zero fields).
+rb_status init_state(guide_state& g, const rb_guide_config* config, int sms, cudaStream_t stream) {
+	release(g);
 	rb_guide_config cfg{};
 	if (config) cfg = *config;
 	if (!(cfg.learning_rate > 0.f)) cfg.learning_rate = 1e-3f;
@@ -157,22 +156,63 @@ rb_status rb_guide_init(rb_context* ctx, const rb_guide_config* config) {
 	uint32_t ring = 1024u;
 	while (ring < cfg.max_samples) ring <<= 1;  // the replay ring holds a power of two
 	cfg.max_samples = ring;
-	guide_state& g = *gc.g;
 	g.cfg = cfg;
 	g.sample_cap = cfg.max_samples;
 	g.weight_clip = cfg.weight_clip == 0.f ? 16.f : (cfg.weight_clip < 0.f ? 0.f : cfg.weight_clip);
-	const cudaError_t e = allocate(g, gc.sms);
+	const cudaError_t e = allocate(g, sms);
 	if (e != cudaSuccess) {
 		release(g);
 		return from_cuda(e);
 	}
+	guide_ctx gc;
+	gc.g = &g;
+	gc.stream = stream;
+	gc.sms = sms;
 	const std::vector<float> p = default_params(cfg.seed);
-	st = upload_params(gc, p.data());
+	const rb_status st = upload_params(gc, p.data());
 	if (st != RB_OK) {
 		release(g);
 		return st;
 	}
 	g.ready = true;
+	return RB_OK;
+}
+
+} // namespace guide
+} // namespace rb
+
+extern "C" {
+
+// Creates the surface guide; the medium guide of volume renders is released
+// here and created again, from the same configuration with seed + 1, by the
+// next guided volume render.
+rb_status rb_guide_init(rb_context* ctx, const rb_guide_config* config) {
+	guide_ctx gc;
+	rb_status st = open_guide(ctx, gc, false);
+	if (st != RB_OK) return st;
+	RB_CUDA(cudaStreamSynchronize(gc.stream));
+	gpu::context_drop_graph(ctx);
+	release(*gpu::context_guide_medium(ctx));
+	return init_state(*gc.g, config, gc.sms, gc.stream);
+}
+
+rb_status rb_guide_medium_stats_get(rb_context* ctx, rb_guide_stats* out) {
+	if (ctx == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	guide_ctx gc;
+	const rb_status st = open_guide(ctx, gc, false);
+	if (st != RB_OK) return st;
+	*out = rb_guide_stats{};
+	guide_state* g = gpu::context_guide_medium(ctx);
+	if (!g->ready) return RB_OK;
+	RB_CUDA(cudaStreamSynchronize(gc.stream));
+	device_state s{};
+	RB_CUDA(cudaMemcpy(&s, g->dstate, sizeof(s), cudaMemcpyDeviceToHost));
+	out->steps = s.step;
+	out->samples_last_wave = s.wave_written;
+	out->candidates_last_wave = s.candidates;
+	out->device_error = s.error;
+	out->last_loss = s.last_loss;
+	out->rows_last_step = s.rows_last;
 	return RB_OK;
 }
 

@@ -77,6 +77,8 @@ struct wave_guide {
 };
 
 void release(guide_state& g);
+// (Re)creates a guide with fresh weights (guide_api.cu); config may be null (defaults).
+rb_status init_state(guide_state& g, const rb_guide_config* config, int sms, cudaStream_t stream);
 cudaError_t allocate(guide_state& g, int ctas);
 cudaError_t allocate_wave(guide_state& g, uint32_t capacity, uint32_t depth);
 

@@ -162,6 +162,35 @@ __device__ __forceinline__ void write_guide_query(const wave_params& p, const su
 	out[2] = make_float4(x[8], 0.f, 0.f, 0.f);
 }
 
+// The medium guide's 9 inputs of a medium vertex: position in the scene box,
+// a zero normal (mapped to 0.5) and the outgoing direction.
+__device__ __forceinline__ void write_guide_query_medium(const wave_params& p, vec3 pos, vec3 wo, float4* out) {
+	float x[9] = {(pos.x - p.box_min[0]) * p.box_inv[0], (pos.y - p.box_min[1]) * p.box_inv[1],
+		(pos.z - p.box_min[2]) * p.box_inv[2], 0.5f, 0.5f, 0.5f, 0.5f * (wo.x + 1.f), 0.5f * (wo.y + 1.f), 0.5f * (wo.z + 1.f)};
+	for (int j = 0; j < 9; j++) x[j] = fminf(1.f, fmaxf(0.f, x[j]));
+	out[0] = make_float4(x[0], x[1], x[2], x[3]);
+	out[1] = make_float4(x[4], x[5], x[6], x[7]);
+	out[2] = make_float4(x[8], 0.f, 0.f, 0.f);
+}
+
+// One training vertex of path i (the wave_guide's layout): the guide inputs,
+// the continuation direction and the pdf of the method that could also have
+// drawn it (BSDF or phase function), the throughput before the continuation
+// and the path radiance after the vertex's direct lighting.
+__device__ __forceinline__ void record_vertex(const guide::wave_guide& g, uint32_t i, vec3 wi, float pb, spectrum beta0,
+	spectrum L0) {
+	const uint32_t nv = g.vertex_count[i];
+	if (nv >= g.depth) return;
+	float4* r = g.vertices + (static_cast<size_t>(i) * g.depth + nv) * guide::kVertexFloat4;
+	const float4* x = g.query_in + 3 * i;
+	r[0] = x[0];
+	r[1] = x[1];
+	r[2] = make_float4(x[2].x, wi.x, wi.y, wi.z);
+	r[3] = make_float4(pb, beta0.x, beta0.y, beta0.z);
+	r[4] = make_float4(L0.x, L0.y, L0.z, 0.f);
+	g.vertex_count[i] = nv + 1u;
+}
+
 // Path continuation by one-sample MIS of the guide q (probability alpha) and
 // the BSDF: the direction comes from either, and beta is multiplied by
 // f cos / (alpha q + (1 - alpha) p_bsdf), which is unbiased for any guide.
@@ -430,7 +459,10 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 			w.pixel[i] = pixel;
 			w.sample[i] = sample;
 			w.result[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-			if (p.guide_flags & GUIDE_TRAIN) w.guide.vertex_count[i] = 0u;
+			if (p.guide_flags & GUIDE_TRAIN) {
+				w.guide.vertex_count[i] = 0u;
+				if (w.guide_medium.vertex_count != nullptr) w.guide_medium.vertex_count[i] = 0u;
+			}
 			store_path(w, i, st);
 		}
 		warp_push(valid, i, w.queue[queue_out], w.counters + CNT_ACTIVE);
@@ -756,7 +788,7 @@ __global__ void __launch_bounds__(256) k_shade_a_medium(scene_view s, wave_buffe
 	const uint32_t* q = w.class_queue + CLASS_MEDIUM * w.capacity;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
-		bool push_shadow = false, push_mis = false;
+		bool push_shadow = false, push_mis = false, push_guide = false, push_guide_m = false;
 		uint32_t i = 0;
 		if (k < n) {
 			i = q[k];
@@ -796,11 +828,26 @@ __global__ void __launch_bounds__(256) k_shade_a_medium(scene_view s, wave_buffe
 					w.sec_o[2 * i + 1] = make_float4(mr.o.x, mr.o.y, mr.o.z, mr.len);
 					w.sec_d[2 * i + 1] = make_float4(mr.d.x, mr.d.y, mr.d.z, 0.f);
 				}
+				if (p.guide_flags != 0u && !r.pass_through) {
+					if (vr.flags & VOL_MEDIUM_VERTEX) {
+						if (w.guide_medium.query_in != nullptr) {
+							write_guide_query_medium(p, r.si.p, r.si.wo, w.guide_medium.query_in + 3 * i);
+							push_guide_m = (p.guide_flags & GUIDE_SAMPLE) && w.guide_medium.dstate->usable != 0u;
+						}
+					} else if (r.guidable) {
+						write_guide_query(p, r.si, w.guide.query_in + 3 * i);
+						push_guide = (p.guide_flags & GUIDE_SAMPLE) && w.guide.dstate->usable != 0u;
+					}
+				}
 			}
 			store_path(w, i, st);
 		}
 		warp_push(push_shadow, 2 * i, w.sec_queue, w.counters + CNT_SECONDARY);
 		warp_push(push_mis, 2 * i + 1, w.sec_queue, w.counters + CNT_SECONDARY);
+		if (p.guide_flags != 0u) {
+			warp_push(push_guide, i, w.guide.queue, w.counters + CNT_GUIDE);
+			warp_push(push_guide_m, i, w.guide_medium.queue, w.counters + CNT_GUIDE_MEDIUM);
+		}
 		const uint32_t ns = __popc(__ballot_sync(0xffffffffu, push_shadow));
 		const uint32_t nm = __popc(__ballot_sync(0xffffffffu, push_mis));
 		if ((threadIdx.x & 31u) == 0) {
@@ -969,19 +1016,50 @@ __device__ bool vol_continue(const scene_view& s, const wave_buffers& w, const w
 			}
 			st.L = st.L + st.beta * L;
 		}
+		const spectrum beta0 = st.beta, L0 = st.L;
+		vec3 wi;
+		float pb;
 		if (medium_vertex) {
-			// sample_medium_interaction (integrator.cpp:408-421): the phase value is its pdf, beta stays
-			vec3 wi;
-			hg_sample(rec.si.wo, vr.g, pcg_2d(st.rng), wi);
+			// sample_medium_interaction (integrator.cpp:408-421): the phase value is its pdf, beta stays;
+			// guided: one-sample MIS of the medium guide and the phase function
+			const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && w.guide_medium.query_out != nullptr &&
+				w.guide_medium.dstate->usable != 0u;
+			if (use_guide) {
+				const float* g = reinterpret_cast<const float*>(w.guide_medium.query_out + 12 * i);
+				const float alpha = g[guide::kAlphaOff];
+				const float u_sel = pcg_real(st.rng);
+				const vec2 u = pcg_2d(st.rng);
+				if (u_sel < alpha) {
+					float d[3];
+					guide::guide_sample(g, u_sel / alpha, u.x, u.y, d);
+					wi = vec3{d[0], d[1], d[2]};
+					pb = hg_phase(dot(rec.si.wo, wi), vr.g);
+				} else {
+					pb = hg_sample(rec.si.wo, vr.g, u, wi);
+				}
+				const float pdf = alpha * guide::guide_pdf(g, wi.x, wi.y, wi.z) + (1.f - alpha) * pb;
+				if (!(pdf > 0.f) || !(pb > 0.f)) return false;
+				st.beta = st.beta * (pb / pdf);
+			} else {
+				pb = hg_sample(rec.si.wo, vr.g, pcg_2d(st.rng), wi);
+			}
 			st.flags &= ~PATH_SPECULAR;
 			const ray_t r = spawn_ray(rec.si.p, vec3{0.f, 0.f, 0.f}, wi);
 			st.o = r.o;
 			st.d = r.d;
 			st.len = r.len;
+			if ((p.guide_flags & GUIDE_TRAIN) && w.guide_medium.vertices != nullptr && st.bounces + 1 < static_cast<int32_t>(p.max_depth))
+				record_vertex(w.guide_medium, i, wi, pb, beta0, L0);
 		} else {
-			vec3 wi;
-			float pdf;
-			if (!continue_bsdf<MAT_ANY>(s, st, rec, wi, pdf)) return false;
+			const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && rec.guidable && w.guide.query_out != nullptr &&
+				w.guide.dstate->usable != 0u;
+			const bool ok = use_guide
+				? continue_guided<MAT_ANY>(s, st, rec, reinterpret_cast<const float*>(w.guide.query_out + 12 * i), wi, pb)
+				: continue_bsdf<MAT_ANY>(s, st, rec, wi, pb);
+			if (!ok) return false;
+			if ((p.guide_flags & GUIDE_TRAIN) && rec.guidable && w.guide.vertices != nullptr &&
+				st.bounces + 1 < static_cast<int32_t>(p.max_depth))
+				record_vertex(w.guide, i, wi, pb, beta0, L0);
 		}
 	}
 	if (!medium_vertex) {
@@ -1041,6 +1119,12 @@ cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t q
 	k_shade_a<CLASS_OTHER, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_MISS, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a_medium<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
+	if (cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
+		e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
+		if (e == cudaSuccess && cfg.guide_medium != nullptr)
+			e = guide::launch_forward_queue(*cfg.guide_medium, w.counters + CNT_GUIDE_MEDIUM, stream);
+		if (e != cudaSuccess) return e;
+	}
 	k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_direct<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_beam<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
@@ -1056,6 +1140,7 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_NEXT] = 0u;
 	counters[CNT_SECONDARY] = 0u;
 	counters[CNT_GUIDE] = 0u;
+	counters[CNT_GUIDE_MEDIUM] = 0u;
 	counters[CNT_BEAM] = 0u;
 	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
 	counters[CNT_TAIL] = 0u;
@@ -1195,18 +1280,29 @@ cudaError_t launch_film_mean(const film_buffers& f, uint32_t pixels, float* rgb,
 cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int grid, const launch_cfg& cfg,
 	cudaStream_t stream) {
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
+	const guide::guide_state* guides[2] = {cfg.guide, cfg.guide_medium};
 	cudaError_t e = cudaSuccess;
-	if (train) e = guide::launch_collect(*cfg.guide, w.result, &w.params->first_item, &w.params->total_items, w.capacity, stream);
+	for (const guide::guide_state* g : guides)
+		if (train && g != nullptr && e == cudaSuccess)
+			e = guide::launch_collect(*g, w.result, &w.params->first_item, &w.params->total_items, w.capacity, stream);
 	if (e == cudaSuccess) e = launch_next_wave(w, f, grid, stream);
-	if (train)
-		for (uint32_t k = 0; k < cfg.guide->cfg.steps_per_wave && e == cudaSuccess; k++)
-			e = guide::launch_train_step(*cfg.guide, cfg.guide->samples, &cfg.guide->dstate->ring_filled,
-				cfg.guide->sample_cap, cfg.guide->cfg.batch_size, cfg.guide->cfg.min_rows, false, true, stream);
+	for (const guide::guide_state* g : guides)
+		if (train && g != nullptr)
+			for (uint32_t k = 0; k < g->cfg.steps_per_wave && e == cudaSuccess; k++)
+				e = guide::launch_train_step(*g, g->samples, &g->dstate->ring_filled, g->sample_cap, g->cfg.batch_size,
+					g->cfg.min_rows, false, true, stream);
 	return e;
 }
 
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
-	if (cfg.volume) return 3u + 12u * max_depth;
+	if (cfg.volume) {
+		const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
+		const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
+		const uint32_t nets = cfg.guide_medium != nullptr ? 2u : 1u;
+		uint32_t n = 3u + (12u + (sample ? nets : 0u)) * max_depth;
+		if (train) n += nets * (3u + 2u * cfg.guide->cfg.steps_per_wave);
+		return n;
+	}
 	if (uses_tail(max_depth, cfg)) return 3u + (cfg.sort == RB_SORT_NONE ? 7u : 12u) * cfg.tail + 2u;
 	if (cfg.sort == RB_SORT_NONE && cfg.guide == nullptr) return 3u + 7u * max_depth;
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);

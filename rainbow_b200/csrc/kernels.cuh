@@ -26,6 +26,7 @@ enum : uint32_t {
 	CNT_TRI_TESTS = 20,
 	CNT_BEAM_RAYS = 22,  // closest-hit queries of the transmittance walks
 	CNT_TAIL = 24,       // paths taken from the active queue by the tail kernel (reset after it)
+	CNT_GUIDE_MEDIUM = 25,  // medium vertices queued for a medium-guide evaluation this bounce
 	CNT_WORDS = 26
 };
 static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
@@ -117,6 +118,7 @@ struct wave_buffers {
 	uint32_t* counters;
 	wave_params* params;
 	guide::wave_guide guide;  // null pointers unless a guided render allocated them
+	guide::wave_guide guide_medium;  // medium vertices of guided volume renders (else null pointers)
 	// volume path tracing (null unless a volume render allocated them)
 	int32_t* medium;         // medium of each path, -1: vacuum
 	pt::vol_rec* vrec;       // light-connection factors of the current vertex
@@ -148,6 +150,7 @@ struct launch_cfg {
 	// learned guiding: the guide state and the host-side mode (GUIDE_SAMPLE |
 	// GUIDE_TRAIN) deciding which guide kernels are launched
 	const guide::guide_state* guide = nullptr;
+	const guide::guide_state* guide_medium = nullptr;  // guided volume renders
 	uint32_t guide_mode = 0;
 	bool volume = false;     // volume_path_integrator instead of path_integrator
 	bool batch = false;      // many scenes per wave (wave_buffers::batch)

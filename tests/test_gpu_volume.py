@@ -1,7 +1,8 @@
 """Volume path tracing (RB_RENDER_VOLUME) against the reference's
 volume_path_integrator: per-sample radiance with the reference's random-number
-order, per-pixel means of an independent render, and bit-identity with plain
-path tracing on a scene without media."""
+order, per-pixel means of an independent render, bit-identity with plain
+path tracing on a scene without media, and guided volume rendering (surface
+and medium guides): plain bits before training, unbiased after it."""
 import numpy as np
 import pytest
 
@@ -81,9 +82,47 @@ def test_volume_without_media_equals_plain():
     assert np.array_equal(plain, plain2)
 
 
-def test_volume_rejects_guiding():
-    scene = rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=16, height=16, num_spheres=4, subdivision=1)
+def _fog(res):
+    return rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=res, height=res, num_spheres=12, subdivision=2)
+
+
+def _mean_var(ctx):
+    s, sq, c = ctx.film()
+    m = s / c[..., None]
+    return m, np.maximum(sq / c[..., None] - m ** 2, 0) / c[..., None]
+
+
+def test_untrained_volume_guides_render_plain_bits():
+    """Guided volume rendering before any training step samples the BSDF and
+    the phase function with plain volume path tracing's random numbers."""
+    scene = _fog(24)
     with rb.Context(0) as ctx:
         ctx.upload(scene)
-        with pytest.raises(rb.RbError):
-            ctx.render(scene.camera, 1, max_depth=4, volume=True, guide=True)
+        ctx.guide_init(seed=0)
+        plain = ctx.render(scene.camera, 8, max_depth=8, seed=5, volume=True)
+        guided = ctx.render(scene.camera, 8, max_depth=8, seed=5, volume=True, guide=True)
+        assert np.array_equal(plain, guided)
+
+
+def test_guided_volume_render_is_unbiased():
+    """Surface and medium guides trained online on the fog scene, then a guided
+    volume render against a converged plain volume render: 4 x 4 block z-scores
+    and the image mean (one-sample MIS keeps the estimator unbiased)."""
+    res, B, depth = 32, 4, 8
+    scene = _fog(res)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        ctx.render(scene.camera, 16384, max_depth=depth, seed=100, volume=True, want_image=False)
+        ref, ref_var = _mean_var(ctx)
+        ctx.guide_init(seed=0, batch_size=16384, min_rows=1024, steps_per_wave=4)
+        ctx.render(scene.camera, 1024, max_depth=depth, seed=7, volume=True, guide=True, train=True,
+                   paths_per_wave=res * res * 64, want_image=False)
+        ms = ctx.guide_medium_stats()
+        assert ms.steps >= 32 and ms.device_error == 0 and ctx.guide_stats().steps >= 32
+        ctx.render(scene.camera, 4096, max_depth=depth, seed=9, volume=True, guide=True, want_image=False)
+        m, var = _mean_var(ctx)
+    blk = lambda a: a.reshape(res // B, B, res // B, B, 3).mean((1, 3))
+    zb = (blk(m) - blk(ref)) / np.sqrt((var + ref_var).reshape(res // B, B, res // B, B, 3).sum((1, 3)) / B ** 4 + 1e-12)
+    assert abs(zb.mean()) < 0.3, zb.mean()
+    assert np.mean(np.abs(zb) > 4) < 0.02, np.mean(np.abs(zb) > 4)
+    assert abs(m.mean() / ref.mean() - 1) < 0.01, m.mean() / ref.mean()
