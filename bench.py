@@ -21,13 +21,12 @@ autotuner, run untimed on 4 samples per pixel first.
 The `guided` object is the metric's comparison itself: on the hard-indirect
 room (2,048,000 clutter triangles of 100 displaced icospheres at subdivision 5,
 a 0.5 x 0.5 emitter of radiance 50 facing away from a 0.3-wide slit, glossy
-Trowbridge-Reitz floor and walls), the device time plain path tracing and
-guided path tracing (the learned guide trained online from scratch inside the
-same run, training time included) need until the relMSE against a converged
-plain render falls to each target. The resolution (256 x 256 by default instead
-of 1024 x 1024) and the reference's spp (16,384 instead of 65,536) are reduced
-so that the default run takes minutes; relMSE is a per-pixel mean, so the spp
-each form needs does not depend on the resolution to first order.
+Trowbridge-Reitz floor and walls) at 1024 x 1024, the device time plain path
+tracing (autotuned launch shapes) and guided path tracing (the learned guide
+trained online from scratch inside the same run, training time included) need
+until the relMSE against a converged plain render falls to each target. The
+reference render has 4,096 spp instead of 65,536 so that the default run takes
+minutes (its own relMSE, about 0.0001 at 0.01 targets, is negligible).
 
 --impl reference times the reference CPU integrator (path_integrator::trace of
 the reference sources, compiled as oracle/_ref) on a bounded sample of each step
@@ -170,7 +169,7 @@ def config_dict(world, l2="flushed before the timed call; per-step inputs exceed
             "parallelism": f"replicas x{world} (sample ranges)", "l2": l2}
 
 
-def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp):
+def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=16):
     """Device time to each relMSE target: plain vs guided (online training)."""
     scene = rb.generate_scene(GUIDED["kind"], seed=GUIDED["seed"], width=res, height=res,
                               num_spheres=GUIDED["num_spheres"], subdivision=GUIDED["subdivision"])
@@ -178,7 +177,7 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp):
     ctx = rb.Context(device)
     ctx.upload(scene)
     t0 = time.perf_counter()
-    ctx.render(scene.camera, ref_spp, max_depth=depth, seed=1000, want_image=False)
+    ctx.render(scene.camera, ref_spp, max_depth=depth, seed=1000, want_image=False, paths_per_wave=1 << 22)
     s, _, c = ctx.film()
     ref = s / c[..., None]
     ref_s = time.perf_counter() - t0
@@ -188,15 +187,20 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp):
         m = s / c[..., None]
         return float(np.mean((m - ref) ** 2 / (ref ** 2 + 1e-2)))
 
+    # plain at its fastest: launch shapes tuned for chunk-sized calls; guided: two waves per chunk on two
+    # lanes (each lane samples the weights trained after its previous wave)
+    plain_tuning, _ = ctx.tune_render(scene.camera, probe_spp=chunk, max_depth=depth, seed=55)
+    guided_tuning = dict(paths_per_wave=res * res * chunk // 2, lanes=2, smem_carveout=plain_tuning.smem_carveout)
     out = {}
     for mode in ("plain", "guided"):
         guided = mode == "guided"
         if guided:
-            ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=1 << 18, steps_per_wave=8, min_rows=4096)
+            ctx.set_tuning(plain_tuning, **guided_tuning)
+            ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=1 << 18, steps_per_wave=steps_per_wave, min_rows=4096)
         ms, spp, left, hit = 0.0, 0, sorted(targets, reverse=True), {}
         while left and spp < max_spp:
             ctx.render(scene.camera, chunk, first_sample=spp, max_depth=depth, seed=7, reset=(spp == 0), guide=guided,
-                       train=guided, paths_per_wave=res * res * chunk, want_image=False)
+                       train=guided, want_image=False)
             ms += ctx.stats().elapsed_ms
             spp += chunk
             e = relmse()
@@ -213,7 +217,8 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp):
         res_t[str(t)] = {"plain_s": p and p["s"], "plain_spp": p and p["spp"], "guided_s": g and g["s"],
                          "guided_spp": g and g["spp"], "speedup": (p["s"] / g["s"]) if (p and g) else None}
     return {"workload": f"slit room, {GUIDED['num_spheres'] * 20480 + 18} triangles, {res}x{res}, max depth {depth}, "
-                        f"chunks of {chunk} spp (one wave each, 8 Adam steps of up to 2^18 samples after each guided wave)",
+                        f"chunks of {chunk} spp; guided: two waves per chunk on two lanes, {steps_per_wave} Adam steps of "
+                        f"up to 2^18 samples after each wave; plain: autotuned launch shapes {plain_tuning.as_dict()}",
             "reference": f"plain, {ref_spp} spp, FP64 accumulation ({ref_s:.1f} s)", "targets": res_t,
             "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}
 
@@ -271,9 +276,9 @@ def main():
     ap.add_argument("--cpu-rows", type=int, default=512, help="rows (a central band) of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
-    ap.add_argument("--guided-res", type=int, default=256)
-    ap.add_argument("--guided-ref-spp", type=int, default=16384)
-    ap.add_argument("--guided-chunk", type=int, default=8)
+    ap.add_argument("--guided-res", type=int, default=1024)
+    ap.add_argument("--guided-ref-spp", type=int, default=4096)
+    ap.add_argument("--guided-chunk", type=int, default=2)
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tuning", default=None, help="launch shapes as JSON (skips the autotuner), e.g. "
@@ -421,7 +426,7 @@ def main():
     guided = None
     if rank == 0 and world == 1 and not args.no_guided:
         try:
-            guided = guided_leg(rb, local, args.guided_res, args.guided_ref_spp, (0.01, 0.001), args.guided_chunk, 8192)
+            guided = guided_leg(rb, local, args.guided_res, args.guided_ref_spp, (0.01, 0.005), args.guided_chunk, 256)
         except Exception as e:  # reported, never required for the throughput line
             guided = {"error": str(e)}
 

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 3
+#define RBGPU_ABI_VERSION 4
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -325,6 +325,11 @@ enum {
 	RB_SORT_MATERIAL = 0,       /* one hit queue per material class (coherent shading warps) */
 	RB_SORT_NONE = 1            /* one hit queue for every surface hit (no sorting) */
 };
+enum {
+	RB_TRAVERSAL_PER_THREAD = 0, /* one ray per thread, traced to the end (grid-stride) */
+	RB_TRAVERSAL_REFILL = 1      /* persistent lanes advance their ray one node at a time and take the next ray
+	                                from the queue as soon as theirs is done */
+};
 typedef struct rb_tuning {
 	uint32_t paths_per_wave;    /* queue capacity, 0: library default (2^21); a render's own
 	                               rb_render_params.paths_per_wave takes precedence */
@@ -339,7 +344,11 @@ typedef struct rb_tuning {
 	                               graph, so the late bounces of one wave overlap the next wave's early
 	                               ones; the film still adds the waves in order (plain and batched
 	                               renders; guided and volume renders use one lane) */
-	uint32_t reserved[1];
+	uint32_t traversal;         /* RB_TRAVERSAL_*: how the traversal kernels take rays */
+	uint32_t smem_carveout;     /* traversal kernels' shared-memory share of the L1 / shared storage, in
+	                               percent + 1 (1..101); 0: the largest share (4 blocks of 256 threads with
+	                               their stacks); smaller shares leave more L1 for tree nodes */
+	uint32_t reserved[3];
 } rb_tuning;
 /* Use `tuning` (NULL: defaults) for the context's later render calls. */
 rb_status rb_set_tuning(rb_context* ctx, const rb_tuning* tuning);

@@ -142,6 +142,8 @@ rb_status capture_into(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s
 	key.grid_shade = static_cast<uint32_t>(cfg.grid_shade);
 	key.sort = cfg.sort;
 	key.tail = cfg.tail;
+	key.refill = cfg.refill;
+	key.carveout = cfg.carveout;
 	if (cfg.guide) {
 		key.guide_steps = cfg.guide->cfg.steps_per_wave;
 		key.guide_batch = cfg.guide->cfg.batch_size;
@@ -189,7 +191,7 @@ rb_status prepare_guide(rb_context* c, const rb_render_params* prm) {
 		const float4* before = g.query_in;
 		RB_CUDA(guide::allocate_wave(g, c->wave_capacity, prm->max_depth));
 		if (g.query_in != before) c->release_graph();
-		w = guide::wave_guide{g.dstate, g.query_in, g.query_out, g.queue, g.vertices, g.vertex_count, g.depth};
+		w = guide::state_view(g);
 		return RB_OK;
 	};
 	rb_status st = attach(c->guide, c->wave.guide);
@@ -236,7 +238,7 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 // path tracing replayed from graphs, with at least two waves.
 uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& cfg) {
 	const uint32_t want = resolved_tuning(c->tuning).lanes;
-	if (want <= 1 || cfg.guide != nullptr || cfg.volume || c->profiling || c->has_invisible) return 1;
+	if (want <= 1 || cfg.volume || c->profiling || c->has_invisible) return 1;
 	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
 	return static_cast<uint32_t>(waves < want ? waves : want);
 }
@@ -264,8 +266,23 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
 	const bool use_graph = !c->has_invisible && !c->profiling;
 	c->next_event = 0;
+	const bool guided = nlanes > 1 && cfg.guide != nullptr;
+	const bool training = guided && (cfg.guide_mode & gpu::GUIDE_TRAIN);
 	if (nlanes > 1) {
 		st = ensure_lanes(c, nlanes);
+		// guided waves on lanes: each lane's own guide buffers and its snapshot of the
+		// weights, taken after the lane's previous wave trained (a fixed lag of
+		// nlanes - 1 waves behind the newest weights, independent of timing)
+		for (uint32_t k = 0; k < nlanes && st == RB_OK && guided; k++) {
+			guide::lane_guide& lg = c->lane_guides[k];
+			const float4* before = lg.query_in;
+			const cudaError_t e = guide::allocate_lane(lg, c->wave_capacity, max_depth);
+			if (e != cudaSuccess) st = from_cuda(e);
+			else if (lg.query_in != before) c->release_graph();
+			const guide::wave_guide wg = guide::lane_view(c->guide, lg);
+			if (k == 0) c->wave.guide = wg;
+			else c->lanes[k - 1].wave.guide = wg;
+		}
 		if (st == RB_OK) st = capture_into(c, c->wave, c->stream, c->counters, max_depth, false, c->graph, c->graph_cfg);
 		for (uint32_t k = 0; k + 1 < nlanes && st == RB_OK; k++) {
 			wave_lane& l = c->lanes[k];
@@ -279,6 +296,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 	uint32_t launches = 0;
 	hp.first_item = 0;
 	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	for (uint32_t k = 0; guided && k < nlanes; k++) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[k], c->stream));
 	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
 	if (nlanes > 1) {
 		for (uint32_t k = 0; k + 1 < nlanes; k++) {
@@ -295,7 +313,9 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			RB_CUDA(gpu::launch_set_first(w.params, j * c->wave_capacity, s));
 			RB_CUDA(cudaGraphLaunch(g, s));
 			if (j > 0) RB_CUDA(cudaStreamWaitEvent(s, c->wave_events[j - 1], 0));
-			RB_CUDA(gpu::launch_next_wave(w, c->film, c->num_sms * 4, s));
+			// in wave order: training-sample collection, film resolve, training, then this lane's snapshot
+			RB_CUDA(gpu::launch_wave_end(w, c->film, c->num_sms * 4, cfg, s));
+			if (training) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[lane], s));
 			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
 			launches += gpu::wave_launches(max_depth, cfg) + 1u;
 		}

@@ -141,8 +141,9 @@ rb_status time_probe(rb_context* c, const rb_tuning& t, Probe&& probe, float* ms
 }
 
 // Coordinate descent over the launch shapes (paths per wave with lanes,
-// block sizes, grid size, sort key, tail bounce), two passes, starting from
-// the context's current tuning. A change is kept when it is at least 1% faster.
+// block sizes, grid size, sort key, tail bounce, traversal kind, shared-memory
+// carve-out), two passes, starting from the context's current tuning. A change
+// is kept when it is at least 1% faster.
 template <typename Probe>
 rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning* best_out, float* best_ms_out) {
 	const rb_tuning start = c->tuning;
@@ -158,6 +159,8 @@ rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning*
 	const uint32_t sorts[] = {RB_SORT_MATERIAL, RB_SORT_NONE};
 	const uint32_t tails[] = {1u, 2u, 3u, 4u, 6u, 64u};
 	const uint32_t lane_counts[] = {1u, 2u, 3u, 4u};
+	const uint32_t traversals[] = {RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL};
+	const uint32_t carveouts[] = {0u, 26u, 51u, 76u};  // largest, 25%, 50%, 75% (stored as percent + 1)
 	auto try_value = [&](uint32_t rb_tuning::*field, uint32_t value) -> rb_status {
 		if (best.*field == value) return RB_OK;
 		rb_tuning t = best;
@@ -202,6 +205,8 @@ rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning*
 		for (uint32_t v : grids) if (st == RB_OK) st = try_value(&rb_tuning::grid_per_sm, v);
 		for (uint32_t v : sorts) if (st == RB_OK) st = try_value(&rb_tuning::sort, v);
 		for (uint32_t v : tails) if (st == RB_OK) st = try_value(&rb_tuning::tail_bounce, v);
+		for (uint32_t v : traversals) if (st == RB_OK) st = try_value(&rb_tuning::traversal, v);
+		for (uint32_t v : carveouts) if (st == RB_OK) st = try_value(&rb_tuning::smem_carveout, v);
 	}
 	if (st != RB_OK) {
 		c->release_graph();

@@ -81,12 +81,14 @@ struct graph_key {
 	bool batch = false;
 	bool with_end = true;  // the graph ends with the film resolve (one lane) or stops after the bounces
 	uint32_t block_trace = 0, block_shade = 0, grid_trace = 0, grid_shade = 0, sort = 0, tail = 0;
+	bool refill = false;
+	int carveout = 0;
 	bool operator==(const graph_key& o) const {
 		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
 			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch &&
 			volume == o.volume && batch == o.batch && block_trace == o.block_trace && block_shade == o.block_shade &&
 			grid_trace == o.grid_trace && grid_shade == o.grid_shade && sort == o.sort && tail == o.tail &&
-			with_end == o.with_end;
+			with_end == o.with_end && refill == o.refill && carveout == o.carveout;
 	}
 };
 
@@ -103,7 +105,8 @@ inline rb_tuning resolved_tuning(const rb_tuning& t) {
 inline bool valid_tuning(const rb_tuning& t) {
 	auto block_ok = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 256 && b % 32 == 0); };
 	return block_ok(t.block_trace) && block_ok(t.block_shade) && t.grid_per_sm <= 64 && t.sort <= RB_SORT_NONE &&
-		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= 4;
+		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= 4 && t.traversal <= RB_TRAVERSAL_REFILL &&
+		t.smem_carveout <= 101;
 }
 
 constexpr uint32_t kMaxLanes = 4;
@@ -190,6 +193,7 @@ struct rb_context {
 	rb_render_stats stats{};
 	guide::guide_state guide;        // learned path guide (allocated on first use)
 	guide::guide_state guide_medium; // guide of medium vertices in guided volume renders
+	guide::lane_guide lane_guides[kMaxLanes];  // per-lane guide buffers and weight snapshots (guided renders on lanes)
 	uint32_t guide_mode = 0;         // gpu::GUIDE_* of the current render call
 	rb_tuning tuning{};              // launch shapes of render calls (zeros: defaults)
 	// batched rendering: the uploaded scenes (geometry part of their records;
@@ -216,6 +220,8 @@ struct rb_context {
 		c.grid_shade = num_sms * static_cast<int>(t.grid_per_sm);
 		c.sort = t.sort;
 		c.tail = t.tail_bounce;
+		c.refill = t.traversal == RB_TRAVERSAL_REFILL;
+		c.carveout = t.smem_carveout == 0 ? 100 : static_cast<int>(t.smem_carveout) - 1;
 		c.batch = is_batch;
 		// the reference-order traversal holds at most depth + 2 entries; the
 		// 4-wide one falls back to it when its stack is full
@@ -269,6 +275,7 @@ struct rb_context {
 	void release_lanes() {
 		for (wave_lane& l : lanes) l.release();
 		lanes.clear();
+		for (guide::lane_guide& g : lane_guides) guide::release_lane(g);
 	}
 	void release_film() {
 		dev_free(film.sum); dev_free(film.sum_sq); dev_free(film.count); dev_free(film_mean);

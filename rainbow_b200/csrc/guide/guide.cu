@@ -22,6 +22,8 @@
 
 #include <cuda_bf16.h>
 
+#include <cstddef>
+
 namespace rb {
 namespace guide {
 namespace {
@@ -736,6 +738,60 @@ cudaError_t allocate_wave(guide_state& g, uint32_t capacity, uint32_t depth) {
 	return e;
 }
 
+cudaError_t allocate_lane(lane_guide& l, uint32_t capacity, uint32_t depth) {
+	if (l.capacity >= capacity && l.depth >= depth && l.query_in) return cudaSuccess;
+	release_lane(l);
+	cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&l.query_in), sizeof(float4) * 3 * static_cast<size_t>(capacity));
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&l.query_out), sizeof(float4) * 12 * static_cast<size_t>(capacity));
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&l.queue), sizeof(uint32_t) * static_cast<size_t>(capacity));
+	if (e == cudaSuccess)
+		e = cudaMalloc(reinterpret_cast<void**>(&l.vertices), sizeof(float4) * kVertexFloat4 * static_cast<size_t>(capacity) * depth);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&l.vertex_count), sizeof(uint32_t) * static_cast<size_t>(capacity));
+	if (e == cudaSuccess) e = cudaMemset(l.vertex_count, 0, sizeof(uint32_t) * static_cast<size_t>(capacity));
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&l.image), kImageBytes);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&l.usable), sizeof(uint32_t));
+	if (e == cudaSuccess) e = cudaMemset(l.usable, 0, sizeof(uint32_t));
+	if (e != cudaSuccess) {
+		release_lane(l);
+		return e;
+	}
+	l.capacity = capacity;
+	l.depth = depth;
+	return cudaSuccess;
+}
+
+void release_lane(lane_guide& l) {
+	void* ptrs[] = {l.query_in, l.query_out, l.queue, l.vertices, l.vertex_count, l.image, l.usable};
+	for (void* p : ptrs)
+		if (p) cudaFree(p);
+	l = lane_guide{};
+}
+
+wave_guide state_view(const guide_state& g) {
+	const uint32_t* usable = g.dstate == nullptr ? nullptr
+		: reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(g.dstate) + offsetof(device_state, usable));
+	return wave_guide{g.dstate, g.query_in, g.query_out, g.queue, g.vertices, g.vertex_count, g.depth, usable, g.image};
+}
+
+wave_guide lane_view(const guide_state& g, const lane_guide& l) {
+	return wave_guide{g.dstate, l.query_in, l.query_out, l.queue, l.vertices, l.vertex_count, l.depth, l.usable, l.image};
+}
+
+__global__ void k_snapshot(const uint4* __restrict__ image, uint4* __restrict__ lane_image, uint32_t n16,
+	const device_state* s, uint32_t* usable) {
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n16) lane_image[i] = image[i];
+	if (i == 0) *usable = s->usable;
+}
+
+cudaError_t launch_snapshot(const guide_state& g, const lane_guide& l, cudaStream_t s) {
+	static_assert(kImageBytes % 16 == 0, "the image is copied in 16-byte units");
+	const uint32_t n16 = kImageBytes / 16;
+	k_snapshot<<<(n16 + 255) / 256, 256, 0, s>>>(reinterpret_cast<const uint4*>(g.image), reinterpret_cast<uint4*>(l.image),
+		n16, g.dstate, l.usable);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_init_image(const guide_state& g, cudaStream_t s) {
 	k_image<<<(kAugParams + 255) / 256, 256, 0, s>>>(g.master, reinterpret_cast<__nv_bfloat16*>(g.image));
 	return cudaGetLastError();
@@ -755,13 +811,13 @@ cudaError_t launch_forward_raw(const guide_state& g, const float* x, uint32_t n,
 	return cudaGetLastError();
 }
 
-cudaError_t launch_forward_queue(const guide_state& g, const uint32_t* count, cudaStream_t s) {
+cudaError_t launch_forward_queue(const guide_state& g, const wave_guide& wg, const uint32_t* count, cudaStream_t s) {
 	fwd_args a{};
-	a.image = g.image;
+	a.image = wg.image;
 	a.count = count;
-	a.queue = g.queue;
-	a.in4 = g.query_in;
-	a.out4 = g.query_out;
+	a.queue = wg.queue;
+	a.in4 = wg.query_in;
+	a.out4 = wg.query_out;
 	a.error = &g.dstate->error;
 	k_forward<true><<<g.ctas, 256, kFwdSmem, s>>>(a);
 	return cudaGetLastError();
@@ -810,7 +866,7 @@ cudaError_t launch_decode_sample(const float* raw, const float* u, uint32_t n, f
 	return cudaGetLastError();
 }
 
-cudaError_t launch_collect(const guide_state& g, const float4* result, const uint64_t* first_item,
+cudaError_t launch_collect(const guide_state& g, const wave_guide& wg, const float4* result, const uint64_t* first_item,
 	const uint64_t* total_items, uint32_t capacity, cudaStream_t s) {
 	k_collect_begin<<<1, 1, 0, s>>>(g.dstate);
 	collect_args a{};
@@ -818,9 +874,9 @@ cudaError_t launch_collect(const guide_state& g, const float4* result, const uin
 	a.first_item = first_item;
 	a.total_items = total_items;
 	a.capacity = capacity;
-	a.vertices = g.vertices;
-	a.vertex_count = g.vertex_count;
-	a.depth = g.depth;
+	a.vertices = wg.vertices;
+	a.vertex_count = wg.vertex_count;
+	a.depth = wg.depth;
 	a.samples = g.samples;
 	a.cap = g.sample_cap;
 	a.state = g.dstate;

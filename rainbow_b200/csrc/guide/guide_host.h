@@ -74,7 +74,31 @@ struct wave_guide {
 	float4* vertices;
 	uint32_t* vertex_count;
 	uint32_t depth;
+	const uint32_t* usable;  // the guide may be sampled: the device_state's flag, or a lane's snapshot of it
+	const uint8_t* image;    // bf16 weights this wave's forward passes read: the training image, or a lane's snapshot
 };
+
+// Per-wave guide buffers of one wave lane, with the lane's snapshot of the
+// weights and of the usable flag (taken after the lane's own wave trained), so
+// that overlapping waves read weights fixed by the wave order alone.
+struct lane_guide {
+	float4* query_in = nullptr;
+	float4* query_out = nullptr;
+	uint32_t* queue = nullptr;
+	float4* vertices = nullptr;
+	uint32_t* vertex_count = nullptr;
+	uint32_t capacity = 0, depth = 0;
+	uint8_t* image = nullptr;
+	uint32_t* usable = nullptr;
+};
+cudaError_t allocate_lane(lane_guide& l, uint32_t capacity, uint32_t depth);
+void release_lane(lane_guide& l);
+// The guide's own buffers, weights and flag (one lane).
+wave_guide state_view(const guide_state& g);
+// A lane's buffers and snapshots.
+wave_guide lane_view(const guide_state& g, const lane_guide& l);
+// Copies the training image and the usable flag into the lane's snapshots.
+cudaError_t launch_snapshot(const guide_state& g, const lane_guide& l, cudaStream_t s);
 
 void release(guide_state& g);
 // (Re)creates a guide with fresh weights (guide_api.cu); config may be null (defaults).
@@ -85,7 +109,8 @@ cudaError_t allocate_wave(guide_state& g, uint32_t capacity, uint32_t depth);
 // Launchers (guide.cu).
 cudaError_t launch_init_image(const guide_state& g, cudaStream_t s);
 cudaError_t launch_forward_raw(const guide_state& g, const float* x, uint32_t n, float* out, cudaStream_t s);
-cudaError_t launch_forward_queue(const guide_state& g, const uint32_t* count, cudaStream_t s);
+// Forward pass of the queued vertices of a wave (wg: its buffers and weights).
+cudaError_t launch_forward_queue(const guide_state& g, const wave_guide& wg, const uint32_t* count, cudaStream_t s);
 // One training step over min(batch, *count, count_cap) samples: the gradient kernel then
 // the reduction + Adam kernel. sequential: row r uses sample r, else rows draw
 // samples by a hash of (step, row). budgeted: the step runs only while the
@@ -93,8 +118,8 @@ cudaError_t launch_forward_queue(const guide_state& g, const uint32_t* count, cu
 cudaError_t launch_train_step(const guide_state& g, const float4* samples, const uint32_t* count, uint32_t count_cap,
 	uint32_t batch, uint32_t min_rows, bool sequential, bool budgeted, cudaStream_t s);
 cudaError_t launch_decode_sample(const float* raw, const float* u, uint32_t n, float* dirs, float* pdfs, cudaStream_t s);
-// Wave end: training samples from the recorded vertices of `paths` paths.
-cudaError_t launch_collect(const guide_state& g, const float4* result, const uint64_t* first_item,
+// Wave end: training samples from the recorded vertices (wg) of the wave's paths.
+cudaError_t launch_collect(const guide_state& g, const wave_guide& wg, const float4* result, const uint64_t* first_item,
 	const uint64_t* total_items, uint32_t capacity, cudaStream_t s);
 
 } // namespace guide

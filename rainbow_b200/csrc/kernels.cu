@@ -246,7 +246,7 @@ __device__ bool shade_b_guided(const scene_view& s, const wave_buffers& w, const
 		const spectrum beta0 = st.beta, L0 = st.L;
 		vec3 wi;
 		float pb;
-		const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && rec.guidable && w.guide.dstate->usable != 0u;
+		const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && rec.guidable && *w.guide.usable != 0u;
 		const bool ok = use_guide
 			? continue_guided<MAT>(s, st, rec, reinterpret_cast<const float*>(w.guide.query_out + 12 * i), wi, pb)
 			: continue_bsdf<MAT>(s, st, rec, wi, pb);
@@ -508,6 +508,156 @@ __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, ui
 	}
 }
 
+// ------------------------------------------------------------------ persistent traversal
+// Lanes take rays one at a time from a queue (one atomic per warp for all the
+// lanes that need a ray) and advance them one node or leaf per iteration, so a
+// warp stays full until the queue is empty instead of idling while its longest
+// ray finishes. Each ray sees exactly the operations of closest_hit_fast.
+struct ray_fetch {
+	bool exhausted = false;
+	// Gives lanes without a ray the next queue positions; k >= n: none left.
+	__device__ __forceinline__ bool take(bool need_ray, uint32_t* counter, uint32_t n, uint32_t& k) {
+		const uint32_t need = __ballot_sync(0xffffffffu, need_ray);
+		if (need == 0u || exhausted) return false;
+		const uint32_t lane = threadIdx.x & 31u, leader = __ffs(need) - 1;
+		uint32_t base = 0;
+		if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(need)));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (base + static_cast<uint32_t>(__popc(need)) >= n) exhausted = true;
+		k = base + __popc(need & lanemask_lt());
+		return need_ray && k < n;
+	}
+};
+
+// The reference-order redo of a ray the 4-wide walk gave up on.
+template <bool SHADOW>
+__device__ __forceinline__ bool trace_exact(const scene_view& sv, vec3 o, vec3 d, float& len, hit_t& h, smem_stack& st) {
+	trace_counters c{0u, 0u};
+	return closest_hit<SHADOW, false>(sv, o, d, len, h, st, c);
+}
+
+template <bool VOL, bool BATCH>
+__global__ void __launch_bounds__(256) k_extend_refill(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
+	uint32_t sort) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st = make_stack(smem, stack_cap);
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	ray_fetch fetch;
+	trav_state t;
+	uint32_t i = 0;
+	float len0 = 0.f;
+	bool active = false;
+	for (;;) {
+		bool finished = false, ok = true;
+		hit_t h{-1, 0.f, 0.f};
+		float len = 0.f;
+		uint32_t k;
+		if (fetch.take(!active, w.counters + CNT_FETCH_EXTEND, n, k)) {
+			i = q[k];
+			const float4 o = w.ray_o[i], d = w.ray_d[i];
+			const vec3 o3{o.x, o.y, o.z}, d3{d.x, d.y, d.z};
+			len0 = o.w;
+			const scene_view sv = BATCH ? batch_view(s, w.batch[w.scene[i]]) : s;
+			if (isnan(len0) || sv.wnodes == nullptr) {
+				len = len0;
+				ok = trace_exact<false>(sv, o3, d3, len, h, st);
+				finished = true;
+			} else if (trav_begin(sv, t, o3, d3, len0, st)) {
+				active = true;
+			} else {
+				len = len0;
+				finished = true;
+			}
+		}
+		if (active) {
+			const int r = trav_step<false>(s, t, st);
+			if (r != 0) {
+				active = false;
+				finished = true;
+				if (r > 0) {
+					h = t.hit;
+					len = t.len;
+				} else {
+					const scene_view sv = BATCH ? batch_view(s, w.batch[w.scene[i]]) : s;
+					len = len0;
+					ok = trace_exact<false>(sv, t.o, t.d, len, h, st);
+				}
+			}
+		}
+		uint32_t key = 0xffffffffu;
+		if (finished) {
+			if (!ok) {
+				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+				h.slot = -1;
+			}
+			w.hit[i] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
+			key = (VOL && w.medium[i] >= 0) ? static_cast<uint32_t>(CLASS_MEDIUM) : shade_class(s, h.slot);
+			if (sort == RB_SORT_NONE && key != CLASS_MISS && key != CLASS_MEDIUM) key = CLASS_OTHER;
+		}
+		if (__any_sync(0xffffffffu, finished)) warp_push_keyed(key, i, w.class_queue, w.capacity, w.counters + CNT_CLASS);
+		if (fetch.exhausted && !__any_sync(0xffffffffu, active)) break;
+	}
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(256) k_secondary_refill(scene_view s, wave_buffers w, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st = make_stack(smem, stack_cap);
+	const uint32_t n = w.counters[CNT_SECONDARY];
+	ray_fetch fetch;
+	trav_state t;
+	uint32_t j = 0;
+	float len0 = 0.f;
+	bool active = false;
+	for (;;) {
+		bool finished = false, ok = true;
+		hit_t h{-1, 0.f, 0.f};
+		float len = 0.f;
+		uint32_t k;
+		if (fetch.take(!active, w.counters + CNT_FETCH_SECONDARY, n, k)) {
+			j = w.sec_queue[k];
+			const float4 o = w.sec_o[j], d = w.sec_d[j];
+			const vec3 o3{o.x, o.y, o.z}, d3{d.x, d.y, d.z};
+			len0 = o.w;
+			const scene_view sv = BATCH ? batch_view(s, w.batch[w.scene[j >> 1]]) : s;
+			if (isnan(len0) || sv.wnodes == nullptr) {
+				len = len0;
+				ok = trace_exact<true>(sv, o3, d3, len, h, st);
+				finished = true;
+			} else if (trav_begin(sv, t, o3, d3, len0, st)) {
+				active = true;
+			} else {
+				len = len0;
+				finished = true;
+			}
+		}
+		if (active) {
+			const int r = trav_step<true>(s, t, st);
+			if (r != 0) {
+				active = false;
+				finished = true;
+				if (r > 0) {
+					h = t.hit;
+					len = t.len;
+				} else {
+					const scene_view sv = BATCH ? batch_view(s, w.batch[w.scene[j >> 1]]) : s;
+					len = len0;
+					ok = trace_exact<true>(sv, t.o, t.d, len, h, st);
+				}
+			}
+		}
+		if (finished) {
+			if (!ok) {
+				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+				h.slot = -1;
+			}
+			w.sec_hit[j] = make_float4(__uint_as_float(static_cast<uint32_t>(h.slot)), len, h.b1, h.b2);
+		}
+		if (fetch.exhausted && !__any_sync(0xffffffffu, active)) break;
+	}
+}
+
 template <uint32_t CLASS, bool VOL, bool BATCH>
 __global__ void __launch_bounds__(256) k_shade_a(scene_view s_all, wave_buffers w) {
 	const wave_params& p = *w.params;
@@ -552,7 +702,7 @@ __global__ void __launch_bounds__(256) k_shade_a(scene_view s_all, wave_buffers 
 					}
 					if (p.guide_flags != 0u && r.guidable && !r.pass_through) {
 						write_guide_query(p, r.si, w.guide.query_in + 3 * i);
-						push_guide = (p.guide_flags & GUIDE_SAMPLE) && w.guide.dstate->usable != 0u;
+						push_guide = (p.guide_flags & GUIDE_SAMPLE) && *w.guide.usable != 0u;
 					}
 				}
 			}
@@ -832,11 +982,11 @@ __global__ void __launch_bounds__(256) k_shade_a_medium(scene_view s, wave_buffe
 					if (vr.flags & VOL_MEDIUM_VERTEX) {
 						if (w.guide_medium.query_in != nullptr) {
 							write_guide_query_medium(p, r.si.p, r.si.wo, w.guide_medium.query_in + 3 * i);
-							push_guide_m = (p.guide_flags & GUIDE_SAMPLE) && w.guide_medium.dstate->usable != 0u;
+							push_guide_m = (p.guide_flags & GUIDE_SAMPLE) && *w.guide_medium.usable != 0u;
 						}
 					} else if (r.guidable) {
 						write_guide_query(p, r.si, w.guide.query_in + 3 * i);
-						push_guide = (p.guide_flags & GUIDE_SAMPLE) && w.guide.dstate->usable != 0u;
+						push_guide = (p.guide_flags & GUIDE_SAMPLE) && *w.guide.usable != 0u;
 					}
 				}
 			}
@@ -1023,7 +1173,7 @@ __device__ bool vol_continue(const scene_view& s, const wave_buffers& w, const w
 			// sample_medium_interaction (integrator.cpp:408-421): the phase value is its pdf, beta stays;
 			// guided: one-sample MIS of the medium guide and the phase function
 			const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && w.guide_medium.query_out != nullptr &&
-				w.guide_medium.dstate->usable != 0u;
+				*w.guide_medium.usable != 0u;
 			if (use_guide) {
 				const float* g = reinterpret_cast<const float*>(w.guide_medium.query_out + 12 * i);
 				const float alpha = g[guide::kAlphaOff];
@@ -1052,7 +1202,7 @@ __device__ bool vol_continue(const scene_view& s, const wave_buffers& w, const w
 				record_vertex(w.guide_medium, i, wi, pb, beta0, L0);
 		} else {
 			const bool use_guide = (p.guide_flags & GUIDE_SAMPLE) && rec.guidable && w.guide.query_out != nullptr &&
-				w.guide.dstate->usable != 0u;
+				*w.guide.usable != 0u;
 			const bool ok = use_guide
 				? continue_guided<MAT_ANY>(s, st, rec, reinterpret_cast<const float*>(w.guide.query_out + 12 * i), wi, pb)
 				: continue_bsdf<MAT_ANY>(s, st, rec, wi, pb);
@@ -1095,11 +1245,12 @@ __global__ void k_advance(uint32_t* counters);
 
 // Traversal kernels keep their stacks in dynamic shared memory; above 48 KB a
 // block needs the kernel's opt-in.
-// They also ask for the largest shared-memory carve-out, so that four blocks
-// of 256 threads with their stacks fit on one SM.
+// They also set their preferred shared-memory carve-out (percent of the
+// combined L1 / shared storage): the largest share fits four blocks of 256
+// threads with their stacks, smaller shares leave more L1 for tree nodes.
 template <typename Kernel>
-cudaError_t allow_smem(Kernel kernel, size_t bytes) {
-	cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+cudaError_t allow_smem(Kernel kernel, size_t bytes, int carveout = 100) {
+	cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
 	if (e != cudaSuccess || bytes <= 48u * 1024u) return e;
 	return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
@@ -1108,11 +1259,15 @@ template <bool COUNT>
 cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t queue_in, const launch_cfg& cfg,
 	cudaStream_t stream) {
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
-	cudaError_t e = allow_smem(k_extend<COUNT, true, false>, smem);
-	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, false>, smem);
-	if (e == cudaSuccess) e = allow_smem(k_beam<COUNT>, smem);
+	const bool refill = !COUNT && cfg.refill;
+	cudaError_t e = allow_smem(k_extend<COUNT, true, false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_beam<COUNT>, smem, cfg.carveout);
+	if (e == cudaSuccess && refill) e = allow_smem(k_extend_refill<true, false>, smem, cfg.carveout);
+	if (e == cudaSuccess && refill) e = allow_smem(k_secondary_refill<false>, smem, cfg.carveout);
 	if (e != cudaSuccess) return e;
-	k_extend<COUNT, true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	if (refill) k_extend_refill<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	else k_extend<COUNT, true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	k_shade_a<CLASS_LAMBERT, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_METAL, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_GLASS_ROUGH, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
@@ -1120,12 +1275,13 @@ cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t q
 	k_shade_a<CLASS_MISS, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a_medium<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	if (cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
-		e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
+		e = guide::launch_forward_queue(*cfg.guide, w.guide, w.counters + CNT_GUIDE, stream);
 		if (e == cudaSuccess && cfg.guide_medium != nullptr)
-			e = guide::launch_forward_queue(*cfg.guide_medium, w.counters + CNT_GUIDE_MEDIUM, stream);
+			e = guide::launch_forward_queue(*cfg.guide_medium, w.guide_medium, w.counters + CNT_GUIDE_MEDIUM, stream);
 		if (e != cudaSuccess) return e;
 	}
-	k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	if (refill) k_secondary_refill<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	else k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_direct<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_beam<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_continue<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -1144,6 +1300,8 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_BEAM] = 0u;
 	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
 	counters[CNT_TAIL] = 0u;
+	counters[CNT_FETCH_EXTEND] = 0u;
+	counters[CNT_FETCH_SECONDARY] = 0u;
 }
 
 // Moves the wave window forward so the next replay of the same graph renders
@@ -1158,13 +1316,17 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	const launch_cfg& cfg, cudaStream_t stream) {
 	if (!BATCH && cfg.volume) return volume_bounce<COUNT>(s, w, queue_in, cfg, stream);
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
-	cudaError_t e = allow_smem(k_extend<COUNT, false, BATCH>, smem);
-	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, BATCH>, smem);
+	const bool refill = !COUNT && cfg.refill;
+	cudaError_t e = allow_smem(k_extend<COUNT, false, BATCH>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, BATCH>, smem, cfg.carveout);
+	if (e == cudaSuccess && refill) e = allow_smem(k_extend_refill<false, BATCH>, smem, cfg.carveout);
+	if (e == cudaSuccess && refill) e = allow_smem(k_secondary_refill<BATCH>, smem, cfg.carveout);
 	if (e != cudaSuccess) return e;
 	const bool timed = cfg.events != nullptr && *cfg.next_event + 2 <= cfg.max_events;
 	uint32_t ev = timed ? *cfg.next_event : 0u;
 	if (timed) { cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 0; }
-	k_extend<COUNT, false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	if (refill) k_extend_refill<false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	else k_extend<COUNT, false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
 	if (cfg.sort == RB_SORT_MATERIAL) {
 		k_shade_a<CLASS_LAMBERT, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
@@ -1174,11 +1336,12 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	k_shade_a<CLASS_OTHER, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_MISS, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	if (!BATCH && cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE)) {
-		e = guide::launch_forward_queue(*cfg.guide, w.counters + CNT_GUIDE, stream);
+		e = guide::launch_forward_queue(*cfg.guide, w.guide, w.counters + CNT_GUIDE, stream);
 		if (e != cudaSuccess) return e;
 	}
 	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
-	k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	if (refill) k_secondary_refill<BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	else k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
 	if (cfg.sort == RB_SORT_MATERIAL) {
 		k_shade_b<CLASS_LAMBERT, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -1232,10 +1395,10 @@ cudaError_t launch_tail(const scene_view& s, const wave_buffers& w, uint32_t que
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	cudaError_t e;
 	if (cfg.count) {
-		e = allow_smem(k_tail<true, BATCH>, smem);
+		e = allow_smem(k_tail<true, BATCH>, smem, cfg.carveout);
 		if (e == cudaSuccess) k_tail<true, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
 	} else {
-		e = allow_smem(k_tail<false, BATCH>, smem);
+		e = allow_smem(k_tail<false, BATCH>, smem, cfg.carveout);
 		if (e == cudaSuccess) k_tail<false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
 	}
 	if (e != cudaSuccess) return e;
@@ -1281,10 +1444,12 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 	cudaStream_t stream) {
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
 	const guide::guide_state* guides[2] = {cfg.guide, cfg.guide_medium};
+	const guide::wave_guide* wgs[2] = {&w.guide, &w.guide_medium};
 	cudaError_t e = cudaSuccess;
-	for (const guide::guide_state* g : guides)
-		if (train && g != nullptr && e == cudaSuccess)
-			e = guide::launch_collect(*g, w.result, &w.params->first_item, &w.params->total_items, w.capacity, stream);
+	for (int k = 0; k < 2; k++)
+		if (train && guides[k] != nullptr && e == cudaSuccess)
+			e = guide::launch_collect(*guides[k], *wgs[k], w.result, &w.params->first_item, &w.params->total_items, w.capacity,
+				stream);
 	if (e == cudaSuccess) e = launch_next_wave(w, f, grid, stream);
 	for (const guide::guide_state* g : guides)
 		if (train && g != nullptr)

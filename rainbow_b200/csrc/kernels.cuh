@@ -27,7 +27,9 @@ enum : uint32_t {
 	CNT_BEAM_RAYS = 22,  // closest-hit queries of the transmittance walks
 	CNT_TAIL = 24,       // paths taken from the active queue by the tail kernel (reset after it)
 	CNT_GUIDE_MEDIUM = 25,  // medium vertices queued for a medium-guide evaluation this bounce
-	CNT_WORDS = 26
+	CNT_FETCH_EXTEND = 26,  // rays taken from the active queue by the persistent extend kernel
+	CNT_FETCH_SECONDARY = 27,  // rays taken from the secondary queue by the persistent secondary kernel
+	CNT_WORDS = 28
 };
 static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
 // words cleared at the start of a wave: everything before the 64-bit stats
@@ -156,6 +158,8 @@ struct launch_cfg {
 	bool batch = false;      // many scenes per wave (wave_buffers::batch)
 	uint32_t sort = 0;       // hit queues: 0 one per material class, 1 a single queue (no sorting)
 	uint32_t tail = 0xffffffffu;  // bounces of separate stages before the tail kernel (>= max_depth: none)
+	bool refill = false;     // traversal kernels: persistent lanes that take a new ray when theirs is done
+	int carveout = 100;      // traversal kernels' preferred shared-memory carve-out, percent
 };
 
 // Ray batches for rb_trace_closest / rb_trace_shadow.

@@ -221,94 +221,132 @@ RB_HD bool slab_pass(float ax, float ay, float az, float bx, float by, float bz,
 template <typename T>
 RB_HD T pick4(T a, T b, T c, T d, uint32_t i) { return i == 0 ? a : i == 1 ? b : i == 2 ? c : d; }
 
-template <bool SHADOW, typename Stack>
-RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack) {
-	const vec3 inv = 1.f / d;
-	const uint32_t neg = (inv.x < 0.f ? 1u : 0u) | (inv.y < 0.f ? 2u : 0u) | (inv.z < 0.f ? 4u : 0u);
-	hit.slot = -1;
-	uint32_t cur_entity = 0xffffffffu;
-	local_ray lr{};
+// Traversal state of one ray, so that a thread can advance it a step at a
+// time (and take a new ray as soon as its ray is done).
+struct trav_state {
+	vec3 o, d, inv;
+	uint32_t neg;        // direction sign bits (x: 1, y: 2, z: 4)
+	float len;
+	hit_t hit;
+	uint32_t cur;        // next node or leaf to visit
+	uint32_t cur_entity;
+	local_ray lr;
+};
+
+// Starts a ray: the root box test of the reference. Returns false when the ray
+// is already done (the root box is missed).
+template <typename Stack>
+RB_HD bool trav_begin(const scene_view& s, trav_state& t, vec3 o, vec3 d, float len, Stack& stack) {
+	t.o = o;
+	t.d = d;
+	t.inv = 1.f / d;
+	t.neg = (t.inv.x < 0.f ? 1u : 0u) | (t.inv.y < 0.f ? 2u : 0u) | (t.inv.z < 0.f ? 4u : 0u);
+	t.len = len;
+	t.hit.slot = -1;
+	t.hit.b1 = t.hit.b2 = 0.f;
+	t.cur_entity = 0xffffffffu;
+	t.lr = local_ray{};
 	stack.reset();
 	float te;
-	if (!slab_pass(s.root_a.x, s.root_a.y, s.root_a.z, s.root_a.w, s.root_b.x, s.root_b.y, o, inv, len, te)) return 1;
-	uint32_t cur = s.root_ref;
-	for (;;) {
-		if (cur & kRefLeaf) {
-			const uint32_t first = cur & 0x00ffffffu, count = (cur >> 24) & 0x7fu;
-			for (uint32_t k = 0; k < count; k++) {
-				const uint32_t slot = first + k;
-				const float2 tc = RB_LDG(s.tri_c + slot);
-				const uint32_t ew = float_as_u32(tc.y);
-				if (SHADOW && (ew & kEntityInvisible)) continue;
-				const uint32_t ent = ew & ~kEntityInvisible;
-				const float4 ta = RB_LDG(s.tri_a + slot);
-				const float4 tb = RB_LDG(s.tri_b + slot);
-				if (ent != cur_entity) {
-					cur_entity = ent;
-					lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
-				}
-				float t, b1, b2;
-				if (triangle_hit(lr.o, lr.d, len * lr.to_local, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y},
-						vec3{tb.z, tb.w, tc.x}, t, b1, b2)) {
-					len = t * lr.to_world;
-					hit.slot = static_cast<int32_t>(slot);
-					hit.b1 = b1;
-					hit.b2 = b2;
-					if (isnan(len)) return -1;
-				}
+	if (!slab_pass(s.root_a.x, s.root_a.y, s.root_a.z, s.root_a.w, s.root_b.x, s.root_b.y, o, t.inv, len, te)) return false;
+	t.cur = s.root_ref;
+	return true;
+}
+
+// One step of a started ray: the current leaf's triangles or the current
+// node's four slots, then the next node (descent or pop). Returns 0 while the
+// ray goes on, 1 when it is done, -1 when it must be redone in the reference's
+// order (a NaN length or a full stack).
+template <bool SHADOW, typename Stack>
+RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
+	if (t.cur & kRefLeaf) {
+		const uint32_t first = t.cur & 0x00ffffffu, count = (t.cur >> 24) & 0x7fu;
+		for (uint32_t k = 0; k < count; k++) {
+			const uint32_t slot = first + k;
+			const float2 tc = RB_LDG(s.tri_c + slot);
+			const uint32_t ew = float_as_u32(tc.y);
+			if (SHADOW && (ew & kEntityInvisible)) continue;
+			const uint32_t ent = ew & ~kEntityInvisible;
+			const float4 ta = RB_LDG(s.tri_a + slot);
+			const float4 tb = RB_LDG(s.tri_b + slot);
+			if (ent != t.cur_entity) {
+				t.cur_entity = ent;
+				t.lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, t.o, t.d);
 			}
-		} else {
-			const node4* nd = s.wnodes + cur;
-			const float4 lx = RB_LDG(&nd->lo_x), ly = RB_LDG(&nd->lo_y), lz = RB_LDG(&nd->lo_z);
-			const float4 hx = RB_LDG(&nd->hi_x), hy = RB_LDG(&nd->hi_y), hz = RB_LDG(&nd->hi_z);
-			const uint4 rf = RB_LDG(&nd->ref);
-			const uint32_t meta = RB_LDG(&nd->meta.x);
-			float t0, t1, t2, t3;
-			uint32_t pass = 0;
-			if ((meta & 0x100u) && slab_pass(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, len, t0)) pass |= 1u;
-			if ((meta & 0x200u) && slab_pass(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, len, t1)) pass |= 2u;
-			if ((meta & 0x400u) && slab_pass(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, len, t2)) pass |= 4u;
-			if ((meta & 0x800u) && slab_pass(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, len, t3)) pass |= 8u;
-			if (pass != 0u) {
-				// the reference's order: near pair first, near slot first within each pair
-				const uint32_t pf = (neg >> (meta & 3u)) & 1u;
-				const uint32_t ax_first = (meta >> (2u + 2u * pf)) & 3u, ax_second = (meta >> (2u + 2u * (pf ^ 1u))) & 3u;
-				const uint32_t o0 = 2u * pf + ((neg >> ax_first) & 1u);
-				const uint32_t o2 = 2u * (pf ^ 1u) + ((neg >> ax_second) & 1u);
-				const uint32_t order = o0 | ((o0 ^ 1u) << 2) | (o2 << 4) | ((o2 ^ 1u) << 6);
-				// walk the order backwards: every passing slot but the first is pushed,
-				// later ones first, so they pop in order
-				uint32_t next = 0xffffffffu;
-				float next_te = 0.f;
+			float th, b1, b2;
+			if (triangle_hit(t.lr.o, t.lr.d, t.len * t.lr.to_local, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y},
+					vec3{tb.z, tb.w, tc.x}, th, b1, b2)) {
+				t.len = th * t.lr.to_world;
+				t.hit.slot = static_cast<int32_t>(slot);
+				t.hit.b1 = b1;
+				t.hit.b2 = b2;
+				if (isnan(t.len)) return -1;
+			}
+		}
+	} else {
+		const node4* nd = s.wnodes + t.cur;
+		const float4 lx = RB_LDG(&nd->lo_x), ly = RB_LDG(&nd->lo_y), lz = RB_LDG(&nd->lo_z);
+		const float4 hx = RB_LDG(&nd->hi_x), hy = RB_LDG(&nd->hi_y), hz = RB_LDG(&nd->hi_z);
+		const uint4 rf = RB_LDG(&nd->ref);
+		const uint32_t meta = RB_LDG(&nd->meta.x);
+		float t0, t1, t2, t3;
+		uint32_t pass = 0;
+		if ((meta & 0x100u) && slab_pass(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, t.o, t.inv, t.len, t0)) pass |= 1u;
+		if ((meta & 0x200u) && slab_pass(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, t.o, t.inv, t.len, t1)) pass |= 2u;
+		if ((meta & 0x400u) && slab_pass(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, t.o, t.inv, t.len, t2)) pass |= 4u;
+		if ((meta & 0x800u) && slab_pass(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, t.o, t.inv, t.len, t3)) pass |= 8u;
+		if (pass != 0u) {
+			// the reference's order: near pair first, near slot first within each pair
+			const uint32_t pf = (t.neg >> (meta & 3u)) & 1u;
+			const uint32_t ax_first = (meta >> (2u + 2u * pf)) & 3u, ax_second = (meta >> (2u + 2u * (pf ^ 1u))) & 3u;
+			const uint32_t o0 = 2u * pf + ((t.neg >> ax_first) & 1u);
+			const uint32_t o2 = 2u * (pf ^ 1u) + ((t.neg >> ax_second) & 1u);
+			const uint32_t order = o0 | ((o0 ^ 1u) << 2) | (o2 << 4) | ((o2 ^ 1u) << 6);
+			// walk the order backwards: every passing slot but the first is pushed,
+			// later ones first, so they pop in order
+			uint32_t next = 0xffffffffu;
+			float next_te = 0.f;
+#if defined(__CUDA_ARCH__)
 #pragma unroll
-				for (int k = 3; k >= 0; k--) {
-					const uint32_t sl = (order >> (2 * k)) & 3u;
-					if (!((pass >> sl) & 1u)) continue;
-					if (next != 0xffffffffu) {
-						if (stack.full()) return -1;
-						stack.push(next, next_te);
-					}
-					next = pick4(rf.x, rf.y, rf.z, rf.w, sl);
-					next_te = pick4(t0, t1, t2, t3, sl);
+#endif
+			for (int k = 3; k >= 0; k--) {
+				const uint32_t sl = (order >> (2 * k)) & 3u;
+				if (!((pass >> sl) & 1u)) continue;
+				if (next != 0xffffffffu) {
+					if (stack.full()) return -1;
+					stack.push(next, next_te);
 				}
-				cur = next;
-				continue;
+				next = pick4(rf.x, rf.y, rf.z, rf.w, sl);
+				next_te = pick4(t0, t1, t2, t3, sl);
 			}
+			t.cur = next;
+			return 0;
 		}
-		// pop the next slot whose box still passes at the current length
-		bool found = false;
-		while (!stack.empty()) {
-			uint32_t ref;
-			float tent;
-			stack.pop(ref, tent);
-			if (!(tent > len)) {
-				cur = ref;
-				found = true;
-				break;
-			}
-		}
-		if (!found) return 1;
 	}
+	// pop the next slot whose box still passes at the current length
+	while (!stack.empty()) {
+		uint32_t ref;
+		float tent;
+		stack.pop(ref, tent);
+		if (!(tent > t.len)) {
+			t.cur = ref;
+			return 0;
+		}
+	}
+	return 1;
+}
+
+template <bool SHADOW, typename Stack>
+RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack) {
+	trav_state t;
+	int r = 1;
+	if (trav_begin(s, t, o, d, len, stack)) {
+		do r = trav_step<SHADOW>(s, t, stack);
+		while (r == 0);
+	}
+	len = t.len;
+	hit = t.hit;
+	return r;
 }
 
 // ------------------------------------------------------------------ surface interaction

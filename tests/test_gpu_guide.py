@@ -210,3 +210,30 @@ def test_trained_guide_reduces_error(ctx):
     ctx.render(scene.camera, 1024, max_depth=depth, seed=11, guide=True, train=True, paths_per_wave=res * res * 32)
     guided = [relmse(ctx.render(scene.camera, 256, max_depth=depth, seed=s, guide=True)) for s in (7, 8)]
     assert np.mean(guided) < 0.8 * np.mean(plain), (guided, plain)
+
+
+def test_guided_lanes_unbiased_and_plain_before_training():
+    """Guided rendering on wave lanes (each lane samples a snapshot of the
+    weights taken after its previous wave trained): identical to plain before
+    any training, unbiased after online training on lanes."""
+    res, B = 32, 4
+    scene = _slit(res)
+    with rb.Context(0) as c:
+        c.upload(scene)
+        c.set_tuning(lanes=3, paths_per_wave=res * res * 4)
+        c.guide_init(seed=0)
+        plain = c.render(scene.camera, 16, max_depth=6, seed=5)
+        assert np.array_equal(plain, c.render(scene.camera, 16, max_depth=6, seed=5, guide=True))
+        c.render(scene.camera, 65536, max_depth=6, seed=100, want_image=False)
+        ref, ref_var = _film_mean_var(c)
+        c.guide_init(seed=0, batch_size=16384, min_rows=1024, steps_per_wave=4)
+        c.set_tuning(lanes=2, paths_per_wave=res * res * 64)
+        c.render(scene.camera, 2048, max_depth=6, seed=7, guide=True, train=True, want_image=False)
+        assert c.guide_stats().steps >= 64 and c.guide_stats().device_error == 0
+        c.render(scene.camera, 8192, max_depth=6, seed=9, guide=True, want_image=False)
+        m, var = _film_mean_var(c)
+    blk = lambda a: a.reshape(res // B, B, res // B, B, 3).mean((1, 3))
+    zb = (blk(m) - blk(ref)) / np.sqrt((var + ref_var).reshape(res // B, B, res // B, B, 3).sum((1, 3)) / B ** 4 + 1e-12)
+    assert abs(zb.mean()) < 0.3, zb.mean()
+    assert np.mean(np.abs(zb) > 4) < 0.02, np.mean(np.abs(zb) > 4)
+    assert abs(m.mean() / ref.mean() - 1) < 0.005, m.mean() / ref.mean()
