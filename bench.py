@@ -223,6 +223,68 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
             "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}
 
 
+def guided_waves(res=1024):
+    """Two plain waves, then three guided training waves (2 spp each) on the slit room: the
+    workload of the guide-network profile in profiles/."""
+    import rainbow_b200 as rb
+    scene = rb.generate_scene(GUIDED["kind"], seed=GUIDED["seed"], width=res, height=res,
+                              num_spheres=GUIDED["num_spheres"], subdivision=GUIDED["subdivision"])
+    ctx = rb.Context(0)
+    ctx.upload(scene)
+    out = {"plain_ms": [], "guided_ms": []}
+    for k in range(2):
+        ctx.render(scene.camera, 2, first_sample=2 * k, max_depth=8, seed=7, reset=(k == 0), paths_per_wave=res * res * 2,
+                   want_image=False)
+        out["plain_ms"].append(ctx.stats().elapsed_ms)
+    ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=1 << 18, steps_per_wave=8, min_rows=4096)
+    for k in range(3):
+        ctx.render(scene.camera, 2, first_sample=2 * k, max_depth=8, seed=7, reset=(k == 0), guide=True, train=True,
+                   paths_per_wave=res * res * 2, want_image=False)
+        out["guided_ms"].append(ctx.stats().elapsed_ms)
+    out["adam_steps"] = ctx.guide_stats().steps
+    ctx.close()
+    print(json.dumps(out))
+    return 0
+
+
+def config1_leg(rb, device, threads):
+    """Configuration 1 as specified: the box room, 256 x 256, 16 spp, depth 5, one render call on the GPU,
+    and the same render by the reference CPU integrator (oracle/_ref) on all host cores."""
+    scene = rb.generate_scene(rb.RB_SCENE_BOX, seed=0, width=256, height=256)
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    ctx.render(scene.camera, 16, max_depth=5, seed=1, want_image=False)  # warm-up (graph capture)
+    best = min((ctx.render(scene.camera, 16, max_depth=5, seed=2 + k, want_image=False), ctx.stats().elapsed_ms)[1]
+               for k in range(3))
+    ctx.close()
+    samples = 256 * 256 * 16
+    out = {"workload": "box room, 32 triangles, 256x256, 16 spp, max depth 5", "gpu_msamples_per_s": samples / best / 1e3,
+           "gpu_ms": best}
+    try:
+        from oracle import ref
+        if ref.available():
+            _, _, sec = ref.RefScene(scene).render(16, 0, 5, 1.0, 0, threads)
+            out.update(cpu_reference_msamples_per_s=samples / sec / 1e6, cpu_reference_s=sec, cpu_cores=threads)
+    except Exception as e:  # reported, never required
+        out["cpu_reference_error"] = str(e)
+    return out
+
+
+def spheres_s5_leg(rb, device, spp=8):
+    """The sphere field at icosphere subdivision 5 (200 spheres, 4,096,002 triangles): one call of `spp`
+    samples per pixel with autotuned launch shapes."""
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=1024, height=1024, num_spheres=200, subdivision=5)
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    t, _ = ctx.tune_render(scene.camera, probe_spp=2, max_depth=8, seed=90)
+    ctx.render(scene.camera, spp, max_depth=8, seed=3, want_image=False)
+    st = ctx.stats()
+    ctx.close()
+    return {"workload": f"sphere field, {scene.num_triangles} triangles (subdivision 5), 1024x1024, {spp} spp, depth 8",
+            "msamples_per_s": 1024 * 1024 * spp / st.elapsed_ms / 1e3,
+            "mrays_per_s": (st.extend_rays + st.shadow_rays + st.mis_rays) / st.elapsed_ms / 1e3, "tuning": t.as_dict()}
+
+
 def batch_workload(seed=2, count=64):
     """The batched configuration: `count` seeded sphere scenes whose triangle counts are
     log-uniform in [1k, 500k] (displaced icospheres: subdivision and sphere count chosen
@@ -280,12 +342,16 @@ def main():
     ap.add_argument("--guided-ref-spp", type=int, default=4096)
     ap.add_argument("--guided-chunk", type=int, default=2)
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--guided-waves", action="store_true",
+                    help="only render 2 plain then 3 guided training waves of 2 spp on the slit room (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tuning", default=None, help="launch shapes as JSON (skips the autotuner), e.g. "
                     "'{\"block_trace\": 256, \"grid_per_sm\": 16}'")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.guided_waves:
+        return guided_waves()
 
     import torch
     import torch.distributed as dist
@@ -416,6 +482,15 @@ def main():
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_batched:
+        for name, leg in (("config1", lambda: config1_leg(rb, local, os.cpu_count() or 1)),
+                          ("spheres_s5", lambda: spheres_s5_leg(rb, local))):
+            try:
+                extra[name] = leg()
+            except Exception as e:  # reported, never required for the throughput line
+                extra[name] = {"error": str(e)}
+
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         try:
@@ -444,7 +519,7 @@ def main():
                          "algorithmic_bytes_per_launch": alg_bytes / nl, "ms_per_launch": trav_ms / nl,
                          "launches": nl},
             "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches, "tuning": tuning,
-            "batched": batched, "guided": guided,
+            "batched": batched, "guided": guided, **extra,
         }
         print(json.dumps(line))
     ctx.close()
