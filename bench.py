@@ -153,7 +153,8 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_dict(world, l2="n/a (CPU)"),
+        "config": config_dict(world, l2="n/a (CPU)", timing="each step: the reference integrator on a band of image "
+                                                            "rows, wall clock, all host threads"),
         "cpu_baseline": {"value": value, "unit": "Msamples/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -161,11 +162,11 @@ def run_reference_arm(args):
 
 
 def config_dict(world, l2="flushed before the timed call; per-step inputs exceed L2 (paths of a wave 0.45-1.8 GB, "
-                             "film 59 MB; the 86 MB scene stays resident across steps as in any multi-sample render)"):
+                             "film 59 MB; the 86 MB scene stays resident across steps as in any multi-sample render)",
+                timing="K steps = one rb_render call of K samples per pixel, CUDA events on the library's stream"):
     return {"workload": "sphere field, 1,024,010 triangles, 1024x1024, 1 spp per step, max depth 8",
             "triangles": 1024010, "width": WORKLOAD["width"], "height": WORKLOAD["height"],
-            "max_depth": WORKLOAD["max_depth"], "spp_per_step": 1,
-            "timing": "K steps = one rb_render call of K samples per pixel, CUDA events on the library's stream",
+            "max_depth": WORKLOAD["max_depth"], "spp_per_step": 1, "timing": timing,
             "parallelism": f"replicas x{world} (sample ranges)", "l2": l2}
 
 

@@ -323,7 +323,10 @@ rb_status rb_checkpoint_load(rb_context* ctx, const char* path);
  * queues. Every setting gives the same image; only the speed changes. */
 enum {
 	RB_SORT_MATERIAL = 0,       /* one hit queue per material class (coherent shading warps) */
-	RB_SORT_NONE = 1            /* one hit queue for every surface hit (no sorting) */
+	RB_SORT_NONE = 1,           /* one hit queue for every surface hit (no sorting) */
+	RB_SORT_RAYS = 2            /* material-class hit queues, and before every bounce's traversal the active
+	                               paths binned by ray direction octant and a Morton cell of the origin
+	                               (coherent traversal warps) */
 };
 enum {
 	RB_TRAVERSAL_PER_THREAD = 0, /* one ray per thread, traced to the end (grid-stride) */
@@ -514,6 +517,17 @@ rb_status rb_scene_generate(const rb_scene_gen_params* params, rb_scene** out);
 /* Pointers stay valid until rb_scene_free. bvh is left empty (num_nodes == 0). */
 rb_status rb_scene_get(const rb_scene* scene, rb_scene_desc* desc, rb_camera_desc* camera);
 void rb_scene_free(rb_scene* scene);
+
+/* ------------------------------------------------------------------ failure detection (no reference counterpart)
+ * Device waits in this library are bounded: a wait that runs out sets an error
+ * word and returns, and the context stays usable. rb_check_bounded_wait runs
+ * one such wait (an mbarrier that nothing arrives on, the wait of the guide
+ * kernels) with a limit of limit_us microseconds and reports what the wait
+ * returned in *status (RB_ERR_DEVICE_TIMEOUT when it ran out). */
+rb_status rb_check_bounded_wait(rb_context* ctx, uint32_t limit_us, rb_status* status);
+/* Host-side fault injection: the `after`-th device allocation from now on
+ * fails as if the device were out of memory (after < 0: off). */
+void rb_inject_allocation_failure(int32_t after);
 
 /* Library ABI version (RBGPU_ABI_VERSION at build time). */
 int32_t rb_abi_version(void);

@@ -24,7 +24,7 @@ from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_RENDER_GUIDE,
     RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
-    RB_SORT_MATERIAL, RB_SORT_NONE, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,
+    RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,
     BvhDesc, CameraDesc, MediaDesc, MediumDesc,
     GuideConfig, GuideStats, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
 )
@@ -343,6 +343,19 @@ class Context:
         img = np.zeros((h, w, 3), dtype=np.float32)
         check(lib().rb_batch_image(self._h, scene, img.ctypes.data), "rb_batch_image")
         return img
+
+
+    # ---- failure detection
+    def check_bounded_wait(self, limit_us: int) -> int:
+        """Runs one bounded device wait that nothing completes; returns the status it led to."""
+        st = C.c_int32()
+        check(lib().rb_check_bounded_wait(self._h, limit_us, C.byref(st)), "rb_check_bounded_wait")
+        return st.value
+
+
+def inject_allocation_failure(after: int) -> None:
+    """The `after`-th device allocation from now on fails as out-of-memory (after < 0: off)."""
+    lib().rb_inject_allocation_failure(after)
 
 
 class PathIntegrator:

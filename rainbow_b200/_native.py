@@ -33,7 +33,7 @@ RB_GUIDE_NUM_PARAMS = 30000
 RB_GUIDE_INPUTS = 9
 RB_GUIDE_OUTPUTS = 48
 RB_BVH_LEAF_FLAG = 0x80000000
-RB_SORT_MATERIAL, RB_SORT_NONE = 0, 1
+RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS = 0, 1, 2
 RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL = 0, 1
 
 F16 = C.c_float * 16
@@ -184,6 +184,8 @@ SIGNATURES = {
     "rb_guide_sample_dirs": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "rb_guide_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GuideStats)]),
     "rb_guide_medium_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GuideStats)]),
+    "rb_check_bounded_wait": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_int32)]),
+    "rb_inject_allocation_failure": (None, [C.c_int32]),
     "rb_set_tuning": (C.c_int32, [C.c_void_p, C.POINTER(Tuning)]),
     "rb_get_tuning": (C.c_int32, [C.c_void_p, C.POINTER(Tuning)]),
     "rb_tune_render": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_uint32, C.POINTER(Tuning),

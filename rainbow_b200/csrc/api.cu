@@ -34,6 +34,10 @@ cudaError_t alloc_wave_buffers(gpu::wave_buffers& w, size_t n) {
 	take(&w.sec_o, 2 * n); take(&w.sec_d, 2 * n); take(&w.sec_hit, 2 * n); take(&w.queue[0], n); take(&w.queue[1], n);
 	take(&w.sec_queue, 2 * n);
 	take(&w.class_queue, static_cast<size_t>(pt::NUM_CLASSES) * n);
+	take(&w.sort_keys, n);
+	take(&w.sort_tmp, n);
+	take(&w.sort_bins, 2 * gpu::kSortBins);
+	if (e == cudaSuccess) e = cudaMemset(w.sort_bins, 0, 2 * gpu::kSortBins * sizeof(uint32_t));
 	return e;
 }
 
@@ -43,6 +47,14 @@ void free_wave_buffers(gpu::wave_buffers& w) {
 	dev_free(w.sec_o); dev_free(w.sec_d); dev_free(w.sec_hit); dev_free(w.queue[0]); dev_free(w.queue[1]);
 	dev_free(w.sec_queue);
 	dev_free(w.class_queue);
+	dev_free(w.sort_keys);
+	dev_free(w.sort_tmp);
+	dev_free(w.sort_bins);
+}
+
+std::atomic<int32_t>& allocation_countdown() {
+	static std::atomic<int32_t> countdown{-1};
+	return countdown;
 }
 
 rb_status ensure_wave(rb_context* c, uint32_t capacity) {
@@ -488,6 +500,8 @@ guide::guide_state* context_guide_medium(rb_context* c) { return &c->guide_mediu
 extern "C" {
 
 int32_t rb_abi_version(void) { return RBGPU_ABI_VERSION; }
+
+void rb_inject_allocation_failure(int32_t after) { allocation_countdown().store(after < 0 ? -1 : after); }
 
 const char* rb_status_string(rb_status s) {
 	switch (s) {

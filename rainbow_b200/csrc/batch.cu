@@ -156,7 +156,7 @@ rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning*
 	const uint32_t waves[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
 	const uint32_t blocks[] = {64u, 128u, 256u};
 	const uint32_t grids[] = {2u, 4u, 8u, 16u};
-	const uint32_t sorts[] = {RB_SORT_MATERIAL, RB_SORT_NONE};
+	const uint32_t sorts[] = {RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS};
 	const uint32_t tails[] = {1u, 2u, 3u, 4u, 6u, 64u};
 	const uint32_t lane_counts[] = {1u, 2u, 3u, 4u};
 	const uint32_t traversals[] = {RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL};

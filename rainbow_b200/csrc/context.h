@@ -6,6 +6,7 @@
 #include "host/scene_pack.h"
 #include "kernels.cuh"
 
+#include <atomic>
 #include <cstring>
 #include <utility>
 #include <vector>
@@ -14,10 +15,16 @@ namespace rb {
 namespace ctx {
 
 
+// Host-side allocation-failure injection (rb_inject_allocation_failure): the
+// countdown of device allocations until one fails, < 0 when off.
+std::atomic<int32_t>& allocation_countdown();
+
 template <typename T>
 inline cudaError_t dev_alloc(T** p, size_t count) {
 	*p = nullptr;
 	if (count == 0) return cudaSuccess;
+	std::atomic<int32_t>& fail = allocation_countdown();
+	if (fail.load() >= 0 && fail.fetch_sub(1) == 0) return cudaErrorMemoryAllocation;
 	return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
 }
 template <typename T>
@@ -104,7 +111,7 @@ inline rb_tuning resolved_tuning(const rb_tuning& t) {
 }
 inline bool valid_tuning(const rb_tuning& t) {
 	auto block_ok = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 256 && b % 32 == 0); };
-	return block_ok(t.block_trace) && block_ok(t.block_shade) && t.grid_per_sm <= 64 && t.sort <= RB_SORT_NONE &&
+	return block_ok(t.block_trace) && block_ok(t.block_shade) && t.grid_per_sm <= 64 && t.sort <= RB_SORT_RAYS &&
 		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= 4 && t.traversal <= RB_TRAVERSAL_REFILL &&
 		t.smem_carveout <= 101;
 }

@@ -784,6 +784,25 @@ __global__ void k_snapshot(const uint4* __restrict__ image, uint4* __restrict__ 
 	if (i == 0) *usable = s->usable;
 }
 
+// A bounded wait that is meant to run out: an mbarrier that nothing arrives
+// on, waited for with mbar_wait (the wait of every guide kernel). Writes the
+// status the wait leads to.
+__global__ void k_bounded_wait(uint64_t limit_ns, uint32_t* status) {
+	__shared__ __align__(8) uint64_t bar;
+	if (threadIdx.x == 0) {
+		mbar_init(&bar, 1);
+		fence_mbar_init();
+	}
+	__syncthreads();
+	const bool arrived = mbar_wait(&bar, 0, limit_ns);
+	if (threadIdx.x == 0) *status = arrived ? RB_OK : RB_ERR_DEVICE_TIMEOUT;
+}
+
+cudaError_t launch_bounded_wait(uint64_t limit_ns, uint32_t* status, cudaStream_t s) {
+	k_bounded_wait<<<1, 32, 0, s>>>(limit_ns, status);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_snapshot(const guide_state& g, const lane_guide& l, cudaStream_t s) {
 	static_assert(kImageBytes % 16 == 0, "the image is copied in 16-byte units");
 	const uint32_t n16 = kImageBytes / 16;

@@ -196,6 +196,22 @@ rb_status rb_guide_init(rb_context* ctx, const rb_guide_config* config) {
 	return init_state(*gc.g, config, gc.sms, gc.stream);
 }
 
+rb_status rb_check_bounded_wait(rb_context* ctx, uint32_t limit_us, rb_status* status) {
+	if (status == nullptr || limit_us == 0 || limit_us > 10000000u) return RB_ERR_INVALID_ARGUMENT;
+	guide_ctx gc;
+	const rb_status st = open_guide(ctx, gc, false);
+	if (st != RB_OK) return st;
+	scratch<uint32_t> d;
+	RB_CUDA(d.alloc(1));
+	RB_CUDA(cudaMemsetAsync(d.p, 0xff, sizeof(uint32_t), gc.stream));
+	RB_CUDA(launch_bounded_wait(static_cast<uint64_t>(limit_us) * 1000ull, d.p, gc.stream));
+	uint32_t h = 0;
+	RB_CUDA(cudaMemcpyAsync(&h, d.p, sizeof(h), cudaMemcpyDeviceToHost, gc.stream));
+	RB_CUDA(cudaStreamSynchronize(gc.stream));
+	*status = static_cast<rb_status>(h);
+	return RB_OK;
+}
+
 rb_status rb_guide_medium_stats_get(rb_context* ctx, rb_guide_stats* out) {
 	if (ctx == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
 	guide_ctx gc;

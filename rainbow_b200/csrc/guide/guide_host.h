@@ -97,6 +97,8 @@ void release_lane(lane_guide& l);
 wave_guide state_view(const guide_state& g);
 // A lane's buffers and snapshots.
 wave_guide lane_view(const guide_state& g, const lane_guide& l);
+// One bounded mbarrier wait that nothing completes (failure-detection check).
+cudaError_t launch_bounded_wait(uint64_t limit_ns, uint32_t* status, cudaStream_t s);
 // Copies the training image and the usable flag into the lane's snapshots.
 cudaError_t launch_snapshot(const guide_state& g, const lane_guide& l, cudaStream_t s);
 

@@ -508,6 +508,92 @@ __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, ui
 	}
 }
 
+// ------------------------------------------------------------------ ray binning
+// RB_SORT_RAYS: before a bounce's traversal the active queue is reordered by a
+// 12-bit key, the ray direction's octant over an 8x8x8 Morton cell of its
+// origin in the scene box, with a counting sort (per-block histograms, one scan,
+// warp-aggregated scatter). Rays of a warp then start near each other in the
+// same direction, which keeps their traversals together and their nodes in
+// cache. Only the order of the queue changes, never a path's arithmetic.
+__device__ __forceinline__ uint32_t ray_bin(const wave_params& p, float4 o, float4 d) {
+	const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+	const float v[3] = {o.x, o.y, o.z};
+	uint32_t morton = 0;
+	for (int j = 0; j < 3; j++) {
+		const float u = (v[j] - p.box_min[j]) * p.box_inv[j] * 8.f;
+		const uint32_t c = u > 0.f ? (u < 7.f ? static_cast<uint32_t>(u) : 7u) : 0u;  // NaN and negatives: cell 0
+		for (int b = 0; b < 3; b++) morton |= ((c >> b) & 1u) << (3 * b + j);
+	}
+	return (oct << 9) | morton;
+}
+
+__global__ void __launch_bounds__(256) k_bin_count(wave_buffers w, uint32_t queue_in) {
+	__shared__ uint32_t hist[kSortBins];
+	for (uint32_t b = threadIdx.x; b < kSortBins; b += blockDim.x) hist[b] = 0u;
+	__syncthreads();
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t i = q[k];
+		const uint32_t key = ray_bin(p, w.ray_o[i], w.ray_d[i]);
+		w.sort_keys[k] = key;
+		atomicAdd(&hist[key], 1u);
+	}
+	__syncthreads();
+	for (uint32_t b = threadIdx.x; b < kSortBins; b += blockDim.x)
+		if (hist[b] != 0u) atomicAdd(w.sort_bins + b, hist[b]);
+}
+
+// One block of 1024 threads: exclusive prefix of the bin counts into the
+// cursors, counts cleared for the next bounce.
+__global__ void __launch_bounds__(1024) k_bin_scan(wave_buffers w) {
+	__shared__ uint32_t part[1024];
+	constexpr uint32_t per = kSortBins / 1024;
+	const uint32_t t = threadIdx.x;
+	uint32_t c[per], sum = 0;
+	for (uint32_t j = 0; j < per; j++) {
+		c[j] = w.sort_bins[t * per + j];
+		sum += c[j];
+	}
+	part[t] = sum;
+	__syncthreads();
+	for (uint32_t off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan of the per-thread sums
+		const uint32_t v = t >= off ? part[t - off] : 0u;
+		__syncthreads();
+		part[t] += v;
+		__syncthreads();
+	}
+	uint32_t run = part[t] - sum;
+	for (uint32_t j = 0; j < per; j++) {
+		w.sort_bins[kSortBins + t * per + j] = run;
+		w.sort_bins[t * per + j] = 0u;
+		run += c[j];
+	}
+}
+
+__global__ void __launch_bounds__(256) k_bin_scatter(wave_buffers w, uint32_t queue_in) {
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	const uint32_t* q = w.queue[queue_in];
+	uint32_t* cursor = w.sort_bins + kSortBins;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		const uint32_t key = k < n ? w.sort_keys[k] : 0xffffffffu;
+		const uint32_t peers = __match_any_sync(0xffffffffu, key);
+		const uint32_t leader = __ffs(peers) - 1;
+		uint32_t pos = 0;
+		if ((threadIdx.x & 31u) == leader && key != 0xffffffffu) pos = atomicAdd(cursor + key, static_cast<uint32_t>(__popc(peers)));
+		pos = __shfl_sync(0xffffffffu, pos, leader);
+		if (k < n) w.sort_tmp[pos + __popc(peers & lanemask_lt())] = q[k];
+	}
+}
+
+__global__ void __launch_bounds__(256) k_bin_copy(wave_buffers w, uint32_t queue_in) {
+	const uint32_t n = w.counters[CNT_ACTIVE];
+	uint32_t* q = w.queue[queue_in];
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) q[k] = w.sort_tmp[k];
+}
+
 // ------------------------------------------------------------------ persistent traversal
 // Lanes take rays one at a time from a queue (one atomic per warp for all the
 // lanes that need a ray) and advance them one node or leaf per iteration, so a
@@ -1328,7 +1414,7 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	if (refill) k_extend_refill<false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	else k_extend<COUNT, false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
-	if (cfg.sort == RB_SORT_MATERIAL) {
+	if (cfg.sort != RB_SORT_NONE) {
 		k_shade_a<CLASS_LAMBERT, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 		k_shade_a<CLASS_METAL, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 		k_shade_a<CLASS_GLASS_ROUGH, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
@@ -1343,7 +1429,7 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	if (refill) k_secondary_refill<BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	else k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
-	if (cfg.sort == RB_SORT_MATERIAL) {
+	if (cfg.sort != RB_SORT_NONE) {
 		k_shade_b<CLASS_LAMBERT, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 		k_shade_b<CLASS_METAL, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 		k_shade_b<CLASS_GLASS_ROUGH, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -1414,7 +1500,16 @@ cudaError_t launch_wave(const scene_view& s, const wave_buffers& w, const film_b
 	uint32_t qi = first_queue;
 	const bool tail = uses_tail(max_depth, cfg);
 	const uint32_t staged = tail ? cfg.tail : max_depth;
+	const bool bin = cfg.sort == RB_SORT_RAYS && w.sort_keys != nullptr;
 	for (uint32_t b = 0; b < staged && err == cudaSuccess; b++) {
+		if (bin && b > 0) {  // camera rays arrive in pixel order, already coherent
+			k_bin_count<<<cfg.grid_shade, 256, 0, stream>>>(w, qi);
+			k_bin_scan<<<1, 1024, 0, stream>>>(w);
+			k_bin_scatter<<<cfg.grid_shade, 256, 0, stream>>>(w, qi);
+			k_bin_copy<<<cfg.grid_shade, 256, 0, stream>>>(w, qi);
+			err = cudaGetLastError();
+			if (err != cudaSuccess) break;
+		}
 		err = launch_bounce(s, w, f, qi, cfg, stream);
 		qi ^= 1u;
 	}
@@ -1459,7 +1554,14 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 	return e;
 }
 
+uint32_t wave_launches_unbinned(uint32_t max_depth, const launch_cfg& cfg);
+
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {
+	const uint32_t staged = uses_tail(max_depth, cfg) ? cfg.tail : max_depth;
+	return wave_launches_unbinned(max_depth, cfg) + (cfg.sort == RB_SORT_RAYS && staged > 1 ? 4u * (staged - 1) : 0u);
+}
+
+uint32_t wave_launches_unbinned(uint32_t max_depth, const launch_cfg& cfg) {
 	if (cfg.volume) {
 		const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 		const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);

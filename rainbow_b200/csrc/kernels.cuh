@@ -126,11 +126,17 @@ struct wave_buffers {
 	pt::vol_rec* vrec;       // light-connection factors of the current vertex
 	float4* beam;            // 2 per path: transmittance of the NEE and MIS connections
 	uint32_t* beam_queue;    // connections (2 i, 2 i + 1) waiting for their transmittance
+	// ray binning before traversal (RB_SORT_RAYS)
+	uint32_t* sort_keys;     // key of every active-queue entry
+	uint32_t* sort_tmp;      // the binned queue before it is copied back
+	uint32_t* sort_bins;     // kSortBins counts, then kSortBins cursors
 	// batched rendering (null unless a batch render allocated them)
 	uint32_t* scene;         // scene of each path
 	const batch_scene* batch;  // num_scenes records
 	uint32_t num_scenes;
 };
+
+constexpr uint32_t kSortBins = 4096;  // 3 direction-octant bits, 9 bits of an 8x8x8 Morton cell of the origin
 
 struct film_buffers {
 	double* sum;             // 3 per pixel

@@ -40,3 +40,15 @@ def test_context_without_device_is_an_error_not_a_fallback():
     h = ctypes.c_void_p()
     assert rb.lib().rb_context_create(ctypes.byref(h), 0) == 11  # RB_ERR_NO_DEVICE
     assert rb.lib().rb_context_create(None, 0) == 1
+
+
+def test_cpp_program_on_the_c_abi_reports_no_device_without_a_gpu():
+    """tests/native/c_abi_example drives the C ABI from C++; without a GPU the
+    library reports RB_ERR_NO_DEVICE (there is no CPU fallback)."""
+    import subprocess
+    import torch
+    if torch.cuda.is_available():
+        return
+    exe = os.path.join(ROOT, "tests", "native", "c_abi_example")
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0 and out.stdout.startswith("no device"), out.stdout + out.stderr

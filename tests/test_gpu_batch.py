@@ -86,7 +86,8 @@ def test_batch_accumulates_and_refuses_single_scene_calls():
                                     dict(lanes=2, paths_per_wave=5000), dict(lanes=3, paths_per_wave=4096, tail_bounce=3),
                                     dict(lanes=4, paths_per_wave=20000), dict(traversal=rb.RB_TRAVERSAL_PER_THREAD),
                                     dict(traversal=rb.RB_TRAVERSAL_REFILL, block_trace=64, grid_per_sm=1),
-                                    dict(smem_carveout=26, block_trace=256)])
+                                    dict(smem_carveout=26, block_trace=256), dict(sort=rb.RB_SORT_RAYS),
+                                    dict(sort=rb.RB_SORT_RAYS, lanes=2, paths_per_wave=6000, tail_bounce=4)])
 def test_launch_shapes_do_not_change_the_image(tuning):
     sc = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=96, height=64, num_spheres=30, subdivision=3)
     with rb.Context(0) as ctx:
@@ -104,7 +105,7 @@ def test_autotuners_pick_valid_shapes():
         ctx.upload(sc)
         t, ms = ctx.tune_render(sc.camera, probe_spp=2, max_depth=6)
         assert ms > 0 and t.block_trace in (64, 128, 256) and t.block_shade in (64, 128, 256)
-        assert t.grid_per_sm in (2, 4, 8, 16) and t.sort in (0, 1) and t.paths_per_wave > 0
+        assert t.grid_per_sm in (2, 4, 8, 16) and t.sort in (0, 1, 2) and t.paths_per_wave > 0
         assert t.tail_bounce in (1, 2, 3, 4, 6, 64) and t.lanes in (1, 2, 3, 4) and t.traversal in (0, 1)
         assert ctx.tuning().as_dict() == t.as_dict()
         ctx.render(sc.camera, 2, max_depth=6, want_image=False)
