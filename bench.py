@@ -16,7 +16,7 @@ call); `per_call_1spp` is the same K steps as K separate one-sample calls with
 L2 flushed before each; `e2e` is the metric through the public C ABI with the
 step's parameters copied in and the image read back to page-locked host memory
 every step. Launch shapes (waves, lanes, blocks) come from the library's
-autotuner, run untimed on 4 samples per pixel first.
+autotuner, run untimed on 8 samples per pixel first.
 
 The `guided` object is the metric's comparison itself: on the hard-indirect
 room (2,048,000 clutter triangles of 100 displaced icospheres at subdivision 5,
@@ -386,8 +386,8 @@ def main():
         ctx.set_tuning(**json.loads(args.tuning))
         tuning = dict(ctx.tuning().as_dict(), source="--tuning")
     elif not args.no_tune:
-        t, probe_ms = ctx.tune_render(scene.camera, probe_spp=min(4, args.steps), max_depth=depth, seed=base + 777)
-        tuning = dict(t.as_dict(), probe_spp=min(4, args.steps), probe_ms=probe_ms)
+        t, probe_ms = ctx.tune_render(scene.camera, probe_spp=min(8, args.steps), max_depth=depth, seed=base + 777)
+        tuning = dict(t.as_dict(), probe_spp=min(8, args.steps), probe_ms=probe_ms)
     # warm-up: W untimed steps (one sample of every pixel each)
     ctx.render(scene.camera, spp=args.warmup, first_sample=base + args.steps, max_depth=depth, want_image=False)
 

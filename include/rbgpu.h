@@ -343,7 +343,7 @@ typedef struct rb_tuning {
 	uint32_t tail_bounce;       /* bounces run as separate wavefront stages before one kernel carries
 	                               every surviving path to its end (one thread per path, the same
 	                               stage code); 0: library default (64: none), >= max_depth: none */
-	uint32_t lanes;             /* wave lanes (1..4, 0: 1): each lane has its own path buffers, stream and
+	uint32_t lanes;             /* wave lanes (1..8, 0: 1): each lane has its own path buffers, stream and
 	                               graph, so the late bounces of one wave overlap the next wave's early
 	                               ones; the film still adds the waves in order (plain and batched
 	                               renders; guided and volume renders use one lane) */

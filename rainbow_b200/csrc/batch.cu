@@ -158,7 +158,7 @@ rb_status autotune(rb_context* c, uint64_t work_items, Probe&& probe, rb_tuning*
 	const uint32_t grids[] = {2u, 4u, 8u, 16u};
 	const uint32_t sorts[] = {RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS};
 	const uint32_t tails[] = {1u, 2u, 3u, 4u, 6u, 64u};
-	const uint32_t lane_counts[] = {1u, 2u, 3u, 4u};
+	const uint32_t lane_counts[] = {1u, 2u, 3u, 4u, 6u, 8u};
 	const uint32_t traversals[] = {RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL};
 	const uint32_t carveouts[] = {0u, 26u, 51u, 76u};  // largest, 25%, 50%, 75% (stored as percent + 1)
 	auto try_value = [&](uint32_t rb_tuning::*field, uint32_t value) -> rb_status {

@@ -99,6 +99,8 @@ struct graph_key {
 	}
 };
 
+constexpr uint32_t kMaxLanes = 8;  // wave lanes of a context
+
 // Launch shapes of a tuning with the defaults filled in.
 inline rb_tuning resolved_tuning(const rb_tuning& t) {
 	rb_tuning r = t;
@@ -112,11 +114,9 @@ inline rb_tuning resolved_tuning(const rb_tuning& t) {
 inline bool valid_tuning(const rb_tuning& t) {
 	auto block_ok = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 256 && b % 32 == 0); };
 	return block_ok(t.block_trace) && block_ok(t.block_shade) && t.grid_per_sm <= 64 && t.sort <= RB_SORT_RAYS &&
-		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= 4 && t.traversal <= RB_TRAVERSAL_REFILL &&
+		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= kMaxLanes && t.traversal <= RB_TRAVERSAL_REFILL &&
 		t.smem_carveout <= 101;
 }
-
-constexpr uint32_t kMaxLanes = 4;
 
 // Path state of one wave: the buffers of wave_buffers for `n` paths.
 cudaError_t alloc_wave_buffers(gpu::wave_buffers& w, size_t n);

@@ -106,7 +106,7 @@ def test_autotuners_pick_valid_shapes():
         t, ms = ctx.tune_render(sc.camera, probe_spp=2, max_depth=6)
         assert ms > 0 and t.block_trace in (64, 128, 256) and t.block_shade in (64, 128, 256)
         assert t.grid_per_sm in (2, 4, 8, 16) and t.sort in (0, 1, 2) and t.paths_per_wave > 0
-        assert t.tail_bounce in (1, 2, 3, 4, 6, 64) and t.lanes in (1, 2, 3, 4) and t.traversal in (0, 1)
+        assert t.tail_bounce in (1, 2, 3, 4, 6, 64) and t.lanes in (1, 2, 3, 4, 6, 8) and t.traversal in (0, 1)
         assert ctx.tuning().as_dict() == t.as_dict()
         ctx.render(sc.camera, 2, max_depth=6, want_image=False)
         assert ctx.stats().device_error == 0
