@@ -435,7 +435,8 @@ typedef struct rb_guide_config {
 	float weight_clip;          /* rendering-time training clips each weight at this multiple of the
 	                               running mean weight (fewer steps dominated by rare paths), 0: 16,
 	                               < 0: no clipping */
-	uint32_t reserved;
+	uint32_t warmup_steps;      /* RB_RENDER_GUIDE samples the guide only after this many Adam steps
+	                               (until then continuations come from the BSDF alone), 0: 1 */
 } rb_guide_config;
 /* One training sample (64 bytes). */
 typedef struct rb_guide_sample {

@@ -207,8 +207,10 @@ class Context:
 
     # ---- learned path guiding
     def guide_init(self, seed: int = 0, learning_rate: float = 1e-3, batch_size: int = 1 << 18, steps_per_wave: int = 8,
-                   max_samples: int = 1 << 21, min_rows: int = 4096, weight_clip: float = 0.0) -> None:
-        cfg = GuideConfig(seed, learning_rate, batch_size, steps_per_wave, max_samples, min_rows, weight_clip)
+                   max_samples: int = 1 << 21, min_rows: int = 4096, weight_clip: float = 0.0,
+                   warmup_steps: int = 0) -> None:
+        cfg = GuideConfig(seed, learning_rate, batch_size, steps_per_wave, max_samples, min_rows, weight_clip,
+                          warmup_steps)
         check(lib().rb_guide_init(self._h, C.byref(cfg)), "rb_guide_init")
 
     def guide_params(self) -> np.ndarray:

@@ -132,7 +132,7 @@ class SceneGenParams(C.Structure):
 class GuideConfig(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("learning_rate", C.c_float), ("batch_size", C.c_uint32),
                 ("steps_per_wave", C.c_uint32), ("max_samples", C.c_uint32), ("min_rows", C.c_uint32),
-                ("weight_clip", C.c_float), ("reserved", C.c_uint32)]
+                ("weight_clip", C.c_float), ("warmup_steps", C.c_uint32)]
 
 
 class GuideStats(C.Structure):

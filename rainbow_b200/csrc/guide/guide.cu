@@ -513,6 +513,7 @@ struct adam_args {
 	uint32_t min_rows;
 	uint32_t budgeted;
 	float lr;
+	uint32_t warmup_steps;      // the guide becomes usable for sampling at this step count
 };
 
 // Sums the per-CTA partials in CTA order, then one Adam step (beta1 0.9,
@@ -553,7 +554,7 @@ __global__ void __launch_bounds__(256) k_adam(adam_args a) {
 		__threadfence();
 		if (atomicAdd(&a.state->ticket, 1u) == gridDim.x - 1u) {
 			a.state->step = t_step;
-			a.state->usable = 1u;
+			if (t_step >= a.warmup_steps) a.state->usable = 1u;
 			a.state->wave_step += 1u;
 			a.state->ticket = 0u;
 			__threadfence();
@@ -875,6 +876,7 @@ cudaError_t launch_train_step(const guide_state& g, const float4* samples, const
 	a.min_rows = min_rows;
 	a.budgeted = budgeted ? 1u : 0u;
 	a.lr = g.cfg.learning_rate;
+	a.warmup_steps = g.cfg.warmup_steps;
 	k_adam<<<(kAugParams + 255) / 256, 256, 0, s>>>(a);
 	return cudaGetLastError();
 }

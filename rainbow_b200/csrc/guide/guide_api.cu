@@ -152,6 +152,7 @@ rb_status init_state(guide_state& g, const rb_guide_config* config, int sms, cud
 	if (cfg.steps_per_wave == 0) cfg.steps_per_wave = 8;
 	if (cfg.max_samples == 0) cfg.max_samples = 1u << 21;
 	if (cfg.min_rows == 0) cfg.min_rows = 4096;
+	if (cfg.warmup_steps == 0) cfg.warmup_steps = 1;
 	if (cfg.batch_size > (1u << 24) || cfg.max_samples > (1u << 26) || cfg.steps_per_wave > 64) return RB_ERR_INVALID_ARGUMENT;
 	uint32_t ring = 1024u;
 	while (ring < cfg.max_samples) ring <<= 1;  // the replay ring holds a power of two
