@@ -170,8 +170,10 @@ def config_dict(world, l2="flushed before the timed call; per-step inputs exceed
             "parallelism": f"replicas x{world} (sample ranges)", "l2": l2}
 
 
-def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=16):
-    """Device time to each relMSE target: plain vs guided (online training)."""
+def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=12, batch=1 << 17, train_chunks=4,
+               lanes=4):
+    """Device time to each relMSE target: plain vs guided (online training during the first train_chunks
+    chunks, then guided sampling with the trained weights)."""
     scene = rb.generate_scene(GUIDED["kind"], seed=GUIDED["seed"], width=res, height=res,
                               num_spheres=GUIDED["num_spheres"], subdivision=GUIDED["subdivision"])
     depth = GUIDED["max_depth"]
@@ -188,20 +190,20 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
         m = s / c[..., None]
         return float(np.mean((m - ref) ** 2 / (ref ** 2 + 1e-2)))
 
-    # plain at its fastest: launch shapes tuned for chunk-sized calls; guided: two waves per chunk on two
-    # lanes (each lane samples the weights trained after its previous wave)
+    # plain at its fastest: launch shapes tuned for chunk-sized calls; guided: `lanes` waves per chunk on as
+    # many lanes (each lane samples the weights trained after its previous wave)
     plain_tuning, _ = ctx.tune_render(scene.camera, probe_spp=chunk, max_depth=depth, seed=55)
-    guided_tuning = dict(paths_per_wave=res * res * chunk // 2, lanes=2, smem_carveout=plain_tuning.smem_carveout)
+    guided_tuning = dict(paths_per_wave=res * res * chunk // lanes, lanes=lanes, smem_carveout=plain_tuning.smem_carveout)
     out = {}
     for mode in ("plain", "guided"):
         guided = mode == "guided"
         if guided:
             ctx.set_tuning(plain_tuning, **guided_tuning)
-            ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=1 << 18, steps_per_wave=steps_per_wave, min_rows=4096)
+            ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=batch, steps_per_wave=steps_per_wave, min_rows=4096)
         ms, spp, left, hit = 0.0, 0, sorted(targets, reverse=True), {}
         while left and spp < max_spp:
             ctx.render(scene.camera, chunk, first_sample=spp, max_depth=depth, seed=7, reset=(spp == 0), guide=guided,
-                       train=guided, want_image=False)
+                       train=guided and spp < train_chunks * chunk, want_image=False)
             ms += ctx.stats().elapsed_ms
             spp += chunk
             e = relmse()
@@ -218,8 +220,9 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
         res_t[str(t)] = {"plain_s": p and p["s"], "plain_spp": p and p["spp"], "guided_s": g and g["s"],
                          "guided_spp": g and g["spp"], "speedup": (p["s"] / g["s"]) if (p and g) else None}
     return {"workload": f"slit room, {GUIDED['num_spheres'] * 20480 + 18} triangles, {res}x{res}, max depth {depth}, "
-                        f"chunks of {chunk} spp; guided: two waves per chunk on two lanes, {steps_per_wave} Adam steps of "
-                        f"up to 2^18 samples after each wave; plain: autotuned launch shapes {plain_tuning.as_dict()}",
+                        f"chunks of {chunk} spp; guided: {lanes} waves per chunk on {lanes} lanes, {steps_per_wave} Adam "
+                        f"steps of up to {batch} samples after each wave of the first {train_chunks} chunks, then guided "
+                        f"sampling without training; plain: autotuned launch shapes {plain_tuning.as_dict()}",
             "reference": f"plain, {ref_spp} spp, FP64 accumulation ({ref_s:.1f} s)", "targets": res_t,
             "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}
 

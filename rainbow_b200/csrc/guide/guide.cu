@@ -37,10 +37,25 @@ constexpr uint32_t kSboHid = kHiddenK * 16;                        // 8-row grou
 constexpr uint32_t kCopyChunk = kImageBytes / 4;                   // 16,768 bytes per bulk copy
 static_assert(kCopyChunk % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-// forward kernel shared memory: weight image, two tiles (one per warpgroup), barriers
+// Forward kernel: four warpgroups per CTA, each with its own 32 KB tile. The
+// encoded input (224 features) goes through layer 1 in two K parts that take
+// turns in that tile: inputs 0..3 (features 0..95, 6 K-steps), then inputs
+// 4..8 and the bias chunk (features 96..223, 8 K-steps). The hidden tiles
+// (80 features, 20 KB) reuse it.
+constexpr uint32_t kFwdGroups = 4;
+constexpr int kPartAInputs = 4;
+constexpr uint32_t kPartAChunks = 3 * kPartAInputs;                 // 12 chunks of 8 features
+constexpr uint32_t kPartBChunks = 3 * (kInputs - kPartAInputs) + 1; // 16 (with the bias chunk)
+constexpr uint32_t kSboPartA = kPartAChunks * 128;
+constexpr uint32_t kSboPartB = kPartBChunks * 128;
+constexpr uint32_t kFwdTile = kTileRows / 8 * kSboPartB;           // 32,768
+static_assert(kPartAChunks % 2 == 0 && kPartBChunks % 2 == 0, "each part is whole K-steps of 16 features");
+static_assert(kPartAChunks + kPartBChunks == kK1 / 8, "the two parts cover the encoded input");
+static_assert(kFwdTile >= kTileRows / 8 * kSboPartA && kFwdTile >= kHidBytes, "the tile holds every operand");
 constexpr uint32_t kFwdAct = kImageBytes;
-constexpr uint32_t kFwdBars = kFwdAct + 2 * kActBytes;
-constexpr uint32_t kFwdSmem = kFwdBars + 64 + 128;
+constexpr uint32_t kFwdBars = kFwdAct + kFwdGroups * kFwdTile;
+constexpr uint32_t kFwdSmem = kFwdBars + 128 + 128;
+static_assert(kFwdSmem <= 232448, "forward kernel exceeds 227 KB of shared memory");
 // training kernel: weight image, X0, X1..X4, signal tile, barriers. A weight-
 // gradient product reads 128 feature rows of an activation tile, past the end
 // of the 80 (or 224) stored ones; those extra rows land in the next buffer and
@@ -79,14 +94,14 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 	return h;
 }
 
-// Row `row` of an encoded tile (K = 224): 27 chunks of 8 features (4 sin/cos
-// pairs), then the constant-1 bias feature and 7 zeros. sin/cos(2^k pi x) by
-// the double-angle recurrence, restarted exactly at k = 4 and k = 8 so that
-// the error stays near 1e-6.
-__device__ __forceinline__ void encode_row(const float (&x)[kInputs], uint8_t* tile, uint32_t row) {
-	uint8_t* base = tile + (row >> 3) * kSboIn + (row & 7u) * 16u;
+// Inputs J0..J1-1 of one row of an encoded tile, from `base` (the row's first
+// core-matrix line): 3 chunks of 8 features (4 sin/cos pairs) per input.
+// sin/cos(2^k pi x) by the double-angle recurrence, restarted exactly at k = 4
+// and k = 8 so that the error stays near 1e-6.
+template <int J0, int J1>
+__device__ __forceinline__ void encode_inputs(const float (&x)[kInputs], uint8_t* base) {
 #pragma unroll
-	for (int j = 0; j < kInputs; j++) {
+	for (int j = J0; j < J1; j++) {
 		float s[kFreqs], c[kFreqs];
 		sincospif(x[j], &s[0], &c[0]);
 #pragma unroll
@@ -105,10 +120,36 @@ __device__ __forceinline__ void encode_row(const float (&x)[kInputs], uint8_t* t
 			v.y = pack2(s[4 * q + 1], c[4 * q + 1]);
 			v.z = pack2(s[4 * q + 2], c[4 * q + 2]);
 			v.w = pack2(s[4 * q + 3], c[4 * q + 3]);
-			*reinterpret_cast<uint4*>(base + (3 * j + q) * 128) = v;
+			*reinterpret_cast<uint4*>(base + (3 * (j - J0) + q) * 128) = v;
 		}
 	}
+}
+
+// Row `row` of an encoded tile (K = 224): 27 chunks of 8 features, then the
+// constant-1 bias feature and 7 zeros.
+__device__ __forceinline__ void encode_row(const float (&x)[kInputs], uint8_t* tile, uint32_t row) {
+	uint8_t* base = tile + (row >> 3) * kSboIn + (row & 7u) * 16u;
+	encode_inputs<0, kInputs>(x, base);
 	*reinterpret_cast<uint4*>(base + 27 * 128) = make_uint4(pack2(1.f, 0.f), 0u, 0u, 0u);
+}
+
+// Four of the eight value chunks of a hidden-tile row (chunks c0 .. c0 + 3: the
+// relu of 32 values); with c0 == 4 also the constant-1 chunk and the zero chunk.
+__device__ __forceinline__ void store_hidden_half(uint8_t* tile, uint32_t row, const float* v, int c0) {
+	uint8_t* base = tile + (row >> 3) * kSboHid + (row & 7u) * 16u;
+#pragma unroll
+	for (int c = 0; c < 4; c++) {
+		uint4 u;
+		u.x = pack2(relu(v[8 * c]), relu(v[8 * c + 1]));
+		u.y = pack2(relu(v[8 * c + 2]), relu(v[8 * c + 3]));
+		u.z = pack2(relu(v[8 * c + 4]), relu(v[8 * c + 5]));
+		u.w = pack2(relu(v[8 * c + 6]), relu(v[8 * c + 7]));
+		*reinterpret_cast<uint4*>(base + (c0 + c) * 128) = u;
+	}
+	if (c0 == 4) {
+		*reinterpret_cast<uint4*>(base + 8 * 128) = make_uint4(pack2(1.f, 0.f), 0u, 0u, 0u);
+		*reinterpret_cast<uint4*>(base + 9 * 128) = make_uint4(0u, 0u, 0u, 0u);
+	}
 }
 
 // Row of a hidden tile (K = 80): relu of 64 values, the constant 1, 15 zeros.
@@ -160,12 +201,13 @@ __device__ __forceinline__ void relu_mask(const uint8_t* tile, uint32_t row, flo
 }
 
 // ---------------------------------------------------------------- MMA issue (one thread)
-// D[128 x n] = A[128 x K] B[n x K]^T, both K-major, K = 16 * ksteps.
+// D[128 x n] (+)= A[128 x K] B[n x K]^T, both K-major, K = 16 * ksteps.
 __device__ __forceinline__ void mma_kk(uint32_t d, uint32_t a, uint32_t a_sbo, uint32_t b, uint32_t b_sbo, uint32_t n,
-	uint32_t ksteps) {
+	uint32_t ksteps, bool accumulate = false) {
 	const uint32_t id = idesc_bf16(128, n, false, false);
 	for (uint32_t ks = 0; ks < ksteps; ks++)
-		umma_bf16(d, sdesc(a + ks * 256u, 128u, a_sbo), sdesc(b + ks * 256u, 128u, b_sbo), id, ks > 0 ? 1u : 0u);
+		umma_bf16(d, sdesc(a + ks * 256u, 128u, a_sbo), sdesc(b + ks * 256u, 128u, b_sbo), id,
+			(accumulate || ks > 0) ? 1u : 0u);
 }
 // D[128 x n] = A[128 x K] (K-major) B[K x n] with B MN-major (8-row K groups b_lbo apart).
 __device__ __forceinline__ void mma_km(uint32_t d, uint32_t a, uint32_t a_sbo, uint32_t b, uint32_t b_lbo, uint32_t n,
@@ -205,7 +247,7 @@ __device__ __forceinline__ void publish(uint32_t barrier_id) {
 
 // Shared start: TMEM allocation by warp 0, barrier set-up, weight image by bulk copy.
 __device__ __forceinline__ bool kernel_begin(uint8_t* img, const uint8_t* image, uint64_t* bars, uint32_t nbars,
-	uint32_t* tptr, volatile uint32_t* fail, uint32_t ncols, uint32_t* error) {
+	uint32_t* tptr, volatile uint32_t* fail, uint32_t nfail, uint32_t ncols, uint32_t* error) {
 	const uint32_t tid = threadIdx.x;
 	if ((tid >> 5) == 0) {
 		tmem_alloc(tptr, ncols);
@@ -213,8 +255,7 @@ __device__ __forceinline__ bool kernel_begin(uint8_t* img, const uint8_t* image,
 	}
 	if (tid == 0) {
 		for (uint32_t i = 0; i < nbars; i++) mbar_init(&bars[i], 1);
-		fail[0] = 0u;
-		fail[1] = 0u;
+		for (uint32_t i = 0; i < nfail; i++) fail[i] = 0u;
 		fence_mbar_init();
 	}
 	tc_fence_before();
@@ -252,19 +293,19 @@ struct fwd_args {
 	uint32_t* error;
 };
 
-// Two warpgroups per CTA, each running its own tiles through the 5 layers
+// Four warpgroups per CTA, each running its own tiles through the 5 layers
 // (TMEM columns 64 g .. 64 g + 63), sharing the weight image.
 template <bool QUEUE>
-__global__ void __launch_bounds__(256, 1) k_forward(fwd_args a) {
+__global__ void __launch_bounds__(kFwdGroups * 128, 1) k_forward(fwd_args a) {
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t* sm = align128(smem_raw);
 	const uint32_t tid = threadIdx.x, grp = tid >> 7, t = tid & 127u, warp = tid >> 5;
 	uint8_t* img = sm;
-	uint8_t* act = sm + kFwdAct + grp * kActBytes;
-	uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kFwdBars);
-	uint32_t* tptr = reinterpret_cast<uint32_t*>(sm + kFwdBars + 32);
-	volatile uint32_t* fail = reinterpret_cast<volatile uint32_t*>(sm + kFwdBars + 40);
-	const bool loaded = kernel_begin(img, a.image, bars, 3, tptr, fail, 128, a.error);
+	uint8_t* act = sm + kFwdAct + grp * kFwdTile;
+	uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kFwdBars);                       // 1 + kFwdGroups
+	uint32_t* tptr = reinterpret_cast<uint32_t*>(sm + kFwdBars + 64);
+	volatile uint32_t* fail = reinterpret_cast<volatile uint32_t*>(sm + kFwdBars + 80); // kFwdGroups
+	const bool loaded = kernel_begin(img, a.image, bars, 1 + kFwdGroups, tptr, fail, kFwdGroups, kFwdGroups * 64, a.error);
 	const uint32_t tmem = *tptr;
 	if (loaded) {
 		const uint32_t n = QUEUE ? *a.count : a.n;
@@ -275,8 +316,10 @@ __global__ void __launch_bounds__(256, 1) k_forward(fwd_args a) {
 		uint64_t* bar = &bars[1 + grp];
 		uint32_t phase = 0;
 		const uint32_t act_s = smem_u32(act), img_s = smem_u32(img);
+		uint8_t* base_a = act + (t >> 3) * kSboPartA + (t & 7u) * 16u;
+		uint8_t* base_b = act + (t >> 3) * kSboPartB + (t & 7u) * 16u;
 		bool failed = false;
-		for (uint32_t tile = blockIdx.x * 2u + grp; tile < tiles; tile += gridDim.x * 2u) {
+		for (uint32_t tile = blockIdx.x * kFwdGroups + grp; tile < tiles; tile += gridDim.x * kFwdGroups) {
 			const uint32_t row = tile * kTileRows + t;
 			const bool valid = row < n;
 			uint32_t path = 0;
@@ -294,20 +337,32 @@ __global__ void __launch_bounds__(256, 1) k_forward(fwd_args a) {
 					for (int j = 0; j < kInputs; j++) x[j] = a.x[static_cast<size_t>(row) * kInputs + j];
 				}
 			}
-			encode_row(x, act, t);
+			// layer 1, first K part
+			encode_inputs<0, kPartAInputs>(x, base_a);
 			publish(bid);
 			if (t == 0) {
 				tc_fence_after();
-				mma_kk(dcol, act_s, kSboIn, img_s, kSboIn, kHidden, kK1 / 16);
+				mma_kk(dcol, act_s, kSboPartA, img_s, kSboIn, kHidden, kPartAChunks / 2);
 				umma_commit(bar);
 			}
 			if (!group_wait(bar, phase, fail + grp, bid)) { failed = true; break; }
-			float v[kHidden];
+			// layer 1, second K part (accumulating), in the same tile
+			encode_inputs<kPartAInputs, kInputs>(x, base_b);
+			*reinterpret_cast<uint4*>(base_b + (kPartBChunks - 1) * 128) = make_uint4(pack2(1.f, 0.f), 0u, 0u, 0u);
+			publish(bid);
+			if (t == 0) {
+				tc_fence_after();
+				mma_kk(dcol, act_s, kSboPartB, img_s + kPartAChunks * 128u, kSboIn, kHidden, kPartBChunks / 2, true);
+				umma_commit(bar);
+			}
+			if (!group_wait(bar, phase, fail + grp, bid)) { failed = true; break; }
 #pragma unroll 1
 			for (int l = 1; l < kLayers; l++) {
+				float v[32];
 				tmem_ld32(lane, v);
-				tmem_ld32(lane + 32u, v + 32);
-				store_hidden_row(act, t, v);
+				store_hidden_half(act, t, v, 0);
+				tmem_ld32(lane + 32u, v);
+				store_hidden_half(act, t, v, 4);
 				publish(bid);
 				if (t == 0) {
 					tc_fence_after();
@@ -317,6 +372,7 @@ __global__ void __launch_bounds__(256, 1) k_forward(fwd_args a) {
 				if (!group_wait(bar, phase, fail + grp, bid)) { failed = true; break; }
 			}
 			if (failed) break;
+			float v[kOutputs];
 			tmem_ld32(lane, v);
 			tmem_ld16(lane + 32u, v + 32);
 			if (valid) {
@@ -338,7 +394,7 @@ __global__ void __launch_bounds__(256, 1) k_forward(fwd_args a) {
 			mbar_wait(bar, phase, kWaitNs);  // the MMAs in flight finish before TMEM is released
 		}
 	}
-	kernel_end(tmem, 128);
+	kernel_end(tmem, kFwdGroups * 64);
 }
 
 // ---------------------------------------------------------------- training
@@ -374,7 +430,7 @@ __global__ void __launch_bounds__(128, 1) k_train(train_args a) {
 	uint32_t* tptr = reinterpret_cast<uint32_t*>(sm + kTrBars + 32);
 	volatile uint32_t* fail = reinterpret_cast<volatile uint32_t*>(sm + kTrBars + 40);
 	float* red = reinterpret_cast<float*>(sm + kTrBars + 48);
-	const bool loaded = kernel_begin(img, a.image, bars, 2, tptr, fail, 512, a.error);
+	const bool loaded = kernel_begin(img, a.image, bars, 2, tptr, fail, 2, 512, a.error);
 	const uint32_t tmem = *tptr;
 	const uint32_t lane_off = (32u * warp) << 16;
 	const uint32_t img_s = smem_u32(img), x0_s = smem_u32(X0), sig_s = smem_u32(sig);
@@ -826,8 +882,9 @@ cudaError_t launch_forward_raw(const guide_state& g, const float* x, uint32_t n,
 	a.out = out;
 	a.error = &g.dstate->error;
 	const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
-	const uint32_t grid = (tiles + 1) / 2 < static_cast<uint32_t>(g.ctas) ? (tiles + 1) / 2 : static_cast<uint32_t>(g.ctas);
-	k_forward<false><<<grid, 256, kFwdSmem, s>>>(a);
+	const uint32_t want = (tiles + kFwdGroups - 1) / kFwdGroups;
+	const uint32_t grid = want < static_cast<uint32_t>(g.ctas) ? want : static_cast<uint32_t>(g.ctas);
+	k_forward<false><<<grid, kFwdGroups * 128, kFwdSmem, s>>>(a);
 	return cudaGetLastError();
 }
 
@@ -839,7 +896,7 @@ cudaError_t launch_forward_queue(const guide_state& g, const wave_guide& wg, con
 	a.in4 = wg.query_in;
 	a.out4 = wg.query_out;
 	a.error = &g.dstate->error;
-	k_forward<true><<<g.ctas, 256, kFwdSmem, s>>>(a);
+	k_forward<true><<<g.ctas, kFwdGroups * 128, kFwdSmem, s>>>(a);
 	return cudaGetLastError();
 }
 
