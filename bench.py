@@ -171,7 +171,7 @@ def config_dict(world, l2="flushed before the timed call; per-step inputs exceed
 
 
 def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=12, batch=1 << 17, train_chunks=4,
-               lanes=4):
+               lanes=4, learning_rate=3e-3, weight_clip=4.0):
     """Device time to each relMSE target: plain vs guided (online training during the first train_chunks
     chunks, then guided sampling with the trained weights)."""
     scene = rb.generate_scene(GUIDED["kind"], seed=GUIDED["seed"], width=res, height=res,
@@ -199,7 +199,8 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
         guided = mode == "guided"
         if guided:
             ctx.set_tuning(plain_tuning, **guided_tuning)
-            ctx.guide_init(seed=0, learning_rate=1e-3, batch_size=batch, steps_per_wave=steps_per_wave, min_rows=4096)
+            ctx.guide_init(seed=0, learning_rate=learning_rate, batch_size=batch, steps_per_wave=steps_per_wave,
+                           min_rows=4096, weight_clip=weight_clip)
         ms, spp, left, hit = 0.0, 0, sorted(targets, reverse=True), {}
         while left and spp < max_spp:
             ctx.render(scene.camera, chunk, first_sample=spp, max_depth=depth, seed=7, reset=(spp == 0), guide=guided,
@@ -221,7 +222,8 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
                          "guided_spp": g and g["spp"], "speedup": (p["s"] / g["s"]) if (p and g) else None}
     return {"workload": f"slit room, {GUIDED['num_spheres'] * 20480 + 18} triangles, {res}x{res}, max depth {depth}, "
                         f"chunks of {chunk} spp; guided: {lanes} waves per chunk on {lanes} lanes, {steps_per_wave} Adam "
-                        f"steps of up to {batch} samples after each wave of the first {train_chunks} chunks, then guided "
+                        f"steps (learning rate {learning_rate}, weights clipped at {weight_clip}x their running mean) of up "
+                        f"to {batch} samples after each wave of the first {train_chunks} chunks, then guided "
                         f"sampling without training; plain: autotuned launch shapes {plain_tuning.as_dict()}",
             "reference": f"plain, {ref_spp} spp, FP64 accumulation ({ref_s:.1f} s)", "targets": res_t,
             "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}

@@ -629,7 +629,8 @@ __global__ void k_image(const float* master, __nv_bfloat16* image) {
 __global__ void k_decode_sample(const float* raw, const float* u, uint32_t n, float* dirs, float* pdfs) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	float o[kOutputs], g[kOutputs], d[3];
+	float o[kOutputs], d[3];
+	alignas(16) float g[kOutputs];
 	for (int c = 0; c < kOutputs; c++) o[c] = raw[static_cast<size_t>(i) * kOutputs + c];
 	decode_outputs(o, g);
 	guide_sample(g, u[3 * i], u[3 * i + 1], u[3 * i + 2], d);

@@ -89,21 +89,25 @@ RB_GHD int aug_to_flat(int l, int o, int k) {
 }
 
 // ------------------------------------------------------------ guide density
-// Decoded guide of one query (48 floats): mu[8][3] at 0, kappa[8] at 24,
-// lobe weights[8] at 32 (summing to 1), alpha at 40.
-constexpr int kMuOff = 0, kKappaOff = 24, kWeightOff = 32, kAlphaOff = 40;
+// Decoded guide of one query (48 floats, 12 float4): lobe i as (mu_i, kappa_i)
+// at 4 i, the lobe's density factor (1 - eps) w_i c(kappa_i) at 32 + i, the
+// cumulative lobe weights w_0 .. w_0 + .. + w_6 at 40 (the last lobe takes the
+// rest of 1), alpha at 47.
+constexpr int kLobeOff = 0, kWcOff = 32, kCdfOff = 40, kAlphaOff = 47;
 
 RB_GHD float vmf_norm(float kappa) { return kappa / (2.f * kPi * (-expm1f(-2.f * kappa))); }
 
 // q(d) = (1 - eps) sum_i w_i c(kappa_i) exp(kappa_i (mu_i . d - 1)) + eps / (4 pi)
 RB_GHD float guide_pdf(const float* g, float dx, float dy, float dz) {
+	const float4* g4 = reinterpret_cast<const float4*>(g);
+	const float4 wa = g4[kWcOff / 4], wb = g4[kWcOff / 4 + 1];
+	const float wc[kLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 	float s = 0.f;
 	for (int i = 0; i < kLobes; i++) {
-		const float k = g[kKappaOff + i];
-		const float c = g[kMuOff + 3 * i] * dx + g[kMuOff + 3 * i + 1] * dy + g[kMuOff + 3 * i + 2] * dz;
-		s += g[kWeightOff + i] * vmf_norm(k) * expf(k * (c - 1.f));
+		const float4 m = g4[kLobeOff / 4 + i];
+		s += wc[i] * expf(m.w * ((m.x * dx + m.y * dy + m.z * dz) - 1.f));
 	}
-	return (1.f - kEpsUniform) * s + kEpsUniform / (4.f * kPi);
+	return s + kEpsUniform / (4.f * kPi);
 }
 
 // Orthonormal basis (t, b) around unit n: Duff et al. 2017, "Building an
@@ -122,24 +126,23 @@ RB_GHD void onb(float nx, float ny, float nz, float* t, float* b) {
 // sampling of the von Mises-Fisher distribution on S^2"):
 // cos = 1 + log(e^{-2 kappa} + u1 (1 - e^{-2 kappa})) / kappa.
 RB_GHD void guide_sample(const float* g, float u_pick, float u1, float u2, float* d) {
+	const float4* g4 = reinterpret_cast<const float4*>(g);
 	float cz, m[3] = {0.f, 0.f, 1.f};
 	if (u_pick < kEpsUniform) {
 		cz = 1.f - 2.f * u1;
 	} else {
 		const float up = (u_pick - kEpsUniform) / (1.f - kEpsUniform);
-		float total = 0.f;
-		for (int i = 0; i < kLobes; i++) total += g[kWeightOff + i];
-		const float target = up * total;
+		const float4 ca = g4[kCdfOff / 4], cb = g4[kCdfOff / 4 + 1];
+		const float cdf[kLobes - 1] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z};
 		int j = kLobes - 1;
-		float acc = 0.f;
-		for (int i = 0; i < kLobes; i++) {
-			acc += g[kWeightOff + i];
-			if (target < acc) { j = i; break; }
+		for (int i = 0; i < kLobes - 1; i++) {
+			if (up < cdf[i]) { j = i; break; }
 		}
-		const float k = g[kKappaOff + j];
+		const float4 lb = g4[kLobeOff / 4 + j];
+		const float k = lb.w;
 		const float e2 = expf(-2.f * k);
 		cz = 1.f + logf(e2 + u1 * (1.f - e2)) / k;
-		m[0] = g[kMuOff + 3 * j]; m[1] = g[kMuOff + 3 * j + 1]; m[2] = g[kMuOff + 3 * j + 2];
+		m[0] = lb.x; m[1] = lb.y; m[2] = lb.z;
 	}
 	cz = fminf(1.f, fmaxf(-1.f, cz));
 	const float s = sqrtf(fmaxf(0.f, 1.f - cz * cz));
@@ -150,25 +153,31 @@ RB_GHD void guide_sample(const float* g, float u_pick, float u1, float u2, float
 	for (int c = 0; c < 3; c++) d[c] = cz * m[c] + s * (cp * t[c] + sp * b[c]);
 }
 
-// Raw network outputs (48) -> decoded guide (48 floats, see kMuOff ..).
+// Raw network outputs (48) -> decoded guide (48 floats, see kLobeOff ..).
 RB_GHD void decode_outputs(const float* o, float* g) {
 	float lmax = o[4];
 	for (int i = 1; i < kLobes; i++) lmax = fmaxf(lmax, o[5 * i + 4]);
 	float e[kLobes], esum = 0.f;
 	for (int i = 0; i < kLobes; i++) { e[i] = expf(o[5 * i + 4] - lmax); esum += e[i]; }
+	float acc = 0.f;
 	for (int i = 0; i < kLobes; i++) {
 		const float mx = o[5 * i], my = o[5 * i + 1], mz = o[5 * i + 2];
 		const float nr = sqrtf(mx * mx + my * my + mz * mz);
 		if (nr > 1e-12f) {
-			g[kMuOff + 3 * i] = mx / nr; g[kMuOff + 3 * i + 1] = my / nr; g[kMuOff + 3 * i + 2] = mz / nr;
+			g[kLobeOff + 4 * i] = mx / nr; g[kLobeOff + 4 * i + 1] = my / nr; g[kLobeOff + 4 * i + 2] = mz / nr;
 		} else {
-			g[kMuOff + 3 * i] = 0.f; g[kMuOff + 3 * i + 1] = 0.f; g[kMuOff + 3 * i + 2] = 1.f;
+			g[kLobeOff + 4 * i] = 0.f; g[kLobeOff + 4 * i + 1] = 0.f; g[kLobeOff + 4 * i + 2] = 1.f;
 		}
-		g[kKappaOff + i] = expf(fminf(kKappaMax, fmaxf(kKappaMin, o[5 * i + 3])));
-		g[kWeightOff + i] = e[i] / esum;
+		const float k = expf(fminf(kKappaMax, fmaxf(kKappaMin, o[5 * i + 3])));
+		const float w = e[i] / esum;
+		g[kLobeOff + 4 * i + 3] = k;
+		g[kWcOff + i] = (1.f - kEpsUniform) * w * vmf_norm(k);
+		if (i < kLobes - 1) {
+			acc += w;
+			g[kCdfOff + i] = acc;
+		}
 	}
 	g[kAlphaOff] = kAlphaLo + (kAlphaHi - kAlphaLo) / (1.f + expf(-o[40]));
-	for (int i = kAlphaOff + 1; i < kOutputs; i++) g[i] = 0.f;
 }
 
 // Gradient of the per-sample loss
