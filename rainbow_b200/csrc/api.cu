@@ -100,10 +100,20 @@ rb_status ensure_lanes(rb_context* c, uint32_t count) {
 		l.wave.counters = l.counters;
 		l.wave.params = l.params;
 		l.wave.guide = guide::wave_guide{};
-		l.wave.medium = nullptr;
-		l.wave.vrec = nullptr;
-		l.wave.beam = nullptr;
-		l.wave.beam_queue = nullptr;
+		if (c->volume && l.vol_alloc < c->wave_capacity) {
+			l.release_graph();
+			dev_free(l.vol_medium); dev_free(l.vol_rec); dev_free(l.vol_beam); dev_free(l.vol_beam_queue);
+			l.vol_alloc = 0;
+			RB_CUDA(dev_alloc(&l.vol_medium, c->wave_capacity));
+			RB_CUDA(dev_alloc(&l.vol_rec, c->wave_capacity));
+			RB_CUDA(dev_alloc(&l.vol_beam, 2 * static_cast<size_t>(c->wave_capacity)));
+			RB_CUDA(dev_alloc(&l.vol_beam_queue, 2 * static_cast<size_t>(c->wave_capacity)));
+			l.vol_alloc = c->wave_capacity;
+		}
+		l.wave.medium = c->volume ? l.vol_medium : nullptr;
+		l.wave.vrec = c->volume ? l.vol_rec : nullptr;
+		l.wave.beam = c->volume ? l.vol_beam : nullptr;
+		l.wave.beam_queue = c->volume ? l.vol_beam_queue : nullptr;
 		l.wave.batch = c->wave.batch;
 		l.wave.num_scenes = c->wave.num_scenes;
 		l.wave.scene = l.path_scene;
@@ -136,6 +146,48 @@ rb_status ensure_film(rb_context* c, int32_t width, int32_t height, bool reset) 
 // Records one wave of buffers `w` on stream `s` into a graph: counter reset,
 // camera rays and bounces, and with_end the film resolve / guide training that
 // close the wave. Kept while the configuration is unchanged.
+// Appends the drain loop to the graph being captured on `s`: a kernel that sets
+// the loop condition from the active count, then a conditional WHILE node whose
+// body (captured on `body`) is two bounces and the condition update. The first
+// body bounce reads the queue the host-driven loop would read after max_depth
+// bounces; a second bounce on an emptied queue launches kernels that find no
+// work.
+cudaError_t capture_drain(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s, cudaStream_t body, uint32_t* counters,
+	uint32_t max_depth, const gpu::launch_cfg& cfg) {
+	cudaStreamCaptureStatus status;
+	cudaGraph_t graph = nullptr;
+	const cudaGraphNode_t* deps = nullptr;
+	size_t ndeps = 0;
+	cudaError_t e = cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps);
+	if (e != cudaSuccess) return e;
+	if (status != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+	cudaGraphConditionalHandle h;
+	e = cudaGraphConditionalHandleCreate(&h, graph, 0u, cudaGraphCondAssignDefault);
+	if (e == cudaSuccess) e = gpu::launch_drain_begin(h, counters, s);
+	if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps);
+	if (e != cudaSuccess) return e;
+	cudaGraphNodeParams np{};
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = h;
+	np.conditional.type = cudaGraphCondTypeWhile;
+	np.conditional.size = 1;
+	cudaGraphNode_t node;
+	e = cudaGraphAddNode(&node, graph, deps, ndeps, &np);
+	if (e != cudaSuccess) return e;
+	cudaGraph_t body_graph = np.conditional.phGraph_out[0];
+	e = cudaStreamBeginCaptureToGraph(body, body_graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+	if (e != cudaSuccess) return e;
+	const uint32_t q = max_depth & 1u;
+	e = gpu::launch_bounce(c->view, w, c->film, q, cfg, body);
+	if (e == cudaSuccess) e = gpu::launch_bounce(c->view, w, c->film, q ^ 1u, cfg, body);
+	if (e == cudaSuccess) e = gpu::launch_drain_step(h, counters, body);
+	cudaGraph_t captured = nullptr;
+	const cudaError_t e2 = cudaStreamEndCapture(body, &captured);
+	if (e != cudaSuccess) return e;
+	if (e2 != cudaSuccess) return e2;
+	return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
 rb_status capture_into(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s, uint32_t* counters, uint32_t max_depth,
 	bool with_end, cudaGraphExec_t& graph, graph_key& current) {
 	const gpu::launch_cfg cfg = c->cfg();
@@ -164,14 +216,26 @@ rb_status capture_into(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s
 	if (graph) cudaGraphExecDestroy(graph);
 	graph = nullptr;
 	current = graph_key();
+	// scenes with invisible entities: the drain loop's body is captured on a
+	// second stream into the conditional node's child graph
+	const bool drain = c->has_invisible;
+	cudaStream_t body_stream = nullptr;
+	if (drain) RB_CUDA(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
 	cudaGraph_t g = nullptr;
-	RB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-	cudaError_t e = cudaMemsetAsync(counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), s);
+	cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+	if (e != cudaSuccess) {
+		if (body_stream) cudaStreamDestroy(body_stream);
+		return from_cuda(e);
+	}
+	e = cudaMemsetAsync(counters, 0, gpu::kWaveCounterWords * sizeof(uint32_t), s);
 	if (e == cudaSuccess) e = gpu::launch_wave(c->view, w, c->film, max_depth, 0u, cfg, s);
+	if (e == cudaSuccess && drain) e = capture_drain(c, w, s, body_stream, counters, max_depth, cfg);
 	if (e == cudaSuccess && with_end) e = gpu::launch_wave_end(w, c->film, c->num_sms * 4, cfg, s);
 	const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+	if (body_stream) cudaStreamDestroy(body_stream);
 	if (e != cudaSuccess || e2 != cudaSuccess) {
 		if (g) cudaGraphDestroy(g);
+		if (drain) c->drain_graph_failed = true;
 		return from_cuda(e != cudaSuccess ? e : e2);
 	}
 	e = cudaGraphInstantiate(&graph, g, 0);
@@ -250,7 +314,8 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 // path tracing replayed from graphs, with at least two waves.
 uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& cfg) {
 	const uint32_t want = resolved_tuning(c->tuning).lanes;
-	if (want <= 1 || cfg.volume || c->profiling || c->has_invisible) return 1;
+	if (want <= 1 || (cfg.volume && cfg.guide != nullptr) || c->profiling || (c->has_invisible && c->drain_graph_failed))
+		return 1;
 	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
 	return static_cast<uint32_t>(waves < want ? waves : want);
 }
@@ -276,7 +341,10 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 		}
 	}
 	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
-	const bool use_graph = !c->has_invisible && !c->profiling;
+	// scenes with invisible entities replay graphs too (their drain loop is a
+	// conditional node) unless the runtime refused that node
+	const bool use_graph = !c->profiling && !(c->has_invisible && c->drain_graph_failed);
+	const uint32_t drain_begin = c->has_invisible ? 1u : 0u;  // launches of the drain set-up per graph wave
 	c->next_event = 0;
 	const bool guided = nlanes > 1 && cfg.guide != nullptr;
 	const bool training = guided && (cfg.guide_mode & gpu::GUIDE_TRAIN);
@@ -300,9 +368,11 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			wave_lane& l = c->lanes[k];
 			st = capture_into(c, l.wave, l.stream, l.counters, max_depth, false, l.graph, l.key);
 		}
+		if (st != RB_OK && c->has_invisible && c->drain_graph_failed) return run_waves(c, total, max_depth, record_waves);
 		if (st != RB_OK) return st;
 	} else if (use_graph) {
 		st = capture_wave(c, max_depth);
+		if (st != RB_OK && c->has_invisible && c->drain_graph_failed) return run_waves(c, total, max_depth, record_waves);
 		if (st != RB_OK) return st;
 	}
 	uint32_t launches = 0;
@@ -329,7 +399,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			RB_CUDA(gpu::launch_wave_end(w, c->film, c->num_sms * 4, cfg, s));
 			if (training) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[lane], s));
 			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
-			launches += gpu::wave_launches(max_depth, cfg) + 1u;
+			launches += gpu::wave_launches(max_depth, cfg) + 1u + drain_begin;
 		}
 		for (uint32_t k = 0; k + 1 < nlanes; k++) {
 			wave_lane& l = c->lanes[k];
@@ -344,7 +414,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			if (use_graph) {
 				// the graph's last node moves params->first_item to the next wave
 				RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
-				launches += gpu::wave_launches(max_depth, cfg);
+				launches += gpu::wave_launches(max_depth, cfg) + drain_begin;
 			} else {
 				// direct launches: profiling, or invisible entities (a pass-through
 				// does not count as a bounce, so keep bouncing until the queue drains)
@@ -381,6 +451,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 		s.node_visits += u64(a, gpu::CNT_NODE_VISITS);
 		s.triangle_tests += u64(a, gpu::CNT_TRI_TESTS);
 		if (s.device_error == 0) s.device_error = a[gpu::CNT_ERROR];
+		if (use_graph) launches += a[gpu::CNT_DRAIN_TOTAL] * gpu::drain_launches(cfg);
 	}
 	h[gpu::CNT_ERROR] = s.device_error;
 	s.samples = total;

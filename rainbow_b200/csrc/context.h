@@ -130,6 +130,11 @@ struct wave_lane {
 	uint32_t* counters = nullptr;    // device
 	gpu::wave_params* params = nullptr;  // device
 	uint32_t* path_scene = nullptr;  // batch renders: scene of each path
+	uint32_t vol_alloc = 0;          // volume renders: paths the lane's medium / beam buffers hold
+	int32_t* vol_medium = nullptr;
+	pt::vol_rec* vol_rec = nullptr;
+	float4* vol_beam = nullptr;
+	uint32_t* vol_beam_queue = nullptr;
 	cudaStream_t stream = nullptr;
 	cudaGraphExec_t graph = nullptr;
 	graph_key key;
@@ -145,6 +150,8 @@ struct wave_lane {
 		dev_free(counters);
 		dev_free(params);
 		dev_free(path_scene);
+		dev_free(vol_medium); dev_free(vol_rec); dev_free(vol_beam); dev_free(vol_beam_queue);
+		vol_alloc = 0;
 		if (done) cudaEventDestroy(done);
 		if (stream) cudaStreamDestroy(stream);
 		done = nullptr;
@@ -168,6 +175,7 @@ struct rb_context {
 
 	bool has_scene = false;
 	bool has_invisible = false;
+	bool drain_graph_failed = false;  // the runtime refused the drain loop's conditional node: host-driven drain
 	uint32_t bvh_depth = 0;
 	uint32_t num_entities = 0;
 	device_scene scene;

@@ -1554,6 +1554,40 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 	return e;
 }
 
+namespace {
+
+__global__ void k_drain_begin(cudaGraphConditionalHandle h, uint32_t* counters) {
+	counters[CNT_DRAIN_WAVE] = 0u;
+	cudaGraphSetConditional(h, counters[CNT_ACTIVE] != 0u ? 1u : 0u);
+}
+
+__global__ void k_drain_step(cudaGraphConditionalHandle h, uint32_t* counters) {
+	const uint32_t it = counters[CNT_DRAIN_WAVE] + 1u;
+	counters[CNT_DRAIN_WAVE] = it;
+	counters[CNT_DRAIN_TOTAL] += 1u;
+	cudaGraphSetConditional(h, counters[CNT_ACTIVE] != 0u && it < kMaxDrainIterations ? 1u : 0u);
+}
+
+} // namespace
+
+cudaError_t launch_drain_begin(cudaGraphConditionalHandle h, uint32_t* counters, cudaStream_t stream) {
+	k_drain_begin<<<1, 1, 0, stream>>>(h, counters);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_drain_step(cudaGraphConditionalHandle h, uint32_t* counters, cudaStream_t stream) {
+	k_drain_step<<<1, 1, 0, stream>>>(h, counters);
+	return cudaGetLastError();
+}
+
+uint32_t bounce_launches(const launch_cfg& cfg) {
+	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
+	if (cfg.volume) return 12u + (sample ? (cfg.guide_medium != nullptr ? 2u : 1u) : 0u);
+	return (cfg.sort == RB_SORT_NONE ? 7u : 12u) + (sample ? 1u : 0u);
+}
+
+uint32_t drain_launches(const launch_cfg& cfg) { return 2u * bounce_launches(cfg) + 1u; }
+
 uint32_t wave_launches_unbinned(uint32_t max_depth, const launch_cfg& cfg);
 
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg) {

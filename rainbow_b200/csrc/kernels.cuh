@@ -29,7 +29,9 @@ enum : uint32_t {
 	CNT_GUIDE_MEDIUM = 25,  // medium vertices queued for a medium-guide evaluation this bounce
 	CNT_FETCH_EXTEND = 26,  // rays taken from the active queue by the persistent extend kernel
 	CNT_FETCH_SECONDARY = 27,  // rays taken from the secondary queue by the persistent secondary kernel
-	CNT_WORDS = 28
+	CNT_DRAIN_WAVE = 28,    // drain-loop iterations of the current wave (below)
+	CNT_DRAIN_TOTAL = 29,   // drain-loop iterations of the render call
+	CNT_WORDS = 30
 };
 static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
 // words cleared at the start of a wave: everything before the 64-bit stats
@@ -194,6 +196,19 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 
 // Kernel launches of one wave for a given configuration (for the stats).
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg);
+
+// Drain loop of scenes with invisible entities. A pass through an invisible
+// boundary is not a bounce, so paths can outlive max_depth iterations; after
+// them a wave keeps bouncing until its active queue is empty. Inside a wave's
+// graph this loop is a conditional WHILE node: launch_drain_begin sets its
+// condition from the active count, and each iteration runs two bounces, then
+// launch_drain_step, which sets the condition again (at most
+// kMaxDrainIterations iterations per wave: 4096 bounces).
+constexpr uint32_t kMaxDrainIterations = 2048;
+cudaError_t launch_drain_begin(cudaGraphConditionalHandle h, uint32_t* counters, cudaStream_t stream);
+cudaError_t launch_drain_step(cudaGraphConditionalHandle h, uint32_t* counters, cudaStream_t stream);
+uint32_t bounce_launches(const launch_cfg& cfg);  // kernels of one launch_bounce
+uint32_t drain_launches(const launch_cfg& cfg);   // kernels of one drain iteration
 
 // One extra bounce (used when invisible entities make paths outlive max_depth iterations).
 cudaError_t launch_bounce(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,

@@ -1,0 +1,37 @@
+"""Scenes with invisible entities (here the boundary of the fog's medium): a
+pass through one is not a bounce, so a wave keeps bouncing after max_depth
+iterations until its paths are done. That drain loop runs inside each wave's
+CUDA graph as a conditional WHILE node, on one or several wave lanes; the
+host-driven loop of direct launches (the profiling path) must give the same
+paths and the same film."""
+import pytest
+
+import rainbow_b200 as rb
+from tests.test_gpu_batch import assert_films_close
+
+pytestmark = pytest.mark.gpu
+
+
+def _fog():
+    return rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=64, height=48, num_spheres=12, subdivision=2)
+
+
+@pytest.mark.parametrize("volume", [True, False])
+def test_drain_graph_equals_host_loop(volume):
+    sc = _fog()
+    with rb.Context(0) as ctx:
+        ctx.upload(sc)
+        # depth 3: most paths cross the medium's boundary more often than that
+        ctx.set_profiling(True)
+        ctx.render(sc.camera, 8, max_depth=3, seed=3, volume=volume, want_image=False, paths_per_wave=4096)
+        want, want_rays = ctx.film(), ctx.stats().extend_rays
+        assert ctx.stats().device_error == 0
+        ctx.set_profiling(False)
+        for tuning in (dict(lanes=1, paths_per_wave=4096), dict(lanes=3, paths_per_wave=4096),
+                       dict(lanes=2, paths_per_wave=7000, sort=rb.RB_SORT_NONE)):
+            ctx.set_tuning(**tuning)
+            ctx.render(sc.camera, 8, max_depth=3, seed=3, volume=volume, want_image=False)
+            st = ctx.stats()
+            assert st.device_error == 0, tuning
+            assert st.extend_rays == want_rays, tuning
+            assert_films_close(ctx.film(), want, str(tuning))
