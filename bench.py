@@ -291,6 +291,22 @@ def spheres_s5_leg(rb, device, spp=8):
             "mrays_per_s": (st.extend_rays + st.shadow_rays + st.mis_rays) / st.elapsed_ms / 1e3, "tuning": t.as_dict()}
 
 
+def config5_leg(rb, device, spp=8):
+    """Configuration 5 without guiding: the fog (400 displaced spheres at subdivision 5, 8,192,046 triangles,
+    inside an invisible box holding a homogeneous medium), 1920 x 1080, depth 12, volume path tracing, one
+    call of `spp` samples per pixel with launch shapes tuned for volume renders."""
+    scene = rb.generate_scene(rb.RB_SCENE_FOG, seed=5, width=1920, height=1080, num_spheres=400, subdivision=5)
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    t, _ = ctx.tune_render(scene.camera, probe_spp=2, max_depth=12, seed=90, volume=True)
+    ctx.render(scene.camera, spp, max_depth=12, seed=3, volume=True, want_image=False)
+    st = ctx.stats()
+    ctx.close()
+    return {"workload": f"fog, {scene.num_triangles} triangles, 1920x1080, {spp} spp, depth 12, volume path tracing",
+            "msamples_per_s": 1920 * 1080 * spp / st.elapsed_ms / 1e3, "ms": st.elapsed_ms,
+            "mrays_per_s": (st.extend_rays + st.shadow_rays + st.mis_rays) / st.elapsed_ms / 1e3, "tuning": t.as_dict()}
+
+
 def batch_workload(seed=2, count=64):
     """The batched configuration: `count` seeded sphere scenes whose triangle counts are
     log-uniform in [1k, 500k] (displaced icospheres: subdivision and sphere count chosen
@@ -491,7 +507,8 @@ def main():
     extra = {}
     if rank == 0 and world == 1 and not args.no_batched:
         for name, leg in (("config1", lambda: config1_leg(rb, local, os.cpu_count() or 1)),
-                          ("spheres_s5", lambda: spheres_s5_leg(rb, local))):
+                          ("spheres_s5", lambda: spheres_s5_leg(rb, local)),
+                          ("config5_plain", lambda: config5_leg(rb, local))):
             try:
                 extra[name] = leg()
             except Exception as e:  # reported, never required for the throughput line
