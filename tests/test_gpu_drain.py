@@ -35,3 +35,20 @@ def test_drain_graph_equals_host_loop(volume):
             assert st.device_error == 0, tuning
             assert st.extend_rays == want_rays, tuning
             assert_films_close(ctx.film(), want, str(tuning))
+
+
+def test_guided_waves_on_lanes_with_invisible_entities():
+    """Guided path tracing with online training on wave lanes, on a scene whose
+    waves drain past max_depth: no device error, the guide trains, and the
+    image mean agrees with a converged plain render."""
+    sc = rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=32, height=24, num_spheres=12, subdivision=2)
+    with rb.Context(0) as ctx:
+        ctx.upload(sc)
+        ref = ctx.render(sc.camera, 8192, max_depth=5, seed=100)
+        ctx.set_tuning(lanes=2, paths_per_wave=8192)
+        ctx.guide_init(seed=0, batch_size=8192, min_rows=1024, steps_per_wave=2)
+        ctx.render(sc.camera, 512, max_depth=5, seed=7, guide=True, train=True, want_image=False)
+        assert ctx.guide_stats().steps > 0
+        img = ctx.render(sc.camera, 4096, max_depth=5, seed=9, guide=True)
+        assert ctx.stats().device_error == 0
+    assert abs(float(img.mean()) / float(ref.mean()) - 1.0) < 0.02, (img.mean(), ref.mean())
