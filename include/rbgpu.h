@@ -345,8 +345,9 @@ typedef struct rb_tuning {
 	                               stage code); 0: library default (64: none), >= max_depth: none */
 	uint32_t lanes;             /* wave lanes (1..8, 0: 1): each lane has its own path buffers, stream and
 	                               graph, so the late bounces of one wave overlap the next wave's early
-	                               ones; the film still adds the waves in order (plain, batched, guided
-	                               and volume renders; guided volume renders use one lane) */
+	                               ones; the film still adds the waves in order (every render kind;
+	                               guided waves sample the weights their lane saw after its previous
+	                               wave trained) */
 	uint32_t traversal;         /* RB_TRAVERSAL_*: how the traversal kernels take rays */
 	uint32_t smem_carveout;     /* traversal kernels' shared-memory share of the L1 / shared storage, in
 	                               percent + 1 (1..101); 0: the largest share (4 blocks of 256 threads with

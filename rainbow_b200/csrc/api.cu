@@ -100,6 +100,7 @@ rb_status ensure_lanes(rb_context* c, uint32_t count) {
 		l.wave.counters = l.counters;
 		l.wave.params = l.params;
 		l.wave.guide = guide::wave_guide{};
+		l.wave.guide_medium = guide::wave_guide{};
 		if (c->volume && l.vol_alloc < c->wave_capacity) {
 			l.release_graph();
 			dev_free(l.vol_medium); dev_free(l.vol_rec); dev_free(l.vol_beam); dev_free(l.vol_beam_queue);
@@ -310,12 +311,11 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 	return RB_OK;
 }
 
-// Wave lanes a render call can use: more than one only for plain and batched
-// path tracing replayed from graphs, with at least two waves.
+// Wave lanes a render call can use: more than one for any render replayed
+// from graphs (not while profiling), with at least two waves.
 uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& cfg) {
 	const uint32_t want = resolved_tuning(c->tuning).lanes;
-	if (want <= 1 || (cfg.volume && cfg.guide != nullptr) || c->profiling || (c->has_invisible && c->drain_graph_failed))
-		return 1;
+	if (want <= 1 || c->profiling || (c->has_invisible && c->drain_graph_failed)) return 1;
 	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
 	return static_cast<uint32_t>(waves < want ? waves : want);
 }
@@ -362,6 +362,16 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			const guide::wave_guide wg = guide::lane_view(c->guide, lg);
 			if (k == 0) c->wave.guide = wg;
 			else c->lanes[k - 1].wave.guide = wg;
+			if (st != RB_OK || cfg.guide_medium == nullptr) continue;
+			// guided volume renders: the medium guide's lane buffers and snapshot alike
+			guide::lane_guide& lm = c->lane_guides_medium[k];
+			const float4* before_m = lm.query_in;
+			const cudaError_t em = guide::allocate_lane(lm, c->wave_capacity, max_depth);
+			if (em != cudaSuccess) st = from_cuda(em);
+			else if (lm.query_in != before_m) c->release_graph();
+			const guide::wave_guide wm = guide::lane_view(c->guide_medium, lm);
+			if (k == 0) c->wave.guide_medium = wm;
+			else c->lanes[k - 1].wave.guide_medium = wm;
 		}
 		if (st == RB_OK) st = capture_into(c, c->wave, c->stream, c->counters, max_depth, false, c->graph, c->graph_cfg);
 		for (uint32_t k = 0; k + 1 < nlanes && st == RB_OK; k++) {
@@ -378,7 +388,11 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 	uint32_t launches = 0;
 	hp.first_item = 0;
 	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
-	for (uint32_t k = 0; guided && k < nlanes; k++) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[k], c->stream));
+	for (uint32_t k = 0; guided && k < nlanes; k++) {
+		RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[k], c->stream));
+		if (cfg.guide_medium != nullptr)
+			RB_CUDA(guide::launch_snapshot(*cfg.guide_medium, c->lane_guides_medium[k], c->stream));
+	}
 	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
 	if (nlanes > 1) {
 		for (uint32_t k = 0; k + 1 < nlanes; k++) {
@@ -398,6 +412,8 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			// in wave order: training-sample collection, film resolve, training, then this lane's snapshot
 			RB_CUDA(gpu::launch_wave_end(w, c->film, c->num_sms * 4, cfg, s));
 			if (training) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[lane], s));
+			if (training && cfg.guide_medium != nullptr)
+				RB_CUDA(guide::launch_snapshot(*cfg.guide_medium, c->lane_guides_medium[lane], s));
 			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
 			launches += gpu::wave_launches(max_depth, cfg) + 1u + drain_begin;
 		}

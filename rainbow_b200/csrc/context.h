@@ -209,6 +209,7 @@ struct rb_context {
 	guide::guide_state guide;        // learned path guide (allocated on first use)
 	guide::guide_state guide_medium; // guide of medium vertices in guided volume renders
 	guide::lane_guide lane_guides[kMaxLanes];  // per-lane guide buffers and weight snapshots (guided renders on lanes)
+	guide::lane_guide lane_guides_medium[kMaxLanes];  // the same for the medium guide (guided volume renders)
 	uint32_t guide_mode = 0;         // gpu::GUIDE_* of the current render call
 	rb_tuning tuning{};              // launch shapes of render calls (zeros: defaults)
 	// batched rendering: the uploaded scenes (geometry part of their records;
@@ -291,6 +292,7 @@ struct rb_context {
 		for (wave_lane& l : lanes) l.release();
 		lanes.clear();
 		for (guide::lane_guide& g : lane_guides) guide::release_lane(g);
+		for (guide::lane_guide& g : lane_guides_medium) guide::release_lane(g);
 	}
 	void release_film() {
 		dev_free(film.sum); dev_free(film.sum_sq); dev_free(film.count); dev_free(film_mean);

@@ -92,26 +92,32 @@ def _mean_var(ctx):
     return m, np.maximum(sq / c[..., None] - m ** 2, 0) / c[..., None]
 
 
-def test_untrained_volume_guides_render_plain_bits():
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_untrained_volume_guides_render_plain_bits(lanes):
     """Guided volume rendering before any training step samples the BSDF and
-    the phase function with plain volume path tracing's random numbers."""
+    the phase function with plain volume path tracing's random numbers (on
+    one lane, and on three lanes of four waves)."""
     scene = _fog(24)
     with rb.Context(0) as ctx:
         ctx.upload(scene)
+        ctx.set_tuning(lanes=lanes, paths_per_wave=24 * 24 * 2)
         ctx.guide_init(seed=0)
         plain = ctx.render(scene.camera, 8, max_depth=8, seed=5, volume=True)
         guided = ctx.render(scene.camera, 8, max_depth=8, seed=5, volume=True, guide=True)
         assert np.array_equal(plain, guided)
 
 
-def test_guided_volume_render_is_unbiased():
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_guided_volume_render_is_unbiased(lanes):
     """Surface and medium guides trained online on the fog scene, then a guided
     volume render against a converged plain volume render: 4 x 4 block z-scores
-    and the image mean (one-sample MIS keeps the estimator unbiased)."""
+    and the image mean (one-sample MIS keeps the estimator unbiased). On three
+    lanes each wave samples both guides' weight snapshots of its lane."""
     res, B, depth = 32, 4, 8
     scene = _fog(res)
     with rb.Context(0) as ctx:
         ctx.upload(scene)
+        ctx.set_tuning(lanes=lanes)
         ctx.render(scene.camera, 16384, max_depth=depth, seed=100, volume=True, want_image=False)
         ref, ref_var = _mean_var(ctx)
         ctx.guide_init(seed=0, batch_size=16384, min_rows=1024, steps_per_wave=4)
