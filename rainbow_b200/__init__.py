@@ -159,16 +159,23 @@ class Context:
 
     def render(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5, threshold: float = 1.0,
                seed: int = 0, reset: bool = True, paths_per_wave: int = 0, want_image: bool = True,
-               guide: bool = False, train: bool = False, volume: bool = False):
+               guide: bool = False, train: bool = False, volume: bool = False, out: np.ndarray = None):
         """guide / train: learned path guiding (RB_RENDER_GUIDE / RB_RENDER_TRAIN); volume:
-        volume_path_integrator instead of path_integrator (RB_RENDER_VOLUME)."""
+        volume_path_integrator instead of path_integrator (RB_RENDER_VOLUME). out: a
+        C-contiguous float32 (height, width, 3) array to write the image into (when its memory
+        is page-locked, slices are copied while later waves still run); returned instead of a
+        new array."""
         p = RenderParams()
         p.camera = camera
         p.spp, p.first_sample, p.max_depth, p.rr_threshold = spp, first_sample, max_depth, threshold
         flags = (RB_RENDER_RESET if reset else 0) | (RB_RENDER_GUIDE if guide else 0) | (RB_RENDER_TRAIN if train else 0)
         flags |= RB_RENDER_VOLUME if volume else 0
         p.seed, p.flags, p.paths_per_wave = seed, flags, paths_per_wave
-        img = np.zeros((camera.height, camera.width, 3), dtype=np.float32) if want_image else None
+        if out is not None:
+            if out.dtype != np.float32 or out.shape != (camera.height, camera.width, 3) or not out.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous float32 array of shape (height, width, 3)")
+            want_image = True
+        img = out if out is not None else (np.zeros((camera.height, camera.width, 3), dtype=np.float32) if want_image else None)
         self._film_shape = (camera.width, camera.height)
         check(lib().rb_render(self._h, C.byref(p), img.ctypes.data if want_image else None), "rb_render")
         return img

@@ -8,6 +8,7 @@
 // work item written to a device-side parameter block before the replay.
 #include "context.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -327,7 +328,30 @@ uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& c
 // and stream) and its film resolve waits for wave j - 1's, so the waves'
 // bounces overlap while the film adds them in order. record_waves: event
 // c->wave_events[j] after wave j's resolve. Fills the call's statistics.
-rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves) {
+bool is_page_locked(const void* p) {
+	cudaPointerAttributes a{};
+	if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+		cudaGetLastError();  // unknown pointers are plain host memory here
+		return false;
+	}
+	return a.type == cudaMemoryTypeHost;
+}
+
+// Means of the pixels made final by the items resolved so far, copied to the
+// caller's buffer on stream s (see image_readback).
+rb_status readback_after(rb_context* c, image_readback* r, uint64_t resolved_items, cudaStream_t s) {
+	if (r == nullptr || resolved_items <= r->final_from) return RB_OK;
+	const uint64_t upto = std::min<uint64_t>(r->pixels, resolved_items - r->final_from);
+	if (upto <= r->done) return RB_OK;
+	const size_t first = static_cast<size_t>(r->done), n = static_cast<size_t>(upto - r->done);
+	const gpu::film_buffers f{c->film.sum + 3 * first, c->film.sum_sq + 3 * first, c->film.count + first};
+	RB_CUDA(gpu::launch_film_mean(f, static_cast<uint32_t>(n), c->film_mean + 3 * first, c->num_sms, s));
+	RB_CUDA(cudaMemcpyAsync(r->host + 3 * first, c->film_mean + 3 * first, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+	r->done = upto;
+	return RB_OK;
+}
+
+rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves, image_readback* readback) {
 	gpu::wave_params& hp = *c->params_host;
 	rb_status st = RB_OK;
 	const gpu::launch_cfg cfg = c->profiled_cfg();
@@ -378,11 +402,13 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			wave_lane& l = c->lanes[k];
 			st = capture_into(c, l.wave, l.stream, l.counters, max_depth, false, l.graph, l.key);
 		}
-		if (st != RB_OK && c->has_invisible && c->drain_graph_failed) return run_waves(c, total, max_depth, record_waves);
+		if (st != RB_OK && c->has_invisible && c->drain_graph_failed)
+			return run_waves(c, total, max_depth, record_waves, readback);
 		if (st != RB_OK) return st;
 	} else if (use_graph) {
 		st = capture_wave(c, max_depth);
-		if (st != RB_OK && c->has_invisible && c->drain_graph_failed) return run_waves(c, total, max_depth, record_waves);
+		if (st != RB_OK && c->has_invisible && c->drain_graph_failed)
+			return run_waves(c, total, max_depth, record_waves, readback);
 		if (st != RB_OK) return st;
 	}
 	uint32_t launches = 0;
@@ -415,6 +441,8 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			if (training && cfg.guide_medium != nullptr)
 				RB_CUDA(guide::launch_snapshot(*cfg.guide_medium, c->lane_guides_medium[lane], s));
 			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
+			st = readback_after(c, readback, std::min<uint64_t>(total, (j + 1) * c->wave_capacity), s);
+			if (st != RB_OK) return st;
 			launches += gpu::wave_launches(max_depth, cfg) + 1u + drain_begin;
 		}
 		for (uint32_t k = 0; k + 1 < nlanes; k++) {
@@ -449,6 +477,8 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 				RB_CUDA(gpu::launch_wave_end(c->wave, c->film, c->num_sms * 4, cfg, c->stream));
 			}
 			if (record_waves) RB_CUDA(cudaEventRecord(c->wave_events[wave], c->stream));
+			st = readback_after(c, readback, std::min<uint64_t>(total, first + c->wave_capacity), c->stream);
+			if (st != RB_OK) return st;
 		}
 	}
 	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
@@ -791,17 +821,29 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		}
 	}
 
-	st = run_waves(c, total, prm->max_depth, false);
+	// a page-locked output buffer receives each slice of the image as soon as
+	// its pixels are final, overlapped with the waves still running
+	image_readback overlap;
+	const bool overlapped = rgb_out != nullptr && is_page_locked(rgb_out);
+	if (overlapped) {
+		overlap.host = rgb_out;
+		overlap.pixels = pixels;
+		overlap.final_from = total - pixels;
+	}
+	st = run_waves(c, total, prm->max_depth, false, overlapped ? &overlap : nullptr);
 	if (st != RB_OK) return st;
 	const uint32_t* h = c->counters_host;
 	c->film_samples += prm->spp;
 	if (h[gpu::CNT_ERROR] != 0) return static_cast<rb_status>(h[gpu::CNT_ERROR]);
 
-	if (rgb_out != nullptr) {
+	if (rgb_out != nullptr && !(overlapped && overlap.done == pixels)) {
 		// means on the device, then one copy of 3 floats per pixel (at full speed
 		// when the caller's buffer is page-locked)
-		RB_CUDA(gpu::launch_film_mean(c->film, static_cast<uint32_t>(pixels), c->film_mean, c->num_sms * 4, c->stream));
-		RB_CUDA(cudaMemcpyAsync(rgb_out, c->film_mean, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+		const size_t first = overlapped ? static_cast<size_t>(overlap.done) : 0u, n = static_cast<size_t>(pixels) - first;
+		const gpu::film_buffers f{c->film.sum + 3 * first, c->film.sum_sq + 3 * first, c->film.count + first};
+		RB_CUDA(gpu::launch_film_mean(f, static_cast<uint32_t>(n), c->film_mean + 3 * first, c->num_sms * 4, c->stream));
+		RB_CUDA(cudaMemcpyAsync(rgb_out + 3 * first, c->film_mean + 3 * first, 3 * n * sizeof(float), cudaMemcpyDeviceToHost,
+			c->stream));
 		RB_CUDA(cudaStreamSynchronize(c->stream));
 	}
 	return RB_OK;

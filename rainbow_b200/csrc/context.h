@@ -315,7 +315,19 @@ rb_status ensure_lanes(rb_context* c, uint32_t count);
 rb_status prepare_guide(rb_context* c, const rb_render_params* prm);
 rb_status prepare_volume(rb_context* c, const rb_render_params* prm);
 bool host_is_valid_camera(const rb_camera_desc& cam);
-rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves);
+// Copy-out of rb_render's image while the call's later waves still run: film
+// resolves add the waves in order and items are sample-major, so once the wave
+// holding item final_from + p has resolved, pixel p has all of the call's
+// samples; its mean then goes to the caller's page-locked buffer on that wave's
+// stream.
+struct image_readback {
+	float* host = nullptr;     // page-locked, 3 floats per pixel
+	uint64_t pixels = 0;
+	uint64_t final_from = 0;   // first item of the call's last sample
+	uint64_t done = 0;         // pixels already copied (or enqueued)
+};
+rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves,
+	image_readback* readback = nullptr);
 // Replaces the context's scene arrays with a packed scene (single or merged).
 rb_status upload_packed(rb_context* c, const host::packed_scene& p);
 
