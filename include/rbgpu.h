@@ -257,7 +257,10 @@ typedef struct rb_render_params {
 /* Render and write the per-pixel mean radiance (box filter, film::add_tile +
  * pixel::spectrum, film.cpp:11-21,207-223) of everything accumulated since the
  * last reset into rgb_out (caller-owned, width * height * 3 floats, row-major,
- * pixel (x, y) at (y * width + x) * 3). rgb_out may be NULL. */
+ * pixel (x, y) at (y * width + x) * 3). rgb_out may be NULL. When rgb_out is
+ * page-locked memory, each slice of it is copied as soon as its pixels have all
+ * of the call's samples, while later waves still run; if the call then fails,
+ * part of rgb_out may already be written. */
 rb_status rb_render(rb_context* ctx, const rb_render_params* params, float* rgb_out);
 
 /* Read back the accumulators: per-pixel sums of radiance (double, 3 per pixel),
