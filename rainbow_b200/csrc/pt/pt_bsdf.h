@@ -210,6 +210,10 @@ struct bsdf_t {
 	const material_rec* m;
 	float eta;  // collection eta (glass IOR, else 1)
 };
+// Lobe i's kind and type by selection rather than by an index into the
+// arrays, so the record stays in registers (at most two lobes).
+RB_HD uint32_t lobe_kind(const bsdf_t& b, uint32_t i) { return i == 0 ? b.kinds[0] : b.kinds[1]; }
+RB_HD uint32_t lobe_type(const bsdf_t& b, uint32_t i) { return i == 0 ? b.types[0] : b.types[1]; }
 
 RB_HD bsdf_t make_bsdf(const material_rec* m) {
 	bsdf_t b;
@@ -225,8 +229,10 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 		break;
 	case MAT_GLASS_ROUGH:
 		b.eta = m->eta;
-		if (m->has_reflect) { b.kinds[b.count] = LOBE_MF_REFLECT; b.types[b.count] = ST_GLOSSY | ST_REFLECTION; b.count++; }
-		if (m->has_transmit) { b.kinds[b.count] = LOBE_MF_TRANSMIT; b.types[b.count] = ST_GLOSSY | ST_TRANSMISSION; b.count++; }
+		b.kinds[0] = b.kinds[1] = LOBE_MF_TRANSMIT;
+		b.types[0] = b.types[1] = ST_GLOSSY | ST_TRANSMISSION;
+		if (m->has_reflect) { b.kinds[0] = LOBE_MF_REFLECT; b.types[0] = ST_GLOSSY | ST_REFLECTION; }
+		b.count = (m->has_reflect ? 1u : 0u) + (m->has_transmit ? 1u : 0u);
 		break;
 	case MAT_GLASS_SMOOTH:
 		b.eta = m->eta;
@@ -298,9 +304,9 @@ RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return b.m->diffuse * kInvPi;
 	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_f<MAT>(b.m, wo, wi);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
-		return b.kinds[i] == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi) : mf_transmit_f(b.m, wo, wi);
+		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi) : mf_transmit_f(b.m, wo, wi);
 	else {
-		switch (b.kinds[i]) {
+		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
 		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi);
 		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
@@ -313,9 +319,9 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
 	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_pdf(b.m, wo, wi);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
-		return b.kinds[i] == LOBE_MF_REFLECT ? mf_reflect_pdf(b.m, wo, wi) : mf_transmit_pdf(b.m, wo, wi);
+		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_pdf(b.m, wo, wi) : mf_transmit_pdf(b.m, wo, wi);
 	else {
-		switch (b.kinds[i]) {
+		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
 		case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
 		case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
@@ -328,7 +334,7 @@ template <int MAT>
 RB_HD lobe_sample sample_lambert(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
 	vec3 wi = cosine_hemisphere(u);
 	if (wo.z < 0.f) wi.z = -wi.z;
-	return lobe_sample{b.types[i], lobe_f<MAT>(b, i, wo, wi), wi, lobe_pdf<MAT>(b, i, wo, wi)};
+	return lobe_sample{lobe_type(b, i), lobe_f<MAT>(b, i, wo, wi), wi, lobe_pdf<MAT>(b, i, wo, wi)};
 }
 template <int MAT>
 RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
@@ -338,7 +344,7 @@ RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u
 	if (dot(wo, wh) < 0.f) return no_sample();
 	const vec3 wi = reflect(wo, wh);
 	if (!same_hemisphere(wo, wi)) return no_sample();
-	return lobe_sample{b.types[i], mf_reflect_f<MAT>(m, wo, wi), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
+	return lobe_sample{lobe_type(b, i), mf_reflect_f<MAT>(m, wo, wi), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
 }
 RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
 	const material_rec* m = b.m;
@@ -349,7 +355,7 @@ RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 
 	const float eta = entering ? (1.f / m->eta) : (m->eta / 1.f);
 	const vec3 wi = refract(wo, wh, eta);
 	if (is_zero(wi)) return no_sample();
-	return lobe_sample{b.types[i], mf_transmit_f(m, wo, wi), wi, mf_transmit_pdf(m, wo, wi)};
+	return lobe_sample{lobe_type(b, i), mf_transmit_f(m, wo, wi), wi, mf_transmit_pdf(m, wo, wi)};
 }
 // fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
 RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
@@ -374,9 +380,9 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return sample_lambert<MAT>(b, i, wo, u);
 	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return sample_mf_reflect<MAT>(b, i, wo, u);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
-		return b.kinds[i] == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u) : sample_mf_transmit(b, i, wo, u);
+		return lobe_kind(b, i) == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u) : sample_mf_transmit(b, i, wo, u);
 	else {
-		switch (b.kinds[i]) {
+		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT: return sample_lambert<MAT_ANY>(b, i, wo, u);
 		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u);
 		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u);
@@ -394,7 +400,7 @@ RB_HD spectrum bsdf_f(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
 	const uint32_t rt = same_hemisphere(wo, wi) ? ST_REFLECTION : ST_TRANSMISSION;
 	spectrum f{0.f, 0.f, 0.f};
 	for (uint32_t i = 0; i < b.count; i++)
-		if (type_match(include, b.types[i]) && type_match(b.types[i], rt)) f = f + lobe_f<MAT>(b, i, wo, wi);
+		if (type_match(include, lobe_type(b, i)) && type_match(lobe_type(b, i), rt)) f = f + lobe_f<MAT>(b, i, wo, wi);
 	return f;
 }
 // scattering_function_collection::pdf (:131-148)
@@ -404,7 +410,7 @@ RB_HD float bsdf_pdf(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
 	uint32_t n = 0;
 	float pdf = 0.f;
 	for (uint32_t i = 0; i < b.count; i++)
-		if (type_match(include, b.types[i])) {
+		if (type_match(include, lobe_type(b, i))) {
 			pdf = pdf + lobe_pdf<MAT>(b, i, wo, wi);
 			n++;
 		}
@@ -413,17 +419,21 @@ RB_HD float bsdf_pdf(const bsdf_t& b, vec3 wo, vec3 wi, uint32_t include) {
 RB_HD uint32_t bsdf_count(const bsdf_t& b, uint32_t include) {
 	uint32_t n = 0;
 	for (uint32_t i = 0; i < b.count; i++)
-		if (type_match(include, b.types[i])) n++;
+		if (type_match(include, lobe_type(b, i))) n++;
 	return n;
 }
 // scattering_function_collection::sample (:48-100) with wo already in the
 // shading frame; the returned wi is in the shading frame too.
 template <int MAT = MAT_ANY>
 RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include) {
-	uint32_t idx[2];
-	uint32_t n = 0;
+	// matching lobes in order: idx0, then idx1
+	uint32_t idx0 = 0, idx1 = 0, n = 0;
 	for (uint32_t i = 0; i < b.count; i++)
-		if (type_match(include, b.types[i])) idx[n++] = i;
+		if (type_match(include, lobe_type(b, i))) {
+			if (n == 0) idx0 = i;
+			else idx1 = i;
+			n++;
+		}
 	if (n == 0) return no_sample();
 	const float fn = static_cast<float>(n);
 	uint32_t which = static_cast<uint32_t>(floorf(u.x * fn));
@@ -431,15 +441,15 @@ RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include
 	const float rx = u.x * fn - static_cast<float>(which);
 	const vec2 ur{(kOneMinusEps < rx) ? kOneMinusEps : rx, u.y};
 	if (wo.z == 0.f) return no_sample();
-	lobe_sample s = lobe_sample_dir<MAT>(b, idx[which], wo, ur);
+	lobe_sample s = lobe_sample_dir<MAT>(b, which == 0 ? idx0 : idx1, wo, ur);
 	if (s.pdf == 0.f) return no_sample();
 	if (!type_match(s.type, ST_SPECULAR)) {
 		const uint32_t rt = same_hemisphere(wo, s.wi) ? ST_REFLECTION : ST_TRANSMISSION;
 		s.f = spectrum{0.f, 0.f, 0.f};
 		s.pdf = 0.f;
 		for (uint32_t k = 0; k < n; k++) {
-			const uint32_t i = idx[k];
-			if (type_match(b.types[i], rt)) s.f = s.f + lobe_f<MAT>(b, i, wo, s.wi);
+			const uint32_t i = k == 0 ? idx0 : idx1;
+			if (type_match(lobe_type(b, i), rt)) s.f = s.f + lobe_f<MAT>(b, i, wo, s.wi);
 			s.pdf = s.pdf + lobe_pdf<MAT>(b, i, wo, s.wi);
 		}
 	}
