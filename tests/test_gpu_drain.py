@@ -52,3 +52,20 @@ def test_guided_waves_on_lanes_with_invisible_entities():
         img = ctx.render(sc.camera, 4096, max_depth=5, seed=9, guide=True)
         assert ctx.stats().device_error == 0
     assert abs(float(img.mean()) / float(ref.mean()) - 1.0) < 0.02, (img.mean(), ref.mean())
+
+
+@pytest.mark.parametrize("wave,lanes", [(0, 1), (3000, 2)])
+def test_batch_with_invisible_entities_equals_separate_renders(wave, lanes):
+    """A batch holding a scene with invisible entities drains each wave inside
+    its graph too: every scene's film equals the film of rendering it alone."""
+    from tests.test_gpu_batch import alone, views
+    scenes = [_fog(), rb.generate_scene(rb.RB_SCENE_SPHERES, seed=5, width=40, height=30, num_spheres=12, subdivision=2)]
+    vs = views(scenes)
+    want = [alone(sc, v, 4) for sc, v in zip(scenes, vs)]
+    with rb.Context(0) as ctx:
+        ctx.set_tuning(paths_per_wave=wave, lanes=lanes)
+        ctx.batch_upload(scenes)
+        ctx.batch_render(vs, max_depth=4)
+        for k in range(len(scenes)):
+            assert_films_close(ctx.batch_film(k), want[k], f"scene {k}")
+        assert ctx.stats().device_error == 0
