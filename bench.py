@@ -288,6 +288,39 @@ def config1_leg(rb, device, threads):
     return out
 
 
+def direct_leg(rb, device, threads, spp=4, rows=(384, 640)):
+    """direct_integrator (RB_RENDER_DIRECT, 4 emitter + 4 BSDF samples) on the sphere field (1,024,010
+    triangles, 1024 x 1024): one call of `spp` samples per pixel on the GPU, and the reference's own
+    direct_integrator on `rows` of the image at 1 spp on all host cores."""
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4)
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    ctx.render(scene.camera, 1, seed=1, want_image=False, direct=(4, 4))  # warm-up
+    best, rays = None, 0
+    for k in range(3):
+        ctx.render(scene.camera, spp, seed=2 + k, want_image=False, direct=(4, 4))
+        st = ctx.stats()
+        if best is None or st.elapsed_ms < best:
+            best, rays = st.elapsed_ms, st.extend_rays
+    ctx.close()
+    samples = 1024 * 1024 * spp
+    out = {"workload": f"sphere field, {scene.num_triangles} triangles, 1024x1024, {spp} spp, direct lighting with "
+                       "4 emitter and 4 BSDF samples", "gpu_msamples_per_s": samples / best / 1e3, "gpu_ms": best,
+           "gpu_mrays_per_s": rays / best / 1e3}
+    try:
+        from oracle import ref
+        if ref.available():
+            R = ref.RefScene(scene)
+            R.set_direct(4, 4)
+            _, _, sec = R.render(1, 0, 5, 1.0, 0, threads, rows=rows)
+            n = 1024 * (rows[1] - rows[0])
+            out.update(cpu_reference_msamples_per_s=n / sec / 1e6, cpu_reference_s=sec, cpu_cores=threads,
+                       cpu_sample=f"rows {rows[0]}-{rows[1] - 1} at 1 spp ({n} samples)")
+    except Exception as e:  # reported, never required
+        out["cpu_reference_error"] = str(e)
+    return out
+
+
 def spheres_s5_leg(rb, device, spp=8):
     """The sphere field at icosphere subdivision 5 (200 spheres, 4,096,002 triangles): one call of `spp`
     samples per pixel with autotuned launch shapes."""
@@ -520,7 +553,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_batched:
         for name, leg in (("config1", lambda: config1_leg(rb, local, os.cpu_count() or 1)),
                           ("spheres_s5", lambda: spheres_s5_leg(rb, local)),
-                          ("config5_plain", lambda: config5_leg(rb, local))):
+                          ("config5_plain", lambda: config5_leg(rb, local)),
+                          ("direct", lambda: direct_leg(rb, local, os.cpu_count() or 1))):
             try:
                 extra[name] = leg()
             except Exception as e:  # reported, never required for the throughput line

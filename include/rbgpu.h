@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 4
+#define RBGPU_ABI_VERSION 5
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -231,11 +231,16 @@ enum {
 	RB_RENDER_RESET = 1u << 0,     /* clear the film accumulators before adding these samples */
 	RB_RENDER_GUIDE = 1u << 1,     /* learned guiding: sample path continuations from the guide (below) */
 	RB_RENDER_TRAIN = 1u << 2,     /* learned guiding: collect training samples and train after every wave */
-	RB_RENDER_VOLUME = 1u << 3     /* volume_path_integrator::trace (volume_path_integrator.cpp:13-79) instead
+	RB_RENDER_VOLUME = 1u << 3,    /* volume_path_integrator::trace (volume_path_integrator.cpp:13-79) instead
 	                                  of path_integrator::trace: free-flight sampling in the media of the
 	                                  path, Henyey-Greenstein scattering, transmittance on every light
 	                                  connection; with learned guiding, medium vertices use a second
 	                                  guide network (rb_guide_medium_stats_get) */
+	RB_RENDER_DIRECT = 1u << 4     /* direct_integrator::trace (direct_integrator.cpp:20-127) instead of
+	                                  path_integrator::trace: at the first visible surface, light samples
+	                                  and BSDF samples combined by the power heuristic (direct_samples
+	                                  below); max_depth and rr_threshold are unused; not combined with
+	                                  RB_RENDER_GUIDE, RB_RENDER_TRAIN or RB_RENDER_VOLUME */
 };
 
 /* One render call: path_integrator::trace (rainbow-cpu/integrators/path_integrator.cpp:15-47)
@@ -251,7 +256,10 @@ typedef struct rb_render_params {
 	uint32_t seed;              /* mixed into every per-sample stream (15 bits used) */
 	uint32_t flags;             /* RB_RENDER_* */
 	uint32_t paths_per_wave;    /* 0: library default */
-	uint32_t reserved;
+	uint32_t direct_samples;    /* RB_RENDER_DIRECT: emitter samples in bits 0-15, BSDF samples in bits
+	                               16-31 (direct_integrator(sampler2d, sampler1d, emitter_samples,
+	                               bsdf_samples), direct_integrator.hpp:9-13); 0: the reference's
+	                               defaults, 4 and 4; both must be non-zero otherwise */
 } rb_render_params;
 
 /* Render and write the per-pixel mean radiance (box filter, film::add_tile +

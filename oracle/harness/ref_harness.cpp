@@ -19,6 +19,7 @@
 
 #include "rainbow-cpu/integrators/path_integrator.hpp"
 #include "rainbow-cpu/integrators/volume_path_integrator.hpp"
+#include "rainbow-cpu/integrators/direct_integrator.hpp"
 #include "rainbow-cpu/media/homogeneous_medium.hpp"
 #include "rainbow-cpu/cameras/perspective_camera.hpp"
 #include "rainbow-cpu/filters/box_filter.hpp"
@@ -88,6 +89,7 @@ struct orc_scene_impl {
 	rb_camera_desc desc{};
 	std::unordered_map<const entity*, int32_t> ordinal;
 	bool volume = false;  // trace with volume_path_integrator instead of path_integrator
+	uint32_t direct_emitter = 0, direct_bsdf = 0;  // > 0: trace with direct_integrator(emitter, bsdf samples)
 
 	std::shared_ptr<perspective_camera> make_camera(const std::shared_ptr<film>& f) const {
 		const vector3 eye(desc.eye[0], desc.eye[1], desc.eye[2]);
@@ -154,10 +156,12 @@ struct sample_driver {
 	std::shared_ptr<sampler_integrator> integrator;
 	std::shared_ptr<sampler1d> proto1;
 	std::shared_ptr<sampler2d> proto2;
-	sample_driver(uint32_t max_depth, float rr, bool volume) {
+	sample_driver(uint32_t max_depth, float rr, bool volume, uint32_t direct_emitter = 0, uint32_t direct_bsdf = 0) {
 		proto1 = std::make_shared<random_sampler1d>(1);
 		proto2 = std::make_shared<random_sampler2d>(1);
-		if (volume) integrator = std::make_shared<volume_path_integrator>(proto2, proto1, max_depth, rr);
+		if (direct_emitter > 0 && direct_bsdf > 0)
+			integrator = std::make_shared<direct_integrator>(proto2, proto1, direct_emitter, direct_bsdf);
+		else if (volume) integrator = std::make_shared<volume_path_integrator>(proto2, proto1, max_depth, rr);
 		else integrator = std::make_shared<path_integrator>(proto2, proto1, max_depth, rr);
 	}
 	// One sample of the body of sampler_integrator::render (sampler_integrator.cpp:102-130),
@@ -236,6 +240,13 @@ void orc_scene_free(orc_scene* s) { delete s; }
 // Selects the integrator of the tracing entry points: path_integrator (0) or
 // volume_path_integrator (1).
 void orc_set_volume(orc_scene* s, int volume) { s->volume = volume != 0; }
+
+// Selects direct_integrator(sampler2d, sampler1d, emitter_samples, bsdf_samples)
+// for the tracing entry points (both > 0), or clears that choice (either 0).
+void orc_set_direct(orc_scene* s, uint32_t emitter_samples, uint32_t bsdf_samples) {
+	s->direct_emitter = emitter_samples;
+	s->direct_bsdf = bsdf_samples;
+}
 
 
 
@@ -424,7 +435,7 @@ int orc_camera_rays(orc_scene* s, const uint32_t* pixels, const uint32_t* sample
 // Radiance of individual (pixel, sample) pairs through path_integrator::trace.
 int orc_trace_samples(orc_scene* s, const uint32_t* pixels, const uint32_t* samples, uint32_t n, uint32_t max_depth, float rr,
 	uint32_t seed, float* radiance) {
-	sample_driver d(max_depth, rr, s->volume);
+	sample_driver d(max_depth, rr, s->volume, s->direct_emitter, s->direct_bsdf);
 	for (uint32_t i = 0; i < n; i++) {
 		const int x = static_cast<int>(pixels[i] % static_cast<uint32_t>(s->width));
 		const int y = static_cast<int>(pixels[i] / static_cast<uint32_t>(s->width));
@@ -444,7 +455,7 @@ int orc_render(orc_scene* s, uint32_t spp, uint32_t first_sample, uint32_t max_d
 	std::atomic<int> next_row(row_begin);
 	const auto t0 = std::chrono::steady_clock::now();
 	auto work = [&]() {
-		sample_driver d(max_depth, rr, s->volume);
+		sample_driver d(max_depth, rr, s->volume, s->direct_emitter, s->direct_bsdf);
 		for (int y = next_row++; y < row_end; y = next_row++) {
 			for (int x = 0; x < s->width; x++) {
 				const size_t p = static_cast<size_t>(y) * s->width + x;

@@ -44,6 +44,7 @@ def lib():
             "orc_pcg32": (i32, [C.c_uint64, u32, vp, vp]),
             "orc_bsdf": (i32, [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
             "orc_set_volume": (None, [vp, i32]),
+            "orc_set_direct": (None, [vp, C.c_uint32, C.c_uint32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -119,6 +120,10 @@ class RefScene:
     def set_volume(self, volume: bool):
         """Trace with volume_path_integrator (True) or path_integrator (False)."""
         lib().orc_set_volume(self.h, 1 if volume else 0)
+
+    def set_direct(self, emitter_samples: int, bsdf_samples: int):
+        """Trace with direct_integrator(emitter_samples, bsdf_samples); (0, 0) goes back."""
+        lib().orc_set_direct(self.h, emitter_samples, bsdf_samples)
 
     def trace_samples(self, pixels, samples, max_depth=5, rr=1.0, seed=0):
         px = np.ascontiguousarray(pixels, dtype=np.uint32)

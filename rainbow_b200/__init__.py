@@ -23,7 +23,7 @@ import numpy as np
 from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_RENDER_GUIDE,
-    RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
+    RB_RENDER_DIRECT, RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
     RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,
     BvhDesc, CameraDesc, MediaDesc, MediumDesc,
     GuideConfig, GuideStats, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
@@ -159,9 +159,12 @@ class Context:
 
     def render(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5, threshold: float = 1.0,
                seed: int = 0, reset: bool = True, paths_per_wave: int = 0, want_image: bool = True,
-               guide: bool = False, train: bool = False, volume: bool = False, out: np.ndarray = None):
+               guide: bool = False, train: bool = False, volume: bool = False, out: np.ndarray = None,
+               direct: tuple = None):
         """guide / train: learned path guiding (RB_RENDER_GUIDE / RB_RENDER_TRAIN); volume:
-        volume_path_integrator instead of path_integrator (RB_RENDER_VOLUME). out: a
+        volume_path_integrator instead of path_integrator (RB_RENDER_VOLUME); direct:
+        (emitter_samples, bsdf_samples) renders with direct_integrator instead (RB_RENDER_DIRECT,
+        the reference's default is (4, 4)). out: a
         C-contiguous float32 (height, width, 3) array to write the image into (when its memory
         is page-locked, slices are copied while later waves still run); returned instead of a
         new array."""
@@ -170,6 +173,9 @@ class Context:
         p.spp, p.first_sample, p.max_depth, p.rr_threshold = spp, first_sample, max_depth, threshold
         flags = (RB_RENDER_RESET if reset else 0) | (RB_RENDER_GUIDE if guide else 0) | (RB_RENDER_TRAIN if train else 0)
         flags |= RB_RENDER_VOLUME if volume else 0
+        if direct is not None:
+            flags |= RB_RENDER_DIRECT
+            p.direct_samples = (int(direct[0]) & 0xFFFF) | ((int(direct[1]) & 0xFFFF) << 16)
         p.seed, p.flags, p.paths_per_wave = seed, flags, paths_per_wave
         if out is not None:
             if out.dtype != np.float32 or out.shape != (camera.height, camera.width, 3) or not out.flags.c_contiguous:

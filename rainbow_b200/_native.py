@@ -28,6 +28,7 @@ RB_RENDER_RESET = 1
 RB_RENDER_GUIDE = 2
 RB_RENDER_TRAIN = 4
 RB_RENDER_VOLUME = 8
+RB_RENDER_DIRECT = 16
 RB_GUIDE_SEQUENTIAL = 1
 RB_GUIDE_NUM_PARAMS = 30000
 RB_GUIDE_INPUTS = 9
@@ -92,7 +93,7 @@ class CameraDesc(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("camera", CameraDesc), ("spp", C.c_uint32), ("first_sample", C.c_uint32),
                 ("max_depth", C.c_uint32), ("rr_threshold", C.c_float), ("seed", C.c_uint32),
-                ("flags", C.c_uint32), ("paths_per_wave", C.c_uint32), ("reserved", C.c_uint32)]
+                ("flags", C.c_uint32), ("paths_per_wave", C.c_uint32), ("direct_samples", C.c_uint32)]
 
 
 class Tuning(C.Structure):

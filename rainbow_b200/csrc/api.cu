@@ -514,6 +514,39 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 	return RB_OK;
 }
 
+// Waves of a RB_RENDER_DIRECT call: one k_direct launch per wave, then its
+// film resolve (in wave order, as in run_waves).
+rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, image_readback* readback) {
+	gpu::wave_params& hp = *c->params_host;
+	const gpu::launch_cfg cfg = c->cfg();
+	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
+	hp.first_item = 0;
+	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
+	uint32_t launches = 0;
+	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
+		RB_CUDA(gpu::launch_direct_wave(c->view, c->wave, c->film, dc, cfg, c->num_sms * 4, c->stream));
+		launches += 3u;
+		const rb_status st = readback_after(c, readback, std::min<uint64_t>(total, first + c->wave_capacity), c->stream);
+		if (st != RB_OK) return st;
+	}
+	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
+	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	RB_CUDA(cudaStreamSynchronize(c->stream));
+	const uint32_t* h = c->counters_host;
+	auto u64 = [&](uint32_t w) { return static_cast<uint64_t>(h[w]) | (static_cast<uint64_t>(h[w + 1]) << 32); };
+	rb_render_stats& s = c->stats;
+	s = rb_render_stats{};
+	s.extend_rays = u64(gpu::CNT_EXTEND_RAYS);
+	s.node_visits = u64(gpu::CNT_NODE_VISITS);
+	s.triangle_tests = u64(gpu::CNT_TRI_TESTS);
+	s.device_error = h[gpu::CNT_ERROR];
+	s.samples = total;
+	s.kernel_launches = launches;
+	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
+	return RB_OK;
+}
+
 // Replaces the context's scene (or batch) with the packed arrays of `p`.
 rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
 	if (p.bvh_depth + 3 > 64) return RB_ERR_UNSUPPORTED;
@@ -781,6 +814,16 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 	const rb_camera_desc& cam = prm->camera;
 	if (!host_is_valid_camera(cam) || prm->max_depth == 0 || prm->max_depth > 64) return RB_ERR_INVALID_ARGUMENT;
 	if (static_cast<uint64_t>(prm->first_sample) + prm->spp > (1u << 24)) return RB_ERR_INVALID_ARGUMENT;
+	const bool direct = (prm->flags & RB_RENDER_DIRECT) != 0;
+	uint32_t direct_emitter = 4u, direct_bsdf = 4u;  // direct_integrator's defaults (direct_integrator.hpp:9-13)
+	if (direct) {
+		if (prm->flags & (RB_RENDER_GUIDE | RB_RENDER_TRAIN | RB_RENDER_VOLUME)) return RB_ERR_INVALID_ARGUMENT;
+		if (prm->direct_samples != 0) {
+			direct_emitter = prm->direct_samples & 0xffffu;
+			direct_bsdf = prm->direct_samples >> 16;
+			if (direct_emitter == 0 || direct_bsdf == 0) return RB_ERR_INVALID_ARGUMENT;
+		}
+	}
 	RB_CUDA(cudaSetDevice(c->device));
 	rb_status st = ensure_film(c, cam.width, cam.height, (prm->flags & RB_RENDER_RESET) != 0);
 	if (st != RB_OK) return st;
@@ -830,7 +873,8 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		overlap.pixels = pixels;
 		overlap.final_from = total - pixels;
 	}
-	st = run_waves(c, total, prm->max_depth, false, overlapped ? &overlap : nullptr);
+	st = direct ? run_direct(c, total, pt::make_direct_cfg(direct_emitter, direct_bsdf), overlapped ? &overlap : nullptr)
+		: run_waves(c, total, prm->max_depth, false, overlapped ? &overlap : nullptr);
 	if (st != RB_OK) return st;
 	const uint32_t* h = c->counters_host;
 	c->film_samples += prm->spp;

@@ -469,6 +469,63 @@ __global__ void __launch_bounds__(256) k_camera(wave_buffers w, uint32_t queue_o
 	}
 }
 
+// The tracer pt::direct_radiance calls: the kernels' traversal on this
+// thread's shared-memory stack; a full stack marks the sample failed.
+template <bool COUNT>
+struct thread_tracer {
+	const scene_view* s;
+	smem_stack* st;
+	uint32_t* nodes;
+	uint32_t* tris;
+	uint32_t* rays;
+	bool* ok;
+	RB_HD hit_t operator()(vec3 o, vec3 d, float& len, bool shadow) const {
+		hit_t h{-1, 0.f, 0.f};
+#if defined(__CUDA_ARCH__)
+		(*rays)++;
+		const bool r = shadow ? trace_one<true, COUNT>(*s, o, d, len, h, *st, *nodes, *tris)
+			: trace_one<false, COUNT>(*s, o, d, len, h, *st, *nodes, *tris);
+		if (!r) {
+			*ok = false;
+			h.slot = -1;
+		}
+#endif
+		return h;
+	}
+};
+
+// direct_integrator (pt::direct_radiance) for every item of the wave, one
+// thread per camera sample; the sample's radiance goes to w.result for the
+// film resolve. Traced rays are counted as extension rays.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_direct(scene_view s, wave_buffers w, direct_cfg dc, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st = make_stack(smem, stack_cap);
+	const wave_params& p = *w.params;
+	const uint64_t pixels = static_cast<uint64_t>(p.width) * p.height;
+	uint32_t nodes = 0, tris = 0, rays = 0;
+	bool ok = true;
+	const thread_tracer<COUNT> tracer{&s, &st, &nodes, &tris, &rays, &ok};
+	for (uint32_t base = blockIdx.x * blockDim.x; base < w.capacity; base += gridDim.x * blockDim.x) {
+		const uint32_t i = base + threadIdx.x;
+		const uint64_t item = p.first_item + i;
+		if (i < w.capacity && item < p.total_items) {
+			const uint32_t pixel = static_cast<uint32_t>(item % pixels);
+			const uint32_t sample = p.first_sample + static_cast<uint32_t>(item / pixels);
+			path_state ps;
+			path_begin(ps, p.r2c, p.c2w, p.lens, p.focus, pixel % p.width, pixel / p.width, pixel, sample, p.seed);
+			direct_radiance(s, dc, ps, tracer);
+			w.result[i] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.f);
+		}
+	}
+	if (!ok) set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+	warp_add64(w.counters, CNT_EXTEND_RAYS, rays);
+	if (COUNT) {
+		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
+		warp_add64(w.counters, CNT_TRI_TESTS, tris);
+	}
+}
+
 template <bool COUNT, bool VOL, bool BATCH>
 __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
 	uint32_t sort) {
@@ -1522,6 +1579,22 @@ cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int g
 	else k_film_resolve<<<grid, 256, 0, stream>>>(w, f);
 	k_next_wave<<<1, 1, 0, stream>>>(w.params, w.capacity);
 	return cudaGetLastError();
+}
+
+cudaError_t launch_direct_wave(const scene_view& s, const wave_buffers& w, const film_buffers& f, const direct_cfg& dc,
+	const launch_cfg& cfg, int resolve_grid, cudaStream_t stream) {
+	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	cudaError_t e;
+	if (cfg.count) {
+		e = allow_smem(k_direct<true>, smem, cfg.carveout);
+		if (e == cudaSuccess) k_direct<true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, dc, cfg.stack_depth);
+	} else {
+		e = allow_smem(k_direct<false>, smem, cfg.carveout);
+		if (e == cudaSuccess) k_direct<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, dc, cfg.stack_depth);
+	}
+	if (e == cudaSuccess) e = cudaGetLastError();
+	if (e == cudaSuccess) e = launch_next_wave(w, f, resolve_grid, stream);
+	return e;
 }
 
 cudaError_t launch_set_first(wave_params* params, uint64_t first, cudaStream_t stream) {

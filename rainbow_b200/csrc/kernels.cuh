@@ -3,6 +3,7 @@
 
 #include "../../include/rbgpu.h"
 #include "guide/guide_host.h"
+#include "pt/pt_direct.h"
 #include "pt/pt_path.h"
 
 #include <cuda_runtime.h>
@@ -196,6 +197,12 @@ cudaError_t launch_wave_end(const wave_buffers& w, const film_buffers& f, int gr
 
 // Kernel launches of one wave for a given configuration (for the stats).
 uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg);
+
+// One wave of direct_integrator samples (RB_RENDER_DIRECT): one thread per
+// camera sample traces its light and BSDF rays itself, then the film resolve
+// and the move to the next wave (3 launches).
+cudaError_t launch_direct_wave(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f,
+	const pt::direct_cfg& dc, const launch_cfg& cfg, int resolve_grid, cudaStream_t stream);
 
 // Drain loop of scenes with invisible entities. A pass through an invisible
 // boundary is not a bounce, so paths can outlive max_depth iterations; after

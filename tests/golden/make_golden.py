@@ -17,8 +17,12 @@ product's seeded scene generator:
   fog_samples    radiance of 1024 (pixel, sample) pairs, volume_path_integrator::trace,
                  depth 12, displaced spheres inside a homogeneous medium box
   fog_image      32 x 32 fog scene, 256 spp, volume_path_integrator, FP64 sums of L and L^2
+  direct_spheres radiance of 1024 (pixel, sample) pairs, direct_integrator::trace with the
+                 default 4 emitter and 4 BSDF samples, on the spheres scene above
+  direct_fog     512 pairs, direct_integrator(2 emitter, 3 BSDF samples), fog scene (rays
+                 pass through the medium's invisible boundary)
 
-Usage: python tests/golden/make_golden.py [--only fog]
+Usage: python tests/golden/make_golden.py [--only fog|direct]
 """
 from __future__ import annotations
 
@@ -78,9 +82,24 @@ def fog_fixtures():
     save("fog_image", params=params_array(small), spp=np.array(256), max_depth=np.array(12), sum=sums, sum_sq=sq)
 
 
+def direct_fixtures():
+    for name, p, n, E, B in (("direct_spheres", SPHERES, 1024, 4, 4), ("direct_fog", FOG, 512, 2, 3)):
+        R = ref.RefScene(scene_of(p))
+        R.set_direct(E, B)
+        rng = np.random.default_rng(17)
+        px = rng.integers(0, p["width"] * p["height"], n).astype(np.uint32)
+        sm = rng.integers(0, 4096, n).astype(np.uint32)
+        L = R.trace_samples(px, sm, seed=0)
+        save(name, params=params_array(p), pixels=px, samples=sm, radiance=L, emitter_samples=np.array(E),
+             bsdf_samples=np.array(B))
+
+
 def main():
-    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "fog":
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if only == "fog":
         return fog_fixtures()
+    if only == "direct":
+        return direct_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -138,6 +157,7 @@ def main():
     save("bvh_c2", params=params_array(C2), digest=np.array(bvh_digest(nodes, pe, pi)),
          num_nodes=np.array(nodes.shape[0]), num_prims=np.array(pe.shape[0]))
     fog_fixtures()
+    direct_fixtures()
 
 
 def material_desc(m):

@@ -28,6 +28,8 @@ class HostPaths:
         L.hp_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
         L.hp_samples.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
                                  C.c_uint32, C.c_void_p]
+        L.hp_direct_samples.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                        C.c_uint32, C.c_uint32, C.c_void_p]
         self.L, self.scene = L, scene
         self.h = C.c_void_p()
         assert L.hp_create(C.byref(scene.desc), C.byref(self.h)) == 0
@@ -49,6 +51,16 @@ class HostPaths:
         out = np.zeros((px.shape[0], 3), dtype=np.float32)
         self.L.hp_samples(self.h, C.byref(camera), px.ctypes.data, sm.ctypes.data, px.shape[0], max_depth, rr, seed,
                           out.ctypes.data)
+        return out
+
+
+    def direct_samples(self, camera, pixels, samples, emitter_samples=4, bsdf_samples=4, seed=0):
+        """direct_integrator radiance of (pixel, sample) pairs (pt::direct_radiance on the host)."""
+        px = np.ascontiguousarray(pixels, dtype=np.uint32)
+        sm = np.ascontiguousarray(samples, dtype=np.uint32)
+        out = np.zeros((px.shape[0], 3), dtype=np.float32)
+        assert self.L.hp_direct_samples(self.h, C.byref(camera), px.ctypes.data, sm.ctypes.data, px.shape[0],
+                                        emitter_samples, bsdf_samples, seed, out.ctypes.data) == 0
         return out
 
 

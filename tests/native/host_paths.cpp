@@ -129,6 +129,25 @@ void samples_view(const scene_view& view, const rb_camera_desc* cam, const uint3
 	}
 }
 
+// Radiance of (pixel, sample) pairs through direct_integrator (pt::direct_radiance),
+// rays traced with the kernels' traversal dispatch.
+void direct_samples_view(const scene_view& view, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples,
+	uint32_t n, uint32_t emitter_samples, uint32_t bsdf_samples, uint32_t seed, float* out) {
+	const direct_cfg dc = make_direct_cfg(emitter_samples, bsdf_samples);
+	auto tracer = [&view](vec3 o, vec3 d, float& len, bool shadow) { return trace(view, o, d, len, shadow); };
+	for (uint32_t i = 0; i < n; i++) {
+		const uint32_t pixel = pixels[i];
+		const uint32_t x = pixel % static_cast<uint32_t>(cam->width), y = pixel / static_cast<uint32_t>(cam->width);
+		path_state p;
+		path_begin(p, cam->raster_to_camera, cam->camera_to_world, cam->lens_radius, cam->focus_distance, x, y, pixel,
+			samples[i], seed);
+		direct_radiance(view, dc, p, tracer);
+		out[3 * i] = p.L.x;
+		out[3 * i + 1] = p.L.y;
+		out[3 * i + 2] = p.L.z;
+	}
+}
+
 // A merged batch (host::merge_scenes) with the per-scene views the kernels
 // build from their batch_scene records (gpu::batch_view).
 struct hp_batch {
@@ -150,6 +169,13 @@ int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits)
 int hp_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples, uint32_t n,
 	uint32_t max_depth, float rr, uint32_t seed, float* out) {
 	samples_view(static_cast<hp_scene*>(hs)->view, cam, pixels, samples, n, max_depth, rr, seed, out);
+	return RB_OK;
+}
+
+int hp_direct_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples, uint32_t n,
+	uint32_t emitter_samples, uint32_t bsdf_samples, uint32_t seed, float* out) {
+	if (emitter_samples == 0 || bsdf_samples == 0) return RB_ERR_INVALID_ARGUMENT;
+	direct_samples_view(static_cast<hp_scene*>(hs)->view, cam, pixels, samples, n, emitter_samples, bsdf_samples, seed, out);
 	return RB_OK;
 }
 
