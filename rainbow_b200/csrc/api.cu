@@ -523,10 +523,31 @@ rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, im
 	hp.first_item = 0;
 	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
 	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
+	// the staged kernels when the light samples fit their records, else one thread per sample
+	const bool staged = dc.emitter_samples <= pt::kDirectStagedLights;
+	if (staged && c->direct_alloc < c->wave_capacity) {
+		gpu::direct_buffers& db = c->direct;
+		dev_free(db.rec); dev_free(db.ray_o); dev_free(db.ray_d); dev_free(db.ray_hit);
+		dev_free(db.ray_queue); dev_free(db.shade_queue);
+		c->direct_alloc = 0;
+		const size_t n = c->wave_capacity, slots = n * gpu::kDirectSlots;
+		RB_CUDA(dev_alloc(&db.rec, n));
+		RB_CUDA(dev_alloc(&db.ray_o, slots));
+		RB_CUDA(dev_alloc(&db.ray_d, slots));
+		RB_CUDA(dev_alloc(&db.ray_hit, slots));
+		RB_CUDA(dev_alloc(&db.ray_queue, slots));
+		RB_CUDA(dev_alloc(&db.shade_queue, n));
+		c->direct_alloc = c->wave_capacity;
+	}
 	uint32_t launches = 0;
 	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
-		RB_CUDA(gpu::launch_direct_wave(c->view, c->wave, c->film, dc, cfg, c->num_sms * 4, c->stream));
-		launches += 3u;
+		if (staged) {
+			RB_CUDA(gpu::launch_direct_staged_wave(c->view, c->wave, c->film, c->direct, dc, cfg, c->num_sms * 4, c->stream));
+			launches += 3u + 2u * dc.bsdf_samples;
+		} else {
+			RB_CUDA(gpu::launch_direct_wave(c->view, c->wave, c->film, dc, cfg, c->num_sms * 4, c->stream));
+			launches += 3u;
+		}
 		const rb_status st = readback_after(c, readback, std::min<uint64_t>(total, first + c->wave_capacity), c->stream);
 		if (st != RB_OK) return st;
 	}

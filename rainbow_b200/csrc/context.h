@@ -224,6 +224,8 @@ struct rb_context {
 	std::vector<cudaEvent_t> wave_events;  // recorded after each wave's film resolve
 	std::vector<wave_lane> lanes;    // wave lanes beyond the context's own (lane 0: wave, stream, graph above)
 	bool volume = false;             // the current render call uses the volume path integrator
+	gpu::direct_buffers direct{};    // staged direct lighting (RB_RENDER_DIRECT), allocated on first use
+	uint32_t direct_alloc = 0;       // paths the direct buffers hold
 	int32_t* vol_medium = nullptr;   // per-path medium buffer (wave.medium points here in volume renders)
 	uint32_t vol_alloc = 0;          // paths the volume buffers hold
 
@@ -269,6 +271,9 @@ struct rb_context {
 		dev_free(vol_medium); dev_free(wave.vrec); dev_free(wave.beam); dev_free(wave.beam_queue);
 		wave.medium = nullptr;
 		vol_alloc = 0;
+		dev_free(direct.rec); dev_free(direct.ray_o); dev_free(direct.ray_d); dev_free(direct.ray_hit);
+		dev_free(direct.ray_queue); dev_free(direct.shade_queue);
+		direct_alloc = 0;
 		dev_free(batch_path_scene);
 		wave.scene = nullptr;
 		batch_path_alloc = 0;

@@ -526,6 +526,122 @@ __global__ void __launch_bounds__(256) k_direct(scene_view s, wave_buffers w, di
 	}
 }
 
+__device__ __forceinline__ void put_ray(const direct_buffers& db, uint32_t slot, const ray_t& r) {
+	db.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, r.len);
+	db.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
+}
+
+// Staged direct lighting, first stage: the camera ray of every item of the
+// wave (and its passes through lobeless surfaces) traced in the thread, then
+// at a shaded surface the light samples and the first BSDF sample, whose rays
+// are queued; a sample without a shaded surface is finished here.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_direct_surface(scene_view s, wave_buffers w, direct_buffers db, direct_cfg dc,
+	uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack st = make_stack(smem, stack_cap);
+	const wave_params& p = *w.params;
+	const uint64_t pixels = static_cast<uint64_t>(p.width) * p.height;
+	uint32_t nodes = 0, tris = 0, rays = 0;
+	bool ok = true;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < w.capacity; base += gridDim.x * blockDim.x) {
+		const uint32_t i = base + threadIdx.x;
+		const uint64_t item = p.first_item + i;
+		bool shaded = false;
+		uint32_t push = 0u;  // bit k: slot k queued
+		if (i < w.capacity && item < p.total_items) {
+			const uint32_t pixel = static_cast<uint32_t>(item % pixels);
+			const uint32_t sample = p.first_sample + static_cast<uint32_t>(item / pixels);
+			path_state ps;
+			path_begin(ps, p.r2c, p.c2w, p.lens, p.focus, pixel % p.width, pixel / p.width, pixel, sample, p.seed);
+			direct_record rec;
+			int state = 1;
+			for (int guard = 0; guard < 4096 && state == 1; guard++) {
+				float len = ps.len;
+				hit_t h;
+				rays++;
+				if (!trace_one<false, COUNT>(s, ps.o, ps.d, len, h, st, nodes, tris)) {
+					ok = false;
+					h.slot = -1;
+				}
+				state = direct_surface(s, ps, h, rec);
+			}
+			if (state == 2) {
+				ray_t out[kDirectSlots];
+				direct_sample_lights(s, dc, ps, rec, out);
+				for (uint32_t k = 0; k < dc.emitter_samples; k++)
+					if (rec.light_entity[k] >= 0) {
+						put_ray(db, i * kDirectSlots + k, out[k]);
+						push |= 1u << k;
+					}
+				if (rec.bsdf_valid) {
+					put_ray(db, i * kDirectSlots + dc.emitter_samples, out[dc.emitter_samples]);
+					push |= 1u << dc.emitter_samples;
+				}
+				db.rec[i] = rec;
+				store_path(w, i, ps);
+				w.pixel[i] = pixel;  // the round kernels rebuild the stream's increment from these
+				w.sample[i] = sample;
+				shaded = true;
+			} else {
+				w.result[i] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.f);
+			}
+		}
+		warp_push(shaded, i, db.shade_queue, w.counters + CNT_NEXT);
+		for (uint32_t k = 0; k <= dc.emitter_samples; k++) {
+			const bool q = (push >> k) & 1u;
+			warp_push(q, i * kDirectSlots + k, db.ray_queue, w.counters + CNT_SECONDARY);
+		}
+		rays += __popc(push);
+	}
+	if (!ok) set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+	warp_add64(w.counters, CNT_EXTEND_RAYS, rays);
+	if (COUNT) {
+		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
+		warp_add64(w.counters, CNT_TRI_TESTS, tris);
+	}
+}
+
+// Staged direct lighting, one round per BSDF sample over the shaded paths: the
+// traced hits of the pending rays (in the first round also the light samples'),
+// then the next BSDF sample's ray queued, or the sample finished.
+__global__ void __launch_bounds__(256) k_direct_round(scene_view s, wave_buffers w, direct_buffers db, direct_cfg dc) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_NEXT];
+	uint32_t rays = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool push = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = db.shade_queue[k];
+			path_state ps = load_path<false>(w, p, i);
+			direct_record rec = db.rec[i];
+			const uint32_t slot0 = i * kDirectSlots;
+			hit_t lh[kDirectStagedLights];
+			for (uint32_t j = 0; j < kDirectStagedLights; j++) {
+				lh[j] = hit_t{-1, 0.f, 0.f};
+				if (rec.round == 0u && j < dc.emitter_samples && rec.light_entity[j] >= 0) lh[j] = to_hit(db.ray_hit[slot0 + j]);
+			}
+			const hit_t bh = rec.bsdf_valid ? to_hit(db.ray_hit[slot0 + dc.emitter_samples]) : hit_t{-1, 0.f, 0.f};
+			ray_t out;
+			if (direct_round(s, dc, ps, rec, lh, bh, out)) {
+				if (rec.bsdf_valid) {
+					put_ray(db, slot0 + dc.emitter_samples, out);
+					push = true;
+				}
+				db.rec[i] = rec;
+				store_path(w, i, ps);
+			} else {
+				w.result[i] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.f);
+			}
+		}
+		warp_push(push, i * kDirectSlots + dc.emitter_samples, db.ray_queue, w.counters + CNT_SECONDARY);
+		rays += push ? 1u : 0u;
+	}
+	warp_add64(w.counters, CNT_EXTEND_RAYS, rays);
+}
+
 template <bool COUNT, bool VOL, bool BATCH>
 __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
 	uint32_t sort) {
@@ -1591,6 +1707,35 @@ cudaError_t launch_direct_wave(const scene_view& s, const wave_buffers& w, const
 	} else {
 		e = allow_smem(k_direct<false>, smem, cfg.carveout);
 		if (e == cudaSuccess) k_direct<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, dc, cfg.stack_depth);
+	}
+	if (e == cudaSuccess) e = cudaGetLastError();
+	if (e == cudaSuccess) e = launch_next_wave(w, f, resolve_grid, stream);
+	return e;
+}
+
+cudaError_t launch_direct_staged_wave(const scene_view& s, const wave_buffers& w, const film_buffers& f,
+	const direct_buffers& db, const direct_cfg& dc, const launch_cfg& cfg, int resolve_grid, cudaStream_t stream) {
+	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
+	cudaError_t e = cfg.count ? allow_smem(k_direct_surface<true>, smem, cfg.carveout)
+		: allow_smem(k_direct_surface<false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<false, false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<true, false>, smem, cfg.carveout);
+	if (e != cudaSuccess) return e;
+	// the traversal kernel reads the queued slots through the secondary-ray fields
+	wave_buffers wr = w;
+	wr.sec_o = db.ray_o;
+	wr.sec_d = db.ray_d;
+	wr.sec_hit = db.ray_hit;
+	wr.sec_queue = db.ray_queue;
+	e = cudaMemsetAsync(w.counters + CNT_NEXT, 0, 2 * sizeof(uint32_t), stream);  // CNT_NEXT, CNT_SECONDARY
+	if (e != cudaSuccess) return e;
+	if (cfg.count) k_direct_surface<true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, db, dc, cfg.stack_depth);
+	else k_direct_surface<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, db, dc, cfg.stack_depth);
+	for (uint32_t r = 0; r < dc.bsdf_samples && e == cudaSuccess; r++) {
+		if (cfg.count) k_trace_secondary<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth);
+		else k_trace_secondary<false, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth);
+		e = cudaMemsetAsync(w.counters + CNT_SECONDARY, 0, sizeof(uint32_t), stream);
+		if (e == cudaSuccess) k_direct_round<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	}
 	if (e == cudaSuccess) e = cudaGetLastError();
 	if (e == cudaSuccess) e = launch_next_wave(w, f, resolve_grid, stream);

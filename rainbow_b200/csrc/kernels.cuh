@@ -204,6 +204,24 @@ uint32_t wave_launches(uint32_t max_depth, const launch_cfg& cfg);
 cudaError_t launch_direct_wave(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f,
 	const pt::direct_cfg& dc, const launch_cfg& cfg, int resolve_grid, cudaStream_t stream);
 
+// Buffers of the staged direct-lighting kernels (at most pt::kDirectStagedLights
+// light samples): per path its record and kDirectSlots ray slots (the light
+// samples, then the pending BSDF sample in slot emitter_samples) with their hits.
+constexpr uint32_t kDirectSlots = pt::kDirectStagedLights + 1;
+struct direct_buffers {
+	pt::direct_record* rec;
+	float4* ray_o;            // kDirectSlots per path: o.xyz, length
+	float4* ray_d;
+	float4* ray_hit;
+	uint32_t* ray_queue;      // slots to trace (path * kDirectSlots + slot), count in CNT_SECONDARY
+	uint32_t* shade_queue;    // paths with a shaded surface, count in CNT_NEXT
+};
+// One wave of direct_integrator samples in stages: camera rays and light
+// samples (one kernel), then per BSDF sample a traversal of the queued rays and
+// a round kernel, then the film resolve (4 + 3 * bsdf_samples launches).
+cudaError_t launch_direct_staged_wave(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f,
+	const direct_buffers& db, const pt::direct_cfg& dc, const launch_cfg& cfg, int resolve_grid, cudaStream_t stream);
+
 // Drain loop of scenes with invisible entities. A pass through an invisible
 // boundary is not a bounce, so paths can outlive max_depth iterations; after
 // them a wave keeps bouncing until its active queue is empty. Inside a wave's

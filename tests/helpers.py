@@ -30,6 +30,7 @@ class HostPaths:
                                  C.c_uint32, C.c_void_p]
         L.hp_direct_samples.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                         C.c_uint32, C.c_uint32, C.c_void_p]
+        L.hp_direct_staged_samples.argtypes = L.hp_direct_samples.argtypes
         self.L, self.scene = L, scene
         self.h = C.c_void_p()
         assert L.hp_create(C.byref(scene.desc), C.byref(self.h)) == 0
@@ -54,13 +55,15 @@ class HostPaths:
         return out
 
 
-    def direct_samples(self, camera, pixels, samples, emitter_samples=4, bsdf_samples=4, seed=0):
-        """direct_integrator radiance of (pixel, sample) pairs (pt::direct_radiance on the host)."""
+    def direct_samples(self, camera, pixels, samples, emitter_samples=4, bsdf_samples=4, seed=0, staged=False):
+        """direct_integrator radiance of (pixel, sample) pairs on the host: pt::direct_radiance, or
+        (staged) its stage functions in the staged kernels' order."""
         px = np.ascontiguousarray(pixels, dtype=np.uint32)
         sm = np.ascontiguousarray(samples, dtype=np.uint32)
         out = np.zeros((px.shape[0], 3), dtype=np.float32)
-        assert self.L.hp_direct_samples(self.h, C.byref(camera), px.ctypes.data, sm.ctypes.data, px.shape[0],
-                                        emitter_samples, bsdf_samples, seed, out.ctypes.data) == 0
+        fn = self.L.hp_direct_staged_samples if staged else self.L.hp_direct_samples
+        assert fn(self.h, C.byref(camera), px.ctypes.data, sm.ctypes.data, px.shape[0], emitter_samples, bsdf_samples,
+                  seed, out.ctypes.data) == 0
         return out
 
 

@@ -179,6 +179,55 @@ int hp_direct_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixel
 	return RB_OK;
 }
 
+// The staged form of the same samples, stage by stage as the staged kernels
+// run them: camera ray (and pass-throughs), light samples and the first BSDF
+// ray, their traces, then one round per BSDF sample.
+int hp_direct_staged_samples(void* hs, const rb_camera_desc* cam, const uint32_t* pixels, const uint32_t* samples,
+	uint32_t n, uint32_t emitter_samples, uint32_t bsdf_samples, uint32_t seed, float* out) {
+	if (emitter_samples == 0 || bsdf_samples == 0 || emitter_samples > kDirectStagedLights) return RB_ERR_INVALID_ARGUMENT;
+	const scene_view& view = static_cast<hp_scene*>(hs)->view;
+	const direct_cfg dc = make_direct_cfg(emitter_samples, bsdf_samples);
+	for (uint32_t i = 0; i < n; i++) {
+		const uint32_t pixel = pixels[i];
+		const uint32_t x = pixel % static_cast<uint32_t>(cam->width), y = pixel / static_cast<uint32_t>(cam->width);
+		path_state p;
+		path_begin(p, cam->raster_to_camera, cam->camera_to_world, cam->lens_radius, cam->focus_distance, x, y, pixel,
+			samples[i], seed);
+		direct_record rec;
+		int state = 1;
+		for (int guard = 0; guard < 4096 && state == 1; guard++) {
+			float len = p.len;
+			const hit_t h = trace(view, p.o, p.d, len, false);
+			state = direct_surface(view, p, h, rec);
+		}
+		if (state == 2) {
+			ray_t rays[kDirectStagedLights + 1];
+			direct_sample_lights(view, dc, p, rec, rays);
+			hit_t lh[kDirectStagedLights];
+			for (uint32_t k = 0; k < emitter_samples; k++) {
+				lh[k] = hit_t{-1, 0.f, 0.f};
+				if (rec.light_entity[k] >= 0) {
+					float l = rays[k].len;
+					lh[k] = trace(view, rays[k].o, rays[k].d, l, true);
+				}
+			}
+			ray_t br = rays[emitter_samples];
+			for (;;) {
+				hit_t bh{-1, 0.f, 0.f};
+				if (rec.bsdf_valid) {
+					float l = br.len;
+					bh = trace(view, br.o, br.d, l, true);
+				}
+				if (!direct_round(view, dc, p, rec, lh, bh, br)) break;
+			}
+		}
+		out[3 * i] = p.L.x;
+		out[3 * i + 1] = p.L.y;
+		out[3 * i + 2] = p.L.z;
+	}
+	return RB_OK;
+}
+
 int hp_batch_create(const rb_scene_desc* descs, uint32_t count, void** out) {
 	auto* b = new (std::nothrow) hp_batch();
 	if (!b) return RB_ERR_OUT_OF_MEMORY;

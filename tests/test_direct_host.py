@@ -13,12 +13,14 @@ from tests import golden
 from tests.helpers import HostPaths, scene_from_params
 
 
+@pytest.mark.parametrize("staged", [False, True])
 @pytest.mark.parametrize("name", ["direct_spheres", "direct_fog"])
-def test_host_direct_matches_fixture(name):
+def test_host_direct_matches_fixture(name, staged):
+    """Both forms: the one-function sample and the stage functions in the staged kernels' order."""
     fx = golden.load(name)
     scene = scene_from_params(fx["params"])
     got = HostPaths(scene).direct_samples(scene.camera, fx["pixels"], fx["samples"], int(fx["emitter_samples"]),
-                                          int(fx["bsdf_samples"]))
+                                          int(fx["bsdf_samples"]), staged=staged)
     assert np.array_equal(got.view(np.uint32), fx["radiance"].view(np.uint32))
 
 
@@ -31,8 +33,10 @@ def test_host_direct_against_reference_other_counts():
     rng = np.random.default_rng(3)
     px = rng.integers(0, 40 * 40, 400).astype(np.uint32)
     sm = rng.integers(0, 500, 400).astype(np.uint32)
-    for E, B in ((1, 1), (3, 1), (1, 5)):
+    hp = HostPaths(scene)
+    for E, B in ((1, 1), (3, 1), (1, 5), (8, 2)):
         R.set_direct(E, B)
         want = R.trace_samples(px, sm)
-        got = HostPaths(scene).direct_samples(scene.camera, px, sm, E, B)
-        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (E, B)
+        for staged in (False, True):
+            got = hp.direct_samples(scene.camera, px, sm, E, B, staged=staged)
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (E, B, staged)

@@ -79,3 +79,22 @@ def test_direct_sample_counts_and_flags():
                     dict(direct=(4, 4), volume=True)):
             with pytest.raises(rb.RbError):
                 ctx.render(scene.camera, 1, **bad)
+
+
+@pytest.mark.parametrize("counts", [(9, 2), (8, 3), (1, 1)])
+def test_direct_both_kernels_match_host_build(counts):
+    """Up to 8 light samples the staged kernels run, beyond that one thread per
+    sample: both against the host build of the same sample."""
+    fx = golden.load("direct_fog")
+    scene = scene_from_params(fx["params"])
+    W, H = scene.camera.width, scene.camera.height
+    px = np.arange(W * H, dtype=np.uint32)
+    want = HostPaths(scene).direct_samples(scene.camera, px, np.full_like(px, 7), *counts)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        ctx.render(scene.camera, spp=1, first_sample=7, want_image=False, direct=counts, paths_per_wave=1000)
+        sums, _, cnt = ctx.film()
+        assert ctx.stats().device_error == 0
+    assert (cnt == 1).all()
+    agree = _agreement(sums.reshape(-1, 3).astype(np.float32), want)
+    assert agree >= 0.97, f"{counts}: only {agree:.4f} of pixels agree"
