@@ -72,7 +72,13 @@ typedef struct rb_mesh_desc {
 enum {
 	RB_MATERIAL_MATTE = 0,  /* rainbow-cpu/materials/matte_material.cpp:13-29 (Lambert when sigma == 0) */
 	RB_MATERIAL_METAL = 1,  /* rainbow-cpu/materials/metal_material.cpp:17-37 */
-	RB_MATERIAL_GLASS = 2   /* rainbow-cpu/materials/glass_material.cpp:25-64 */
+	RB_MATERIAL_GLASS = 2,  /* rainbow-cpu/materials/glass_material.cpp:25-64 */
+	RB_MATERIAL_PLASTIC = 3, /* rainbow-cpu/materials/plastic_material.cpp:9-55: diffuse = Kd (Lambert lobe),
+	                            reflectance = Ks (Trowbridge-Reitz reflection with a dielectric Fresnel
+	                            of ior, 1.49 in the reference's default constructor), roughness_u the
+	                            isotropic roughness */
+	RB_MATERIAL_MIRROR = 4   /* rainbow-cpu/materials/mirror_material.cpp:9-26: reflectance (specular
+	                            reflection, no Fresnel term) */
 };
 
 /* Constant-texture material parameters (constant_texture_t, textures/detail/constant_texture.hpp:25-35). */

@@ -28,6 +28,8 @@
 #include "rainbow-cpu/materials/matte_material.hpp"
 #include "rainbow-cpu/materials/metal_material.hpp"
 #include "rainbow-cpu/materials/glass_material.hpp"
+#include "rainbow-cpu/materials/mirror_material.hpp"
+#include "rainbow-cpu/materials/plastic_material.hpp"
 #include "rainbow-cpu/emitters/surface_light.hpp"
 #include "rainbow-cpu/emitters/environment_light.hpp"
 #include "rainbow-cpu/textures/constant_texture.hpp"
@@ -122,6 +124,10 @@ std::shared_ptr<material> make_material(const rb_material_desc& m) {
 	case RB_MATERIAL_GLASS:
 		return std::make_shared<glass_material>(spectrum_texture(m.reflectance), spectrum_texture(m.transmission),
 			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
+	case RB_MATERIAL_PLASTIC:
+		return std::make_shared<plastic_material>(spectrum_texture(m.reflectance), spectrum_texture(m.diffuse),
+			real_texture(m.roughness_u), real_texture(m.ior), m.remap_roughness != 0);
+	case RB_MATERIAL_MIRROR: return std::make_shared<mirror_material>(spectrum_texture(m.reflectance));
 	default: return nullptr;
 	}
 }

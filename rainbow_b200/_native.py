@@ -21,7 +21,7 @@ STATUS_NAMES = {
     12: "RB_ERR_TOO_LARGE",
 }
 
-RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS = 0, 1, 2
+RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS, RB_MATERIAL_PLASTIC, RB_MATERIAL_MIRROR = 0, 1, 2, 3, 4
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
 RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM, RB_SCENE_FOG = 0, 1, 2, 3
 RB_RENDER_RESET = 1

@@ -118,6 +118,20 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 				r.has_transmit = black3(md.transmission) ? 0u : 1u;
 				break;
 			}
+			case RB_MATERIAL_PLASTIC: {
+				if (!(md.ior > 0.f)) return RB_ERR_INVALID_ARGUMENT;
+				r.kind = pt::MAT_PLASTIC;
+				r.alpha_x = r.alpha_y = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_u) : md.roughness_u;
+				r.eta = md.ior;
+				r.diffuse = vec3{md.diffuse[0], md.diffuse[1], md.diffuse[2]};
+				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
+				r.has_reflect = black3(md.reflectance) ? 0u : 1u;
+				break;
+			}
+			case RB_MATERIAL_MIRROR:
+				r.kind = black3(md.reflectance) ? pt::MAT_BLACK : pt::MAT_MIRROR;
+				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
+				break;
 			default: return RB_ERR_INVALID_ARGUMENT;
 			}
 			out.materials.push_back(r);

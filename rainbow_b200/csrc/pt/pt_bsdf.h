@@ -201,7 +201,8 @@ struct lobe_sample {
 RB_HD lobe_sample no_sample() { return lobe_sample{0u, spectrum{0.f, 0.f, 0.f}, vec3{0.f, 0.f, 0.f}, 0.f}; }
 
 // Lobe kinds in collection order for each material.
-enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, LOBE_FRESNEL_SPECULAR = 3 };
+enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, LOBE_FRESNEL_SPECULAR = 3,
+	LOBE_SPECULAR_REFLECT = 4 };
 
 struct bsdf_t {
 	uint32_t kinds[2];
@@ -239,6 +240,18 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 		if (m->has_reflect || m->has_transmit) {
 			b.kinds[0] = LOBE_FRESNEL_SPECULAR; b.types[0] = ST_REFLECTION | ST_TRANSMISSION | ST_SPECULAR; b.count = 1;
 		}
+		break;
+	case MAT_PLASTIC:
+		// plastic_material::build_surface_properties (plastic_material.cpp:30-55): the
+		// collection's eta, then the Lambert lobe, then the reflection lobe, each if not black
+		b.eta = m->eta;
+		b.kinds[0] = b.kinds[1] = LOBE_MF_REFLECT;
+		b.types[0] = b.types[1] = ST_GLOSSY | ST_REFLECTION;
+		if (!is_black(m->diffuse)) { b.kinds[0] = LOBE_LAMBERT; b.types[0] = ST_DIFFUSE | ST_REFLECTION; }
+		b.count = (is_black(m->diffuse) ? 0u : 1u) + (m->has_reflect ? 1u : 0u);
+		break;
+	case MAT_MIRROR:
+		b.kinds[0] = LOBE_SPECULAR_REFLECT; b.types[0] = ST_SPECULAR | ST_REFLECTION; b.count = 1;
 		break;
 	default: break;  // black matte: no lobes
 	}
@@ -375,6 +388,13 @@ RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
 	return lobe_sample{ST_TRANSMISSION | ST_SPECULAR, v, wi, 1.f - F};
 }
 
+// specular_reflection::sample with fresnel_effect_nop (specular_reflection.cpp:16-31):
+// the mirror direction, f = reflectance / |cos theta_i|, pdf 1.
+RB_HD lobe_sample sample_specular_reflect(const bsdf_t& b, vec3 wo) {
+	const vec3 wi{-wo.x, -wo.y, wo.z};
+	return lobe_sample{ST_SPECULAR | ST_REFLECTION, b.m->reflectance / fabs_ref(wi.z), wi, 1.f};
+}
+
 template <int MAT>
 RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return sample_lambert<MAT>(b, i, wo, u);
@@ -387,6 +407,7 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u);
 		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u);
 		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(b, wo, u);
+		case LOBE_SPECULAR_REFLECT: return sample_specular_reflect(b, wo);
 		default: return no_sample();
 		}
 	}

@@ -115,14 +115,15 @@ struct mesh_rec {
 	uint32_t flags;
 };
 
-enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4 };
+enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4, MAT_PLASTIC = 5,
+	MAT_MIRROR = 6 };
 
 struct material_rec {
 	uint32_t kind;
 	float alpha_x, alpha_y;   // Trowbridge-Reitz alphas (roughness_to_alpha applied on the host)
-	float eta;                // glass IOR
-	spectrum diffuse;         // lambert reflectance
-	spectrum reflectance;     // glass reflectance
+	float eta;                // glass / plastic IOR
+	spectrum diffuse;         // lambert reflectance (matte, plastic Kd)
+	spectrum reflectance;     // glass reflectance, plastic Ks, mirror reflectance
 	spectrum transmission;    // glass transmission
 	spectrum cond_eta;        // conductor eta
 	spectrum cond_k;          // conductor k

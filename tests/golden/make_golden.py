@@ -21,8 +21,11 @@ product's seeded scene generator:
                  default 4 emitter and 4 BSDF samples, on the spheres scene above
   direct_fog     512 pairs, direct_integrator(2 emitter, 3 BSDF samples), fog scene (rays
                  pass through the medium's invisible boundary)
+  materials_samples  radiance of 1024 pairs, path_integrator::trace depth 8, on the spheres
+                 scene with plastic and mirror materials (tests.helpers.plastic_mirror_scene)
+  bsdf_plastic_*, bsdf_mirror_*  the BSDF tables of those two materials
 
-Usage: python tests/golden/make_golden.py [--only fog|direct]
+Usage: python tests/golden/make_golden.py [--only fog|direct|materials]
 """
 from __future__ import annotations
 
@@ -94,8 +97,39 @@ def direct_fixtures():
              bsdf_samples=np.array(B))
 
 
+def materials_fixtures():
+    from tests.helpers import plastic_mirror_scene
+    R = ref.RefScene(plastic_mirror_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(19)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("materials_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8))
+    bsdf_fixtures({"plastic": dict(kind=rb.RB_MATERIAL_PLASTIC, rough=0.3),
+                   "mirror": dict(kind=rb.RB_MATERIAL_MIRROR)})
+
+
+def bsdf_fixtures(mats):
+    # BSDF known answers on the shading frame = world axes
+    rng = np.random.default_rng(5)
+    n = 512
+    wo = rng.normal(size=(n, 3)).astype(np.float32)
+    wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    wi = rng.normal(size=(n, 3)).astype(np.float32)
+    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    u = rng.random((n, 2), dtype=np.float32)
+    for key, m in mats.items():
+        md = material_desc(m)
+        for include_name, include in (("all", 31), ("nonspec", 27)):
+            out = ref.bsdf(md, wo, u, wi, include)
+            save(f"bsdf_{key}_{include_name}", wo=wo, u=u, wi_eval=wi, include=np.array(include),
+                 material=np.frombuffer(bytes(md), dtype=np.uint8), **out)
+
+
 def main():
     only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if only == "materials":
+        return materials_fixtures()
     if only == "fog":
         return fog_fixtures()
     if only == "direct":
@@ -125,26 +159,12 @@ def main():
         L = R.trace_samples(px, sm, max_depth=depth, rr=1.0, seed=0)
         save(f"{name}_samples", params=params_array(p), pixels=px, samples=sm, radiance=L, max_depth=np.array(depth))
 
-    # BSDF known answers on the shading frame = world axes
-    rng = np.random.default_rng(5)
-    n = 512
-    wo = rng.normal(size=(n, 3)).astype(np.float32)
-    wo /= np.linalg.norm(wo, axis=1, keepdims=True)
-    wi = rng.normal(size=(n, 3)).astype(np.float32)
-    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
-    u = rng.random((n, 2), dtype=np.float32)
-    mats = {
+    bsdf_fixtures({
         "lambert": dict(kind=rb.RB_MATERIAL_MATTE, diffuse=(0.7, 0.4, 0.2)),
         "metal": dict(kind=rb.RB_MATERIAL_METAL, rough=0.3),
         "glass_rough": dict(kind=rb.RB_MATERIAL_GLASS, rough=0.2),
         "glass_smooth": dict(kind=rb.RB_MATERIAL_GLASS, rough=0.0),
-    }
-    for key, m in mats.items():
-        md = material_desc(m)
-        for include_name, include in (("all", 31), ("nonspec", 27)):
-            out = ref.bsdf(md, wo, u, wi, include)
-            save(f"bsdf_{key}_{include_name}", wo=wo, u=u, wi_eval=wi, include=np.array(include),
-                 material=np.frombuffer(bytes(md), dtype=np.uint8), **out)
+    })
 
     s = scene_of(dict(BOX, width=32, height=32))
     R = ref.RefScene(s)
@@ -158,6 +178,7 @@ def main():
          num_nodes=np.array(nodes.shape[0]), num_prims=np.array(pe.shape[0]))
     fog_fixtures()
     direct_fixtures()
+    materials_fixtures()
 
 
 def material_desc(m):
@@ -166,6 +187,14 @@ def material_desc(m):
     if m["kind"] == rb.RB_MATERIAL_MATTE:
         md.diffuse[:] = m["diffuse"]
         md.sigma = 0.0
+    elif m["kind"] == rb.RB_MATERIAL_PLASTIC:
+        md.remap_roughness = 1
+        md.diffuse[:] = (0.6, 0.3, 0.2)
+        md.reflectance[:] = (0.5, 0.45, 0.4)
+        md.roughness_u = m["rough"]
+        md.ior = 1.49
+    elif m["kind"] == rb.RB_MATERIAL_MIRROR:
+        md.reflectance[:] = (0.9, 0.85, 0.8)
     elif m["kind"] == rb.RB_MATERIAL_METAL:
         md.remap_roughness = 1
         md.eta[:] = (0.200438, 0.924033, 1.102212)

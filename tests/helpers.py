@@ -18,6 +18,30 @@ def scene_from_params(params) -> rb.Scene:
     return rb.generate_scene(kind, seed=seed, width=w, height=h, num_spheres=n, subdivision=sub)
 
 
+def plastic_mirror_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with every fourth material (from the second) plastic and every
+    fourth (from the third) a mirror; the rest unchanged."""
+    mats = []
+    for k in range(scene.desc.num_materials):
+        m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
+        if k % 4 == 1:
+            src = m
+            m = rb.MaterialDesc()
+            m.kind = rb.RB_MATERIAL_PLASTIC
+            m.diffuse[:] = (0.6, 0.3, 0.2) if k % 8 == 1 else (0.0, 0.0, 0.0)
+            m.reflectance[:] = (0.5, 0.45, 0.4)
+            m.roughness_u = 0.05 + 0.1 * (k % 5)
+            m.remap_roughness = 1
+            m.ior = 1.49
+            del src
+        elif k % 4 == 2:
+            m = rb.MaterialDesc()
+            m.kind = rb.RB_MATERIAL_MIRROR
+            m.reflectance[:] = (0.9, 0.85, 0.8)
+        mats.append(m)
+    return scene.with_materials(mats)
+
+
 class HostPaths:
     """Stage functions of the kernels compiled for the host (bit-exact reference arithmetic)."""
 

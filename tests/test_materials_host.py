@@ -1,0 +1,29 @@
+"""Plastic and mirror materials (plastic_material.cpp, mirror_material.cpp) in
+the path integrator's stages and in direct lighting, compiled for the host,
+against the reference (fixture from the compiled reference, and the reference
+itself where it is built): bit-equal radiance per (pixel, sample)."""
+import numpy as np
+import pytest
+
+from oracle import ref
+from tests import golden
+from tests.helpers import HostPaths, plastic_mirror_scene, scene_from_params
+
+
+def test_host_stages_plastic_mirror_match_fixture():
+    fx = golden.load("materials_samples")
+    scene = plastic_mirror_scene(scene_from_params(fx["params"]))
+    got = HostPaths(scene).samples(scene.camera, fx["pixels"], fx["samples"], int(fx["max_depth"]))
+    assert np.array_equal(got.view(np.uint32), fx["radiance"].view(np.uint32))
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference oracle not built")
+def test_host_direct_plastic_mirror_against_reference():
+    fx = golden.load("materials_samples")
+    scene = plastic_mirror_scene(scene_from_params(fx["params"]))
+    R = ref.RefScene(scene)
+    R.set_direct(3, 2)
+    want = R.trace_samples(fx["pixels"], fx["samples"])
+    for staged in (False, True):
+        got = HostPaths(scene).direct_samples(scene.camera, fx["pixels"], fx["samples"], 3, 2, staged=staged)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), staged
