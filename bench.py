@@ -241,6 +241,20 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
             "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}
 
 
+def direct_waves(res=1024, spp=2):
+    """One direct-lighting call (4 emitter + 4 BSDF samples, staged kernels) of `spp` samples on the sphere
+    field: the workload of the direct-lighting profile in profiles/."""
+    import rainbow_b200 as rb
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=res, height=res, num_spheres=200, subdivision=4)
+    ctx = rb.Context(0)
+    ctx.upload(scene)
+    ctx.render(scene.camera, spp, seed=3, want_image=False, direct=(4, 4), paths_per_wave=res * res)
+    st = ctx.stats()
+    ctx.close()
+    print(json.dumps({"ms": st.elapsed_ms, "rays": st.extend_rays, "launches": st.kernel_launches}))
+    return 0
+
+
 def guided_waves(res=1024):
     """Two plain waves, then three guided training waves (2 spp each) on the slit room: the
     workload of the guide-network profile in profiles/."""
@@ -411,6 +425,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--guided-waves", action="store_true",
                     help="only render 2 plain then 3 guided training waves of 2 spp on the slit room (profiling)")
+    ap.add_argument("--direct-waves", action="store_true",
+                    help="only render one 2-spp direct-lighting call on the sphere field (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tuning", default=None, help="launch shapes as JSON (skips the autotuner), e.g. "
                     "'{\"block_trace\": 256, \"grid_per_sm\": 16}'")
@@ -419,6 +435,8 @@ def main():
         return run_reference_arm(args)
     if args.guided_waves:
         return guided_waves()
+    if args.direct_waves:
+        return direct_waves()
 
     import torch
     import torch.distributed as dist

@@ -519,11 +519,8 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, image_readback* readback) {
 	gpu::wave_params& hp = *c->params_host;
 	const gpu::launch_cfg cfg = c->cfg();
-	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
-	hp.first_item = 0;
-	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
-	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
-	// the staged kernels when the light samples fit their records, else one thread per sample
+	// the staged kernels when the light samples fit their records, else one thread per sample;
+	// their buffers are allocated before the timed region
 	const bool staged = dc.emitter_samples <= pt::kDirectStagedLights;
 	if (staged && c->direct_alloc < c->wave_capacity) {
 		gpu::direct_buffers& db = c->direct;
@@ -539,6 +536,10 @@ rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, im
 		RB_CUDA(dev_alloc(&db.shade_queue, n));
 		c->direct_alloc = c->wave_capacity;
 	}
+	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
+	hp.first_item = 0;
+	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
 	uint32_t launches = 0;
 	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
 		if (staged) {
