@@ -375,7 +375,8 @@ typedef struct rb_tuning {
 rb_status rb_set_tuning(rb_context* ctx, const rb_tuning* tuning);
 rb_status rb_get_tuning(rb_context* ctx, rb_tuning* tuning);
 /* Autotuner: times renders of `probe_spp` samples per pixel of `params`
- * (its camera, depth and seed; the film is left cleared) under candidate
+ * (its camera, depth, seed, and RB_RENDER_VOLUME or RB_RENDER_DIRECT with its
+ * direct_samples; guiding is refused; the film is left cleared) under candidate
  * tunings by coordinate descent over the settings above (CUDA events, best of
  * repeats), keeps the fastest for the context and returns it with its time. */
 rb_status rb_tune_render(rb_context* ctx, const rb_render_params* params, uint32_t probe_spp, rb_tuning* best,

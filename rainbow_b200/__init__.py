@@ -297,12 +297,16 @@ class Context:
         return t
 
     def tune_render(self, camera: CameraDesc, probe_spp: int = 1, max_depth: int = 5, threshold: float = 1.0,
-                    seed: int = 0, volume: bool = False):
-        """Autotune the launch shapes on `probe_spp` samples per pixel; returns (Tuning, ms)."""
+                    seed: int = 0, volume: bool = False, direct: tuple = None):
+        """Autotune the launch shapes on `probe_spp` samples per pixel (of a volume or direct-lighting
+        render when asked); returns (Tuning, ms)."""
         p = RenderParams()
         p.camera = camera
         p.spp, p.max_depth, p.rr_threshold, p.seed = probe_spp, max_depth, threshold, seed
         p.flags = RB_RENDER_VOLUME if volume else 0
+        if direct is not None:
+            p.flags |= RB_RENDER_DIRECT
+            p.direct_samples = (int(direct[0]) & 0xFFFF) | ((int(direct[1]) & 0xFFFF) << 16)
         t, ms = Tuning(), C.c_float()
         check(lib().rb_tune_render(self._h, C.byref(p), probe_spp, C.byref(t), C.byref(ms)), "rb_tune_render")
         self._film_shape = (camera.width, camera.height)

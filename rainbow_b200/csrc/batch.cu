@@ -247,7 +247,7 @@ rb_status rb_tune_render(rb_context* c, const rb_render_params* params, uint32_t
 	rb_render_params p = *params;
 	p.spp = probe_spp;
 	p.paths_per_wave = 0;  // the tuning's
-	p.flags = (params->flags & RB_RENDER_VOLUME) | RB_RENDER_RESET;
+	p.flags = (params->flags & (RB_RENDER_VOLUME | RB_RENDER_DIRECT)) | RB_RENDER_RESET;
 	const uint64_t items = static_cast<uint64_t>(p.camera.width > 0 ? p.camera.width : 0) *
 		static_cast<uint64_t>(p.camera.height > 0 ? p.camera.height : 0) * probe_spp;
 	return autotune(c, items, [&]() { return rb_render(c, &p, nullptr); }, best, best_ms);

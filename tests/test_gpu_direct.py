@@ -98,3 +98,14 @@ def test_direct_both_kernels_match_host_build(counts):
     assert (cnt == 1).all()
     agree = _agreement(sums.reshape(-1, 3).astype(np.float32), want)
     assert agree >= 0.97, f"{counts}: only {agree:.4f} of pixels agree"
+
+
+def test_direct_launch_shapes_tuned_and_image_unchanged():
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=2, width=64, height=48, num_spheres=20, subdivision=2)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        want = ctx.render(scene.camera, 3, seed=4, direct=(2, 2))
+        t, ms = ctx.tune_render(scene.camera, probe_spp=2, direct=(2, 2))
+        assert ms > 0 and t.block_trace in (64, 128, 256)
+        got = ctx.render(scene.camera, 3, seed=4, direct=(2, 2))
+    np.testing.assert_allclose(got, want, rtol=1e-6, atol=0)
