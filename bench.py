@@ -309,7 +309,8 @@ def direct_leg(rb, device, threads, spp=4, rows=(384, 640)):
     scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4)
     ctx = rb.Context(device)
     ctx.upload(scene)
-    ctx.render(scene.camera, 1, seed=1, want_image=False, direct=(4, 4))  # warm-up
+    ctx.render(scene.camera, 1, seed=1, want_image=False, direct=(4, 4))  # warm-up (module loading, buffers)
+    tuning, _ = ctx.tune_render(scene.camera, probe_spp=1, seed=90, direct=(4, 4))
     best, rays = None, 0
     for k in range(3):
         ctx.render(scene.camera, spp, seed=2 + k, want_image=False, direct=(4, 4))
@@ -320,7 +321,7 @@ def direct_leg(rb, device, threads, spp=4, rows=(384, 640)):
     samples = 1024 * 1024 * spp
     out = {"workload": f"sphere field, {scene.num_triangles} triangles, 1024x1024, {spp} spp, direct lighting with "
                        "4 emitter and 4 BSDF samples", "gpu_msamples_per_s": samples / best / 1e3, "gpu_ms": best,
-           "gpu_mrays_per_s": rays / best / 1e3}
+           "gpu_mrays_per_s": rays / best / 1e3, "tuning": tuning.as_dict()}
     try:
         from oracle import ref
         if ref.available():
