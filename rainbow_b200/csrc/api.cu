@@ -544,7 +544,7 @@ rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, im
 	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
 		if (staged) {
 			RB_CUDA(gpu::launch_direct_staged_wave(c->view, c->wave, c->film, c->direct, dc, cfg, c->num_sms * 4, c->stream));
-			launches += 3u + 2u * dc.bsdf_samples;
+			launches += 7u + 5u * dc.bsdf_samples;
 		} else {
 			RB_CUDA(gpu::launch_direct_wave(c->view, c->wave, c->film, dc, cfg, c->num_sms * 4, c->stream));
 			launches += 3u;

@@ -532,12 +532,11 @@ __device__ __forceinline__ void put_ray(const direct_buffers& db, uint32_t slot,
 }
 
 // Staged direct lighting, first stage: the camera ray of every item of the
-// wave (and its passes through lobeless surfaces) traced in the thread, then
-// at a shaded surface the light samples and the first BSDF sample, whose rays
-// are queued; a sample without a shaded surface is finished here.
+// wave (and its passes through lobeless surfaces) traced in the thread; a
+// sample with a shaded surface is queued by the surface's material class for
+// the light-sampling kernels, the others are finished here.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_direct_surface(scene_view s, wave_buffers w, direct_buffers db, direct_cfg dc,
-	uint32_t stack_cap) {
+__global__ void __launch_bounds__(256) k_direct_surface(scene_view s, wave_buffers w, direct_buffers db, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
 	smem_stack st = make_stack(smem, stack_cap);
 	const wave_params& p = *w.params;
@@ -547,8 +546,7 @@ __global__ void __launch_bounds__(256) k_direct_surface(scene_view s, wave_buffe
 	for (uint32_t base = blockIdx.x * blockDim.x; base < w.capacity; base += gridDim.x * blockDim.x) {
 		const uint32_t i = base + threadIdx.x;
 		const uint64_t item = p.first_item + i;
-		bool shaded = false;
-		uint32_t push = 0u;  // bit k: slot k queued
+		uint32_t cls = CLASS_MISS;  // CLASS_MISS: nothing to queue
 		if (i < w.capacity && item < p.total_items) {
 			const uint32_t pixel = static_cast<uint32_t>(item % pixels);
 			const uint32_t sample = p.first_sample + static_cast<uint32_t>(item / pixels);
@@ -567,32 +565,20 @@ __global__ void __launch_bounds__(256) k_direct_surface(scene_view s, wave_buffe
 				state = direct_surface(s, ps, h, rec);
 			}
 			if (state == 2) {
-				ray_t out[kDirectSlots];
-				direct_sample_lights(s, dc, ps, rec, out);
-				for (uint32_t k = 0; k < dc.emitter_samples; k++)
-					if (rec.light_entity[k] >= 0) {
-						put_ray(db, i * kDirectSlots + k, out[k]);
-						push |= 1u << k;
-					}
-				if (rec.bsdf_valid) {
-					put_ray(db, i * kDirectSlots + dc.emitter_samples, out[dc.emitter_samples]);
-					push |= 1u << dc.emitter_samples;
-				}
-				db.rec[i] = rec;
+				db.rec[i].si = rec.si;
+				db.rec[i].material = rec.material;
+				db.rec[i].round = 0u;
 				store_path(w, i, ps);
-				w.pixel[i] = pixel;  // the round kernels rebuild the stream's increment from these
+				w.pixel[i] = pixel;  // the later stages rebuild the stream's increment from these
 				w.sample[i] = sample;
-				shaded = true;
+				cls = class_of_material(static_cast<int32_t>(rec.material), s);
 			} else {
 				w.result[i] = make_float4(ps.L.x, ps.L.y, ps.L.z, 1.f);
 			}
 		}
-		warp_push(shaded, i, db.shade_queue, w.counters + CNT_NEXT);
-		for (uint32_t k = 0; k <= dc.emitter_samples; k++) {
-			const bool q = (push >> k) & 1u;
-			warp_push(q, i * kDirectSlots + k, db.ray_queue, w.counters + CNT_SECONDARY);
-		}
-		rays += __popc(push);
+#pragma unroll
+		for (uint32_t c = CLASS_LAMBERT; c <= CLASS_OTHER; c++)
+			warp_push(cls == c, i, w.class_queue + c * w.capacity, w.counters + CNT_CLASS + c);
 	}
 	if (!ok) set_error(w.counters, RB_ERR_STACK_OVERFLOW);
 	warp_add64(w.counters, CNT_EXTEND_RAYS, rays);
@@ -602,19 +588,62 @@ __global__ void __launch_bounds__(256) k_direct_surface(scene_view s, wave_buffe
 	}
 }
 
-// Staged direct lighting, one round per BSDF sample over the shaded paths: the
-// traced hits of the pending rays (in the first round also the light samples'),
-// then the next BSDF sample's ray queued, or the sample finished.
+// Staged direct lighting, second stage, for the shaded surfaces of one
+// material class: the light samples and the first BSDF sample, their rays
+// queued for the traversal kernel.
+template <uint32_t CLASS>
+__global__ void __launch_bounds__(256) k_direct_lights(scene_view s, wave_buffers w, direct_buffers db, direct_cfg dc) {
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_CLASS + CLASS];
+	const uint32_t* q = w.class_queue + CLASS * w.capacity;
+	uint32_t rays = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		uint32_t i = 0, push = 0u;  // bit j: slot j queued
+		if (k < n) {
+			i = q[k];
+			path_state ps = load_path<false>(w, p, i);
+			direct_record rec;
+			rec.si = db.rec[i].si;
+			rec.material = db.rec[i].material;
+			rec.round = 0u;
+			ray_t out[kDirectSlots];
+			direct_sample_lights<class_material(CLASS)>(s, dc, ps, rec, out);
+			for (uint32_t j = 0; j < dc.emitter_samples; j++)
+				if (rec.light_entity[j] >= 0) {
+					put_ray(db, i * kDirectSlots + j, out[j]);
+					push |= 1u << j;
+				}
+			if (rec.bsdf_valid) {
+				put_ray(db, i * kDirectSlots + dc.emitter_samples, out[dc.emitter_samples]);
+				push |= 1u << dc.emitter_samples;
+			}
+			db.rec[i] = rec;
+			store_path(w, i, ps);
+		}
+		for (uint32_t j = 0; j <= dc.emitter_samples; j++)
+			warp_push((push >> j) & 1u, i * kDirectSlots + j, db.ray_queue, w.counters + CNT_SECONDARY);
+		rays += __popc(push);
+	}
+	warp_add64(w.counters, CNT_EXTEND_RAYS, rays);
+}
+
+// Staged direct lighting, one round per BSDF sample over one material class's
+// shaded paths: the traced hits of the pending rays (in the first round also
+// the light samples'), then the next BSDF sample's ray queued, or the sample
+// finished.
+template <uint32_t CLASS>
 __global__ void __launch_bounds__(256) k_direct_round(scene_view s, wave_buffers w, direct_buffers db, direct_cfg dc) {
 	const wave_params& p = *w.params;
-	const uint32_t n = w.counters[CNT_NEXT];
+	const uint32_t n = w.counters[CNT_CLASS + CLASS];
+	const uint32_t* q = w.class_queue + CLASS * w.capacity;
 	uint32_t rays = 0;
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
 		bool push = false;
 		uint32_t i = 0;
 		if (k < n) {
-			i = db.shade_queue[k];
+			i = q[k];
 			path_state ps = load_path<false>(w, p, i);
 			direct_record rec = db.rec[i];
 			const uint32_t slot0 = i * kDirectSlots;
@@ -625,7 +654,7 @@ __global__ void __launch_bounds__(256) k_direct_round(scene_view s, wave_buffers
 			}
 			const hit_t bh = rec.bsdf_valid ? to_hit(db.ray_hit[slot0 + dc.emitter_samples]) : hit_t{-1, 0.f, 0.f};
 			ray_t out;
-			if (direct_round(s, dc, ps, rec, lh, bh, out)) {
+			if (direct_round<class_material(CLASS)>(s, dc, ps, rec, lh, bh, out)) {
 				if (rec.bsdf_valid) {
 					put_ray(db, slot0 + dc.emitter_samples, out);
 					push = true;
@@ -1727,15 +1756,24 @@ cudaError_t launch_direct_staged_wave(const scene_view& s, const wave_buffers& w
 	wr.sec_d = db.ray_d;
 	wr.sec_hit = db.ray_hit;
 	wr.sec_queue = db.ray_queue;
-	e = cudaMemsetAsync(w.counters + CNT_NEXT, 0, 2 * sizeof(uint32_t), stream);  // CNT_NEXT, CNT_SECONDARY
+	e = cudaMemsetAsync(w.counters + CNT_SECONDARY, 0, sizeof(uint32_t), stream);
+	if (e == cudaSuccess) e = cudaMemsetAsync(w.counters + CNT_CLASS, 0, NUM_CLASSES * sizeof(uint32_t), stream);
 	if (e != cudaSuccess) return e;
-	if (cfg.count) k_direct_surface<true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, db, dc, cfg.stack_depth);
-	else k_direct_surface<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, db, dc, cfg.stack_depth);
+	if (cfg.count) k_direct_surface<true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, db, cfg.stack_depth);
+	else k_direct_surface<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, db, cfg.stack_depth);
+	k_direct_lights<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+	k_direct_lights<CLASS_METAL><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+	k_direct_lights<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+	k_direct_lights<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	for (uint32_t r = 0; r < dc.bsdf_samples && e == cudaSuccess; r++) {
 		if (cfg.count) k_trace_secondary<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth);
 		else k_trace_secondary<false, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth);
 		e = cudaMemsetAsync(w.counters + CNT_SECONDARY, 0, sizeof(uint32_t), stream);
-		if (e == cudaSuccess) k_direct_round<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+		if (e != cudaSuccess) break;
+		k_direct_round<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+		k_direct_round<CLASS_METAL><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+		k_direct_round<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
+		k_direct_round<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	}
 	if (e == cudaSuccess) e = cudaGetLastError();
 	if (e == cudaSuccess) e = launch_next_wave(w, f, resolve_grid, stream);

@@ -214,11 +214,12 @@ struct direct_buffers {
 	float4* ray_d;
 	float4* ray_hit;
 	uint32_t* ray_queue;      // slots to trace (path * kDirectSlots + slot), count in CNT_SECONDARY
-	uint32_t* shade_queue;    // paths with a shaded surface, count in CNT_NEXT
+	uint32_t* shade_queue;    // unused (the shaded paths wait in the wave's material-class queues)
 };
-// One wave of direct_integrator samples in stages: camera rays and light
-// samples (one kernel), then per BSDF sample a traversal of the queued rays and
-// a round kernel, then the film resolve (4 + 3 * bsdf_samples launches).
+// One wave of direct_integrator samples in stages: camera rays, then per
+// material class the light samples, then per BSDF sample a traversal of the
+// queued rays and one round kernel per class, then the film resolve
+// (7 + 5 * bsdf_samples launches).
 cudaError_t launch_direct_staged_wave(const pt::scene_view& s, const wave_buffers& w, const film_buffers& f,
 	const direct_buffers& db, const pt::direct_cfg& dc, const launch_cfg& cfg, int resolve_grid, cudaStream_t stream);
 

@@ -177,10 +177,12 @@ RB_HD int direct_surface(const scene_view& s, path_state& p, const hit_t& h, dir
 }
 
 // Draws the next BSDF sample of a shaded surface; out: its ray when rec.bsdf_valid.
+// MAT: the material kind when the caller knows it (a shading class), else MAT_ANY.
+template <int MAT = MAT_ANY>
 RB_HD void direct_next_bsdf(const scene_view& s, path_state& p, direct_record& rec, ray_t& out) {
 	const surface_t& si = rec.si;
 	const bsdf_t b = make_bsdf(s.materials + rec.material);
-	const lobe_sample bs = bsdf_sample(b, to_local(si, si.wo), pcg_2d(p.rng), ST_ALL);
+	const lobe_sample bs = bsdf_sample<MAT>(b, to_local(si, si.wo), pcg_2d(p.rng), ST_ALL);
 	const vec3 wi = bs.pdf > 0.f ? to_world(si, bs.wi) : vec3{0.f, 0.f, 0.f};
 	const spectrum v = bs.f * fabs_ref(dot(wi, si.sz));
 	rec.bsdf_valid = (!is_black(v) && bs.pdf > 0.f) ? 1u : 0u;
@@ -194,6 +196,7 @@ RB_HD void direct_next_bsdf(const scene_view& s, path_state& p, direct_record& r
 // The light samples (cfg.emitter_samples <= kDirectStagedLights): shadow ray k
 // in out[k] where rec.light_entity[k] >= 0; then the first BSDF sample, its ray
 // in out[cfg.emitter_samples].
+template <int MAT = MAT_ANY>
 RB_HD void direct_sample_lights(const scene_view& s, const direct_cfg& cfg, path_state& p, direct_record& rec,
 	ray_t* out) {
 	const surface_t& si = rec.si;
@@ -210,8 +213,8 @@ RB_HD void direct_sample_lights(const scene_view& s, const direct_cfg& cfg, path
 		ls.pdf = ls.pdf * pick_pdf;
 		if (is_black(ls.L) || !(ls.pdf > 0.f)) continue;
 		const vec3 wi = to_local(si, ls.wi);
-		spectrum f = bsdf_f(b, wo, wi, ST_ALL);
-		const float fpdf = bsdf_pdf(b, wo, wi, ST_ALL);
+		spectrum f = bsdf_f<MAT>(b, wo, wi, ST_ALL);
+		const float fpdf = bsdf_pdf<MAT>(b, wo, wi, ST_ALL);
 		f = f * fabs_ref(dot(ls.wi, si.sz));
 		if (is_black(f) || fpdf <= 0.f) continue;
 		out[k] = spawn_ray_to(si.p, si.n, ls.p);
@@ -219,13 +222,14 @@ RB_HD void direct_sample_lights(const scene_view& s, const direct_cfg& cfg, path
 		rec.light_L[k] = f * ls.L * w / ls.pdf;
 		rec.light_entity[k] = em.entity;
 	}
-	direct_next_bsdf(s, p, rec, out[cfg.emitter_samples]);
+	direct_next_bsdf<MAT>(s, p, rec, out[cfg.emitter_samples]);
 }
 
 // After the traces of the pending rays: in round 0 first the light samples
 // (light_hits[k], closest visible hit of shadow ray k), then the pending BSDF
 // sample (hit bh of its ray); draws the next BSDF sample into out. Returns true
 // while a BSDF sample is pending (rec.bsdf_valid: its ray needs tracing).
+template <int MAT = MAT_ANY>
 RB_HD bool direct_round(const scene_view& s, const direct_cfg& cfg, path_state& p, direct_record& rec,
 	const hit_t* light_hits, const hit_t& bh, ray_t& out) {
 	const surface_t& si = rec.si;
@@ -268,7 +272,7 @@ RB_HD bool direct_round(const scene_view& s, const direct_cfg& cfg, path_state& 
 	}
 	rec.round++;
 	if (rec.round >= cfg.bsdf_samples) return false;
-	direct_next_bsdf(s, p, rec, out);
+	direct_next_bsdf<MAT>(s, p, rec, out);
 	return true;
 }
 
