@@ -77,8 +77,12 @@ enum {
 	                            reflectance = Ks (Trowbridge-Reitz reflection with a dielectric Fresnel
 	                            of ior, 1.49 in the reference's default constructor), roughness_u the
 	                            isotropic roughness */
-	RB_MATERIAL_MIRROR = 4   /* rainbow-cpu/materials/mirror_material.cpp:9-26: reflectance (specular
+	RB_MATERIAL_MIRROR = 4,  /* rainbow-cpu/materials/mirror_material.cpp:9-26: reflectance (specular
 	                            reflection, no Fresnel term) */
+	RB_MATERIAL_SUBSTRATE = 5 /* rainbow-cpu/materials/substrate_material.cpp: the Fresnel-blend
+	                            layer (scatterings/reflection/fresnel_blend_reflection.cpp) of
+	                            reflectance = specular Rs over diffuse = Rd, Trowbridge-Reitz
+	                            roughness_u / roughness_v */
 };
 
 /* Constant-texture material parameters (constant_texture_t, textures/detail/constant_texture.hpp:25-35). */

@@ -30,6 +30,7 @@
 #include "rainbow-cpu/materials/glass_material.hpp"
 #include "rainbow-cpu/materials/mirror_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
+#include "rainbow-cpu/materials/substrate_material.hpp"
 #include "rainbow-cpu/emitters/surface_light.hpp"
 #include "rainbow-cpu/emitters/environment_light.hpp"
 #include "rainbow-cpu/textures/constant_texture.hpp"
@@ -128,6 +129,9 @@ std::shared_ptr<material> make_material(const rb_material_desc& m) {
 		return std::make_shared<plastic_material>(spectrum_texture(m.reflectance), spectrum_texture(m.diffuse),
 			real_texture(m.roughness_u), real_texture(m.ior), m.remap_roughness != 0);
 	case RB_MATERIAL_MIRROR: return std::make_shared<mirror_material>(spectrum_texture(m.reflectance));
+	case RB_MATERIAL_SUBSTRATE:
+		return std::make_shared<substrate_material>(spectrum_texture(m.reflectance), spectrum_texture(m.diffuse),
+			real_texture(m.roughness_u), real_texture(m.roughness_v), m.remap_roughness != 0);
 	default: return nullptr;
 	}
 }

@@ -22,6 +22,7 @@ STATUS_NAMES = {
 }
 
 RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS, RB_MATERIAL_PLASTIC, RB_MATERIAL_MIRROR = 0, 1, 2, 3, 4
+RB_MATERIAL_SUBSTRATE = 5
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
 RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM, RB_SCENE_FOG = 0, 1, 2, 3
 RB_RENDER_RESET = 1

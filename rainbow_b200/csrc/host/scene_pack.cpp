@@ -128,6 +128,13 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 				r.has_reflect = black3(md.reflectance) ? 0u : 1u;
 				break;
 			}
+			case RB_MATERIAL_SUBSTRATE:
+				r.kind = (black3(md.reflectance) && black3(md.diffuse)) ? pt::MAT_BLACK : pt::MAT_SUBSTRATE;
+				r.alpha_x = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_u) : md.roughness_u;
+				r.alpha_y = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_v) : md.roughness_v;
+				r.diffuse = vec3{md.diffuse[0], md.diffuse[1], md.diffuse[2]};
+				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
+				break;
 			case RB_MATERIAL_MIRROR:
 				r.kind = black3(md.reflectance) ? pt::MAT_BLACK : pt::MAT_MIRROR;
 				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};

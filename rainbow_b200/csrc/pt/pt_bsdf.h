@@ -202,7 +202,7 @@ RB_HD lobe_sample no_sample() { return lobe_sample{0u, spectrum{0.f, 0.f, 0.f}, 
 
 // Lobe kinds in collection order for each material.
 enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, LOBE_FRESNEL_SPECULAR = 3,
-	LOBE_SPECULAR_REFLECT = 4 };
+	LOBE_SPECULAR_REFLECT = 4, LOBE_FRESNEL_BLEND = 5 };
 
 struct bsdf_t {
 	uint32_t kinds[2];
@@ -252,6 +252,9 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 		break;
 	case MAT_MIRROR:
 		b.kinds[0] = LOBE_SPECULAR_REFLECT; b.types[0] = ST_SPECULAR | ST_REFLECTION; b.count = 1;
+		break;
+	case MAT_SUBSTRATE:
+		b.kinds[0] = LOBE_FRESNEL_BLEND; b.types[0] = ST_GLOSSY | ST_REFLECTION; b.count = 1;
 		break;
 	default: break;  // black matte: no lobes
 	}
@@ -312,6 +315,29 @@ RB_HD float mf_transmit_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	return tr_pdf(m->alpha_x, m->alpha_y, wo, wh) * fabs_ref((eta * eta * dot(wi, wh)) / (denom * denom));
 }
 
+// fresnel_blend_reflection (scatterings/reflection/fresnel_blend_reflection.cpp):
+// Rd (28 / (23 pi)) (1 - Rs) (1 - (1 - |cos_i| / 2)^5) (1 - (1 - |cos_o| / 2)^5)
+// plus the Schlick-Fresnel glossy term F(wo . wh) D / (4 |wi . wh| max(|cos_i|, |cos_o|)).
+RB_HD float pow5(float v) { return (v * v) * (v * v) * v; }
+RB_HD spectrum fresnel_blend_f(const material_rec* m, vec3 wo, vec3 wi) {
+	vec3 wh = wo + wi;
+	if (wh.x == 0.f && wh.y == 0.f && wh.z == 0.f) return spectrum{0.f, 0.f, 0.f};
+	wh = normalize(wh);
+	const spectrum diffuse = m->diffuse * (28.f / (23.f * kPi)) * (splat3(1.f) - m->reflectance) *
+		(1.f - pow5(1.f - 0.5f * fabs_ref(wi.z))) * (1.f - pow5(1.f - 0.5f * fabs_ref(wo.z)));
+	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
+	const spectrum fresnel = m->reflectance + (splat3(1.f) - m->reflectance) * pow5(1.f - dot(wo, wh));
+	const spectrum specular = fresnel * D / (4.f * fabs_ref(dot(wi, wh)) * fmax_ref(fabs_ref(wi.z), fabs_ref(wo.z)));
+	return specular + diffuse;  // times the layer's scale, 1
+}
+RB_HD float fresnel_blend_pdf(const material_rec* m, vec3 wo, vec3 wi) {
+	if (!same_hemisphere(wo, wi)) return 0.f;
+	const vec3 wh = normalize(wo + wi);
+	const float pd = tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh));
+	const float ph = cosine_hemisphere_pdf(fabs_ref(wi.z));
+	return 0.5f * (pd + ph);
+}
+
 template <int MAT>
 RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return b.m->diffuse * kInvPi;
@@ -323,6 +349,7 @@ RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
 		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi);
 		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
+		case LOBE_FRESNEL_BLEND: return fresnel_blend_f(b.m, wo, wi);
 		default: return spectrum{0.f, 0.f, 0.f};
 		}
 	}
@@ -338,6 +365,7 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		case LOBE_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
 		case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
 		case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
+		case LOBE_FRESNEL_BLEND: return fresnel_blend_pdf(b.m, wo, wi);
 		default: return 0.f;
 		}
 	}
@@ -388,6 +416,22 @@ RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
 	return lobe_sample{ST_TRANSMISSION | ST_SPECULAR, v, wi, 1.f - F};
 }
 
+// fresnel_blend_reflection::sample: u.x below one half picks the cosine
+// hemisphere, above it the Trowbridge-Reitz half vector, u.x remapped to [0, 1).
+RB_HD lobe_sample sample_fresnel_blend(const bsdf_t& b, vec3 wo, vec2 u) {
+	const material_rec* m = b.m;
+	vec3 wi;
+	if (u.x < 0.5f) {
+		wi = cosine_hemisphere(vec2{fmin_ref(2.f * u.x, kOneMinusEps), u.y});
+		if (wo.z < 0.f) wi.z = -wi.z;
+	} else {
+		const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, vec2{fmin_ref(2.f * (u.x - 0.5f), kOneMinusEps), u.y});
+		wi = reflect(wo, wh);
+		if (!same_hemisphere(wo, wi)) return no_sample();
+	}
+	return lobe_sample{ST_GLOSSY | ST_REFLECTION, fresnel_blend_f(m, wo, wi), wi, fresnel_blend_pdf(m, wo, wi)};
+}
+
 // specular_reflection::sample with fresnel_effect_nop (specular_reflection.cpp:16-31):
 // the mirror direction, f = reflectance / |cos theta_i|, pdf 1.
 RB_HD lobe_sample sample_specular_reflect(const bsdf_t& b, vec3 wo) {
@@ -408,6 +452,7 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u);
 		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(b, wo, u);
 		case LOBE_SPECULAR_REFLECT: return sample_specular_reflect(b, wo);
+		case LOBE_FRESNEL_BLEND: return sample_fresnel_blend(b, wo, u);
 		default: return no_sample();
 		}
 	}

@@ -116,7 +116,7 @@ struct mesh_rec {
 };
 
 enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4, MAT_PLASTIC = 5,
-	MAT_MIRROR = 6 };
+	MAT_MIRROR = 6, MAT_SUBSTRATE = 7 };
 
 struct material_rec {
 	uint32_t kind;

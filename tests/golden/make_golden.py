@@ -22,8 +22,8 @@ product's seeded scene generator:
   direct_fog     512 pairs, direct_integrator(2 emitter, 3 BSDF samples), fog scene (rays
                  pass through the medium's invisible boundary)
   materials_samples  radiance of 1024 pairs, path_integrator::trace depth 8, on the spheres
-                 scene with plastic and mirror materials (tests.helpers.plastic_mirror_scene)
-  bsdf_plastic_*, bsdf_mirror_*  the BSDF tables of those two materials
+                 scene with plastic and mirror materials (tests.helpers.extra_materials_scene)
+  bsdf_plastic_*, bsdf_mirror_*, bsdf_substrate_*  the BSDF tables of those materials
 
 Usage: python tests/golden/make_golden.py [--only fog|direct|materials]
 """
@@ -98,15 +98,16 @@ def direct_fixtures():
 
 
 def materials_fixtures():
-    from tests.helpers import plastic_mirror_scene
-    R = ref.RefScene(plastic_mirror_scene(scene_of(SPHERES)))
+    from tests.helpers import extra_materials_scene
+    R = ref.RefScene(extra_materials_scene(scene_of(SPHERES)))
     rng = np.random.default_rng(19)
     px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
     sm = rng.integers(0, 4096, 1024).astype(np.uint32)
     L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
     save("materials_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8))
     bsdf_fixtures({"plastic": dict(kind=rb.RB_MATERIAL_PLASTIC, rough=0.3),
-                   "mirror": dict(kind=rb.RB_MATERIAL_MIRROR)})
+                   "mirror": dict(kind=rb.RB_MATERIAL_MIRROR),
+                   "substrate": dict(kind=rb.RB_MATERIAL_SUBSTRATE, rough=0.2)})
 
 
 def bsdf_fixtures(mats):
@@ -195,6 +196,11 @@ def material_desc(m):
         md.ior = 1.49
     elif m["kind"] == rb.RB_MATERIAL_MIRROR:
         md.reflectance[:] = (0.9, 0.85, 0.8)
+    elif m["kind"] == rb.RB_MATERIAL_SUBSTRATE:
+        md.remap_roughness = 1
+        md.diffuse[:] = (0.5, 0.35, 0.2)
+        md.reflectance[:] = (0.05, 0.05, 0.05)
+        md.roughness_u, md.roughness_v = m["rough"], 0.5 * m["rough"]
     elif m["kind"] == rb.RB_MATERIAL_METAL:
         md.remap_roughness = 1
         md.eta[:] = (0.200438, 0.924033, 1.102212)

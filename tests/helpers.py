@@ -18,9 +18,10 @@ def scene_from_params(params) -> rb.Scene:
     return rb.generate_scene(kind, seed=seed, width=w, height=h, num_spheres=n, subdivision=sub)
 
 
-def plastic_mirror_scene(scene: rb.Scene) -> rb.Scene:
-    """The scene with every fourth material (from the second) plastic and every
-    fourth (from the third) a mirror; the rest unchanged."""
+def extra_materials_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with every fourth material (from the second) plastic, every
+    fourth (from the third) a mirror and every eighth (from the fourth) a
+    substrate; the rest unchanged."""
     mats = []
     for k in range(scene.desc.num_materials):
         m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
@@ -38,6 +39,13 @@ def plastic_mirror_scene(scene: rb.Scene) -> rb.Scene:
             m = rb.MaterialDesc()
             m.kind = rb.RB_MATERIAL_MIRROR
             m.reflectance[:] = (0.9, 0.85, 0.8)
+        elif k % 8 == 3:
+            m = rb.MaterialDesc()
+            m.kind = rb.RB_MATERIAL_SUBSTRATE
+            m.diffuse[:] = (0.5, 0.35, 0.2)
+            m.reflectance[:] = (0.05, 0.05, 0.05)
+            m.roughness_u, m.roughness_v = 0.1, 0.25
+            m.remap_roughness = 1
         mats.append(m)
     return scene.with_materials(mats)
 

@@ -1,13 +1,13 @@
-"""Plastic and mirror materials on the GPU: with spp = 1 the film sum of a pixel
+"""Plastic, mirror and substrate materials on the GPU: with spp = 1 the film sum of a pixel
 is one sample's radiance, against the reference's path_integrator::trace on the
-spheres scene with plastic and mirror materials (golden fixture), and the same
+spheres scene with plastic, mirror and substrate materials (golden fixture), and the same
 scene in direct lighting against the host build."""
 import numpy as np
 import pytest
 
 import rainbow_b200 as rb
 from tests import golden
-from tests.helpers import HostPaths, plastic_mirror_scene, scene_from_params
+from tests.helpers import HostPaths, extra_materials_scene, scene_from_params
 
 pytestmark = pytest.mark.gpu
 
@@ -19,9 +19,9 @@ def _agreement(gpu, want):
     return ok.all(axis=1).mean()
 
 
-def test_plastic_mirror_samples_match_reference():
+def test_extra_materials_samples_match_reference():
     fx = golden.load("materials_samples")
-    scene = plastic_mirror_scene(scene_from_params(fx["params"]))
+    scene = extra_materials_scene(scene_from_params(fx["params"]))
     depth = int(fx["max_depth"])
     px, sm, want = fx["pixels"], fx["samples"], fx["radiance"]
     got = np.zeros_like(want)
@@ -39,9 +39,9 @@ def test_plastic_mirror_samples_match_reference():
     assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
 
 
-def test_plastic_mirror_direct_matches_host_build():
+def test_extra_materials_direct_matches_host_build():
     fx = golden.load("materials_samples")
-    scene = plastic_mirror_scene(scene_from_params(fx["params"]))
+    scene = extra_materials_scene(scene_from_params(fx["params"]))
     W, H = scene.camera.width, scene.camera.height
     px = np.arange(W * H, dtype=np.uint32)
     want = HostPaths(scene).direct_samples(scene.camera, px, np.full_like(px, 2), 4, 4)
