@@ -290,19 +290,26 @@ rb_status rb_film_read(rb_context* ctx, double* sum_rgb, double* sum_sq_rgb, uin
  * render time (code that runs inside a framework which owns the device memory
  * pool, or a real-time loop where an allocation's implicit synchronisation is
  * not allowed). No counterpart in the reference, which has no device.
- * Same work as rb_render for samples [first_sample, first_sample + spp) of
- * every pixel, but all per-path state, queues and counters live in one static
- * device array of RB_NOALLOC_SCRATCH_BYTES that every GPU loading the library
- * keeps until exit; at most RB_NOALLOC_MAX_PATHS = width * height * spp paths
- * per call (larger requests return RB_ERR_TOO_LARGE). Results are ADDED to the
- * caller's device accumulators d_sum_rgb / d_sum_sq_rgb (3 doubles per pixel)
- * and d_count (one uint32 per pixel), which the caller zeroes before the first
- * call. The scene must have been uploaded with rb_scene_upload beforehand. The
- * first call on a device looks up the scratch array's device address, so make
- * it before any stream capture. Every call shares the one scratch array: calls
- * that overlap on the GPU (other streams, other threads) race, so serialise
- * them. `stream` is a cudaStream_t (NULL: the context's stream); the call
- * waits for its work to finish and returns the first device error, if any. */
+ * The plain path integrator only: the same work as rb_render without flags for
+ * samples [first_sample, first_sample + spp) of every pixel (scenes with
+ * invisible entities included: paths keep bouncing past max_depth until done,
+ * with a host read of the active count between those bounces). Any flag but
+ * RB_RENDER_RESET returns RB_ERR_UNSUPPORTED; RESET clears the caller's
+ * accumulators first. All per-path state, queues and counters live in one
+ * static device array of RB_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library keeps until exit; at most RB_NOALLOC_MAX_PATHS = width * height * spp
+ * paths per call (larger requests return RB_ERR_TOO_LARGE). Results are ADDED
+ * to the caller's device accumulators d_sum_rgb / d_sum_sq_rgb (3 doubles per
+ * pixel) and d_count (one uint32 per pixel), which the caller zeroes before the
+ * first call (or clears with RB_RENDER_RESET). The scene must have been
+ * uploaded with rb_scene_upload beforehand. The first call on a device looks up
+ * the scratch array's device address, so make it before any stream capture.
+ * Every call shares the one scratch array: calls that overlap on the GPU (other
+ * streams, other threads) race, so serialise them; the call also reads its
+ * counters through the context's page-locked buffer, so serialise it with every
+ * other call on the same context too. `stream` is a cudaStream_t (NULL: the
+ * context's stream); the call waits for its work to finish and returns the
+ * first device error, if any. */
 #define RB_NOALLOC_MAX_PATHS 16384u
 #define RB_NOALLOC_SCRATCH_BYTES (8u << 20)
 rb_status rb_render_noalloc(rb_context* ctx, const rb_render_params* params, double* d_sum_rgb, double* d_sum_sq_rgb,

@@ -635,19 +635,24 @@ bool host_is_valid_camera(const rb_camera_desc& cam) {
 
 namespace rb {
 namespace gpu {
-// Scene view, launch configuration, stream, device and pinned counter buffer of
-// a context, for entry points defined in other files of the library.
+// Scene view, launch configuration of a plain surface render (no counting, no
+// guide, no media: whatever the context's last rb_render used), stream, device,
+// pinned counter buffer and whether the scene has invisible entities, for entry
+// points defined in other files of the library.
 bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStream_t* stream, int* device,
-	uint32_t** counters_host) {
+	uint32_t** counters_host, bool* has_invisible) {
 	if (c == nullptr || !c->has_scene || c->is_batch) return false;
 	*view = c->view;
 	*cfg = c->cfg();
 	cfg->count = false;
 	cfg->guide = nullptr;
+	cfg->guide_medium = nullptr;
 	cfg->guide_mode = 0u;
+	cfg->volume = false;
 	*stream = c->stream;
 	*device = c->device;
 	*counters_host = c->counters_host;
+	*has_invisible = c->has_invisible;
 	return true;
 }
 

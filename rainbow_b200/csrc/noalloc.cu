@@ -7,6 +7,13 @@
 // nothing: per-path state, queues, counters and the wave parameter block are
 // carved out of g_noalloc_scratch below, and the film is the caller's.
 //
+// Only the plain path integrator is available here (RB_RENDER_RESET is the one
+// flag accepted): the volume, direct-lighting and guided renders need buffers
+// that the scratch array does not hold. Scenes with invisible entities get the
+// same bounded drain loop as rb_render's direct launches (a pass through a
+// shape without a material is not a bounce, so paths can outlive max_depth
+// iterations), with a host read of the active count between bounces.
+//
 // g_noalloc_scratch is a file-scope __device__ array, so every GPU that loads
 // the library holds its RB_NOALLOC_SCRATCH_BYTES until the process exits. In
 // host code its name only stands in for the device object: the device address
@@ -14,16 +21,17 @@
 // current, on the first call there (make that call before any stream capture).
 // Every call reuses the same array and finds the previous call's contents in
 // it; the counters and parameter block are rewritten by each call, so calls
-// that overlap on the GPU race and must be serialised by the caller.
-#include "../../include/rbgpu.h"
-#include "kernels.cuh"
+// that overlap on the GPU race and must be serialised by the caller. The call
+// also reads its counters back through the context's page-locked counter
+// buffer, so it must be serialised with every other call on the same context.
+#include "context.h"
 
 #include <mutex>
 
 namespace rb {
 namespace gpu {
 bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStream_t* stream, int* device,
-	uint32_t** counters_host);
+	uint32_t** counters_host, bool* has_invisible);
 } // namespace gpu
 } // namespace rb
 
@@ -104,11 +112,14 @@ extern "C" rb_status rb_render_noalloc(rb_context* ctx, const rb_render_params* 
 	cudaStream_t own = nullptr;
 	int device = 0;
 	uint32_t* counters_host = nullptr;
-	if (!rb::gpu::context_view(ctx, &view, &cfg, &own, &device, &counters_host)) return RB_ERR_NO_SCENE;
+	bool has_invisible = false;
+	if (!rb::gpu::context_view(ctx, &view, &cfg, &own, &device, &counters_host, &has_invisible)) return RB_ERR_NO_SCENE;
+	if (prm->flags & ~static_cast<uint32_t>(RB_RENDER_RESET)) return RB_ERR_UNSUPPORTED;  // plain path tracing only
 	const rb_camera_desc& cam = prm->camera;
-	if (cam.width <= 0 || cam.height <= 0 || prm->spp == 0 || prm->max_depth == 0 || prm->max_depth > 64)
+	if (!rb::ctx::host_is_valid_camera(cam) || prm->spp == 0 || prm->max_depth == 0 || prm->max_depth > 64)
 		return RB_ERR_INVALID_ARGUMENT;
 	if (static_cast<uint64_t>(prm->first_sample) + prm->spp > (1u << 24)) return RB_ERR_INVALID_ARGUMENT;
+	// both factors are below 2^24 here, so the product cannot wrap
 	const uint64_t pixels = static_cast<uint64_t>(cam.width) * static_cast<uint64_t>(cam.height);
 	const uint64_t paths = pixels * prm->spp;
 	if (paths > RB_NOALLOC_MAX_PATHS) return RB_ERR_TOO_LARGE;
@@ -161,14 +172,34 @@ extern "C" rb_status rb_render_noalloc(rb_context* ctx, const rb_render_params* 
 	p.max_depth = prm->max_depth;
 	p.rr_threshold = prm->rr_threshold;
 
+	// the call's own slot of the context's page-locked counter buffer (the last
+	// lane's; rb_render only touches it while it runs and returns synchronised)
+	uint32_t* h = counters_host + (rb::ctx::kMaxLanes - 1) * rb::gpu::CNT_WORDS;
+	cudaError_t e = cudaSuccess;
+	if (prm->flags & RB_RENDER_RESET) {  // the caller's accumulators, as rb_render clears its film
+		e = cudaMemsetAsync(d_sum_rgb, 0, 3 * pixels * sizeof(double), s);
+		if (e == cudaSuccess) e = cudaMemsetAsync(d_sum_sq_rgb, 0, 3 * pixels * sizeof(double), s);
+		if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, pixels * sizeof(uint32_t), s);
+	}
 	// everything that must start at zero: counters (queues, error word, stats)
-	if (cudaMemsetAsync(w.counters, 0, rb::gpu::CNT_WORDS * sizeof(uint32_t), s) != cudaSuccess) return RB_ERR_CUDA;
+	if (e == cudaSuccess) e = cudaMemsetAsync(w.counters, 0, rb::gpu::CNT_WORDS * sizeof(uint32_t), s);
+	if (e != cudaSuccess) return RB_ERR_CUDA;
 	k_noalloc_params<<<1, 1, 0, s>>>(p, w.params);
-	cudaError_t e = cudaGetLastError();
+	e = cudaGetLastError();
 	if (e == cudaSuccess) e = rb::gpu::launch_wave(view, w, f, prm->max_depth, 0u, cfg, s);
+	// scenes with invisible entities: keep bouncing until the active queue is
+	// empty, at most 4096 more bounces (rb_render's direct-launch drain)
+	uint32_t q = prm->max_depth & 1u;
+	for (int guard = 0; guard < 4096 && has_invisible && e == cudaSuccess; guard++) {
+		e = cudaMemcpyAsync(h, w.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+		if (e != cudaSuccess || h[rb::gpu::CNT_ACTIVE] == 0) break;
+		e = rb::gpu::launch_bounce(view, w, f, q, cfg, s);
+		q ^= 1u;
+	}
 	if (e == cudaSuccess) e = rb::gpu::launch_next_wave(w, f, cfg.grid_shade, s);
-	if (e == cudaSuccess) e = cudaMemcpyAsync(counters_host, w.counters, rb::gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(h, w.counters, rb::gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(s);
 	if (e != cudaSuccess) return RB_ERR_CUDA;
-	return counters_host[rb::gpu::CNT_ERROR] != 0 ? static_cast<rb_status>(counters_host[rb::gpu::CNT_ERROR]) : RB_OK;
+	return h[rb::gpu::CNT_ERROR] != 0 ? static_cast<rb_status>(h[rb::gpu::CNT_ERROR]) : RB_OK;
 }
