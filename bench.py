@@ -29,8 +29,10 @@ reference render has 4,096 spp instead of 65,536 so that the default run takes
 minutes (its own relMSE, about 0.0001 at 0.01 targets, is negligible).
 
 --impl reference times the reference CPU integrator (path_integrator::trace of
-the reference sources, compiled as oracle/_ref) on a bounded sample of each step
-on all host cores.
+the reference sources, compiled as oracle/_ref) on each step's whole workload
+(every pixel at one sample) on all host cores; its scene comes from the same
+seeded generator compiled into oracle/_ref, so that arm loads nothing of the
+product.
 """
 from __future__ import annotations
 
@@ -114,60 +116,60 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_reference_rate(scene, rows, spp, threads, first_sample=0):
-    """Msamples/s of the reference integrator (oracle/_ref) on image rows [rows[0], rows[1])."""
+def reference_scene():
+    """The workload's scene built by the oracle library alone (no product code imported or loaded)."""
     from oracle import ref
-    R = ref.RefScene(scene)
-    _, _, sec = R.render(spp, first_sample, WORKLOAD["max_depth"], 1.0, 0, threads, rows=rows)
-    samples = (rows[1] - rows[0]) * scene.camera.width * spp
-    return samples / sec / 1e6, sec, samples
+    return ref.RefScene.generated(WORKLOAD["kind"], WORKLOAD["seed"], WORKLOAD["width"], WORKLOAD["height"],
+                                  WORKLOAD["num_spheres"], WORKLOAD["subdivision"])
+
+
+def cpu_reference_frame(R, first_sample, threads):
+    """Seconds the reference integrator (oracle/_ref) takes for one step of the workload: every pixel of the
+    1024 x 1024 frame at one sample, on `threads` host threads."""
+    _, _, sec = R.render(1, first_sample, WORKLOAD["max_depth"], 1.0, 0, threads)
+    return sec
 
 
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    import rainbow_b200 as rb
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liboracle_ref.so not built"}))
         return 0
-    scene = rb.generate_scene(WORKLOAD["kind"], seed=WORKLOAD["seed"], width=WORKLOAD["width"],
-                              height=WORKLOAD["height"], num_spheres=WORKLOAD["num_spheres"],
-                              subdivision=WORKLOAD["subdivision"])
+    R = reference_scene()
     threads = os.cpu_count() or 1
-    rows = args.ref_rows
-    r0 = (WORKLOAD["height"] - rows) // 2
-    band = (r0, r0 + rows)
-    R = ref.RefScene(scene)
+    pixels = WORKLOAD["width"] * WORKLOAD["height"]
     for k in range(args.warmup):
-        R.render(1, 10_000 + k, WORKLOAD["max_depth"], 1.0, 0, threads, rows=(r0, r0 + max(1, rows // 4)))
-    total_s, total_samples = 0.0, 0
+        cpu_reference_frame(R, 10_000 + k, threads)
+    total_s = 0.0
     for k in range(args.steps):
-        _, _, sec = R.render(1, k, WORKLOAD["max_depth"], 1.0, 0, threads, rows=band)
-        total_s += sec
-        total_samples += rows * scene.camera.width
-    value = total_samples / total_s / 1e6
-    sample = f"rows {band[0]}-{band[1] - 1} of the 1024x1024 image, 1 spp per step ({rows * 1024} paths)"
+        total_s += cpu_reference_frame(R, k, threads)
+    value = args.steps * pixels / total_s / 1e6
+    sample = f"the whole step: all {pixels} pixels of the 1024x1024 frame at 1 spp per step"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_dict(world, l2="n/a (CPU)", timing="each step: the reference integrator on a band of image "
-                                                            "rows, wall clock, all host threads"),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural scene)", "config": config_dict(world),
+        "timing": "each step: the reference's path_integrator::trace (oracle/_ref, compiled from the reference "
+                  "sources) over every pixel at 1 spp, wall clock, all host threads; scene generated inside "
+                  f"oracle/_ref ({R.triangles} triangles)",
         "cpu_baseline": {"value": value, "unit": "Msamples/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
 
 
-def config_dict(world, l2="flushed before the timed call; per-step inputs exceed L2 (paths of a wave 0.45-1.8 GB, "
-                             "film 59 MB; the 86 MB scene stays resident across steps as in any multi-sample render)",
-                timing="K steps = one rb_render call of K samples per pixel, CUDA events on the library's stream"):
+def config_dict(world):
+    """The workload of one step, identical for both arms."""
     return {"workload": "sphere field, 1,024,010 triangles, 1024x1024, 1 spp per step, max depth 8",
             "triangles": 1024010, "width": WORKLOAD["width"], "height": WORKLOAD["height"],
-            "max_depth": WORKLOAD["max_depth"], "spp_per_step": 1, "timing": timing,
-            "parallelism": f"replicas x{world} (sample ranges)", "l2": l2}
+            "max_depth": WORKLOAD["max_depth"], "spp_per_step": 1,
+            "parallelism": f"replicas x{world} (sample ranges)",
+            "l2": "GPU arm: flushed before the timed call; per-step inputs exceed L2 (paths of a wave 0.45-1.8 GB, "
+                  "film 59 MB); the 86 MB scene stays resident across steps as in any multi-sample render"}
 
 
 def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=12, batch=1 << 17, train_chunks=4,
@@ -416,8 +418,6 @@ def main():
     ap.add_argument("--steps", type=int, default=32)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-rows", type=int, default=64, help="image rows per step timed on the CPU reference")
-    ap.add_argument("--cpu-rows", type=int, default=512, help="rows (a central band) of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
     ap.add_argument("--guided-res", type=int, default=1024)
@@ -556,15 +556,14 @@ def main():
             traffic = json.load(f).get("dram_bytes_per_launch")
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle import ref
             if ref.available():
                 threads = os.cpu_count() or 1
-                r0 = (H - args.cpu_rows) // 2
-                v, sec, n = cpu_reference_rate(scene, (r0, r0 + args.cpu_rows), 1, threads)
-                cpu = {"value": v, "unit": "Msamples/s", "cores": threads, "kind": "reference",
-                       "sample": f"rows {r0}-{r0 + args.cpu_rows - 1} of the image at 1 spp ({n} paths, {sec:.1f} s)"}
+                sec = cpu_reference_frame(reference_scene(), base, threads)
+                cpu = {"value": pixels / sec / 1e6, "unit": "Msamples/s", "cores": threads, "kind": "reference",
+                       "sample": f"one step: all {pixels} pixels at 1 spp ({sec:.2f} s)"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Msamples/s", "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
@@ -598,7 +597,9 @@ def main():
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": config_dict(world), "mrays_per_s": mrays, "per_call_1spp": per_call,
+            "config": config_dict(world),
+            "timing": "K steps = one rb_render call of K samples per pixel, CUDA events on the library's stream",
+            "mrays_per_s": mrays, "per_call_1spp": per_call,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "calls": "one rb_render per step (1 spp, image read back each call)", "tuning": e2e_tuning},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -5,7 +5,8 @@
 // tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it, as the
 // checker. It exposes C entry points that:
 //  - build a reference `scene` (entity / mesh / material / emitter objects, then
-//    scene::build_accelerator) and a `perspective_camera` from an rb_scene_desc;
+//    scene::build_accelerator) and a `perspective_camera` from an rb_scene_desc,
+//    or from the seeded scene generator of the benchmark configurations;
 //  - export the reference's own BVH, camera matrices and emitter areas;
 //  - trace rays through scene::intersect / intersect_with_shadow_ray;
 //  - render through path_integrator::trace with one PCG32 stream per
@@ -246,6 +247,30 @@ int orc_scene_build(const rb_scene_desc* desc, const rb_camera_desc* cam, orc_sc
 }
 
 void orc_scene_free(orc_scene* s) { delete s; }
+
+// The seeded synthetic scene of the benchmark configurations
+// (rb_scene_generate, compiled into this library from the same source file as
+// the product's generator), built directly as a reference scene and camera, so
+// that a CPU-only caller needs nothing but this library. *triangles: the
+// scene's triangle count.
+int orc_scene_generate(const rb_scene_gen_params* params, orc_scene** out, uint32_t* triangles) {
+	if (params == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	rb_scene* gen = nullptr;
+	int st = rb_scene_generate(params, &gen);
+	if (st != RB_OK) return st;
+	rb_scene_desc desc{};
+	rb_camera_desc cam{};
+	st = rb_scene_get(gen, &desc, &cam);
+	if (st == RB_OK && triangles != nullptr) {
+		uint64_t n = 0;
+		for (uint32_t i = 0; i < desc.num_entities; i++)
+			if (desc.entities[i].mesh >= 0) n += desc.meshes[desc.entities[i].mesh].num_triangles;
+		*triangles = static_cast<uint32_t>(n);
+	}
+	if (st == RB_OK) st = orc_scene_build(&desc, &cam, out);
+	rb_scene_free(gen);
+	return st;
+}
 
 // Selects the integrator of the tracing entry points: path_integrator (0) or
 // volume_path_integrator (1).

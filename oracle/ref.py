@@ -2,7 +2,9 @@
 
 The library is the reference renderer itself (rainbow-core + rainbow-cpu sources
 compiled by oracle/Makefile) plus oracle/harness/ref_harness.cpp. Entry points
-take the same rb_scene_desc / rb_camera_desc structures as the product.
+take the same rb_scene_desc / rb_camera_desc structures as the product, or build
+the seeded benchmark scenes themselves (RefScene.generated), in which case
+nothing of the product is imported or loaded.
 """
 from __future__ import annotations
 
@@ -24,13 +26,13 @@ def available() -> bool:
 def lib():
     global _LIB
     if _LIB is None:
-        from rainbow_b200._native import CameraDesc, SceneDesc
         if not available():
             raise FileNotFoundError(f"{LIB_PATH} missing (build with `make -C oracle ref` where the reference is present)")
         L = C.CDLL(LIB_PATH)
         vp, u32, f32, i32 = C.c_void_p, C.c_uint32, C.c_float, C.c_int
         sig = {
-            "orc_scene_build": (i32, [C.POINTER(SceneDesc), C.POINTER(CameraDesc), C.POINTER(vp)]),
+            "orc_scene_build": (i32, [vp, vp, C.POINTER(vp)]),
+            "orc_scene_generate": (i32, [vp, C.POINTER(vp), C.POINTER(u32)]),
             "orc_scene_free": (None, [vp]),
             "orc_export_bvh": (i32, [vp, vp, vp, vp, C.POINTER(u32), C.POINTER(u32)]),
             "orc_export_camera": (i32, [vp, vp, vp]),
@@ -58,14 +60,36 @@ def _ok(st, where):
         raise RuntimeError(f"{where} returned {st}")
 
 
+class _GenParams(C.Structure):
+    """rb_scene_gen_params of include/rbgpu.h."""
+    _fields_ = [("kind", C.c_uint32), ("seed", C.c_uint32), ("num_spheres", C.c_uint32), ("subdivision", C.c_uint32),
+                ("width", C.c_int32), ("height", C.c_int32)]
+
+
 class RefScene:
     """A reference `scene` + `perspective_camera` built from a product Scene description."""
 
     def __init__(self, scene):
         self.scene = scene
         self.h = C.c_void_p()
-        _ok(lib().orc_scene_build(C.byref(scene.desc), C.byref(scene.camera), C.byref(self.h)), "orc_scene_build")
+        _ok(lib().orc_scene_build(C.addressof(scene.desc), C.addressof(scene.camera), C.byref(self.h)),
+            "orc_scene_build")
         self.width, self.height = scene.camera.width, scene.camera.height
+        self.num_entities = scene.desc.num_entities
+
+    @classmethod
+    def generated(cls, kind, seed, width, height, num_spheres=0, subdivision=0):
+        """The seeded benchmark scene (kind: RB_SCENE_* of include/rbgpu.h) generated and built inside the oracle
+        library; .triangles holds its triangle count."""
+        self = cls.__new__(cls)
+        self.scene = None
+        self.h = C.c_void_p()
+        tris = C.c_uint32()
+        gp = _GenParams(kind, seed, num_spheres, subdivision, width, height)
+        _ok(lib().orc_scene_generate(C.addressof(gp), C.byref(self.h), C.byref(tris)), "orc_scene_generate")
+        self.width, self.height, self.triangles = width, height, tris.value
+        self.num_entities = None
+        return self
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -89,7 +113,7 @@ class RefScene:
         return r2c, c2w
 
     def areas(self):
-        a = np.zeros(self.scene.desc.num_entities, dtype=np.float32)
+        a = np.zeros(self.num_entities, dtype=np.float32)
         _ok(lib().orc_export_areas(self.h, a.ctypes.data), "orc_export_areas")
         return a
 

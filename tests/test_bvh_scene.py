@@ -78,3 +78,19 @@ def test_areas_equal_reference():
     fx = golden.load("spheres_rays")
     R = ref.RefScene(scene_from_params(fx["params"]))
     assert np.array_equal(R.areas(), fx["areas"])
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kind,n,sub", [(rb.RB_SCENE_BOX, 0, 0), (rb.RB_SCENE_SPHERES, 20, 2), (rb.RB_SCENE_FOG, 6, 2)])
+def test_oracle_generated_scene_equals_product_scene(kind, n, sub):
+    """The timed CPU reference builds its scene with the generator compiled into
+    the oracle library (so it loads nothing of the product); that scene must be
+    the one the GPU arm renders: same reference BVH, camera and triangle count."""
+    a = ref.RefScene.generated(kind, 5, 40, 30, n, sub)
+    sc = rb.generate_scene(kind, seed=5, width=40, height=30, num_spheres=n, subdivision=sub)
+    b = ref.RefScene(sc)
+    assert a.triangles == sc.num_triangles
+    for x, y in zip(a.bvh(), b.bvh()):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    for x, y in zip(a.camera_matrices(), b.camera_matrices()):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
