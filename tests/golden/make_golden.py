@@ -25,7 +25,32 @@ product's seeded scene generator:
                  scene with plastic and mirror materials (tests.helpers.extra_materials_scene)
   bsdf_plastic_*, bsdf_mirror_*, bsdf_substrate_*  the BSDF tables of those materials
 
-Usage: python tests/golden/make_golden.py [--only fog|direct|materials]
+The benchmark configurations themselves (--only baseline):
+  config1_image  configuration 1 as specified (box room, 256 x 256, depth 5):
+                 per-pixel mean and per-sample variance of a 512-spp render
+  c2_ray_levels  the 1,024,010-triangle sphere field of configuration 2: 2^19
+                 seeded camera rays and two generations of bounce rays from their
+                 hits (tests.helpers.ray_levels), traced by scene::intersect;
+                 per level the ray count, hit count, SHA-256 of every 4096 hits
+                 (entity, triangle, bits of t) and the first 4096 hits in full
+  slit_samples   configuration 4's slit room (2,048,018 triangles) at 64 x 64:
+                 radiance of 1024 (pixel, sample) pairs, path_integrator, depth 8
+  slit_image     the same room, 64 x 64, 1024 spp: per-pixel mean and variance
+  fog5_samples   configuration 5's fog (8,192,046 triangles) at 64 x 36: 512 pairs,
+                 volume_path_integrator, depth 12
+  fog5_image     the same fog, 64 x 36, 1024 spp: per-pixel mean and variance
+  box_converged  box room, 64 x 64, depth 5, 8192 spp: FP64 per-pixel means (the
+                 high-spp plain render that relMSE is measured against)
+  first_entity   added to box_samples, spheres_samples, materials_samples and
+                 fog_samples: the entity of each sample's camera-ray hit
+
+The reference's two-level tree (--only two_level):
+  two_level      tests.helpers.two_level_scene (a 327,680-triangle mesh and a mesh
+                 shared by two entities): 8192 seeded rays with scene::intersect and
+                 intersect_with_shadow_ray hits, and the radiance of 512 (pixel,
+                 sample) pairs, path_integrator, depth 5
+
+Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level]
 """
 from __future__ import annotations
 
@@ -67,6 +92,107 @@ def bvh_digest(nodes, pe, pi):
     for a in (nodes.astype(np.float32).view(np.uint32), pe.astype(np.uint32), pi.astype(np.uint32)):
         h.update(np.ascontiguousarray(a).tobytes())
     return h.hexdigest()
+
+
+C1 = dict(kind=rb.RB_SCENE_BOX, seed=0, width=256, height=256, num_spheres=0, subdivision=0)
+SLIT = dict(kind=rb.RB_SCENE_SLIT_ROOM, seed=3, width=64, height=64, num_spheres=100, subdivision=5)
+FOG5 = dict(kind=rb.RB_SCENE_FOG, seed=5, width=64, height=36, num_spheres=400, subdivision=5)
+
+
+def parallel_trace(R, rays, chunk=1 << 14):
+    """scene::intersect of a large batch on all host threads (ctypes releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    hits = np.zeros(rays.shape[0], dtype=rb.HIT_DTYPE)
+
+    def part(a):
+        hits[a:a + chunk] = R.trace(rays[a:a + chunk])
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        list(ex.map(part, range(0, rays.shape[0], chunk)))
+    return hits
+
+
+def mean_var(sums, sq, n):
+    mean = sums / n
+    var = np.maximum(sq / n - mean ** 2, 0.0)
+    return mean.astype(np.float32), var.astype(np.float32)
+
+
+def baseline_fixtures():
+    from tests.helpers import hit_digests, ray_levels
+    s = scene_of(C1)
+    R = ref.RefScene(s)
+    n = 512
+    sums, sq, sec = R.render(n, 0, 5, 1.0, 0, 0)
+    mean, var = mean_var(sums, sq, n)
+    save("config1_image", params=params_array(C1), spp=np.array(n), max_depth=np.array(5), mean=mean, var=var,
+         seconds=np.array(sec))
+
+    s = scene_of(dict(BOX, width=64, height=64))
+    R = ref.RefScene(s)
+    n = 8192
+    sums, _, sec = R.render(n, 0, 5, 1.0, 0, 0)
+    save("box_converged", params=params_array(dict(BOX, width=64, height=64)), spp=np.array(n), max_depth=np.array(5),
+         mean=sums / n)
+
+    s = scene_of(C2)
+    R = ref.RefScene(s)
+    levels = ray_levels(s.camera, lambda r: parallel_trace(R, r), 1 << 19, 21)
+    out = dict(params=params_array(C2), seed=np.array(21), n0=np.array(1 << 19))
+    for k, (rays, hits) in enumerate(levels):
+        out[f"count{k}"] = np.array(rays.shape[0])
+        out[f"hit_count{k}"] = np.array((hits["entity"] >= 0).sum())
+        out[f"digests{k}"] = hit_digests(hits)
+        out[f"head{k}"] = hits[:4096]
+    save("c2_ray_levels", **out)
+
+    for name, p, vol, depth, npairs in (("slit", SLIT, False, 8, 1024), ("fog5", FOG5, True, 12, 512)):
+        s = scene_of(p)
+        R = ref.RefScene(s)
+        R.set_volume(vol)
+        rng = np.random.default_rng(23)
+        px = rng.integers(0, p["width"] * p["height"], npairs).astype(np.uint32)
+        sm = rng.integers(0, 4096, npairs).astype(np.uint32)
+        L = R.trace_samples(px, sm, max_depth=depth, rr=1.0, seed=0)
+        save(f"{name}_samples", params=params_array(p), pixels=px, samples=sm, radiance=L, max_depth=np.array(depth),
+             first_entity=first_entity(R, px, sm))
+        n = 1024
+        sums, sq, sec = R.render(n, 0, depth, 1.0, 0, 0)
+        mean, var = mean_var(sums, sq, n)
+        save(f"{name}_image", params=params_array(p), spp=np.array(n), max_depth=np.array(depth), mean=mean, var=var,
+             seconds=np.array(sec))
+    add_first_entity()
+
+
+def two_level_fixtures():
+    from tests.helpers import random_rays, two_level_scene
+    s = two_level_scene()
+    R = ref.RefScene(s)
+    rays = random_rays(s, 8192, 35)
+    rng = np.random.default_rng(29)
+    px = rng.integers(0, s.camera.width * s.camera.height, 512).astype(np.uint32)
+    sm = rng.integers(0, 4096, 512).astype(np.uint32)
+    save("two_level", rays=rays, hits_closest=R.trace(rays), hits_shadow=R.trace(rays, shadow=True), pixels=px,
+         samples=sm, radiance=R.trace_samples(px, sm, max_depth=5, rr=1.0, seed=0), max_depth=np.array(5),
+         first_entity=first_entity(R, px, sm))
+
+
+def first_entity(R, px, sm):
+    """Entity ordinal of each (pixel, sample)'s camera-ray hit (-1: miss)."""
+    return R.trace(R.camera_rays(px, sm, 0))["entity"].astype(np.int32)
+
+
+def add_first_entity():
+    """Adds first_entity to the per-sample fixtures, leaving their other arrays as they are."""
+    from tests import golden
+    for name in ("box_samples", "spheres_samples", "materials_samples", "fog_samples"):
+        fx = golden.load(name)
+        sc = scene_of(dict(zip(("kind", "seed", "width", "height", "num_spheres", "subdivision"),
+                               (int(x) for x in fx["params"]))))
+        if name == "materials_samples":
+            from tests.helpers import extra_materials_scene
+            sc = extra_materials_scene(sc)
+        fx["first_entity"] = first_entity(ref.RefScene(sc), fx["pixels"], fx["samples"])
+        save(name, **fx)
 
 
 def fog_fixtures():
@@ -135,6 +261,10 @@ def main():
         return fog_fixtures()
     if only == "direct":
         return direct_fixtures()
+    if only == "baseline":
+        return baseline_fixtures()
+    if only == "two_level":
+        return two_level_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -180,6 +310,8 @@ def main():
     fog_fixtures()
     direct_fixtures()
     materials_fixtures()
+    baseline_fixtures()
+    two_level_fixtures()
 
 
 def material_desc(m):

@@ -8,6 +8,7 @@ import os
 import numpy as np
 
 import rainbow_b200 as rb
+from rainbow_b200 import _native
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HOSTPATHS = os.path.join(HERE, "native", "libhostpaths.so")
@@ -177,3 +178,187 @@ def random_rays(scene, n, seed):
     rays["direction"] = dirs.astype(np.float32)
     rays["length"] = np.inf
     return rays
+
+
+def _normalize32(x, y, z):
+    inv = np.float32(1.0) / np.sqrt((x * x + y * y) + z * z)
+    return x * inv, y * inv, z * inv
+
+
+def camera_ray_batch(camera, n, seed):
+    """n seeded camera rays of `camera`: raster point (x + u, y + v) of a random
+    pixel through raster_to_camera, normalised, then camera_to_world. Written as
+    element-wise float32 operations (each exactly rounded, no FMA, no BLAS), so
+    the batch is the same on every host."""
+    rng = np.random.default_rng(seed)
+    W, H = camera.width, camera.height
+    px = rng.integers(0, W * H, n)
+    jit = rng.random((n, 2)).astype(np.float32)
+    fx = (px % W).astype(np.float32) + jit[:, 0]
+    fy = (px // W).astype(np.float32) + jit[:, 1]
+    R = np.array(camera.raster_to_camera[:], dtype=np.float32)
+    Cw = np.array(camera.camera_to_world[:], dtype=np.float32)
+    cx, cy, cz = ((R[r] * fx + R[4 + r] * fy) + R[12 + r] for r in range(3))
+    cx, cy, cz = _normalize32(cx, cy, cz)
+    dx, dy, dz = ((Cw[r] * cx + Cw[4 + r] * cy) + Cw[8 + r] * cz for r in range(3))
+    dx, dy, dz = _normalize32(dx, dy, dz)
+    rays = np.zeros(n, dtype=rb.RAY_DTYPE)
+    rays["origin"] = np.array([Cw[12], Cw[13], Cw[14]], dtype=np.float32)
+    rays["direction"] = np.stack([dx, dy, dz], axis=1)
+    rays["length"] = np.inf
+    return rays
+
+
+def bounce_ray_batch(rays, hits, seed):
+    """One secondary ray from every hit of `rays`: origin at the hit point
+    o + t d stepped back toward the ray's origin by 1e-3 (1 + max |p|), direction
+    uniform over the hemisphere facing back along the ray (the side the ray came
+    from), length +inf. Element-wise float32 arithmetic on the given hits, so two
+    hosts with the same hits make the same rays."""
+    sel = np.flatnonzero(hits["entity"] >= 0)
+    o, d, t = rays["origin"][sel], rays["direction"][sel], hits["t"][sel]
+    p = o + t[:, None] * d
+    step = np.float32(1e-3) * (np.float32(1.0) + np.abs(p).max(axis=1))
+    org = p - d * step[:, None]
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(sel.shape[0], 3))
+    norm = np.sqrt((v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1]) + v[:, 2] * v[:, 2])
+    v = (v / norm[:, None]).astype(np.float32)
+    facing = (v[:, 0] * d[:, 0] + v[:, 1] * d[:, 1]) + v[:, 2] * d[:, 2]
+    v[facing > 0] *= np.float32(-1.0)
+    out = np.zeros(sel.shape[0], dtype=rb.RAY_DTYPE)
+    out["origin"], out["direction"], out["length"] = org, v, np.inf
+    return out
+
+
+def ray_levels(camera, trace, n0, seed, levels=3):
+    """Camera rays, then levels - 1 generations of bounce rays from the previous
+    generation's hits; trace(rays) -> hits. Returns [(rays, hits)] per level."""
+    out = []
+    rays = camera_ray_batch(camera, n0, seed)
+    for k in range(levels):
+        hits = trace(rays)
+        out.append((rays, hits))
+        if k + 1 < levels:
+            rays = bounce_ray_batch(rays, hits, seed + 1 + k)
+    return out
+
+
+def hit_digests(hits, chunk=4096):
+    """SHA-256 per chunk of `chunk` hits over entity, triangle and the bits of t."""
+    import hashlib
+    out = []
+    for a in range(0, hits.shape[0], chunk):
+        h = hashlib.sha256()
+        b = hits[a:a + chunk]
+        for col in (b["entity"].astype(np.int32), b["triangle"].astype(np.int32), b["t"].astype(np.float32).view(np.uint32)):
+            h.update(np.ascontiguousarray(col).tobytes())
+        out.append(h.hexdigest()[:16])
+    return np.array(out)
+
+
+SAMPLE_RTOL = 1e-3  # per-channel agreement of one sample: |a - b| <= 1e-3 * max(1, |b|)
+
+
+def sample_agreement(got, want):
+    """Per sample: every channel within SAMPLE_RTOL of the reference."""
+    return (np.abs(got - want) <= SAMPLE_RTOL * np.maximum(1.0, np.abs(want))).all(axis=1)
+
+
+def _material_kind(scene, entity):
+    if entity < 0:
+        return "miss"
+    e = scene.desc.entities[int(entity)]
+    if e.material < 0:
+        return "invisible"
+    return {0: "matte", 1: "metal", 2: "glass", 3: "plastic", 4: "mirror", 5: "substrate"}.get(
+        scene.desc.materials[e.material].kind, "other")
+
+
+def assert_disagreements_unbiased(scene, got, want, first_entity, what=""):
+    """The samples that differ from the reference (paths that diverged where
+    CUDA's and glibc's transcendental functions round differently) must scatter
+    around it without a systematic sign, overall and per material of the first
+    hit: with d the luminance difference of each disagreeing sample,
+    |sum d| <= 4 sqrt(sum d^2) (a zero-mean sum of n terms has that spread), and
+    the count of d > 0 is within 4 sigma of n / 2."""
+    ok = sample_agreement(got, want)
+    lum = np.array([0.212671, 0.715160, 0.072169])
+    d = (got.astype(np.float64) - want.astype(np.float64)) @ lum
+    kinds = np.array([_material_kind(scene, e) for e in first_entity])
+    groups = [("all", np.ones_like(ok))] + [(k, kinds == k) for k in np.unique(kinds)]
+    for name, sel in groups:
+        m = sel & ~ok & (d != 0)
+        n = int(m.sum())
+        if n < 8:
+            continue
+        dd = d[m]
+        assert abs(dd.sum()) <= 4.0 * np.sqrt((dd ** 2).sum()), \
+            f"{what}: {n} disagreeing samples on {name} are biased (sum {dd.sum():.4g}, rms {np.sqrt((dd ** 2).mean()):.4g})"
+        pos = int((dd > 0).sum())
+        assert abs(pos - n / 2) <= 4.0 * np.sqrt(n / 4), f"{what}: {pos} of {n} disagreeing samples on {name} are higher"
+
+
+def per_sample_radiance(ctx, scene, pixels, samples, depth, volume=False):
+    """Radiance of (pixel, sample) pairs: one one-sample render per distinct sample index."""
+    got = np.zeros((pixels.shape[0], 3), dtype=np.float32)
+    for s in np.unique(samples):
+        ctx.render(scene.camera, spp=1, first_sample=int(s), max_depth=depth, want_image=False, volume=volume)
+        sums, _, cnt = ctx.film()
+        sel = samples == s
+        got[sel] = sums.reshape(-1, 3)[pixels[sel]]
+        assert (cnt.reshape(-1)[pixels[sel]] == 1).all()
+    return got
+
+
+def block_z(mean, ref_mean, ref_var, n, n_ref, block=4):
+    """z-scores of block means (block x block pixels, per channel) of an n-spp
+    render against an n_ref-spp reference, with the reference's per-sample
+    variance for both (under equal distributions the two share it)."""
+    H, W, _ = mean.shape
+    h, w = H // block * block, W // block * block
+
+    def blocks(a):
+        return a[:h, :w].reshape(h // block, block, w // block, block, 3)
+
+    bm = blocks(mean).mean(axis=(1, 3))
+    br = blocks(ref_mean).mean(axis=(1, 3))
+    bv = blocks(ref_var).sum(axis=(1, 3)) / block ** 4
+    se = np.sqrt(bv * (1.0 / n + 1.0 / n_ref))
+    return np.where(se > 0, (bm - br) / np.where(se > 0, se, 1), 0.0)
+
+
+def two_level_scene(width=64, height=48):
+    """A scene that needs the reference's two-level tree (scene.cpp:41-75): the
+    seeded sphere field of 6 spheres (1,280 triangles each) with spheres 1 and 2
+    sharing sphere 1's mesh (each keeps its own transform), plus one sphere of
+    327,680 triangles (icosphere subdivision 7, more than 2^17) taken from a
+    second seeded scene. Meshes used by one entity and below 2^17 triangles
+    keep one leaf per triangle."""
+    base = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=9, width=width, height=height, num_spheres=6, subdivision=3)
+    big = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=10, width=width, height=height, num_spheres=1, subdivision=7)
+    d = base.desc
+    meshes = [_native.MeshDesc.from_buffer_copy(bytes(d.meshes[i])) for i in range(d.num_meshes)]
+    ents = [_native.EntityDesc.from_buffer_copy(bytes(d.entities[i])) for i in range(d.num_entities)]
+    sphere_ents = [k for k, e in enumerate(ents) if e.mesh >= 0 and e.emitter < 0 and
+                   d.meshes[e.mesh].num_triangles == 1280]
+    a, b = sphere_ents[1], sphere_ents[2]
+    ents[b].mesh = ents[a].mesh
+    bd = big.desc
+    big_ent = next(k for k in range(bd.num_entities) if bd.entities[k].mesh >= 0 and
+                   bd.meshes[bd.entities[k].mesh].num_triangles == 327680)
+    meshes.append(_native.MeshDesc.from_buffer_copy(bytes(bd.meshes[bd.entities[big_ent].mesh])))
+    e = _native.EntityDesc.from_buffer_copy(bytes(bd.entities[big_ent]))
+    e.mesh = len(meshes) - 1
+    e.material = ents[sphere_ents[0]].material
+    e.emitter = -1
+    ents.append(e)
+    mesh_arr = (_native.MeshDesc * len(meshes))(*meshes)
+    ent_arr = (_native.EntityDesc * len(ents))(*ents)
+    nd = rb.SceneDesc()
+    C.pointer(nd)[0] = d
+    nd.meshes = C.cast(mesh_arr, type(nd.meshes))
+    nd.num_meshes = len(meshes)
+    nd.entities = C.cast(ent_arr, type(nd.entities))
+    nd.num_entities = len(ents)
+    return rb.Scene(None, nd, base.camera, keepalive=[base, big, mesh_arr, ent_arr])

@@ -7,7 +7,8 @@ import pytest
 
 import rainbow_b200 as rb
 from tests import golden
-from tests.helpers import HostPaths, extra_materials_scene, scene_from_params
+from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, per_sample_radiance,
+                           scene_from_params)
 
 pytestmark = pytest.mark.gpu
 
@@ -24,19 +25,13 @@ def test_extra_materials_samples_match_reference():
     scene = extra_materials_scene(scene_from_params(fx["params"]))
     depth = int(fx["max_depth"])
     px, sm, want = fx["pixels"], fx["samples"], fx["radiance"]
-    got = np.zeros_like(want)
-    idx = np.unique(sm)[:64]
     with rb.Context(0) as ctx:
         ctx.upload(scene)
-        for s in idx:
-            ctx.render(scene.camera, spp=1, first_sample=int(s), max_depth=depth, want_image=False)
-            sums, _, cnt = ctx.film()
-            sel = sm == s
-            got[sel] = sums.reshape(-1, 3)[px[sel]]
+        got = per_sample_radiance(ctx, scene, px, sm, depth)
         assert ctx.stats().device_error == 0
-    used = np.isin(sm, idx)
-    agree = _agreement(got[used], want[used])
+    agree = _agreement(got, want)
     assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
+    assert_disagreements_unbiased(scene, got, want, fx["first_entity"], "materials")
 
 
 def test_extra_materials_direct_matches_host_build():

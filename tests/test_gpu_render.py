@@ -13,7 +13,7 @@ import pytest
 
 import rainbow_b200 as rb
 from tests import golden
-from tests.helpers import HostPaths, scene_from_params
+from tests.helpers import HostPaths, assert_disagreements_unbiased, per_sample_radiance, scene_from_params
 
 pytestmark = pytest.mark.gpu
 
@@ -28,25 +28,19 @@ def _sample_agreement(gpu, ref):
 
 @pytest.mark.parametrize("name,min_agree", [("box_samples", 0.99), ("spheres_samples", 0.97)])
 def test_single_sample_radiance_matches_reference(name, min_agree):
+    """Every (pixel, sample) pair of the fixture (one one-sample render per
+    distinct sample index); the few that disagree must show no bias overall or
+    per material of the first hit."""
     fx = golden.load(name)
     scene = scene_from_params(fx["params"])
     depth = int(fx["max_depth"])
-    W, H = scene.camera.width, scene.camera.height
-    # fixture pairs: group by sample index, one spp=1 render per distinct index
     px, sm, want = fx["pixels"], fx["samples"], fx["radiance"]
-    got = np.zeros_like(want)
     with rb.Context(0) as ctx:
         ctx.upload(scene)
-        for s in np.unique(sm)[:64]:
-            ctx.render(scene.camera, spp=1, first_sample=int(s), max_depth=depth, want_image=False)
-            sums, _, cnt = ctx.film()
-            sel = sm == s
-            flat = sums.reshape(-1, 3)
-            got[sel] = flat[px[sel]]
-            assert (cnt.reshape(-1)[px[sel]] == 1).all()
-        used = np.isin(sm, np.unique(sm)[:64])
-    agree = _sample_agreement(got[used], want[used])
+        got = per_sample_radiance(ctx, scene, px, sm, depth)
+    agree = _sample_agreement(got, want)
     assert agree >= min_agree, f"{name}: only {agree:.4f} of samples agree with the reference"
+    assert_disagreements_unbiased(scene, got, want, fx["first_entity"], name)
 
 
 def test_whole_image_one_sample_matches_host_stage_build():

@@ -8,7 +8,7 @@ import pytest
 
 import rainbow_b200 as rb
 from tests import golden
-from tests.helpers import scene_from_params
+from tests.helpers import assert_disagreements_unbiased, per_sample_radiance, scene_from_params
 
 pytestmark = pytest.mark.gpu
 
@@ -20,23 +20,16 @@ def test_volume_samples_match_reference():
     scene = scene_from_params(fx["params"])
     depth = int(fx["max_depth"])
     px, sm, want = fx["pixels"], fx["samples"], fx["radiance"]
-    got = np.zeros_like(want)
     with rb.Context(0) as ctx:
         ctx.upload(scene)
-        idx = np.unique(sm)[:96]
-        for s in idx:
-            ctx.render(scene.camera, spp=1, first_sample=int(s), max_depth=depth, want_image=False, volume=True)
-            sums, _, cnt = ctx.film()
-            sel = sm == s
-            got[sel] = sums.reshape(-1, 3)[px[sel]]
-            assert (cnt.reshape(-1)[px[sel]] == 1).all()
+        got = per_sample_radiance(ctx, scene, px, sm, depth, volume=True)
         assert ctx.stats().device_error == 0
-    used = np.isin(sm, idx)
-    ok = np.abs(got[used] - want[used]) <= SAMPLE_RTOL * np.maximum(1.0, np.abs(want[used]))
+    ok = np.abs(got - want) <= SAMPLE_RTOL * np.maximum(1.0, np.abs(want))
     agree = ok.all(axis=1).mean()
     # samples that scatter in the medium draw several log / exp / sin / cos per
     # vertex, where CUDA and glibc may round differently and a path then diverges
     assert agree >= 0.9, f"only {agree:.4f} of volume samples agree with the reference"
+    assert_disagreements_unbiased(scene, got, want, fx["first_entity"], "fog")
 
 
 def test_volume_image_means_within_three_sigma():
