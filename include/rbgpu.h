@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 5
+#define RBGPU_ABI_VERSION 6
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -147,8 +147,13 @@ typedef struct rb_entity_desc {
  * Node i is 8 words: min.xyz, max.xyz (float), then w0, w1 (uint32 bit patterns):
  *   interior: left child = i + 1, w0 = right child index, w1 = split axis (0..2)
  *   leaf:     w0 = first prim slot, w1 = RB_BVH_LEAF_FLAG | count
- * Prim slot s refers to triangle prim_index[s] of entity prim_entity[s]. */
+ * Prim slot s refers to triangle prim_index[s] of entity prim_entity[s], or,
+ * when prim_index[s] is RB_BVH_ALL_TRIANGLES, to the whole entity: its mesh has
+ * a tree of its own in local space (the reference's two-level case,
+ * scene::build_accelerator, scene.cpp:41-75, for a mesh used by several
+ * entities or with more than 2^17 triangles; rb_bvh_get_mesh_tree). */
 #define RB_BVH_LEAF_FLAG 0x80000000u
+#define RB_BVH_ALL_TRIANGLES 0xffffffffu
 typedef struct rb_bvh_desc {
 	const float* nodes;         /* 8 * num_nodes words */
 	uint32_t num_nodes;
@@ -169,7 +174,8 @@ typedef struct rb_scene_desc {
 	uint32_t num_materials;
 	uint32_t num_emitters;
 	const rb_emitter_desc* emitters;
-	rb_bvh_desc bvh;            /* num_nodes == 0: rb_scene_upload builds it (rb_bvh_build) */
+	rb_bvh_desc bvh;            /* num_nodes == 0: rb_scene_upload builds it (rb_bvh_build); a supplied
+	                               tree's RB_BVH_ALL_TRIANGLES prims get their mesh trees built */
 	const rb_medium_desc* mediums;
 	uint32_t num_mediums;
 	uint32_t num_media;
@@ -517,15 +523,24 @@ rb_status rb_guide_medium_stats_get(rb_context* ctx, rb_guide_stats* out);
 
 /* ------------------------------------------------------------------ host-side helpers (no GPU) */
 
-/* Build the flattened BVH of a scene with the reference's rules: one leaf per
- * triangle of each entity, median split on the widest centroid axis with
- * std::nth_element (detail/bounding_volume_hierarchy.hpp:162-233). Returns
- * RB_ERR_UNSUPPORTED for scenes that need the reference's two-level tree
- * (a shape referenced more than once or more than 2^17 triangles, scene.cpp:41-75). */
+/* Build the flattened BVH of a scene with the reference's rules
+ * (scene::build_accelerator, scene.cpp:30-80): one leaf per triangle of each
+ * entity whose mesh is used by that entity only and has at most 2^17
+ * triangles, one leaf for the whole entity otherwise (prim_index
+ * RB_BVH_ALL_TRIANGLES), whose mesh then gets its own tree over its faces in
+ * local space (mesh::build_accelerator, mesh.cpp:159-172); median split on the
+ * widest centroid axis with std::nth_element (detail/bounding_volume_hierarchy.hpp:162-233).
+ * rb_bvh_depth: the deepest nesting, a mesh tree's levels counted below the
+ * scene tree's entity leaf. */
 typedef struct rb_bvh rb_bvh;
 rb_status rb_bvh_build(const rb_scene_desc* desc, rb_bvh** out);
 rb_status rb_bvh_get(const rb_bvh* bvh, rb_bvh_desc* out);
 rb_status rb_bvh_depth(const rb_bvh* bvh, uint32_t* max_depth);
+/* The mesh trees of the two-level case (mesh::mAccelerator), in order of first
+ * use: tree k belongs to mesh *mesh; in *out, prim slot p is face prim_index[p]
+ * of that mesh and prim_entity is NULL. */
+rb_status rb_bvh_mesh_tree_count(const rb_bvh* bvh, uint32_t* count);
+rb_status rb_bvh_get_mesh_tree(const rb_bvh* bvh, uint32_t k, int32_t* mesh, rb_bvh_desc* out);
 void rb_bvh_free(rb_bvh* bvh);
 
 /* Seeded synthetic scenes of the benchmark configurations. */

@@ -73,6 +73,10 @@ struct entity_instance_tag { friend constexpr auto member_of(entity_instance_tag
 struct camera_raster_to_camera_tag { friend constexpr auto member_of(camera_raster_to_camera_tag); };
 struct camera_to_world_tag { friend constexpr auto member_of(camera_to_world_tag); };
 struct film_pixels_tag { friend constexpr auto member_of(film_pixels_tag); };
+struct mesh_accelerator_tag { friend constexpr auto member_of(mesh_accelerator_tag); };
+struct mesh_bvh_root_tag { friend constexpr auto member_of(mesh_bvh_root_tag); };
+struct mesh_bvh_boxes_tag { friend constexpr auto member_of(mesh_bvh_boxes_tag); };
+struct entity_world_to_local_tag { friend constexpr auto member_of(entity_world_to_local_tag); };
 
 template struct access_bind<&scene::mAccelerator, scene_accelerator_tag>;
 template struct access_bind<&bounding_volume_hierarchy<scene::entity_reference>::mRoot, bvh_root_tag>;
@@ -81,6 +85,10 @@ template struct access_bind<&entity::mShapeInstanceProperties, entity_instance_t
 template struct access_bind<&projective_camera::mRasterToCamera, camera_raster_to_camera_tag>;
 template struct access_bind<&camera::mCameraToWorld, camera_to_world_tag>;
 template struct access_bind<&film::mPixels, film_pixels_tag>;
+template struct access_bind<&mesh::mAccelerator, mesh_accelerator_tag>;
+template struct access_bind<&bounding_volume_hierarchy<mesh::mesh_reference>::mRoot, mesh_bvh_root_tag>;
+template struct access_bind<&accelerator<mesh::mesh_reference>::mBoundingBoxes, mesh_bvh_boxes_tag>;
+template struct access_bind<&entity::mWorldToLocal, entity_world_to_local_tag>;
 
 namespace {
 
@@ -298,6 +306,27 @@ template <typename T>
 const std::vector<bounding_box<T>>& bvh_boxes(const accelerator<T>& acc) {
 	return acc.*member_of(bvh_boxes_tag{});
 }
+// mesh::mesh_reference is a private type: it is recovered from the type of the
+// mAccelerator member pointer (types carry no access checks, names do).
+template <typename> struct member_type;
+template <typename C, typename M> struct member_type<M C::*> { using type = M; };
+template <typename> struct accelerator_element;
+template <typename T> struct accelerator_element<accelerator<T>> { using type = T; };
+using mesh_ref = typename accelerator_element<
+	typename member_type<decltype(member_of(mesh_accelerator_tag{}))>::type::element_type>::type;
+const bounding_volume_hierarchy_node<mesh_ref>* bvh_root(const accelerator<mesh_ref>& acc) {
+	const auto& bvh = dynamic_cast<const bounding_volume_hierarchy<mesh_ref>&>(acc);
+	return bvh.*member_of(mesh_bvh_root_tag{});
+}
+const std::vector<bounding_box<mesh_ref>>& bvh_boxes(const accelerator<mesh_ref>& acc) {
+	return acc.*member_of(mesh_bvh_boxes_tag{});
+}
+// The accelerator of an entity's mesh (built by scene::build_accelerator in the
+// two-level case), or null.
+const accelerator<mesh_ref>* mesh_accelerator(const entity& e) {
+	const auto m = std::dynamic_pointer_cast<mesh>(e.component<shape>());
+	return m ? ((*m).*member_of(mesh_accelerator_tag{})).get() : nullptr;
+}
 
 void put_u32(float* dst, uint32_t v) { std::memcpy(dst, &v, sizeof(v)); }
 
@@ -321,6 +350,29 @@ void flatten(const orc_scene* s, const bounding_volume_hierarchy_node<T>* n, std
 	put_u32(w + 7, static_cast<uint32_t>(n->axis));
 }
 
+// The walk of mesh::intersect over a mesh's own tree (the reference's
+// bounding_volume_hierarchy<mesh_reference>::intersect order) on a local ray,
+// calling the reference's triangle test; *face: the last face that hit.
+void mesh_walk(const accelerator<mesh_ref>& acc, const ray& r, int32_t* face) {
+	const auto* root = bvh_root(acc);
+	const auto& boxes = bvh_boxes(acc);
+	std::vector<const bounding_volume_hierarchy_node<mesh_ref>*> stack{root};
+	const auto inv = static_cast<real>(1) / r.direction;
+	const bool neg[3] = {inv.x < 0, inv.y < 0, inv.z < 0};
+	while (!stack.empty()) {
+		const auto* n = stack.back();
+		stack.pop_back();
+		if (!n->box.intersect(r)) continue;
+		if (n->is_leaf()) {
+			for (auto i = n->begin; i < n->end; i++)
+				if (boxes[i].entity->intersect(r).has_value()) *face = static_cast<int32_t>(boxes[i].entity->face);
+			continue;
+		}
+		if (neg[n->axis]) { stack.push_back(n->left); stack.push_back(n->right); }
+		else { stack.push_back(n->right); stack.push_back(n->left); }
+	}
+}
+
 // Closest-hit walk over the reference's tree in the order of
 // bounding_volume_hierarchy<T>::intersect (detail/bounding_volume_hierarchy.hpp:60-108),
 // calling the reference's own leaf test, to learn which triangle was hit (the
@@ -342,6 +394,18 @@ void walk(const accelerator<T>& acc, const ray& r, bool shadow, const orc_scene*
 			for (auto i = n->begin; i < n->end; i++) {
 				const auto& ref = *boxes[i].entity;
 				if (shadow && !ref.entity->visible()) continue;
+				if (ref.index == std::numeric_limits<size_t>::max()) {
+					// the whole entity: entity::intersect walks its mesh's tree with the
+					// local ray; the same walk on a copy of that local ray names the face
+					const ray local = ((*ref.entity).*member_of(entity_world_to_local_tag{}))(r);
+					int32_t face = -1;
+					mesh_walk(*mesh_accelerator(*ref.entity), local, &face);
+					if (ref.intersect(r).has_value()) {
+						*ent = s->ordinal.at(ref.entity.get());
+						*tri = face;
+					}
+					continue;
+				}
 				if (ref.intersect(r).has_value()) {
 					*ent = s->ordinal.at(ref.entity.get());
 					*tri = static_cast<int32_t>(ref.index);
@@ -371,10 +435,27 @@ int orc_export_bvh(orc_scene* s, float* nodes, uint32_t* prim_entity, uint32_t* 
 	std::memcpy(nodes, flat.data(), flat.size() * sizeof(float));
 	for (size_t i = 0; i < boxes.size(); i++) {
 		const auto& ref = *boxes[i].entity;
-		if (ref.index == std::numeric_limits<size_t>::max()) return RB_ERR_UNSUPPORTED;  // two-level leaf
 		prim_entity[i] = static_cast<uint32_t>(s->ordinal.at(ref.entity.get()));
-		prim_index[i] = static_cast<uint32_t>(ref.index);
+		prim_index[i] = ref.index == std::numeric_limits<size_t>::max() ? RB_BVH_ALL_TRIANGLES : static_cast<uint32_t>(ref.index);
 	}
+	return RB_OK;
+}
+
+// Flattened copy of the reference's own tree of entity `entity`'s mesh (the
+// two-level case: mesh::build_accelerator); faces[p] is the face of leaf
+// element p. RB_ERR_UNSUPPORTED when the mesh has no tree. NULL arrays: sizes only.
+int orc_export_mesh_bvh(orc_scene* s, uint32_t entity, float* nodes, uint32_t* faces, uint32_t* num_nodes, uint32_t* num_prims) {
+	if (entity >= s->entities.size()) return RB_ERR_INVALID_ARGUMENT;
+	const auto* acc = mesh_accelerator(*s->entities[entity]);
+	if (acc == nullptr) return RB_ERR_UNSUPPORTED;
+	const auto& boxes = bvh_boxes(*acc);
+	std::vector<float> flat;
+	flatten(s, bvh_root(*acc), flat);
+	*num_nodes = static_cast<uint32_t>(flat.size() / 8);
+	*num_prims = static_cast<uint32_t>(boxes.size());
+	if (nodes == nullptr) return RB_OK;
+	std::memcpy(nodes, flat.data(), flat.size() * sizeof(float));
+	for (size_t i = 0; i < boxes.size(); i++) faces[i] = static_cast<uint32_t>(boxes[i].entity->face);
 	return RB_OK;
 }
 

@@ -35,6 +35,7 @@ def lib():
             "orc_scene_generate": (i32, [vp, C.POINTER(vp), C.POINTER(u32)]),
             "orc_scene_free": (None, [vp]),
             "orc_export_bvh": (i32, [vp, vp, vp, vp, C.POINTER(u32), C.POINTER(u32)]),
+            "orc_export_mesh_bvh": (i32, [vp, u32, vp, vp, C.POINTER(u32), C.POINTER(u32)]),
             "orc_export_camera": (i32, [vp, vp, vp]),
             "orc_export_areas": (i32, [vp, vp]),
             "orc_trace": (i32, [vp, vp, u32, i32, vp, vp]),
@@ -105,6 +106,16 @@ class RefScene:
         _ok(lib().orc_export_bvh(self.h, nodes.ctypes.data, pe.ctypes.data, pi.ctypes.data, C.byref(nn), C.byref(npr)),
             "orc_export_bvh")
         return nodes, pe, pi
+
+    def mesh_bvh(self, entity):
+        """The reference's own tree of entity `entity`'s mesh (two-level case): nodes (n, 8) and leaf faces."""
+        nn, npr = C.c_uint32(), C.c_uint32()
+        _ok(lib().orc_export_mesh_bvh(self.h, entity, None, None, C.byref(nn), C.byref(npr)), "orc_export_mesh_bvh")
+        nodes = np.zeros((nn.value, 8), dtype=np.float32)
+        faces = np.zeros(npr.value, dtype=np.uint32)
+        _ok(lib().orc_export_mesh_bvh(self.h, entity, nodes.ctypes.data, faces.ctypes.data, C.byref(nn), C.byref(npr)),
+            "orc_export_mesh_bvh")
+        return nodes, faces
 
     def camera_matrices(self):
         r2c = np.zeros(16, dtype=np.float32)

@@ -21,7 +21,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._native import (  # noqa: F401  (re-exported constants)
-    GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
+    GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_BVH_ALL_TRIANGLES, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_MIRROR, RB_MATERIAL_PLASTIC, RB_MATERIAL_SUBSTRATE,
     RB_RENDER_GUIDE,
     RB_RENDER_DIRECT, RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
@@ -86,9 +86,10 @@ def generate_scene(kind: int, seed: int = 0, width: int = 256, height: int = 256
 class Bvh:
     nodes: np.ndarray        # (num_nodes, 8) float32 words
     prim_entity: np.ndarray  # uint32
-    prim_index: np.ndarray   # uint32
+    prim_index: np.ndarray   # uint32 (RB_BVH_ALL_TRIANGLES: the entity's whole mesh, which has its own tree)
     depth: int
     desc: BvhDesc
+    mesh_trees: list = None  # [(mesh index, nodes (n, 8) float32, faces uint32)] of the two-level case
 
 
 def build_bvh(scene: Scene) -> Bvh:
@@ -103,9 +104,20 @@ def build_bvh(scene: Scene) -> Bvh:
         nodes = np.ctypeslib.as_array(d.nodes, (d.num_nodes * 8,)).reshape(-1, 8).copy()
         pe = np.ctypeslib.as_array(d.prim_entity, (d.num_prims,)).copy()
         pi = np.ctypeslib.as_array(d.prim_index, (d.num_prims,)).copy()
+        count = C.c_uint32()
+        check(lib().rb_bvh_mesh_tree_count(h, C.byref(count)), "rb_bvh_mesh_tree_count")
+        trees = []
+        for k in range(count.value):
+            mesh = C.c_int32()
+            t = BvhDesc()
+            check(lib().rb_bvh_get_mesh_tree(h, k, C.byref(mesh), C.byref(t)), "rb_bvh_get_mesh_tree")
+            trees.append((mesh.value, np.ctypeslib.as_array(t.nodes, (t.num_nodes * 8,)).reshape(-1, 8).copy(),
+                          np.ctypeslib.as_array(t.prim_index, (t.num_prims,)).copy()))
     finally:
         lib().rb_bvh_free(h)
-    return bvh_from_arrays(nodes, pe, pi, int(depth.value))
+    b = bvh_from_arrays(nodes, pe, pi, int(depth.value))
+    b.mesh_trees = trees
+    return b
 
 
 def bvh_from_arrays(nodes: np.ndarray, prim_entity: np.ndarray, prim_index: np.ndarray, depth: int = 0) -> Bvh:

@@ -35,6 +35,7 @@ RB_GUIDE_NUM_PARAMS = 30000
 RB_GUIDE_INPUTS = 9
 RB_GUIDE_OUTPUTS = 48
 RB_BVH_LEAF_FLAG = 0x80000000
+RB_BVH_ALL_TRIANGLES = 0xFFFFFFFF
 RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS = 0, 1, 2
 RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL = 0, 1
 
@@ -172,6 +173,8 @@ SIGNATURES = {
     "rb_bvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),
     "rb_bvh_get": (C.c_int32, [C.c_void_p, C.POINTER(BvhDesc)]),
     "rb_bvh_depth": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "rb_bvh_mesh_tree_count": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "rb_bvh_get_mesh_tree": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(BvhDesc)]),
     "rb_bvh_free": (None, [C.c_void_p]),
     "rb_scene_generate": (C.c_int32, [C.POINTER(SceneGenParams), C.POINTER(C.c_void_p)]),
     "rb_scene_get": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(CameraDesc)]),

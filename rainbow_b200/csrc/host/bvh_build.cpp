@@ -3,15 +3,21 @@
 // Follows scene::build_accelerator (rainbow-cpu/scenes/scene.cpp:30-80) and
 // bounding_volume_hierarchy<T>::recursive_build / split_equal_count
 // (rainbow-cpu/shared/accelerators/detail/bounding_volume_hierarchy.hpp:162-233):
-//  - one leaf element per triangle of each shaped entity, in entity order,
-//    boxed in world space (mesh::bounding_box(transform, index), mesh.cpp:45-62);
+//  - one leaf element per triangle of each shaped entity whose mesh is used by
+//    that entity alone and has at most 2^17 triangles, in entity order, boxed in
+//    world space (mesh::bounding_box(transform, index), mesh.cpp:45-62);
+//  - one element for the whole entity otherwise (a mesh shared by several
+//    entities, or a larger one), boxed by transform::operator()(bound3)
+//    (transform.cpp:78-92) of the mesh's local box, with the mesh given its own
+//    tree over its faces in local space (mesh::build_accelerator, mesh.cpp:159-172);
 //  - a node over one element, or over elements whose centroids coincide on the
 //    widest centroid axis, is a leaf;
 //  - otherwise std::nth_element splits at (begin + end) / 2 on that axis.
 // std::nth_element is implementation-defined; this file and the reference are
 // both compiled against libstdc++, and with the same element order and
 // comparator it makes the same permutation, hence the same tree.
-#include "../../../include/rbgpu.h"
+#include "bvh_build.h"
+
 #include "../rb_math.h"
 
 #include <algorithm>
@@ -24,8 +30,9 @@ using rb::vec3;
 struct rb_bvh {
 	std::vector<float> nodes;          // 8 words per node
 	std::vector<uint32_t> prim_entity;
-	std::vector<uint32_t> prim_index;
-	uint32_t depth = 0;
+	std::vector<uint32_t> prim_index;  // RB_BVH_ALL_TRIANGLES: the entity's whole mesh (its own tree)
+	uint32_t depth = 0;                // of the scene tree
+	std::vector<rb::host::mesh_tree> meshes;
 };
 
 namespace {
@@ -43,6 +50,38 @@ box3 triangle_box(const float* l2w, vec3 p0, vec3 p1, vec3 p2) {
 	b.min = rb::vmin(b.min, p2);
 	b.max = rb::vmax(b.max, p2);
 	return b;
+}
+
+// transform::operator()(bound3) (transform.cpp:78-92): the box of min and
+// max, then the other six corners in the reference's order.
+box3 transform_box(const float* m, const box3& b) {
+	const vec3 a = rb::xform_point(m, b.min), c = rb::xform_point(m, b.max);
+	box3 r{rb::vmin(a, c), rb::vmax(a, c)};
+	const vec3 corners[6] = {
+		{b.min.x, b.min.y, b.max.z}, {b.min.x, b.max.y, b.min.z}, {b.min.x, b.max.y, b.max.z},
+		{b.max.x, b.min.y, b.min.z}, {b.max.x, b.min.y, b.max.z}, {b.max.x, b.max.y, b.min.z}};
+	for (const vec3& k : corners) {
+		const vec3 p = rb::xform_point(m, k);
+		r.min = rb::vmin(r.min, p);
+		r.max = rb::vmax(r.max, p);
+	}
+	return r;
+}
+
+const float kIdentity[16] = {1.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 1.f};
+
+vec3 vertex(const rb_mesh_desc& m, uint32_t i) { return vec3{m.positions[3 * i], m.positions[3 * i + 1], m.positions[3 * i + 2]}; }
+
+// Box of face t of mesh m under transform l2w (mesh::bounding_box(transform, index)).
+box3 face_box(const float* l2w, const rb_mesh_desc& m, uint32_t t) {
+	const uint32_t* idx = m.indices + 3 * t;
+	return triangle_box(l2w, vertex(m, idx[0]), vertex(m, idx[1]), vertex(m, idx[2]));
+}
+
+bool faces_valid(const rb_mesh_desc& m) {
+	for (uint64_t i = 0; i < 3ull * m.num_triangles; i++)
+		if (m.indices[i] >= m.num_vertices) return false;
+	return true;
 }
 
 struct element {
@@ -155,23 +194,36 @@ extern "C" rb_status rb_bvh_build(const rb_scene_desc* desc, rb_bvh** out) {
 	}
 
 	builder b;
+	std::vector<rb::host::mesh_tree> trees;
+	std::vector<int32_t> tree_of(desc->num_meshes, -1);
 	try {
 		for (uint32_t e = 0; e < desc->num_entities; e++) {
 			const rb_entity_desc& ent = desc->entities[e];
 			if (ent.mesh < 0) continue;
 			const rb_mesh_desc& mesh = desc->meshes[ent.mesh];
+			if (mesh.positions == nullptr || mesh.indices == nullptr || !faces_valid(mesh)) return RB_ERR_INVALID_ARGUMENT;
 			const uint64_t count = refs[ent.mesh];
-			if (!(count <= 1 && count * mesh.num_triangles <= (1u << 17))) return RB_ERR_UNSUPPORTED;
-			for (uint32_t t = 0; t < mesh.num_triangles; t++) {
-				const uint32_t* idx = mesh.indices + 3 * t;
-				if (idx[0] >= mesh.num_vertices || idx[1] >= mesh.num_vertices || idx[2] >= mesh.num_vertices)
-					return RB_ERR_INVALID_ARGUMENT;
-				const float* p = mesh.positions;
-				const vec3 p0{p[3 * idx[0]], p[3 * idx[0] + 1], p[3 * idx[0] + 2]};
-				const vec3 p1{p[3 * idx[1]], p[3 * idx[1] + 1], p[3 * idx[1] + 2]};
-				const vec3 p2{p[3 * idx[2]], p[3 * idx[2] + 1], p[3 * idx[2] + 2]};
-				b.elems.push_back(element{triangle_box(ent.local_to_world, p0, p1, p2), e, t});
+			if (count <= 1 && count * mesh.num_triangles <= (1u << 17)) {
+				for (uint32_t t = 0; t < mesh.num_triangles; t++)
+					b.elems.push_back(element{face_box(ent.local_to_world, mesh, t), e, t});
+				continue;
 			}
+			// the whole entity as one element, the mesh with its own tree (built once)
+			if (tree_of[ent.mesh] < 0) {
+				rb::host::mesh_tree tree;
+				const rb_status st = rb::host::build_mesh_tree(mesh, ent.mesh, tree);
+				if (st != RB_OK) return st;
+				tree_of[ent.mesh] = static_cast<int32_t>(trees.size());
+				trees.push_back(std::move(tree));
+			}
+			// the mesh's local box (mesh constructor, mesh.cpp:31-36), then entity::bounding_box
+			box3 local = face_box(kIdentity, mesh, 0);
+			for (uint32_t t = 1; t < mesh.num_triangles; t++) {
+				const box3 f = face_box(kIdentity, mesh, t);
+				local.min = rb::vmin(local.min, f.min);
+				local.max = rb::vmax(local.max, f.max);
+			}
+			b.elems.push_back(element{transform_box(ent.local_to_world, local), e, RB_BVH_ALL_TRIANGLES});
 		}
 		if (b.elems.empty()) return RB_ERR_INVALID_ARGUMENT;
 		b.nodes.reserve(2 * b.elems.size());
@@ -187,12 +239,43 @@ extern "C" rb_status rb_bvh_build(const rb_scene_desc* desc, rb_bvh** out) {
 			bvh->prim_index[i] = b.elems[i].triangle;
 		}
 		bvh->depth = b.max_depth;
+		bvh->meshes = std::move(trees);
 		*out = bvh;
 	} catch (const std::bad_alloc&) {
 		return RB_ERR_OUT_OF_MEMORY;
 	}
 	return RB_OK;
 }
+
+namespace rb {
+namespace host {
+
+rb_status build_mesh_tree(const rb_mesh_desc& mesh, int32_t mesh_index, mesh_tree& out) {
+	if (mesh.num_triangles == 0 || mesh.positions == nullptr || mesh.indices == nullptr || !faces_valid(mesh))
+		return RB_ERR_INVALID_ARGUMENT;
+	try {
+		builder b;
+		b.elems.reserve(mesh.num_triangles);
+		for (uint32_t t = 0; t < mesh.num_triangles; t++) b.elems.push_back(element{face_box(kIdentity, mesh, t), 0u, t});
+		b.nodes.reserve(2 * b.elems.size());
+		const int root = b.build(0, b.elems.size(), 0);
+		out = mesh_tree();
+		out.mesh = mesh_index;
+		out.nodes.reserve(b.nodes.size() * 8);
+		flatten(b, root, out.nodes);
+		out.faces.resize(b.elems.size());
+		for (size_t i = 0; i < b.elems.size(); i++) out.faces[i] = b.elems[i].triangle;
+		out.depth = b.max_depth;
+	} catch (const std::bad_alloc&) {
+		return RB_ERR_OUT_OF_MEMORY;
+	}
+	return RB_OK;
+}
+
+const std::vector<mesh_tree>& bvh_mesh_trees(const rb_bvh* bvh) { return bvh->meshes; }
+
+} // namespace host
+} // namespace rb
 
 extern "C" rb_status rb_bvh_get(const rb_bvh* bvh, rb_bvh_desc* out) {
 	if (bvh == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
@@ -206,7 +289,28 @@ extern "C" rb_status rb_bvh_get(const rb_bvh* bvh, rb_bvh_desc* out) {
 
 extern "C" rb_status rb_bvh_depth(const rb_bvh* bvh, uint32_t* max_depth) {
 	if (bvh == nullptr || max_depth == nullptr) return RB_ERR_INVALID_ARGUMENT;
-	*max_depth = bvh->depth;
+	uint32_t deepest_mesh = 0;
+	for (const auto& t : bvh->meshes) deepest_mesh = t.depth > deepest_mesh ? t.depth : deepest_mesh;
+	// a walk into a mesh tree continues below the scene tree's entity leaf
+	*max_depth = bvh->meshes.empty() ? bvh->depth : bvh->depth + 1 + deepest_mesh;
+	return RB_OK;
+}
+
+extern "C" rb_status rb_bvh_mesh_tree_count(const rb_bvh* bvh, uint32_t* count) {
+	if (bvh == nullptr || count == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	*count = static_cast<uint32_t>(bvh->meshes.size());
+	return RB_OK;
+}
+
+extern "C" rb_status rb_bvh_get_mesh_tree(const rb_bvh* bvh, uint32_t k, int32_t* mesh, rb_bvh_desc* out) {
+	if (bvh == nullptr || mesh == nullptr || out == nullptr || k >= bvh->meshes.size()) return RB_ERR_INVALID_ARGUMENT;
+	const auto& t = bvh->meshes[k];
+	*mesh = t.mesh;
+	out->nodes = t.nodes.data();
+	out->num_nodes = static_cast<uint32_t>(t.nodes.size() / 8);
+	out->num_prims = static_cast<uint32_t>(t.faces.size());
+	out->prim_entity = nullptr;
+	out->prim_index = t.faces.data();
 	return RB_OK;
 }
 

@@ -8,6 +8,8 @@
 //  - local-space triangle edges e1 = p1 - p0, e2 = p2 - p0 (mesh.cpp:334-335)
 #include "scene_pack.h"
 
+#include "bvh_build.h"
+
 #include "../pt/pt_bsdf.h"
 #include "../pt/pt_geom.h"
 
@@ -249,10 +251,58 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			}
 			out.bvh_depth = depth;
 		}
+		// ---- mesh trees of entities that the scene tree holds whole (prim index
+		// RB_BVH_ALL_TRIANGLES): the builder's, or built here with the same rules
+		// for a caller-supplied scene tree. Appended after the scene's nodes;
+		// their leaves are marked kMeshLeaf, with w0 relative to the first slot
+		// of the instance being walked (each instance has its own copy of the
+		// mesh's triangle slots, so a hit slot still names its entity).
+		std::vector<host::mesh_tree> own_trees;
+		std::vector<int32_t> tree_of(desc->num_meshes, -1);
+		if (built != nullptr) {
+			const auto& bt = host::bvh_mesh_trees(built);
+			for (size_t k = 0; k < bt.size(); k++) tree_of[bt[k].mesh] = static_cast<int32_t>(k);
+		} else {
+			for (uint32_t s = 0; s < bvh.num_prims; s++) {
+				if (bvh.prim_index[s] != RB_BVH_ALL_TRIANGLES) continue;
+				const uint32_t e = bvh.prim_entity[s];
+				if (e >= desc->num_entities || desc->entities[e].mesh < 0) return RB_ERR_INVALID_ARGUMENT;
+				const int32_t m = desc->entities[e].mesh;
+				if (tree_of[m] >= 0) continue;
+				host::mesh_tree t;
+				const rb_status st = host::build_mesh_tree(desc->meshes[m], m, t);
+				if (st != RB_OK) return st;
+				tree_of[m] = static_cast<int32_t>(own_trees.size());
+				own_trees.push_back(std::move(t));
+			}
+		}
+		const std::vector<host::mesh_tree>& trees = built != nullptr ? host::bvh_mesh_trees(built) : own_trees;
+		std::vector<uint32_t> tree_root(trees.size(), 0);
+		uint32_t deepest_tree = 0;
+		for (size_t k = 0; k < trees.size(); k++) {
+			const uint32_t base = static_cast<uint32_t>(out.nodes.size() / 2);
+			tree_root[k] = base;
+			deepest_tree = trees[k].depth > deepest_tree ? trees[k].depth : deepest_tree;
+			const std::vector<float>& tn = trees[k].nodes;
+			for (size_t n = 0; n < tn.size() / 8; n++) {
+				const float* w = tn.data() + 8 * n;
+				uint32_t w0, w1;
+				std::memcpy(&w0, w + 6, 4);
+				std::memcpy(&w1, w + 7, 4);
+				if (w1 & RB_BVH_LEAF_FLAG) w1 |= pt::kMeshLeaf;
+				else w0 += base;
+				float f0, f1;
+				std::memcpy(&f0, &w0, 4);
+				std::memcpy(&f1, &w1, 4);
+				out.nodes.push_back(float4{w[0], w[1], w[2], w[3]});
+				out.nodes.push_back(float4{w[4], w[5], f0, f1});
+			}
+		}
+		if (built == nullptr && !trees.empty()) out.bvh_depth += 1 + deepest_tree;
 		// ---- 4-wide nodes: every binary node at an even depth with its
-		// grandchildren as slots, numbered in preorder
+		// grandchildren as slots, numbered in preorder (the scene tree only)
 		{
-			const uint32_t nn = bvh.num_nodes;
+			const uint32_t nn = bvh.num_nodes;  // the scene tree's nodes (mesh trees follow them)
 			auto word = [&](uint32_t n, int k) {
 				uint32_t v;
 				std::memcpy(&v, bvh.nodes + 8ull * n + k, 4);
@@ -320,27 +370,63 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			out.wide_ok = ok;
 			if (!ok) out.wnodes.clear();
 		}
-		out.tri_a.resize(bvh.num_prims);
-		out.tri_b.resize(bvh.num_prims);
-		out.tri_c.resize(bvh.num_prims);
-		out.prim_index.assign(bvh.prim_index, bvh.prim_index + bvh.num_prims);
-		out.prim_entity.assign(bvh.prim_entity, bvh.prim_entity + bvh.num_prims);
+		// ---- prim slots: the scene tree's, then one block per whole-entity slot
+		uint64_t total = bvh.num_prims;
+		std::vector<uint32_t> block(bvh.num_prims, 0);
+		for (uint32_t s = 0; s < bvh.num_prims; s++) {
+			if (bvh.prim_index[s] != RB_BVH_ALL_TRIANGLES) continue;
+			const uint32_t e = bvh.prim_entity[s];
+			if (e >= desc->num_entities || desc->entities[e].mesh < 0) { rb_bvh_free(built); return RB_ERR_INVALID_ARGUMENT; }
+			block[s] = static_cast<uint32_t>(total);
+			total += trees[tree_of[desc->entities[e].mesh]].faces.size();
+		}
+		if (total >= (1ull << 31)) { rb_bvh_free(built); return RB_ERR_UNSUPPORTED; }
+		out.tri_a.resize(total);
+		out.tri_b.resize(total);
+		out.tri_c.resize(total);
+		out.prim_index.resize(total);
+		out.prim_entity.resize(total);
+		auto entity_word = [&](uint32_t e, uint32_t flags) {
+			uint32_t word = e | flags;
+			if (!(out.entities[e].flags & pt::ENT_VISIBLE)) word |= pt::kEntityInvisible;
+			float wf;
+			std::memcpy(&wf, &word, 4);
+			return wf;
+		};
+		// entity-local p0, e1 = p1 - p0, e2 = p2 - p0 of face t of entity e's mesh in slot `slot`
+		auto pack_triangle = [&](uint64_t slot, uint32_t e, uint32_t t) {
+			const rb_mesh_desc& md = desc->meshes[desc->entities[e].mesh];
+			const uint32_t* idx = md.indices + 3 * t;
+			const vec3 p0 = v3(md.positions, idx[0]), p1 = v3(md.positions, idx[1]), p2 = v3(md.positions, idx[2]);
+			const vec3 e1 = p1 - p0, e2 = p2 - p0;
+			out.tri_a[slot] = float4{p0.x, p0.y, p0.z, e1.x};
+			out.tri_b[slot] = float4{e1.y, e1.z, e2.x, e2.y};
+			out.tri_c[slot] = float2{e2.z, entity_word(e, 0u)};
+			out.prim_index[slot] = t;
+			out.prim_entity[slot] = e;
+		};
 		for (uint32_t s = 0; s < bvh.num_prims; s++) {
 			const uint32_t e = bvh.prim_entity[s];
 			if (e >= desc->num_entities || desc->entities[e].mesh < 0) { rb_bvh_free(built); return RB_ERR_INVALID_ARGUMENT; }
 			const rb_mesh_desc& md = desc->meshes[desc->entities[e].mesh];
 			const uint32_t t = bvh.prim_index[s];
+			if (t == RB_BVH_ALL_TRIANGLES) {
+				// the whole entity: its mesh tree's root and its block of slots
+				const int32_t k = tree_of[desc->entities[e].mesh];
+				float root, first;
+				std::memcpy(&root, &tree_root[k], 4);
+				std::memcpy(&first, &block[s], 4);
+				out.tri_a[s] = float4{root, first, 0.f, 0.f};
+				out.tri_b[s] = float4{0.f, 0.f, 0.f, 0.f};
+				out.tri_c[s] = float2{0.f, entity_word(e, pt::kEntityInstance)};
+				out.prim_index[s] = RB_BVH_ALL_TRIANGLES;
+				out.prim_entity[s] = e;
+				const std::vector<uint32_t>& faces = trees[k].faces;
+				for (size_t p = 0; p < faces.size(); p++) pack_triangle(block[s] + p, e, faces[p]);
+				continue;
+			}
 			if (t >= md.num_triangles) { rb_bvh_free(built); return RB_ERR_INVALID_ARGUMENT; }
-			const uint32_t* idx = md.indices + 3 * t;
-			const vec3 p0 = v3(md.positions, idx[0]), p1 = v3(md.positions, idx[1]), p2 = v3(md.positions, idx[2]);
-			const vec3 e1 = p1 - p0, e2 = p2 - p0;
-			uint32_t word = e;
-			if (!(out.entities[e].flags & pt::ENT_VISIBLE)) word |= 0x80000000u;
-			float wf;
-			std::memcpy(&wf, &word, 4);
-			out.tri_a[s] = float4{p0.x, p0.y, p0.z, e1.x};
-			out.tri_b[s] = float4{e1.y, e1.z, e2.x, e2.y};
-			out.tri_c[s] = float2{e2.z, wf};
+			pack_triangle(s, e, t);
 		}
 		rb_bvh_free(built);
 	} catch (const std::bad_alloc&) {
@@ -382,10 +468,12 @@ rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out
 			const int32_t medium_base = static_cast<int32_t>(out.mediums.size());
 			const int32_t media_base = static_cast<int32_t>(out.media.size());
 			// reference-layout nodes: interior w0 = right child, leaf w0 = first slot
+			// (a mesh tree's leaf: relative to the instance's block, unchanged)
 			for (size_t n = 0; n < p.nodes.size() / 2; n++) {
 				float4 a = p.nodes[2 * n], b = p.nodes[2 * n + 1];
 				const uint32_t w1 = bits(b.w);
-				b.z = from_bits(bits(b.z) + ((w1 & RB_BVH_LEAF_FLAG) ? slot_base : node_base));
+				if (!(w1 & RB_BVH_LEAF_FLAG)) b.z = from_bits(bits(b.z) + node_base);
+				else if (!(w1 & pt::kMeshLeaf)) b.z = from_bits(bits(b.z) + slot_base);
 				out.nodes.push_back(a);
 				out.nodes.push_back(b);
 			}
@@ -404,12 +492,17 @@ rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out
 			}
 			for (size_t k = 0; k < p.tri_a.size(); k++) {
 				float2 c = p.tri_c[k];
-				const uint32_t w = bits(c.y);
-				c.y = from_bits(((w & ~pt::kEntityInvisible) + entity_base) | (w & pt::kEntityInvisible));
+				const uint32_t w = bits(c.y), flags = w & ~pt::kEntityMask;
+				c.y = from_bits(((w & pt::kEntityMask) + entity_base) | flags);
 				out.tri_c.push_back(c);
 				out.prim_entity.push_back(p.prim_entity[k] + entity_base);
+				float4 a = p.tri_a[k];
+				if (w & pt::kEntityInstance) {  // a whole entity: its mesh tree's root and its block of slots
+					a.x = from_bits(bits(a.x) + node_base);
+					a.y = from_bits(bits(a.y) + slot_base);
+				}
+				out.tri_a.push_back(a);
 			}
-			append_vec(out.tri_a, p.tri_a);
 			append_vec(out.tri_b, p.tri_b);
 			append_vec(out.prim_index, p.prim_index);
 			for (pt::entity_rec e : p.entities) {

@@ -32,6 +32,7 @@ struct smem_stack {
 	__device__ void pop(uint32_t& v, float& t) { sp--; v = base[sp * stride]; t = te[sp * stride]; }
 	__device__ bool empty() const { return sp == 0; }
 	__device__ bool full() const { return sp + 2 > cap; }
+	__device__ uint32_t size() const { return sp; }
 };
 
 __device__ __forceinline__ smem_stack make_stack(uint32_t* smem, uint32_t cap) {

@@ -95,6 +95,13 @@ struct trace_counters {
 };
 
 constexpr uint32_t kEntityInvisible = 0x80000000u;  // flag in the tri_c entity word
+// flag in the tri_c entity word: the slot stands for a whole entity whose mesh
+// has its own tree (tri_a.x = the tree's root node, tri_a.y = the first slot of
+// the entity's copy of the mesh's triangles, in the tree's leaf order)
+constexpr uint32_t kEntityInstance = 0x40000000u;
+constexpr uint32_t kEntityMask = 0x3fffffffu;
+// flag in a mesh tree leaf's w1: w0 counts from the walked instance's first slot
+constexpr uint32_t kMeshLeaf = 0x40000000u;
 
 RB_HD float u32_as_float(uint32_t v) {
 #if defined(__CUDA_ARCH__)
@@ -113,6 +120,61 @@ RB_HD uint32_t float_as_u32(float f) {
 	__builtin_memcpy(&v, &f, 4);
 	return v;
 #endif
+}
+
+// entity::intersect(ray) for an entity held whole by the scene tree
+// (rainbow-cpu/scenes/entity.cpp:39-58 with mesh::intersect, mesh.cpp:45-57):
+// the ray goes to local space once, the mesh's own tree is walked in the
+// reference's visiting order with the local ray and the local length (which
+// every hit shortens), and if anything was hit the world length becomes local
+// length * |L2W d_local|. The walk uses the stack above the caller's entries and
+// leaves them as it found them. Returns false when the stack overflowed.
+template <bool COUNT, typename Stack>
+RB_HD bool instance_hit(const scene_view& s, uint32_t slot, uint32_t ent, vec3 o, vec3 d, float& len, hit_t& hit,
+	Stack& stack, trace_counters& cnt) {
+	const float4 ia = RB_LDG(s.tri_a + slot);
+	const uint32_t root = float_as_u32(ia.x), first = float_as_u32(ia.y);
+	const local_ray lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
+	const vec3 inv = 1.f / lr.d;
+	const bool neg[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+	float llen = len * lr.to_local;
+	bool any = false;
+	const uint32_t base = stack.size();
+	if (stack.full()) return false;
+	stack.push(root);
+	while (stack.size() > base) {
+		const uint32_t n = stack.pop();
+		const float4 a = RB_LDG(s.nodes + 2 * n);
+		const float4 b = RB_LDG(s.nodes + 2 * n + 1);
+		if (COUNT) cnt.nodes++;
+		if (!slab_hit(a, b, lr.o, inv, llen)) continue;
+		const uint32_t w0 = float_as_u32(b.z), w1 = float_as_u32(b.w);
+		if (w1 & RB_BVH_LEAF_FLAG) {
+			const uint32_t count = w1 & ~(RB_BVH_LEAF_FLAG | kMeshLeaf);
+			for (uint32_t k = 0; k < count; k++) {
+				const uint32_t sl = first + w0 + k;
+				const float4 ta = RB_LDG(s.tri_a + sl);
+				const float4 tb = RB_LDG(s.tri_b + sl);
+				const float2 tc = RB_LDG(s.tri_c + sl);
+				if (COUNT) cnt.tris++;
+				float t, b1, b2;
+				if (triangle_hit(lr.o, lr.d, llen, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y}, vec3{tb.z, tb.w, tc.x}, t,
+						b1, b2)) {
+					llen = t;
+					hit.slot = static_cast<int32_t>(sl);
+					hit.b1 = b1;
+					hit.b2 = b2;
+					any = true;
+				}
+			}
+			continue;
+		}
+		if (stack.full()) return false;
+		if (neg[w1]) { stack.push(n + 1); stack.push(w0); }
+		else { stack.push(w0); stack.push(n + 1); }
+	}
+	if (any) len = llen * lr.to_world;
+	return true;
 }
 
 // Closest hit in the visiting order of bounding_volume_hierarchy<T>::intersect
@@ -146,7 +208,11 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 				const float2 tc = RB_LDG(s.tri_c + slot);
 				const uint32_t ew = float_as_u32(tc.y);
 				if (SHADOW && (ew & kEntityInvisible)) continue;
-				const uint32_t ent = ew & ~kEntityInvisible;
+				const uint32_t ent = ew & kEntityMask;
+				if (ew & kEntityInstance) {
+					if (!instance_hit<COUNT>(s, slot, ent, o, d, len, hit, stack, cnt)) return false;
+					continue;
+				}
 				const float4 ta = RB_LDG(s.tri_a + slot);
 				const float4 tb = RB_LDG(s.tri_b + slot);
 				if (ent != cur_entity) {
@@ -266,7 +332,13 @@ RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 			const float2 tc = RB_LDG(s.tri_c + slot);
 			const uint32_t ew = float_as_u32(tc.y);
 			if (SHADOW && (ew & kEntityInvisible)) continue;
-			const uint32_t ent = ew & ~kEntityInvisible;
+			const uint32_t ent = ew & kEntityMask;
+			if (ew & kEntityInstance) {
+				trace_counters none{0u, 0u};
+				if (!instance_hit<false>(s, slot, ent, t.o, t.d, t.len, t.hit, stack, none)) return -1;
+				if (isnan(t.len)) return -1;
+				continue;
+			}
 			const float4 ta = RB_LDG(s.tri_a + slot);
 			const float4 tb = RB_LDG(s.tri_b + slot);
 			if (ent != t.cur_entity) {

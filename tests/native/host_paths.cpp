@@ -31,6 +31,7 @@ struct host_stack {
 	void pop(uint32_t& v, float& t) { sp--; v = data[sp]; t = te[sp]; }
 	bool empty() const { return sp == 0; }
 	bool full() const { return sp + 2 > 128; }
+	uint32_t size() const { return sp; }
 };
 
 struct hp_scene {

@@ -59,7 +59,7 @@ def test_scene_sizes_and_determinism():
     assert room.desc.num_emitters == 1
 
 
-def test_bvh_rejects_shared_meshes_and_bad_indices():
+def test_bvh_shared_mesh_is_two_level_and_bad_indices_rejected():
     s = rb.generate_scene(rb.RB_SCENE_BOX, width=16, height=16)
     d = rb.SceneDesc()
     ctypes.pointer(d)[0] = s.desc
@@ -69,8 +69,19 @@ def test_bvh_rejects_shared_meshes_and_bad_indices():
     ents[1].mesh = ents[0].mesh  # one shape referenced twice: the reference builds a two-level tree
     d.entities = ctypes.cast(ents, ctypes.POINTER(rb._native.EntityDesc))
     h = ctypes.c_void_p()
-    assert rb.lib().rb_bvh_build(ctypes.byref(d), ctypes.byref(h)) == 7  # RB_ERR_UNSUPPORTED
+    assert rb.lib().rb_bvh_build(ctypes.byref(d), ctypes.byref(h)) == 0
+    count = ctypes.c_uint32()
+    assert rb.lib().rb_bvh_mesh_tree_count(h, ctypes.byref(count)) == 0 and count.value == 1
+    rb.lib().rb_bvh_free(h)
     assert rb.lib().rb_bvh_build(None, ctypes.byref(h)) == 1
+    bad = (rb._native.MeshDesc * s.desc.num_meshes)()
+    for i in range(s.desc.num_meshes):
+        bad[i] = s.desc.meshes[i]
+    idx = (ctypes.c_uint32 * 3)(0, 1, 10 ** 6)
+    bad[0].indices = ctypes.cast(idx, ctypes.POINTER(ctypes.c_uint32))
+    bad[0].num_triangles = 1
+    d.meshes = ctypes.cast(bad, ctypes.POINTER(rb._native.MeshDesc))
+    assert rb.lib().rb_bvh_build(ctypes.byref(d), ctypes.byref(h)) == 1
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference oracle not built")

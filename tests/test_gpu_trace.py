@@ -71,3 +71,37 @@ def test_trace_empty_and_errors():
         r["length"] = [0.0, np.inf]
         h = ctx.trace_closest(r)
         assert h["entity"][0] == -1
+
+
+def test_two_level_scene_hits_match_reference():
+    """A 327,680-triangle mesh and a mesh shared by two entities: the scene tree
+    holds those entities whole and their meshes have their own trees (the
+    reference's two-level case). Hits bit-equal to scene::intersect and
+    intersect_with_shadow_ray, on the 4-wide path and on the reference-order
+    path (counting launches walk that one)."""
+    from tests.helpers import two_level_scene
+    fx = golden.load("two_level")
+    scene = two_level_scene()
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        assert_hits_equal(ctx.trace_closest(fx["rays"]), fx["hits_closest"], "two-level closest")
+        assert_hits_equal(ctx.trace_shadow(fx["rays"]), fx["hits_shadow"], "two-level shadow")
+        ctx.set_counting(True)
+        assert_hits_equal(ctx.trace_closest(fx["rays"]), fx["hits_closest"], "two-level closest, reference order")
+
+
+def test_two_level_scene_samples_match_reference():
+    from tests.helpers import assert_disagreements_unbiased, per_sample_radiance, sample_agreement, two_level_scene
+    fx = golden.load("two_level")
+    scene = two_level_scene()
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        got = per_sample_radiance(ctx, scene, fx["pixels"], fx["samples"], int(fx["max_depth"]))
+        assert ctx.stats().device_error == 0
+        # and whole renders on wave lanes with the 4-wide traversal
+        ctx.set_tuning(lanes=2, paths_per_wave=1024)
+        img = ctx.render(scene.camera, 8, max_depth=5, seed=3)
+        assert ctx.stats().device_error == 0 and np.isfinite(img).all()
+    agree = sample_agreement(got, fx["radiance"]).mean()
+    assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
+    assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], "two-level")
