@@ -256,6 +256,26 @@ int orc_scene_build(const rb_scene_desc* desc, const rb_camera_desc* cam, orc_sc
 
 void orc_scene_free(orc_scene* s) { delete s; }
 
+// The reference scene and camera of a harness scene (pointers to their
+// shared_ptrs), for other test libraries that drive reference objects.
+int orc_scene_objects(orc_scene* s, const void** world, const void** cam) {
+	if (s == nullptr || world == nullptr || cam == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	*world = &s->world;
+	*cam = &s->cam;
+	return RB_OK;
+}
+
+// The camera's film as an integrator left it: pixel::spectrum() of every pixel
+// (film.cpp:11-21), W * H * 3 floats.
+int orc_film_read(orc_scene* s, float* rgb) {
+	const auto& pixels = (*s->film_ptr).*member_of(film_pixels_tag{});
+	for (size_t i = 0; i < pixels.size(); i++) {
+		const spectrum L = pixels[i].spectrum();
+		rgb[3 * i] = L[0]; rgb[3 * i + 1] = L[1]; rgb[3 * i + 2] = L[2];
+	}
+	return RB_OK;
+}
+
 // The seeded synthetic scene of the benchmark configurations
 // (rb_scene_generate, compiled into this library from the same source file as
 // the product's generator), built directly as a reference scene and camera, so

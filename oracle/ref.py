@@ -48,6 +48,7 @@ def lib():
             "orc_bsdf": (i32, [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
             "orc_set_volume": (None, [vp, i32]),
             "orc_set_direct": (None, [vp, C.c_uint32, C.c_uint32]),
+            "orc_film_read": (i32, [vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -177,6 +178,12 @@ class RefScene:
                              q.ctypes.data, C.byref(sec)), "orc_render")
         return s, q, sec.value
 
+    def film(self):
+        """The camera's film as an integrator left it: pixel::spectrum() of every pixel (H, W, 3)."""
+        img = np.zeros((self.height, self.width, 3), dtype=np.float32)
+        _ok(lib().orc_film_read(self.h, img.ctypes.data), "orc_film_read")
+        return img
+
     def render_shipped(self, spp, max_depth=5, rr=1.0):
         img = np.zeros((self.height, self.width, 3), dtype=np.float32)
         sec = C.c_double()
@@ -203,3 +210,54 @@ def bsdf(material, wo, u, wi_eval, include):
                        out["wi"].ctypes.data, out["f"].ctypes.data, out["pdf"].ctypes.data, out["type"].ctypes.data,
                        out["f_eval"].ctypes.data, out["pdf_eval"].ctypes.data), "orc_bsdf")
     return out
+
+
+ADAPTER_PATH = os.path.join(HERE, "_ref", "libadapter_check.so")
+_ADAPTER = None
+
+
+def adapter_available() -> bool:
+    return os.path.exists(ADAPTER_PATH) and available()
+
+
+def adapter_lib():
+    """The drop-in adapter (rainbow_b200/adapter, wavefront_path_integrator) compiled against the reference,
+    with its test entry points; it loads the reference library and the product library."""
+    global _ADAPTER
+    if _ADAPTER is None:
+        lib()
+        L = C.CDLL(ADAPTER_PATH)
+        vp, u32, f32, i32 = C.c_void_p, C.c_uint32, C.c_float, C.c_int
+        L.adp_render.restype, L.adp_render.argtypes = i32, [vp, u32, u32, f32, u32, C.c_char_p, u32]
+        L.adp_export.restype = i32
+        L.adp_export.argtypes = [vp, vp, vp, vp, C.POINTER(u32), C.POINTER(u32), vp, vp, vp, vp]
+        _ADAPTER = L
+    return _ADAPTER
+
+
+def adapter_render(R, spp, max_depth=5, threshold=1.0, seed=0):
+    """wavefront_path_integrator(random_sampler2d(spp), random_sampler1d(spp), max_depth, threshold)
+    .render(camera, scene) on the reference scene of R; returns the camera's film (H, W, 3)."""
+    err = C.create_string_buffer(512)
+    st = adapter_lib().adp_render(R.h, spp, max_depth, threshold, seed, err, 512)
+    if st != 0:
+        raise RuntimeError(f"wavefront_path_integrator::render failed ({st}): {err.value.decode()}")
+    return R.film()
+
+
+def adapter_export(R, material_type, emitter_type, camera_type):
+    """The adapter's export of R's reference scene: (nodes, prim_entity, prim_index) of rb_bvh_build on it,
+    per-entity material / emitter descriptions with presence flags, and the camera description."""
+    L = adapter_lib()
+    nn, npr = C.c_uint32(), C.c_uint32()
+    _ok(L.adp_export(R.h, None, None, None, C.byref(nn), C.byref(npr), None, None, None, None), "adp_export")
+    nodes = np.zeros((nn.value, 8), dtype=np.float32)
+    pe = np.zeros(npr.value, dtype=np.uint32)
+    pi = np.zeros(npr.value, dtype=np.uint32)
+    ne = R.num_entities
+    mats, ems = (material_type * ne)(), (emitter_type * ne)()
+    has = np.zeros(2 * ne, dtype=np.int32)
+    cam = camera_type()
+    _ok(L.adp_export(R.h, nodes.ctypes.data, pe.ctypes.data, pi.ctypes.data, C.byref(nn), C.byref(npr), C.addressof(mats),
+                     C.addressof(ems), has.ctypes.data, C.addressof(cam)), "adp_export")
+    return (nodes, pe, pi), mats, ems, has.reshape(ne, 2), cam

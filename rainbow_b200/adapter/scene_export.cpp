@@ -1,0 +1,306 @@
+// Reference scene and camera -> rb_scene_desc / rb_camera_desc.
+//
+// The reference's classes keep every parameter private and offer no getters
+// (e.g. matte_material::mDiffuse, materials/matte_material.hpp:26-28;
+// surface_light::mRadiance, emitters/surface_light.hpp:24-25;
+// projective_camera::mRasterToCamera, cameras/camera.hpp:73-80). This file reads
+// them through member pointers formed in explicit template instantiations, where
+// the language does not apply access checks, and carried out by a friend
+// function of a tag type. A maintainer adding this adapter inside the
+// reference would give those classes const accessors instead and drop the
+// access_bind lines; nothing else here would change.
+#include "scene_export.hpp"
+
+#include "rainbow-cpu/cameras/perspective_camera.hpp"
+#include "rainbow-cpu/emitters/environment_light.hpp"
+#include "rainbow-cpu/emitters/surface_light.hpp"
+#include "rainbow-cpu/materials/glass_material.hpp"
+#include "rainbow-cpu/materials/matte_material.hpp"
+#include "rainbow-cpu/materials/metal_material.hpp"
+#include "rainbow-cpu/materials/mirror_material.hpp"
+#include "rainbow-cpu/materials/plastic_material.hpp"
+#include "rainbow-cpu/materials/substrate_material.hpp"
+#include "rainbow-cpu/media/homogeneous_medium.hpp"
+#include "rainbow-cpu/shapes/mesh.hpp"
+#include "rainbow-cpu/textures/constant_texture.hpp"
+
+#include <unordered_map>
+
+using namespace rainbow::cpus;
+
+namespace rb {
+namespace adapter {
+namespace {
+
+template <auto Member, typename Tag>
+struct access_bind {
+	friend constexpr auto member_of(Tag) { return Member; }
+};
+#define RB_PRIVATE_MEMBER(tag, member)                              \
+	struct tag { friend constexpr auto member_of(tag); };          \
+	template struct access_bind<&member, tag>
+
+RB_PRIVATE_MEMBER(mesh_positions, shapes::mesh::mPositions);
+RB_PRIVATE_MEMBER(mesh_normals, shapes::mesh::mNormals);
+RB_PRIVATE_MEMBER(mesh_tangents, shapes::mesh::mTangents);
+RB_PRIVATE_MEMBER(mesh_uvs, shapes::mesh::mUVs);
+RB_PRIVATE_MEMBER(mesh_indices, shapes::mesh::mIndices);
+RB_PRIVATE_MEMBER(mesh_mask, shapes::mesh::mMask);
+RB_PRIVATE_MEMBER(matte_diffuse, materials::matte_material::mDiffuse);
+RB_PRIVATE_MEMBER(matte_sigma, materials::matte_material::mSigma);
+RB_PRIVATE_MEMBER(metal_eta, materials::metal_material::mEta);
+RB_PRIVATE_MEMBER(metal_k, materials::metal_material::mK);
+RB_PRIVATE_MEMBER(metal_ru, materials::metal_material::mRoughnessU);
+RB_PRIVATE_MEMBER(metal_rv, materials::metal_material::mRoughnessV);
+RB_PRIVATE_MEMBER(metal_remap, materials::metal_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(glass_reflectance, materials::glass_material::mReflectance);
+RB_PRIVATE_MEMBER(glass_transmission, materials::glass_material::mTransmission);
+RB_PRIVATE_MEMBER(glass_ru, materials::glass_material::mRoughnessU);
+RB_PRIVATE_MEMBER(glass_rv, materials::glass_material::mRoughnessV);
+RB_PRIVATE_MEMBER(glass_eta, materials::glass_material::mEta);
+RB_PRIVATE_MEMBER(glass_remap, materials::glass_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(plastic_specular, materials::plastic_material::mSpecular);
+RB_PRIVATE_MEMBER(plastic_diffuse, materials::plastic_material::mDiffuse);
+RB_PRIVATE_MEMBER(plastic_roughness, materials::plastic_material::mRoughness);
+RB_PRIVATE_MEMBER(plastic_eta, materials::plastic_material::mEta);
+RB_PRIVATE_MEMBER(plastic_remap, materials::plastic_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(mirror_reflectance, materials::mirror_material::mReflectance);
+RB_PRIVATE_MEMBER(substrate_specular, materials::substrate_material::mSpecular);
+RB_PRIVATE_MEMBER(substrate_diffuse, materials::substrate_material::mDiffuse);
+RB_PRIVATE_MEMBER(substrate_ru, materials::substrate_material::mRoughnessU);
+RB_PRIVATE_MEMBER(substrate_rv, materials::substrate_material::mRoughnessV);
+RB_PRIVATE_MEMBER(substrate_remap, materials::substrate_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(surface_radiance, emitters::surface_light::mRadiance);
+RB_PRIVATE_MEMBER(environment_map, emitters::environment_light::mEnvironmentMap);
+RB_PRIVATE_MEMBER(environment_intensity, emitters::environment_light::mIntensity);
+RB_PRIVATE_MEMBER(environment_radius, emitters::environment_light::mRadius);
+RB_PRIVATE_MEMBER(medium_sigma_a, media::homogeneous_medium::mSigmaA);
+RB_PRIVATE_MEMBER(medium_sigma_s, media::homogeneous_medium::mSigmaS);
+RB_PRIVATE_MEMBER(medium_g, media::homogeneous_medium::mG);
+RB_PRIVATE_MEMBER(camera_raster_to_camera, cameras::projective_camera::mRasterToCamera);
+RB_PRIVATE_MEMBER(camera_focus, cameras::projective_camera::mFocus);
+RB_PRIVATE_MEMBER(camera_lens, cameras::projective_camera::mLens);
+RB_PRIVATE_MEMBER(camera_to_world, cameras::camera::mCameraToWorld);
+#undef RB_PRIVATE_MEMBER
+
+template <typename Tag, typename Object>
+const auto& read(const Object& o, Tag tag) { return o.*member_of(tag); }
+
+// The value of a constant texture (constant_texture_t::sample returns it
+// anywhere); false for any other texture.
+template <typename T>
+bool constant_value(const std::shared_ptr<textures::texture2d<T>>& t, T& out) {
+	const auto c = std::dynamic_pointer_cast<textures::constant_texture2d<T>>(t);
+	if (c == nullptr) return false;
+	out = c->sample(rainbow::core::math::vector2(0));
+	return true;
+}
+bool constant_rgb(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, float* rgb) {
+	shared::spectrums::spectrum v;
+	if (!constant_value(t, v)) return false;
+	rgb[0] = v[0]; rgb[1] = v[1]; rgb[2] = v[2];
+	return true;
+}
+bool constant_real(const std::shared_ptr<textures::texture2d<rainbow::core::real>>& t, float& v) { return constant_value(t, v); }
+
+void put_rgb(const shared::spectrums::spectrum& s, float* rgb) { rgb[0] = s[0]; rgb[1] = s[1]; rgb[2] = s[2]; }
+
+// glm's column-major storage, element (row r, column c) at [c * 4 + r].
+void put_matrix(const rainbow::core::math::matrix4x4& m, float* out) {
+	for (int c = 0; c < 4; c++)
+		for (int r = 0; r < 4; r++) out[c * 4 + r] = m[c][r];
+}
+
+rb_status export_material(const std::shared_ptr<materials::material>& m, rb_material_desc& d) {
+	d = rb_material_desc{};
+	bool ok = true;
+	if (const auto x = std::dynamic_pointer_cast<materials::matte_material>(m)) {
+		d.kind = RB_MATERIAL_MATTE;
+		ok = constant_rgb(read(*x, matte_diffuse{}), d.diffuse) && constant_real(read(*x, matte_sigma{}), d.sigma);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::metal_material>(m)) {
+		d.kind = RB_MATERIAL_METAL;
+		d.remap_roughness = read(*x, metal_remap{}) ? 1 : 0;
+		ok = constant_rgb(read(*x, metal_eta{}), d.eta) && constant_rgb(read(*x, metal_k{}), d.k) &&
+			constant_real(read(*x, metal_ru{}), d.roughness_u) && constant_real(read(*x, metal_rv{}), d.roughness_v);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::glass_material>(m)) {
+		d.kind = RB_MATERIAL_GLASS;
+		d.remap_roughness = read(*x, glass_remap{}) ? 1 : 0;
+		ok = constant_rgb(read(*x, glass_reflectance{}), d.reflectance) &&
+			constant_rgb(read(*x, glass_transmission{}), d.transmission) &&
+			constant_real(read(*x, glass_ru{}), d.roughness_u) && constant_real(read(*x, glass_rv{}), d.roughness_v) &&
+			constant_real(read(*x, glass_eta{}), d.ior);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::plastic_material>(m)) {
+		d.kind = RB_MATERIAL_PLASTIC;
+		d.remap_roughness = read(*x, plastic_remap{}) ? 1 : 0;
+		ok = constant_rgb(read(*x, plastic_specular{}), d.reflectance) && constant_rgb(read(*x, plastic_diffuse{}), d.diffuse) &&
+			constant_real(read(*x, plastic_roughness{}), d.roughness_u) && constant_real(read(*x, plastic_eta{}), d.ior);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::mirror_material>(m)) {
+		d.kind = RB_MATERIAL_MIRROR;
+		ok = constant_rgb(read(*x, mirror_reflectance{}), d.reflectance);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::substrate_material>(m)) {
+		d.kind = RB_MATERIAL_SUBSTRATE;
+		d.remap_roughness = read(*x, substrate_remap{}) ? 1 : 0;
+		ok = constant_rgb(read(*x, substrate_specular{}), d.reflectance) &&
+			constant_rgb(read(*x, substrate_diffuse{}), d.diffuse) && constant_real(read(*x, substrate_ru{}), d.roughness_u) &&
+			constant_real(read(*x, substrate_rv{}), d.roughness_v);
+	} else {
+		return RB_ERR_UNSUPPORTED;  // uber, translucent, mixture, subsurface
+	}
+	return ok ? RB_OK : RB_ERR_UNSUPPORTED;  // a texture that is not constant
+}
+
+rb_status export_emitter(const std::shared_ptr<emitters::emitter>& e, rb_emitter_desc& d) {
+	d = rb_emitter_desc{};
+	if (const auto x = std::dynamic_pointer_cast<emitters::surface_light>(e)) {
+		d.kind = RB_EMITTER_SURFACE;
+		put_rgb(read(*x, surface_radiance{}), d.radiance);
+		return RB_OK;
+	}
+	if (const auto x = std::dynamic_pointer_cast<emitters::environment_light>(e)) {
+		// the core renders the constant map of 1 that environment_light(intensity, radius) makes
+		shared::spectrums::spectrum map;
+		if (!constant_value(read(*x, environment_map{}), map) || map[0] != 1.f || map[1] != 1.f || map[2] != 1.f)
+			return RB_ERR_UNSUPPORTED;
+		d.kind = RB_EMITTER_ENVIRONMENT;
+		put_rgb(read(*x, environment_intensity{}), d.radiance);
+		d.radius = read(*x, environment_radius{});
+		return RB_OK;
+	}
+	return RB_ERR_UNSUPPORTED;  // point and directional lights
+}
+
+template <typename T>
+std::vector<float> flat(const std::vector<T>& v) {
+	std::vector<float> out;
+	out.reserve(3 * v.size());
+	for (const auto& p : v) { out.push_back(p.x); out.push_back(p.y); out.push_back(p.z); }
+	return out;
+}
+
+} // namespace
+
+rb_status export_scene(const scenes::scene& s, exported_scene& out) {
+	out = exported_scene();
+	std::unordered_map<const void*, int32_t> mesh_of, material_of, medium_of;
+	try {
+		for (const auto& ent : s.entities()) {
+			rb_entity_desc ed{};
+			ed.mesh = ed.material = ed.emitter = ed.medium = -1;
+			put_matrix(ent->transform().matrix(), ed.local_to_world);
+			put_matrix(ent->transform().inverse_matrix(), ed.world_to_local);
+			if (ent->has_component<shapes::shape>()) {
+				const auto shape = ent->component<shapes::shape>();
+				const auto m = std::dynamic_pointer_cast<shapes::mesh>(shape);
+				if (m == nullptr || read(*m, mesh_mask{}) != nullptr) return RB_ERR_UNSUPPORTED;  // sphere, disk, curve; alpha masks
+				auto it = mesh_of.find(shape.get());
+				if (it == mesh_of.end()) {
+					const auto& idx = read(*m, mesh_indices{});
+					out.positions.push_back(flat(read(*m, mesh_positions{})));
+					out.normals.push_back(flat(read(*m, mesh_normals{})));
+					out.tangents.push_back(flat(read(*m, mesh_tangents{})));
+					out.uvs.push_back(flat(read(*m, mesh_uvs{})));
+					out.indices.emplace_back(idx.begin(), idx.end());
+					rb_mesh_desc md{};
+					md.num_vertices = static_cast<uint32_t>(read(*m, mesh_positions{}).size());
+					md.num_triangles = static_cast<uint32_t>(idx.size() / 3);
+					md.reverse_orientation = m->reverse_orientation() ? 1 : 0;
+					out.meshes.push_back(md);
+					it = mesh_of.emplace(shape.get(), static_cast<int32_t>(out.meshes.size() - 1)).first;
+				}
+				ed.mesh = it->second;
+			}
+			if (ent->has_component<materials::material>()) {
+				const auto mat = ent->component<materials::material>();
+				auto it = material_of.find(mat.get());
+				if (it == material_of.end()) {
+					rb_material_desc md;
+					const rb_status st = export_material(mat, md);
+					if (st != RB_OK) return st;
+					out.materials.push_back(md);
+					it = material_of.emplace(mat.get(), static_cast<int32_t>(out.materials.size() - 1)).first;
+				}
+				ed.material = it->second;
+			}
+			if (ent->has_component<emitters::emitter>()) {
+				rb_emitter_desc em;
+				const rb_status st = export_emitter(ent->component<emitters::emitter>(), em);
+				if (st != RB_OK) return st;
+				out.emitters.push_back(em);
+				ed.emitter = static_cast<int32_t>(out.emitters.size() - 1);
+			}
+			if (ent->has_component<media::media>()) {
+				const auto md = ent->component<media::media>();
+				auto medium_index = [&](const std::shared_ptr<media::medium>& m, int32_t& index) -> rb_status {
+					index = -1;
+					if (m == nullptr) return RB_OK;
+					auto it = medium_of.find(m.get());
+					if (it == medium_of.end()) {
+						const auto h = std::dynamic_pointer_cast<media::homogeneous_medium>(m);
+						if (h == nullptr) return RB_ERR_UNSUPPORTED;  // heterogeneous media
+						rb_medium_desc r{};
+						put_rgb(read(*h, medium_sigma_a{}), r.sigma_a);
+						put_rgb(read(*h, medium_sigma_s{}), r.sigma_s);
+						r.g = read(*h, medium_g{});
+						out.mediums.push_back(r);
+						it = medium_of.emplace(m.get(), static_cast<int32_t>(out.mediums.size() - 1)).first;
+					}
+					index = it->second;
+					return RB_OK;
+				};
+				rb_media_desc r{};
+				rb_status st = medium_index(md->inside(), r.inside);
+				if (st == RB_OK) st = medium_index(md->outside(), r.outside);
+				if (st != RB_OK) return st;
+				out.media.push_back(r);
+				ed.medium = static_cast<int32_t>(out.media.size() - 1);
+			}
+			out.entities.push_back(ed);
+		}
+	} catch (const std::bad_alloc&) {
+		return RB_ERR_OUT_OF_MEMORY;
+	}
+	for (size_t i = 0; i < out.meshes.size(); i++) {
+		rb_mesh_desc& md = out.meshes[i];
+		md.positions = out.positions[i].data();
+		md.normals = out.normals[i].empty() ? nullptr : out.normals[i].data();
+		md.tangents = out.tangents[i].empty() ? nullptr : out.tangents[i].data();
+		md.uvs = out.uvs[i].empty() ? nullptr : out.uvs[i].data();
+		md.indices = out.indices[i].data();
+	}
+	rb_scene_desc& d = out.desc;
+	d = rb_scene_desc{};
+	d.meshes = out.meshes.data();
+	d.num_meshes = static_cast<uint32_t>(out.meshes.size());
+	d.entities = out.entities.data();
+	d.num_entities = static_cast<uint32_t>(out.entities.size());
+	d.materials = out.materials.data();
+	d.num_materials = static_cast<uint32_t>(out.materials.size());
+	d.emitters = out.emitters.data();
+	d.num_emitters = static_cast<uint32_t>(out.emitters.size());
+	d.mediums = out.mediums.data();
+	d.num_mediums = static_cast<uint32_t>(out.mediums.size());
+	d.media = out.media.data();
+	d.num_media = static_cast<uint32_t>(out.media.size());
+	return RB_OK;
+}
+
+rb_status export_camera(const cameras::camera& c, rb_camera_desc& out) {
+	const auto* p = dynamic_cast<const cameras::perspective_camera*>(&c);
+	if (p == nullptr) return RB_ERR_UNSUPPORTED;  // other camera models
+	out = rb_camera_desc{};
+	const auto& c2w = read(*p, camera_to_world{});
+	put_matrix(read(*p, camera_raster_to_camera{}).matrix(), out.raster_to_camera);
+	put_matrix(c2w.matrix(), out.camera_to_world);
+	out.eye[0] = out.camera_to_world[12];
+	out.eye[1] = out.camera_to_world[13];
+	out.eye[2] = out.camera_to_world[14];
+	out.lens_radius = read(*p, camera_lens{});
+	out.focus_distance = read(*p, camera_focus{});
+	const auto res = c.film()->resolution();
+	out.width = res.x;
+	out.height = res.y;
+	return RB_OK;
+}
+
+} // namespace adapter
+} // namespace rb
