@@ -57,6 +57,26 @@ METRIC = "time to relMSE 0.01: guided vs plain wavefront PT on 1 B200; Msamples/
 FALLBACK_HBM_GBS = 6650.0
 
 
+def measured_l2_copy_gbs(buf, mib=32, reps=50):
+    """Read + write GB/s of a device copy whose source and destination (2 x `mib` MiB) stay in the 126 MB L2,
+    best of three CUDA-event-timed loops of `reps` copies."""
+    import torch
+    n = mib << 20
+    src, dst = buf[:n], buf[n:2 * n]
+    dst.copy_(src)
+    best = None
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            dst.copy_(src)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+    return 2 * n * reps / (best / 1e3) / 1e9
+
+
 def measured_peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -412,6 +432,28 @@ def batched_leg(rb, device, spp=32, depth=6, probe_items=1 << 23):
             "tuning": tuning.as_dict(), "tuning_probe_ms": probe_ms, "device_error": st.device_error}
 
 
+def summary_of(extra, batched, guided):
+    """The headline figures of the extra legs in a few hundred characters."""
+    def pick(d, *keys):
+        return {k: (round(d[k], 4) if isinstance(d.get(k), float) else d.get(k)) for k in keys} if isinstance(d, dict) else d
+    out = {name: pick(extra.get(name), "gpu_msamples_per_s", "msamples_per_s", "cpu_reference_msamples_per_s", "error")
+           for name in ("config1", "direct", "spheres_s5", "config5_plain")}
+    out = {k: {a: b for a, b in v.items() if b is not None} if isinstance(v, dict) else v for k, v in out.items()}
+    if isinstance(batched, dict):
+        out["batched"] = {k: v for k, v in pick(batched, "msamples_per_s", "error").items() if v is not None}
+        if "scene_latency_ms" in batched:
+            out["batched"]["latency_ms_p50_p90_max"] = [round(batched["scene_latency_ms"][k], 1) for k in ("p50", "p90", "max")]
+    if isinstance(guided, dict) and "targets" in guided:
+        out["guided_time_to_relmse"] = {t: {"plain_s": r["plain_s"] and round(r["plain_s"], 4),
+                                            "guided_s": r["guided_s"] and round(r["guided_s"], 4),
+                                            "speedup": r["speedup"] and round(r["speedup"], 3),
+                                            "guided_s_per_seed": [g["s"] and round(g["s"], 4) for g in r["guided_runs"]]}
+                                        for t, r in guided["targets"].items()}
+    elif isinstance(guided, dict):
+        out["guided"] = guided
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -530,30 +572,27 @@ def main():
     h2d = 176  # wave parameter block copied in per call
     d2h = pixels * 3 * 4  # the image (per-pixel means, 3 floats) read back per call
 
-    # ---- roofline of the traversal kernels (separate untimed passes of the same step)
-    # (one wave of all 1,048,576 paths per launch, as in the ncu capture of profiles/)
-    timed_tuning = ctx.tuning()
-    ctx.set_tuning(timed_tuning, paths_per_wave=pixels, lanes=1)
+    # ---- roofline of the traversal kernels, from the timed call itself: the kernels time every launch on the
+    # device clock (first warp's start to last warp's end, inside the graphs and lanes of the timed run), and a
+    # counting pass over exactly the timed samples gives the reference traversal's box and triangle tests
+    trav_ms = st.extend_ms + st.secondary_ms
+    nl = max(1, st.extend_launches + st.secondary_launches)
     ctx.set_counting(True)
-    ctx.render(scene.camera, spp=1, first_sample=base, max_depth=depth, reset=True, want_image=False)
+    ctx.render(scene.camera, spp=args.steps, first_sample=base, max_depth=depth, reset=True, want_image=False)
     cst = ctx.stats()
     ctx.set_counting(False)
-    ctx.set_profiling(True)
-    ctx.render(scene.camera, spp=1, first_sample=base, max_depth=depth, reset=True, want_image=False)
-    pst = ctx.stats()
-    ctx.set_profiling(False)
-    ctx.set_tuning(timed_tuning)
     trav_rays = cst.extend_rays + cst.shadow_rays + cst.mis_rays
     alg_bytes = 32 * cst.node_visits + 40 * cst.triangle_tests + 48 * trav_rays
-    trav_ms = pst.extend_ms + pst.secondary_ms
-    nl = max(1, pst.extend_launches + pst.secondary_launches)
     peak, peak_kind = measured_peak_hbm()
-    achieved = alg_bytes / (trav_ms / 1e3) / 1e9
+    achieved = alg_bytes / (trav_ms / 1e3) / 1e9 if trav_ms > 0 else None
+    l2_peak = measured_l2_copy_gbs(flush)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traversal_sphere_field.json")
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            per_ray = json.load(f).get("dram_bytes_per_ray")
+        if per_ray:
+            traffic = per_ray * trav_rays / nl  # the captured launches' DRAM bytes per ray, per timed launch
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -602,14 +641,24 @@ def main():
             "mrays_per_s": mrays, "per_call_1spp": per_call,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "calls": "one rb_render per step (1 spp, image read back each call)", "tuning": e2e_tuning},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_extend + k_trace_secondary (BVH traversal)",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_extend + k_trace_secondary (BVH traversal), launches of the timed call",
                          "algorithmic_bytes_per_launch": alg_bytes / nl, "ms_per_launch": trav_ms / nl,
-                         "launches": nl},
+                         "launches": nl, "traversal_ms_summed_over_lanes": trav_ms, "step_ms": device_ms,
+                         "step_bound": {"achieved": alg_bytes / (device_ms / 1e3) / 1e9,
+                                        "frac": alg_bytes / (device_ms / 1e3) / 1e9 / peak,
+                                        "what": "all traversal bytes of the step over the whole step's time"},
+                         "l2": {"achieved": achieved, "peak": l2_peak,
+                                "frac": achieved / l2_peak if achieved and l2_peak else None,
+                                "peak_source": "measured in this run: copy of 32 MiB into 32 MiB, both L2-resident"}},
             "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches, "tuning": tuning,
-            "batched": batched, "guided": guided, **extra,
+            **{k: v for k, v in extra.items()},
+            "batched": batched, "guided": guided,
+            "summary": summary_of(extra, batched, guided),
         }
+        # "summary" is the line's last key, so that a reader that keeps only the
+        # end of the output still has every leg's headline figures
         print(json.dumps(line))
     ctx.close()
     if world > 1:

@@ -332,9 +332,11 @@ typedef struct rb_render_stats {
 	uint32_t device_error;      /* rb_status raised inside a kernel, RB_OK if none */
 	uint32_t kernel_launches;
 	float elapsed_ms;           /* device time of the call, CUDA events */
-	float extend_ms;            /* device time of the extend (closest-hit) launches; profiling only */
-	float secondary_ms;         /* device time of the shadow / MIS traversal launches; profiling only */
-	uint32_t extend_launches;   /* traversal launches timed by profiling */
+	float extend_ms;            /* device time of the extend (closest-hit) launches */
+	float secondary_ms;         /* device time of the shadow / MIS traversal launches */
+	uint32_t extend_launches;   /* traversal launches timed: with rb_set_profiling, by CUDA events around each
+	                               launch; otherwise by the device clock inside the kernels (from the first
+	                               warp's start to the last warp's end of each launch), on every lane */
 	uint32_t secondary_launches;
 } rb_render_stats;
 rb_status rb_render_stats_get(rb_context* ctx, rb_render_stats* out);

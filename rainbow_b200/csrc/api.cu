@@ -321,6 +321,35 @@ uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& c
 	return static_cast<uint32_t>(waves < want ? waves : want);
 }
 
+// Traversal time of a render call: with profiling, CUDA events around each
+// launch; otherwise the device-clock timers the traversal kernels keep in the
+// counters of each lane (the span of each launch from its first warp's start to
+// its last warp's end), summed over the lanes.
+void traversal_times(rb_context* c, uint32_t nlanes, rb_render_stats& s) {
+	s.extend_ms = s.secondary_ms = 0.f;
+	s.extend_launches = s.secondary_launches = 0;
+	if (c->profiling) {
+		for (uint32_t k = 0; k < c->next_event; k++) {
+			float ms = 0.f;
+			cudaEventElapsedTime(&ms, c->events[2 * k], c->events[2 * k + 1]);
+			if (c->event_kind[k] == 0) { s.extend_ms += ms; s.extend_launches++; }
+			else { s.secondary_ms += ms; s.secondary_launches++; }
+		}
+		return;
+	}
+	auto u64 = [](const uint32_t* a, uint32_t w) { return static_cast<uint64_t>(a[w]) | (static_cast<uint64_t>(a[w + 1]) << 32); };
+	uint64_t ext_ns = 0, sec_ns = 0;
+	for (uint32_t k = 0; k < nlanes; k++) {
+		const uint32_t* a = c->counters_host + k * gpu::CNT_WORDS;
+		ext_ns += u64(a, gpu::CNT_TIMER_EXTEND + gpu::TIMER_TOTAL_NS);
+		sec_ns += u64(a, gpu::CNT_TIMER_SECONDARY + gpu::TIMER_TOTAL_NS);
+		s.extend_launches += a[gpu::CNT_TIMER_EXTEND + gpu::TIMER_LAUNCHES];
+		s.secondary_launches += a[gpu::CNT_TIMER_SECONDARY + gpu::TIMER_LAUNCHES];
+	}
+	s.extend_ms = static_cast<float>(ext_ns * 1e-6);
+	s.secondary_ms = static_cast<float>(sec_ns * 1e-6);
+}
+
 // Runs the waves of one render call, whose parameters are in c->params_host
 // (first_item is set here): one graph replay per wave, or direct launches when
 // profiling or when invisible entities make paths outlive max_depth
@@ -503,14 +532,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 	s.samples = total;
 	s.kernel_launches = launches;
 	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
-	s.extend_ms = s.secondary_ms = 0.f;
-	s.extend_launches = s.secondary_launches = 0;
-	for (uint32_t k = 0; c->profiling && k < c->next_event; k++) {
-		float ms = 0.f;
-		cudaEventElapsedTime(&ms, c->events[2 * k], c->events[2 * k + 1]);
-		if (c->event_kind[k] == 0) { s.extend_ms += ms; s.extend_launches++; }
-		else { s.secondary_ms += ms; s.secondary_launches++; }
-	}
+	traversal_times(c, nlanes, s);
 	return RB_OK;
 }
 
@@ -566,6 +588,7 @@ rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, im
 	s.samples = total;
 	s.kernel_launches = launches;
 	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
+	traversal_times(c, 1u, s);
 	return RB_OK;
 }
 

@@ -83,6 +83,39 @@ __device__ __forceinline__ void warp_add64(uint32_t* counters, uint32_t word, ui
 
 __device__ __forceinline__ void set_error(uint32_t* counters, uint32_t code) { atomicCAS(counters + CNT_ERROR, 0u, code); }
 
+// Device-clock time of a launch, measured inside it: every warp marks its
+// start and its end with %globaltimer, and the last warp to finish adds the
+// span from the earliest start to the latest end to the timer's total and
+// counts the launch. The timer's words (kernels.cuh) live in the counters of
+// the launching lane, so launches of one timer never overlap. Every warp of the
+// launch must call launch_timer_end exactly once, after all its work.
+__device__ __forceinline__ uint64_t global_time_ns() {
+	uint64_t t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+__device__ __forceinline__ unsigned long long* timer_u64(uint32_t* counters, uint32_t word) {
+	return reinterpret_cast<unsigned long long*>(counters + word);
+}
+__device__ __forceinline__ void launch_timer_begin(uint32_t* counters, uint32_t timer) {
+	if ((threadIdx.x & 31u) == 0) atomicMax(timer_u64(counters, timer + TIMER_START), ~global_time_ns());
+}
+__device__ __forceinline__ void launch_timer_end(uint32_t* counters, uint32_t timer) {
+	__syncwarp();
+	if ((threadIdx.x & 31u) != 0) return;
+	atomicMax(timer_u64(counters, timer + TIMER_END), global_time_ns());
+	__threadfence();
+	const uint32_t warps = gridDim.x * ((blockDim.x + 31u) / 32u);
+	if (atomicAdd(counters + timer + TIMER_WARPS, 1u) != warps - 1u) return;
+	// the last warp: every other warp's marks are in place
+	__threadfence();
+	const uint64_t start = ~atomicExch(timer_u64(counters, timer + TIMER_START), 0ull);
+	const uint64_t end = atomicExch(timer_u64(counters, timer + TIMER_END), 0ull);
+	atomicExch(counters + timer + TIMER_WARPS, 0u);
+	atomicAdd(timer_u64(counters, timer + TIMER_TOTAL_NS), static_cast<unsigned long long>(end > start ? end - start : 0ull));
+	atomicAdd(counters + timer + TIMER_LAUNCHES, 1u);
+}
+
 __device__ __forceinline__ hit_t to_hit(float4 h) {
 	hit_t r;
 	r.slot = static_cast<int32_t>(__float_as_uint(h.x));
@@ -676,6 +709,7 @@ template <bool COUNT, bool VOL, bool BATCH>
 __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
 	uint32_t sort) {
 	extern __shared__ uint32_t smem[];
+	launch_timer_begin(w.counters, CNT_TIMER_EXTEND);
 	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_ACTIVE];
 	const uint32_t* q = w.queue[queue_in];
@@ -709,6 +743,7 @@ __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, ui
 		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
 		warp_add64(w.counters, CNT_TRI_TESTS, tris);
 	}
+	launch_timer_end(w.counters, CNT_TIMER_EXTEND);
 }
 
 // ------------------------------------------------------------------ ray binning
@@ -829,6 +864,7 @@ template <bool VOL, bool BATCH>
 __global__ void __launch_bounds__(256) k_extend_refill(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
 	uint32_t sort) {
 	extern __shared__ uint32_t smem[];
+	launch_timer_begin(w.counters, CNT_TIMER_EXTEND);
 	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_ACTIVE];
 	const uint32_t* q = w.queue[queue_in];
@@ -887,11 +923,13 @@ __global__ void __launch_bounds__(256) k_extend_refill(scene_view s, wave_buffer
 		if (__any_sync(0xffffffffu, finished)) warp_push_keyed(key, i, w.class_queue, w.capacity, w.counters + CNT_CLASS);
 		if (fetch.exhausted && !__any_sync(0xffffffffu, active)) break;
 	}
+	launch_timer_end(w.counters, CNT_TIMER_EXTEND);
 }
 
 template <bool BATCH>
 __global__ void __launch_bounds__(256) k_secondary_refill(scene_view s, wave_buffers w, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
+	launch_timer_begin(w.counters, CNT_TIMER_SECONDARY);
 	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_SECONDARY];
 	ray_fetch fetch;
@@ -945,6 +983,7 @@ __global__ void __launch_bounds__(256) k_secondary_refill(scene_view s, wave_buf
 		}
 		if (fetch.exhausted && !__any_sync(0xffffffffu, active)) break;
 	}
+	launch_timer_end(w.counters, CNT_TIMER_SECONDARY);
 }
 
 template <uint32_t CLASS, bool VOL, bool BATCH>
@@ -1012,6 +1051,7 @@ __global__ void __launch_bounds__(256) k_shade_a(scene_view s_all, wave_buffers 
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap) {
 	extern __shared__ uint32_t smem[];
+	launch_timer_begin(w.counters, CNT_TIMER_SECONDARY);
 	smem_stack st = make_stack(smem, stack_cap);
 	const uint32_t n = w.counters[CNT_SECONDARY];
 	uint32_t nodes = 0, tris = 0;
@@ -1040,6 +1080,7 @@ __global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buff
 		warp_add64(w.counters, CNT_NODE_VISITS, nodes);
 		warp_add64(w.counters, CNT_TRI_TESTS, tris);
 	}
+	launch_timer_end(w.counters, CNT_TIMER_SECONDARY);
 }
 
 template <uint32_t CLASS, bool BATCH>

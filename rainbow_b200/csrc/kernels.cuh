@@ -32,8 +32,20 @@ enum : uint32_t {
 	CNT_FETCH_SECONDARY = 27,  // rays taken from the secondary queue by the persistent secondary kernel
 	CNT_DRAIN_WAVE = 28,    // drain-loop iterations of the current wave (below)
 	CNT_DRAIN_TOTAL = 29,   // drain-loop iterations of the render call
-	CNT_WORDS = 30
+	// device-clock timers of the traversal launches (launch_timer in kernels.cu),
+	// kTimerWords words each from these (even, so the 64-bit words are aligned)
+	CNT_TIMER_EXTEND = 30,
+	CNT_TIMER_SECONDARY = 40,
+	CNT_WORDS = 50
 };
+// launch timer layout, offsets from its first word: the complement of the
+// earliest warp start (64-bit, so that an atomic max keeps the minimum), the
+// latest warp end (64-bit), warps finished in the current launch, the total
+// nanoseconds of the finished launches (64-bit) and their count
+enum : uint32_t { TIMER_START = 0, TIMER_END = 2, TIMER_WARPS = 4, TIMER_TOTAL_NS = 6, TIMER_LAUNCHES = 8, kTimerWords = 10 };
+static_assert(CNT_TIMER_EXTEND % 2 == 0 && CNT_TIMER_SECONDARY % 2 == 0, "64-bit timer words must be aligned");
+static_assert(CNT_TIMER_EXTEND >= CNT_DRAIN_TOTAL + 1 && CNT_TIMER_SECONDARY >= CNT_TIMER_EXTEND + kTimerWords &&
+	CNT_WORDS >= CNT_TIMER_SECONDARY + kTimerWords, "counter words overlap");
 static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
 // words cleared at the start of a wave: everything before the 64-bit stats
 constexpr uint32_t kWaveCounterWords = CNT_EXTEND_RAYS;
