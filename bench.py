@@ -536,6 +536,30 @@ def main():
     value = world * args.steps * pixels / (max_ms / 1e3) / 1e6
     mrays = world * rays / (max_ms / 1e3) / 1e6
 
+    # ---- N > 1: the ranks' films (disjoint sample ranges) summed by one all-reduce over NCCL, then checked on
+    # rank 0 against a render of the union of the ranges on its own GPU (outside the timed region)
+    film_reduce = None
+    if world > 1:
+        from rainbow_b200.distributed import reduce_context_film
+        before = ctx.film()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        reduce_context_film(ctx, world * args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        reduced = ctx.film()
+        film_reduce = {"ms": e0.elapsed_time(e1), "bytes_per_rank": int(before[0].nbytes + before[1].nbytes + before[2].nbytes)}
+        if rank == 0:
+            for r in range(world):
+                ctx.render(scene.camera, spp=args.steps, first_sample=r * (args.steps + args.warmup + 8), max_depth=depth,
+                           reset=(r == 0), want_image=False)
+            union = ctx.film()
+            rel = float(np.max(np.abs(reduced[0] - union[0]) / np.maximum(np.abs(union[0]), 1e-300)))
+            film_reduce.update(counts_equal=bool(np.array_equal(reduced[2], union[2])), max_rel_diff_sums=rel,
+                               checked="reduced film vs one-GPU render of the union of the ranks' sample ranges")
+        barrier()
+
     # ---- the same steps as K separate 1-spp calls with L2 flushed before each (reported beside value)
     call_ms = 0.0
     for k in range(args.steps):
@@ -653,6 +677,7 @@ def main():
                                 "frac": achieved / l2_peak if achieved and l2_peak else None,
                                 "peak_source": "measured in this run: copy of 32 MiB into 32 MiB, both L2-resident"}},
             "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches, "tuning": tuning,
+            "film_reduce": film_reduce,
             **{k: v for k, v in extra.items()},
             "batched": batched, "guided": guided,
             "summary": summary_of(extra, batched, guided),

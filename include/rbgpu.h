@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 6
+#define RBGPU_ABI_VERSION 7
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -291,6 +291,21 @@ rb_status rb_render(rb_context* ctx, const rb_render_params* params, float* rgb_
  * of squared radiance (double, 3 per pixel) and the sample count per pixel.
  * Any output may be NULL. */
 rb_status rb_film_read(rb_context* ctx, double* sum_rgb, double* sum_sq_rgb, uint32_t* sample_count);
+
+/* The film accumulators (layout as rb_film_read) copied to, or replaced from,
+ * device memory the caller owns, enqueued on `stream` (a cudaStream_t, NULL: the
+ * context's stream). No counterpart in the reference, which renders on one
+ * machine. For renders over several GPUs: every rank's context renders its own
+ * range of sample indices of the same image, copies its film out, the ranks sum
+ * the buffers (an all-reduce, e.g. NCCL over NVLink), and each copies the sums
+ * back, after which its film holds the union of the ranges.
+ * rb_film_to_device returns once the copies are enqueued (after the context's
+ * own pending work); rb_film_from_device waits for its copies, needs the film
+ * of the same size to exist (a render made it) and records samples_per_pixel as
+ * the film's sample count. */
+rb_status rb_film_to_device(rb_context* ctx, double* d_sum_rgb, double* d_sum_sq_rgb, uint32_t* d_count, void* stream);
+rb_status rb_film_from_device(rb_context* ctx, const double* d_sum_rgb, const double* d_sum_sq_rgb, const uint32_t* d_count,
+	uint64_t samples_per_pixel, void* stream);
 
 /* Render without allocating: for callers that must not call cudaMalloc at
  * render time (code that runs inside a framework which owns the device memory

@@ -266,11 +266,12 @@ int orc_scene_objects(orc_scene* s, const void** world, const void** cam) {
 }
 
 // The camera's film as an integrator left it: pixel::spectrum() of every pixel
-// (film.cpp:11-21), W * H * 3 floats.
+// (film.cpp:19-24), W * H * 3 floats; 0 for a pixel nothing has written yet
+// (pixel::spectrum asserts a non-zero filter weight).
 int orc_film_read(orc_scene* s, float* rgb) {
 	const auto& pixels = (*s->film_ptr).*member_of(film_pixels_tag{});
 	for (size_t i = 0; i < pixels.size(); i++) {
-		const spectrum L = pixels[i].spectrum();
+		const spectrum L = pixels[i].filter_weight != 0 ? pixels[i].spectrum() : spectrum(0);
 		rgb[3 * i] = L[0]; rgb[3 * i + 1] = L[1]; rgb[3 * i + 2] = L[2];
 	}
 	return RB_OK;

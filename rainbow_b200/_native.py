@@ -173,6 +173,8 @@ SIGNATURES = {
     "rb_bvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),
     "rb_bvh_get": (C.c_int32, [C.c_void_p, C.POINTER(BvhDesc)]),
     "rb_bvh_depth": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "rb_film_to_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rb_film_from_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "rb_bvh_mesh_tree_count": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32)]),
     "rb_bvh_get_mesh_tree": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(BvhDesc)]),
     "rb_bvh_free": (None, [C.c_void_p]),

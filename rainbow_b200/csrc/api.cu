@@ -955,6 +955,34 @@ rb_status rb_film_read(rb_context* c, double* sum_rgb, double* sum_sq_rgb, uint3
 	return RB_OK;
 }
 
+rb_status rb_film_to_device(rb_context* c, double* d_sum, double* d_sum_sq, uint32_t* d_count, void* stream) {
+	if (c == nullptr || d_sum == nullptr || d_sum_sq == nullptr || d_count == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (c->film_w == 0) return RB_ERR_NO_SCENE;
+	RB_CUDA(cudaSetDevice(c->device));
+	const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+	if (s != c->stream) RB_CUDA(cudaStreamSynchronize(c->stream));  // the film's last writes are on the context's stream
+	const size_t px = static_cast<size_t>(c->film_w) * c->film_h;
+	RB_CUDA(cudaMemcpyAsync(d_sum, c->film.sum, 3 * px * sizeof(double), cudaMemcpyDeviceToDevice, s));
+	RB_CUDA(cudaMemcpyAsync(d_sum_sq, c->film.sum_sq, 3 * px * sizeof(double), cudaMemcpyDeviceToDevice, s));
+	RB_CUDA(cudaMemcpyAsync(d_count, c->film.count, px * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+	return RB_OK;
+}
+
+rb_status rb_film_from_device(rb_context* c, const double* d_sum, const double* d_sum_sq, const uint32_t* d_count,
+	uint64_t samples_per_pixel, void* stream) {
+	if (c == nullptr || d_sum == nullptr || d_sum_sq == nullptr || d_count == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (c->film_w == 0) return RB_ERR_NO_SCENE;
+	RB_CUDA(cudaSetDevice(c->device));
+	const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+	const size_t px = static_cast<size_t>(c->film_w) * c->film_h;
+	RB_CUDA(cudaMemcpyAsync(c->film.sum, d_sum, 3 * px * sizeof(double), cudaMemcpyDeviceToDevice, s));
+	RB_CUDA(cudaMemcpyAsync(c->film.sum_sq, d_sum_sq, 3 * px * sizeof(double), cudaMemcpyDeviceToDevice, s));
+	RB_CUDA(cudaMemcpyAsync(c->film.count, d_count, px * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+	RB_CUDA(cudaStreamSynchronize(s));  // later calls run on the context's stream
+	c->film_samples = samples_per_pixel;
+	return RB_OK;
+}
+
 rb_status rb_render_stats_get(rb_context* c, rb_render_stats* out) {
 	if (c == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
 	*out = c->stats;

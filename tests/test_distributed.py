@@ -1,7 +1,8 @@
 """Multi-rank path: each rank renders its own range of sample indices of the
 same image (weak scaling, no collective on the data path) and one all-reduce
-sums the film. Run as two gloo ranks on the CPU, each rank rendering with the
-C restatement; the reduced film must equal a single-process render of the
+sums the film (rainbow_b200.distributed, the code bench.py --gpus N runs over
+NCCL). Run here as two gloo ranks on the CPU, each rank rendering with the C
+restatement; the reduced film must equal a single-process render of the
 union of the sample ranges."""
 import os
 import socket
@@ -13,13 +14,9 @@ import torch.multiprocessing as mp
 
 import rainbow_b200 as rb
 from oracle import port
+from rainbow_b200.distributed import reduce_film_tensors, sample_range
 
 SPP_PER_RANK = 4
-
-
-def sample_range(rank: int, spp: int) -> tuple:
-    """First sample index and count of a rank (the scheme bench.py uses)."""
-    return rank * spp, spp
 
 
 def _worker(rank, world, port_no, out):
@@ -30,10 +27,11 @@ def _worker(rank, world, port_no, out):
     sb = scene.with_bvh(rb.build_bvh(scene))
     first, n = sample_range(rank, SPP_PER_RANK)
     s, q, _ = port.render(sb, scene.camera, n, first, 5, 1.0, seed=0, threads=1)
-    t = torch.from_numpy(np.concatenate([s.ravel(), q.ravel()]))
-    dist.all_reduce(t)
+    ts, tq = torch.from_numpy(s.ravel().copy()), torch.from_numpy(q.ravel().copy())
+    tc = torch.full((16 * 16,), n, dtype=torch.int32)
+    reduce_film_tensors(ts, tq, tc)
     if rank == 0:
-        out.put(t.numpy())
+        out.put((np.concatenate([ts.numpy(), tq.numpy()]), tc.numpy()))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -47,12 +45,11 @@ def _free_port():
 def test_two_rank_sample_ranges_reduce_to_single_render():
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, 2, _free_port() if r < 0 else None, q)) for r in range(0)]
     port_no = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, 2, port_no, q)) for r in range(2)]
     for p in procs:
         p.start()
-    reduced = q.get(timeout=120)
+    reduced, counts = q.get(timeout=120)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -61,6 +58,7 @@ def test_two_rank_sample_ranges_reduce_to_single_render():
     s, sq, _ = port.render(sb, scene.camera, 2 * SPP_PER_RANK, 0, 5, 1.0, seed=0, threads=2)
     want = np.concatenate([s.ravel(), sq.ravel()])
     np.testing.assert_allclose(reduced, want, rtol=1e-12, atol=1e-12)
+    assert (counts == 2 * SPP_PER_RANK).all()
 
 
 def test_sample_ranges_are_disjoint_and_cover():
