@@ -70,7 +70,8 @@ typedef struct rb_mesh_desc {
 } rb_mesh_desc;
 
 enum {
-	RB_MATERIAL_MATTE = 0,  /* rainbow-cpu/materials/matte_material.cpp:13-29 (Lambert when sigma == 0) */
+	RB_MATERIAL_MATTE = 0,  /* rainbow-cpu/materials/matte_material.cpp:13-29 (Lambert when sigma == 0, else
+	                           Oren-Nayar, scatterings/reflection/oren_nayar_reflection.cpp) */
 	RB_MATERIAL_METAL = 1,  /* rainbow-cpu/materials/metal_material.cpp:17-37 */
 	RB_MATERIAL_GLASS = 2,  /* rainbow-cpu/materials/glass_material.cpp:25-64 */
 	RB_MATERIAL_PLASTIC = 3, /* rainbow-cpu/materials/plastic_material.cpp:9-55: diffuse = Kd (Lambert lobe),
@@ -90,7 +91,7 @@ typedef struct rb_material_desc {
 	uint32_t kind;
 	int32_t remap_roughness;    /* metal/glass: apply trowbridge_reitz_distribution::roughness_to_alpha */
 	float diffuse[3];           /* matte */
-	float sigma;                /* matte Oren-Nayar sigma; only 0 (Lambert) is supported */
+	float sigma;                /* matte: Oren-Nayar sigma in degrees, clamped to [0, 90]; 0 gives Lambert */
 	float eta[3];               /* metal: conductor eta (RGB) */
 	float k[3];                 /* metal: conductor absorption k (RGB) */
 	float reflectance[3];       /* glass */

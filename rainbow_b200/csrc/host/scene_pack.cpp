@@ -94,8 +94,15 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			case RB_MATERIAL_MATTE: {
 				const float sigma = fclamp_ref(md.sigma, 0.f, 90.f);
 				if (black3(md.diffuse)) r.kind = pt::MAT_BLACK;
-				else if (sigma != 0.f) return RB_ERR_UNSUPPORTED;  // Oren-Nayar is outside the supported subset
-				else r.kind = pt::MAT_LAMBERT;
+				else if (sigma != 0.f) {
+					// oren_nayar_reflection's constructor (oren_nayar_reflection.cpp:5-16):
+					// radians in float, then A and B in double, rounded to float
+					r.kind = pt::MAT_OREN_NAYAR;
+					const float sr = sigma * 0.01745329251994329576923690768489f;
+					const float s2 = sr * sr;
+					r.alpha_x = static_cast<float>(1. - (s2 / (2 * (s2 + 0.33))));
+					r.alpha_y = static_cast<float>(0.45 * s2 / (s2 + 0.09));
+				} else r.kind = pt::MAT_LAMBERT;
 				r.diffuse = vec3{md.diffuse[0], md.diffuse[1], md.diffuse[2]};
 				break;
 			}

@@ -202,7 +202,7 @@ RB_HD lobe_sample no_sample() { return lobe_sample{0u, spectrum{0.f, 0.f, 0.f}, 
 
 // Lobe kinds in collection order for each material.
 enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, LOBE_FRESNEL_SPECULAR = 3,
-	LOBE_SPECULAR_REFLECT = 4, LOBE_FRESNEL_BLEND = 5 };
+	LOBE_SPECULAR_REFLECT = 4, LOBE_FRESNEL_BLEND = 5, LOBE_OREN_NAYAR = 6 };
 
 struct bsdf_t {
 	uint32_t kinds[2];
@@ -224,6 +224,9 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 	switch (m->kind) {
 	case MAT_LAMBERT:
 		b.kinds[0] = LOBE_LAMBERT; b.types[0] = ST_DIFFUSE | ST_REFLECTION; b.count = 1;
+		break;
+	case MAT_OREN_NAYAR:
+		b.kinds[0] = LOBE_OREN_NAYAR; b.types[0] = ST_DIFFUSE | ST_REFLECTION; b.count = 1;
 		break;
 	case MAT_METAL:
 		b.kinds[0] = LOBE_MF_REFLECT; b.types[0] = ST_GLOSSY | ST_REFLECTION; b.count = 1;
@@ -338,6 +341,29 @@ RB_HD float fresnel_blend_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	return 0.5f * (pd + ph);
 }
 
+// oren_nayar_reflection::evaluate (scatterings/reflection/oren_nayar_reflection.cpp:18-47):
+// R / pi * (A + B max(0, cos(phi_i - phi_o)) sin(alpha) tan(beta)), with A and B
+// (the material's alpha_x / alpha_y) computed on the host from sigma. The
+// 1e-4 threshold is a double literal in the reference, so the test is in double.
+RB_HD spectrum oren_nayar_f(const material_rec* m, vec3 wo, vec3 wi) {
+	const float sin_theta_i = sin_theta(wi), sin_theta_o = sin_theta(wo);
+	float max_cos = 0.f;
+	if (static_cast<double>(sin_theta_i) > 1e-4 && static_cast<double>(sin_theta_o) > 1e-4) {
+		const float sin_phi_i = sin_phi(wi), sin_phi_o = sin_phi(wo);
+		const float cos_phi_i = cos_phi(wi), cos_phi_o = cos_phi(wo);
+		max_cos = fmax_ref(0.f, cos_phi_i * cos_phi_o + sin_phi_i * sin_phi_o);
+	}
+	float sin_alpha, tan_beta;
+	if (fabs_ref(wi.z) > fabs_ref(wo.z)) {
+		sin_alpha = sin_theta_o;
+		tan_beta = sin_theta_i / fabs_ref(wi.z);
+	} else {
+		sin_alpha = sin_theta_i;
+		tan_beta = sin_theta_o / fabs_ref(wo.z);
+	}
+	return m->diffuse * kInvPi * (m->alpha_x + m->alpha_y * max_cos * sin_alpha * tan_beta);
+}
+
 template <int MAT>
 RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return b.m->diffuse * kInvPi;
@@ -347,6 +373,7 @@ RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	else {
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
+		case LOBE_OREN_NAYAR: return oren_nayar_f(b.m, wo, wi);
 		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi);
 		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
 		case LOBE_FRESNEL_BLEND: return fresnel_blend_f(b.m, wo, wi);
@@ -362,7 +389,8 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_pdf(b.m, wo, wi) : mf_transmit_pdf(b.m, wo, wi);
 	else {
 		switch (lobe_kind(b, i)) {
-		case LOBE_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
+		case LOBE_LAMBERT:
+		case LOBE_OREN_NAYAR: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
 		case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
 		case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
 		case LOBE_FRESNEL_BLEND: return fresnel_blend_pdf(b.m, wo, wi);
@@ -447,7 +475,8 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 		return lobe_kind(b, i) == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u) : sample_mf_transmit(b, i, wo, u);
 	else {
 		switch (lobe_kind(b, i)) {
-		case LOBE_LAMBERT: return sample_lambert<MAT_ANY>(b, i, wo, u);
+		case LOBE_LAMBERT:
+		case LOBE_OREN_NAYAR: return sample_lambert<MAT_ANY>(b, i, wo, u);  // reflection_function::sample, cosine
 		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u);
 		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u);
 		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(b, wo, u);

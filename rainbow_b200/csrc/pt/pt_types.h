@@ -116,11 +116,12 @@ struct mesh_rec {
 };
 
 enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4, MAT_PLASTIC = 5,
-	MAT_MIRROR = 6, MAT_SUBSTRATE = 7 };
+	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8 };
 
 struct material_rec {
 	uint32_t kind;
-	float alpha_x, alpha_y;   // Trowbridge-Reitz alphas (roughness_to_alpha applied on the host)
+	float alpha_x, alpha_y;   // Trowbridge-Reitz alphas (roughness_to_alpha applied on the host);
+	                          // Oren-Nayar (matte with sigma != 0): its A and B
 	float eta;                // glass / plastic IOR
 	spectrum diffuse;         // lambert reflectance (matte, plastic Kd)
 	spectrum reflectance;     // glass reflectance, plastic Ks, mirror reflectance

@@ -24,6 +24,9 @@ product's seeded scene generator:
   materials_samples  radiance of 1024 pairs, path_integrator::trace depth 8, on the spheres
                  scene with plastic and mirror materials (tests.helpers.extra_materials_scene)
   bsdf_plastic_*, bsdf_mirror_*, bsdf_substrate_*  the BSDF tables of those materials
+  oren_nayar_samples  radiance of 1024 pairs, path_integrator::trace depth 8, on the spheres
+                 scene with Oren-Nayar matte (tests.helpers.oren_nayar_scene)
+  bsdf_oren_nayar_*  the BSDF tables of a matte material with sigma 20 (--only oren_nayar)
 
 The benchmark configurations themselves (--only baseline):
   config1_image  configuration 1 as specified (box room, 256 x 256, depth 5):
@@ -50,7 +53,7 @@ The reference's two-level tree (--only two_level):
                  intersect_with_shadow_ray hits, and the radiance of 512 (pixel,
                  sample) pairs, path_integrator, depth 5
 
-Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level]
+Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level|oren_nayar]
 """
 from __future__ import annotations
 
@@ -223,6 +226,18 @@ def direct_fixtures():
              bsdf_samples=np.array(B))
 
 
+def oren_nayar_fixtures():
+    from tests.helpers import oren_nayar_scene
+    R = ref.RefScene(oren_nayar_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(37)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("oren_nayar_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8),
+         first_entity=first_entity(R, px, sm))
+    bsdf_fixtures({"oren_nayar": dict(kind=rb.RB_MATERIAL_MATTE, diffuse=(0.7, 0.4, 0.2), sigma=20.0)})
+
+
 def materials_fixtures():
     from tests.helpers import extra_materials_scene
     R = ref.RefScene(extra_materials_scene(scene_of(SPHERES)))
@@ -265,6 +280,8 @@ def main():
         return baseline_fixtures()
     if only == "two_level":
         return two_level_fixtures()
+    if only == "oren_nayar":
+        return oren_nayar_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -312,6 +329,7 @@ def main():
     materials_fixtures()
     baseline_fixtures()
     two_level_fixtures()
+    oren_nayar_fixtures()
 
 
 def material_desc(m):
@@ -319,7 +337,7 @@ def material_desc(m):
     md.kind = m["kind"]
     if m["kind"] == rb.RB_MATERIAL_MATTE:
         md.diffuse[:] = m["diffuse"]
-        md.sigma = 0.0
+        md.sigma = m.get("sigma", 0.0)
     elif m["kind"] == rb.RB_MATERIAL_PLASTIC:
         md.remap_roughness = 1
         md.diffuse[:] = (0.6, 0.3, 0.2)

@@ -6,6 +6,8 @@ in the reference `film` through film::set_pixel (film.cpp:197-205). The film
 must hold what rb_render computes for the same samples, and lie within 3 sigma
 of path_integrator::render as shipped (the reference's own per-tile sampler
 streams) on the same scene."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -44,21 +46,22 @@ def test_adapter_film_within_three_sigma_of_shipped_path_integrator():
 
 def test_adapter_two_level_scene_and_refusal():
     """The two-level scene renders through the adapter. A scene the core does
-    not render (a matte material with an Oren-Nayar sigma) makes render() throw
-    with the C ABI's reason and leaves the film as it was."""
+    not render (no emitter: uniform_sample_one_emitter needs one) makes render()
+    throw with the C ABI's reason and leaves the film as it was."""
     from tests.helpers import two_level_scene
     scene = two_level_scene(32, 24)
     R = ref.RefScene(scene)
     film = ref.adapter_render(R, 4, max_depth=5)
     assert np.isfinite(film).all() and film.mean() > 0
-    mats = []
-    for k in range(scene.desc.num_materials):
-        m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
-        if m.kind == rb.RB_MATERIAL_MATTE:
-            m.sigma = 20.0
-        mats.append(m)
-    R2 = ref.RefScene(scene.with_materials(mats))
+    dark = rb.SceneDesc.from_buffer_copy(bytes(scene.desc))
+    ents = (rb._native.EntityDesc * dark.num_entities)()
+    for k in range(dark.num_entities):
+        ents[k] = scene.desc.entities[k]
+        ents[k].emitter = -1
+    dark.entities = ctypes.cast(ents, ctypes.POINTER(rb._native.EntityDesc))
+    dark.num_emitters = 0
+    R2 = ref.RefScene(rb.Scene(None, dark, scene.camera, keepalive=[scene, ents]))
     before = R2.film()
-    with pytest.raises(RuntimeError, match="not supported"):
+    with pytest.raises(RuntimeError, match="invalid argument"):
         ref.adapter_render(R2, 4)
     np.testing.assert_array_equal(R2.film(), before)

@@ -42,8 +42,8 @@ def test_config1_as_specified_within_three_sigma():
     n_ref, depth = int(fx["spp"]), int(fx["max_depth"])
     ref_mean, ref_var = fx["mean"].astype(np.float64), fx["var"].astype(np.float64)
     # the configuration's own frame: 16 spp, compared on 4 x 4 pixel blocks
-    mean, _ = _render_mean_var(scene, 16, depth, seed=1)
-    z = block_z(mean, ref_mean, ref_var, 16, n_ref)
+    mean, var = _render_mean_var(scene, 16, depth, seed=1)
+    z = block_z(mean, ref_mean, ref_var, 16, n_ref, var=var)
     assert (np.abs(z) > 3).mean() < 0.01, f"{(np.abs(z) > 3).mean():.4f} of 16-spp block channels outside 3 sigma"
     assert abs(z.mean()) < 0.1, z.mean()
     # and per pixel at 256 spp
@@ -96,10 +96,11 @@ def test_large_config_images_within_three_sigma(name, volume):
     scene = scene_from_params(fx["params"])
     n_ref, depth = int(fx["spp"]), int(fx["max_depth"])
     n = 4096
-    mean, _ = _render_mean_var(scene, n, depth, seed=3, volume=volume)
+    mean, var = _render_mean_var(scene, n, depth, seed=3, volume=volume)
     # heavy-tailed paths (the slit, scattering in the fog) leave per-pixel
-    # variance estimates low, so the check is on 4 x 4 blocks plus the mean
-    z = block_z(mean, fx["mean"].astype(np.float64), fx["var"].astype(np.float64), n, n_ref)
+    # variance estimates low, so the check is on 4 x 4 blocks, with each
+    # render's own variance, plus the mean z
+    z = block_z(mean, fx["mean"].astype(np.float64), fx["var"].astype(np.float64), n, n_ref, var=var)
     assert (np.abs(z) > 3).mean() < 0.02, f"{name}: {(np.abs(z) > 3).mean():.4f} of block channels outside 3 sigma"
     assert abs(z.mean()) < 0.15, z.mean()
 

@@ -7,8 +7,8 @@ import pytest
 
 import rainbow_b200 as rb
 from tests import golden
-from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, per_sample_radiance,
-                           scene_from_params)
+from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, oren_nayar_scene,
+                           per_sample_radiance, scene_from_params)
 
 pytestmark = pytest.mark.gpu
 
@@ -32,6 +32,18 @@ def test_extra_materials_samples_match_reference():
     agree = _agreement(got, want)
     assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
     assert_disagreements_unbiased(scene, got, want, fx["first_entity"], "materials")
+
+
+def test_oren_nayar_samples_match_reference():
+    fx = golden.load("oren_nayar_samples")
+    scene = oren_nayar_scene(scene_from_params(fx["params"]))
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        got = per_sample_radiance(ctx, scene, fx["pixels"], fx["samples"], int(fx["max_depth"]))
+        assert ctx.stats().device_error == 0
+    agree = _agreement(got, fx["radiance"])
+    assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
+    assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], "oren-nayar")
 
 
 def test_extra_materials_direct_matches_host_build():

@@ -80,7 +80,8 @@ def test_reference_samples_match_fixture(name):
 
 
 @needs_ref
-@pytest.mark.parametrize("mat", ["lambert", "metal", "glass_rough", "glass_smooth", "plastic", "mirror", "substrate"])
+@pytest.mark.parametrize("mat", ["lambert", "metal", "glass_rough", "glass_smooth", "plastic", "mirror", "substrate",
+                                 "oren_nayar"])
 @pytest.mark.parametrize("inc", ["all", "nonspec"])
 def test_reference_bsdf_matches_fixture(mat, inc):
     fx = golden.load(f"bsdf_{mat}_{inc}")
