@@ -381,6 +381,14 @@ enum {
 	                               (coherent traversal warps) */
 };
 enum {
+	RB_SHADOW_CLOSEST = 0,       /* NEE shadow rays find their closest visible hit, as scene::intersect_with_shadow_ray */
+	RB_SHADOW_FIRST_OCCLUDER = 1 /* NEE shadow rays of plain path tracing: the sampled emitter's own triangles first,
+	                                then the traversal stops at the first visible hit closer than the emitter's (the
+	                                reference's accept rule, integrator.cpp:131-136, needs no more); the same
+	                                visibility except where an occluder and the emitter are hit at distances equal
+	                                to float rounding */
+};
+enum {
 	RB_TRAVERSAL_PER_THREAD = 0, /* one ray per thread, traced to the end (grid-stride) */
 	RB_TRAVERSAL_REFILL = 1      /* persistent lanes advance their ray one node at a time and take the next ray
 	                                from the queue as soon as theirs is done */
@@ -404,7 +412,8 @@ typedef struct rb_tuning {
 	uint32_t smem_carveout;     /* traversal kernels' shared-memory share of the L1 / shared storage, in
 	                               percent + 1 (1..101); 0: the largest share (4 blocks of 256 threads with
 	                               their stacks); smaller shares leave more L1 for tree nodes */
-	uint32_t reserved[3];
+	uint32_t shadow_test;       /* RB_SHADOW_* */
+	uint32_t reserved[2];
 } rb_tuning;
 /* Use `tuning` (NULL: defaults) for the context's later render calls. */
 rb_status rb_set_tuning(rb_context* ctx, const rb_tuning* tuning);

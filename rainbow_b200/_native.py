@@ -38,6 +38,7 @@ RB_BVH_LEAF_FLAG = 0x80000000
 RB_BVH_ALL_TRIANGLES = 0xFFFFFFFF
 RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS = 0, 1, 2
 RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL = 0, 1
+RB_SHADOW_CLOSEST, RB_SHADOW_FIRST_OCCLUDER = 0, 1
 
 F16 = C.c_float * 16
 F3 = C.c_float * 3
@@ -102,11 +103,11 @@ class Tuning(C.Structure):
     _fields_ = [("paths_per_wave", C.c_uint32), ("block_trace", C.c_uint32), ("block_shade", C.c_uint32),
                 ("grid_per_sm", C.c_uint32), ("sort", C.c_uint32), ("tail_bounce", C.c_uint32),
                 ("lanes", C.c_uint32), ("traversal", C.c_uint32), ("smem_carveout", C.c_uint32),
-                ("reserved", C.c_uint32 * 3)]
+                ("shadow_test", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k in ("paths_per_wave", "block_trace", "block_shade", "grid_per_sm", "sort",
-                                              "tail_bounce", "lanes", "traversal", "smem_carveout")}
+                                              "tail_bounce", "lanes", "traversal", "smem_carveout", "shadow_test")}
 
 
 class BatchView(C.Structure):

@@ -209,6 +209,7 @@ rb_status capture_into(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s
 	key.sort = cfg.sort;
 	key.tail = cfg.tail;
 	key.refill = cfg.refill;
+	key.shadow_first = cfg.shadow_first;
 	key.carveout = cfg.carveout;
 	if (cfg.guide) {
 		key.guide_steps = cfg.guide->cfg.steps_per_wave;

@@ -89,13 +89,14 @@ struct graph_key {
 	bool with_end = true;  // the graph ends with the film resolve (one lane) or stops after the bounces
 	uint32_t block_trace = 0, block_shade = 0, grid_trace = 0, grid_shade = 0, sort = 0, tail = 0;
 	bool refill = false;
+	bool shadow_first = false;
 	int carveout = 0;
 	bool operator==(const graph_key& o) const {
 		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
 			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch &&
 			volume == o.volume && batch == o.batch && block_trace == o.block_trace && block_shade == o.block_shade &&
 			grid_trace == o.grid_trace && grid_shade == o.grid_shade && sort == o.sort && tail == o.tail &&
-			with_end == o.with_end && refill == o.refill && carveout == o.carveout;
+			with_end == o.with_end && refill == o.refill && carveout == o.carveout && shadow_first == o.shadow_first;
 	}
 };
 
@@ -115,7 +116,7 @@ inline bool valid_tuning(const rb_tuning& t) {
 	auto block_ok = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 256 && b % 32 == 0); };
 	return block_ok(t.block_trace) && block_ok(t.block_shade) && t.grid_per_sm <= 64 && t.sort <= RB_SORT_RAYS &&
 		t.paths_per_wave <= (1u << 24) && t.tail_bounce <= 64 && t.lanes <= kMaxLanes && t.traversal <= RB_TRAVERSAL_REFILL &&
-		t.smem_carveout <= 101;
+		t.smem_carveout <= 101 && t.shadow_test <= RB_SHADOW_FIRST_OCCLUDER;
 }
 
 // Path state of one wave: the buffers of wave_buffers for `n` paths.
@@ -239,6 +240,7 @@ struct rb_context {
 		c.sort = t.sort;
 		c.tail = t.tail_bounce;
 		c.refill = t.traversal == RB_TRAVERSAL_REFILL;
+		c.shadow_first = t.shadow_test == RB_SHADOW_FIRST_OCCLUDER;
 		c.carveout = t.smem_carveout == 0 ? 100 : static_cast<int>(t.smem_carveout) - 1;
 		c.batch = is_batch;
 		// the reference-order traversal holds at most depth + 2 entries; the

@@ -124,14 +124,17 @@ __device__ __forceinline__ hit_t to_hit(float4 h) {
 	return r;
 }
 
+// first: an occlusion query (any hit accepted at len will do) on the 4-wide
+// path; its reference-order fallback finds the closest hit, which answers the
+// same question.
 template <bool SHADOW, bool COUNT>
 __device__ __forceinline__ bool trace_one(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h, smem_stack& st,
-	uint32_t& nodes, uint32_t& tris) {
+	uint32_t& nodes, uint32_t& tris, bool first = false) {
 	trace_counters c{0u, 0u};
 	bool ok;
 	if (!COUNT && s.wnodes != nullptr && !isnan(len)) {
 		const float len0 = len;
-		const int r = closest_hit_fast<SHADOW>(s, o, d, len, h, st);
+		const int r = closest_hit_fast<SHADOW>(s, o, d, len, h, st, first);
 		ok = r == 1;
 		if (r < 0) {  // a NaN length or a full stack: redo the ray in the reference's own visiting order
 			len = len0;
@@ -1048,8 +1051,19 @@ __global__ void __launch_bounds__(256) k_shade_a(scene_view s_all, wave_buffers 
 	}
 }
 
+// Secondary rays: 2 i is path i's NEE shadow ray, 2 i + 1 its MIS ray (closest
+// visible hits). shadow_first (plain path-tracing bounces only): the shadow ray
+// is answered as an occlusion query. The reference accepts it when its closest
+// visible hit is the sampled emitter or nothing (integrator.cpp:131-136), that
+// is, when no other visible hit lies closer than the emitter's own closest hit;
+// so the emitter's triangles are tested first, the ray is cut at that hit, and
+// the traversal stops at the first occluder found before it (shade_b needs only
+// whether the hit slot is the emitter, nothing or something else). Emitters of
+// more than kShadowFirstTris triangles keep the closest-hit query.
+constexpr uint32_t kShadowFirstTris = 64;
 template <bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap) {
+__global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap,
+	uint32_t shadow_first) {
 	extern __shared__ uint32_t smem[];
 	launch_timer_begin(w.counters, CNT_TIMER_SECONDARY);
 	smem_stack st = make_stack(smem, stack_cap);
@@ -1063,12 +1077,18 @@ __global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buff
 			float len = o.w;
 			hit_t h;
 			bool ok;
-			if (BATCH) {
-				const scene_view sv = batch_view(s, w.batch[w.scene[j >> 1]]);
-				ok = trace_one<true, COUNT>(sv, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
-			} else {
-				ok = trace_one<true, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+			const scene_view sv = BATCH ? batch_view(s, w.batch[w.scene[j >> 1]]) : s;
+			const vec3 o3{o.x, o.y, o.z}, d3{d.x, d.y, d.z};
+			bool first = false;
+			if (!COUNT && shadow_first && !(j & 1u)) {
+				const int32_t e = w.rec[j >> 1].nee_entity;
+				float cut;
+				if (e >= 0 && entity_closest_length(sv, static_cast<uint32_t>(e), o3, d3, len, kShadowFirstTris, cut)) {
+					len = cut;
+					first = true;
+				}
 			}
+			ok = trace_one<true, COUNT>(sv, o3, d3, len, h, st, nodes, tris, first);
 			if (!ok) {
 				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
 				h.slot = -1;
@@ -1611,7 +1631,7 @@ cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t q
 		if (e != cudaSuccess) return e;
 	}
 	if (refill) k_secondary_refill<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
-	else k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	else k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth, 0u);
 	k_vol_direct<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_beam<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_continue<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -1671,7 +1691,8 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	}
 	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
 	if (refill) k_secondary_refill<BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
-	else k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
+	else k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth,
+		cfg.shadow_first ? 1u : 0u);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
 	if (cfg.sort != RB_SORT_NONE) {
 		k_shade_b<CLASS_LAMBERT, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -1808,8 +1829,8 @@ cudaError_t launch_direct_staged_wave(const scene_view& s, const wave_buffers& w
 	k_direct_lights<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	k_direct_lights<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	for (uint32_t r = 0; r < dc.bsdf_samples && e == cudaSuccess; r++) {
-		if (cfg.count) k_trace_secondary<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth);
-		else k_trace_secondary<false, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth);
+		if (cfg.count) k_trace_secondary<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth, 0u);
+		else k_trace_secondary<false, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth, 0u);
 		e = cudaMemsetAsync(w.counters + CNT_SECONDARY, 0, sizeof(uint32_t), stream);
 		if (e != cudaSuccess) break;
 		k_direct_round<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);

@@ -180,6 +180,7 @@ struct launch_cfg {
 	uint32_t sort = 0;       // hit queues: 0 one per material class, 1 a single queue (no sorting)
 	uint32_t tail = 0xffffffffu;  // bounces of separate stages before the tail kernel (>= max_depth: none)
 	bool refill = false;     // traversal kernels: persistent lanes that take a new ray when theirs is done
+	bool shadow_first = false;  // NEE shadow rays of plain path tracing as occlusion queries (k_trace_secondary)
 	int carveout = 100;      // traversal kernels' preferred shared-memory carve-out, percent
 };
 

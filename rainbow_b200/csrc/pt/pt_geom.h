@@ -131,7 +131,7 @@ RB_HD uint32_t float_as_u32(float f) {
 // leaves them as it found them. Returns false when the stack overflowed.
 template <bool COUNT, typename Stack>
 RB_HD bool instance_hit(const scene_view& s, uint32_t slot, uint32_t ent, vec3 o, vec3 d, float& len, hit_t& hit,
-	Stack& stack, trace_counters& cnt) {
+	Stack& stack, trace_counters& cnt, bool occlusion = false) {
 	const float4 ia = RB_LDG(s.tri_a + slot);
 	const uint32_t root = float_as_u32(ia.x), first = float_as_u32(ia.y);
 	const local_ray lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
@@ -165,6 +165,10 @@ RB_HD bool instance_hit(const scene_view& s, uint32_t slot, uint32_t ent, vec3 o
 					hit.b1 = b1;
 					hit.b2 = b2;
 					any = true;
+					if (occlusion) {  // any hit will do: leave the caller's entries as they were
+						while (stack.size() > base) stack.pop();
+						break;
+					}
 				}
 			}
 			continue;
@@ -297,12 +301,14 @@ struct trav_state {
 	uint32_t cur;        // next node or leaf to visit
 	uint32_t cur_entity;
 	local_ray lr;
+	bool first;          // stop at the first accepted hit (occlusion only)
 };
 
 // Starts a ray: the root box test of the reference. Returns false when the ray
 // is already done (the root box is missed).
 template <typename Stack>
-RB_HD bool trav_begin(const scene_view& s, trav_state& t, vec3 o, vec3 d, float len, Stack& stack) {
+RB_HD bool trav_begin(const scene_view& s, trav_state& t, vec3 o, vec3 d, float len, Stack& stack, bool first = false) {
+	t.first = first;
 	t.o = o;
 	t.d = d;
 	t.inv = 1.f / d;
@@ -335,8 +341,9 @@ RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 			const uint32_t ent = ew & kEntityMask;
 			if (ew & kEntityInstance) {
 				trace_counters none{0u, 0u};
-				if (!instance_hit<false>(s, slot, ent, t.o, t.d, t.len, t.hit, stack, none)) return -1;
+				if (!instance_hit<false>(s, slot, ent, t.o, t.d, t.len, t.hit, stack, none, t.first)) return -1;
 				if (isnan(t.len)) return -1;
+				if (t.first && t.hit.slot >= 0) return 1;
 				continue;
 			}
 			const float4 ta = RB_LDG(s.tri_a + slot);
@@ -353,6 +360,7 @@ RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 				t.hit.b1 = b1;
 				t.hit.b2 = b2;
 				if (isnan(t.len)) return -1;
+				if (t.first) return 1;
 			}
 		}
 	} else {
@@ -408,17 +416,46 @@ RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 	return 1;
 }
 
+// first: stop at the first hit accepted at the ray's length (an occlusion
+// query), instead of the closest.
 template <bool SHADOW, typename Stack>
-RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack) {
+RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack, bool first = false) {
 	trav_state t;
 	int r = 1;
-	if (trav_begin(s, t, o, d, len, stack)) {
+	if (trav_begin(s, t, o, d, len, stack, first)) {
 		do r = trav_step<SHADOW>(s, t, stack);
 		while (r == 0);
 	}
 	len = t.len;
 	hit = t.hit;
 	return r;
+}
+
+// World length of the closest hit of ray (o, d) on entity ent's own triangles
+// within len (len when none), with the arithmetic entity::intersect uses; false
+// when the entity has more than max_tris triangles (then it is not worth it).
+RB_HD bool entity_closest_length(const scene_view& s, uint32_t ent, vec3 o, vec3 d, float len, uint32_t max_tris,
+	float& out) {
+	const entity_rec& e = s.entities[ent];
+	if (e.mesh < 0) return false;
+	const mesh_rec& m = s.meshes[e.mesh];
+	if (m.num_triangles > max_tris) return false;
+	const local_ray lr = make_local_ray(e.w2l, e.l2w, o, d);
+	float llen = len * lr.to_local;
+	bool any = false;
+	for (uint32_t k = 0; k < m.num_triangles; k++) {
+		const uint32_t* idx = s.indices + m.index_offset + 3 * k;
+		const float* p = s.positions;
+		const uint32_t i0 = 3 * (m.vertex_offset + idx[0]), i1 = 3 * (m.vertex_offset + idx[1]), i2 = 3 * (m.vertex_offset + idx[2]);
+		const vec3 p0{p[i0], p[i0 + 1], p[i0 + 2]}, p1{p[i1], p[i1 + 1], p[i1 + 2]}, p2{p[i2], p[i2 + 1], p[i2 + 2]};
+		float t, b1, b2;
+		if (triangle_hit(lr.o, lr.d, llen, p0, p1 - p0, p2 - p0, t, b1, b2)) {
+			llen = t;
+			any = true;
+		}
+	}
+	out = any ? llen * lr.to_world : len;
+	return true;
 }
 
 // ------------------------------------------------------------------ surface interaction

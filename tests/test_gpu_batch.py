@@ -87,7 +87,9 @@ def test_batch_accumulates_and_refuses_single_scene_calls():
                                     dict(lanes=4, paths_per_wave=20000), dict(traversal=rb.RB_TRAVERSAL_PER_THREAD),
                                     dict(traversal=rb.RB_TRAVERSAL_REFILL, block_trace=64, grid_per_sm=1),
                                     dict(smem_carveout=26, block_trace=256), dict(sort=rb.RB_SORT_RAYS),
-                                    dict(sort=rb.RB_SORT_RAYS, lanes=2, paths_per_wave=6000, tail_bounce=4)])
+                                    dict(sort=rb.RB_SORT_RAYS, lanes=2, paths_per_wave=6000, tail_bounce=4),
+                                    dict(shadow_test=rb.RB_SHADOW_FIRST_OCCLUDER),
+                                    dict(shadow_test=rb.RB_SHADOW_FIRST_OCCLUDER, lanes=2, paths_per_wave=6000)])
 def test_launch_shapes_do_not_change_the_image(tuning):
     sc = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=96, height=64, num_spheres=30, subdivision=3)
     with rb.Context(0) as ctx:
