@@ -577,7 +577,10 @@ def main():
     if not args.tuning and not args.no_tune:
         t1, _ = ctx.tune_render(scene.camera, probe_spp=1, max_depth=depth, seed=base + 999)
         e2e_tuning = t1.as_dict()
-    img = torch.zeros((H, W, 3), dtype=torch.float32, pin_memory=True)  # page-locked host output
+    # every step: one rb_render_async call (its parameters in by kernel argument), the step's image out to its
+    # own page-locked buffer (a ring of 4, as a double-buffering viewer would keep them); the calls overlap on the
+    # GPU and rb_render_wait ends the run
+    imgs = [torch.zeros((H, W, 3), dtype=torch.float32, pin_memory=True) for _ in range(min(4, args.steps))]
     barrier()
     t0 = time.perf_counter()
     for k in range(args.steps):
@@ -585,7 +588,9 @@ def main():
         p.camera = scene.camera
         p.spp, p.first_sample, p.max_depth, p.rr_threshold, p.seed = 1, base + k, depth, 1.0, 0
         p.flags = rb.RB_RENDER_RESET if k == 0 else 0
-        rb.check(rb.lib().rb_render(ctx._h, ctypes.byref(p), ctypes.c_void_p(img.data_ptr())), "rb_render")
+        rb.check(rb.lib().rb_render_async(ctx._h, ctypes.byref(p), ctypes.c_void_p(imgs[k % len(imgs)].data_ptr())),
+                 "rb_render_async")
+    rb.check(rb.lib().rb_render_wait(ctx._h), "rb_render_wait")
     barrier()
     e2e_s = time.perf_counter() - t0
     tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -664,7 +669,8 @@ def main():
             "timing": "K steps = one rb_render call of K samples per pixel, CUDA events on the library's stream",
             "mrays_per_s": mrays, "per_call_1spp": per_call,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "calls": "one rb_render per step (1 spp, image read back each call)", "tuning": e2e_tuning},
+                    "calls": "one rb_render_async per step (1 spp, the step's image read back to page-locked memory), "
+                             "rb_render_wait after the last", "tuning": e2e_tuning},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": "k_extend + k_trace_secondary (BVH traversal), launches of the timed call",

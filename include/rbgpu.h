@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 7
+#define RBGPU_ABI_VERSION 8
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -287,6 +287,22 @@ typedef struct rb_render_params {
  * of the call's samples, while later waves still run; if the call then fails,
  * part of rgb_out may already be written. */
 rb_status rb_render(rb_context* ctx, const rb_render_params* params, float* rgb_out);
+
+/* rb_render without waiting: returns once the call's work is enqueued, so that
+ * consecutive calls overlap on the GPU (the late bounces of one call with the
+ * first waves of the next, on the wave lanes) while the film still adds their
+ * samples in call order. No counterpart in the reference, whose render() is
+ * synchronous. Plain path tracing only: flags other than RB_RENDER_RESET return
+ * RB_ERR_UNSUPPORTED. rgb_out, if not NULL, must be page-locked; its slices are
+ * written as the call's pixels complete, and it must not be read or reused
+ * before rb_render_wait. A call whose camera, spp, max_depth, rr_threshold or
+ * paths_per_wave differs from the pending calls', or that sets RB_RENDER_RESET,
+ * first waits for them; so does every other entry point on the context.
+ * rb_render_wait returns once every pending call has finished, with the first
+ * device error of any of them; rb_render_stats_get then covers all of them
+ * (samples, rays, elapsed time from the first call's start). */
+rb_status rb_render_async(rb_context* ctx, const rb_render_params* params, float* rgb_out);
+rb_status rb_render_wait(rb_context* ctx);
 
 /* Read back the accumulators: per-pixel sums of radiance (double, 3 per pixel),
  * of squared radiance (double, 3 per pixel) and the sample count per pixel.

@@ -208,6 +208,23 @@ class Context:
         check(lib().rb_render(self._h, C.byref(p), img.ctypes.data if want_image else None), "rb_render")
         return img
 
+    def render_async(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5,
+                     threshold: float = 1.0, seed: int = 0, reset: bool = False, paths_per_wave: int = 0,
+                     out_ptr: int = 0) -> None:
+        """rb_render_async: plain path tracing enqueued without waiting (calls overlap on the GPU; the film
+        adds them in order). out_ptr: address of page-locked float32 (height, width, 3) memory for the image,
+        or 0; it is complete at render_wait."""
+        p = RenderParams()
+        p.camera = camera
+        p.spp, p.first_sample, p.max_depth, p.rr_threshold = spp, first_sample, max_depth, threshold
+        p.seed, p.flags, p.paths_per_wave = seed, RB_RENDER_RESET if reset else 0, paths_per_wave
+        self._film_shape = (camera.width, camera.height)
+        check(lib().rb_render_async(self._h, C.byref(p), C.c_void_p(out_ptr) if out_ptr else None), "rb_render_async")
+
+    def render_wait(self) -> None:
+        """rb_render_wait: every pending render_async call has finished (first device error raised)."""
+        check(lib().rb_render_wait(self._h), "rb_render_wait")
+
     def film(self):
         """(sum, sum_sq, count) FP64 accumulators of every pixel."""
         s = lib()

@@ -174,6 +174,8 @@ SIGNATURES = {
     "rb_bvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.POINTER(C.c_void_p)]),
     "rb_bvh_get": (C.c_int32, [C.c_void_p, C.POINTER(BvhDesc)]),
     "rb_bvh_depth": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "rb_render_async": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p]),
+    "rb_render_wait": (C.c_int32, [C.c_void_p]),
     "rb_film_to_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rb_film_from_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "rb_bvh_mesh_tree_count": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32)]),

@@ -381,10 +381,52 @@ rb_status readback_after(rb_context* c, image_readback* r, uint64_t resolved_ite
 	return RB_OK;
 }
 
-rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves, image_readback* readback) {
+// The statistics of the waves that ran since the counters were last cleared:
+// lane 0's counters, with the other lanes' statistics and first error added.
+void take_stats(rb_context* c, uint32_t nlanes, uint64_t samples, uint32_t launches, bool use_graph,
+	const gpu::launch_cfg& cfg) {
+	uint32_t* h = c->counters_host;
+	auto u64 = [&](const uint32_t* a, uint32_t w) { return static_cast<uint64_t>(a[w]) | (static_cast<uint64_t>(a[w + 1]) << 32); };
+	rb_render_stats& s = c->stats;
+	s = rb_render_stats{};
+	for (uint32_t k = 0; k < nlanes; k++) {
+		const uint32_t* a = h + k * gpu::CNT_WORDS;
+		s.extend_rays += u64(a, gpu::CNT_EXTEND_RAYS);
+		s.shadow_rays += u64(a, gpu::CNT_SHADOW_RAYS);
+		s.mis_rays += u64(a, gpu::CNT_MIS_RAYS);
+		s.node_visits += u64(a, gpu::CNT_NODE_VISITS);
+		s.triangle_tests += u64(a, gpu::CNT_TRI_TESTS);
+		if (s.device_error == 0) s.device_error = a[gpu::CNT_ERROR];
+		if (use_graph) launches += a[gpu::CNT_DRAIN_TOTAL] * gpu::drain_launches(cfg);
+	}
+	h[gpu::CNT_ERROR] = s.device_error;
+	s.samples = samples;
+	s.kernel_launches = launches;
+	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
+	traversal_times(c, nlanes, s);
+}
+
+rb_status async_finish(rb_context* c) {
+	if (c->async.pending == 0) return RB_OK;
+	const uint32_t nlanes = c->async.lanes;
+	for (uint32_t k = 0; k + 1 < nlanes; k++) RB_CUDA(cudaStreamWaitEvent(c->stream, c->lanes[k].done, 0));
+	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
+	const cudaError_t e = cudaStreamSynchronize(c->stream);
+	const rb_context::async_state a = c->async;
+	c->async = rb_context::async_state{};
+	RB_CUDA(e);
+	take_stats(c, nlanes, a.samples, a.launches, a.use_graph, c->profiled_cfg());
+	return c->counters_host[gpu::CNT_ERROR] != 0 ? static_cast<rb_status>(c->counters_host[gpu::CNT_ERROR]) : RB_OK;
+}
+
+rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves, image_readback* readback,
+	bool async) {
 	gpu::wave_params& hp = *c->params_host;
 	rb_status st = RB_OK;
 	const gpu::launch_cfg cfg = c->profiled_cfg();
+	// a later async call of the same configuration: no clearing, no start
+	// barrier across the lanes; its counters add to the pending calls'
+	const bool continuing = async && c->async.pending > 0;
 	const uint32_t nlanes = lanes_for(c, total, cfg);
 	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
 	if (record_waves || nlanes > 1) {
@@ -394,7 +436,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			c->wave_events.push_back(e);
 		}
 	}
-	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
+	if (!continuing) RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
 	// scenes with invisible entities replay graphs too (their drain loop is a
 	// conditional node) unless the runtime refused that node
 	const bool use_graph = !c->profiling && !(c->has_invisible && c->drain_graph_failed);
@@ -433,29 +475,31 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			st = capture_into(c, l.wave, l.stream, l.counters, max_depth, false, l.graph, l.key);
 		}
 		if (st != RB_OK && c->has_invisible && c->drain_graph_failed)
-			return run_waves(c, total, max_depth, record_waves, readback);
+			return run_waves(c, total, max_depth, record_waves, readback, async);
 		if (st != RB_OK) return st;
 	} else if (use_graph) {
 		st = capture_wave(c, max_depth);
 		if (st != RB_OK && c->has_invisible && c->drain_graph_failed)
-			return run_waves(c, total, max_depth, record_waves, readback);
+			return run_waves(c, total, max_depth, record_waves, readback, async);
 		if (st != RB_OK) return st;
 	}
 	uint32_t launches = 0;
 	hp.first_item = 0;
-	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(gpu::launch_set_params(hp, c->wave.params, c->stream));
 	for (uint32_t k = 0; guided && k < nlanes; k++) {
 		RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[k], c->stream));
 		if (cfg.guide_medium != nullptr)
 			RB_CUDA(guide::launch_snapshot(*cfg.guide_medium, c->lane_guides_medium[k], c->stream));
 	}
-	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
+	if (!continuing) RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
 	if (nlanes > 1) {
 		for (uint32_t k = 0; k + 1 < nlanes; k++) {
 			wave_lane& l = c->lanes[k];
-			RB_CUDA(cudaStreamWaitEvent(l.stream, c->ev_begin, 0));
-			RB_CUDA(cudaMemsetAsync(l.counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), l.stream));
-			RB_CUDA(cudaMemcpyAsync(l.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, l.stream));
+			if (!continuing) {
+				RB_CUDA(cudaStreamWaitEvent(l.stream, c->ev_begin, 0));
+				RB_CUDA(cudaMemsetAsync(l.counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), l.stream));
+			}
+			RB_CUDA(gpu::launch_set_params(hp, l.params, l.stream));
 		}
 		for (uint64_t j = 0; j < waves; j++) {
 			const uint32_t lane = static_cast<uint32_t>(j % nlanes);
@@ -465,6 +509,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			RB_CUDA(gpu::launch_set_first(w.params, j * c->wave_capacity, s));
 			RB_CUDA(cudaGraphLaunch(g, s));
 			if (j > 0) RB_CUDA(cudaStreamWaitEvent(s, c->wave_events[j - 1], 0));
+			else if (continuing) RB_CUDA(cudaStreamWaitEvent(s, c->wave_events[c->async.waves - 1], 0));  // the previous call's last wave
 			// in wave order: training-sample collection, film resolve, training, then this lane's snapshot
 			RB_CUDA(gpu::launch_wave_end(w, c->film, c->num_sms * 4, cfg, s));
 			if (training) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[lane], s));
@@ -480,7 +525,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			RB_CUDA(cudaMemcpyAsync(c->counters_host + (k + 1) * gpu::CNT_WORDS, l.counters, gpu::CNT_WORDS * sizeof(uint32_t),
 				cudaMemcpyDeviceToHost, l.stream));
 			RB_CUDA(cudaEventRecord(l.done, l.stream));
-			RB_CUDA(cudaStreamWaitEvent(c->stream, l.done, 0));
+			if (!async) RB_CUDA(cudaStreamWaitEvent(c->stream, l.done, 0));
 		}
 	} else {
 		uint64_t wave = 0;
@@ -511,29 +556,22 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			if (st != RB_OK) return st;
 		}
 	}
+	if (async) {
+		// lane 0's counters follow its last wave; the host reads them at rb_render_wait
+		RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+			c->stream));
+		c->async.pending++;
+		c->async.waves = waves;
+		c->async.lanes = nlanes;
+		c->async.samples += total;
+		c->async.launches += launches;
+		c->async.use_graph = use_graph;
+		return RB_OK;
+	}
 	RB_CUDA(cudaEventRecord(c->ev_end, c->stream));
 	RB_CUDA(cudaMemcpyAsync(c->counters_host, c->counters, gpu::CNT_WORDS * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
-	// lane 0's counters, with the other lanes' statistics and first error added
-	uint32_t* h = c->counters_host;
-	auto u64 = [&](const uint32_t* a, uint32_t w) { return static_cast<uint64_t>(a[w]) | (static_cast<uint64_t>(a[w + 1]) << 32); };
-	rb_render_stats& s = c->stats;
-	s = rb_render_stats{};
-	for (uint32_t k = 0; k < nlanes; k++) {
-		const uint32_t* a = h + k * gpu::CNT_WORDS;
-		s.extend_rays += u64(a, gpu::CNT_EXTEND_RAYS);
-		s.shadow_rays += u64(a, gpu::CNT_SHADOW_RAYS);
-		s.mis_rays += u64(a, gpu::CNT_MIS_RAYS);
-		s.node_visits += u64(a, gpu::CNT_NODE_VISITS);
-		s.triangle_tests += u64(a, gpu::CNT_TRI_TESTS);
-		if (s.device_error == 0) s.device_error = a[gpu::CNT_ERROR];
-		if (use_graph) launches += a[gpu::CNT_DRAIN_TOTAL] * gpu::drain_launches(cfg);
-	}
-	h[gpu::CNT_ERROR] = s.device_error;
-	s.samples = total;
-	s.kernel_launches = launches;
-	cudaEventElapsedTime(&s.elapsed_ms, c->ev_begin, c->ev_end);
-	traversal_times(c, nlanes, s);
+	take_stats(c, nlanes, total, launches, use_graph, cfg);
 	return RB_OK;
 }
 
@@ -561,7 +599,7 @@ rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, im
 	}
 	RB_CUDA(cudaMemsetAsync(c->counters, 0, gpu::CNT_WORDS * sizeof(uint32_t), c->stream));
 	hp.first_item = 0;
-	RB_CUDA(cudaMemcpyAsync(c->wave.params, &hp, sizeof(hp), cudaMemcpyHostToDevice, c->stream));
+	RB_CUDA(gpu::launch_set_params(hp, c->wave.params, c->stream));
 	RB_CUDA(cudaEventRecord(c->ev_begin, c->stream));
 	uint32_t launches = 0;
 	for (uint64_t first = 0; first < total; first += c->wave_capacity) {
@@ -596,6 +634,8 @@ rb_status run_direct(rb_context* c, uint64_t total, const pt::direct_cfg& dc, im
 // Replaces the context's scene (or batch) with the packed arrays of `p`.
 rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
 	if (p.bvh_depth + 3 > 64) return RB_ERR_UNSUPPORTED;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	RB_CUDA(cudaSetDevice(c->device));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
 	c->release_graph();
@@ -666,6 +706,7 @@ namespace gpu {
 bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStream_t* stream, int* device,
 	uint32_t** counters_host, bool* has_invisible) {
 	if (c == nullptr || !c->has_scene || c->is_batch) return false;
+	if (async_finish(c) != RB_OK) return false;
 	*view = c->view;
 	*cfg = c->cfg();
 	cfg->count = false;
@@ -684,6 +725,7 @@ bool context_view(rb_context* c, pt::scene_view* view, launch_cfg* cfg, cudaStre
 // rb_guide_* entry points (guide_api.cu).
 guide::guide_state* context_guide(rb_context* c, cudaStream_t* stream, int* device, int* num_sms) {
 	if (c == nullptr) return nullptr;
+	async_finish(c);  // the guide entry points use the context's stream and buffers
 	*stream = c->stream;
 	*device = c->device;
 	*num_sms = c->num_sms;
@@ -758,6 +800,7 @@ rb_status rb_context_create(rb_context** out, int device) {
 rb_status rb_context_destroy(rb_context* c) {
 	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
 	cudaSetDevice(c->device);
+	async_finish(c);
 	if (c->stream) cudaStreamSynchronize(c->stream);
 	c->release_graph();
 	c->release_lanes();
@@ -784,6 +827,8 @@ rb_status rb_context_destroy(rb_context* c) {
 
 rb_status rb_scene_upload(rb_context* c, const rb_scene_desc* desc) {
 	if (c == nullptr || desc == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	host::packed_scene p;
 	const rb_status st = host::pack_scene(desc, p);
 	if (st != RB_OK) return st;
@@ -841,6 +886,8 @@ rb_status rb_trace_shadow_device(rb_context* c, const rb_ray* d_rays, uint32_t n
 
 rb_status rb_set_counting(rb_context* c, int enabled) {
 	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	if (c->counting != (enabled != 0)) c->release_graph();
 	c->counting = enabled != 0;
 	return RB_OK;
@@ -848,6 +895,8 @@ rb_status rb_set_counting(rb_context* c, int enabled) {
 
 rb_status rb_set_profiling(rb_context* c, int enabled) {
 	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	c->profiling = enabled != 0;
 	if (c->profiling && c->events.empty()) {
 		RB_CUDA(cudaSetDevice(c->device));
@@ -858,8 +907,56 @@ rb_status rb_set_profiling(rb_context* c, int enabled) {
 	return RB_OK;
 }
 
+static rb_status render_call(rb_context* c, const rb_render_params* prm, float* rgb_out, bool async);
+
 rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) {
 	if (c == nullptr || prm == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
+	return render_call(c, prm, rgb_out, false);
+}
+
+rb_status rb_render_async(rb_context* c, const rb_render_params* prm, float* rgb_out) {
+	if (c == nullptr || prm == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	if (prm->flags & ~static_cast<uint32_t>(RB_RENDER_RESET)) return RB_ERR_UNSUPPORTED;  // plain path tracing only
+	if (rgb_out != nullptr && !is_page_locked(rgb_out)) return RB_ERR_INVALID_ARGUMENT;
+	// what later calls must share with the pending ones to continue them
+	struct signature {
+		rb_camera_desc camera;
+		uint32_t spp, max_depth, paths_per_wave;
+		float rr_threshold;
+		rb_tuning tuning;
+		uint32_t counting, profiling;
+	} sig;
+	std::memset(&sig, 0, sizeof(sig));
+	sig.camera = prm->camera;
+	sig.spp = prm->spp;
+	sig.max_depth = prm->max_depth;
+	sig.paths_per_wave = prm->paths_per_wave;
+	sig.rr_threshold = prm->rr_threshold;
+	sig.tuning = c->tuning;
+	sig.counting = c->counting;
+	sig.profiling = c->profiling;
+	static_assert(sizeof(signature) <= sizeof(c->async.signature), "async signature too large");
+	const bool same = c->async.signature_size == sizeof(sig) && std::memcmp(c->async.signature, &sig, sizeof(sig)) == 0;
+	if (c->async.pending > 0 && (!same || (prm->flags & RB_RENDER_RESET) || c->profiling)) {
+		const rb_status st = async_finish(c);
+		if (st != RB_OK) return st;
+	}
+	std::memcpy(c->async.signature, &sig, sizeof(sig));
+	c->async.signature_size = sizeof(sig);
+	const rb_status st = render_call(c, prm, rgb_out, !c->profiling);
+	if (st != RB_OK) c->async = rb_context::async_state{};  // (the failed call was synchronised or never enqueued)
+	return st;
+}
+
+rb_status rb_render_wait(rb_context* c) {
+	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	RB_CUDA(cudaSetDevice(c->device));
+	return async_finish(c);
+}
+
+static rb_status render_call(rb_context* c, const rb_render_params* prm, float* rgb_out, bool async) {
 	if (!c->has_scene) return RB_ERR_NO_SCENE;
 	if (c->is_batch) return RB_ERR_INVALID_ARGUMENT;
 	const rb_camera_desc& cam = prm->camera;
@@ -925,10 +1022,11 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 		overlap.final_from = total - pixels;
 	}
 	st = direct ? run_direct(c, total, pt::make_direct_cfg(direct_emitter, direct_bsdf), overlapped ? &overlap : nullptr)
-		: run_waves(c, total, prm->max_depth, false, overlapped ? &overlap : nullptr);
+		: run_waves(c, total, prm->max_depth, false, overlapped ? &overlap : nullptr, async);
 	if (st != RB_OK) return st;
-	const uint32_t* h = c->counters_host;
 	c->film_samples += prm->spp;
+	if (async) return RB_OK;  // the page-locked image arrives slice by slice; rb_render_wait ends the calls
+	const uint32_t* h = c->counters_host;
 	if (h[gpu::CNT_ERROR] != 0) return static_cast<rb_status>(h[gpu::CNT_ERROR]);
 
 	if (rgb_out != nullptr && !(overlapped && overlap.done == pixels)) {
@@ -946,6 +1044,8 @@ rb_status rb_render(rb_context* c, const rb_render_params* prm, float* rgb_out) 
 
 rb_status rb_film_read(rb_context* c, double* sum_rgb, double* sum_sq_rgb, uint32_t* count) {
 	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	if (c->film_w == 0) return RB_ERR_NO_SCENE;
 	RB_CUDA(cudaSetDevice(c->device));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
@@ -958,6 +1058,8 @@ rb_status rb_film_read(rb_context* c, double* sum_rgb, double* sum_sq_rgb, uint3
 
 rb_status rb_film_to_device(rb_context* c, double* d_sum, double* d_sum_sq, uint32_t* d_count, void* stream) {
 	if (c == nullptr || d_sum == nullptr || d_sum_sq == nullptr || d_count == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	if (c->film_w == 0) return RB_ERR_NO_SCENE;
 	RB_CUDA(cudaSetDevice(c->device));
 	const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
@@ -972,6 +1074,8 @@ rb_status rb_film_to_device(rb_context* c, double* d_sum, double* d_sum_sq, uint
 rb_status rb_film_from_device(rb_context* c, const double* d_sum, const double* d_sum_sq, const uint32_t* d_count,
 	uint64_t samples_per_pixel, void* stream) {
 	if (c == nullptr || d_sum == nullptr || d_sum_sq == nullptr || d_count == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	if (c->film_w == 0) return RB_ERR_NO_SCENE;
 	RB_CUDA(cudaSetDevice(c->device));
 	const cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
@@ -986,6 +1090,8 @@ rb_status rb_film_from_device(rb_context* c, const double* d_sum, const double* 
 
 rb_status rb_render_stats_get(rb_context* c, rb_render_stats* out) {
 	if (c == nullptr || out == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	*out = c->stats;
 	return RB_OK;
 }
@@ -1014,6 +1120,8 @@ rb_status rb_checkpoint_save(rb_context* c, const char* path) {
 
 rb_status rb_checkpoint_load(rb_context* c, const char* path) {
 	if (c == nullptr || path == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);
+	if (pending != RB_OK) return pending;
 	FILE* f = std::fopen(path, "rb");
 	if (f == nullptr) return RB_ERR_IO;
 	uint32_t head[4];

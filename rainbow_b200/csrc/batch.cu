@@ -226,6 +226,8 @@ extern "C" {
 
 rb_status rb_set_tuning(rb_context* c, const rb_tuning* t) {
 	if (c == nullptr) return RB_ERR_INVALID_ARGUMENT;
+	const rb_status pending = async_finish(c);  // its graphs may be released below
+	if (pending != RB_OK) return pending;
 	rb_tuning v{};
 	if (t != nullptr) v = *t;
 	if (!valid_tuning(v)) return RB_ERR_INVALID_ARGUMENT;

@@ -229,6 +229,20 @@ struct rb_context {
 	uint32_t direct_alloc = 0;       // paths the direct buffers hold
 	int32_t* vol_medium = nullptr;   // per-path medium buffer (wave.medium points here in volume renders)
 	uint32_t vol_alloc = 0;          // paths the volume buffers hold
+	// rb_render_async calls enqueued since the last wait: their count, the
+	// configuration they share, the waves and lanes of each (the first wave of
+	// the next call waits for the last of the previous one), and the samples and
+	// launches to report at rb_render_wait
+	struct async_state {
+		uint32_t pending = 0;
+		uint64_t waves = 0;
+		uint32_t lanes = 0;
+		uint64_t samples = 0;
+		uint32_t launches = 0;
+		unsigned char signature[512];
+		size_t signature_size = 0;
+		bool use_graph = true;
+	} async;
 
 	gpu::launch_cfg cfg() const {
 		gpu::launch_cfg c;
@@ -333,8 +347,13 @@ struct image_readback {
 	uint64_t final_from = 0;   // first item of the call's last sample
 	uint64_t done = 0;         // pixels already copied (or enqueued)
 };
+// async: an rb_render_async call, which returns once its work is enqueued and
+// continues the film order of the pending async calls (statistics are taken at
+// rb_render_wait by async_finish).
 rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool record_waves,
-	image_readback* readback = nullptr);
+	image_readback* readback = nullptr, bool async = false);
+// Waits for the pending rb_render_async calls and takes their statistics.
+rb_status async_finish(rb_context* c);
 // Replaces the context's scene arrays with a packed scene (single or merged).
 rb_status upload_packed(rb_context* c, const host::packed_scene& p);
 

@@ -1661,6 +1661,10 @@ __global__ void k_next_wave(wave_params* p, uint32_t capacity) { p->first_item +
 // The first work item of the next wave of a lane (several lanes take turns).
 __global__ void k_set_first(wave_params* p, uint64_t first) { p->first_item = first; }
 
+// Writes a lane's parameter block from a kernel argument, so that no host
+// buffer has to outlive the enqueued call.
+__global__ void k_set_params(wave_params p, wave_params* dst) { *dst = p; }
+
 template <bool COUNT, bool BATCH>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
@@ -1841,6 +1845,11 @@ cudaError_t launch_direct_staged_wave(const scene_view& s, const wave_buffers& w
 	if (e == cudaSuccess) e = cudaGetLastError();
 	if (e == cudaSuccess) e = launch_next_wave(w, f, resolve_grid, stream);
 	return e;
+}
+
+cudaError_t launch_set_params(const wave_params& p, wave_params* dst, cudaStream_t stream) {
+	k_set_params<<<1, 1, 0, stream>>>(p, dst);
+	return cudaGetLastError();
 }
 
 cudaError_t launch_set_first(wave_params* params, uint64_t first, cudaStream_t stream) {

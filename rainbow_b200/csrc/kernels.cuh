@@ -197,6 +197,9 @@ cudaError_t launch_wave(const pt::scene_view& s, const wave_buffers& w, const fi
 // params->first_item by the wave capacity (the last nodes of a wave).
 cudaError_t launch_next_wave(const wave_buffers& w, const film_buffers& f, int grid, cudaStream_t stream);
 
+// Writes the parameter block `dst` from `p` (passed by value at launch time).
+cudaError_t launch_set_params(const wave_params& p, wave_params* dst, cudaStream_t stream);
+
 // Sets params->first_item (the wave window of a lane).
 cudaError_t launch_set_first(wave_params* params, uint64_t first, cudaStream_t stream);
 
