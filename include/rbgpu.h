@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 8
+#define RBGPU_ABI_VERSION 9
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -80,10 +80,22 @@ enum {
 	                            isotropic roughness */
 	RB_MATERIAL_MIRROR = 4,  /* rainbow-cpu/materials/mirror_material.cpp:9-26: reflectance (specular
 	                            reflection, no Fresnel term) */
-	RB_MATERIAL_SUBSTRATE = 5 /* rainbow-cpu/materials/substrate_material.cpp: the Fresnel-blend
+	RB_MATERIAL_SUBSTRATE = 5, /* rainbow-cpu/materials/substrate_material.cpp: the Fresnel-blend
 	                            layer (scatterings/reflection/fresnel_blend_reflection.cpp) of
 	                            reflectance = specular Rs over diffuse = Rd, Trowbridge-Reitz
 	                            roughness_u / roughness_v */
+	RB_MATERIAL_UBER = 6,    /* rainbow-cpu/materials/uber_material.cpp:26-75: with O = opacity, the lobes
+	                            specular transmission of clamp(1 - O) (eta 1 / 1), Lambert of O diffuse,
+	                            Trowbridge-Reitz reflection of O specular (dielectric Fresnel of ior,
+	                            roughness_u / roughness_v), specular reflection of O reflectance
+	                            (dielectric Fresnel of ior) and specular transmission of
+	                            O transmission (eta 1 / ior), each if not black */
+	RB_MATERIAL_TRANSLUCENT = 7 /* rainbow-cpu/materials/translucent_material.cpp:23-69: IOR 1.5; no lobes
+	                            when reflectance and transmission are both black; else Lambert
+	                            reflection of diffuse reflectance and Lambert transmission of diffuse
+	                            transmission (if diffuse is not black), Trowbridge-Reitz reflection of
+	                            specular reflectance and transmission of specular transmission (if
+	                            specular is not black), isotropic roughness_u */
 };
 
 /* Constant-texture material parameters (constant_texture_t, textures/detail/constant_texture.hpp:25-35). */
@@ -94,11 +106,13 @@ typedef struct rb_material_desc {
 	float sigma;                /* matte: Oren-Nayar sigma in degrees, clamped to [0, 90]; 0 gives Lambert */
 	float eta[3];               /* metal: conductor eta (RGB) */
 	float k[3];                 /* metal: conductor absorption k (RGB) */
-	float reflectance[3];       /* glass */
-	float transmission[3];      /* glass */
-	float ior;                  /* glass */
+	float reflectance[3];       /* glass, plastic, mirror, substrate, uber, translucent */
+	float transmission[3];      /* glass, uber, translucent */
+	float ior;                  /* glass, plastic, uber */
 	float roughness_u;          /* metal, glass (glass with both zero -> fresnel_specular) */
 	float roughness_v;
+	float specular[3];          /* uber, translucent: the glossy reflection's spectrum */
+	float opacity[3];           /* uber */
 } rb_material_desc;
 
 enum {

@@ -32,6 +32,8 @@
 #include "rainbow-cpu/materials/mirror_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
 #include "rainbow-cpu/materials/substrate_material.hpp"
+#include "rainbow-cpu/materials/translucent_material.hpp"
+#include "rainbow-cpu/materials/uber_material.hpp"
 #include "rainbow-cpu/emitters/surface_light.hpp"
 #include "rainbow-cpu/emitters/environment_light.hpp"
 #include "rainbow-cpu/textures/constant_texture.hpp"
@@ -141,6 +143,13 @@ std::shared_ptr<material> make_material(const rb_material_desc& m) {
 	case RB_MATERIAL_SUBSTRATE:
 		return std::make_shared<substrate_material>(spectrum_texture(m.reflectance), spectrum_texture(m.diffuse),
 			real_texture(m.roughness_u), real_texture(m.roughness_v), m.remap_roughness != 0);
+	case RB_MATERIAL_UBER:
+		return std::make_shared<uber_material>(spectrum_texture(m.transmission), spectrum_texture(m.reflectance),
+			spectrum_texture(m.specular), spectrum_texture(m.diffuse), spectrum_texture(m.opacity),
+			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
+	case RB_MATERIAL_TRANSLUCENT:
+		return std::make_shared<translucent_material>(spectrum_texture(m.transmission), spectrum_texture(m.reflectance),
+			spectrum_texture(m.specular), spectrum_texture(m.diffuse), real_texture(m.roughness_u), m.remap_roughness != 0);
 	default: return nullptr;
 	}
 }

@@ -23,6 +23,7 @@ import numpy as np
 from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_BVH_ALL_TRIANGLES, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_MIRROR, RB_MATERIAL_PLASTIC, RB_MATERIAL_SUBSTRATE,
+    RB_MATERIAL_TRANSLUCENT, RB_MATERIAL_UBER,
     RB_RENDER_GUIDE,
     RB_RENDER_DIRECT, RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
     RB_SHADOW_CLOSEST, RB_SHADOW_FIRST_OCCLUDER, RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,
@@ -41,13 +42,14 @@ class Scene:
 
     def __init__(self, handle, desc: SceneDesc, camera: CameraDesc, keepalive=()):
         self._handle = handle
+        self._free = lib().rb_scene_free  # held so that teardown at interpreter exit still frees
         self.desc = desc
         self.camera = camera
         self._keepalive = list(keepalive)
 
     def __del__(self):
         if getattr(self, "_handle", None):
-            lib().rb_scene_free(self._handle)
+            self._free(self._handle)
             self._handle = None
 
     @property

@@ -23,6 +23,8 @@ STATUS_NAMES = {
 
 RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS, RB_MATERIAL_PLASTIC, RB_MATERIAL_MIRROR = 0, 1, 2, 3, 4
 RB_MATERIAL_SUBSTRATE = 5
+RB_MATERIAL_UBER = 6
+RB_MATERIAL_TRANSLUCENT = 7
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
 RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM, RB_SCENE_FOG = 0, 1, 2, 3
 RB_RENDER_RESET = 1
@@ -54,7 +56,7 @@ class MeshDesc(C.Structure):
 class MaterialDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("remap_roughness", C.c_int32), ("diffuse", F3), ("sigma", C.c_float),
                 ("eta", F3), ("k", F3), ("reflectance", F3), ("transmission", F3), ("ior", C.c_float),
-                ("roughness_u", C.c_float), ("roughness_v", C.c_float)]
+                ("roughness_u", C.c_float), ("roughness_v", C.c_float), ("specular", F3), ("opacity", F3)]
 
 
 class MediumDesc(C.Structure):

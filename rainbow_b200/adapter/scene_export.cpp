@@ -20,6 +20,8 @@
 #include "rainbow-cpu/materials/mirror_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
 #include "rainbow-cpu/materials/substrate_material.hpp"
+#include "rainbow-cpu/materials/translucent_material.hpp"
+#include "rainbow-cpu/materials/uber_material.hpp"
 #include "rainbow-cpu/media/homogeneous_medium.hpp"
 #include "rainbow-cpu/shapes/mesh.hpp"
 #include "rainbow-cpu/textures/constant_texture.hpp"
@@ -70,6 +72,21 @@ RB_PRIVATE_MEMBER(substrate_diffuse, materials::substrate_material::mDiffuse);
 RB_PRIVATE_MEMBER(substrate_ru, materials::substrate_material::mRoughnessU);
 RB_PRIVATE_MEMBER(substrate_rv, materials::substrate_material::mRoughnessV);
 RB_PRIVATE_MEMBER(substrate_remap, materials::substrate_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(uber_transmission, materials::uber_material::mTransmission);
+RB_PRIVATE_MEMBER(uber_reflectance, materials::uber_material::mReflectance);
+RB_PRIVATE_MEMBER(uber_specular, materials::uber_material::mSpecular);
+RB_PRIVATE_MEMBER(uber_diffuse, materials::uber_material::mDiffuse);
+RB_PRIVATE_MEMBER(uber_opacity, materials::uber_material::mOpacity);
+RB_PRIVATE_MEMBER(uber_ru, materials::uber_material::mRoughnessU);
+RB_PRIVATE_MEMBER(uber_rv, materials::uber_material::mRoughnessV);
+RB_PRIVATE_MEMBER(uber_eta, materials::uber_material::mEta);
+RB_PRIVATE_MEMBER(uber_remap, materials::uber_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(translucent_transmission, materials::translucent_material::mTransmission);
+RB_PRIVATE_MEMBER(translucent_reflectance, materials::translucent_material::mReflectance);
+RB_PRIVATE_MEMBER(translucent_specular, materials::translucent_material::mSpecular);
+RB_PRIVATE_MEMBER(translucent_diffuse, materials::translucent_material::mDiffuse);
+RB_PRIVATE_MEMBER(translucent_roughness, materials::translucent_material::mRoughness);
+RB_PRIVATE_MEMBER(translucent_remap, materials::translucent_material::mMapRoughnessToAlpha);
 RB_PRIVATE_MEMBER(surface_radiance, emitters::surface_light::mRadiance);
 RB_PRIVATE_MEMBER(environment_map, emitters::environment_light::mEnvironmentMap);
 RB_PRIVATE_MEMBER(environment_intensity, emitters::environment_light::mIntensity);
@@ -143,8 +160,25 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 		ok = constant_rgb(read(*x, substrate_specular{}), d.reflectance) &&
 			constant_rgb(read(*x, substrate_diffuse{}), d.diffuse) && constant_real(read(*x, substrate_ru{}), d.roughness_u) &&
 			constant_real(read(*x, substrate_rv{}), d.roughness_v);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::uber_material>(m)) {
+		d.kind = RB_MATERIAL_UBER;
+		d.remap_roughness = read(*x, uber_remap{}) ? 1 : 0;
+		ok = constant_rgb(read(*x, uber_transmission{}), d.transmission) &&
+			constant_rgb(read(*x, uber_reflectance{}), d.reflectance) && constant_rgb(read(*x, uber_specular{}), d.specular) &&
+			constant_rgb(read(*x, uber_diffuse{}), d.diffuse) && constant_rgb(read(*x, uber_opacity{}), d.opacity) &&
+			constant_real(read(*x, uber_ru{}), d.roughness_u) && constant_real(read(*x, uber_rv{}), d.roughness_v) &&
+			constant_real(read(*x, uber_eta{}), d.ior);
+	} else if (const auto x = std::dynamic_pointer_cast<materials::translucent_material>(m)) {
+		d.kind = RB_MATERIAL_TRANSLUCENT;
+		d.remap_roughness = read(*x, translucent_remap{}) ? 1 : 0;
+		ok = constant_rgb(read(*x, translucent_transmission{}), d.transmission) &&
+			constant_rgb(read(*x, translucent_reflectance{}), d.reflectance) &&
+			constant_rgb(read(*x, translucent_specular{}), d.specular) &&
+			constant_rgb(read(*x, translucent_diffuse{}), d.diffuse) &&
+			constant_real(read(*x, translucent_roughness{}), d.roughness_u);
+		d.roughness_v = d.roughness_u;
 	} else {
-		return RB_ERR_UNSUPPORTED;  // uber, translucent, mixture, subsurface
+		return RB_ERR_UNSUPPORTED;  // mixture, subsurface
 	}
 	return ok ? RB_OK : RB_ERR_UNSUPPORTED;  // a texture that is not constant
 }

@@ -24,6 +24,61 @@ namespace {
 
 vec3 v3(const float* a, uint32_t i) { return vec3{a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
 bool black3(const float* c) { return c[0] == 0.f && c[1] == 0.f && c[2] == 0.f; }
+bool black(vec3 c) { return c.x == 0.f && c.y == 0.f && c.z == 0.f; }
+vec3 mul3(const float* a, const float* b) { return vec3{a[0] * b[0], a[1] * b[1], a[2] * b[2]}; }
+
+void layered_lobe(pt::material_rec& r, uint32_t kind, uint32_t type, vec3 spectrum, float eta = 1.f) {
+	r.lobe_kinds |= kind << (4u * r.lobe_count);
+	r.lobe_types |= type << (5u * r.lobe_count);
+	r.lobe_r[r.lobe_count] = spectrum;
+	r.lobe_eta[r.lobe_count] = eta;
+	r.lobe_count++;
+}
+
+// The lobe lists of uber_material::build_surface_properties (uber_material.cpp:26-75)
+// and translucent_material::build_surface_properties (translucent_material.cpp:23-69)
+// for constant textures, radiance transport: the same lobes, spectra and order.
+bool pack_layered(const rb_material_desc& md, pt::material_rec& r) {
+	using namespace pt;
+	r.kind = MAT_LAYERED;
+	if (md.kind == RB_MATERIAL_UBER) {
+		if (!(md.ior > 0.f)) return false;
+		const float eta = md.ior;
+		r.eta = r.collection_eta = eta;
+		r.alpha_x = md.remap_roughness ? roughness_to_alpha(md.roughness_u) : md.roughness_u;
+		r.alpha_y = md.remap_roughness ? roughness_to_alpha(md.roughness_v) : md.roughness_v;
+		const vec3 reflectance = mul3(md.opacity, md.reflectance);
+		const vec3 transmission = mul3(md.opacity, md.transmission);
+		const vec3 specular = mul3(md.opacity, md.specular);
+		const vec3 diffuse = mul3(md.opacity, md.diffuse);
+		// clamp(spectrum(1) - opacity) to [0, 1]
+		vec3 invert;
+		invert.x = fclamp_ref(1.f - md.opacity[0], 0.f, 1.f);
+		invert.y = fclamp_ref(1.f - md.opacity[1], 0.f, 1.f);
+		invert.z = fclamp_ref(1.f - md.opacity[2], 0.f, 1.f);
+		if (!black(invert)) layered_lobe(r, LOBE_L_SPECULAR_TRANSMIT, ST_SPECULAR | ST_TRANSMISSION, invert, 1.f);
+		if (!black(diffuse)) layered_lobe(r, LOBE_L_LAMBERT, ST_DIFFUSE | ST_REFLECTION, diffuse);
+		if (!black(specular)) layered_lobe(r, LOBE_L_MF_REFLECT, ST_GLOSSY | ST_REFLECTION, specular);
+		if (!black(reflectance)) layered_lobe(r, LOBE_L_SPECULAR_REFLECT, ST_SPECULAR | ST_REFLECTION, reflectance);
+		if (!black(transmission)) layered_lobe(r, LOBE_L_SPECULAR_TRANSMIT, ST_SPECULAR | ST_TRANSMISSION, transmission, eta);
+		return true;
+	}
+	// translucent: IOR 1.5, one isotropic roughness
+	const float eta = 1.5f;
+	r.eta = r.collection_eta = eta;
+	r.alpha_x = r.alpha_y = md.remap_roughness ? roughness_to_alpha(md.roughness_u) : md.roughness_u;
+	const bool has_r = !black3(md.reflectance), has_t = !black3(md.transmission);
+	if (!has_r && !has_t) return true;
+	if (!black3(md.diffuse)) {
+		if (has_r) layered_lobe(r, LOBE_L_LAMBERT, ST_DIFFUSE | ST_REFLECTION, mul3(md.diffuse, md.reflectance));
+		if (has_t) layered_lobe(r, LOBE_L_LAMBERT_TRANSMIT, ST_DIFFUSE | ST_TRANSMISSION, mul3(md.diffuse, md.transmission));
+	}
+	if (!black3(md.specular)) {
+		if (has_r) layered_lobe(r, LOBE_L_MF_REFLECT, ST_GLOSSY | ST_REFLECTION, mul3(md.specular, md.reflectance));
+		if (has_t) layered_lobe(r, LOBE_L_MF_TRANSMIT, ST_GLOSSY | ST_TRANSMISSION, mul3(md.specular, md.transmission));
+	}
+	return true;
+}
 
 // distribution1d over n values (distributions/detail/distribution.hpp:48-77)
 void dist1(const float* values, int n, float* cdf, float& integral) {
@@ -147,6 +202,10 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			case RB_MATERIAL_MIRROR:
 				r.kind = black3(md.reflectance) ? pt::MAT_BLACK : pt::MAT_MIRROR;
 				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
+				break;
+			case RB_MATERIAL_UBER:
+			case RB_MATERIAL_TRANSLUCENT:
+				if (!pack_layered(md, r)) return RB_ERR_INVALID_ARGUMENT;
 				break;
 			default: return RB_ERR_INVALID_ARGUMENT;
 			}

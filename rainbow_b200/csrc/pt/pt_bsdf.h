@@ -200,64 +200,81 @@ struct lobe_sample {
 };
 RB_HD lobe_sample no_sample() { return lobe_sample{0u, spectrum{0.f, 0.f, 0.f}, vec3{0.f, 0.f, 0.f}, 0.f}; }
 
-// Lobe kinds in collection order for each material.
+// Lobe kinds in collection order for each material. The LOBE_L_* kinds are
+// the lobes of layered materials, whose spectrum (and specular transmission's
+// IOR) is the material's per-lobe entry rather than a named field.
 enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, LOBE_FRESNEL_SPECULAR = 3,
-	LOBE_SPECULAR_REFLECT = 4, LOBE_FRESNEL_BLEND = 5, LOBE_OREN_NAYAR = 6 };
+	LOBE_SPECULAR_REFLECT = 4, LOBE_FRESNEL_BLEND = 5, LOBE_OREN_NAYAR = 6,
+	LOBE_L_LAMBERT = 7,           // lambertian_reflection(R)
+	LOBE_L_LAMBERT_TRANSMIT = 8,  // lambertian_transmission(T)
+	LOBE_L_MF_REFLECT = 9,        // microfacet_reflection(TR, dielectric Fresnel (1, eta), R)
+	LOBE_L_MF_TRANSMIT = 10,      // microfacet_transmission(TR, T, 1, eta)
+	LOBE_L_SPECULAR_REFLECT = 11, // specular_reflection(dielectric Fresnel (1, eta), R)
+	LOBE_L_SPECULAR_TRANSMIT = 12 // specular_transmission(T, 1, lobe_eta)
+};
 
+// The lobe list: kinds (4 bits each) and scattering types (5 bits each) packed
+// in two words, so that a lobe is selected by a shift and the record stays in
+// registers whatever the lobe index.
 struct bsdf_t {
-	uint32_t kinds[2];
-	uint32_t types[2];
+	uint32_t kinds;
+	uint32_t types;
 	uint32_t count;
 	const material_rec* m;
 	float eta;  // collection eta (glass IOR, else 1)
 };
-// Lobe i's kind and type by selection rather than by an index into the
-// arrays, so the record stays in registers (at most two lobes).
-RB_HD uint32_t lobe_kind(const bsdf_t& b, uint32_t i) { return i == 0 ? b.kinds[0] : b.kinds[1]; }
-RB_HD uint32_t lobe_type(const bsdf_t& b, uint32_t i) { return i == 0 ? b.types[0] : b.types[1]; }
+RB_HD uint32_t lobe_kind(const bsdf_t& b, uint32_t i) { return (b.kinds >> (4u * i)) & 15u; }
+RB_HD uint32_t lobe_type(const bsdf_t& b, uint32_t i) { return (b.types >> (5u * i)) & 31u; }
+RB_HD void add_lobe(bsdf_t& b, uint32_t kind, uint32_t type) {
+	b.kinds |= kind << (4u * b.count);
+	b.types |= type << (5u * b.count);
+	b.count++;
+}
 
 RB_HD bsdf_t make_bsdf(const material_rec* m) {
 	bsdf_t b;
 	b.m = m;
 	b.count = 0;
+	b.kinds = 0;
+	b.types = 0;
 	b.eta = 1.f;
 	switch (m->kind) {
 	case MAT_LAMBERT:
-		b.kinds[0] = LOBE_LAMBERT; b.types[0] = ST_DIFFUSE | ST_REFLECTION; b.count = 1;
+		add_lobe(b, LOBE_LAMBERT, ST_DIFFUSE | ST_REFLECTION);
 		break;
 	case MAT_OREN_NAYAR:
-		b.kinds[0] = LOBE_OREN_NAYAR; b.types[0] = ST_DIFFUSE | ST_REFLECTION; b.count = 1;
+		add_lobe(b, LOBE_OREN_NAYAR, ST_DIFFUSE | ST_REFLECTION);
 		break;
 	case MAT_METAL:
-		b.kinds[0] = LOBE_MF_REFLECT; b.types[0] = ST_GLOSSY | ST_REFLECTION; b.count = 1;
+		add_lobe(b, LOBE_MF_REFLECT, ST_GLOSSY | ST_REFLECTION);
 		break;
 	case MAT_GLASS_ROUGH:
 		b.eta = m->eta;
-		b.kinds[0] = b.kinds[1] = LOBE_MF_TRANSMIT;
-		b.types[0] = b.types[1] = ST_GLOSSY | ST_TRANSMISSION;
-		if (m->has_reflect) { b.kinds[0] = LOBE_MF_REFLECT; b.types[0] = ST_GLOSSY | ST_REFLECTION; }
-		b.count = (m->has_reflect ? 1u : 0u) + (m->has_transmit ? 1u : 0u);
+		if (m->has_reflect) add_lobe(b, LOBE_MF_REFLECT, ST_GLOSSY | ST_REFLECTION);
+		if (m->has_transmit) add_lobe(b, LOBE_MF_TRANSMIT, ST_GLOSSY | ST_TRANSMISSION);
 		break;
 	case MAT_GLASS_SMOOTH:
 		b.eta = m->eta;
-		if (m->has_reflect || m->has_transmit) {
-			b.kinds[0] = LOBE_FRESNEL_SPECULAR; b.types[0] = ST_REFLECTION | ST_TRANSMISSION | ST_SPECULAR; b.count = 1;
-		}
+		if (m->has_reflect || m->has_transmit) add_lobe(b, LOBE_FRESNEL_SPECULAR, ST_REFLECTION | ST_TRANSMISSION | ST_SPECULAR);
 		break;
 	case MAT_PLASTIC:
 		// plastic_material::build_surface_properties (plastic_material.cpp:30-55): the
 		// collection's eta, then the Lambert lobe, then the reflection lobe, each if not black
 		b.eta = m->eta;
-		b.kinds[0] = b.kinds[1] = LOBE_MF_REFLECT;
-		b.types[0] = b.types[1] = ST_GLOSSY | ST_REFLECTION;
-		if (!is_black(m->diffuse)) { b.kinds[0] = LOBE_LAMBERT; b.types[0] = ST_DIFFUSE | ST_REFLECTION; }
-		b.count = (is_black(m->diffuse) ? 0u : 1u) + (m->has_reflect ? 1u : 0u);
+		if (!is_black(m->diffuse)) add_lobe(b, LOBE_LAMBERT, ST_DIFFUSE | ST_REFLECTION);
+		if (m->has_reflect) add_lobe(b, LOBE_MF_REFLECT, ST_GLOSSY | ST_REFLECTION);
 		break;
 	case MAT_MIRROR:
-		b.kinds[0] = LOBE_SPECULAR_REFLECT; b.types[0] = ST_SPECULAR | ST_REFLECTION; b.count = 1;
+		add_lobe(b, LOBE_SPECULAR_REFLECT, ST_SPECULAR | ST_REFLECTION);
 		break;
 	case MAT_SUBSTRATE:
-		b.kinds[0] = LOBE_FRESNEL_BLEND; b.types[0] = ST_GLOSSY | ST_REFLECTION; b.count = 1;
+		add_lobe(b, LOBE_FRESNEL_BLEND, ST_GLOSSY | ST_REFLECTION);
+		break;
+	case MAT_LAYERED:
+		b.eta = m->collection_eta;
+		b.kinds = m->lobe_kinds;
+		b.types = m->lobe_types;
+		b.count = m->lobe_count;
 		break;
 	default: break;  // black matte: no lobes
 	}
@@ -268,21 +285,23 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 // run-time switch. Specialised code keeps each shading kernel small.
 constexpr int MAT_ANY = -1;
 
+// microfacet_reflection::evaluate (scatterings/reflection/microfacet_reflection.cpp):
+// conductor Fresnel for metal, else dielectric Fresnel (1, m->eta) scaled by R
+// (the material's reflectance, or a layered lobe's own spectrum).
 template <int MAT = MAT_ANY>
-RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi) {
+RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi, spectrum R) {
 	const float co = fabs_ref(wo.z), ci = fabs_ref(wi.z);
 	vec3 wh = wi + wo;
 	if (co == 0.f || ci == 0.f) return spectrum{0.f, 0.f, 0.f};
 	if (wh.x == 0.f && wh.y == 0.f && wh.z == 0.f) return spectrum{0.f, 0.f, 0.f};
 	wh = face_forward(normalize(wh), vec3{0.f, 0.f, 1.f});
-	spectrum F, R;
+	spectrum F;
 	const bool conductor = MAT == MAT_ANY ? (m->kind == MAT_METAL) : (MAT == static_cast<int>(MAT_METAL));
 	if (conductor) {
 		F = fresnel_conductor(dot(wi, wh), m->cond_eta, m->cond_k);
 		R = spectrum{1.f, 1.f, 1.f};
 	} else {
 		F = splat3(fresnel_dielectric(dot(wi, wh), 1.f, m->eta));
-		R = m->reflectance;
 	}
 	const float G = tr_g(m->alpha_x, m->alpha_y, wo, wi);
 	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
@@ -293,7 +312,9 @@ RB_HD float mf_reflect_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	const vec3 wh = normalize(wo + wi);
 	return tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh));
 }
-RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi) {
+// microfacet_transmission::evaluate (scatterings/transmission/microfacet_transmission.cpp:14-37),
+// radiance transport, eta (1, m->eta), scaled by T.
+RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi, spectrum T) {
 	if (same_hemisphere(wo, wi)) return spectrum{0.f, 0.f, 0.f};
 	const float co = wo.z, ci = wi.z;
 	if (co == 0.f || ci == 0.f) return spectrum{0.f, 0.f, 0.f};
@@ -307,7 +328,7 @@ RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi) {
 	const float G = tr_g(m->alpha_x, m->alpha_y, wo, wi);
 	const float v = fabs_ref(D * G * eta * eta * fabs_ref(dot(wi, wh)) * fabs_ref(dot(wo, wh) * factor * factor) /
 		(ci * co * denom * denom));
-	return (splat3(1.f) - splat3(F)) * m->transmission * v;
+	return (splat3(1.f) - splat3(F)) * T * v;
 }
 RB_HD float mf_transmit_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	if (same_hemisphere(wo, wi)) return 0.f;
@@ -364,20 +385,30 @@ RB_HD spectrum oren_nayar_f(const material_rec* m, vec3 wo, vec3 wi) {
 	return m->diffuse * kInvPi * (m->alpha_x + m->alpha_y * max_cos * sin_alpha * tan_beta);
 }
 
+// The spectrum a lobe scales by: a layered lobe's own entry, else the
+// material's named field the lobe kind reads.
+RB_HD spectrum layered_r(const bsdf_t& b, uint32_t i) { return b.m->lobe_r[i]; }
+
 template <int MAT>
 RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return b.m->diffuse * kInvPi;
-	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_f<MAT>(b.m, wo, wi);
+	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_f<MAT>(b.m, wo, wi, b.m->reflectance);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
-		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi) : mf_transmit_f(b.m, wo, wi);
+		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi, b.m->reflectance)
+		                                          : mf_transmit_f(b.m, wo, wi, b.m->transmission);
 	else {
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
 		case LOBE_OREN_NAYAR: return oren_nayar_f(b.m, wo, wi);
-		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi);
-		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi);
+		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi, b.m->reflectance);
+		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi, b.m->transmission);
 		case LOBE_FRESNEL_BLEND: return fresnel_blend_f(b.m, wo, wi);
-		default: return spectrum{0.f, 0.f, 0.f};
+		// lambertian_reflection / lambertian_transmission::evaluate: R / pi, T / pi
+		case LOBE_L_LAMBERT:
+		case LOBE_L_LAMBERT_TRANSMIT: return layered_r(b, i) * kInvPi;
+		case LOBE_L_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi, layered_r(b, i));
+		case LOBE_L_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi, layered_r(b, i));
+		default: return spectrum{0.f, 0.f, 0.f};  // specular lobes evaluate to 0
 		}
 	}
 }
@@ -390,11 +421,16 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	else {
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT:
-		case LOBE_OREN_NAYAR: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
-		case LOBE_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
-		case LOBE_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
+		case LOBE_OREN_NAYAR:
+		case LOBE_L_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
+		// transmission_function::pdf (scatterings/transmission/transmission_function.cpp:25-28)
+		case LOBE_L_LAMBERT_TRANSMIT: return same_hemisphere(wo, wi) ? 0.f : cosine_hemisphere_pdf(fabs_ref(wi.z));
+		case LOBE_MF_REFLECT:
+		case LOBE_L_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
+		case LOBE_MF_TRANSMIT:
+		case LOBE_L_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
 		case LOBE_FRESNEL_BLEND: return fresnel_blend_pdf(b.m, wo, wi);
-		default: return 0.f;
+		default: return 0.f;  // specular lobes: pdf 0
 		}
 	}
 }
@@ -405,17 +441,24 @@ RB_HD lobe_sample sample_lambert(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
 	if (wo.z < 0.f) wi.z = -wi.z;
 	return lobe_sample{lobe_type(b, i), lobe_f<MAT>(b, i, wo, wi), wi, lobe_pdf<MAT>(b, i, wo, wi)};
 }
+// transmission_function::sample (scatterings/transmission/transmission_function.cpp:11-23):
+// the cosine hemisphere on the side opposite wo.
+RB_HD lobe_sample sample_lambert_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+	vec3 wi = cosine_hemisphere(u);
+	if (wo.z > 0.f) wi.z = -wi.z;
+	return lobe_sample{lobe_type(b, i), lobe_f<MAT_ANY>(b, i, wo, wi), wi, lobe_pdf<MAT_ANY>(b, i, wo, wi)};
+}
 template <int MAT>
-RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u, spectrum R) {
 	const material_rec* m = b.m;
 	if (wo.z == 0.f) return no_sample();
 	const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
 	if (dot(wo, wh) < 0.f) return no_sample();
 	const vec3 wi = reflect(wo, wh);
 	if (!same_hemisphere(wo, wi)) return no_sample();
-	return lobe_sample{lobe_type(b, i), mf_reflect_f<MAT>(m, wo, wi), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
+	return lobe_sample{lobe_type(b, i), mf_reflect_f<MAT>(m, wo, wi, R), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
 }
-RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
+RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u, spectrum T) {
 	const material_rec* m = b.m;
 	if (wo.z == 0.f) return no_sample();
 	const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
@@ -424,7 +467,7 @@ RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 
 	const float eta = entering ? (1.f / m->eta) : (m->eta / 1.f);
 	const vec3 wi = refract(wo, wh, eta);
 	if (is_zero(wi)) return no_sample();
-	return lobe_sample{lobe_type(b, i), mf_transmit_f(m, wo, wi), wi, mf_transmit_pdf(m, wo, wi)};
+	return lobe_sample{lobe_type(b, i), mf_transmit_f(m, wo, wi, T), wi, mf_transmit_pdf(m, wo, wi)};
 }
 // fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
 RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
@@ -466,21 +509,50 @@ RB_HD lobe_sample sample_specular_reflect(const bsdf_t& b, vec3 wo) {
 	const vec3 wi{-wo.x, -wo.y, wo.z};
 	return lobe_sample{ST_SPECULAR | ST_REFLECTION, b.m->reflectance / fabs_ref(wi.z), wi, 1.f};
 }
+// specular_reflection::sample with a dielectric Fresnel (1, m->eta):
+// f = F(cos theta_i) R / |cos theta_i|, pdf 1.
+RB_HD lobe_sample sample_layered_specular_reflect(const bsdf_t& b, uint32_t i, vec3 wo) {
+	const vec3 wi{-wo.x, -wo.y, wo.z};
+	const float F = fresnel_dielectric(wi.z, 1.f, b.m->eta);
+	return lobe_sample{ST_SPECULAR | ST_REFLECTION, splat3(F) * layered_r(b, i) / fabs_ref(wi.z), wi, 1.f};
+}
+// specular_transmission::sample (scatterings/transmission/specular_transmission.cpp:17-46),
+// radiance transport, eta (1, lobe_eta): refraction about the normal on wo's
+// side, f = T (1 - F(cos theta_i)) (eta_i / eta_o)^2 / |cos theta_i|, pdf 1.
+RB_HD lobe_sample sample_specular_transmit(const bsdf_t& b, uint32_t i, vec3 wo) {
+	const float lobe_eta = b.m->lobe_eta[i];
+	const bool entering = wo.z > 0.f;
+	const float ei = entering ? 1.f : lobe_eta;
+	const float eo = entering ? lobe_eta : 1.f;
+	const vec3 wi = refract(wo, face_forward(vec3{0.f, 0.f, 1.f}, wo), ei / eo);
+	if (is_zero(wi)) return no_sample();
+	const float F = fresnel_dielectric(wi.z, 1.f, lobe_eta);
+	const float factor = (ei * ei) / (eo * eo);
+	const spectrum v = layered_r(b, i) * (splat3(1.f) - splat3(F)) * factor / fabs_ref(wi.z);
+	return lobe_sample{ST_SPECULAR | ST_TRANSMISSION, v, wi, 1.f};
+}
 
 template <int MAT>
 RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) {
 	if constexpr (MAT == static_cast<int>(MAT_LAMBERT)) return sample_lambert<MAT>(b, i, wo, u);
-	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return sample_mf_reflect<MAT>(b, i, wo, u);
+	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return sample_mf_reflect<MAT>(b, i, wo, u, b.m->reflectance);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
-		return lobe_kind(b, i) == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u) : sample_mf_transmit(b, i, wo, u);
+		return lobe_kind(b, i) == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u, b.m->reflectance)
+		                                          : sample_mf_transmit(b, i, wo, u, b.m->transmission);
 	else {
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT:
-		case LOBE_OREN_NAYAR: return sample_lambert<MAT_ANY>(b, i, wo, u);  // reflection_function::sample, cosine
-		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u);
-		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u);
+		case LOBE_OREN_NAYAR:
+		case LOBE_L_LAMBERT: return sample_lambert<MAT_ANY>(b, i, wo, u);  // reflection_function::sample, cosine
+		case LOBE_L_LAMBERT_TRANSMIT: return sample_lambert_transmit(b, i, wo, u);
+		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, b.m->reflectance);
+		case LOBE_L_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, layered_r(b, i));
+		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u, b.m->transmission);
+		case LOBE_L_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u, layered_r(b, i));
 		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(b, wo, u);
 		case LOBE_SPECULAR_REFLECT: return sample_specular_reflect(b, wo);
+		case LOBE_L_SPECULAR_REFLECT: return sample_layered_specular_reflect(b, i, wo);
+		case LOBE_L_SPECULAR_TRANSMIT: return sample_specular_transmit(b, i, wo);
 		case LOBE_FRESNEL_BLEND: return sample_fresnel_blend(b, wo, u);
 		default: return no_sample();
 		}
@@ -521,14 +593,7 @@ RB_HD uint32_t bsdf_count(const bsdf_t& b, uint32_t include) {
 // shading frame; the returned wi is in the shading frame too.
 template <int MAT = MAT_ANY>
 RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include) {
-	// matching lobes in order: idx0, then idx1
-	uint32_t idx0 = 0, idx1 = 0, n = 0;
-	for (uint32_t i = 0; i < b.count; i++)
-		if (type_match(include, lobe_type(b, i))) {
-			if (n == 0) idx0 = i;
-			else idx1 = i;
-			n++;
-		}
+	const uint32_t n = bsdf_count(b, include);
 	if (n == 0) return no_sample();
 	const float fn = static_cast<float>(n);
 	uint32_t which = static_cast<uint32_t>(floorf(u.x * fn));
@@ -536,14 +601,21 @@ RB_HD lobe_sample bsdf_sample(const bsdf_t& b, vec3 wo, vec2 u, uint32_t include
 	const float rx = u.x * fn - static_cast<float>(which);
 	const vec2 ur{(kOneMinusEps < rx) ? kOneMinusEps : rx, u.y};
 	if (wo.z == 0.f) return no_sample();
-	lobe_sample s = lobe_sample_dir<MAT>(b, which == 0 ? idx0 : idx1, wo, ur);
+	// the which-th lobe matching include, in collection order
+	uint32_t pick = 0;
+	for (uint32_t i = 0, k = 0; i < b.count; i++)
+		if (type_match(include, lobe_type(b, i))) {
+			if (k == which) pick = i;
+			k++;
+		}
+	lobe_sample s = lobe_sample_dir<MAT>(b, pick, wo, ur);
 	if (s.pdf == 0.f) return no_sample();
 	if (!type_match(s.type, ST_SPECULAR)) {
 		const uint32_t rt = same_hemisphere(wo, s.wi) ? ST_REFLECTION : ST_TRANSMISSION;
 		s.f = spectrum{0.f, 0.f, 0.f};
 		s.pdf = 0.f;
-		for (uint32_t k = 0; k < n; k++) {
-			const uint32_t i = k == 0 ? idx0 : idx1;
+		for (uint32_t i = 0; i < b.count; i++) {
+			if (!type_match(include, lobe_type(b, i))) continue;
 			if (type_match(lobe_type(b, i), rt)) s.f = s.f + lobe_f<MAT>(b, i, wo, s.wi);
 			s.pdf = s.pdf + lobe_pdf<MAT>(b, i, wo, s.wi);
 		}

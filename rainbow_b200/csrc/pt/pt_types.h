@@ -116,7 +116,10 @@ struct mesh_rec {
 };
 
 enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4, MAT_PLASTIC = 5,
-	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8 };
+	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8, MAT_LAYERED = 9 };
+
+// Lobes of a layered material (uber, translucent): at most kMaxLayeredLobes.
+constexpr uint32_t kMaxLayeredLobes = 6;
 
 struct material_rec {
 	uint32_t kind;
@@ -130,6 +133,15 @@ struct material_rec {
 	spectrum cond_k;          // conductor k
 	uint32_t has_reflect;     // glass: reflectance not black
 	uint32_t has_transmit;    // glass: transmission not black
+	// layered materials (MAT_LAYERED: uber, translucent), whose lobe list is
+	// built on the host: the lobe kinds (4 bits each) and scattering types (5
+	// bits each) in collection order, their count, each lobe's spectrum and the
+	// outer IOR of its specular transmission, and the collection's eta (eta is
+	// the IOR of the dielectric Fresnel of its reflection lobes)
+	uint32_t lobe_kinds, lobe_types, lobe_count;
+	float collection_eta;
+	spectrum lobe_r[kMaxLayeredLobes];
+	float lobe_eta[kMaxLayeredLobes];
 };
 
 enum : uint32_t { EMIT_SURFACE = 0, EMIT_ENVIRONMENT = 1 };

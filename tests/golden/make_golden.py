@@ -238,6 +238,20 @@ def oren_nayar_fixtures():
     bsdf_fixtures({"oren_nayar": dict(kind=rb.RB_MATERIAL_MATTE, diffuse=(0.7, 0.4, 0.2), sigma=20.0)})
 
 
+def layered_fixtures():
+    from tests.helpers import layered_scene
+    R = ref.RefScene(layered_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(41)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("layered_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8),
+         first_entity=first_entity(R, px, sm))
+    bsdf_fixtures({"uber": dict(kind=rb.RB_MATERIAL_UBER, opacity=(0.7, 0.8, 0.9)),
+                   "uber_opaque": dict(kind=rb.RB_MATERIAL_UBER, opacity=(1.0, 1.0, 1.0)),
+                   "translucent": dict(kind=rb.RB_MATERIAL_TRANSLUCENT)})
+
+
 def materials_fixtures():
     from tests.helpers import extra_materials_scene
     R = ref.RefScene(extra_materials_scene(scene_of(SPHERES)))
@@ -282,6 +296,8 @@ def main():
         return two_level_fixtures()
     if only == "oren_nayar":
         return oren_nayar_fixtures()
+    if only == "layered":
+        return layered_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -330,6 +346,7 @@ def main():
     baseline_fixtures()
     two_level_fixtures()
     oren_nayar_fixtures()
+    layered_fixtures()
 
 
 def material_desc(m):
@@ -351,6 +368,22 @@ def material_desc(m):
         md.diffuse[:] = (0.5, 0.35, 0.2)
         md.reflectance[:] = (0.05, 0.05, 0.05)
         md.roughness_u, md.roughness_v = m["rough"], 0.5 * m["rough"]
+    elif m["kind"] == rb.RB_MATERIAL_UBER:
+        md.remap_roughness = 1
+        md.diffuse[:] = (0.5, 0.3, 0.2)
+        md.specular[:] = (0.3, 0.3, 0.25)
+        md.reflectance[:] = (0.1, 0.1, 0.1)
+        md.transmission[:] = (0.2, 0.25, 0.3)
+        md.opacity[:] = m["opacity"]
+        md.roughness_u, md.roughness_v = 0.15, 0.3
+        md.ior = 1.5
+    elif m["kind"] == rb.RB_MATERIAL_TRANSLUCENT:
+        md.remap_roughness = 1
+        md.diffuse[:] = (0.6, 0.5, 0.4)
+        md.specular[:] = (0.4, 0.4, 0.4)
+        md.reflectance[:] = (0.5, 0.5, 0.5)
+        md.transmission[:] = (0.4, 0.45, 0.5)
+        md.roughness_u = 0.2
     elif m["kind"] == rb.RB_MATERIAL_METAL:
         md.remap_roughness = 1
         md.eta[:] = (0.200438, 0.924033, 1.102212)

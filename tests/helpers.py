@@ -19,6 +19,30 @@ def scene_from_params(params) -> rb.Scene:
     return rb.generate_scene(kind, seed=seed, width=w, height=h, num_spheres=n, subdivision=sub)
 
 
+def material_from_bytes(raw: bytes) -> rb.MaterialDesc:
+    """A material descriptor from a fixture's bytes; fields added to the
+    descriptor after the fixture was written (at its end) read as zero."""
+    size = C.sizeof(rb.MaterialDesc)
+    return rb.MaterialDesc.from_buffer_copy(bytes(raw)[:size].ljust(size, b"\0"))
+
+
+_LOBE_NAMES = {0: "lambert", 1: "microfacet_reflection", 2: "microfacet_transmission", 3: "fresnel_specular",
+               4: "specular_reflection", 5: "fresnel_blend", 6: "oren_nayar", 7: "lambert",
+               8: "lambert_transmission", 9: "microfacet_reflection", 10: "microfacet_transmission",
+               11: "specular_reflection", 12: "specular_transmission"}
+
+
+def material_lobes(md: rb.MaterialDesc) -> list:
+    """Names of the lobes that the host packing of one material gives, in
+    collection order (host build of the kernels' make_bsdf)."""
+    L = C.CDLL(HOSTPATHS)
+    L.hp_material_lobes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    kinds = (C.c_uint32 * 8)()
+    n = C.c_uint32(0)
+    rb.check(L.hp_material_lobes(C.byref(md), kinds, C.byref(n)), "hp_material_lobes")
+    return [_LOBE_NAMES[kinds[i]] for i in range(n.value)]
+
+
 def extra_materials_scene(scene: rb.Scene) -> rb.Scene:
     """The scene with every fourth material (from the second) plastic, every
     fourth (from the third) a mirror and every eighth (from the fourth) a
@@ -369,6 +393,39 @@ def two_level_scene(width=64, height=48):
     nd.num_entities = len(ents)
     return rb.Scene(None, nd, base.camera, keepalive=[base, big, mesh_arr, ent_arr])
 
+
+
+def layered_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with every third material (from the second, the floor's) an
+    uber material (uber_material.cpp; opacity below one on every other one, so
+    that its pass-through specular transmission is in the lobe list) and every
+    third (from the first) a translucent material (translucent_material.cpp;
+    every fourth of those without its specular lobes); the rest unchanged."""
+    mats = []
+    for k in range(scene.desc.num_materials):
+        m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
+        if k % 3 == 1:
+            m = rb.MaterialDesc()
+            m.kind = rb.RB_MATERIAL_UBER
+            m.remap_roughness = 1
+            m.diffuse[:] = (0.5, 0.3, 0.2)
+            m.specular[:] = (0.3, 0.3, 0.25)
+            m.reflectance[:] = (0.1, 0.1, 0.1) if k % 4 == 1 else (0.0, 0.0, 0.0)
+            m.transmission[:] = (0.2, 0.25, 0.3) if k % 5 == 1 else (0.0, 0.0, 0.0)
+            m.opacity[:] = (0.7, 0.8, 0.9) if k % 2 == 1 else (1.0, 1.0, 1.0)
+            m.roughness_u, m.roughness_v = 0.1 + 0.05 * (k % 4), 0.2
+            m.ior = 1.5
+        elif k % 3 == 0:
+            m = rb.MaterialDesc()
+            m.kind = rb.RB_MATERIAL_TRANSLUCENT
+            m.remap_roughness = 1
+            m.diffuse[:] = (0.6, 0.5, 0.4)
+            m.specular[:] = (0.0, 0.0, 0.0) if k % 4 == 0 else (0.4, 0.4, 0.4)
+            m.reflectance[:] = (0.5, 0.5, 0.5)
+            m.transmission[:] = (0.4, 0.45, 0.5)
+            m.roughness_u = m.roughness_v = 0.15 + 0.05 * (k % 3)  # translucent reads roughness_u alone
+        mats.append(m)
+    return scene.with_materials(mats)
 
 
 def oren_nayar_scene(scene: rb.Scene) -> rb.Scene:

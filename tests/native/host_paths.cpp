@@ -161,6 +161,46 @@ struct hp_batch {
 
 extern "C" {
 
+// The lobe list that the packed record of one material gives make_bsdf: the
+// lobe kinds (LOBE_*) in collection order. Returns the packing status.
+int hp_material_lobes(const rb_material_desc* md, uint32_t* kinds, uint32_t* count) {
+	// one triangle with the material, and an environment emitter (a scene needs one)
+	const float pos[9] = {0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f, 0.f};
+	const uint32_t idx[3] = {0, 1, 2};
+	rb_mesh_desc mesh{};
+	mesh.positions = pos;
+	mesh.indices = idx;
+	mesh.num_vertices = 3;
+	mesh.num_triangles = 1;
+	rb_emitter_desc em{};
+	em.kind = RB_EMITTER_ENVIRONMENT;
+	em.radius = 1.f;
+	rb_entity_desc ents[2]{};
+	for (int e = 0; e < 2; e++) {
+		ents[e].mesh = e == 0 ? 0 : -1;
+		ents[e].material = e == 0 ? 0 : -1;
+		ents[e].emitter = e == 0 ? -1 : 0;
+		ents[e].medium = -1;
+		for (int i = 0; i < 16; i++) ents[e].local_to_world[i] = ents[e].world_to_local[i] = (i % 5 == 0) ? 1.f : 0.f;
+	}
+	rb_scene_desc d{};
+	d.meshes = &mesh;
+	d.num_meshes = 1;
+	d.materials = md;
+	d.num_materials = 1;
+	d.emitters = &em;
+	d.num_emitters = 1;
+	d.entities = ents;
+	d.num_entities = 2;
+	host::packed_scene p;
+	const rb_status st = host::pack_scene(&d, p);
+	if (st != RB_OK) return st;
+	const bsdf_t b = make_bsdf(p.materials.data());
+	*count = b.count;
+	for (uint32_t i = 0; i < b.count; i++) kinds[i] = lobe_kind(b, i);
+	return RB_OK;
+}
+
 int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {
 	const hp_scene& s = *static_cast<hp_scene*>(hs);
 	trace_batch(s.packed, s.view, 0u, rays, n, shadow, hits);

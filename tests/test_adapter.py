@@ -10,7 +10,7 @@ import pytest
 
 import rainbow_b200 as rb
 from oracle import ref
-from tests.helpers import extra_materials_scene, two_level_scene
+from tests.helpers import extra_materials_scene, layered_scene, two_level_scene
 
 pytestmark = pytest.mark.skipif(not ref.adapter_available(), reason="oracle/_ref/libadapter_check.so not built")
 
@@ -21,12 +21,15 @@ def _scene(name):
     if name == "spheres_materials":
         return extra_materials_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
                                                        subdivision=2))
+    if name == "spheres_layered":
+        return layered_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
+                                               subdivision=2))
     if name == "fog":
         return rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=40, height=30, num_spheres=6, subdivision=2)
     return two_level_scene()
 
 
-@pytest.mark.parametrize("name", ["box", "spheres_materials", "fog", "two_level"])
+@pytest.mark.parametrize("name", ["box", "spheres_materials", "spheres_layered", "fog", "two_level"])
 def test_export_describes_the_reference_scene(name):
     scene = _scene(name)
     R = ref.RefScene(scene)

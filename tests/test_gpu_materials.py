@@ -1,4 +1,4 @@
-"""Plastic, mirror and substrate materials on the GPU: with spp = 1 the film sum of a pixel
+"""Plastic, mirror, substrate, Oren-Nayar, uber and translucent materials on the GPU: with spp = 1 the film sum of a pixel
 is one sample's radiance, against the reference's path_integrator::trace on the
 spheres scene with plastic, mirror and substrate materials (golden fixture), and the same
 scene in direct lighting against the host build."""
@@ -7,8 +7,8 @@ import pytest
 
 import rainbow_b200 as rb
 from tests import golden
-from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, oren_nayar_scene,
-                           per_sample_radiance, scene_from_params)
+from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, layered_scene,
+                           oren_nayar_scene, per_sample_radiance, scene_from_params)
 
 pytestmark = pytest.mark.gpu
 
@@ -44,6 +44,33 @@ def test_oren_nayar_samples_match_reference():
     agree = _agreement(got, fx["radiance"])
     assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
     assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], "oren-nayar")
+
+
+def test_layered_samples_match_reference():
+    fx = golden.load("layered_samples")
+    scene = layered_scene(scene_from_params(fx["params"]))
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        got = per_sample_radiance(ctx, scene, fx["pixels"], fx["samples"], int(fx["max_depth"]))
+        assert ctx.stats().device_error == 0
+    agree = _agreement(got, fx["radiance"])
+    assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
+    assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], "layered")
+
+
+def test_layered_direct_matches_host_build():
+    fx = golden.load("layered_samples")
+    scene = layered_scene(scene_from_params(fx["params"]))
+    W, H = scene.camera.width, scene.camera.height
+    px = np.arange(W * H, dtype=np.uint32)
+    want = HostPaths(scene).direct_samples(scene.camera, px, np.full_like(px, 2), 4, 4)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        ctx.render(scene.camera, spp=1, first_sample=2, want_image=False, direct=(4, 4))
+        sums, _, cnt = ctx.film()
+    assert (cnt == 1).all()
+    agree = _agreement(sums.reshape(-1, 3).astype(np.float32), want)
+    assert agree >= 0.97, f"only {agree:.4f} of pixels agree"
 
 
 def test_extra_materials_direct_matches_host_build():

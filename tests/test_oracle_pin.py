@@ -12,7 +12,7 @@ import pytest
 import rainbow_b200 as rb
 from oracle import port, ref
 from tests import golden
-from tests.helpers import assert_hits_equal, scene_from_params
+from tests.helpers import assert_hits_equal, material_from_bytes, scene_from_params
 
 needs_ref = pytest.mark.skipif(not ref.available(), reason="reference oracle not built (needs the reference sources)")
 
@@ -81,11 +81,11 @@ def test_reference_samples_match_fixture(name):
 
 @needs_ref
 @pytest.mark.parametrize("mat", ["lambert", "metal", "glass_rough", "glass_smooth", "plastic", "mirror", "substrate",
-                                 "oren_nayar"])
+                                 "oren_nayar", "uber", "uber_opaque", "translucent"])
 @pytest.mark.parametrize("inc", ["all", "nonspec"])
 def test_reference_bsdf_matches_fixture(mat, inc):
     fx = golden.load(f"bsdf_{mat}_{inc}")
-    md = rb._native.MaterialDesc.from_buffer_copy(fx["material"].tobytes())
+    md = material_from_bytes(fx["material"].tobytes())
     out = ref.bsdf(md, fx["wo"], fx["u"], fx["wi_eval"], int(fx["include"]))
     for k in ("wi", "f", "pdf", "f_eval", "pdf_eval"):
         assert np.array_equal(out[k].view(np.uint32), fx[k].view(np.uint32)), k
