@@ -277,6 +277,25 @@ def direct_waves(res=1024, spp=2):
     return 0
 
 
+def trace_waves(res=512, shadow_test=0):
+    """Two one-sample calls on the sphere field at res x res, one lane of one wave (the reduced workload of the
+    traversal profile in profiles/: inputs above L2, a few hundred MB on the device)."""
+    import rainbow_b200 as rb
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=res, height=res, num_spheres=200, subdivision=4)
+    ctx = rb.Context(0)
+    ctx.upload(scene)
+    ctx.set_tuning(paths_per_wave=res * res, block_trace=64, block_shade=128, grid_per_sm=8, sort=rb.RB_SORT_RAYS, lanes=1,
+                   smem_carveout=76, shadow_test=shadow_test)
+    for k in range(2):
+        ctx.render(scene.camera, 1, first_sample=k, max_depth=8, reset=True, want_image=False)
+    st = ctx.stats()
+    ctx.close()
+    print(json.dumps({"ms": st.elapsed_ms, "extend_ms": st.extend_ms, "secondary_ms": st.secondary_ms,
+                      "traversal_rays": st.extend_rays + st.shadow_rays + st.mis_rays, "extend_rays": st.extend_rays,
+                      "secondary_rays": st.shadow_rays + st.mis_rays, "device_error": st.device_error}))
+    return 0
+
+
 def guided_waves(res=1024):
     """Two plain waves, then three guided training waves (2 spp each) on the slit room: the
     workload of the guide-network profile in profiles/."""
@@ -468,6 +487,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--guided-waves", action="store_true",
                     help="only render 2 plain then 3 guided training waves of 2 spp on the slit room (profiling)")
+    ap.add_argument("--trace-waves", action="store_true",
+                    help="only render two 1-spp calls of the sphere field at 512x512 on one lane (profiling)")
     ap.add_argument("--direct-waves", action="store_true",
                     help="only render one 2-spp direct-lighting call on the sphere field (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
@@ -480,6 +501,8 @@ def main():
         return guided_waves()
     if args.direct_waves:
         return direct_waves()
+    if args.trace_waves:
+        return trace_waves()
 
     import torch
     import torch.distributed as dist
