@@ -192,8 +192,8 @@ def config_dict(world):
                   "film 59 MB); the 86 MB scene stays resident across steps as in any multi-sample render"}
 
 
-def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=12, batch=1 << 17, train_chunks=4,
-               lanes=4, learning_rate=3e-3, weight_clip=4.0, guide_seeds=(0, 1, 2)):
+def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave=12, batch=1 << 18, train_chunks=4,
+               lanes=4, learning_rate=1e-3, weight_clip=4.0, guide_seeds=(0, 1, 2, 3, 4)):
     """Device time to each relMSE target: plain vs guided (online training during the first train_chunks
     chunks, then guided sampling with the trained weights). Guided runs once per guide seed (the trained
     guide, and so the time to a target, varies with the weight initialisation and the training order); the

@@ -90,15 +90,31 @@ enum {
 	                            roughness_u / roughness_v), specular reflection of O reflectance
 	                            (dielectric Fresnel of ior) and specular transmission of
 	                            O transmission (eta 1 / ior), each if not black */
-	RB_MATERIAL_TRANSLUCENT = 7 /* rainbow-cpu/materials/translucent_material.cpp:23-69: IOR 1.5; no lobes
+	RB_MATERIAL_TRANSLUCENT = 7, /* rainbow-cpu/materials/translucent_material.cpp:23-69: IOR 1.5; no lobes
 	                            when reflectance and transmission are both black; else Lambert
 	                            reflection of diffuse reflectance and Lambert transmission of diffuse
 	                            transmission (if diffuse is not black), Trowbridge-Reitz reflection of
 	                            specular reflectance and transmission of specular transmission (if
 	                            specular is not black), isotropic roughness_u */
+	RB_MATERIAL_MIXTURE = 8  /* rainbow-cpu/materials/mixture_material.cpp:13-43: the lobes of material
+	                            components[0] built with the weight amount and of components[1] with
+	                            clamp(1 - amount), each by its material's build with a scale (mixtures
+	                            nest up to 8 deep; at most 6 lobes in all, else RB_ERR_UNSUPPORTED) */
 };
 
-/* Constant-texture material parameters (constant_texture_t, textures/detail/constant_texture.hpp:25-35). */
+/* An RGB image texture (image_texture_t<2, spectrum>, textures/detail/image_texture.hpp):
+ * width * height texels, row-major, texel (x, y) at rgb[3 * (y * width + x)]. Sampled at
+ * a hit's uv (the triangle's vertex uvs, or (0, 0), (1, 0), (1, 1) without them) with the
+ * uv wrapped to [0, 1) and bilinear filtering between the four nearest texels. */
+typedef struct rb_texture_desc {
+	const float* rgb;
+	uint32_t width;
+	uint32_t height;
+} rb_texture_desc;
+
+/* Material parameters: constant textures (constant_texture_t,
+ * textures/detail/constant_texture.hpp:25-35), and for the spectra named by the
+ * *_texture fields image textures instead. */
 typedef struct rb_material_desc {
 	uint32_t kind;
 	int32_t remap_roughness;    /* metal/glass: apply trowbridge_reitz_distribution::roughness_to_alpha */
@@ -113,6 +129,15 @@ typedef struct rb_material_desc {
 	float roughness_v;
 	float specular[3];          /* uber, translucent: the glossy reflection's spectrum */
 	float opacity[3];           /* uber */
+	int32_t components[2];      /* mixture: indices of its two materials in rb_scene_desc.materials */
+	float amount[3];            /* mixture: the weight of components[0] (mixture_material's alpha) */
+	/* 0: the constant spectrum above; k > 0: image texture rb_scene_desc.textures[k - 1] instead
+	 * (for the spectra the material reads; not inside a mixture) */
+	uint32_t diffuse_texture;
+	uint32_t reflectance_texture;
+	uint32_t transmission_texture;
+	uint32_t specular_texture;
+	uint32_t opacity_texture;
 } rb_material_desc;
 
 enum {
@@ -195,6 +220,9 @@ typedef struct rb_scene_desc {
 	uint32_t num_mediums;
 	uint32_t num_media;
 	const rb_media_desc* media;
+	const rb_texture_desc* textures;  /* image textures that materials refer to (*_texture fields) */
+	uint32_t num_textures;
+	uint32_t reserved;
 } rb_scene_desc;
 
 /* Pinhole / thin-lens perspective camera: rainbow-cpu/cameras/perspective_camera.cpp:78-99.

@@ -88,4 +88,40 @@ int adp_export(orc_scene* s, float* nodes, uint32_t* prim_entity, uint32_t* prim
 	return st;
 }
 
+// The adapter's material list of a harness scene (sizes first with NULL
+// arrays) and each entity's index into it (-1: none).
+int adp_export_materials(orc_scene* s, rb_material_desc* materials, uint32_t* count, int32_t* entity_material,
+	uint32_t* num_entities) {
+	std::shared_ptr<scenes::scene> world;
+	std::shared_ptr<cameras::camera> cam;
+	if (!objects(s, world, cam)) return RB_ERR_INVALID_ARGUMENT;
+	rb::adapter::exported_scene ex;
+	const rb_status st = rb::adapter::export_scene(*world, ex);
+	if (st != RB_OK) return st;
+	*count = static_cast<uint32_t>(ex.materials.size());
+	*num_entities = static_cast<uint32_t>(ex.entities.size());
+	if (materials != nullptr) {
+		for (size_t k = 0; k < ex.materials.size(); k++) materials[k] = ex.materials[k];
+		for (size_t e = 0; e < ex.entities.size(); e++) entity_material[e] = ex.entities[e].material;
+	}
+	return RB_OK;
+}
+
+// Texture t of the adapter's export of a harness scene: its size (and the
+// number of textures) first with rgb NULL, then its texels.
+int adp_export_texture(orc_scene* s, uint32_t t, float* rgb, uint32_t* width, uint32_t* height, uint32_t* count) {
+	std::shared_ptr<scenes::scene> world;
+	std::shared_ptr<cameras::camera> cam;
+	if (!objects(s, world, cam)) return RB_ERR_INVALID_ARGUMENT;
+	rb::adapter::exported_scene ex;
+	const rb_status st = rb::adapter::export_scene(*world, ex);
+	if (st != RB_OK) return st;
+	*count = static_cast<uint32_t>(ex.textures.size());
+	if (t >= ex.textures.size()) return RB_OK;
+	*width = ex.textures[t].width;
+	*height = ex.textures[t].height;
+	if (rgb != nullptr) std::memcpy(rgb, ex.textures[t].rgb, 3ull * *width * *height * sizeof(float));
+	return RB_OK;
+}
+
 } // extern "C"

@@ -28,6 +28,7 @@
 #include "rainbow-cpu/shapes/mesh.hpp"
 #include "rainbow-cpu/materials/matte_material.hpp"
 #include "rainbow-cpu/materials/metal_material.hpp"
+#include "rainbow-cpu/materials/mixture_material.hpp"
 #include "rainbow-cpu/materials/glass_material.hpp"
 #include "rainbow-cpu/materials/mirror_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
@@ -37,6 +38,8 @@
 #include "rainbow-cpu/emitters/surface_light.hpp"
 #include "rainbow-cpu/emitters/environment_light.hpp"
 #include "rainbow-cpu/textures/constant_texture.hpp"
+#include "texture_lookup.hpp"  // before the image texture definitions (shim/)
+#include "rainbow-cpu/textures/image_texture.hpp"
 #include "rainbow-cpu/shared/accelerators/bounding_volume_hierarchy.hpp"
 #include "rainbow-core/sample_function.hpp"
 
@@ -127,29 +130,70 @@ std::shared_ptr<constant_texture2d<real>> real_texture(float v) {
 	return std::make_shared<constant_texture2d<real>>(v);
 }
 
-std::shared_ptr<material> make_material(const rb_material_desc& m) {
+// The scene's image textures as reference image_texture2d<spectrum>s, made once
+// each (materials that name the same texture share it).
+struct texture_set {
+	const rb_texture_desc* descs = nullptr;
+	uint32_t count = 0;
+	std::vector<std::shared_ptr<texture2d<spectrum>>> made;
+	// a constant texture of v, or with ref > 0 the image texture ref - 1
+	std::shared_ptr<texture2d<spectrum>> spectrum_of(const float* v, uint32_t ref) {
+		if (ref == 0) return spectrum_texture(v);
+		if (ref > count) return nullptr;
+		if (made.size() < count) made.resize(count);
+		auto& t = made[ref - 1];
+		if (!t) {
+			const rb_texture_desc& d = descs[ref - 1];
+			std::vector<spectrum> values;
+			values.reserve(static_cast<size_t>(d.width) * d.height);
+			for (size_t i = 0; i < static_cast<size_t>(d.width) * d.height; i++)
+				values.emplace_back(d.rgb[3 * i], d.rgb[3 * i + 1], d.rgb[3 * i + 2]);
+			t = std::make_shared<image_texture2d<spectrum>>(rainbow::core::math::vector_t<2, size_t>(d.width, d.height), values);
+		}
+		return t;
+	}
+};
+
+// Material k of the array `all` (count entries); a mixture's components are
+// indices into the same array (nesting up to 8 deep).
+std::shared_ptr<material> make_material(const rb_material_desc* all, uint32_t count, uint32_t k, texture_set& tex,
+	int depth = 0) {
+	if (k >= count || depth > 8) return nullptr;
+	const rb_material_desc& m = all[k];
+	const auto diffuse = tex.spectrum_of(m.diffuse, m.diffuse_texture);
+	const auto reflectance = tex.spectrum_of(m.reflectance, m.reflectance_texture);
+	const auto transmission = tex.spectrum_of(m.transmission, m.transmission_texture);
+	const auto specular = tex.spectrum_of(m.specular, m.specular_texture);
+	const auto opacity = tex.spectrum_of(m.opacity, m.opacity_texture);
+	if (!diffuse || !reflectance || !transmission || !specular || !opacity) return nullptr;
 	switch (m.kind) {
-	case RB_MATERIAL_MATTE: return std::make_shared<matte_material>(spectrum_texture(m.diffuse), real_texture(m.sigma));
+	case RB_MATERIAL_MATTE: return std::make_shared<matte_material>(diffuse, real_texture(m.sigma));
 	case RB_MATERIAL_METAL:
 		return std::make_shared<metal_material>(spectrum_texture(m.eta), spectrum_texture(m.k), real_texture(m.roughness_u),
 			real_texture(m.roughness_v), m.remap_roughness != 0);
 	case RB_MATERIAL_GLASS:
-		return std::make_shared<glass_material>(spectrum_texture(m.reflectance), spectrum_texture(m.transmission),
-			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
+		return std::make_shared<glass_material>(reflectance, transmission, real_texture(m.roughness_u),
+			real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
 	case RB_MATERIAL_PLASTIC:
-		return std::make_shared<plastic_material>(spectrum_texture(m.reflectance), spectrum_texture(m.diffuse),
-			real_texture(m.roughness_u), real_texture(m.ior), m.remap_roughness != 0);
-	case RB_MATERIAL_MIRROR: return std::make_shared<mirror_material>(spectrum_texture(m.reflectance));
+		return std::make_shared<plastic_material>(reflectance, diffuse, real_texture(m.roughness_u), real_texture(m.ior),
+			m.remap_roughness != 0);
+	case RB_MATERIAL_MIRROR: return std::make_shared<mirror_material>(reflectance);
 	case RB_MATERIAL_SUBSTRATE:
-		return std::make_shared<substrate_material>(spectrum_texture(m.reflectance), spectrum_texture(m.diffuse),
-			real_texture(m.roughness_u), real_texture(m.roughness_v), m.remap_roughness != 0);
+		return std::make_shared<substrate_material>(reflectance, diffuse, real_texture(m.roughness_u),
+			real_texture(m.roughness_v), m.remap_roughness != 0);
 	case RB_MATERIAL_UBER:
-		return std::make_shared<uber_material>(spectrum_texture(m.transmission), spectrum_texture(m.reflectance),
-			spectrum_texture(m.specular), spectrum_texture(m.diffuse), spectrum_texture(m.opacity),
+		return std::make_shared<uber_material>(transmission, reflectance, specular, diffuse, opacity,
 			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
 	case RB_MATERIAL_TRANSLUCENT:
-		return std::make_shared<translucent_material>(spectrum_texture(m.transmission), spectrum_texture(m.reflectance),
-			spectrum_texture(m.specular), spectrum_texture(m.diffuse), real_texture(m.roughness_u), m.remap_roughness != 0);
+		return std::make_shared<translucent_material>(transmission, reflectance, specular, diffuse,
+			real_texture(m.roughness_u), m.remap_roughness != 0);
+	case RB_MATERIAL_MIXTURE: {
+		if (m.components[0] < 0 || m.components[1] < 0) return nullptr;
+		const auto m0 = make_material(all, count, static_cast<uint32_t>(m.components[0]), tex, depth + 1);
+		const auto m1 = make_material(all, count, static_cast<uint32_t>(m.components[1]), tex, depth + 1);
+		if (!m0 || !m1) return nullptr;
+		return std::make_shared<mixture_material>(spectrum_texture(m.amount), m0, m1);
+	}
 	default: return nullptr;
 	}
 }
@@ -221,7 +265,9 @@ int orc_scene_build(const rb_scene_desc* desc, const rb_camera_desc* cam, orc_sc
 			to_vec3(m.normals, m.num_vertices), to_vec3(m.uvs, m.num_vertices), idx, m.reverse_orientation != 0));
 	}
 	std::vector<std::shared_ptr<material>> materials;
-	for (uint32_t i = 0; i < desc->num_materials; i++) materials.push_back(make_material(desc->materials[i]));
+	texture_set tex{desc->textures, desc->num_textures, {}};
+	for (uint32_t i = 0; i < desc->num_materials; i++)
+		materials.push_back(make_material(desc->materials, desc->num_materials, i, tex));
 	std::vector<std::shared_ptr<emitter>> emitter_list;
 	for (uint32_t i = 0; i < desc->num_emitters; i++) {
 		const rb_emitter_desc& e = desc->emitters[i];
@@ -655,12 +701,31 @@ int orc_pcg32(uint64_t seed, uint32_t n, uint32_t* u32, float* reals) {
 	return RB_OK;
 }
 
+// image_texture2d<spectrum>(size, texels).sample(uv) for n texture coordinates.
+int orc_texture_sample(const float* rgb, uint32_t width, uint32_t height, uint32_t n, const float* uv, float* out) {
+	if (rgb == nullptr || width == 0 || height == 0) return RB_ERR_INVALID_ARGUMENT;
+	rb_texture_desc d{rgb, width, height};
+	texture_set tex{&d, 1u, {}};
+	const float zero[3] = {0.f, 0.f, 0.f};
+	const auto t = tex.spectrum_of(zero, 1u);
+	for (uint32_t i = 0; i < n; i++) {
+		const auto v = t->sample(vector2(uv[2 * i], uv[2 * i + 1]));
+		out[3 * i] = v[0];
+		out[3 * i + 1] = v[1];
+		out[3 * i + 2] = v[2];
+	}
+	return RB_OK;
+}
+
 // BSDF known answers on the shading frame = world axes: for each (wo, u)
 // scattering_function_collection::sample(interaction, u, include); for each
 // (wo, wi) evaluate and pdf with `include`.
-int orc_bsdf(const rb_material_desc* m, uint32_t n, const float* wo, const float* u, const float* wi_eval, uint32_t include,
-	float* wi_out, float* f_out, float* pdf_out, uint32_t* type_out, float* f_eval, float* pdf_eval) {
-	const auto mat = make_material(*m);
+// m[0] is the material; a mixture's components index m[0 .. num_materials).
+int orc_bsdf(const rb_material_desc* m, uint32_t num_materials, uint32_t n, const float* wo, const float* u,
+	const float* wi_eval, uint32_t include, float* wi_out, float* f_out, float* pdf_out, uint32_t* type_out, float* f_eval,
+	float* pdf_eval) {
+	texture_set tex;
+	const auto mat = make_material(m, num_materials, 0, tex);
 	if (!mat) return RB_ERR_INVALID_ARGUMENT;
 	for (uint32_t i = 0; i < n; i++) {
 		surface_interaction si;

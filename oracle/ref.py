@@ -45,7 +45,8 @@ def lib():
             "orc_render": (i32, [vp, u32, u32, u32, f32, u32, i32, i32, i32, vp, vp, C.POINTER(C.c_double)]),
             "orc_render_shipped": (i32, [vp, u32, u32, f32, vp, C.POINTER(C.c_double)]),
             "orc_pcg32": (i32, [C.c_uint64, u32, vp, vp]),
-            "orc_bsdf": (i32, [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
+            "orc_bsdf": (i32, [vp, u32, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
+            "orc_texture_sample": (i32, [vp, u32, u32, u32, vp, vp]),
             "orc_set_volume": (None, [vp, i32]),
             "orc_set_direct": (None, [vp, C.c_uint32, C.c_uint32]),
             "orc_film_read": (i32, [vp, vp]),
@@ -199,16 +200,29 @@ def pcg32(seed, n):
 
 
 def bsdf(material, wo, u, wi_eval, include):
-    """scattering_function_collection sample / evaluate / pdf for one material."""
+    """scattering_function_collection sample / evaluate / pdf for one material
+    (a descriptor, or a ctypes array of descriptors whose first entry is the
+    material and whose other entries are a mixture's components)."""
+    count = len(material) if isinstance(material, C.Array) else 1
     n = wo.shape[0]
     wo = np.ascontiguousarray(wo, dtype=np.float32)
     u = np.ascontiguousarray(u, dtype=np.float32)
     wie = np.ascontiguousarray(wi_eval, dtype=np.float32)
     out = dict(wi=np.zeros((n, 3), np.float32), f=np.zeros((n, 3), np.float32), pdf=np.zeros(n, np.float32),
                type=np.zeros(n, np.uint32), f_eval=np.zeros((n, 3), np.float32), pdf_eval=np.zeros(n, np.float32))
-    _ok(lib().orc_bsdf(C.byref(material), n, wo.ctypes.data, u.ctypes.data, wie.ctypes.data, include,
+    _ok(lib().orc_bsdf(C.byref(material), count, n, wo.ctypes.data, u.ctypes.data, wie.ctypes.data, include,
                        out["wi"].ctypes.data, out["f"].ctypes.data, out["pdf"].ctypes.data, out["type"].ctypes.data,
                        out["f_eval"].ctypes.data, out["pdf_eval"].ctypes.data), "orc_bsdf")
+    return out
+
+
+def texture_sample(image, uv):
+    """image_texture2d<spectrum>::sample at each uv of an (height, width, 3) image."""
+    img = np.ascontiguousarray(image, dtype=np.float32)
+    uv = np.ascontiguousarray(uv, dtype=np.float32)
+    out = np.zeros((uv.shape[0], 3), np.float32)
+    _ok(lib().orc_texture_sample(img.ctypes.data, img.shape[1], img.shape[0], uv.shape[0], uv.ctypes.data,
+                                 out.ctypes.data), "orc_texture_sample")
     return out
 
 
@@ -231,6 +245,10 @@ def adapter_lib():
         L.adp_render.restype, L.adp_render.argtypes = i32, [vp, u32, u32, f32, u32, C.c_char_p, u32]
         L.adp_export.restype = i32
         L.adp_export.argtypes = [vp, vp, vp, vp, C.POINTER(u32), C.POINTER(u32), vp, vp, vp, vp]
+        L.adp_export_materials.restype = i32
+        L.adp_export_materials.argtypes = [vp, vp, C.POINTER(u32), vp, C.POINTER(u32)]
+        L.adp_export_texture.restype = i32
+        L.adp_export_texture.argtypes = [vp, u32, vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
         _ADAPTER = L
     return _ADAPTER
 
@@ -243,6 +261,31 @@ def adapter_render(R, spp, max_depth=5, threshold=1.0, seed=0):
     if st != 0:
         raise RuntimeError(f"wavefront_path_integrator::render failed ({st}): {err.value.decode()}")
     return R.film()
+
+
+def adapter_export_materials(R, material_type):
+    """The adapter's exported material list of R's reference scene and each entity's index into it."""
+    L = adapter_lib()
+    n, ne = C.c_uint32(), C.c_uint32()
+    _ok(L.adp_export_materials(R.h, None, C.byref(n), None, C.byref(ne)), "adp_export_materials")
+    mats = (material_type * max(1, n.value))()
+    ent = np.zeros(max(1, ne.value), dtype=np.int32)
+    _ok(L.adp_export_materials(R.h, C.addressof(mats), C.byref(n), ent.ctypes.data, C.byref(ne)), "adp_export_materials")
+    return mats, ent[:ne.value]
+
+
+def adapter_export_textures(R):
+    """The adapter's exported image textures of R's reference scene, as (height, width, 3) arrays in export order."""
+    L = adapter_lib()
+    w, h, n = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    _ok(L.adp_export_texture(R.h, 0, None, C.byref(w), C.byref(h), C.byref(n)), "adp_export_texture")
+    out = []
+    for t in range(n.value):
+        _ok(L.adp_export_texture(R.h, t, None, C.byref(w), C.byref(h), C.byref(n)), "adp_export_texture")
+        a = np.zeros((h.value, w.value, 3), dtype=np.float32)
+        _ok(L.adp_export_texture(R.h, t, a.ctypes.data, C.byref(w), C.byref(h), C.byref(n)), "adp_export_texture")
+        out.append(a)
+    return out
 
 
 def adapter_export(R, material_type, emitter_type, camera_type):

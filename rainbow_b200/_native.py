@@ -25,6 +25,7 @@ RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_GLASS, RB_MATERIAL_PLASTIC, RB
 RB_MATERIAL_SUBSTRATE = 5
 RB_MATERIAL_UBER = 6
 RB_MATERIAL_TRANSLUCENT = 7
+RB_MATERIAL_MIXTURE = 8
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
 RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM, RB_SCENE_FOG = 0, 1, 2, 3
 RB_RENDER_RESET = 1
@@ -56,7 +57,14 @@ class MeshDesc(C.Structure):
 class MaterialDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("remap_roughness", C.c_int32), ("diffuse", F3), ("sigma", C.c_float),
                 ("eta", F3), ("k", F3), ("reflectance", F3), ("transmission", F3), ("ior", C.c_float),
-                ("roughness_u", C.c_float), ("roughness_v", C.c_float), ("specular", F3), ("opacity", F3)]
+                ("roughness_u", C.c_float), ("roughness_v", C.c_float), ("specular", F3), ("opacity", F3),
+                ("components", C.c_int32 * 2), ("amount", F3), ("diffuse_texture", C.c_uint32),
+                ("reflectance_texture", C.c_uint32), ("transmission_texture", C.c_uint32),
+                ("specular_texture", C.c_uint32), ("opacity_texture", C.c_uint32)]
+
+
+class TextureDesc(C.Structure):
+    _fields_ = [("rgb", C.POINTER(C.c_float)), ("width", C.c_uint32), ("height", C.c_uint32)]
 
 
 class MediumDesc(C.Structure):
@@ -86,7 +94,8 @@ class SceneDesc(C.Structure):
                 ("entities", C.POINTER(EntityDesc)), ("materials", C.POINTER(MaterialDesc)),
                 ("num_materials", C.c_uint32), ("num_emitters", C.c_uint32), ("emitters", C.POINTER(EmitterDesc)),
                 ("bvh", BvhDesc), ("mediums", C.POINTER(MediumDesc)), ("num_mediums", C.c_uint32),
-                ("num_media", C.c_uint32), ("media", C.POINTER(MediaDesc))]
+                ("num_media", C.c_uint32), ("media", C.POINTER(MediaDesc)), ("textures", C.POINTER(TextureDesc)),
+                ("num_textures", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class CameraDesc(C.Structure):

@@ -18,6 +18,7 @@
 #include "rainbow-cpu/materials/matte_material.hpp"
 #include "rainbow-cpu/materials/metal_material.hpp"
 #include "rainbow-cpu/materials/mirror_material.hpp"
+#include "rainbow-cpu/materials/mixture_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
 #include "rainbow-cpu/materials/substrate_material.hpp"
 #include "rainbow-cpu/materials/translucent_material.hpp"
@@ -25,7 +26,19 @@
 #include "rainbow-cpu/media/homogeneous_medium.hpp"
 #include "rainbow-cpu/shapes/mesh.hpp"
 #include "rainbow-cpu/textures/constant_texture.hpp"
+#include "rainbow-cpu/textures/texture.hpp"
 
+// image_texture_t<2, T>::sample (textures/detail/image_texture.hpp:65-66) calls
+// clamp(float, real, real) unqualified; under standard two-phase lookup (g++)
+// the spectrum clamp made visible by a using-directive hides the scalar one of
+// rainbow-core, so the reference's header only compiles with the scalar clamp
+// declared in the textures namespace first. It changes nothing the header computes.
+namespace rainbow::cpus::textures {
+using rainbow::core::math::clamp;
+}
+#include "rainbow-cpu/textures/image_texture.hpp"
+
+#include <functional>
 #include <unordered_map>
 
 using namespace rainbow::cpus;
@@ -87,6 +100,8 @@ RB_PRIVATE_MEMBER(translucent_specular, materials::translucent_material::mSpecul
 RB_PRIVATE_MEMBER(translucent_diffuse, materials::translucent_material::mDiffuse);
 RB_PRIVATE_MEMBER(translucent_roughness, materials::translucent_material::mRoughness);
 RB_PRIVATE_MEMBER(translucent_remap, materials::translucent_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(mixture_alpha, materials::mixture_material::mAlpha);
+RB_PRIVATE_MEMBER(mixture_materials, materials::mixture_material::mMaterials);
 RB_PRIVATE_MEMBER(surface_radiance, emitters::surface_light::mRadiance);
 RB_PRIVATE_MEMBER(environment_map, emitters::environment_light::mEnvironmentMap);
 RB_PRIVATE_MEMBER(environment_intensity, emitters::environment_light::mIntensity);
@@ -128,12 +143,52 @@ void put_matrix(const rainbow::core::math::matrix4x4& m, float* out) {
 		for (int r = 0; r < 4; r++) out[c * 4 + r] = m[c][r];
 }
 
-rb_status export_material(const std::shared_ptr<materials::material>& m, rb_material_desc& d) {
+// The scene's image textures (image_texture2d<spectrum>), each exported once.
+struct texture_registry {
+	exported_scene& out;
+	std::unordered_map<const void*, uint32_t> ref_of;
+	// A spectrum parameter: a constant texture's value in rgb (ref 0), or an
+	// image texture's reference (index + 1 into out.textures); false for
+	// other textures.
+	bool spectrum(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, float* rgb, uint32_t& ref) {
+		ref = 0;
+		if (constant_rgb(t, rgb)) return true;
+		const auto img = std::dynamic_pointer_cast<textures::image_texture2d<shared::spectrums::spectrum>>(t);
+		if (img == nullptr) return false;
+		const auto it = ref_of.find(img.get());
+		if (it != ref_of.end()) {
+			ref = it->second;
+			return true;
+		}
+		const auto size = img->size();
+		if (size.x == 0 || size.y == 0 || size.x > (1u << 15) || size.y > (1u << 15)) return false;
+		std::vector<float> texels(3 * size.x * size.y);
+		for (size_t i = 0; i < size.x * size.y; i++) {
+			const auto v = img->value(i);
+			texels[3 * i] = v[0];
+			texels[3 * i + 1] = v[1];
+			texels[3 * i + 2] = v[2];
+		}
+		out.texels.push_back(std::move(texels));
+		rb_texture_desc td{};
+		td.width = static_cast<uint32_t>(size.x);
+		td.height = static_cast<uint32_t>(size.y);
+		out.textures.push_back(td);
+		ref = static_cast<uint32_t>(out.textures.size());
+		ref_of.emplace(img.get(), ref);
+		return true;
+	}
+};
+
+rb_status export_material(const std::shared_ptr<materials::material>& m, rb_material_desc& d, texture_registry& tex) {
 	d = rb_material_desc{};
 	bool ok = true;
+	// a spectrum parameter that may be an image texture
+	const auto spec = [&](const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, float* rgb,
+		uint32_t& ref) { return tex.spectrum(t, rgb, ref); };
 	if (const auto x = std::dynamic_pointer_cast<materials::matte_material>(m)) {
 		d.kind = RB_MATERIAL_MATTE;
-		ok = constant_rgb(read(*x, matte_diffuse{}), d.diffuse) && constant_real(read(*x, matte_sigma{}), d.sigma);
+		ok = spec(read(*x, matte_diffuse{}), d.diffuse, d.diffuse_texture) && constant_real(read(*x, matte_sigma{}), d.sigma);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::metal_material>(m)) {
 		d.kind = RB_MATERIAL_METAL;
 		d.remap_roughness = read(*x, metal_remap{}) ? 1 : 0;
@@ -142,45 +197,47 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 	} else if (const auto x = std::dynamic_pointer_cast<materials::glass_material>(m)) {
 		d.kind = RB_MATERIAL_GLASS;
 		d.remap_roughness = read(*x, glass_remap{}) ? 1 : 0;
-		ok = constant_rgb(read(*x, glass_reflectance{}), d.reflectance) &&
-			constant_rgb(read(*x, glass_transmission{}), d.transmission) &&
+		ok = spec(read(*x, glass_reflectance{}), d.reflectance, d.reflectance_texture) &&
+			spec(read(*x, glass_transmission{}), d.transmission, d.transmission_texture) &&
 			constant_real(read(*x, glass_ru{}), d.roughness_u) && constant_real(read(*x, glass_rv{}), d.roughness_v) &&
 			constant_real(read(*x, glass_eta{}), d.ior);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::plastic_material>(m)) {
 		d.kind = RB_MATERIAL_PLASTIC;
 		d.remap_roughness = read(*x, plastic_remap{}) ? 1 : 0;
-		ok = constant_rgb(read(*x, plastic_specular{}), d.reflectance) && constant_rgb(read(*x, plastic_diffuse{}), d.diffuse) &&
+		ok = spec(read(*x, plastic_specular{}), d.reflectance, d.reflectance_texture) &&
+			spec(read(*x, plastic_diffuse{}), d.diffuse, d.diffuse_texture) &&
 			constant_real(read(*x, plastic_roughness{}), d.roughness_u) && constant_real(read(*x, plastic_eta{}), d.ior);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::mirror_material>(m)) {
 		d.kind = RB_MATERIAL_MIRROR;
-		ok = constant_rgb(read(*x, mirror_reflectance{}), d.reflectance);
+		ok = spec(read(*x, mirror_reflectance{}), d.reflectance, d.reflectance_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::substrate_material>(m)) {
 		d.kind = RB_MATERIAL_SUBSTRATE;
 		d.remap_roughness = read(*x, substrate_remap{}) ? 1 : 0;
-		ok = constant_rgb(read(*x, substrate_specular{}), d.reflectance) &&
-			constant_rgb(read(*x, substrate_diffuse{}), d.diffuse) && constant_real(read(*x, substrate_ru{}), d.roughness_u) &&
+		ok = spec(read(*x, substrate_specular{}), d.reflectance, d.reflectance_texture) &&
+			spec(read(*x, substrate_diffuse{}), d.diffuse, d.diffuse_texture) && constant_real(read(*x, substrate_ru{}), d.roughness_u) &&
 			constant_real(read(*x, substrate_rv{}), d.roughness_v);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::uber_material>(m)) {
 		d.kind = RB_MATERIAL_UBER;
 		d.remap_roughness = read(*x, uber_remap{}) ? 1 : 0;
-		ok = constant_rgb(read(*x, uber_transmission{}), d.transmission) &&
-			constant_rgb(read(*x, uber_reflectance{}), d.reflectance) && constant_rgb(read(*x, uber_specular{}), d.specular) &&
-			constant_rgb(read(*x, uber_diffuse{}), d.diffuse) && constant_rgb(read(*x, uber_opacity{}), d.opacity) &&
+		ok = spec(read(*x, uber_transmission{}), d.transmission, d.transmission_texture) &&
+			spec(read(*x, uber_reflectance{}), d.reflectance, d.reflectance_texture) &&
+			spec(read(*x, uber_specular{}), d.specular, d.specular_texture) &&
+			spec(read(*x, uber_diffuse{}), d.diffuse, d.diffuse_texture) && spec(read(*x, uber_opacity{}), d.opacity, d.opacity_texture) &&
 			constant_real(read(*x, uber_ru{}), d.roughness_u) && constant_real(read(*x, uber_rv{}), d.roughness_v) &&
 			constant_real(read(*x, uber_eta{}), d.ior);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::translucent_material>(m)) {
 		d.kind = RB_MATERIAL_TRANSLUCENT;
 		d.remap_roughness = read(*x, translucent_remap{}) ? 1 : 0;
-		ok = constant_rgb(read(*x, translucent_transmission{}), d.transmission) &&
-			constant_rgb(read(*x, translucent_reflectance{}), d.reflectance) &&
-			constant_rgb(read(*x, translucent_specular{}), d.specular) &&
-			constant_rgb(read(*x, translucent_diffuse{}), d.diffuse) &&
+		ok = spec(read(*x, translucent_transmission{}), d.transmission, d.transmission_texture) &&
+			spec(read(*x, translucent_reflectance{}), d.reflectance, d.reflectance_texture) &&
+			spec(read(*x, translucent_specular{}), d.specular, d.specular_texture) &&
+			spec(read(*x, translucent_diffuse{}), d.diffuse, d.diffuse_texture) &&
 			constant_real(read(*x, translucent_roughness{}), d.roughness_u);
 		d.roughness_v = d.roughness_u;
 	} else {
-		return RB_ERR_UNSUPPORTED;  // mixture, subsurface
+		return RB_ERR_UNSUPPORTED;  // subsurface (a mixture is exported by export_scene)
 	}
-	return ok ? RB_OK : RB_ERR_UNSUPPORTED;  // a texture that is not constant
+	return ok ? RB_OK : RB_ERR_UNSUPPORTED;  // a texture that is neither constant nor an RGB image
 }
 
 rb_status export_emitter(const std::shared_ptr<emitters::emitter>& e, rb_emitter_desc& d) {
@@ -216,6 +273,35 @@ std::vector<float> flat(const std::vector<T>& v) {
 rb_status export_scene(const scenes::scene& s, exported_scene& out) {
 	out = exported_scene();
 	std::unordered_map<const void*, int32_t> mesh_of, material_of, medium_of;
+	texture_registry tex{out, {}};
+	// a material's index in out.materials, exported on first use; a mixture's
+	// two materials are exported before it (mixture_material.hpp: mAlpha, mMaterials)
+	std::function<rb_status(const std::shared_ptr<materials::material>&, int, int32_t&)> material_index =
+		[&](const std::shared_ptr<materials::material>& mat, int depth, int32_t& index) -> rb_status {
+		if (mat == nullptr || depth > 8) return RB_ERR_UNSUPPORTED;
+		const auto it = material_of.find(mat.get());
+		if (it != material_of.end()) {
+			index = it->second;
+			return RB_OK;
+		}
+		rb_material_desc md{};
+		if (const auto x = std::dynamic_pointer_cast<materials::mixture_material>(mat)) {
+			md.kind = RB_MATERIAL_MIXTURE;
+			if (!constant_rgb(read(*x, mixture_alpha{}), md.amount)) return RB_ERR_UNSUPPORTED;
+			const auto& parts = read(*x, mixture_materials{});
+			for (int c = 0; c < 2; c++) {
+				const rb_status st = material_index(parts[c], depth + 1, md.components[c]);
+				if (st != RB_OK) return st;
+			}
+		} else {
+			const rb_status st = export_material(mat, md, tex);
+			if (st != RB_OK) return st;
+		}
+		out.materials.push_back(md);
+		index = static_cast<int32_t>(out.materials.size() - 1);
+		material_of.emplace(mat.get(), index);
+		return RB_OK;
+	};
 	try {
 		for (const auto& ent : s.entities()) {
 			rb_entity_desc ed{};
@@ -244,16 +330,8 @@ rb_status export_scene(const scenes::scene& s, exported_scene& out) {
 				ed.mesh = it->second;
 			}
 			if (ent->has_component<materials::material>()) {
-				const auto mat = ent->component<materials::material>();
-				auto it = material_of.find(mat.get());
-				if (it == material_of.end()) {
-					rb_material_desc md;
-					const rb_status st = export_material(mat, md);
-					if (st != RB_OK) return st;
-					out.materials.push_back(md);
-					it = material_of.emplace(mat.get(), static_cast<int32_t>(out.materials.size() - 1)).first;
-				}
-				ed.material = it->second;
+				const rb_status st = material_index(ent->component<materials::material>(), 0, ed.material);
+				if (st != RB_OK) return st;
 			}
 			if (ent->has_component<emitters::emitter>()) {
 				rb_emitter_desc em;
@@ -315,6 +393,9 @@ rb_status export_scene(const scenes::scene& s, exported_scene& out) {
 	d.num_mediums = static_cast<uint32_t>(out.mediums.size());
 	d.media = out.media.data();
 	d.num_media = static_cast<uint32_t>(out.media.size());
+	for (size_t t = 0; t < out.textures.size(); t++) out.textures[t].rgb = out.texels[t].data();
+	d.textures = out.textures.data();
+	d.num_textures = static_cast<uint32_t>(out.textures.size());
 	return RB_OK;
 }
 

@@ -5,9 +5,10 @@
 // the reference's own headers (the include root is the reference checkout).
 //
 // Supported, as the wavefront core renders them: triangle meshes without alpha
-// masks; matte, metal, glass, plastic, mirror and substrate materials with
-// constant textures; surface lights and constant environment lights;
-// homogeneous media. Anything else returns RB_ERR_UNSUPPORTED, so a caller can
+// masks; matte, metal, glass, plastic, mirror, substrate, uber, translucent and
+// mixture materials with constant textures, and RGB image textures for their
+// spectra (not inside a mixture); surface lights and constant environment
+// lights; homogeneous media. Anything else returns RB_ERR_UNSUPPORTED, so a caller can
 // fall back to the reference integrator for that scene.
 #pragma once
 
@@ -32,6 +33,8 @@ struct exported_scene {
 	std::vector<rb_emitter_desc> emitters;
 	std::vector<rb_medium_desc> mediums;
 	std::vector<rb_media_desc> media;
+	std::vector<std::vector<float>> texels;
+	std::vector<rb_texture_desc> textures;
 	rb_scene_desc desc{};  // valid while this object lives and is not copied
 };
 

@@ -662,6 +662,9 @@ rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
 	RB_CUDA(dev_upload(&d.environments, p.environments, c->stream));
 	RB_CUDA(dev_upload(&d.mediums, p.mediums, c->stream));
 	RB_CUDA(dev_upload(&d.media, p.media, c->stream));
+	RB_CUDA(dev_upload(&d.material_srcs, p.material_srcs, c->stream));
+	RB_CUDA(dev_upload(&d.textures, p.textures, c->stream));
+	RB_CUDA(dev_upload(&d.texels, p.texels, c->stream));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
 	pt::scene_view v{};
 	v.wnodes = p.wide_ok ? d.wnodes : nullptr;
@@ -679,6 +682,11 @@ rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
 	v.mediums = d.mediums;
 	v.media = d.media;
 	v.num_media = static_cast<uint32_t>(p.media.size());
+	v.instances = p.instances ? 1u : 0u;
+	v.material_srcs = d.material_srcs;
+	v.textures = d.textures;
+	v.texels = d.texels;
+	v.num_textures = static_cast<uint32_t>(p.textures.size());
 	c->view = v;
 	c->bvh_depth = p.bvh_depth;
 	c->num_entities = v.num_entities;

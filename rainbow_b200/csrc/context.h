@@ -72,11 +72,14 @@ struct device_scene {
 	int32_t* environments = nullptr;
 	pt::medium_rec* mediums = nullptr;
 	pt::media_rec* media = nullptr;
+	pt::material_src* material_srcs = nullptr;
+	pt::texture_rec* textures = nullptr;
+	float* texels = nullptr;
 	void release() {
 		dev_free(wnodes); dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
 		dev_free(entities); dev_free(meshes); dev_free(positions); dev_free(normals); dev_free(tangents); dev_free(uvs);
 		dev_free(indices); dev_free(materials); dev_free(emitters); dev_free(environments);
-		dev_free(mediums); dev_free(media);
+		dev_free(mediums); dev_free(media); dev_free(material_srcs); dev_free(textures); dev_free(texels);
 	}
 };
 

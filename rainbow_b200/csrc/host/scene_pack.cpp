@@ -12,6 +12,7 @@
 
 #include "../pt/pt_bsdf.h"
 #include "../pt/pt_geom.h"
+#include "../pt/pt_material.h"
 
 #include <cmath>
 #include <cstring>
@@ -23,61 +24,168 @@ namespace host {
 namespace {
 
 vec3 v3(const float* a, uint32_t i) { return vec3{a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
-bool black3(const float* c) { return c[0] == 0.f && c[1] == 0.f && c[2] == 0.f; }
-bool black(vec3 c) { return c.x == 0.f && c.y == 0.f && c.z == 0.f; }
-vec3 mul3(const float* a, const float* b) { return vec3{a[0] * b[0], a[1] * b[1], a[2] * b[2]}; }
 
-void layered_lobe(pt::material_rec& r, uint32_t kind, uint32_t type, vec3 spectrum, float eta = 1.f) {
-	r.lobe_kinds |= kind << (4u * r.lobe_count);
-	r.lobe_types |= type << (5u * r.lobe_count);
-	r.lobe_r[r.lobe_count] = spectrum;
-	r.lobe_eta[r.lobe_count] = eta;
-	r.lobe_count++;
-}
-
-// The lobe lists of uber_material::build_surface_properties (uber_material.cpp:26-75)
-// and translucent_material::build_surface_properties (translucent_material.cpp:23-69)
-// for constant textures, radiance transport: the same lobes, spectra and order.
-bool pack_layered(const rb_material_desc& md, pt::material_rec& r) {
-	using namespace pt;
-	r.kind = MAT_LAYERED;
-	if (md.kind == RB_MATERIAL_UBER) {
-		if (!(md.ior > 0.f)) return false;
-		const float eta = md.ior;
-		r.eta = r.collection_eta = eta;
-		r.alpha_x = md.remap_roughness ? roughness_to_alpha(md.roughness_u) : md.roughness_u;
-		r.alpha_y = md.remap_roughness ? roughness_to_alpha(md.roughness_v) : md.roughness_v;
-		const vec3 reflectance = mul3(md.opacity, md.reflectance);
-		const vec3 transmission = mul3(md.opacity, md.transmission);
-		const vec3 specular = mul3(md.opacity, md.specular);
-		const vec3 diffuse = mul3(md.opacity, md.diffuse);
-		// clamp(spectrum(1) - opacity) to [0, 1]
-		vec3 invert;
-		invert.x = fclamp_ref(1.f - md.opacity[0], 0.f, 1.f);
-		invert.y = fclamp_ref(1.f - md.opacity[1], 0.f, 1.f);
-		invert.z = fclamp_ref(1.f - md.opacity[2], 0.f, 1.f);
-		if (!black(invert)) layered_lobe(r, LOBE_L_SPECULAR_TRANSMIT, ST_SPECULAR | ST_TRANSMISSION, invert, 1.f);
-		if (!black(diffuse)) layered_lobe(r, LOBE_L_LAMBERT, ST_DIFFUSE | ST_REFLECTION, diffuse);
-		if (!black(specular)) layered_lobe(r, LOBE_L_MF_REFLECT, ST_GLOSSY | ST_REFLECTION, specular);
-		if (!black(reflectance)) layered_lobe(r, LOBE_L_SPECULAR_REFLECT, ST_SPECULAR | ST_REFLECTION, reflectance);
-		if (!black(transmission)) layered_lobe(r, LOBE_L_SPECULAR_TRANSMIT, ST_SPECULAR | ST_TRANSMISSION, transmission, eta);
+// A material's parameters with what only the host computes applied:
+// trowbridge_reitz_distribution::roughness_to_alpha where the material maps
+// roughness (trowbridge_reitz_distribution.cpp:128-137), the sigma clamp and
+// oren_nayar_reflection's A and B (oren_nayar_reflection.cpp:5-16: radians in
+// float, then A and B in double, rounded to float). False for parameters the
+// reference material would not take (an IOR that is not positive).
+bool make_src(const rb_material_desc& md, pt::material_src& p) {
+	p = pt::material_src{};
+	p.kind = md.kind;
+	const auto alpha = [&](float r) { return md.remap_roughness ? pt::roughness_to_alpha(r) : r; };
+	p.diffuse = v3(md.diffuse, 0);
+	p.reflectance = v3(md.reflectance, 0);
+	p.transmission = v3(md.transmission, 0);
+	p.specular = v3(md.specular, 0);
+	p.opacity = v3(md.opacity, 0);
+	p.ior = md.ior;
+	p.tex[pt::TEX_DIFFUSE] = md.diffuse_texture;
+	p.tex[pt::TEX_REFLECTANCE] = md.reflectance_texture;
+	p.tex[pt::TEX_TRANSMISSION] = md.transmission_texture;
+	p.tex[pt::TEX_SPECULAR] = md.specular_texture;
+	p.tex[pt::TEX_OPACITY] = md.opacity_texture;
+	switch (md.kind) {
+	case RB_MATERIAL_MATTE: {
+		const float sigma = fclamp_ref(md.sigma, 0.f, 90.f);
+		if (sigma != 0.f) {
+			p.oren_nayar = 1u;
+			const float sr = sigma * 0.01745329251994329576923690768489f;
+			const float s2 = sr * sr;
+			p.on_a = static_cast<float>(1. - (s2 / (2 * (s2 + 0.33))));
+			p.on_b = static_cast<float>(0.45 * s2 / (s2 + 0.09));
+		}
 		return true;
 	}
-	// translucent: IOR 1.5, one isotropic roughness
-	const float eta = 1.5f;
-	r.eta = r.collection_eta = eta;
-	r.alpha_x = r.alpha_y = md.remap_roughness ? roughness_to_alpha(md.roughness_u) : md.roughness_u;
-	const bool has_r = !black3(md.reflectance), has_t = !black3(md.transmission);
-	if (!has_r && !has_t) return true;
-	if (!black3(md.diffuse)) {
-		if (has_r) layered_lobe(r, LOBE_L_LAMBERT, ST_DIFFUSE | ST_REFLECTION, mul3(md.diffuse, md.reflectance));
-		if (has_t) layered_lobe(r, LOBE_L_LAMBERT_TRANSMIT, ST_DIFFUSE | ST_TRANSMISSION, mul3(md.diffuse, md.transmission));
+	case RB_MATERIAL_METAL:
+		p.alpha_x = alpha(md.roughness_u);
+		p.alpha_y = alpha(md.roughness_v);
+		p.cond_eta = v3(md.eta, 0);
+		p.cond_k = v3(md.k, 0);
+		return true;
+	case RB_MATERIAL_GLASS:
+		p.smooth = (md.roughness_u == 0.f && md.roughness_v == 0.f) ? 1u : 0u;
+		if (!p.smooth) {
+			p.alpha_x = alpha(md.roughness_u);
+			p.alpha_y = alpha(md.roughness_v);
+		}
+		return true;
+	case RB_MATERIAL_PLASTIC:
+	case RB_MATERIAL_TRANSLUCENT:
+		if (md.kind == RB_MATERIAL_PLASTIC && !(md.ior > 0.f)) return false;
+		p.alpha_x = p.alpha_y = alpha(md.roughness_u);
+		return true;
+	case RB_MATERIAL_SUBSTRATE:
+	case RB_MATERIAL_UBER:
+		if (md.kind == RB_MATERIAL_UBER && !(md.ior > 0.f)) return false;
+		p.alpha_x = alpha(md.roughness_u);
+		p.alpha_y = alpha(md.roughness_v);
+		return true;
+	case RB_MATERIAL_MIRROR: return true;
+	default: return false;
 	}
-	if (!black3(md.specular)) {
-		if (has_r) layered_lobe(r, LOBE_L_MF_REFLECT, ST_GLOSSY | ST_REFLECTION, mul3(md.specular, md.reflectance));
-		if (has_t) layered_lobe(r, LOBE_L_MF_TRANSMIT, ST_GLOSSY | ST_TRANSMISSION, mul3(md.specular, md.transmission));
+}
+
+bool textured(const rb_material_desc& md) {
+	return md.diffuse_texture || md.reflectance_texture || md.transmission_texture || md.specular_texture ||
+		md.opacity_texture;
+}
+
+// One material's record (pt::build_record), or with `scale` its scaled build.
+rb_status pack_material(const rb_material_desc& md, const vec3* scale, pt::material_rec& r) {
+	pt::material_src p;
+	if (!make_src(md, p)) return RB_ERR_INVALID_ARGUMENT;
+	return pt::build_record(p, scale, r) ? RB_OK : RB_ERR_INVALID_ARGUMENT;
+}
+
+// A lobe of a mixture: the component record it lives in and its index there.
+struct mixture_lobe {
+	uint32_t record, local, kind, type;
+};
+
+// The lobes that material k contributes, built with `scale`, in collection
+// order; component records are appended to `records`. A mixture contributes
+// its two components' lobes (mixture_material.cpp:29-43): material0 with
+// alpha * scale, material1 with clamp(1 - alpha) * scale (without a scale,
+// alpha and clamp(1 - alpha)). Mixtures nest up to 8 deep.
+rb_status mixture_lobes(const rb_scene_desc* desc, uint32_t k, const vec3* scale, int depth,
+	std::vector<pt::material_rec>& records, std::vector<mixture_lobe>& lobes) {
+	const rb_material_desc& md = desc->materials[k];
+	if (md.kind == RB_MATERIAL_MIXTURE) {
+		if (depth >= 8) return RB_ERR_INVALID_ARGUMENT;
+		for (int c = 0; c < 2; c++)
+			if (md.components[c] < 0 || md.components[c] >= static_cast<int32_t>(desc->num_materials))
+				return RB_ERR_INVALID_ARGUMENT;
+		const vec3 alpha0 = v3(md.amount, 0);
+		vec3 alpha1;
+		alpha1.x = fclamp_ref(1.f - alpha0.x, 0.f, 1.f);
+		alpha1.y = fclamp_ref(1.f - alpha0.y, 0.f, 1.f);
+		alpha1.z = fclamp_ref(1.f - alpha0.z, 0.f, 1.f);
+		const vec3 s0 = scale ? alpha0 * *scale : alpha0;
+		const vec3 s1 = scale ? alpha1 * *scale : alpha1;
+		rb_status st = mixture_lobes(desc, static_cast<uint32_t>(md.components[0]), &s0, depth + 1, records, lobes);
+		if (st != RB_OK) return st;
+		return mixture_lobes(desc, static_cast<uint32_t>(md.components[1]), &s1, depth + 1, records, lobes);
 	}
-	return true;
+	if (textured(md)) return RB_ERR_UNSUPPORTED;  // a mixture's components are built once, on the host
+	pt::material_rec r;
+	const rb_status st = pack_material(md, scale, r);
+	if (st != RB_OK) return st;
+	const pt::bsdf_t b = pt::make_bsdf(&r);
+	if (b.count == 0) return RB_OK;
+	const uint32_t index = static_cast<uint32_t>(records.size());
+	records.push_back(r);
+	for (uint32_t i = 0; i < b.count; i++) lobes.push_back(mixture_lobe{index, i, pt::lobe_kind(b, i), pt::lobe_type(b, i)});
+	return RB_OK;
+}
+
+// Every material's record, in order, then the component records of mixtures;
+// a material with image-textured spectra gets a MAT_TEXTURED record and its
+// parameters in `srcs`.
+rb_status pack_materials(const rb_scene_desc* desc, std::vector<pt::material_rec>& out,
+	std::vector<pt::material_src>& srcs) {
+	const uint32_t n = desc->num_materials;
+	out.resize(n);
+	std::vector<pt::material_rec> components;
+	for (uint32_t k = 0; k < n; k++) {
+		const rb_material_desc& md = desc->materials[k];
+		if (md.kind != RB_MATERIAL_MIXTURE && textured(md)) {
+			pt::material_src p;
+			if (!make_src(md, p)) return RB_ERR_INVALID_ARGUMENT;
+			for (uint32_t t = 0; t < pt::kNumTexSlots; t++)
+				if (p.tex[t] > desc->num_textures) return RB_ERR_INVALID_ARGUMENT;
+			out[k] = pt::material_rec{};
+			out[k].kind = pt::MAT_TEXTURED;
+			out[k].src = static_cast<uint32_t>(srcs.size());
+			srcs.push_back(p);
+			continue;
+		}
+		if (md.kind != RB_MATERIAL_MIXTURE) {
+			const rb_status st = pack_material(md, nullptr, out[k]);
+			if (st != RB_OK) return st;
+			continue;
+		}
+		std::vector<pt::material_rec> recs;
+		std::vector<mixture_lobe> lobes;
+		const rb_status st = mixture_lobes(desc, k, nullptr, 0, recs, lobes);
+		if (st != RB_OK) return st;
+		if (lobes.size() > pt::kMaxLayeredLobes) return RB_ERR_UNSUPPORTED;
+		pt::material_rec& r = out[k];
+		r = pt::material_rec{};
+		r.kind = pt::MAT_MIXTURE;
+		r.blend_scale = vec3{1.f, 1.f, 1.f};
+		const uint32_t base = n + static_cast<uint32_t>(components.size());  // index of recs[0]
+		for (const mixture_lobe& l : lobes) {
+			r.lobe_kinds |= l.kind << (4u * r.lobe_count);
+			r.lobe_types |= l.type << (5u * r.lobe_count);
+			r.lobe_ref[r.lobe_count] = ((base + l.record - k) << 4) | l.local;
+			r.lobe_count++;
+		}
+		components.insert(components.end(), recs.begin(), recs.end());
+	}
+	out.insert(out.end(), components.begin(), components.end());
+	return RB_OK;
 }
 
 // distribution1d over n values (distributions/detail/distribution.hpp:48-77)
@@ -141,75 +249,23 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			}
 			out.meshes.push_back(r);
 		}
-		// ---- materials
-		for (uint32_t i = 0; i < desc->num_materials; i++) {
-			const rb_material_desc& md = desc->materials[i];
-			pt::material_rec r{};
-			switch (md.kind) {
-			case RB_MATERIAL_MATTE: {
-				const float sigma = fclamp_ref(md.sigma, 0.f, 90.f);
-				if (black3(md.diffuse)) r.kind = pt::MAT_BLACK;
-				else if (sigma != 0.f) {
-					// oren_nayar_reflection's constructor (oren_nayar_reflection.cpp:5-16):
-					// radians in float, then A and B in double, rounded to float
-					r.kind = pt::MAT_OREN_NAYAR;
-					const float sr = sigma * 0.01745329251994329576923690768489f;
-					const float s2 = sr * sr;
-					r.alpha_x = static_cast<float>(1. - (s2 / (2 * (s2 + 0.33))));
-					r.alpha_y = static_cast<float>(0.45 * s2 / (s2 + 0.09));
-				} else r.kind = pt::MAT_LAMBERT;
-				r.diffuse = vec3{md.diffuse[0], md.diffuse[1], md.diffuse[2]};
-				break;
-			}
-			case RB_MATERIAL_METAL:
-				r.kind = pt::MAT_METAL;
-				r.alpha_x = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_u) : md.roughness_u;
-				r.alpha_y = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_v) : md.roughness_v;
-				r.cond_eta = vec3{md.eta[0], md.eta[1], md.eta[2]};
-				r.cond_k = vec3{md.k[0], md.k[1], md.k[2]};
-				break;
-			case RB_MATERIAL_GLASS: {
-				const bool specular = md.roughness_u == 0.f && md.roughness_v == 0.f;
-				r.kind = specular ? pt::MAT_GLASS_SMOOTH : pt::MAT_GLASS_ROUGH;
-				if (!specular) {
-					r.alpha_x = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_u) : md.roughness_u;
-					r.alpha_y = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_v) : md.roughness_v;
-				}
-				r.eta = md.ior;
-				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
-				r.transmission = vec3{md.transmission[0], md.transmission[1], md.transmission[2]};
-				r.has_reflect = black3(md.reflectance) ? 0u : 1u;
-				r.has_transmit = black3(md.transmission) ? 0u : 1u;
-				break;
-			}
-			case RB_MATERIAL_PLASTIC: {
-				if (!(md.ior > 0.f)) return RB_ERR_INVALID_ARGUMENT;
-				r.kind = pt::MAT_PLASTIC;
-				r.alpha_x = r.alpha_y = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_u) : md.roughness_u;
-				r.eta = md.ior;
-				r.diffuse = vec3{md.diffuse[0], md.diffuse[1], md.diffuse[2]};
-				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
-				r.has_reflect = black3(md.reflectance) ? 0u : 1u;
-				break;
-			}
-			case RB_MATERIAL_SUBSTRATE:
-				r.kind = (black3(md.reflectance) && black3(md.diffuse)) ? pt::MAT_BLACK : pt::MAT_SUBSTRATE;
-				r.alpha_x = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_u) : md.roughness_u;
-				r.alpha_y = md.remap_roughness ? pt::roughness_to_alpha(md.roughness_v) : md.roughness_v;
-				r.diffuse = vec3{md.diffuse[0], md.diffuse[1], md.diffuse[2]};
-				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
-				break;
-			case RB_MATERIAL_MIRROR:
-				r.kind = black3(md.reflectance) ? pt::MAT_BLACK : pt::MAT_MIRROR;
-				r.reflectance = vec3{md.reflectance[0], md.reflectance[1], md.reflectance[2]};
-				break;
-			case RB_MATERIAL_UBER:
-			case RB_MATERIAL_TRANSLUCENT:
-				if (!pack_layered(md, r)) return RB_ERR_INVALID_ARGUMENT;
-				break;
-			default: return RB_ERR_INVALID_ARGUMENT;
-			}
-			out.materials.push_back(r);
+		// ---- image textures, then materials (records 0 .. n-1; component records of mixtures follow them)
+		if (desc->num_textures > 0 && desc->textures == nullptr) return RB_ERR_INVALID_ARGUMENT;
+		for (uint32_t t = 0; t < desc->num_textures; t++) {
+			const rb_texture_desc& td = desc->textures[t];
+			if (td.rgb == nullptr || td.width == 0 || td.height == 0 || td.width > (1u << 15) || td.height > (1u << 15))
+				return RB_ERR_INVALID_ARGUMENT;
+			pt::texture_rec tr{};
+			tr.offset = static_cast<uint32_t>(out.texels.size());
+			tr.width = td.width;
+			tr.height = td.height;
+			if (out.texels.size() + 3ull * td.width * td.height > 0xffffffffull) return RB_ERR_INVALID_ARGUMENT;
+			out.texels.insert(out.texels.end(), td.rgb, td.rgb + 3ull * td.width * td.height);
+			out.textures.push_back(tr);
+		}
+		{
+			const rb_status st = pack_materials(desc, out.materials, out.material_srcs);
+			if (st != RB_OK) return st;
 		}
 		// ---- homogeneous media and media components
 		if ((desc->num_mediums > 0 && desc->mediums == nullptr) || (desc->num_media > 0 && desc->media == nullptr))
@@ -365,6 +421,7 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 			}
 		}
 		if (built == nullptr && !trees.empty()) out.bvh_depth += 1 + deepest_tree;
+		out.instances = !trees.empty();
 		// ---- 4-wide nodes: every binary node at an even depth with its
 		// grandchildren as slots, numbered in preorder (the scene tree only)
 		{
@@ -588,7 +645,24 @@ rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out
 			append_vec(out.tangents, p.tangents);
 			append_vec(out.uvs, p.uvs);
 			append_vec(out.indices, p.indices);
-			append_vec(out.materials, p.materials);
+			// materials: a textured record names its parameters, whose textures name their texels
+			const uint32_t src_base = static_cast<uint32_t>(out.material_srcs.size());
+			const uint32_t texture_base = static_cast<uint32_t>(out.textures.size());
+			const uint32_t texel_base = static_cast<uint32_t>(out.texels.size());
+			for (pt::material_rec m : p.materials) {
+				if (m.kind == pt::MAT_TEXTURED) m.src += src_base;
+				out.materials.push_back(m);
+			}
+			for (pt::material_src ms : p.material_srcs) {
+				for (uint32_t t = 0; t < pt::kNumTexSlots; t++)
+					if (ms.tex[t]) ms.tex[t] += texture_base;
+				out.material_srcs.push_back(ms);
+			}
+			for (pt::texture_rec tr : p.textures) {
+				tr.offset += texel_base;
+				out.textures.push_back(tr);
+			}
+			append_vec(out.texels, p.texels);
 			for (pt::emitter_rec e : p.emitters) {
 				e.entity += static_cast<int32_t>(entity_base);
 				out.emitters.push_back(e);
@@ -612,6 +686,7 @@ rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out
 			pl.env = p.env;
 			places.push_back(pl);
 			out.bvh_depth = p.bvh_depth > out.bvh_depth ? p.bvh_depth : out.bvh_depth;
+			out.instances = out.instances || p.instances;
 		}
 		out.wide_ok = wide_ok;
 		if (!wide_ok) out.wnodes.clear();
@@ -654,6 +729,11 @@ pt::scene_view host_view(const packed_scene& p) {
 	v.mediums = p.mediums.data();
 	v.media = p.media.data();
 	v.num_media = static_cast<uint32_t>(p.media.size());
+	v.instances = p.instances ? 1u : 0u;
+	v.material_srcs = p.material_srcs.data();
+	v.textures = p.textures.data();
+	v.texels = p.texels.data();
+	v.num_textures = static_cast<uint32_t>(p.textures.size());
 	return v;
 }
 

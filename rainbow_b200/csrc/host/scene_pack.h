@@ -24,12 +24,16 @@ struct packed_scene {
 	std::vector<float> positions, normals, tangents, uvs;
 	std::vector<uint32_t> indices;
 	std::vector<pt::material_rec> materials;
+	std::vector<pt::material_src> material_srcs;  // parameters of the MAT_TEXTURED records
+	std::vector<pt::texture_rec> textures;
+	std::vector<float> texels;
 	std::vector<pt::emitter_rec> emitters;
 	std::vector<pt::medium_rec> mediums;
 	std::vector<pt::media_rec> media;
 	std::vector<int32_t> environments;
 	pt::env_distribution env{};
 	uint32_t bvh_depth = 0;
+	bool instances = false;               // some prim slots are whole entities with their own mesh tree
 };
 
 // Validates and packs a scene. Builds the BVH with rb_bvh_build when the

@@ -33,6 +33,7 @@ struct smem_stack {
 	__device__ bool empty() const { return sp == 0; }
 	__device__ bool full() const { return sp + 2 > cap; }
 	__device__ uint32_t size() const { return sp; }
+	__device__ raw_stack raw() const { return raw_stack{base, stride, sp, cap}; }
 };
 
 __device__ __forceinline__ smem_stack make_stack(uint32_t* smem, uint32_t cap) {
@@ -127,22 +128,23 @@ __device__ __forceinline__ hit_t to_hit(float4 h) {
 // first: an occlusion query (any hit accepted at len will do) on the 4-wide
 // path; its reference-order fallback finds the closest hit, which answers the
 // same question.
-template <bool SHADOW, bool COUNT>
+// INST: instantiated without the instance-slot branch for single-level scenes.
+template <bool SHADOW, bool COUNT, bool INST = true>
 __device__ __forceinline__ bool trace_one(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h, smem_stack& st,
 	uint32_t& nodes, uint32_t& tris, bool first = false) {
 	trace_counters c{0u, 0u};
 	bool ok;
 	if (!COUNT && s.wnodes != nullptr && !isnan(len)) {
 		const float len0 = len;
-		const int r = closest_hit_fast<SHADOW>(s, o, d, len, h, st, first);
+		const int r = closest_hit_fast<SHADOW, INST>(s, o, d, len, h, st, first);
 		ok = r == 1;
 		if (r < 0) {  // a NaN length or a full stack: redo the ray in the reference's own visiting order
 			len = len0;
-			ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
+			ok = closest_hit<SHADOW, COUNT, INST>(s, o, d, len, h, st, c);
 		}
 	} else {
 		// counting passes count the box and triangle tests of the reference's traversal
-		ok = closest_hit<SHADOW, COUNT>(s, o, d, len, h, st, c);
+		ok = closest_hit<SHADOW, COUNT, INST>(s, o, d, len, h, st, c);
 	}
 	nodes += c.nodes;
 	tris += c.tris;
@@ -236,7 +238,8 @@ template <int MAT>
 __device__ bool continue_guided(const scene_view& s, path_state& p, const shade_record& rec, const float* g, vec3& wi_out,
 	float& pb_out) {
 	const surface_t& si = rec.si;
-	const bsdf_t b = make_bsdf(s.materials + rec.material);
+	material_rec mat_scratch;
+	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si.uv, mat_scratch));
 	const vec3 wo = to_local(si, si.wo);
 	const float alpha = g[guide::kAlphaOff];
 	const float u_sel = pcg_real(p.rng);
@@ -708,7 +711,7 @@ __global__ void __launch_bounds__(256) k_direct_round(scene_view s, wave_buffers
 	warp_add64(w.counters, CNT_EXTEND_RAYS, rays);
 }
 
-template <bool COUNT, bool VOL, bool BATCH>
+template <bool COUNT, bool VOL, bool BATCH, bool INST>
 __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, uint32_t queue_in, uint32_t stack_cap,
 	uint32_t sort) {
 	extern __shared__ uint32_t smem[];
@@ -728,9 +731,9 @@ __global__ void __launch_bounds__(256) k_extend(scene_view s, wave_buffers w, ui
 			bool ok;
 			if (BATCH) {
 				const scene_view sv = batch_view(s, w.batch[w.scene[i]]);
-				ok = trace_one<false, COUNT>(sv, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+				ok = trace_one<false, COUNT, INST>(sv, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
 			} else {
-				ok = trace_one<false, COUNT>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
+				ok = trace_one<false, COUNT, INST>(s, vec3{o.x, o.y, o.z}, vec3{d.x, d.y, d.z}, len, h, st, nodes, tris);
 			}
 			if (!ok) {
 				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
@@ -1061,7 +1064,7 @@ __global__ void __launch_bounds__(256) k_shade_a(scene_view s_all, wave_buffers 
 // whether the hit slot is the emitter, nothing or something else). Emitters of
 // more than kShadowFirstTris triangles keep the closest-hit query.
 constexpr uint32_t kShadowFirstTris = 64;
-template <bool COUNT, bool BATCH>
+template <bool COUNT, bool BATCH, bool INST>
 __global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buffers w, uint32_t stack_cap,
 	uint32_t shadow_first) {
 	extern __shared__ uint32_t smem[];
@@ -1088,7 +1091,7 @@ __global__ void __launch_bounds__(256) k_trace_secondary(scene_view s, wave_buff
 					first = true;
 				}
 			}
-			ok = trace_one<true, COUNT>(sv, o3, d3, len, h, st, nodes, tris, first);
+			ok = trace_one<true, COUNT, INST>(sv, o3, d3, len, h, st, nodes, tris, first);
 			if (!ok) {
 				set_error(w.counters, RB_ERR_STACK_OVERFLOW);
 				h.slot = -1;
@@ -1605,19 +1608,19 @@ cudaError_t allow_smem(Kernel kernel, size_t bytes, int carveout = 100) {
 	return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
 
-template <bool COUNT>
+template <bool COUNT, bool INST>
 cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t queue_in, const launch_cfg& cfg,
 	cudaStream_t stream) {
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	const bool refill = !COUNT && cfg.refill;
-	cudaError_t e = allow_smem(k_extend<COUNT, true, false>, smem, cfg.carveout);
-	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, false>, smem, cfg.carveout);
+	cudaError_t e = allow_smem(k_extend<COUNT, true, false, INST>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, false, INST>, smem, cfg.carveout);
 	if (e == cudaSuccess) e = allow_smem(k_beam<COUNT>, smem, cfg.carveout);
 	if (e == cudaSuccess && refill) e = allow_smem(k_extend_refill<true, false>, smem, cfg.carveout);
 	if (e == cudaSuccess && refill) e = allow_smem(k_secondary_refill<false>, smem, cfg.carveout);
 	if (e != cudaSuccess) return e;
 	if (refill) k_extend_refill<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
-	else k_extend<COUNT, true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	else k_extend<COUNT, true, false, INST><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	k_shade_a<CLASS_LAMBERT, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_METAL, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
 	k_shade_a<CLASS_GLASS_ROUGH, true, false><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
@@ -1631,7 +1634,7 @@ cudaError_t volume_bounce(const scene_view& s, const wave_buffers& w, uint32_t q
 		if (e != cudaSuccess) return e;
 	}
 	if (refill) k_secondary_refill<false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
-	else k_trace_secondary<COUNT, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth, 0u);
+	else k_trace_secondary<COUNT, false, INST><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth, 0u);
 	k_vol_direct<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	k_beam<COUNT><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
 	k_vol_continue<<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
@@ -1665,14 +1668,16 @@ __global__ void k_set_first(wave_params* p, uint64_t first) { p->first_item = fi
 // buffer has to outlive the enqueued call.
 __global__ void k_set_params(wave_params p, wave_params* dst) { *dst = p; }
 
-template <bool COUNT, bool BATCH>
+// INST: the scene holds instance slots (scene_view::instances); the traversal
+// kernels of single-level scenes are instantiated without that branch.
+template <bool COUNT, bool BATCH, bool INST>
 cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
-	if (!BATCH && cfg.volume) return volume_bounce<COUNT>(s, w, queue_in, cfg, stream);
+	if (!BATCH && cfg.volume) return volume_bounce<COUNT, INST>(s, w, queue_in, cfg, stream);
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	const bool refill = !COUNT && cfg.refill;
-	cudaError_t e = allow_smem(k_extend<COUNT, false, BATCH>, smem, cfg.carveout);
-	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, BATCH>, smem, cfg.carveout);
+	cudaError_t e = allow_smem(k_extend<COUNT, false, BATCH, INST>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<COUNT, BATCH, INST>, smem, cfg.carveout);
 	if (e == cudaSuccess && refill) e = allow_smem(k_extend_refill<false, BATCH>, smem, cfg.carveout);
 	if (e == cudaSuccess && refill) e = allow_smem(k_secondary_refill<BATCH>, smem, cfg.carveout);
 	if (e != cudaSuccess) return e;
@@ -1680,7 +1685,7 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	uint32_t ev = timed ? *cfg.next_event : 0u;
 	if (timed) { cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 0; }
 	if (refill) k_extend_refill<false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
-	else k_extend<COUNT, false, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
+	else k_extend<COUNT, false, BATCH, INST><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth, cfg.sort);
 	if (timed) cudaEventRecord(cfg.events[2 * ev + 1], stream);
 	if (cfg.sort != RB_SORT_NONE) {
 		k_shade_a<CLASS_LAMBERT, false, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w);
@@ -1695,7 +1700,7 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 	}
 	if (timed) { ev++; cudaEventRecord(cfg.events[2 * ev], stream); cfg.event_kind[ev] = 1; }
 	if (refill) k_secondary_refill<BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth);
-	else k_trace_secondary<COUNT, BATCH><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth,
+	else k_trace_secondary<COUNT, BATCH, INST><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, cfg.stack_depth,
 		cfg.shadow_first ? 1u : 0u);
 	if (timed) { cudaEventRecord(cfg.events[2 * ev + 1], stream); *cfg.next_event = ev + 1; }
 	if (cfg.sort != RB_SORT_NONE) {
@@ -1731,11 +1736,26 @@ cudaError_t launch_trace_rays(const scene_view& s, const uint32_t* prim_entity, 
 	return cudaGetLastError();
 }
 
-cudaError_t launch_bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
+template <bool INST>
+cudaError_t bounce_inst(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
 	const launch_cfg& cfg, cudaStream_t stream) {
 	if (cfg.batch)
-		return cfg.count ? bounce<true, true>(s, w, f, queue_in, cfg, stream) : bounce<false, true>(s, w, f, queue_in, cfg, stream);
-	return cfg.count ? bounce<true, false>(s, w, f, queue_in, cfg, stream) : bounce<false, false>(s, w, f, queue_in, cfg, stream);
+		return cfg.count ? bounce<true, true, INST>(s, w, f, queue_in, cfg, stream)
+			: bounce<false, true, INST>(s, w, f, queue_in, cfg, stream);
+	return cfg.count ? bounce<true, false, INST>(s, w, f, queue_in, cfg, stream)
+		: bounce<false, false, INST>(s, w, f, queue_in, cfg, stream);
+}
+
+cudaError_t launch_bounce(const scene_view& s, const wave_buffers& w, const film_buffers& f, uint32_t queue_in,
+	const launch_cfg& cfg, cudaStream_t stream) {
+	return s.instances ? bounce_inst<true>(s, w, f, queue_in, cfg, stream) : bounce_inst<false>(s, w, f, queue_in, cfg, stream);
+}
+
+// The secondary traversal of the staged direct-lighting rounds.
+template <bool COUNT>
+void direct_secondary(const scene_view& s, const wave_buffers& wr, const launch_cfg& cfg, size_t smem, cudaStream_t stream) {
+	if (s.instances) k_trace_secondary<COUNT, false, true><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth, 0u);
+	else k_trace_secondary<COUNT, false, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth, 0u);
 }
 
 // Whether a wave ends with the tail kernel after cfg.tail bounces (plain
@@ -1814,8 +1834,10 @@ cudaError_t launch_direct_staged_wave(const scene_view& s, const wave_buffers& w
 	const size_t smem = 2 * static_cast<size_t>(cfg.stack_depth) * cfg.block_trace * sizeof(uint32_t);
 	cudaError_t e = cfg.count ? allow_smem(k_direct_surface<true>, smem, cfg.carveout)
 		: allow_smem(k_direct_surface<false>, smem, cfg.carveout);
-	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<false, false>, smem, cfg.carveout);
-	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<true, false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<false, false, false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<true, false, false>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<false, false, true>, smem, cfg.carveout);
+	if (e == cudaSuccess) e = allow_smem(k_trace_secondary<true, false, true>, smem, cfg.carveout);
 	if (e != cudaSuccess) return e;
 	// the traversal kernel reads the queued slots through the secondary-ray fields
 	wave_buffers wr = w;
@@ -1833,8 +1855,8 @@ cudaError_t launch_direct_staged_wave(const scene_view& s, const wave_buffers& w
 	k_direct_lights<CLASS_GLASS_ROUGH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	k_direct_lights<CLASS_OTHER><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);
 	for (uint32_t r = 0; r < dc.bsdf_samples && e == cudaSuccess; r++) {
-		if (cfg.count) k_trace_secondary<true, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth, 0u);
-		else k_trace_secondary<false, false><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, wr, cfg.stack_depth, 0u);
+		if (cfg.count) direct_secondary<true>(s, wr, cfg, smem, stream);
+		else direct_secondary<false>(s, wr, cfg, smem, stream);
 		e = cudaMemsetAsync(w.counters + CNT_SECONDARY, 0, sizeof(uint32_t), stream);
 		if (e != cudaSuccess) break;
 		k_direct_round<CLASS_LAMBERT><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, db, dc);

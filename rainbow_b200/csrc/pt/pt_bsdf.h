@@ -221,7 +221,8 @@ struct bsdf_t {
 	uint32_t types;
 	uint32_t count;
 	const material_rec* m;
-	float eta;  // collection eta (glass IOR, else 1)
+	float eta;     // collection eta (glass IOR, else 1)
+	uint32_t mix;  // a mixture: each lobe reads its own component record (lobe_ref)
 };
 RB_HD uint32_t lobe_kind(const bsdf_t& b, uint32_t i) { return (b.kinds >> (4u * i)) & 15u; }
 RB_HD uint32_t lobe_type(const bsdf_t& b, uint32_t i) { return (b.types >> (5u * i)) & 31u; }
@@ -238,6 +239,7 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 	b.kinds = 0;
 	b.types = 0;
 	b.eta = 1.f;
+	b.mix = 0;
 	switch (m->kind) {
 	case MAT_LAMBERT:
 		add_lobe(b, LOBE_LAMBERT, ST_DIFFUSE | ST_REFLECTION);
@@ -276,6 +278,14 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 		b.types = m->lobe_types;
 		b.count = m->lobe_count;
 		break;
+	case MAT_MIXTURE:
+		// mixture_material::build_surface_properties (mixture_material.cpp:13-27): the
+		// lobes of both components, the collection's eta left at its default of 1
+		b.kinds = m->lobe_kinds;
+		b.types = m->lobe_types;
+		b.count = m->lobe_count;
+		b.mix = 1;
+		break;
 	default: break;  // black matte: no lobes
 	}
 	return b;
@@ -286,8 +296,8 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 constexpr int MAT_ANY = -1;
 
 // microfacet_reflection::evaluate (scatterings/reflection/microfacet_reflection.cpp):
-// conductor Fresnel for metal, else dielectric Fresnel (1, m->eta) scaled by R
-// (the material's reflectance, or a layered lobe's own spectrum).
+// conductor Fresnel for metal, else dielectric Fresnel (1, m->eta), scaled by R
+// (the material's reflectance field, or a layered lobe's own spectrum).
 template <int MAT = MAT_ANY>
 RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi, spectrum R) {
 	const float co = fabs_ref(wo.z), ci = fabs_ref(wi.z);
@@ -297,12 +307,8 @@ RB_HD spectrum mf_reflect_f(const material_rec* m, vec3 wo, vec3 wi, spectrum R)
 	wh = face_forward(normalize(wh), vec3{0.f, 0.f, 1.f});
 	spectrum F;
 	const bool conductor = MAT == MAT_ANY ? (m->kind == MAT_METAL) : (MAT == static_cast<int>(MAT_METAL));
-	if (conductor) {
-		F = fresnel_conductor(dot(wi, wh), m->cond_eta, m->cond_k);
-		R = spectrum{1.f, 1.f, 1.f};
-	} else {
-		F = splat3(fresnel_dielectric(dot(wi, wh), 1.f, m->eta));
-	}
+	if (conductor) F = fresnel_conductor(dot(wi, wh), m->cond_eta, m->cond_k);  // R: 1, or a mixture's weight
+	else F = splat3(fresnel_dielectric(dot(wi, wh), 1.f, m->eta));
 	const float G = tr_g(m->alpha_x, m->alpha_y, wo, wi);
 	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
 	return R * (G * D) * F / (4.f * ci * co);
@@ -352,7 +358,7 @@ RB_HD spectrum fresnel_blend_f(const material_rec* m, vec3 wo, vec3 wi) {
 	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
 	const spectrum fresnel = m->reflectance + (splat3(1.f) - m->reflectance) * pow5(1.f - dot(wo, wh));
 	const spectrum specular = fresnel * D / (4.f * fabs_ref(dot(wi, wh)) * fmax_ref(fabs_ref(wi.z), fabs_ref(wo.z)));
-	return specular + diffuse;  // times the layer's scale, 1
+	return m->blend_scale * (specular + diffuse);  // the layer's scale: 1, or a mixture's weight
 }
 RB_HD float fresnel_blend_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	if (!same_hemisphere(wo, wi)) return 0.f;
@@ -385,9 +391,16 @@ RB_HD spectrum oren_nayar_f(const material_rec* m, vec3 wo, vec3 wi) {
 	return m->diffuse * kInvPi * (m->alpha_x + m->alpha_y * max_cos * sin_alpha * tan_beta);
 }
 
-// The spectrum a lobe scales by: a layered lobe's own entry, else the
-// material's named field the lobe kind reads.
-RB_HD spectrum layered_r(const bsdf_t& b, uint32_t i) { return b.m->lobe_r[i]; }
+// The record a lobe reads and the lobe's index in it: the material's own
+// record, or for a mixture the component record the lobe came from.
+template <int MAT = MAT_ANY>
+RB_HD const material_rec* lobe_rec(const bsdf_t& b, uint32_t i) {
+	if constexpr (MAT != MAT_ANY) return b.m;
+	else return b.mix ? b.m + (b.m->lobe_ref[i] >> 4) : b.m;
+}
+RB_HD uint32_t lobe_local(const bsdf_t& b, uint32_t i) { return b.mix ? (b.m->lobe_ref[i] & 15u) : i; }
+// A layered lobe's own spectrum.
+RB_HD spectrum layered_r(const bsdf_t& b, uint32_t i) { return lobe_rec(b, i)->lobe_r[lobe_local(b, i)]; }
 
 template <int MAT>
 RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
@@ -397,17 +410,18 @@ RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi, b.m->reflectance)
 		                                          : mf_transmit_f(b.m, wo, wi, b.m->transmission);
 	else {
+		const material_rec* m = lobe_rec(b, i);
 		switch (lobe_kind(b, i)) {
-		case LOBE_LAMBERT: return b.m->diffuse * kInvPi;
-		case LOBE_OREN_NAYAR: return oren_nayar_f(b.m, wo, wi);
-		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi, b.m->reflectance);
-		case LOBE_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi, b.m->transmission);
-		case LOBE_FRESNEL_BLEND: return fresnel_blend_f(b.m, wo, wi);
+		case LOBE_LAMBERT: return m->diffuse * kInvPi;
+		case LOBE_OREN_NAYAR: return oren_nayar_f(m, wo, wi);
+		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(m, wo, wi, m->reflectance);
+		case LOBE_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, m->transmission);
+		case LOBE_FRESNEL_BLEND: return fresnel_blend_f(m, wo, wi);
 		// lambertian_reflection / lambertian_transmission::evaluate: R / pi, T / pi
 		case LOBE_L_LAMBERT:
 		case LOBE_L_LAMBERT_TRANSMIT: return layered_r(b, i) * kInvPi;
-		case LOBE_L_MF_REFLECT: return mf_reflect_f<MAT_ANY>(b.m, wo, wi, layered_r(b, i));
-		case LOBE_L_MF_TRANSMIT: return mf_transmit_f(b.m, wo, wi, layered_r(b, i));
+		case LOBE_L_MF_REFLECT: return mf_reflect_f<MAT_ANY>(m, wo, wi, layered_r(b, i));
+		case LOBE_L_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, layered_r(b, i));
 		default: return spectrum{0.f, 0.f, 0.f};  // specular lobes evaluate to 0
 		}
 	}
@@ -419,6 +433,7 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
 		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_pdf(b.m, wo, wi) : mf_transmit_pdf(b.m, wo, wi);
 	else {
+		const material_rec* m = lobe_rec(b, i);
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT:
 		case LOBE_OREN_NAYAR:
@@ -426,10 +441,10 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		// transmission_function::pdf (scatterings/transmission/transmission_function.cpp:25-28)
 		case LOBE_L_LAMBERT_TRANSMIT: return same_hemisphere(wo, wi) ? 0.f : cosine_hemisphere_pdf(fabs_ref(wi.z));
 		case LOBE_MF_REFLECT:
-		case LOBE_L_MF_REFLECT: return mf_reflect_pdf(b.m, wo, wi);
+		case LOBE_L_MF_REFLECT: return mf_reflect_pdf(m, wo, wi);
 		case LOBE_MF_TRANSMIT:
-		case LOBE_L_MF_TRANSMIT: return mf_transmit_pdf(b.m, wo, wi);
-		case LOBE_FRESNEL_BLEND: return fresnel_blend_pdf(b.m, wo, wi);
+		case LOBE_L_MF_TRANSMIT: return mf_transmit_pdf(m, wo, wi);
+		case LOBE_FRESNEL_BLEND: return fresnel_blend_pdf(m, wo, wi);
 		default: return 0.f;  // specular lobes: pdf 0
 		}
 	}
@@ -450,7 +465,7 @@ RB_HD lobe_sample sample_lambert_transmit(const bsdf_t& b, uint32_t i, vec3 wo, 
 }
 template <int MAT>
 RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u, spectrum R) {
-	const material_rec* m = b.m;
+	const material_rec* m = lobe_rec<MAT>(b, i);
 	if (wo.z == 0.f) return no_sample();
 	const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
 	if (dot(wo, wh) < 0.f) return no_sample();
@@ -458,8 +473,9 @@ RB_HD lobe_sample sample_mf_reflect(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u
 	if (!same_hemisphere(wo, wi)) return no_sample();
 	return lobe_sample{lobe_type(b, i), mf_reflect_f<MAT>(m, wo, wi, R), wi, tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh))};
 }
+template <int MAT>
 RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u, spectrum T) {
-	const material_rec* m = b.m;
+	const material_rec* m = lobe_rec<MAT>(b, i);
 	if (wo.z == 0.f) return no_sample();
 	const vec3 wh = tr_sample(m->alpha_x, m->alpha_y, wo, u);
 	if (dot(wo, wh) < 0.f) return no_sample();
@@ -470,8 +486,7 @@ RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 
 	return lobe_sample{lobe_type(b, i), mf_transmit_f(m, wo, wi, T), wi, mf_transmit_pdf(m, wo, wi)};
 }
 // fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
-RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
-	const material_rec* m = b.m;
+RB_HD lobe_sample sample_fresnel_specular(const material_rec* m, vec3 wo, vec2 u) {
 	const float F = fresnel_dielectric(wo.z, 1.f, m->eta);
 	if (u.x < F) {
 		const vec3 wi{-wo.x, -wo.y, wo.z};
@@ -489,8 +504,7 @@ RB_HD lobe_sample sample_fresnel_specular(const bsdf_t& b, vec3 wo, vec2 u) {
 
 // fresnel_blend_reflection::sample: u.x below one half picks the cosine
 // hemisphere, above it the Trowbridge-Reitz half vector, u.x remapped to [0, 1).
-RB_HD lobe_sample sample_fresnel_blend(const bsdf_t& b, vec3 wo, vec2 u) {
-	const material_rec* m = b.m;
+RB_HD lobe_sample sample_fresnel_blend(const material_rec* m, vec3 wo, vec2 u) {
 	vec3 wi;
 	if (u.x < 0.5f) {
 		wi = cosine_hemisphere(vec2{fmin_ref(2.f * u.x, kOneMinusEps), u.y});
@@ -505,22 +519,22 @@ RB_HD lobe_sample sample_fresnel_blend(const bsdf_t& b, vec3 wo, vec2 u) {
 
 // specular_reflection::sample with fresnel_effect_nop (specular_reflection.cpp:16-31):
 // the mirror direction, f = reflectance / |cos theta_i|, pdf 1.
-RB_HD lobe_sample sample_specular_reflect(const bsdf_t& b, vec3 wo) {
+RB_HD lobe_sample sample_specular_reflect(const material_rec* m, vec3 wo) {
 	const vec3 wi{-wo.x, -wo.y, wo.z};
-	return lobe_sample{ST_SPECULAR | ST_REFLECTION, b.m->reflectance / fabs_ref(wi.z), wi, 1.f};
+	return lobe_sample{ST_SPECULAR | ST_REFLECTION, m->reflectance / fabs_ref(wi.z), wi, 1.f};
 }
 // specular_reflection::sample with a dielectric Fresnel (1, m->eta):
 // f = F(cos theta_i) R / |cos theta_i|, pdf 1.
 RB_HD lobe_sample sample_layered_specular_reflect(const bsdf_t& b, uint32_t i, vec3 wo) {
 	const vec3 wi{-wo.x, -wo.y, wo.z};
-	const float F = fresnel_dielectric(wi.z, 1.f, b.m->eta);
+	const float F = fresnel_dielectric(wi.z, 1.f, lobe_rec(b, i)->eta);
 	return lobe_sample{ST_SPECULAR | ST_REFLECTION, splat3(F) * layered_r(b, i) / fabs_ref(wi.z), wi, 1.f};
 }
 // specular_transmission::sample (scatterings/transmission/specular_transmission.cpp:17-46),
 // radiance transport, eta (1, lobe_eta): refraction about the normal on wo's
 // side, f = T (1 - F(cos theta_i)) (eta_i / eta_o)^2 / |cos theta_i|, pdf 1.
 RB_HD lobe_sample sample_specular_transmit(const bsdf_t& b, uint32_t i, vec3 wo) {
-	const float lobe_eta = b.m->lobe_eta[i];
+	const float lobe_eta = lobe_rec(b, i)->lobe_eta[lobe_local(b, i)];
 	const bool entering = wo.z > 0.f;
 	const float ei = entering ? 1.f : lobe_eta;
 	const float eo = entering ? lobe_eta : 1.f;
@@ -538,22 +552,23 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return sample_mf_reflect<MAT>(b, i, wo, u, b.m->reflectance);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
 		return lobe_kind(b, i) == LOBE_MF_REFLECT ? sample_mf_reflect<MAT>(b, i, wo, u, b.m->reflectance)
-		                                          : sample_mf_transmit(b, i, wo, u, b.m->transmission);
+		                                          : sample_mf_transmit<MAT>(b, i, wo, u, b.m->transmission);
 	else {
+		const material_rec* m = lobe_rec(b, i);
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT:
 		case LOBE_OREN_NAYAR:
 		case LOBE_L_LAMBERT: return sample_lambert<MAT_ANY>(b, i, wo, u);  // reflection_function::sample, cosine
 		case LOBE_L_LAMBERT_TRANSMIT: return sample_lambert_transmit(b, i, wo, u);
-		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, b.m->reflectance);
+		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, m->reflectance);
 		case LOBE_L_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, layered_r(b, i));
-		case LOBE_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u, b.m->transmission);
-		case LOBE_L_MF_TRANSMIT: return sample_mf_transmit(b, i, wo, u, layered_r(b, i));
-		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(b, wo, u);
-		case LOBE_SPECULAR_REFLECT: return sample_specular_reflect(b, wo);
+		case LOBE_MF_TRANSMIT: return sample_mf_transmit<MAT_ANY>(b, i, wo, u, m->transmission);
+		case LOBE_L_MF_TRANSMIT: return sample_mf_transmit<MAT_ANY>(b, i, wo, u, layered_r(b, i));
+		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(m, wo, u);
+		case LOBE_SPECULAR_REFLECT: return sample_specular_reflect(m, wo);
 		case LOBE_L_SPECULAR_REFLECT: return sample_layered_specular_reflect(b, i, wo);
 		case LOBE_L_SPECULAR_TRANSMIT: return sample_specular_transmit(b, i, wo);
-		case LOBE_FRESNEL_BLEND: return sample_fresnel_blend(b, wo, u);
+		case LOBE_FRESNEL_BLEND: return sample_fresnel_blend(m, wo, u);
 		default: return no_sample();
 		}
 	}

@@ -122,62 +122,103 @@ RB_HD uint32_t float_as_u32(float f) {
 #endif
 }
 
+// A traversal stack as raw words (entry i at base[i * stride], at most cap):
+// what the mesh-tree walk below gets by value from its caller's stack.
+struct raw_stack {
+	uint32_t* base;
+	uint32_t stride;
+	uint32_t sp;
+	uint32_t cap;
+	RB_HD void push(uint32_t v) { base[sp * stride] = v; sp++; }
+	RB_HD uint32_t pop() { sp--; return base[sp * stride]; }
+	RB_HD bool full() const { return sp + 2 > cap; }
+};
+
+struct instance_result {
+	uint32_t status;  // 0: no hit, 1: a hit (len, slot, b1, b2), 2: the stack overflowed
+	float len;        // world length of the hit
+	int32_t slot;
+	float b1, b2;
+	uint32_t nodes, tris;  // box and triangle tests (counting passes)
+};
+
 // entity::intersect(ray) for an entity held whole by the scene tree
 // (rainbow-cpu/scenes/entity.cpp:39-58 with mesh::intersect, mesh.cpp:45-57):
 // the ray goes to local space once, the mesh's own tree is walked in the
 // reference's visiting order with the local ray and the local length (which
 // every hit shortens), and if anything was hit the world length becomes local
-// length * |L2W d_local|. The walk uses the stack above the caller's entries and
-// leaves them as it found them. Returns false when the stack overflowed.
-template <bool COUNT, typename Stack>
-RB_HD bool instance_hit(const scene_view& s, uint32_t slot, uint32_t ent, vec3 o, vec3 d, float& len, hit_t& hit,
-	Stack& stack, trace_counters& cnt, bool occlusion = false) {
-	const float4 ia = RB_LDG(s.tri_a + slot);
+// length * |L2W d_local|. The walk uses the stack above the caller's entries.
+// occlusion: stop at the first hit.
+template <bool COUNT>
+RB_HD instance_result instance_walk(const float4* nodes, const float4* tri_a, const float4* tri_b,
+	const float2* tri_c, const entity_rec* ent, uint32_t slot, vec3 o, vec3 d, float len, raw_stack stack, bool occlusion) {
+	instance_result r{0u, len, -1, 0.f, 0.f, 0u, 0u};
+	const float4 ia = RB_LDG(tri_a + slot);
 	const uint32_t root = float_as_u32(ia.x), first = float_as_u32(ia.y);
-	const local_ray lr = make_local_ray(s.entities[ent].w2l, s.entities[ent].l2w, o, d);
+	const local_ray lr = make_local_ray(ent->w2l, ent->l2w, o, d);
 	const vec3 inv = 1.f / lr.d;
-	const bool neg[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+	const uint32_t neg = (inv.x < 0.f ? 1u : 0u) | (inv.y < 0.f ? 2u : 0u) | (inv.z < 0.f ? 4u : 0u);
 	float llen = len * lr.to_local;
-	bool any = false;
-	const uint32_t base = stack.size();
-	if (stack.full()) return false;
+	const uint32_t base = stack.sp;
+	if (stack.full()) { r.status = 2u; return r; }
 	stack.push(root);
-	while (stack.size() > base) {
+	while (stack.sp > base) {
 		const uint32_t n = stack.pop();
-		const float4 a = RB_LDG(s.nodes + 2 * n);
-		const float4 b = RB_LDG(s.nodes + 2 * n + 1);
-		if (COUNT) cnt.nodes++;
+		const float4 a = RB_LDG(nodes + 2 * n);
+		const float4 b = RB_LDG(nodes + 2 * n + 1);
+		if (COUNT) r.nodes++;
 		if (!slab_hit(a, b, lr.o, inv, llen)) continue;
 		const uint32_t w0 = float_as_u32(b.z), w1 = float_as_u32(b.w);
 		if (w1 & RB_BVH_LEAF_FLAG) {
 			const uint32_t count = w1 & ~(RB_BVH_LEAF_FLAG | kMeshLeaf);
 			for (uint32_t k = 0; k < count; k++) {
 				const uint32_t sl = first + w0 + k;
-				const float4 ta = RB_LDG(s.tri_a + sl);
-				const float4 tb = RB_LDG(s.tri_b + sl);
-				const float2 tc = RB_LDG(s.tri_c + sl);
-				if (COUNT) cnt.tris++;
+				const float4 ta = RB_LDG(tri_a + sl);
+				const float4 tb = RB_LDG(tri_b + sl);
+				const float2 tc = RB_LDG(tri_c + sl);
+				if (COUNT) r.tris++;
 				float t, b1, b2;
 				if (triangle_hit(lr.o, lr.d, llen, vec3{ta.x, ta.y, ta.z}, vec3{ta.w, tb.x, tb.y}, vec3{tb.z, tb.w, tc.x}, t,
 						b1, b2)) {
 					llen = t;
-					hit.slot = static_cast<int32_t>(sl);
-					hit.b1 = b1;
-					hit.b2 = b2;
-					any = true;
-					if (occlusion) {  // any hit will do: leave the caller's entries as they were
-						while (stack.size() > base) stack.pop();
+					r.slot = static_cast<int32_t>(sl);
+					r.b1 = b1;
+					r.b2 = b2;
+					r.status = 1u;
+					if (occlusion) {  // any hit will do
+						stack.sp = base;
 						break;
 					}
 				}
 			}
 			continue;
 		}
-		if (stack.full()) return false;
-		if (neg[w1]) { stack.push(n + 1); stack.push(w0); }
+		if (stack.full()) { r.status = 2u; return r; }
+		if ((neg >> w1) & 1u) { stack.push(n + 1); stack.push(w0); }
 		else { stack.push(w0); stack.push(n + 1); }
 	}
-	if (any) len = llen * lr.to_world;
+	if (r.status == 1u) r.len = llen * lr.to_world;
+	return r;
+}
+
+// The walk above for a caller's stack (which provides raw()); false when the
+// stack overflowed. The caller's entries and stack pointer are left as they were.
+template <bool COUNT, typename Stack>
+RB_HD bool instance_hit(const scene_view& s, uint32_t slot, uint32_t ent, vec3 o, vec3 d, float& len, hit_t& hit,
+	Stack& stack, trace_counters& cnt, bool occlusion = false) {
+	const instance_result r =
+		instance_walk<COUNT>(s.nodes, s.tri_a, s.tri_b, s.tri_c, s.entities + ent, slot, o, d, len, stack.raw(), occlusion);
+	if (COUNT) {
+		cnt.nodes += r.nodes;
+		cnt.tris += r.tris;
+	}
+	if (r.status == 2u) return false;
+	if (r.status == 1u) {
+		len = r.len;
+		hit.slot = r.slot;
+		hit.b1 = r.b1;
+		hit.b2 = r.b2;
+	}
 	return true;
 }
 
@@ -189,10 +230,12 @@ RB_HD bool instance_hit(const scene_view& s, uint32_t slot, uint32_t ent, vec3 o
 // (intersect_with_shadow_ray, :110-160). `len` is updated in place like the
 // reference's mutable ray.length. Stack provides push/pop/empty/full.
 // Returns false when the stack overflowed (the hit is then incomplete).
-template <bool SHADOW, bool COUNT, typename Stack>
+// INST: the scene may hold instance slots (scene_view::instances); kernels for
+// single-level scenes instantiate the traversals without that branch.
+template <bool SHADOW, bool COUNT, bool INST = true, typename Stack>
 RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack, trace_counters& cnt) {
 	const vec3 inv = 1.f / d;
-	const bool neg[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+	const uint32_t neg = (inv.x < 0.f ? 1u : 0u) | (inv.y < 0.f ? 2u : 0u) | (inv.z < 0.f ? 4u : 0u);
 	hit.slot = -1;
 	uint32_t cur_entity = 0xffffffffu;
 	local_ray lr{};
@@ -213,7 +256,7 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 				const uint32_t ew = float_as_u32(tc.y);
 				if (SHADOW && (ew & kEntityInvisible)) continue;
 				const uint32_t ent = ew & kEntityMask;
-				if (ew & kEntityInstance) {
+				if (INST && (ew & kEntityInstance)) {
 					if (!instance_hit<COUNT>(s, slot, ent, o, d, len, hit, stack, cnt)) return false;
 					continue;
 				}
@@ -237,7 +280,7 @@ RB_HD bool closest_hit(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& h
 		}
 		const uint32_t left = n + 1, right = w0;
 		if (stack.full()) return false;
-		if (neg[w1]) { stack.push(left); stack.push(right); }
+		if ((neg >> w1) & 1u) { stack.push(left); stack.push(right); }
 		else { stack.push(right); stack.push(left); }
 	}
 	return true;
@@ -329,7 +372,7 @@ RB_HD bool trav_begin(const scene_view& s, trav_state& t, vec3 o, vec3 d, float 
 // node's four slots, then the next node (descent or pop). Returns 0 while the
 // ray goes on, 1 when it is done, -1 when it must be redone in the reference's
 // order (a NaN length or a full stack).
-template <bool SHADOW, typename Stack>
+template <bool SHADOW, bool INST = true, typename Stack>
 RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 	if (t.cur & kRefLeaf) {
 		const uint32_t first = t.cur & 0x00ffffffu, count = (t.cur >> 24) & 0x7fu;
@@ -339,7 +382,7 @@ RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 			const uint32_t ew = float_as_u32(tc.y);
 			if (SHADOW && (ew & kEntityInvisible)) continue;
 			const uint32_t ent = ew & kEntityMask;
-			if (ew & kEntityInstance) {
+			if (INST && (ew & kEntityInstance)) {
 				trace_counters none{0u, 0u};
 				if (!instance_hit<false>(s, slot, ent, t.o, t.d, t.len, t.hit, stack, none, t.first)) return -1;
 				if (isnan(t.len)) return -1;
@@ -418,12 +461,12 @@ RB_HD int trav_step(const scene_view& s, trav_state& t, Stack& stack) {
 
 // first: stop at the first hit accepted at the ray's length (an occlusion
 // query), instead of the closest.
-template <bool SHADOW, typename Stack>
+template <bool SHADOW, bool INST = true, typename Stack>
 RB_HD int closest_hit_fast(const scene_view& s, vec3 o, vec3 d, float& len, hit_t& hit, Stack& stack, bool first = false) {
 	trav_state t;
 	int r = 1;
 	if (trav_begin(s, t, o, d, len, stack, first)) {
-		do r = trav_step<SHADOW>(s, t, stack);
+		do r = trav_step<SHADOW, INST>(s, t, stack);
 		while (r == 0);
 	}
 	len = t.len;
@@ -468,6 +511,7 @@ struct surface_t {
 	vec3 sx, sy, sz;
 	vec3 wo;
 	int32_t entity;
+	vec2 uv;       // texture coordinates (mesh.cpp:355)
 };
 
 RB_HD vec3 load3(const float* a, uint32_t i) { return vec3{a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
@@ -483,6 +527,7 @@ RB_HD void frame_from_normal(vec3 normal, vec3& x, vec3& y, vec3& z) {
 // Local interaction pieces of one triangle at barycentrics (b1, b2).
 struct local_surface {
 	vec3 p, n, sx, sy, sz;
+	vec2 uv;
 };
 
 RB_HD local_surface triangle_surface(const scene_view& s, const mesh_rec& m, uint32_t tri, float b1, float b2) {
@@ -496,6 +541,8 @@ RB_HD local_surface triangle_surface(const scene_view& s, const mesh_rec& m, uin
 	const float b0 = 1.f - b1 - b2;
 	local_surface out;
 	out.p = p0 * b0 + p1 * b1 + p2 * b2;
+	const vec3 uv = uv0 * b0 + uv1 * b1 + uv2 * b2;
+	out.uv = vec2{uv.x, uv.y};
 	const vec3 normal = reverse ? -normalize(cross(e1, e2)) : normalize(cross(e1, e2));
 	const vec3 duv02 = uv0 - uv2, duv12 = uv1 - uv2;
 	const vec3 dp02 = p0 - p2, dp12 = p1 - p2;
@@ -559,6 +606,7 @@ RB_HD surface_t make_surface(const scene_view& s, int32_t slot, float b1, float 
 	out.p = xform_point(e.l2w, ls.p);
 	out.wo = normalize(xform_vector(e.l2w, -lr.d));
 	out.entity = static_cast<int32_t>(ent);
+	out.uv = ls.uv;
 	return out;
 }
 

@@ -116,9 +116,10 @@ struct mesh_rec {
 };
 
 enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4, MAT_PLASTIC = 5,
-	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8, MAT_LAYERED = 9 };
+	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8, MAT_LAYERED = 9, MAT_MIXTURE = 10, MAT_TEXTURED = 11 };
 
-// Lobes of a layered material (uber, translucent): at most kMaxLayeredLobes.
+// Lobes of a layered material (uber, translucent) or of a mixture: at most
+// kMaxLayeredLobes.
 constexpr uint32_t kMaxLayeredLobes = 6;
 
 struct material_rec {
@@ -127,7 +128,8 @@ struct material_rec {
 	                          // Oren-Nayar (matte with sigma != 0): its A and B
 	float eta;                // glass / plastic IOR
 	spectrum diffuse;         // lambert reflectance (matte, plastic Kd)
-	spectrum reflectance;     // glass reflectance, plastic Ks, mirror reflectance
+	spectrum reflectance;     // glass reflectance, plastic Ks, mirror reflectance; metal: the
+	                          // microfacet reflection's scale (1, or a mixture's weight)
 	spectrum transmission;    // glass transmission
 	spectrum cond_eta;        // conductor eta
 	spectrum cond_k;          // conductor k
@@ -142,6 +144,41 @@ struct material_rec {
 	float collection_eta;
 	spectrum lobe_r[kMaxLayeredLobes];
 	float lobe_eta[kMaxLayeredLobes];
+	// mixtures (MAT_MIXTURE): the lobe list of both components in order, each
+	// lobe a lobe of a component record built with the mixture's weight on the
+	// host: (record offset from this record << 4) | the lobe's index there
+	uint32_t lobe_ref[kMaxLayeredLobes];
+	spectrum blend_scale;     // substrate: the Fresnel-blend layer's scale (1, or a mixture's weight)
+	// MAT_TEXTURED: a material with image-textured spectra, built at every hit
+	// from material_src[src] and its textures at the hit's uv
+	uint32_t src;
+};
+
+// Textured spectra of a material: diffuse, reflectance, transmission, specular, opacity.
+enum : uint32_t { TEX_DIFFUSE = 0, TEX_REFLECTANCE = 1, TEX_TRANSMISSION = 2, TEX_SPECULAR = 3, TEX_OPACITY = 4,
+	kNumTexSlots = 5 };
+
+// A material's parameters with what only the host computes already applied
+// (roughness_to_alpha, Oren-Nayar's A and B), from which its record is built
+// (pt_material.h): once on the host for constant textures, at every hit for
+// image-textured spectra.
+struct material_src {
+	uint32_t kind;            // RB_MATERIAL_* of its description
+	float alpha_x, alpha_y;   // Trowbridge-Reitz alphas (metal, rough glass, plastic, substrate, uber, translucent)
+	float ior;                // glass, plastic, uber
+	uint32_t smooth;          // glass: both roughnesses 0 (Fresnel-specular)
+	uint32_t oren_nayar;      // matte: sigma != 0
+	float on_a, on_b;         // matte: Oren-Nayar's A and B
+	spectrum diffuse, reflectance, transmission, specular, opacity;
+	spectrum cond_eta, cond_k;
+	uint32_t tex[kNumTexSlots];  // 0: the constant above; k > 0: texture k - 1 of the scene
+};
+
+// An RGB image texture: texels row-major, (x, y) at data[offset + 3 (y width + x)].
+struct texture_rec {
+	uint32_t offset;          // in floats
+	uint32_t width, height;
+	uint32_t pad;
 };
 
 enum : uint32_t { EMIT_SURFACE = 0, EMIT_ENVIRONMENT = 1 };
@@ -209,7 +246,12 @@ struct scene_view {
 	const medium_rec* mediums;
 	const media_rec* media;
 	uint32_t num_media;
-	uint32_t pad1;
+	uint32_t instances;           // non-zero: some prim slots hold a whole entity walked in its mesh's own tree
+	const material_src* material_srcs;  // parameters of the MAT_TEXTURED records
+	const texture_rec* textures;
+	const float* texels;
+	uint32_t num_textures;
+	uint32_t pad2;
 };
 
 } // namespace pt

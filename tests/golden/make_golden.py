@@ -61,6 +61,8 @@ import hashlib
 import os
 import sys
 
+import ctypes as C
+
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -252,6 +254,35 @@ def layered_fixtures():
                    "translucent": dict(kind=rb.RB_MATERIAL_TRANSLUCENT)})
 
 
+def mixture_fixtures():
+    from tests.helpers import _desc, mixture_scene
+    R = ref.RefScene(mixture_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(43)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("mixture_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8),
+         first_entity=first_entity(R, px, sm))
+    # BSDF tables of a mixture of an Oren-Nayar matte and a rough glass (its array: mixture, then the two)
+    mats = (rb.MaterialDesc * 3)(
+        _desc(rb.RB_MATERIAL_MIXTURE, amount=(0.3, 0.5, 0.7), components=(1, 2)),
+        _desc(rb.RB_MATERIAL_MATTE, diffuse=(0.7, 0.5, 0.3), sigma=25.0),
+        _desc(rb.RB_MATERIAL_GLASS, remap_roughness=1, reflectance=(1.0, 1.0, 1.0), transmission=(1.0, 1.0, 1.0),
+              ior=1.5, roughness_u=0.2, roughness_v=0.2))
+    bsdf_tables("mixture", mats)
+
+
+def texture_fixtures():
+    from tests.helpers import textured_scene
+    R = ref.RefScene(textured_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(47)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("texture_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8),
+         first_entity=first_entity(R, px, sm))
+
+
 def materials_fixtures():
     from tests.helpers import extra_materials_scene
     R = ref.RefScene(extra_materials_scene(scene_of(SPHERES)))
@@ -266,7 +297,13 @@ def materials_fixtures():
 
 
 def bsdf_fixtures(mats):
-    # BSDF known answers on the shading frame = world axes
+    for key, m in mats.items():
+        bsdf_tables(key, material_desc(m))
+
+
+def bsdf_tables(key, md):
+    # BSDF known answers on the shading frame = world axes; md: one descriptor,
+    # or an array whose first entry is the material (a mixture's components after it)
     rng = np.random.default_rng(5)
     n = 512
     wo = rng.normal(size=(n, 3)).astype(np.float32)
@@ -274,12 +311,11 @@ def bsdf_fixtures(mats):
     wi = rng.normal(size=(n, 3)).astype(np.float32)
     wi /= np.linalg.norm(wi, axis=1, keepdims=True)
     u = rng.random((n, 2), dtype=np.float32)
-    for key, m in mats.items():
-        md = material_desc(m)
-        for include_name, include in (("all", 31), ("nonspec", 27)):
-            out = ref.bsdf(md, wo, u, wi, include)
-            save(f"bsdf_{key}_{include_name}", wo=wo, u=u, wi_eval=wi, include=np.array(include),
-                 material=np.frombuffer(bytes(md), dtype=np.uint8), **out)
+    for include_name, include in (("all", 31), ("nonspec", 27)):
+        out = ref.bsdf(md, wo, u, wi, include)
+        save(f"bsdf_{key}_{include_name}", wo=wo, u=u, wi_eval=wi, include=np.array(include),
+             material=np.frombuffer(bytes(md), dtype=np.uint8),
+             material_count=np.array(len(md) if isinstance(md, C.Array) else 1), **out)
 
 
 def main():
@@ -298,6 +334,10 @@ def main():
         return oren_nayar_fixtures()
     if only == "layered":
         return layered_fixtures()
+    if only == "mixture":
+        return mixture_fixtures()
+    if only == "textures":
+        return texture_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -347,6 +387,8 @@ def main():
     two_level_fixtures()
     oren_nayar_fixtures()
     layered_fixtures()
+    mixture_fixtures()
+    texture_fixtures()
 
 
 def material_desc(m):

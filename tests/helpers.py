@@ -19,11 +19,17 @@ def scene_from_params(params) -> rb.Scene:
     return rb.generate_scene(kind, seed=seed, width=w, height=h, num_spheres=n, subdivision=sub)
 
 
-def material_from_bytes(raw: bytes) -> rb.MaterialDesc:
-    """A material descriptor from a fixture's bytes; fields added to the
-    descriptor after the fixture was written (at its end) read as zero."""
+def material_from_bytes(raw: bytes, count: int = 1):
+    """Material descriptors from a fixture's bytes (`count` of them, a mixture
+    and its components when more than one); fields added to the descriptor
+    after the fixture was written (at its end) read as zero."""
     size = C.sizeof(rb.MaterialDesc)
-    return rb.MaterialDesc.from_buffer_copy(bytes(raw)[:size].ljust(size, b"\0"))
+    raw = bytes(raw)
+    old = len(raw) // count
+    parts = [raw[k * old:(k + 1) * old][:size].ljust(size, b"\0") for k in range(count)]
+    if count == 1:
+        return rb.MaterialDesc.from_buffer_copy(parts[0])
+    return (rb.MaterialDesc * count).from_buffer_copy(b"".join(parts))
 
 
 _LOBE_NAMES = {0: "lambert", 1: "microfacet_reflection", 2: "microfacet_transmission", 3: "fresnel_specular",
@@ -426,6 +432,100 @@ def layered_scene(scene: rb.Scene) -> rb.Scene:
             m.roughness_u = m.roughness_v = 0.15 + 0.05 * (k % 3)  # translucent reads roughness_u alone
         mats.append(m)
     return scene.with_materials(mats)
+
+
+def _desc(kind, **kw) -> rb.MaterialDesc:
+    m = rb.MaterialDesc()
+    m.kind = kind
+    for k, v in kw.items():
+        if isinstance(v, tuple):
+            getattr(m, k)[:] = v
+        else:
+            setattr(m, k, v)
+    return m
+
+
+def mixture_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with every third material (from the second, the floor's) a
+    mixture (mixture_material.cpp) of two component materials appended after
+    the scene's own: Oren-Nayar matte with metal, translucent with smooth
+    glass, uber with metal, and a mixture of plastic and mirror mixed with
+    substrate (nested), in turn; the rest unchanged."""
+    mats = [rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k])) for k in range(scene.desc.num_materials)]
+    n = len(mats)
+    extra = []
+
+    def add(m):
+        extra.append(m)
+        return n + len(extra) - 1
+
+    metal = dict(remap_roughness=1, eta=(0.200438, 0.924033, 1.102212), k=(3.912949, 2.452848, 2.142188),
+                 roughness_u=0.2, roughness_v=0.3)
+    for k in range(1, n, 3):
+        variant = (k // 3) % 4
+        if variant == 0:
+            c = (add(_desc(rb.RB_MATERIAL_MATTE, diffuse=(0.7, 0.5, 0.3), sigma=25.0)),
+                 add(_desc(rb.RB_MATERIAL_METAL, **metal)))
+        elif variant == 1:
+            c = (add(_desc(rb.RB_MATERIAL_TRANSLUCENT, remap_roughness=1, diffuse=(0.6, 0.5, 0.4),
+                           specular=(0.4, 0.4, 0.4), reflectance=(0.5, 0.5, 0.5), transmission=(0.4, 0.45, 0.5),
+                           roughness_u=0.2, roughness_v=0.2)),
+                 add(_desc(rb.RB_MATERIAL_GLASS, reflectance=(1.0, 1.0, 1.0), transmission=(1.0, 1.0, 1.0), ior=1.5)))
+        elif variant == 2:
+            c = (add(_desc(rb.RB_MATERIAL_UBER, remap_roughness=1, diffuse=(0.5, 0.3, 0.2), specular=(0.3, 0.3, 0.25),
+                           reflectance=(0.1, 0.1, 0.1), opacity=(0.8, 0.9, 1.0), roughness_u=0.15, roughness_v=0.2,
+                           ior=1.5)),
+                 add(_desc(rb.RB_MATERIAL_METAL, **metal)))
+        else:
+            inner = add(_desc(rb.RB_MATERIAL_MIXTURE, amount=(0.5, 0.6, 0.7),
+                              components=(add(_desc(rb.RB_MATERIAL_PLASTIC, remap_roughness=1, diffuse=(0.6, 0.3, 0.2),
+                                                    reflectance=(0.5, 0.45, 0.4), roughness_u=0.1, ior=1.49)),
+                                          add(_desc(rb.RB_MATERIAL_MIRROR, reflectance=(0.9, 0.85, 0.8))))))
+            c = (inner, add(_desc(rb.RB_MATERIAL_SUBSTRATE, remap_roughness=1, diffuse=(0.5, 0.35, 0.2),
+                                  reflectance=(0.05, 0.05, 0.05), roughness_u=0.1, roughness_v=0.25)))
+        mats[k] = _desc(rb.RB_MATERIAL_MIXTURE, amount=(0.25 + 0.1 * (k % 3), 0.5, 0.75), components=c)
+    return scene.with_materials(mats + extra)
+
+
+def texture_images():
+    """Two seeded RGB images: 16 x 8 random texels and a 5 x 3 checker of two colours."""
+    rng = np.random.default_rng(23)
+    noise = rng.random((8, 16, 3), dtype=np.float32) * 0.8 + 0.1
+    yy, xx = np.mgrid[0:3, 0:5]
+    checker = np.where(((xx + yy) % 2 == 0)[..., None], np.float32([0.8, 0.2, 0.1]), np.float32([0.1, 0.3, 0.7]))
+    return [noise, checker.astype(np.float32)]
+
+
+def textured_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with image textures (texture_images): every matte material's
+    diffuse from the noise image; every third material (from the second, the
+    floor's) a plastic with a textured diffuse (checker) and specular (noise),
+    every third (from the third) in turn a translucent material with a textured
+    transmission, an uber material with a textured opacity, and a glass with a
+    textured transmission."""
+    mats = []
+    for k in range(scene.desc.num_materials):
+        m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
+        if k % 3 == 1:
+            m = _desc(rb.RB_MATERIAL_PLASTIC, remap_roughness=1, diffuse=(0.5, 0.5, 0.5), reflectance=(0.3, 0.3, 0.3),
+                      roughness_u=0.15, ior=1.49, diffuse_texture=2, reflectance_texture=1)
+        elif k % 3 == 2:
+            variant = (k // 3) % 3
+            if variant == 0:
+                m = _desc(rb.RB_MATERIAL_TRANSLUCENT, remap_roughness=1, diffuse=(0.6, 0.5, 0.4), specular=(0.4, 0.4, 0.4),
+                          reflectance=(0.5, 0.5, 0.5), transmission=(0.4, 0.45, 0.5), roughness_u=0.2, roughness_v=0.2,
+                          transmission_texture=1)
+            elif variant == 1:
+                m = _desc(rb.RB_MATERIAL_UBER, remap_roughness=1, diffuse=(0.5, 0.3, 0.2), specular=(0.3, 0.3, 0.25),
+                          reflectance=(0.1, 0.1, 0.1), opacity=(1.0, 1.0, 1.0), roughness_u=0.15, roughness_v=0.2, ior=1.5,
+                          opacity_texture=2)
+            else:
+                m = _desc(rb.RB_MATERIAL_GLASS, reflectance=(1.0, 1.0, 1.0), transmission=(1.0, 1.0, 1.0), ior=1.5,
+                          transmission_texture=1)
+        elif m.kind == rb.RB_MATERIAL_MATTE:
+            m.diffuse_texture = 1
+        mats.append(m)
+    return scene.with_materials(mats).with_textures(texture_images())
 
 
 def oren_nayar_scene(scene: rb.Scene) -> rb.Scene:

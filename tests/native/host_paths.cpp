@@ -32,6 +32,7 @@ struct host_stack {
 	bool empty() const { return sp == 0; }
 	bool full() const { return sp + 2 > 128; }
 	uint32_t size() const { return sp; }
+	raw_stack raw() { return raw_stack{data, 1u, sp, 128u}; }
 };
 
 struct hp_scene {
@@ -161,9 +162,14 @@ struct hp_batch {
 
 extern "C" {
 
-// The lobe list that the packed record of one material gives make_bsdf: the
-// lobe kinds (LOBE_*) in collection order. Returns the packing status.
+// The lobe list that the packed record of material 0 of `mds` (count materials,
+// a mixture's components among them) gives make_bsdf: the lobe kinds (LOBE_*)
+// in collection order. Returns the packing status.
+int hp_material_set_lobes(const rb_material_desc* mds, uint32_t num, uint32_t* kinds, uint32_t* count);
 int hp_material_lobes(const rb_material_desc* md, uint32_t* kinds, uint32_t* count) {
+	return hp_material_set_lobes(md, 1, kinds, count);
+}
+int hp_material_set_lobes(const rb_material_desc* mds, uint32_t num, uint32_t* kinds, uint32_t* count) {
 	// one triangle with the material, and an environment emitter (a scene needs one)
 	const float pos[9] = {0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f, 0.f};
 	const uint32_t idx[3] = {0, 1, 2};
@@ -186,8 +192,8 @@ int hp_material_lobes(const rb_material_desc* md, uint32_t* kinds, uint32_t* cou
 	rb_scene_desc d{};
 	d.meshes = &mesh;
 	d.num_meshes = 1;
-	d.materials = md;
-	d.num_materials = 1;
+	d.materials = mds;
+	d.num_materials = num;
 	d.emitters = &em;
 	d.num_emitters = 1;
 	d.entities = ents;
@@ -199,6 +205,22 @@ int hp_material_lobes(const rb_material_desc* md, uint32_t* kinds, uint32_t* cou
 	*count = b.count;
 	for (uint32_t i = 0; i < b.count; i++) kinds[i] = lobe_kind(b, i);
 	return RB_OK;
+}
+
+// The kernels' image texture lookup (pt::sample_texture) at n texture coordinates.
+int hp_texture_sample(const float* rgb, uint32_t width, uint32_t height, uint32_t n, const float* uv, float* out) {
+	texture_rec tr{0u, width, height, 0u};
+	scene_view v{};
+	v.textures = &tr;
+	v.texels = rgb;
+	v.num_textures = 1;
+	for (uint32_t i = 0; i < n; i++) {
+		const vec3 c = sample_texture(v, 0u, vec2{uv[2 * i], uv[2 * i + 1]});
+		out[3 * i] = c.x;
+		out[3 * i + 1] = c.y;
+		out[3 * i + 2] = c.z;
+	}
+	return 0;
 }
 
 int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {

@@ -10,7 +10,7 @@ import pytest
 
 import rainbow_b200 as rb
 from oracle import ref
-from tests.helpers import extra_materials_scene, layered_scene, two_level_scene
+from tests.helpers import extra_materials_scene, layered_scene, mixture_scene, textured_scene, two_level_scene
 
 pytestmark = pytest.mark.skipif(not ref.adapter_available(), reason="oracle/_ref/libadapter_check.so not built")
 
@@ -24,12 +24,15 @@ def _scene(name):
     if name == "spheres_layered":
         return layered_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
                                                subdivision=2))
+    if name == "spheres_mixture":
+        return mixture_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
+                                               subdivision=2))
     if name == "fog":
         return rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=40, height=30, num_spheres=6, subdivision=2)
     return two_level_scene()
 
 
-@pytest.mark.parametrize("name", ["box", "spheres_materials", "spheres_layered", "fog", "two_level"])
+@pytest.mark.parametrize("name", ["box", "spheres_materials", "spheres_layered", "spheres_mixture", "fog", "two_level"])
 def test_export_describes_the_reference_scene(name):
     scene = _scene(name)
     R = ref.RefScene(scene)
@@ -40,10 +43,75 @@ def test_export_describes_the_reference_scene(name):
     for e in range(d.num_entities):
         ent = d.entities[e]
         assert bool(has[e, 0]) == (ent.material >= 0) and bool(has[e, 1]) == (ent.emitter >= 0), e
-        if ent.material >= 0:
+        if ent.material >= 0 and d.materials[ent.material].kind != rb.RB_MATERIAL_MIXTURE:
             assert bytes(mats[e]) == bytes(d.materials[ent.material]), f"entity {e}: material differs"
         if ent.emitter >= 0:
             assert bytes(ems[e]) == bytes(d.emitters[ent.emitter]), f"entity {e}: emitter differs"
     for field in ("raster_to_camera", "camera_to_world"):
         assert np.array_equal(np.array(getattr(cam, field)[:], np.float32), np.array(getattr(scene.camera, field)[:], np.float32))
     assert (cam.width, cam.height, cam.lens_radius) == (scene.camera.width, scene.camera.height, scene.camera.lens_radius)
+
+
+def _expand(mats, k):
+    """A material with its mixture components resolved (their indices replaced by the components themselves)."""
+    m = mats[k]
+    if m.kind != rb.RB_MATERIAL_MIXTURE:
+        return bytes(m)
+    own = rb.MaterialDesc.from_buffer_copy(bytes(m))
+    own.components[0] = own.components[1] = 0
+    return (bytes(own), _expand(mats, m.components[0]), _expand(mats, m.components[1]))
+
+
+def test_export_keeps_mixtures():
+    """Mixtures (nested too) are exported with their components, weights and
+    the components' parameters; shared components stay shared."""
+    scene = _scene("spheres_mixture")
+    R = ref.RefScene(scene)
+    mats, ent = ref.adapter_export_materials(R, rb.MaterialDesc)
+    d = scene.desc
+    assert ent.shape[0] == d.num_entities
+    seen = 0
+    for e in range(d.num_entities):
+        k = d.entities[e].material
+        assert (k >= 0) == (ent[e] >= 0)
+        if k >= 0:
+            assert _expand(mats, int(ent[e])) == _expand(d.materials, k), f"entity {e}"
+            seen += d.materials[k].kind == rb.RB_MATERIAL_MIXTURE
+    assert seen > 0
+
+
+_TEX_FIELDS = ("diffuse_texture", "reflectance_texture", "transmission_texture", "specular_texture", "opacity_texture")
+
+
+def test_export_keeps_image_textures():
+    """Image-textured spectra are exported as image textures with the same
+    texels, each texture once, and the material's other parameters kept."""
+    scene = textured_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
+                                             subdivision=2))
+    R = ref.RefScene(scene)
+    mats, ent = ref.adapter_export_materials(R, rb.MaterialDesc)
+    tex = ref.adapter_export_textures(R)
+    src_tex = [np.ctypeslib.as_array(scene.desc.textures[t].rgb, (scene.desc.textures[t].height,
+                                                                  scene.desc.textures[t].width, 3))
+               for t in range(scene.desc.num_textures)]
+    d = scene.desc
+    used = 0
+    for e in range(d.num_entities):
+        k = d.entities[e].material
+        if k < 0:
+            continue
+        a = rb.MaterialDesc.from_buffer_copy(bytes(mats[int(ent[e])]))
+        b = rb.MaterialDesc.from_buffer_copy(bytes(d.materials[k]))
+        for f in _TEX_FIELDS:
+            ra, rb_ = getattr(a, f), getattr(b, f)
+            assert (ra == 0) == (rb_ == 0), (e, f)
+            if ra:
+                assert np.array_equal(tex[ra - 1], src_tex[rb_ - 1]), (e, f)
+                used += 1
+                value = f[:-len("_texture")]  # the constant the texture replaces is not read
+                getattr(a, value)[:] = (0.0, 0.0, 0.0)
+                getattr(b, value)[:] = (0.0, 0.0, 0.0)
+            setattr(a, f, 0)
+            setattr(b, f, 0)
+        assert bytes(a) == bytes(b), f"entity {e}"
+    assert used > 0 and len(tex) == len(src_tex)

@@ -1,4 +1,4 @@
-"""Plastic, mirror, substrate, Oren-Nayar, uber and translucent materials on the GPU: with spp = 1 the film sum of a pixel
+"""Plastic, mirror, substrate, Oren-Nayar, uber, translucent and mixture materials and image textures on the GPU: with spp = 1 the film sum of a pixel
 is one sample's radiance, against the reference's path_integrator::trace on the
 spheres scene with plastic, mirror and substrate materials (golden fixture), and the same
 scene in direct lighting against the host build."""
@@ -8,7 +8,7 @@ import pytest
 import rainbow_b200 as rb
 from tests import golden
 from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, layered_scene,
-                           oren_nayar_scene, per_sample_radiance, scene_from_params)
+                           mixture_scene, oren_nayar_scene, per_sample_radiance, scene_from_params, textured_scene)
 
 pytestmark = pytest.mark.gpu
 
@@ -46,21 +46,25 @@ def test_oren_nayar_samples_match_reference():
     assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], "oren-nayar")
 
 
-def test_layered_samples_match_reference():
-    fx = golden.load("layered_samples")
-    scene = layered_scene(scene_from_params(fx["params"]))
+@pytest.mark.parametrize("name,make", [("layered_samples", layered_scene), ("mixture_samples", mixture_scene),
+                                       ("texture_samples", textured_scene)])
+def test_layered_samples_match_reference(name, make):
+    fx = golden.load(name)
+    scene = make(scene_from_params(fx["params"]))
     with rb.Context(0) as ctx:
         ctx.upload(scene)
         got = per_sample_radiance(ctx, scene, fx["pixels"], fx["samples"], int(fx["max_depth"]))
         assert ctx.stats().device_error == 0
     agree = _agreement(got, fx["radiance"])
     assert agree >= 0.97, f"only {agree:.4f} of samples agree with the reference"
-    assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], "layered")
+    assert_disagreements_unbiased(scene, got, fx["radiance"], fx["first_entity"], name)
 
 
-def test_layered_direct_matches_host_build():
-    fx = golden.load("layered_samples")
-    scene = layered_scene(scene_from_params(fx["params"]))
+@pytest.mark.parametrize("name,make", [("layered_samples", layered_scene), ("mixture_samples", mixture_scene),
+                                       ("texture_samples", textured_scene)])
+def test_layered_direct_matches_host_build(name, make):
+    fx = golden.load(name)
+    scene = make(scene_from_params(fx["params"]))
     W, H = scene.camera.width, scene.camera.height
     px = np.arange(W * H, dtype=np.uint32)
     want = HostPaths(scene).direct_samples(scene.camera, px, np.full_like(px, 2), 4, 4)

@@ -81,11 +81,11 @@ def test_reference_samples_match_fixture(name):
 
 @needs_ref
 @pytest.mark.parametrize("mat", ["lambert", "metal", "glass_rough", "glass_smooth", "plastic", "mirror", "substrate",
-                                 "oren_nayar", "uber", "uber_opaque", "translucent"])
+                                 "oren_nayar", "uber", "uber_opaque", "translucent", "mixture"])
 @pytest.mark.parametrize("inc", ["all", "nonspec"])
 def test_reference_bsdf_matches_fixture(mat, inc):
     fx = golden.load(f"bsdf_{mat}_{inc}")
-    md = material_from_bytes(fx["material"].tobytes())
+    md = material_from_bytes(fx["material"].tobytes(), int(fx["material_count"]) if "material_count" in fx else 1)
     out = ref.bsdf(md, fx["wo"], fx["u"], fx["wi_eval"], int(fx["include"]))
     for k in ("wi", "f", "pdf", "f_eval", "pdf_eval"):
         assert np.array_equal(out[k].view(np.uint32), fx[k].view(np.uint32)), k
