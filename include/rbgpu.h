@@ -102,14 +102,29 @@ enum {
 	                            nest up to 8 deep; at most 6 lobes in all, else RB_ERR_UNSUPPORTED) */
 };
 
-/* An RGB image texture (image_texture_t<2, spectrum>, textures/detail/image_texture.hpp):
- * width * height texels, row-major, texel (x, y) at rgb[3 * (y * width + x)]. Sampled at
- * a hit's uv (the triangle's vertex uvs, or (0, 0), (1, 0), (1, 1) without them) with the
- * uv wrapped to [0, 1) and bilinear filtering between the four nearest texels. */
+enum {
+	RB_TEXTURE_IMAGE = 0,    /* image_texture_t<2, spectrum> (textures/detail/image_texture.hpp) */
+	RB_TEXTURE_SCALE = 1,    /* scale_texture_t<2, spectrum> (textures/detail/scale_texture.hpp):
+	                            base * scale, inputs[0] the scale, inputs[1] the base */
+	RB_TEXTURE_MIXTURE = 2   /* mixture_texture_t<2, spectrum> (textures/detail/mixture_texture.hpp):
+	                            t0 a + t1 clamp(1 - a) with a = clamp(alpha) to [0, 1]; inputs[0] t0,
+	                            inputs[1] t1, inputs[2] alpha (a real texture: channel 0). Like the
+	                            reference, it samples its inputs at the hit point's world x and y */
+};
+
+/* A texture for a material's spectrum. RB_TEXTURE_IMAGE: width * height RGB
+ * texels, row-major, texel (x, y) at rgb[3 * (y * width + x)], sampled at a
+ * hit's uv (the triangle's vertex uvs, or (0, 0), (1, 0), (1, 1) without them)
+ * with the uv wrapped to [0, 1) and bilinear filtering between the four nearest
+ * texels. RB_TEXTURE_SCALE / MIXTURE combine inputs: inputs[i] = k > 0 is
+ * texture k - 1 (an image), 0 the constant constants[i]. */
 typedef struct rb_texture_desc {
 	const float* rgb;
 	uint32_t width;
 	uint32_t height;
+	uint32_t kind;
+	uint32_t inputs[3];
+	float constants[3][3];
 } rb_texture_desc;
 
 /* Material parameters: constant textures (constant_texture_t,

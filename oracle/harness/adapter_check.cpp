@@ -109,7 +109,9 @@ int adp_export_materials(orc_scene* s, rb_material_desc* materials, uint32_t* co
 
 // Texture t of the adapter's export of a harness scene: its size (and the
 // number of textures) first with rgb NULL, then its texels.
-int adp_export_texture(orc_scene* s, uint32_t t, float* rgb, uint32_t* width, uint32_t* height, uint32_t* count) {
+// desc (not NULL): the texture's description, its rgb pointer cleared.
+int adp_export_texture(orc_scene* s, uint32_t t, float* rgb, uint32_t* width, uint32_t* height, uint32_t* count,
+	rb_texture_desc* desc) {
 	std::shared_ptr<scenes::scene> world;
 	std::shared_ptr<cameras::camera> cam;
 	if (!objects(s, world, cam)) return RB_ERR_INVALID_ARGUMENT;
@@ -120,7 +122,12 @@ int adp_export_texture(orc_scene* s, uint32_t t, float* rgb, uint32_t* width, ui
 	if (t >= ex.textures.size()) return RB_OK;
 	*width = ex.textures[t].width;
 	*height = ex.textures[t].height;
-	if (rgb != nullptr) std::memcpy(rgb, ex.textures[t].rgb, 3ull * *width * *height * sizeof(float));
+	if (desc != nullptr) {
+		*desc = ex.textures[t];
+		desc->rgb = nullptr;
+	}
+	if (rgb != nullptr && ex.textures[t].rgb != nullptr)
+		std::memcpy(rgb, ex.textures[t].rgb, 3ull * *width * *height * sizeof(float));
 	return RB_OK;
 }
 

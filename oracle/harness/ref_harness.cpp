@@ -40,6 +40,8 @@
 #include "rainbow-cpu/textures/constant_texture.hpp"
 #include "texture_lookup.hpp"  // before the image texture definitions (shim/)
 #include "rainbow-cpu/textures/image_texture.hpp"
+#include "rainbow-cpu/textures/mixture_texture.hpp"
+#include "rainbow-cpu/textures/scale_texture.hpp"
 #include "rainbow-cpu/shared/accelerators/bounding_volume_hierarchy.hpp"
 #include "rainbow-core/sample_function.hpp"
 
@@ -136,21 +138,43 @@ struct texture_set {
 	const rb_texture_desc* descs = nullptr;
 	uint32_t count = 0;
 	std::vector<std::shared_ptr<texture2d<spectrum>>> made;
-	// a constant texture of v, or with ref > 0 the image texture ref - 1
-	std::shared_ptr<texture2d<spectrum>> spectrum_of(const float* v, uint32_t ref) {
+	// a constant texture of v, or with ref > 0 texture ref - 1: an image, or a
+	// scale_texture_t / mixture_texture_t of images and constants
+	std::shared_ptr<texture2d<spectrum>> spectrum_of(const float* v, uint32_t ref, int depth = 0) {
 		if (ref == 0) return spectrum_texture(v);
-		if (ref > count) return nullptr;
+		if (ref > count || depth > 1) return nullptr;
 		if (made.size() < count) made.resize(count);
 		auto& t = made[ref - 1];
-		if (!t) {
-			const rb_texture_desc& d = descs[ref - 1];
+		if (t) return t;
+		const rb_texture_desc& d = descs[ref - 1];
+		if (d.kind == RB_TEXTURE_IMAGE) {
 			std::vector<spectrum> values;
 			values.reserve(static_cast<size_t>(d.width) * d.height);
 			for (size_t i = 0; i < static_cast<size_t>(d.width) * d.height; i++)
 				values.emplace_back(d.rgb[3 * i], d.rgb[3 * i + 1], d.rgb[3 * i + 2]);
 			t = std::make_shared<image_texture2d<spectrum>>(rainbow::core::math::vector_t<2, size_t>(d.width, d.height), values);
+		} else if (d.kind == RB_TEXTURE_SCALE) {
+			const auto scale = spectrum_of(d.constants[0], d.inputs[0], depth + 1);
+			const auto base = spectrum_of(d.constants[1], d.inputs[1], depth + 1);
+			if (!scale || !base) return nullptr;
+			t = std::make_shared<scale_texture_t<2, spectrum>>(scale, base);
+		} else if (d.kind == RB_TEXTURE_MIXTURE) {
+			const auto t0 = spectrum_of(d.constants[0], d.inputs[0], depth + 1);
+			const auto t1 = spectrum_of(d.constants[1], d.inputs[1], depth + 1);
+			if (!t0 || !t1) return nullptr;
+			t = std::make_shared<mixture_texture_t<2, spectrum>>(t0, t1, real_of(d.constants[2][0], d.inputs[2]));
+		} else {
+			return nullptr;
 		}
 		return t;
+	}
+	// a real texture: a constant, or channel 0 of image ref - 1
+	std::shared_ptr<texture2d<real>> real_of(float v, uint32_t ref) {
+		if (ref == 0 || ref > count || descs[ref - 1].kind != RB_TEXTURE_IMAGE) return real_texture(v);
+		const rb_texture_desc& d = descs[ref - 1];
+		std::vector<real> values;
+		for (size_t i = 0; i < static_cast<size_t>(d.width) * d.height; i++) values.push_back(d.rgb[3 * i]);
+		return std::make_shared<image_texture2d<real>>(rainbow::core::math::vector_t<2, size_t>(d.width, d.height), values);
 	}
 };
 

@@ -248,7 +248,7 @@ def adapter_lib():
         L.adp_export_materials.restype = i32
         L.adp_export_materials.argtypes = [vp, vp, C.POINTER(u32), vp, C.POINTER(u32)]
         L.adp_export_texture.restype = i32
-        L.adp_export_texture.argtypes = [vp, u32, vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
+        L.adp_export_texture.argtypes = [vp, u32, vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), vp]
         _ADAPTER = L
     return _ADAPTER
 
@@ -274,17 +274,22 @@ def adapter_export_materials(R, material_type):
     return mats, ent[:ne.value]
 
 
-def adapter_export_textures(R):
-    """The adapter's exported image textures of R's reference scene, as (height, width, 3) arrays in export order."""
+def adapter_export_textures(R, texture_type):
+    """The adapter's exported textures of R's reference scene in export order: (description with its rgb
+    pointer cleared, (height, width, 3) texels of an image or None)."""
     L = adapter_lib()
     w, h, n = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    _ok(L.adp_export_texture(R.h, 0, None, C.byref(w), C.byref(h), C.byref(n)), "adp_export_texture")
+    _ok(L.adp_export_texture(R.h, 0, None, C.byref(w), C.byref(h), C.byref(n), None), "adp_export_texture")
     out = []
     for t in range(n.value):
-        _ok(L.adp_export_texture(R.h, t, None, C.byref(w), C.byref(h), C.byref(n)), "adp_export_texture")
-        a = np.zeros((h.value, w.value, 3), dtype=np.float32)
-        _ok(L.adp_export_texture(R.h, t, a.ctypes.data, C.byref(w), C.byref(h), C.byref(n)), "adp_export_texture")
-        out.append(a)
+        d = texture_type()
+        _ok(L.adp_export_texture(R.h, t, None, C.byref(w), C.byref(h), C.byref(n), C.byref(d)), "adp_export_texture")
+        a = None
+        if w.value and h.value:
+            a = np.zeros((h.value, w.value, 3), dtype=np.float32)
+            _ok(L.adp_export_texture(R.h, t, a.ctypes.data, C.byref(w), C.byref(h), C.byref(n), None),
+                "adp_export_texture")
+        out.append((d, a))
     return out
 
 

@@ -23,7 +23,7 @@ import numpy as np
 from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_BVH_ALL_TRIANGLES, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_MIRROR, RB_MATERIAL_PLASTIC, RB_MATERIAL_SUBSTRATE,
-    RB_MATERIAL_MIXTURE, RB_MATERIAL_TRANSLUCENT, RB_MATERIAL_UBER,
+    RB_MATERIAL_MIXTURE, RB_MATERIAL_TRANSLUCENT, RB_MATERIAL_UBER, RB_TEXTURE_IMAGE, RB_TEXTURE_MIXTURE, RB_TEXTURE_SCALE,
     RB_RENDER_GUIDE,
     RB_RENDER_DIRECT, RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
     RB_SHADOW_CLOSEST, RB_SHADOW_FIRST_OCCLUDER, RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,
@@ -66,17 +66,27 @@ class Scene:
         return Scene(None, d, self.camera, keepalive=[self, arr])
 
     def with_textures(self, textures) -> "Scene":
-        """A view of this scene with image textures (a sequence of (height, width, 3) float32 arrays) that
-        materials refer to by index + 1 in their *_texture fields."""
-        arrs = [np.ascontiguousarray(t, dtype=np.float32) for t in textures]
-        descs = (TextureDesc * max(1, len(arrs)))()
-        for k, a in enumerate(arrs):
+        """A view of this scene with textures that materials refer to by index + 1 in their *_texture fields:
+        each a (height, width, 3) float32 image, or a dict (kind=RB_TEXTURE_SCALE / RB_TEXTURE_MIXTURE,
+        inputs=[texture index + 1 or 0], constants=[rgb of the constant inputs])."""
+        arrs = []
+        descs = (TextureDesc * max(1, len(textures)))()
+        for k, t in enumerate(textures):
+            if isinstance(t, dict):
+                descs[k].kind = t["kind"]
+                for i, v in enumerate(t.get("inputs", ())):
+                    descs[k].inputs[i] = v
+                for i, c in enumerate(t.get("constants", ())):
+                    descs[k].constants[i][:] = [float(x) for x in c]
+                continue
+            a = np.ascontiguousarray(t, dtype=np.float32)
+            arrs.append(a)
             descs[k].rgb = a.ctypes.data_as(C.POINTER(C.c_float))
             descs[k].height, descs[k].width = a.shape[0], a.shape[1]
         d = SceneDesc()
         C.pointer(d)[0] = self.desc
         d.textures = C.cast(descs, type(d.textures))
-        d.num_textures = len(arrs)
+        d.num_textures = len(textures)
         return Scene(None, d, self.camera, keepalive=[self, descs] + arrs)
 
     def with_bvh(self, bvh: "Bvh") -> "Scene":

@@ -26,6 +26,9 @@ RB_MATERIAL_SUBSTRATE = 5
 RB_MATERIAL_UBER = 6
 RB_MATERIAL_TRANSLUCENT = 7
 RB_MATERIAL_MIXTURE = 8
+RB_TEXTURE_IMAGE = 0
+RB_TEXTURE_SCALE = 1
+RB_TEXTURE_MIXTURE = 2
 RB_EMITTER_SURFACE, RB_EMITTER_ENVIRONMENT = 0, 1
 RB_SCENE_BOX, RB_SCENE_SPHERES, RB_SCENE_SLIT_ROOM, RB_SCENE_FOG = 0, 1, 2, 3
 RB_RENDER_RESET = 1
@@ -64,7 +67,8 @@ class MaterialDesc(C.Structure):
 
 
 class TextureDesc(C.Structure):
-    _fields_ = [("rgb", C.POINTER(C.c_float)), ("width", C.c_uint32), ("height", C.c_uint32)]
+    _fields_ = [("rgb", C.POINTER(C.c_float)), ("width", C.c_uint32), ("height", C.c_uint32), ("kind", C.c_uint32),
+                ("inputs", C.c_uint32 * 3), ("constants", (C.c_float * 3) * 3)]
 
 
 class MediumDesc(C.Structure):

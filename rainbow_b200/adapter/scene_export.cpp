@@ -37,6 +37,8 @@ namespace rainbow::cpus::textures {
 using rainbow::core::math::clamp;
 }
 #include "rainbow-cpu/textures/image_texture.hpp"
+#include "rainbow-cpu/textures/mixture_texture.hpp"
+#include "rainbow-cpu/textures/scale_texture.hpp"
 
 #include <functional>
 #include <unordered_map>
@@ -51,6 +53,7 @@ template <auto Member, typename Tag>
 struct access_bind {
 	friend constexpr auto member_of(Tag) { return Member; }
 };
+#define COMMA ,
 #define RB_PRIVATE_MEMBER(tag, member)                              \
 	struct tag { friend constexpr auto member_of(tag); };          \
 	template struct access_bind<&member, tag>
@@ -102,6 +105,11 @@ RB_PRIVATE_MEMBER(translucent_roughness, materials::translucent_material::mRough
 RB_PRIVATE_MEMBER(translucent_remap, materials::translucent_material::mMapRoughnessToAlpha);
 RB_PRIVATE_MEMBER(mixture_alpha, materials::mixture_material::mAlpha);
 RB_PRIVATE_MEMBER(mixture_materials, materials::mixture_material::mMaterials);
+RB_PRIVATE_MEMBER(scale_scale, textures::scale_texture_t<2 COMMA shared::spectrums::spectrum>::mScale);
+RB_PRIVATE_MEMBER(scale_base, textures::scale_texture_t<2 COMMA shared::spectrums::spectrum>::mBase);
+RB_PRIVATE_MEMBER(mixture_t0, textures::mixture_texture_t<2 COMMA shared::spectrums::spectrum>::mTexture0);
+RB_PRIVATE_MEMBER(mixture_t1, textures::mixture_texture_t<2 COMMA shared::spectrums::spectrum>::mTexture1);
+RB_PRIVATE_MEMBER(mixture_alpha_texture, textures::mixture_texture_t<2 COMMA shared::spectrums::spectrum>::mAlpha);
 RB_PRIVATE_MEMBER(surface_radiance, emitters::surface_light::mRadiance);
 RB_PRIVATE_MEMBER(environment_map, emitters::environment_light::mEnvironmentMap);
 RB_PRIVATE_MEMBER(environment_intensity, emitters::environment_light::mIntensity);
@@ -114,6 +122,7 @@ RB_PRIVATE_MEMBER(camera_focus, cameras::projective_camera::mFocus);
 RB_PRIVATE_MEMBER(camera_lens, cameras::projective_camera::mLens);
 RB_PRIVATE_MEMBER(camera_to_world, cameras::camera::mCameraToWorld);
 #undef RB_PRIVATE_MEMBER
+#undef COMMA
 
 template <typename Tag, typename Object>
 const auto& read(const Object& o, Tag tag) { return o.*member_of(tag); }
@@ -153,29 +162,71 @@ struct texture_registry {
 	bool spectrum(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, float* rgb, uint32_t& ref) {
 		ref = 0;
 		if (constant_rgb(t, rgb)) return true;
-		const auto img = std::dynamic_pointer_cast<textures::image_texture2d<shared::spectrums::spectrum>>(t);
-		if (img == nullptr) return false;
-		const auto it = ref_of.find(img.get());
+		if (image(t, ref)) return true;
+		return composite(t, ref);
+	}
+	// A scale or mixture texture whose inputs are images or constants.
+	bool composite(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, uint32_t& ref) {
+		using S = shared::spectrums::spectrum;
+		const auto it = ref_of.find(t.get());
 		if (it != ref_of.end()) {
 			ref = it->second;
 			return true;
 		}
-		const auto size = img->size();
-		if (size.x == 0 || size.y == 0 || size.x > (1u << 15) || size.y > (1u << 15)) return false;
-		std::vector<float> texels(3 * size.x * size.y);
-		for (size_t i = 0; i < size.x * size.y; i++) {
-			const auto v = img->value(i);
-			texels[3 * i] = v[0];
-			texels[3 * i + 1] = v[1];
-			texels[3 * i + 2] = v[2];
-		}
-		out.texels.push_back(std::move(texels));
 		rb_texture_desc td{};
-		td.width = static_cast<uint32_t>(size.x);
-		td.height = static_cast<uint32_t>(size.y);
+		const auto input = [&](const std::shared_ptr<textures::texture2d<S>>& in, uint32_t i) {
+			return constant_rgb(in, td.constants[i]) || image(in, td.inputs[i]);
+		};
+		if (const auto x = std::dynamic_pointer_cast<textures::scale_texture_t<2, S>>(t)) {
+			td.kind = RB_TEXTURE_SCALE;
+			if (!input(read(*x, scale_scale{}), 0) || !input(read(*x, scale_base{}), 1)) return false;
+		} else if (const auto x = std::dynamic_pointer_cast<textures::mixture_texture_t<2, S>>(t)) {
+			td.kind = RB_TEXTURE_MIXTURE;
+			if (!input(read(*x, mixture_t0{}), 0) || !input(read(*x, mixture_t1{}), 1)) return false;
+			// the real-valued alpha: a constant, or a real image exported as an RGB image (channel 0)
+			const auto& alpha = read(*x, mixture_alpha_texture{});
+			if (!constant_real(alpha, td.constants[2][0])) {
+				const auto img = std::dynamic_pointer_cast<textures::image_texture2d<rainbow::core::real>>(alpha);
+				if (img == nullptr || !add_image(img.get(), img->size().x, img->size().y,
+						[&](size_t i, float* c) { c[0] = c[1] = c[2] = img->value(i); }, td.inputs[2]))
+					return false;
+			}
+		} else {
+			return false;
+		}
+		out.texels.emplace_back();
 		out.textures.push_back(td);
 		ref = static_cast<uint32_t>(out.textures.size());
-		ref_of.emplace(img.get(), ref);
+		ref_of.emplace(t.get(), ref);
+		return true;
+	}
+	// An RGB image texture, exported once.
+	bool image(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, uint32_t& ref) {
+		const auto img = std::dynamic_pointer_cast<textures::image_texture2d<shared::spectrums::spectrum>>(t);
+		if (img == nullptr) return false;
+		return add_image(img.get(), img->size().x, img->size().y, [&](size_t i, float* c) {
+			const auto v = img->value(i);
+			c[0] = v[0]; c[1] = v[1]; c[2] = v[2];
+		}, ref);
+	}
+	template <typename Texel>
+	bool add_image(const void* key, size_t w, size_t h, Texel texel, uint32_t& ref) {
+		const auto it = ref_of.find(key);
+		if (it != ref_of.end()) {
+			ref = it->second;
+			return true;
+		}
+		if (w == 0 || h == 0 || w > (1u << 15) || h > (1u << 15)) return false;
+		std::vector<float> texels(3 * w * h);
+		for (size_t i = 0; i < w * h; i++) texel(i, texels.data() + 3 * i);
+		out.texels.push_back(std::move(texels));
+		rb_texture_desc td{};
+		td.kind = RB_TEXTURE_IMAGE;
+		td.width = static_cast<uint32_t>(w);
+		td.height = static_cast<uint32_t>(h);
+		out.textures.push_back(td);
+		ref = static_cast<uint32_t>(out.textures.size());
+		ref_of.emplace(key, ref);
 		return true;
 	}
 };
@@ -393,7 +444,8 @@ rb_status export_scene(const scenes::scene& s, exported_scene& out) {
 	d.num_mediums = static_cast<uint32_t>(out.mediums.size());
 	d.media = out.media.data();
 	d.num_media = static_cast<uint32_t>(out.media.size());
-	for (size_t t = 0; t < out.textures.size(); t++) out.textures[t].rgb = out.texels[t].data();
+	for (size_t t = 0; t < out.textures.size(); t++)
+		out.textures[t].rgb = out.texels[t].empty() ? nullptr : out.texels[t].data();
 	d.textures = out.textures.data();
 	d.num_textures = static_cast<uint32_t>(out.textures.size());
 	return RB_OK;

@@ -253,14 +253,28 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 		if (desc->num_textures > 0 && desc->textures == nullptr) return RB_ERR_INVALID_ARGUMENT;
 		for (uint32_t t = 0; t < desc->num_textures; t++) {
 			const rb_texture_desc& td = desc->textures[t];
-			if (td.rgb == nullptr || td.width == 0 || td.height == 0 || td.width > (1u << 15) || td.height > (1u << 15))
-				return RB_ERR_INVALID_ARGUMENT;
 			pt::texture_rec tr{};
-			tr.offset = static_cast<uint32_t>(out.texels.size());
-			tr.width = td.width;
-			tr.height = td.height;
-			if (out.texels.size() + 3ull * td.width * td.height > 0xffffffffull) return RB_ERR_INVALID_ARGUMENT;
-			out.texels.insert(out.texels.end(), td.rgb, td.rgb + 3ull * td.width * td.height);
+			tr.kind = td.kind;
+			if (td.kind == RB_TEXTURE_IMAGE) {
+				if (td.rgb == nullptr || td.width == 0 || td.height == 0 || td.width > (1u << 15) || td.height > (1u << 15))
+					return RB_ERR_INVALID_ARGUMENT;
+				tr.offset = static_cast<uint32_t>(out.texels.size());
+				tr.width = td.width;
+				tr.height = td.height;
+				if (out.texels.size() + 3ull * td.width * td.height > 0xffffffffull) return RB_ERR_INVALID_ARGUMENT;
+				out.texels.insert(out.texels.end(), td.rgb, td.rgb + 3ull * td.width * td.height);
+			} else if (td.kind == RB_TEXTURE_SCALE || td.kind == RB_TEXTURE_MIXTURE) {
+				// inputs: images or constants (one level of composition)
+				for (uint32_t i = 0; i < 3; i++) {
+					const uint32_t in = td.inputs[i];
+					if (in > desc->num_textures) return RB_ERR_INVALID_ARGUMENT;
+					if (in && desc->textures[in - 1].kind != RB_TEXTURE_IMAGE) return RB_ERR_UNSUPPORTED;
+					tr.inputs[i] = in;
+					tr.constants[i] = v3(td.constants[i], 0);
+				}
+			} else {
+				return RB_ERR_INVALID_ARGUMENT;
+			}
 			out.textures.push_back(tr);
 		}
 		{
@@ -659,7 +673,9 @@ rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out
 				out.material_srcs.push_back(ms);
 			}
 			for (pt::texture_rec tr : p.textures) {
-				tr.offset += texel_base;
+				if (tr.kind == pt::TEXK_IMAGE) tr.offset += texel_base;
+				for (uint32_t i = 0; i < 3; i++)
+					if (tr.inputs[i]) tr.inputs[i] += texture_base;
 				out.textures.push_back(tr);
 			}
 			append_vec(out.texels, p.texels);

@@ -239,7 +239,7 @@ __device__ bool continue_guided(const scene_view& s, path_state& p, const shade_
 	float& pb_out) {
 	const surface_t& si = rec.si;
 	material_rec mat_scratch;
-	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si.uv, mat_scratch));
+	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si, mat_scratch));
 	const vec3 wo = to_local(si, si.wo);
 	const float alpha = g[guide::kAlphaOff];
 	const float u_sel = pcg_real(p.rng);

@@ -62,7 +62,7 @@ RB_HD void direct_radiance(const scene_view& s, const direct_cfg& cfg, path_stat
 		bsdf_t b;
 		b.count = 0;
 		material_rec mat_scratch;
-		if (ent.flags & ENT_HAS_MATERIAL) b = make_bsdf(hit_material(s, static_cast<uint32_t>(ent.material), si.uv, mat_scratch));
+		if (ent.flags & ENT_HAS_MATERIAL) b = make_bsdf(hit_material(s, static_cast<uint32_t>(ent.material), si.uv, si.p, mat_scratch));
 		if (b.count == 0) {
 			// no scattering functions: continue the ray through the surface
 			const ray_t r = spawn_ray(si.p, si.n, d);
@@ -166,7 +166,7 @@ RB_HD int direct_surface(const scene_view& s, path_state& p, const hit_t& h, dir
 	if (ent.flags & ENT_HAS_EMITTER) p.L = p.L + surface_emission(ent, s.emitters[ent.emitter], si.n, -p.d);
 	material_rec mat_scratch;
 	if (!(ent.flags & ENT_HAS_MATERIAL) ||
-		make_bsdf(hit_material(s, static_cast<uint32_t>(ent.material), si.uv, mat_scratch)).count == 0) {
+		make_bsdf(hit_material(s, static_cast<uint32_t>(ent.material), si.uv, si.p, mat_scratch)).count == 0) {
 		const ray_t r = spawn_ray(si.p, si.n, p.d);
 		p.o = r.o;
 		p.d = r.d;
@@ -185,7 +185,7 @@ template <int MAT = MAT_ANY>
 RB_HD void direct_next_bsdf(const scene_view& s, path_state& p, direct_record& rec, ray_t& out) {
 	const surface_t& si = rec.si;
 	material_rec mat_scratch;
-	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si.uv, mat_scratch));
+	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si, mat_scratch));
 	const lobe_sample bs = bsdf_sample<MAT>(b, to_local(si, si.wo), pcg_2d(p.rng), ST_ALL);
 	const vec3 wi = bs.pdf > 0.f ? to_world(si, bs.wi) : vec3{0.f, 0.f, 0.f};
 	const spectrum v = bs.f * fabs_ref(dot(wi, si.sz));
@@ -205,7 +205,7 @@ RB_HD void direct_sample_lights(const scene_view& s, const direct_cfg& cfg, path
 	ray_t* out) {
 	const surface_t& si = rec.si;
 	material_rec mat_scratch;
-	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si.uv, mat_scratch));
+	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si, mat_scratch));
 	const vec3 wo = to_local(si, si.wo);
 	const float n_emitters = static_cast<float>(s.num_emitters);
 	const float pick_pdf = 1.f / n_emitters;

@@ -10,6 +10,7 @@
 
 #include "../../../include/rbgpu.h"
 #include "pt_bsdf.h"
+#include "pt_geom.h"
 
 namespace rb {
 namespace pt {
@@ -154,8 +155,7 @@ RB_HD bool build_record(const material_src& p, const vec3* scale, material_rec& 
 // uv wrapped to [0, 1) (glm::mod(x, 1) = x - floor(x)), scaled to texels and
 // shifted by half a texel, the four neighbours clamped to the image, and two
 // lerps s (1 - x) + t x along u then one along v.
-RB_HD spectrum sample_texture(const scene_view& s, uint32_t t, vec2 uv) {
-	const texture_rec tr = s.textures[t];
+RB_HD spectrum sample_image(const scene_view& s, const texture_rec& tr, vec2 uv) {
 	const float* px = s.texels + tr.offset;
 	const float fw = static_cast<float>(tr.width), fh = static_cast<float>(tr.height);
 	const float x = (uv.x - floorf(uv.x)) * fw - 0.5f;
@@ -175,28 +175,55 @@ RB_HD spectrum sample_texture(const scene_view& s, uint32_t t, vec2 uv) {
 	return v0 * (1.f - dv) + v1 * dv;
 }
 
-// The record of material `index` at a hit with texture coordinates uv: the
-// uploaded record, or for MAT_TEXTURED one built into `scratch` from the
-// material's parameters with its textured spectra sampled at uv.
-RB_HD const material_rec* hit_material(const scene_view& s, uint32_t index, vec2 uv, material_rec& scratch) {
+// Input i of a composite texture at coordinates c: its image, or its constant.
+RB_HD spectrum texture_input(const scene_view& s, const texture_rec& tr, uint32_t i, vec2 c) {
+	return tr.inputs[i] ? sample_image(s, s.textures[tr.inputs[i] - 1u], c) : tr.constants[i];
+}
+
+// Texture t at a hit with texture coordinates uv and world point p, as
+// texture_t::sample(surface_interaction) does: an image samples uv; a scale
+// texture samples its inputs at uv and gives base * scale
+// (textures/detail/scale_texture.hpp:33-43); a mixture samples its inputs at
+// (p.x, p.y), the interaction's point converted to a 2D coordinate
+// (textures/detail/mixture_texture.hpp:36-48), and gives t0 a + t1 clamp(1 - a)
+// with a = clamp(alpha, 0, 1).
+RB_HD spectrum sample_texture(const scene_view& s, uint32_t t, vec2 uv, vec3 p) {
+	const texture_rec& tr = s.textures[t];
+	switch (tr.kind) {
+	case TEXK_SCALE: return texture_input(s, tr, 1u, uv) * texture_input(s, tr, 0u, uv);
+	case TEXK_MIXTURE: {
+		const vec2 c{p.x, p.y};
+		const float a0 = fclamp_ref(texture_input(s, tr, 2u, c).x, 0.f, 1.f);
+		const float a1 = fclamp_ref(1.f - a0, 0.f, 1.f);
+		return texture_input(s, tr, 0u, c) * a0 + texture_input(s, tr, 1u, c) * a1;
+	}
+	default: return sample_image(s, tr, uv);
+	}
+}
+
+// The record of material `index` at a hit with texture coordinates uv and
+// world point p: the uploaded record, or for MAT_TEXTURED one built into
+// `scratch` from the material's parameters with its textured spectra sampled.
+RB_HD const material_rec* hit_material(const scene_view& s, uint32_t index, vec2 uv, vec3 p, material_rec& scratch) {
 	const material_rec* m = s.materials + index;
 	if (m->kind != MAT_TEXTURED) return m;
-	material_src p = s.material_srcs[m->src];
-	if (p.tex[TEX_DIFFUSE]) p.diffuse = sample_texture(s, p.tex[TEX_DIFFUSE] - 1u, uv);
-	if (p.tex[TEX_REFLECTANCE]) p.reflectance = sample_texture(s, p.tex[TEX_REFLECTANCE] - 1u, uv);
-	if (p.tex[TEX_TRANSMISSION]) p.transmission = sample_texture(s, p.tex[TEX_TRANSMISSION] - 1u, uv);
-	if (p.tex[TEX_SPECULAR]) p.specular = sample_texture(s, p.tex[TEX_SPECULAR] - 1u, uv);
-	if (p.tex[TEX_OPACITY]) p.opacity = sample_texture(s, p.tex[TEX_OPACITY] - 1u, uv);
-	build_record(p, nullptr, scratch);
+	material_src q = s.material_srcs[m->src];
+	if (q.tex[TEX_DIFFUSE]) q.diffuse = sample_texture(s, q.tex[TEX_DIFFUSE] - 1u, uv, p);
+	if (q.tex[TEX_REFLECTANCE]) q.reflectance = sample_texture(s, q.tex[TEX_REFLECTANCE] - 1u, uv, p);
+	if (q.tex[TEX_TRANSMISSION]) q.transmission = sample_texture(s, q.tex[TEX_TRANSMISSION] - 1u, uv, p);
+	if (q.tex[TEX_SPECULAR]) q.specular = sample_texture(s, q.tex[TEX_SPECULAR] - 1u, uv, p);
+	if (q.tex[TEX_OPACITY]) q.opacity = sample_texture(s, q.tex[TEX_OPACITY] - 1u, uv, p);
+	build_record(q, nullptr, scratch);
 	return &scratch;
 }
 
 // The record a shading stage uses at a hit: a shading class's material kind
 // (MAT) is never textured (textured records are shaded as MAT_ANY).
 template <int MAT>
-RB_HD const material_rec* surface_material(const scene_view& s, uint32_t index, vec2 uv, material_rec& scratch) {
+RB_HD const material_rec* surface_material(const scene_view& s, uint32_t index, const surface_t& si,
+	material_rec& scratch) {
 	if constexpr (MAT != MAT_ANY) return s.materials + index;
-	else return hit_material(s, index, uv, scratch);
+	else return hit_material(s, index, si.uv, si.p, scratch);
 }
 
 } // namespace pt

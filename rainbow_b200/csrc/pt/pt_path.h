@@ -170,7 +170,7 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 	}
 	rec.material = static_cast<uint32_t>(ent.material);
 	material_rec mat_scratch;
-	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si.uv, mat_scratch));
+	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si, mat_scratch));
 	if (bsdf_count(b, ST_NON_SPECULAR) == 0) return true;
 	rec.did_nee = 1u;
 	rec.guidable = bsdf_count(b, ST_SPECULAR) == 0 ? 1u : 0u;
@@ -266,7 +266,7 @@ template <int MAT = MAT_ANY>
 RB_HD bool continue_bsdf(const scene_view& s, path_state& p, const shade_record& rec, vec3& wi_out, float& pdf_out) {
 	const surface_t& si = rec.si;
 	material_rec mat_scratch;
-	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si.uv, mat_scratch));
+	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si, mat_scratch));
 	const vec3 wo = to_local(si, si.wo);
 	const lobe_sample bs = bsdf_sample<MAT>(b, wo, pcg_2d(p.rng), ST_ALL);
 	if (is_black(bs.f) || bs.pdf == 0.f) return false;

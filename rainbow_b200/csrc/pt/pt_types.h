@@ -174,11 +174,17 @@ struct material_src {
 	uint32_t tex[kNumTexSlots];  // 0: the constant above; k > 0: texture k - 1 of the scene
 };
 
-// An RGB image texture: texels row-major, (x, y) at data[offset + 3 (y width + x)].
+enum : uint32_t { TEXK_IMAGE = 0, TEXK_SCALE = 1, TEXK_MIXTURE = 2 };
+
+// A texture: an RGB image (texels row-major, (x, y) at texels[offset + 3 (y
+// width + x)]), or a scale / mixture of inputs that are images (inputs[i] =
+// image index + 1) or constants (inputs[i] = 0: constants[i]).
 struct texture_rec {
-	uint32_t offset;          // in floats
+	uint32_t kind;
+	uint32_t offset;          // image: in floats
 	uint32_t width, height;
-	uint32_t pad;
+	uint32_t inputs[3];
+	spectrum constants[3];
 };
 
 enum : uint32_t { EMIT_SURFACE = 0, EMIT_ENVIRONMENT = 1 };

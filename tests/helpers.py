@@ -496,19 +496,29 @@ def texture_images():
     return [noise, checker.astype(np.float32)]
 
 
+def scene_textures():
+    """texture_images, then a scale texture (a constant times the checker) and a mixture texture (noise and
+    checker mixed by the noise's first channel), as textures 1-4."""
+    return texture_images() + [
+        dict(kind=rb.RB_TEXTURE_SCALE, inputs=[0, 2], constants=[(0.5, 0.7, 0.9)]),
+        dict(kind=rb.RB_TEXTURE_MIXTURE, inputs=[1, 2, 1]),
+    ]
+
+
 def textured_scene(scene: rb.Scene) -> rb.Scene:
-    """The scene with image textures (texture_images): every matte material's
-    diffuse from the noise image; every third material (from the second, the
-    floor's) a plastic with a textured diffuse (checker) and specular (noise),
-    every third (from the third) in turn a translucent material with a textured
-    transmission, an uber material with a textured opacity, and a glass with a
-    textured transmission."""
+    """The scene with textures (scene_textures): every matte material's diffuse
+    from the noise image or (every other one) the mixture texture; every third
+    material (from the second, the floor's) a plastic with its diffuse from the
+    scale texture and its specular from the noise, every third (from the third)
+    in turn a translucent material with a textured transmission, an uber
+    material with a textured opacity, and a glass whose transmission is the
+    mixture texture."""
     mats = []
     for k in range(scene.desc.num_materials):
         m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
         if k % 3 == 1:
             m = _desc(rb.RB_MATERIAL_PLASTIC, remap_roughness=1, diffuse=(0.5, 0.5, 0.5), reflectance=(0.3, 0.3, 0.3),
-                      roughness_u=0.15, ior=1.49, diffuse_texture=2, reflectance_texture=1)
+                      roughness_u=0.15, ior=1.49, diffuse_texture=3, reflectance_texture=1)
         elif k % 3 == 2:
             variant = (k // 3) % 3
             if variant == 0:
@@ -521,11 +531,11 @@ def textured_scene(scene: rb.Scene) -> rb.Scene:
                           opacity_texture=2)
             else:
                 m = _desc(rb.RB_MATERIAL_GLASS, reflectance=(1.0, 1.0, 1.0), transmission=(1.0, 1.0, 1.0), ior=1.5,
-                          transmission_texture=1)
+                          transmission_texture=4)
         elif m.kind == rb.RB_MATERIAL_MATTE:
-            m.diffuse_texture = 1
+            m.diffuse_texture = 1 if k % 2 == 0 else 4
         mats.append(m)
-    return scene.with_materials(mats).with_textures(texture_images())
+    return scene.with_materials(mats).with_textures(scene_textures())
 
 
 def oren_nayar_scene(scene: rb.Scene) -> rb.Scene:

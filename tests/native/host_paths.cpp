@@ -209,13 +209,16 @@ int hp_material_set_lobes(const rb_material_desc* mds, uint32_t num, uint32_t* k
 
 // The kernels' image texture lookup (pt::sample_texture) at n texture coordinates.
 int hp_texture_sample(const float* rgb, uint32_t width, uint32_t height, uint32_t n, const float* uv, float* out) {
-	texture_rec tr{0u, width, height, 0u};
+	texture_rec tr{};
+	tr.kind = TEXK_IMAGE;
+	tr.width = width;
+	tr.height = height;
 	scene_view v{};
 	v.textures = &tr;
 	v.texels = rgb;
 	v.num_textures = 1;
 	for (uint32_t i = 0; i < n; i++) {
-		const vec3 c = sample_texture(v, 0u, vec2{uv[2 * i], uv[2 * i + 1]});
+		const vec3 c = sample_texture(v, 0u, vec2{uv[2 * i], uv[2 * i + 1]}, vec3{0.f, 0.f, 0.f});
 		out[3 * i] = c.x;
 		out[3 * i + 1] = c.y;
 		out[3 * i + 2] = c.z;

@@ -83,18 +83,40 @@ def test_export_keeps_mixtures():
 _TEX_FIELDS = ("diffuse_texture", "reflectance_texture", "transmission_texture", "specular_texture", "opacity_texture")
 
 
+def _resolve_texture(descs, texels, ref, channel0=False):
+    """Texture ref (index + 1) with its inputs resolved: an image's shape and texel bytes (channel 0 alone for
+    a mixture's real-valued alpha), or a composite's kind, resolved inputs and the constants it reads."""
+    d = descs[ref - 1]
+    if d.kind == rb.RB_TEXTURE_IMAGE:
+        a = texels(ref - 1)
+        return ("image", a.shape[:2], np.ascontiguousarray(a[..., 0] if channel0 else a).tobytes())
+    mixture = d.kind == rb.RB_TEXTURE_MIXTURE
+    out = [d.kind]
+    for i in range(3 if mixture else 2):
+        alpha = mixture and i == 2
+        if d.inputs[i]:
+            out.append(_resolve_texture(descs, texels, d.inputs[i], channel0=alpha))
+        else:
+            out.append((d.constants[i][0],) if alpha else tuple(d.constants[i]))
+    return tuple(out)
+
+
 def test_export_keeps_image_textures():
-    """Image-textured spectra are exported as image textures with the same
-    texels, each texture once, and the material's other parameters kept."""
+    """Image, scale and mixture textures of material spectra are exported with
+    the same texels, inputs and constants, each texture once, and the
+    material's other parameters kept."""
     scene = textured_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
                                              subdivision=2))
     R = ref.RefScene(scene)
     mats, ent = ref.adapter_export_materials(R, rb.MaterialDesc)
-    tex = ref.adapter_export_textures(R)
-    src_tex = [np.ctypeslib.as_array(scene.desc.textures[t].rgb, (scene.desc.textures[t].height,
-                                                                  scene.desc.textures[t].width, 3))
-               for t in range(scene.desc.num_textures)]
+    exported = ref.adapter_export_textures(R, rb.TextureDesc)
     d = scene.desc
+    src_descs = [d.textures[t] for t in range(d.num_textures)]
+
+    def src_texels(t):
+        return np.ctypeslib.as_array(d.textures[t].rgb, (d.textures[t].height, d.textures[t].width, 3))
+
+    exp_descs = [e[0] for e in exported]
     used = 0
     for e in range(d.num_entities):
         k = d.entities[e].material
@@ -106,7 +128,8 @@ def test_export_keeps_image_textures():
             ra, rb_ = getattr(a, f), getattr(b, f)
             assert (ra == 0) == (rb_ == 0), (e, f)
             if ra:
-                assert np.array_equal(tex[ra - 1], src_tex[rb_ - 1]), (e, f)
+                assert _resolve_texture(exp_descs, lambda t: exported[t][1], ra) == \
+                    _resolve_texture(src_descs, src_texels, rb_), (e, f)
                 used += 1
                 value = f[:-len("_texture")]  # the constant the texture replaces is not read
                 getattr(a, value)[:] = (0.0, 0.0, 0.0)
@@ -114,4 +137,5 @@ def test_export_keeps_image_textures():
             setattr(a, f, 0)
             setattr(b, f, 0)
         assert bytes(a) == bytes(b), f"entity {e}"
-    assert used > 0 and len(tex) == len(src_tex)
+    kinds = {dd.kind for dd in exp_descs}
+    assert used > 0 and kinds == {rb.RB_TEXTURE_IMAGE, rb.RB_TEXTURE_SCALE, rb.RB_TEXTURE_MIXTURE}
