@@ -596,24 +596,46 @@ def main():
     # ---- end to end through the C ABI with host buffers (params in, image out every step), with the
     # launch shapes tuned for one-sample calls (untimed), as a caller rendering progressively would
     timed_tuning = ctx.tuning()
+    # every step: one rb_render_async call (its parameters in by kernel argument), the step's image out to its
+    # own page-locked buffer; the calls overlap on the GPU and rb_render_wait ends the run
+    imgs = [torch.zeros((H, W, 3), dtype=torch.float32, pin_memory=True) for _ in range(args.steps)]
+
+    def async_calls(n, first):
+        for k in range(n):
+            p = rb.RenderParams()
+            p.camera = scene.camera
+            p.spp, p.first_sample, p.max_depth, p.rr_threshold, p.seed = 1, first + k, depth, 1.0, 0
+            p.flags = rb.RB_RENDER_RESET if k == 0 else 0
+            rb.check(rb.lib().rb_render_async(ctx._h, ctypes.byref(p), ctypes.c_void_p(imgs[k].data_ptr())),
+                     "rb_render_async")
+        rb.check(rb.lib().rb_render_wait(ctx._h), "rb_render_wait")
+
     e2e_tuning = None
     if not args.tuning and not args.no_tune:
+        # launch shapes for back-to-back one-sample calls (untimed): the tuner's pick for one synchronous call,
+        # then the wave sizes and lane counts around it (and the timed call's shapes), each run as the timed
+        # loop runs them (overlapping async calls, images read back), the fastest kept
         t1, _ = ctx.tune_render(scene.camera, probe_spp=1, max_depth=depth, seed=base + 999)
-        e2e_tuning = t1.as_dict()
-    # every step: one rb_render_async call (its parameters in by kernel argument), the step's image out to its
-    # own page-locked buffer (a ring of 4, as a double-buffering viewer would keep them); the calls overlap on the
-    # GPU and rb_render_wait ends the run
-    imgs = [torch.zeros((H, W, 3), dtype=torch.float32, pin_memory=True) for _ in range(min(4, args.steps))]
+        cands = [t1.as_dict(), dict(timed_tuning.as_dict())]
+        for ppw in (1 << 18, 1 << 19, 1 << 20):
+            for lanes in (2, 4, 8):
+                cands.append(dict(t1.as_dict(), paths_per_wave=ppw, lanes=lanes))
+        best = None
+        n_probe = min(8, args.steps)
+        for c in cands:
+            ctx.set_tuning(**c)
+            async_calls(2, base + 5000)  # graph capture for these shapes
+            t0 = time.perf_counter()
+            async_calls(n_probe, base + 6000)
+            dt = time.perf_counter() - t0
+            if best is None or dt < best[0]:
+                best = (dt, c)
+        e2e_tuning = dict(best[1], probe_calls=n_probe, probe_ms=best[0] * 1e3, candidates=len(cands))
+        ctx.set_tuning(**best[1])
+    async_calls(2, base + 7000)  # warm-up: graphs of the chosen shapes
     barrier()
     t0 = time.perf_counter()
-    for k in range(args.steps):
-        p = rb.RenderParams()
-        p.camera = scene.camera
-        p.spp, p.first_sample, p.max_depth, p.rr_threshold, p.seed = 1, base + k, depth, 1.0, 0
-        p.flags = rb.RB_RENDER_RESET if k == 0 else 0
-        rb.check(rb.lib().rb_render_async(ctx._h, ctypes.byref(p), ctypes.c_void_p(imgs[k % len(imgs)].data_ptr())),
-                 "rb_render_async")
-    rb.check(rb.lib().rb_render_wait(ctx._h), "rb_render_wait")
+    async_calls(args.steps, base)
     barrier()
     e2e_s = time.perf_counter() - t0
     tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
