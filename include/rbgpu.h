@@ -96,6 +96,14 @@ enum {
 	                            transmission (if diffuse is not black), Trowbridge-Reitz reflection of
 	                            specular reflectance and transmission of specular transmission (if
 	                            specular is not black), isotropic roughness_u */
+	RB_MATERIAL_SUBSURFACE = 9, /* rainbow-cpu/materials/subsurface_material.cpp:24-66: glass lobes of
+	                            reflectance / transmission (Fresnel-specular when both roughnesses are
+	                            0, else Trowbridge-Reitz reflection and transmission, IOR ior) and a
+	                            normalized-diffusion BSSRDF (scatterings/bssrdf/normalized_diffusion.cpp)
+	                            of albedo diffuse and mean free path mfp; nothing when reflectance or
+	                            transmission is black, and nothing inside a mixture. Plain path tracing
+	                            and direct lighting only (guided and volume renders return
+	                            RB_ERR_UNSUPPORTED) */
 	RB_MATERIAL_MIXTURE = 8  /* rainbow-cpu/materials/mixture_material.cpp:13-43: the lobes of material
 	                            components[0] built with the weight amount and of components[1] with
 	                            clamp(1 - amount), each by its material's build with a scale (mixtures
@@ -153,6 +161,7 @@ typedef struct rb_material_desc {
 	uint32_t transmission_texture;
 	uint32_t specular_texture;
 	uint32_t opacity_texture;
+	float mfp[3];               /* subsurface: mean free path (RGB) */
 } rb_material_desc;
 
 enum {

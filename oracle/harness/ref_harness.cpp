@@ -33,6 +33,7 @@
 #include "rainbow-cpu/materials/mirror_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
 #include "rainbow-cpu/materials/substrate_material.hpp"
+#include "rainbow-cpu/materials/subsurface_material.hpp"
 #include "rainbow-cpu/materials/translucent_material.hpp"
 #include "rainbow-cpu/materials/uber_material.hpp"
 #include "rainbow-cpu/emitters/surface_light.hpp"
@@ -211,6 +212,9 @@ std::shared_ptr<material> make_material(const rb_material_desc* all, uint32_t co
 	case RB_MATERIAL_TRANSLUCENT:
 		return std::make_shared<translucent_material>(transmission, reflectance, specular, diffuse,
 			real_texture(m.roughness_u), m.remap_roughness != 0);
+	case RB_MATERIAL_SUBSURFACE:
+		return std::make_shared<subsurface_material>(transmission, reflectance, diffuse, spectrum_texture(m.mfp),
+			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
 	case RB_MATERIAL_MIXTURE: {
 		if (m.components[0] < 0 || m.components[1] < 0) return nullptr;
 		const auto m0 = make_material(all, count, static_cast<uint32_t>(m.components[0]), tex, depth + 1);

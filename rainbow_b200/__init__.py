@@ -23,7 +23,7 @@ import numpy as np
 from ._native import (  # noqa: F401  (re-exported constants)
     GUIDE_SAMPLE_DTYPE, HIT_DTYPE, RAY_DTYPE, RB_BVH_ALL_TRIANGLES, RB_EMITTER_ENVIRONMENT, RB_EMITTER_SURFACE, RB_GUIDE_NUM_PARAMS,
     RB_GUIDE_OUTPUTS, RB_GUIDE_SEQUENTIAL, RB_MATERIAL_GLASS, RB_MATERIAL_MATTE, RB_MATERIAL_METAL, RB_MATERIAL_MIRROR, RB_MATERIAL_PLASTIC, RB_MATERIAL_SUBSTRATE,
-    RB_MATERIAL_MIXTURE, RB_MATERIAL_TRANSLUCENT, RB_MATERIAL_UBER, RB_TEXTURE_IMAGE, RB_TEXTURE_MIXTURE, RB_TEXTURE_SCALE,
+    RB_MATERIAL_MIXTURE, RB_MATERIAL_SUBSURFACE, RB_MATERIAL_TRANSLUCENT, RB_MATERIAL_UBER, RB_TEXTURE_IMAGE, RB_TEXTURE_MIXTURE, RB_TEXTURE_SCALE,
     RB_RENDER_GUIDE,
     RB_RENDER_DIRECT, RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
     RB_SHADOW_CLOSEST, RB_SHADOW_FIRST_OCCLUDER, RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,

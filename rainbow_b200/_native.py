@@ -26,6 +26,7 @@ RB_MATERIAL_SUBSTRATE = 5
 RB_MATERIAL_UBER = 6
 RB_MATERIAL_TRANSLUCENT = 7
 RB_MATERIAL_MIXTURE = 8
+RB_MATERIAL_SUBSURFACE = 9
 RB_TEXTURE_IMAGE = 0
 RB_TEXTURE_SCALE = 1
 RB_TEXTURE_MIXTURE = 2
@@ -63,7 +64,7 @@ class MaterialDesc(C.Structure):
                 ("roughness_u", C.c_float), ("roughness_v", C.c_float), ("specular", F3), ("opacity", F3),
                 ("components", C.c_int32 * 2), ("amount", F3), ("diffuse_texture", C.c_uint32),
                 ("reflectance_texture", C.c_uint32), ("transmission_texture", C.c_uint32),
-                ("specular_texture", C.c_uint32), ("opacity_texture", C.c_uint32)]
+                ("specular_texture", C.c_uint32), ("opacity_texture", C.c_uint32), ("mfp", F3)]
 
 
 class TextureDesc(C.Structure):

@@ -21,6 +21,7 @@
 #include "rainbow-cpu/materials/mixture_material.hpp"
 #include "rainbow-cpu/materials/plastic_material.hpp"
 #include "rainbow-cpu/materials/substrate_material.hpp"
+#include "rainbow-cpu/materials/subsurface_material.hpp"
 #include "rainbow-cpu/materials/translucent_material.hpp"
 #include "rainbow-cpu/materials/uber_material.hpp"
 #include "rainbow-cpu/media/homogeneous_medium.hpp"
@@ -103,6 +104,14 @@ RB_PRIVATE_MEMBER(translucent_specular, materials::translucent_material::mSpecul
 RB_PRIVATE_MEMBER(translucent_diffuse, materials::translucent_material::mDiffuse);
 RB_PRIVATE_MEMBER(translucent_roughness, materials::translucent_material::mRoughness);
 RB_PRIVATE_MEMBER(translucent_remap, materials::translucent_material::mMapRoughnessToAlpha);
+RB_PRIVATE_MEMBER(subsurface_transmission, materials::subsurface_material::mTransmission);
+RB_PRIVATE_MEMBER(subsurface_reflectance, materials::subsurface_material::mReflectance);
+RB_PRIVATE_MEMBER(subsurface_diffuse, materials::subsurface_material::mDiffuse);
+RB_PRIVATE_MEMBER(subsurface_mfp, materials::subsurface_material::mMFP);
+RB_PRIVATE_MEMBER(subsurface_ru, materials::subsurface_material::mRoughnessU);
+RB_PRIVATE_MEMBER(subsurface_rv, materials::subsurface_material::mRoughnessV);
+RB_PRIVATE_MEMBER(subsurface_eta, materials::subsurface_material::mEta);
+RB_PRIVATE_MEMBER(subsurface_remap, materials::subsurface_material::mMapRoughnessToAlpha);
 RB_PRIVATE_MEMBER(mixture_alpha, materials::mixture_material::mAlpha);
 RB_PRIVATE_MEMBER(mixture_materials, materials::mixture_material::mMaterials);
 RB_PRIVATE_MEMBER(scale_scale, textures::scale_texture_t<2 COMMA shared::spectrums::spectrum>::mScale);
@@ -285,8 +294,16 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 			spec(read(*x, translucent_diffuse{}), d.diffuse, d.diffuse_texture) &&
 			constant_real(read(*x, translucent_roughness{}), d.roughness_u);
 		d.roughness_v = d.roughness_u;
+	} else if (const auto x = std::dynamic_pointer_cast<materials::subsurface_material>(m)) {
+		d.kind = RB_MATERIAL_SUBSURFACE;
+		d.remap_roughness = read(*x, subsurface_remap{}) ? 1 : 0;
+		ok = spec(read(*x, subsurface_transmission{}), d.transmission, d.transmission_texture) &&
+			spec(read(*x, subsurface_reflectance{}), d.reflectance, d.reflectance_texture) &&
+			spec(read(*x, subsurface_diffuse{}), d.diffuse, d.diffuse_texture) &&
+			constant_rgb(read(*x, subsurface_mfp{}), d.mfp) && constant_real(read(*x, subsurface_ru{}), d.roughness_u) &&
+			constant_real(read(*x, subsurface_rv{}), d.roughness_v) && constant_real(read(*x, subsurface_eta{}), d.ior);
 	} else {
-		return RB_ERR_UNSUPPORTED;  // subsurface (a mixture is exported by export_scene)
+		return RB_ERR_UNSUPPORTED;  // a material kind outside these (a mixture is exported by export_scene)
 	}
 	return ok ? RB_OK : RB_ERR_UNSUPPORTED;  // a texture that is neither constant nor an RGB image
 }

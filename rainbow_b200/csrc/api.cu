@@ -210,6 +210,7 @@ rb_status capture_into(rb_context* c, const gpu::wave_buffers& w, cudaStream_t s
 	key.tail = cfg.tail;
 	key.refill = cfg.refill;
 	key.shadow_first = cfg.shadow_first;
+	key.sss = cfg.sss;
 	key.carveout = cfg.carveout;
 	if (cfg.guide) {
 		key.guide_steps = cfg.guide->cfg.steps_per_wave;
@@ -665,6 +666,7 @@ rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
 	RB_CUDA(dev_upload(&d.material_srcs, p.material_srcs, c->stream));
 	RB_CUDA(dev_upload(&d.textures, p.textures, c->stream));
 	RB_CUDA(dev_upload(&d.texels, p.texels, c->stream));
+	RB_CUDA(dev_upload(&d.sss_table, p.sss_table, c->stream));
 	RB_CUDA(cudaStreamSynchronize(c->stream));
 	pt::scene_view v{};
 	v.wnodes = p.wide_ok ? d.wnodes : nullptr;
@@ -687,6 +689,8 @@ rb_status upload_packed(rb_context* c, const host::packed_scene& p) {
 	v.textures = d.textures;
 	v.texels = d.texels;
 	v.num_textures = static_cast<uint32_t>(p.textures.size());
+	v.sss_table = p.sss_table.empty() ? nullptr : d.sss_table;
+	v.sss = p.sss_table.empty() ? 0u : 1u;
 	c->view = v;
 	c->bvh_depth = p.bvh_depth;
 	c->num_entities = v.num_entities;
@@ -980,6 +984,8 @@ static rb_status render_call(rb_context* c, const rb_render_params* prm, float* 
 			if (direct_emitter == 0 || direct_bsdf == 0) return RB_ERR_INVALID_ARGUMENT;
 		}
 	}
+	// the BSSRDF stage runs in the plain path tracer only
+	if (c->view.sss && (prm->flags & (RB_RENDER_GUIDE | RB_RENDER_TRAIN | RB_RENDER_VOLUME))) return RB_ERR_UNSUPPORTED;
 	RB_CUDA(cudaSetDevice(c->device));
 	rb_status st = ensure_film(c, cam.width, cam.height, (prm->flags & RB_RENDER_RESET) != 0);
 	if (st != RB_OK) return st;

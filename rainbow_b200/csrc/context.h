@@ -75,11 +75,12 @@ struct device_scene {
 	pt::material_src* material_srcs = nullptr;
 	pt::texture_rec* textures = nullptr;
 	float* texels = nullptr;
+	float* sss_table = nullptr;
 	void release() {
 		dev_free(wnodes); dev_free(nodes); dev_free(tri_a); dev_free(tri_b); dev_free(tri_c); dev_free(prim_index); dev_free(prim_entity);
 		dev_free(entities); dev_free(meshes); dev_free(positions); dev_free(normals); dev_free(tangents); dev_free(uvs);
 		dev_free(indices); dev_free(materials); dev_free(emitters); dev_free(environments);
-		dev_free(mediums); dev_free(media); dev_free(material_srcs); dev_free(textures); dev_free(texels);
+		dev_free(mediums); dev_free(media); dev_free(material_srcs); dev_free(textures); dev_free(texels); dev_free(sss_table);
 	}
 };
 
@@ -93,13 +94,15 @@ struct graph_key {
 	uint32_t block_trace = 0, block_shade = 0, grid_trace = 0, grid_shade = 0, sort = 0, tail = 0;
 	bool refill = false;
 	bool shadow_first = false;
+	bool sss = false;
 	int carveout = 0;
 	bool operator==(const graph_key& o) const {
 		return capacity == o.capacity && max_depth == o.max_depth && stack == o.stack && count == o.count &&
 			guide_mode == o.guide_mode && guide_steps == o.guide_steps && guide_batch == o.guide_batch &&
 			volume == o.volume && batch == o.batch && block_trace == o.block_trace && block_shade == o.block_shade &&
 			grid_trace == o.grid_trace && grid_shade == o.grid_shade && sort == o.sort && tail == o.tail &&
-			with_end == o.with_end && refill == o.refill && carveout == o.carveout && shadow_first == o.shadow_first;
+			with_end == o.with_end && refill == o.refill && carveout == o.carveout && shadow_first == o.shadow_first &&
+			sss == o.sss;
 	}
 };
 
@@ -271,6 +274,7 @@ struct rb_context {
 			if (volume && guide_medium.ready) c.guide_medium = &guide_medium;
 		}
 		c.volume = volume;
+		c.sss = view.sss != 0u;
 		return c;
 	}
 	gpu::launch_cfg profiled_cfg() {

@@ -13,6 +13,7 @@
 #include "../pt/pt_bsdf.h"
 #include "../pt/pt_geom.h"
 #include "../pt/pt_material.h"
+#include "../pt/pt_sss.h"
 
 #include <cmath>
 #include <cstring>
@@ -65,6 +66,8 @@ bool make_src(const rb_material_desc& md, pt::material_src& p) {
 		p.cond_k = v3(md.k, 0);
 		return true;
 	case RB_MATERIAL_GLASS:
+	case RB_MATERIAL_SUBSURFACE:
+		p.mfp = v3(md.mfp, 0);
 		p.smooth = (md.roughness_u == 0.f && md.roughness_v == 0.f) ? 1u : 0u;
 		if (!p.smooth) {
 			p.alpha_x = alpha(md.roughness_u);
@@ -280,6 +283,13 @@ rb_status pack_scene(const rb_scene_desc* desc, packed_scene& out) {
 		{
 			const rb_status st = pack_materials(desc, out.materials, out.material_srcs);
 			if (st != RB_OK) return st;
+			bool sss = false;
+			for (const pt::material_rec& m : out.materials) sss = sss || m.sss;
+			for (const pt::material_src& m : out.material_srcs) sss = sss || m.kind == RB_MATERIAL_SUBSURFACE;
+			if (sss) {
+				out.sss_table.resize(pt::kSssTableSize);
+				pt::sss_build_table(out.sss_table.data());
+			}
 		}
 		// ---- homogeneous media and media components
 		if ((desc->num_mediums > 0 && desc->mediums == nullptr) || (desc->num_media > 0 && desc->media == nullptr))
@@ -679,6 +689,7 @@ rb_status merge_scenes(const std::vector<packed_scene>& parts, packed_scene& out
 				out.textures.push_back(tr);
 			}
 			append_vec(out.texels, p.texels);
+			if (!p.sss_table.empty()) out.sss_table = p.sss_table;
 			for (pt::emitter_rec e : p.emitters) {
 				e.entity += static_cast<int32_t>(entity_base);
 				out.emitters.push_back(e);
@@ -750,6 +761,8 @@ pt::scene_view host_view(const packed_scene& p) {
 	v.textures = p.textures.data();
 	v.texels = p.texels.data();
 	v.num_textures = static_cast<uint32_t>(p.textures.size());
+	v.sss_table = p.sss_table.empty() ? nullptr : p.sss_table.data();
+	v.sss = p.sss_table.empty() ? 0u : 1u;
 	return v;
 }
 

@@ -27,6 +27,7 @@ struct packed_scene {
 	std::vector<pt::material_src> material_srcs;  // parameters of the MAT_TEXTURED records
 	std::vector<pt::texture_rec> textures;
 	std::vector<float> texels;
+	std::vector<float> sss_table;                 // the normalized-diffusion inverse CDF when some material has a BSSRDF
 	std::vector<pt::emitter_rec> emitters;
 	std::vector<pt::medium_rec> mediums;
 	std::vector<pt::media_rec> media;

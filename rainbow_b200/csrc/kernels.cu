@@ -378,6 +378,11 @@ __device__ __forceinline__ void store_path(const wave_buffers& w, uint32_t i, co
 	if (w.medium != nullptr) w.medium[i] = st.medium;
 }
 
+// Queue of the paths of the subsurface stage: the medium class's segment of
+// the class queues, which only volume renders use (those refuse subsurface
+// materials).
+__device__ __forceinline__ uint32_t* sss_queue(const wave_buffers& w) { return w.class_queue + CLASS_MEDIUM * w.capacity; }
+
 __device__ __forceinline__ void finish(const wave_buffers& w, uint32_t i, vec3 L) {
 	w.result[i] = make_float4(L.x, L.y, L.z, 1.f);
 }
@@ -1114,7 +1119,7 @@ __global__ void __launch_bounds__(256) k_shade_b(scene_view s_all, wave_buffers 
 	uint32_t* qn = w.queue[queue_in ^ 1u];
 	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
 		const uint32_t k = base + threadIdx.x;
-		bool alive = false;
+		bool alive = false, sss = false;
 		uint32_t i = 0;
 		if (k < n) {
 			i = q[k];
@@ -1132,10 +1137,78 @@ __global__ void __launch_bounds__(256) k_shade_b(scene_view s_all, wave_buffers 
 						: shade_b<class_material(CLASS)>(s, st, rec, sh, mh, p.max_depth, p.rr_threshold);
 				if (!alive) finish(w, i, st.L);
 				store_path(w, i, st);
+				// paths whose BSDF sample entered a subsurface material go on in k_subsurface
+				sss = CLASS == CLASS_OTHER && alive && (st.flags & PATH_SSS);
 			}
+		}
+		if (CLASS == CLASS_OTHER) {
+			warp_push(sss, i, sss_queue(w), w.counters + CNT_SSS);
+			alive = alive && !sss;
 		}
 		warp_push(alive, i, qn, w.counters + CNT_NEXT);
 	}
+}
+
+// ------------------------------------------------------------------ subsurface
+// The BSSRDF stage of the paths that k_shade_b<CLASS_OTHER> queued: a path
+// whose BSDF sample transmitted into a subsurface material takes its exit
+// point, the light sample there and its continuation
+// (sample_scattering_surface_function, integrator.cpp:290-327), then Russian
+// roulette, as path_integrator::trace orders them (path_integrator.cpp:30-43).
+// The probe rays and the exit's shadow and MIS rays are traced in the thread:
+// few paths reach this stage, and each needs two probe walks whose lengths
+// depend on the geometry.
+// One ray of the subsurface stage, closest hit (shadow: visible entities
+// only), out of line so that the stage's several call sites share one copy of
+// the traversal. A full stack sets `failed` and reports no hit.
+template <bool INST>
+__device__ __noinline__ hit_t sss_trace(const scene_view& s, vec3 o, vec3 d, float& len, bool shadow, smem_stack& stk,
+	bool& failed) {
+	hit_t h{-1, 0.f, 0.f};
+	uint32_t nodes = 0, tris = 0;
+	const bool ok = shadow ? trace_one<true, false, INST>(s, o, d, len, h, stk, nodes, tris)
+		: trace_one<false, false, INST>(s, o, d, len, h, stk, nodes, tris);
+	if (!ok) {
+		failed = true;
+		h.slot = -1;
+	}
+	return h;
+}
+
+// Counting passes count the stage's rays but not their box and triangle tests.
+template <bool BATCH, bool INST>
+__global__ void __launch_bounds__(256) k_subsurface(scene_view s_all, wave_buffers w, uint32_t queue_in, uint32_t stack_cap) {
+	extern __shared__ uint32_t smem[];
+	smem_stack stk = make_stack(smem, stack_cap);
+	const wave_params& p = *w.params;
+	const uint32_t n = w.counters[CNT_SSS];
+	const uint32_t* q = sss_queue(w);
+	uint32_t* qn = w.queue[queue_in ^ 1u];
+	uint32_t nprobe = 0, nshadow = 0;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
+		bool alive = false;
+		uint32_t i = 0;
+		if (k < n) {
+			i = q[k];
+			path_state st = load_path<BATCH>(w, p, i);
+			const scene_view s = BATCH ? batch_view(s_all, w.batch[w.scene[i]]) : s_all;
+			bool failed = false;
+			auto trace = [&](vec3 o, vec3 d, float& len, bool shadow) {
+				if (shadow) nshadow++;
+				else nprobe++;
+				return sss_trace<INST>(s, o, d, len, shadow, stk, failed);
+			};
+			st.flags &= ~PATH_SSS;
+			alive = subsurface_walk(s, st, w.rec[i], to_hit(w.hit[i]), trace) && roulette(st, p.max_depth, p.rr_threshold);
+			if (failed) set_error(w.counters, RB_ERR_STACK_OVERFLOW);
+			if (!alive) finish(w, i, st.L);
+			store_path(w, i, st);
+		}
+		warp_push(alive, i, qn, w.counters + CNT_NEXT);
+	}
+	warp_add64(w.counters, CNT_EXTEND_RAYS, nprobe);
+	warp_add64(w.counters, CNT_SHADOW_RAYS, nshadow);
 }
 
 // ------------------------------------------------------------------ tail
@@ -1653,6 +1726,7 @@ __global__ void k_advance(uint32_t* counters) {
 	counters[CNT_BEAM] = 0u;
 	for (uint32_t c = 0; c < NUM_CLASSES; c++) counters[CNT_CLASS + c] = 0u;
 	counters[CNT_TAIL] = 0u;
+	counters[CNT_SSS] = 0u;
 	counters[CNT_FETCH_EXTEND] = 0u;
 	counters[CNT_FETCH_SECONDARY] = 0u;
 }
@@ -1709,6 +1783,11 @@ cudaError_t bounce(const scene_view& s, const wave_buffers& w, const film_buffer
 		k_shade_b<CLASS_GLASS_ROUGH, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
 	}
 	k_shade_b<CLASS_OTHER, BATCH><<<cfg.grid_shade, cfg.block_shade, 0, stream>>>(s, w, queue_in);
+	if (cfg.sss) {
+		e = allow_smem(k_subsurface<BATCH, INST>, smem, cfg.carveout);
+		if (e != cudaSuccess) return e;
+		k_subsurface<BATCH, INST><<<cfg.grid_trace, cfg.block_trace, smem, stream>>>(s, w, queue_in, cfg.stack_depth);
+	}
 	k_advance<<<1, 1, 0, stream>>>(w.counters);
 	return cudaGetLastError();
 }
@@ -1760,8 +1839,10 @@ void direct_secondary(const scene_view& s, const wave_buffers& wr, const launch_
 
 // Whether a wave ends with the tail kernel after cfg.tail bounces (plain
 // surface path tracing only: guided and volume paths keep their stages).
+// Scenes with subsurface materials run every bounce staged: their BSSRDF
+// stage is a kernel of its own (k_subsurface), not part of the tail.
 bool uses_tail(uint32_t max_depth, const launch_cfg& cfg) {
-	return cfg.tail < max_depth && !cfg.volume && cfg.guide == nullptr;
+	return cfg.tail < max_depth && !cfg.volume && cfg.guide == nullptr && !cfg.sss;
 }
 
 template <bool BATCH>
@@ -1933,7 +2014,7 @@ cudaError_t launch_drain_step(cudaGraphConditionalHandle h, uint32_t* counters, 
 uint32_t bounce_launches(const launch_cfg& cfg) {
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 	if (cfg.volume) return 12u + (sample ? (cfg.guide_medium != nullptr ? 2u : 1u) : 0u);
-	return (cfg.sort == RB_SORT_NONE ? 7u : 12u) + (sample ? 1u : 0u);
+	return (cfg.sort == RB_SORT_NONE ? 7u : 12u) + (sample ? 1u : 0u) + (cfg.sss ? 1u : 0u);
 }
 
 uint32_t drain_launches(const launch_cfg& cfg) { return 2u * bounce_launches(cfg) + 1u; }
@@ -1955,10 +2036,11 @@ uint32_t wave_launches_unbinned(uint32_t max_depth, const launch_cfg& cfg) {
 		return n;
 	}
 	if (uses_tail(max_depth, cfg)) return 3u + (cfg.sort == RB_SORT_NONE ? 7u : 12u) * cfg.tail + 2u;
-	if (cfg.sort == RB_SORT_NONE && cfg.guide == nullptr) return 3u + 7u * max_depth;
+	const uint32_t sss = cfg.sss ? 1u : 0u;
+	if (cfg.sort == RB_SORT_NONE && cfg.guide == nullptr) return 3u + (7u + sss) * max_depth;
 	const bool sample = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_SAMPLE);
 	const bool train = cfg.guide != nullptr && (cfg.guide_mode & GUIDE_TRAIN);
-	uint32_t n = 3u + (12u + (sample ? 1u : 0u)) * max_depth;
+	uint32_t n = 3u + (12u + sss + (sample ? 1u : 0u)) * max_depth;
 	if (train) n += 3u + 2u * cfg.guide->cfg.steps_per_wave;
 	return n;
 }

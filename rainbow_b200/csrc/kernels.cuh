@@ -5,6 +5,7 @@
 #include "guide/guide_host.h"
 #include "pt/pt_direct.h"
 #include "pt/pt_path.h"
+#include "pt/pt_sss.h"
 
 #include <cuda_runtime.h>
 
@@ -36,7 +37,8 @@ enum : uint32_t {
 	// kTimerWords words each from these (even, so the 64-bit words are aligned)
 	CNT_TIMER_EXTEND = 30,
 	CNT_TIMER_SECONDARY = 40,
-	CNT_WORDS = 50
+	CNT_SSS = 50,           // paths queued for the subsurface stage this bounce
+	CNT_WORDS = 52          // even, so that each lane's 64-bit words stay aligned
 };
 // launch timer layout, offsets from its first word: the complement of the
 // earliest warp start (64-bit, so that an atomic max keeps the minimum), the
@@ -45,7 +47,7 @@ enum : uint32_t {
 enum : uint32_t { TIMER_START = 0, TIMER_END = 2, TIMER_WARPS = 4, TIMER_TOTAL_NS = 6, TIMER_LAUNCHES = 8, kTimerWords = 10 };
 static_assert(CNT_TIMER_EXTEND % 2 == 0 && CNT_TIMER_SECONDARY % 2 == 0, "64-bit timer words must be aligned");
 static_assert(CNT_TIMER_EXTEND >= CNT_DRAIN_TOTAL + 1 && CNT_TIMER_SECONDARY >= CNT_TIMER_EXTEND + kTimerWords &&
-	CNT_WORDS >= CNT_TIMER_SECONDARY + kTimerWords, "counter words overlap");
+	CNT_SSS >= CNT_TIMER_SECONDARY + kTimerWords && CNT_WORDS > CNT_SSS && CNT_WORDS % 2 == 0, "counter words overlap");
 static_assert(CNT_CLASS + pt::NUM_CLASSES <= CNT_GUIDE, "class counters overlap");
 // words cleared at the start of a wave: everything before the 64-bit stats
 constexpr uint32_t kWaveCounterWords = CNT_EXTEND_RAYS;
@@ -181,6 +183,7 @@ struct launch_cfg {
 	uint32_t tail = 0xffffffffu;  // bounces of separate stages before the tail kernel (>= max_depth: none)
 	bool refill = false;     // traversal kernels: persistent lanes that take a new ray when theirs is done
 	bool shadow_first = false;  // NEE shadow rays of plain path tracing as occlusion queries (k_trace_secondary)
+	bool sss = false;        // subsurface materials: a k_subsurface launch after shade_b, every bounce staged
 	int carveout = 100;      // traversal kernels' preferred shared-memory carve-out, percent
 };
 

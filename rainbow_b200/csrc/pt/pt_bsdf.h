@@ -210,7 +210,8 @@ enum : uint32_t { LOBE_LAMBERT = 0, LOBE_MF_REFLECT = 1, LOBE_MF_TRANSMIT = 2, L
 	LOBE_L_MF_REFLECT = 9,        // microfacet_reflection(TR, dielectric Fresnel (1, eta), R)
 	LOBE_L_MF_TRANSMIT = 10,      // microfacet_transmission(TR, T, 1, eta)
 	LOBE_L_SPECULAR_REFLECT = 11, // specular_reflection(dielectric Fresnel (1, eta), R)
-	LOBE_L_SPECULAR_TRANSMIT = 12 // specular_transmission(T, 1, lobe_eta)
+	LOBE_L_SPECULAR_TRANSMIT = 12, // specular_transmission(T, 1, lobe_eta)
+	LOBE_SSS_EXIT = 13            // separable_bssrdf_reflection(eta) at a subsurface walk's exit
 };
 
 // The lobe list: kinds (4 bits each) and scattering types (5 bits each) packed
@@ -277,6 +278,10 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 		b.kinds = m->lobe_kinds;
 		b.types = m->lobe_types;
 		b.count = m->lobe_count;
+		break;
+	case MAT_SSS_EXIT:
+		// sample_scattering_surface_function's collection (scattering_surface_function.cpp:131-135)
+		add_lobe(b, LOBE_SSS_EXIT, ST_DIFFUSE | ST_REFLECTION);
 		break;
 	case MAT_MIXTURE:
 		// mixture_material::build_surface_properties (mixture_material.cpp:13-27): the
@@ -391,6 +396,23 @@ RB_HD spectrum oren_nayar_f(const material_rec* m, vec3 wo, vec3 wi) {
 	return m->diffuse * kInvPi * (m->alpha_x + m->alpha_y * max_cos * sin_alpha * tan_beta);
 }
 
+// fresnel_moment1 (scatterings/reflection/separable_bssrdf_reflection.cpp:7-20):
+// the first moment of the dielectric Fresnel reflectance as a polynomial in
+// eta, the published fit of d'Eon and Irving (2011), in float.
+RB_HD float fresnel_moment1(float eta) {
+	const float eta2 = eta * eta, eta3 = eta2 * eta, eta4 = eta3 * eta, eta5 = eta4 * eta;
+	if (eta < 1.f)
+		return 0.45966f - 1.73965f * eta + 3.37668f * eta2 - 3.904945f * eta3 + 2.49277f * eta4 - 0.68441f * eta5;
+	return -4.61686f + 11.1136f * eta - 10.4646f * eta2 + 5.11455f * eta3 - 1.27198f * eta4 + 0.12746f * eta5;
+}
+// separable_bssrdf_reflection::evaluate (separable_bssrdf_reflection.cpp:27-34),
+// radiance transport: (1 - Fr(cos theta_i)) / (c pi) eta^2, c = 1 - 2 moment1(1 / eta).
+RB_HD float sss_exit_f(float eta, float cos_i) {
+	const float c = 1.f - 2.f * fresnel_moment1(1.f / eta);
+	const float value = (1.f - fresnel_dielectric(cos_i, 1.f, eta)) / (c * kPi);
+	return value * (eta * eta);
+}
+
 // The record a lobe reads and the lobe's index in it: the material's own
 // record, or for a mixture the component record the lobe came from.
 template <int MAT = MAT_ANY>
@@ -422,6 +444,7 @@ RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		case LOBE_L_LAMBERT_TRANSMIT: return layered_r(b, i) * kInvPi;
 		case LOBE_L_MF_REFLECT: return mf_reflect_f<MAT_ANY>(m, wo, wi, layered_r(b, i));
 		case LOBE_L_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, layered_r(b, i));
+		case LOBE_SSS_EXIT: return splat3(sss_exit_f(m->eta, wi.z));
 		default: return spectrum{0.f, 0.f, 0.f};  // specular lobes evaluate to 0
 		}
 	}
@@ -437,7 +460,8 @@ RB_HD float lobe_pdf(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT:
 		case LOBE_OREN_NAYAR:
-		case LOBE_L_LAMBERT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
+		case LOBE_L_LAMBERT:
+		case LOBE_SSS_EXIT: return same_hemisphere(wo, wi) ? cosine_hemisphere_pdf(fabs_ref(wi.z)) : 0.f;
 		// transmission_function::pdf (scatterings/transmission/transmission_function.cpp:25-28)
 		case LOBE_L_LAMBERT_TRANSMIT: return same_hemisphere(wo, wi) ? 0.f : cosine_hemisphere_pdf(fabs_ref(wi.z));
 		case LOBE_MF_REFLECT:
@@ -558,7 +582,8 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT:
 		case LOBE_OREN_NAYAR:
-		case LOBE_L_LAMBERT: return sample_lambert<MAT_ANY>(b, i, wo, u);  // reflection_function::sample, cosine
+		case LOBE_L_LAMBERT:
+		case LOBE_SSS_EXIT: return sample_lambert<MAT_ANY>(b, i, wo, u);  // reflection_function::sample, cosine
 		case LOBE_L_LAMBERT_TRANSMIT: return sample_lambert_transmit(b, i, wo, u);
 		case LOBE_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, m->reflectance);
 		case LOBE_L_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, layered_r(b, i));

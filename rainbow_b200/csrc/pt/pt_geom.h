@@ -528,6 +528,7 @@ RB_HD void frame_from_normal(vec3 normal, vec3& x, vec3& y, vec3& z) {
 struct local_surface {
 	vec3 p, n, sx, sy, sz;
 	vec2 uv;
+	vec3 dp_du;    // local dp/du (after the degenerate-uv fallback)
 };
 
 RB_HD local_surface triangle_surface(const scene_view& s, const mesh_rec& m, uint32_t tri, float b1, float b2) {
@@ -582,6 +583,7 @@ RB_HD local_surface triangle_surface(const scene_view& s, const mesh_rec& m, uin
 	out.sy = y;
 	out.sz = z;
 	out.n = dot(normal, z) > 0.f ? normal : -normal;  // face_forward(normal, shading z)
+	out.dp_du = dp_du;
 	return out;
 }
 

@@ -147,6 +147,36 @@ RB_HD bool build_record(const material_src& p, const vec3* scale, material_rec& 
 	case RB_MATERIAL_TRANSLUCENT:
 		build_layered(p, scale, r);
 		return true;
+	case RB_MATERIAL_SUBSURFACE: {
+		// subsurface_material::build_surface_properties (subsurface_material.cpp:24-66):
+		// nothing when transmission or reflectance is black, nor in the overload with a
+		// scale (:68-73); else glass lobes and the normalized-diffusion BSSRDF, whose
+		// constructor (normalized_diffusion.cpp:358-377) sets s = 1.85 - A + 7 |A - 0.8|^3
+		// and d = mfp / s
+		if (scale != nullptr || is_black3(p.transmission) || is_black3(p.reflectance)) {
+			r.kind = MAT_BLACK;
+			return true;
+		}
+		r.kind = p.smooth ? MAT_GLASS_SMOOTH : MAT_GLASS_ROUGH;
+		if (!p.smooth) {
+			r.alpha_x = p.alpha_x;
+			r.alpha_y = p.alpha_y;
+		}
+		r.eta = p.ior;
+		r.reflectance = p.reflectance;
+		r.transmission = p.transmission;
+		r.has_reflect = 1u;
+		r.has_transmit = 1u;
+		r.sss = 1u;
+		r.sss_a = p.diffuse;
+		vec3 t;
+		t.x = fabs_ref(p.diffuse.x - 0.8f);
+		t.y = fabs_ref(p.diffuse.y - 0.8f);
+		t.z = fabs_ref(p.diffuse.z - 0.8f);
+		const vec3 sd = (splat3(1.85f) - p.diffuse) + t * t * t * 7.f;
+		r.sss_d = p.mfp / sd;
+		return true;
+	}
 	default: return false;
 	}
 }

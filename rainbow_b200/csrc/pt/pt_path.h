@@ -20,7 +20,10 @@
 namespace rb {
 namespace pt {
 
-enum : uint32_t { PATH_SPECULAR = 1u << 0 };
+enum : uint32_t {
+	PATH_SPECULAR = 1u << 0,
+	PATH_SSS = 1u << 1  // the last BSDF sample transmitted into a subsurface material: the BSSRDF stage is next
+};
 
 struct path_state {
 	vec3 o, d;
@@ -121,7 +124,7 @@ constexpr int class_material(uint32_t c) {
 		: c == CLASS_GLASS_ROUGH ? static_cast<int>(MAT_GLASS_ROUGH) : MAT_ANY;
 }
 RB_HD uint32_t class_of_material(int32_t material, const scene_view& s) {
-	if (material < 0) return CLASS_OTHER;
+	if (material < 0 || s.materials[material].sss) return CLASS_OTHER;
 	const uint32_t k = s.materials[material].kind;
 	return k == MAT_LAMBERT ? CLASS_LAMBERT : k == MAT_METAL ? CLASS_METAL : k == MAT_GLASS_ROUGH ? CLASS_GLASS_ROUGH : CLASS_OTHER;
 }
@@ -137,6 +140,10 @@ RB_HD void shade_miss(const scene_view& s, path_state& p) {
 	if (p.bounces == 0 || (p.flags & PATH_SPECULAR))
 		for (uint32_t i = 0; i < s.num_environments; i++) p.L = p.L + p.beta * s.emitters[s.environments[i]].radiance;
 }
+
+template <int MAT = MAT_ANY>
+RB_HD void nee_sample(const scene_view& s, path_state& p, const surface_t& si, const bsdf_t& b, shade_record& rec,
+	vol_rec* vr = nullptr);
 
 // Returns false when the path ends here (a miss). vr (volume path tracing
 // only): receives the factors of the emitter-sampling connection.
@@ -172,8 +179,19 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 	material_rec mat_scratch;
 	const bsdf_t b = make_bsdf(surface_material<MAT>(s, rec.material, si, mat_scratch));
 	if (bsdf_count(b, ST_NON_SPECULAR) == 0) return true;
-	rec.did_nee = 1u;
 	rec.guidable = bsdf_count(b, ST_SPECULAR) == 0 ? 1u : 0u;
+	nee_sample<MAT>(s, p, si, b, rec, vr);
+	return true;
+}
+
+// uniform_sample_one_emitter's draws and rays (integrator.cpp:101-201) at
+// surface si with BSDF b: emitter pick (1D), light sample (2D) -> rec's shadow
+// ray and its unoccluded contribution; the MIS BSDF sample (2D) -> rec's MIS
+// ray. shade_b_direct adds what the two rays find.
+template <int MAT>
+RB_HD void nee_sample(const scene_view& s, path_state& p, const surface_t& si, const bsdf_t& b, shade_record& rec,
+	vol_rec* vr) {
+	rec.did_nee = 1u;
 	const vec3 wo = to_local(si, si.wo);
 	// emitter sampling half (integrator.cpp:121-159)
 	const float n = static_cast<float>(s.num_emitters);
@@ -214,7 +232,6 @@ RB_HD bool shade_a(const scene_view& s, path_state& p, const hit_t& h, shade_rec
 		rec.mis_pdf = bs.pdf;
 		rec.mis_ray = spawn_ray(si.p, si.n, wi_w);
 	}
-	return true;
 }
 
 // Direct lighting half of shade_b: the unoccluded NEE sample and the MIS
@@ -279,6 +296,9 @@ RB_HD bool continue_bsdf(const scene_view& s, path_state& p, const shade_record&
 	p.o = r.o;
 	p.d = r.d;
 	p.len = r.len;
+	// a transmission into a material with a BSSRDF (integrator.cpp:401-402)
+	if constexpr (MAT == MAT_ANY)
+		if (b.m->sss && type_match(bs.type, ST_TRANSMISSION)) p.flags |= PATH_SSS;
 	wi_out = wi;
 	pdf_out = bs.pdf;
 	return true;
@@ -307,6 +327,7 @@ RB_HD bool shade_b(const scene_view& s, path_state& p, const shade_record& rec, 
 		vec3 wi;
 		float pdf;
 		if (!continue_bsdf<MAT>(s, p, rec, wi, pdf)) return false;
+		if (p.flags & PATH_SSS) return true;  // the BSSRDF stage, then Russian roulette
 	}
 	return roulette(p, max_depth, rr_threshold);
 }

@@ -116,7 +116,8 @@ struct mesh_rec {
 };
 
 enum : uint32_t { MAT_LAMBERT = 0, MAT_METAL = 1, MAT_GLASS_ROUGH = 2, MAT_GLASS_SMOOTH = 3, MAT_BLACK = 4, MAT_PLASTIC = 5,
-	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8, MAT_LAYERED = 9, MAT_MIXTURE = 10, MAT_TEXTURED = 11 };
+	MAT_MIRROR = 6, MAT_SUBSTRATE = 7, MAT_OREN_NAYAR = 8, MAT_LAYERED = 9, MAT_MIXTURE = 10, MAT_TEXTURED = 11,
+	MAT_SSS_EXIT = 12 };  // the exit point of a subsurface walk: one separable_bssrdf_reflection lobe
 
 // Lobes of a layered material (uber, translucent) or of a mixture: at most
 // kMaxLayeredLobes.
@@ -152,6 +153,10 @@ struct material_rec {
 	// MAT_TEXTURED: a material with image-textured spectra, built at every hit
 	// from material_src[src] and its textures at the hit's uv
 	uint32_t src;
+	// subsurface (a glass-kind record with a BSSRDF): the normalized-diffusion
+	// profile's A (diffuse) and d (mfp / s(A)) per channel; eta is the IOR
+	uint32_t sss;
+	spectrum sss_a, sss_d;
 };
 
 // Textured spectra of a material: diffuse, reflectance, transmission, specular, opacity.
@@ -171,6 +176,7 @@ struct material_src {
 	float on_a, on_b;         // matte: Oren-Nayar's A and B
 	spectrum diffuse, reflectance, transmission, specular, opacity;
 	spectrum cond_eta, cond_k;
+	spectrum mfp;             // subsurface: mean free path
 	uint32_t tex[kNumTexSlots];  // 0: the constant above; k > 0: texture k - 1 of the scene
 };
 
@@ -253,6 +259,9 @@ struct scene_view {
 	const media_rec* media;
 	uint32_t num_media;
 	uint32_t instances;           // non-zero: some prim slots hold a whole entity walked in its mesh's own tree
+	const float* sss_table;             // the normalized-diffusion inverse CDF (kSssTableSize knots), or null
+	uint32_t sss;                       // non-zero: some material has a BSSRDF
+	uint32_t pad3;
 	const material_src* material_srcs;  // parameters of the MAT_TEXTURED records
 	const texture_rec* textures;
 	const float* texels;

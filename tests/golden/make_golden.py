@@ -27,6 +27,12 @@ product's seeded scene generator:
   oren_nayar_samples  radiance of 1024 pairs, path_integrator::trace depth 8, on the spheres
                  scene with Oren-Nayar matte (tests.helpers.oren_nayar_scene)
   bsdf_oren_nayar_*  the BSDF tables of a matte material with sigma 20 (--only oren_nayar)
+  layered_samples, mixture_samples, texture_samples, subsurface_samples  radiance of 1024
+                 pairs, path_integrator::trace depth 8, on the spheres scene with uber and
+                 translucent, mixture, textured and subsurface materials (tests.helpers
+                 layered_scene, mixture_scene, textured_scene, subsurface_scene; --only
+                 layered|mixture|textures|subsurface), with first_entity
+  bsdf_uber_*, bsdf_translucent_*, bsdf_mixture_*  the BSDF tables of those materials
 
 The benchmark configurations themselves (--only baseline):
   config1_image  configuration 1 as specified (box room, 256 x 256, depth 5):
@@ -53,7 +59,8 @@ The reference's two-level tree (--only two_level):
                  intersect_with_shadow_ray hits, and the radiance of 512 (pixel,
                  sample) pairs, path_integrator, depth 5
 
-Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level|oren_nayar]
+Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level|oren_nayar|layered|
+       mixture|textures|subsurface]
 """
 from __future__ import annotations
 
@@ -283,6 +290,17 @@ def texture_fixtures():
          first_entity=first_entity(R, px, sm))
 
 
+def subsurface_fixtures():
+    from tests.helpers import subsurface_scene
+    R = ref.RefScene(subsurface_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(53)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("subsurface_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L, max_depth=np.array(8),
+         first_entity=first_entity(R, px, sm))
+
+
 def materials_fixtures():
     from tests.helpers import extra_materials_scene
     R = ref.RefScene(extra_materials_scene(scene_of(SPHERES)))
@@ -338,6 +356,8 @@ def main():
         return mixture_fixtures()
     if only == "textures":
         return texture_fixtures()
+    if only == "subsurface":
+        return subsurface_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -389,6 +409,7 @@ def main():
     layered_fixtures()
     mixture_fixtures()
     texture_fixtures()
+    subsurface_fixtures()
 
 
 def material_desc(m):

@@ -538,6 +538,23 @@ def textured_scene(scene: rb.Scene) -> rb.Scene:
     return scene.with_materials(mats).with_textures(scene_textures())
 
 
+def subsurface_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with every third material (from the second, the floor's) a
+    subsurface material (subsurface_material.cpp: glass lobes over a
+    normalized-diffusion BSSRDF), smooth and rough in turn, mean free paths
+    of 0.05-0.4 scene units; the rest unchanged."""
+    mats = []
+    for k in range(scene.desc.num_materials):
+        m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
+        if k % 3 == 1:
+            rough = 0.0 if (k // 3) % 2 == 0 else 0.2
+            m = _desc(rb.RB_MATERIAL_SUBSURFACE, remap_roughness=1, reflectance=(1.0, 1.0, 1.0),
+                      transmission=(1.0, 1.0, 1.0), diffuse=(0.8, 0.5, 0.3), mfp=(0.4, 0.2, 0.05), ior=1.33,
+                      roughness_u=rough, roughness_v=rough)
+        mats.append(m)
+    return scene.with_materials(mats)
+
+
 def oren_nayar_scene(scene: rb.Scene) -> rb.Scene:
     """The scene with every matte material given an Oren-Nayar sigma of
     10-50 degrees (matte_material.cpp:13-29 then builds oren_nayar_reflection),

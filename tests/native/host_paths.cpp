@@ -10,6 +10,7 @@
 #include "../../rainbow_b200/csrc/host/scene_pack.h"
 #include "../../rainbow_b200/csrc/kernels.cuh"
 #include "../../rainbow_b200/csrc/pt/pt_path.h"
+#include "../../rainbow_b200/csrc/pt/pt_sss.h"
 
 #include <cmath>
 #include <new>
@@ -124,6 +125,13 @@ void samples_view(const scene_view& view, const rb_camera_desc* cam, const uint3
 				mh = trace(view, rec.mis_ray.o, rec.mis_ray.d, l, true);
 			}
 			if (!shade_b_any(view, p, rec, sh, mh, max_depth, rr)) break;
+			if (p.flags & PATH_SSS) {
+				// the BSSRDF stage (k_subsurface), then Russian roulette
+				p.flags &= ~PATH_SSS;
+				auto tracer = [&view](vec3 o, vec3 d, float& l, bool shadow) { return trace(view, o, d, l, shadow); };
+				if (!subsurface_walk(view, p, rec, h, tracer)) break;
+				if (!roulette(p, max_depth, rr)) break;
+			}
 		}
 		out[3 * i] = p.L.x;
 		out[3 * i + 1] = p.L.y;
@@ -224,6 +232,16 @@ int hp_texture_sample(const float* rgb, uint32_t width, uint32_t height, uint32_
 		out[3 * i + 2] = c.z;
 	}
 	return 0;
+}
+
+// The normalized-diffusion inverse CDF table (kSssTableSize knots) the scene
+// packer builds, and sss_sample_profile(table, d, u) at n (d, u) pairs.
+int hp_sss_table(float* table, uint32_t n, const float* du, float* r) {
+	std::vector<float> t(kSssTableSize);
+	sss_build_table(t.data());
+	for (uint32_t i = 0; i < kSssTableSize; i++) table[i] = t[i];
+	for (uint32_t i = 0; i < n; i++) r[i] = sss_sample_profile(t.data(), du[2 * i], du[2 * i + 1]);
+	return static_cast<int>(kSssTableSize);
 }
 
 int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {

@@ -10,7 +10,8 @@ import pytest
 
 import rainbow_b200 as rb
 from oracle import ref
-from tests.helpers import extra_materials_scene, layered_scene, mixture_scene, textured_scene, two_level_scene
+from tests.helpers import (extra_materials_scene, layered_scene, mixture_scene, subsurface_scene, textured_scene,
+                           two_level_scene)
 
 pytestmark = pytest.mark.skipif(not ref.adapter_available(), reason="oracle/_ref/libadapter_check.so not built")
 
@@ -27,12 +28,16 @@ def _scene(name):
     if name == "spheres_mixture":
         return mixture_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
                                                subdivision=2))
+    if name == "spheres_subsurface":
+        return subsurface_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
+                                                  subdivision=2))
     if name == "fog":
         return rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=40, height=30, num_spheres=6, subdivision=2)
     return two_level_scene()
 
 
-@pytest.mark.parametrize("name", ["box", "spheres_materials", "spheres_layered", "spheres_mixture", "fog", "two_level"])
+@pytest.mark.parametrize("name", ["box", "spheres_materials", "spheres_layered", "spheres_mixture", "spheres_subsurface",
+                                  "fog", "two_level"])
 def test_export_describes_the_reference_scene(name):
     scene = _scene(name)
     R = ref.RefScene(scene)

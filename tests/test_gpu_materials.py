@@ -1,4 +1,5 @@
-"""Plastic, mirror, substrate, Oren-Nayar, uber, translucent and mixture materials and image textures on the GPU: with spp = 1 the film sum of a pixel
+"""Plastic, mirror, substrate, Oren-Nayar, uber, translucent, mixture and subsurface materials and image
+textures on the GPU: with spp = 1 the film sum of a pixel
 is one sample's radiance, against the reference's path_integrator::trace on the
 spheres scene with plastic, mirror and substrate materials (golden fixture), and the same
 scene in direct lighting against the host build."""
@@ -8,7 +9,8 @@ import pytest
 import rainbow_b200 as rb
 from tests import golden
 from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, layered_scene,
-                           mixture_scene, oren_nayar_scene, per_sample_radiance, scene_from_params, textured_scene)
+                           mixture_scene, oren_nayar_scene, per_sample_radiance, scene_from_params, subsurface_scene,
+                           textured_scene)
 
 pytestmark = pytest.mark.gpu
 
@@ -47,7 +49,7 @@ def test_oren_nayar_samples_match_reference():
 
 
 @pytest.mark.parametrize("name,make", [("layered_samples", layered_scene), ("mixture_samples", mixture_scene),
-                                       ("texture_samples", textured_scene)])
+                                       ("texture_samples", textured_scene), ("subsurface_samples", subsurface_scene)])
 def test_layered_samples_match_reference(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))
@@ -61,7 +63,7 @@ def test_layered_samples_match_reference(name, make):
 
 
 @pytest.mark.parametrize("name,make", [("layered_samples", layered_scene), ("mixture_samples", mixture_scene),
-                                       ("texture_samples", textured_scene)])
+                                       ("texture_samples", textured_scene), ("subsurface_samples", subsurface_scene)])
 def test_layered_direct_matches_host_build(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))
@@ -90,3 +92,40 @@ def test_extra_materials_direct_matches_host_build():
     assert (cnt == 1).all()
     agree = _agreement(sums.reshape(-1, 3).astype(np.float32), want)
     assert agree >= 0.97, f"only {agree:.4f} of pixels agree"
+
+
+@pytest.mark.parametrize("tuning", [dict(), dict(sort=rb.RB_SORT_NONE), dict(tail_bounce=2),
+                                    dict(traversal=rb.RB_TRAVERSAL_REFILL), dict(lanes=2, paths_per_wave=3000)])
+def test_subsurface_image_matches_host_build(tuning):
+    """Whole 1-spp image of the subsurface scene against the host build of the
+    same stages (every pixel's sample 5), under several launch shapes (a tail
+    bounce below the depth is ignored: subsurface scenes run every bounce
+    staged); the BSSRDF stage is taken by about half the paths."""
+    fx = golden.load("subsurface_samples")
+    scene = subsurface_scene(scene_from_params(fx["params"]))
+    W, H = scene.camera.width, scene.camera.height
+    px = np.arange(W * H, dtype=np.uint32)
+    want = HostPaths(scene).samples(scene.camera, px, np.full_like(px, 5), 8)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        if tuning:
+            ctx.set_tuning(**tuning)
+        ctx.render(scene.camera, spp=1, first_sample=5, max_depth=8, want_image=False)
+        sums, _, cnt = ctx.film()
+        st = ctx.stats()
+    assert (cnt == 1).all() and st.device_error == 0
+    agree = _agreement(sums.reshape(-1, 3).astype(np.float32), want)
+    assert agree >= 0.97, f"only {agree:.4f} of pixels agree ({tuning})"
+
+
+def test_subsurface_refuses_guided_and_volume_renders():
+    fx = golden.load("subsurface_samples")
+    scene = subsurface_scene(scene_from_params(fx["params"]))
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        for kw in (dict(volume=True), dict(guide=True), dict(train=True)):
+            with pytest.raises(rb.RbError) as e:
+                ctx.render(scene.camera, spp=1, max_depth=8, want_image=False, **kw)
+            assert e.value.status == 7, kw  # RB_ERR_UNSUPPORTED
+        ctx.render(scene.camera, spp=1, max_depth=8, want_image=False)  # the context stays usable
+        assert ctx.stats().device_error == 0

@@ -1,6 +1,7 @@
-"""Plastic, mirror, substrate, Oren-Nayar matte, uber, translucent and mixture materials
-(plastic_material.cpp, mirror_material.cpp, substrate_material.cpp, matte_material.cpp
-with sigma != 0, uber_material.cpp, translucent_material.cpp, mixture_material.cpp), and
+"""Plastic, mirror, substrate, Oren-Nayar matte, uber, translucent, mixture and subsurface
+materials (plastic_material.cpp, mirror_material.cpp, substrate_material.cpp,
+matte_material.cpp with sigma != 0, uber_material.cpp, translucent_material.cpp,
+mixture_material.cpp, subsurface_material.cpp with the normalized-diffusion BSSRDF), and
 image textures (textures/detail/image_texture.hpp), in
 the path integrator's stages and in direct lighting, compiled for the host,
 against the reference (fixture from the compiled reference, and the reference
@@ -15,7 +16,8 @@ import ctypes as C
 from oracle import ref
 from tests import golden
 from tests.helpers import (HOSTPATHS, _LOBE_NAMES, HostPaths, _desc, extra_materials_scene, layered_scene, material_lobes,
-                           mixture_scene, oren_nayar_scene, scene_from_params, texture_images, textured_scene)
+                           mixture_scene, oren_nayar_scene, scene_from_params, subsurface_scene, texture_images,
+                           textured_scene)
 
 
 def test_host_stages_extra_materials_match_fixture():
@@ -88,7 +90,8 @@ def test_layered_lobe_lists():
         lobes(kind=rb.RB_MATERIAL_UBER, ior=0.0)
 
 
-@pytest.mark.parametrize("name,make", [("mixture_samples", mixture_scene), ("texture_samples", textured_scene)])
+@pytest.mark.parametrize("name,make", [("mixture_samples", mixture_scene), ("texture_samples", textured_scene),
+                                       ("subsurface_samples", subsurface_scene)])
 def test_host_stages_mixture_match_fixture(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))
@@ -97,7 +100,8 @@ def test_host_stages_mixture_match_fixture(name, make):
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference oracle not built")
-@pytest.mark.parametrize("name,make", [("mixture_samples", mixture_scene), ("texture_samples", textured_scene)])
+@pytest.mark.parametrize("name,make", [("mixture_samples", mixture_scene), ("texture_samples", textured_scene),
+                                       ("subsurface_samples", subsurface_scene)])
 def test_host_direct_mixture_against_reference(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))
@@ -160,3 +164,45 @@ def test_texture_lookup_matches_reference():
         L.hp_texture_sample(img.ctypes.data, img.shape[1], img.shape[0], uv.shape[0], uv.ctypes.data, got.ctypes.data)
         want = ref.texture_sample(img, uv)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), img.shape
+
+
+def test_subsurface_walks_change_the_samples():
+    """About half the subsurface fixture's samples go through the BSSRDF: the
+    same scene with the subsurface materials made plain glass (the same lobes,
+    no BSSRDF) changes them, and leaves the rest bit-equal."""
+    fx = golden.load("subsurface_samples")
+    scene = subsurface_scene(scene_from_params(fx["params"]))
+    mats = [rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k])) for k in range(scene.desc.num_materials)]
+    for m in mats:
+        if m.kind == rb.RB_MATERIAL_SUBSURFACE:
+            m.kind = rb.RB_MATERIAL_GLASS
+    glass = scene.with_materials(mats)
+    args = (fx["pixels"], fx["samples"], int(fx["max_depth"]))
+    got = HostPaths(glass).samples(glass.camera, *args)
+    changed = (got.view(np.uint32) != fx["radiance"].view(np.uint32)).any(axis=1).mean()
+    assert 0.3 < changed < 0.7, changed
+
+
+def test_subsurface_profile_table():
+    """The normalized-diffusion inverse CDF (normalized_diffusion.cpp): knot k
+    of the d = 1 table is the radius where cdf(r) = 1 - e^-r / 4 - 3 e^(-r / 3) / 4
+    reaches k / 2047, the last knot the reference's finite end value, and a
+    sample interpolates the knots linearly and scales by d."""
+    lib = C.CDLL(HOSTPATHS)
+    lib.hp_sss_table.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(3)
+    du = np.stack([rng.random(256) * 2.0 + 0.01, rng.random(256)], axis=1).astype(np.float32)
+    table = np.zeros(2048, np.float32)
+    r = np.zeros(256, np.float32)
+    assert lib.hp_sss_table(table.ctypes.data, 256, du.ctypes.data, r.ctypes.data) == 2048
+    assert table[0] == 0.0 and np.all(np.diff(table) > 0)
+    assert table[-1] == np.float32(111.686673513429369)
+    k = np.arange(1, 2047)
+    x = table[1:-1].astype(np.float64)
+    cdf = 1.0 - np.exp(-x) / 4.0 - 0.75 * np.exp(-x / 3.0)
+    assert np.all(np.abs(cdf - k / 2047.0) < 1e-6)
+    u = du[:, 1] * np.float32(2047)
+    which = np.minimum(u.astype(np.int64), 2046)
+    t = u - which.astype(np.float32)
+    want = (table[which] * (np.float32(1) - t) + table[which + 1] * t) * du[:, 0]
+    assert np.array_equal(r, want.astype(np.float32))
