@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RBGPU_ABI_VERSION 9
+#define RBGPU_ABI_VERSION 10
 
 /* ------------------------------------------------------------------ status */
 typedef int32_t rb_status;
@@ -418,6 +418,31 @@ rb_status rb_film_from_device(rb_context* ctx, const double* d_sum_rgb, const do
 #define RB_NOALLOC_SCRATCH_BYTES (8u << 20)
 rb_status rb_render_noalloc(rb_context* ctx, const rb_render_params* params, double* d_sum_rgb, double* d_sum_sq_rgb,
 	uint32_t* d_count, void* stream);
+
+/* Stochastic progressive photon mapping:
+ * photon_mapping_integrator(sampler2d, sampler1d, iterations, max_depth,
+ * photons, radius)::render (rainbow-cpu/integrators/photon_mapping_integrator.hpp:9-13,
+ * photon_mapping_integrator.cpp:386-560). Each iteration traces a visible point
+ * per pixel, hashes the visible points' search spheres into a grid, traces
+ * `photons` photons (0: one per pixel) that deposit flux at the visible points
+ * they land near, and shrinks each pixel's radius by the photons it received.
+ * The image (W * H * 3 floats into rgb_out, host memory) is the reference's
+ * film value: L / iterations + tau / (iterations * photons * pi * r^2). Each
+ * pixel and each photon draws from its own PCG32 stream (pixel, iteration,
+ * seed) / (photon, iteration, seed), where the reference shares one stream per
+ * 16 x 16 tile and per chunk of 8192 photons. Media and BSSRDFs are ignored, as
+ * in the reference. The call allocates its buffers (about 270 bytes per pixel),
+ * waits for its work and returns the first device error, if any. */
+typedef struct rb_photon_params {
+	rb_camera_desc camera;
+	uint32_t iterations;  /* 1 .. 65535 (the reference's default: 64) */
+	uint32_t max_depth;   /* 1 .. 64 (5) */
+	uint32_t photons;     /* per iteration; 0: width * height (the reference's default) */
+	float radius;         /* initial search radius (1) */
+	uint32_t seed;        /* stream seed, 14 bits */
+	uint32_t reserved;
+} rb_photon_params;
+rb_status rb_render_photons(rb_context* ctx, const rb_photon_params* params, float* rgb_out);
 
 /* Counters of the last rb_render call. */
 typedef struct rb_render_stats {

@@ -21,6 +21,7 @@
 #include "rainbow-cpu/integrators/path_integrator.hpp"
 #include "rainbow-cpu/integrators/volume_path_integrator.hpp"
 #include "rainbow-cpu/integrators/direct_integrator.hpp"
+#include "rainbow-cpu/integrators/photon_mapping_integrator.hpp"
 #include "rainbow-cpu/media/homogeneous_medium.hpp"
 #include "rainbow-cpu/cameras/perspective_camera.hpp"
 #include "rainbow-cpu/filters/box_filter.hpp"
@@ -707,6 +708,26 @@ int orc_render_shipped(orc_scene* s, uint32_t spp, uint32_t max_depth, float rr,
 	const auto f = s->make_film();
 	const auto cam = s->make_camera(f);
 	path_integrator integrator(std::make_shared<random_sampler2d>(spp), std::make_shared<random_sampler1d>(spp), max_depth, rr);
+	const auto t0 = std::chrono::steady_clock::now();
+	integrator.render(cam, s->world);
+	if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	const auto& pixels = (*f).*member_of(film_pixels_tag{});
+	for (size_t i = 0; i < pixels.size(); i++) {
+		const spectrum L = pixels[i].spectrum();
+		rgb[3 * i] = L[0]; rgb[3 * i + 1] = L[1]; rgb[3 * i + 2] = L[2];
+	}
+	return RB_OK;
+}
+
+// photon_mapping_integrator::render as shipped (stochastic progressive photon
+// mapping: per-tile and per-chunk seeds; the parallel loops run in order with
+// libstdc++'s serial backend), then the film (W * H * 3 floats, set_pixel values).
+int orc_render_photons(orc_scene* s, uint32_t iterations, uint32_t max_depth, uint32_t photons, float radius, float* rgb,
+	double* seconds) {
+	const auto f = s->make_film();
+	const auto cam = s->make_camera(f);
+	photon_mapping_integrator integrator(std::make_shared<random_sampler2d>(1), std::make_shared<random_sampler1d>(1),
+		iterations, max_depth, photons, radius);
 	const auto t0 = std::chrono::steady_clock::now();
 	integrator.render(cam, s->world);
 	if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

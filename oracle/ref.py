@@ -44,6 +44,7 @@ def lib():
             "orc_trace_samples": (i32, [vp, vp, vp, u32, u32, f32, u32, vp]),
             "orc_render": (i32, [vp, u32, u32, u32, f32, u32, i32, i32, i32, vp, vp, C.POINTER(C.c_double)]),
             "orc_render_shipped": (i32, [vp, u32, u32, f32, vp, C.POINTER(C.c_double)]),
+            "orc_render_photons": (i32, [vp, u32, u32, u32, f32, vp, C.POINTER(C.c_double)]),
             "orc_pcg32": (i32, [C.c_uint64, u32, vp, vp]),
             "orc_bsdf": (i32, [vp, u32, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp]),
             "orc_texture_sample": (i32, [vp, u32, u32, u32, vp, vp]),
@@ -189,6 +190,15 @@ class RefScene:
         img = np.zeros((self.height, self.width, 3), dtype=np.float32)
         sec = C.c_double()
         _ok(lib().orc_render_shipped(self.h, spp, max_depth, rr, img.ctypes.data, C.byref(sec)), "orc_render_shipped")
+        return img, sec.value
+
+
+    def render_photons(self, iterations, max_depth=5, photons=0, radius=1.0):
+        """photon_mapping_integrator::render (iterations, max_depth, photons, radius) as shipped: the image."""
+        img = np.zeros((self.height, self.width, 3), dtype=np.float32)
+        sec = C.c_double()
+        _ok(lib().orc_render_photons(self.h, iterations, max_depth, photons, radius, img.ctypes.data, C.byref(sec)),
+            "orc_render_photons")
         return img, sec.value
 
 

@@ -28,7 +28,7 @@ from ._native import (  # noqa: F401  (re-exported constants)
     RB_RENDER_DIRECT, RB_RENDER_RESET, RB_RENDER_TRAIN, RB_RENDER_VOLUME, RB_SCENE_BOX, RB_SCENE_FOG, RB_SCENE_SLIT_ROOM, RB_SCENE_SPHERES,
     RB_SHADOW_CLOSEST, RB_SHADOW_FIRST_OCCLUDER, RB_SORT_MATERIAL, RB_SORT_NONE, RB_SORT_RAYS, RB_TRAVERSAL_PER_THREAD, RB_TRAVERSAL_REFILL, BatchParams, BatchView, Tuning,
     BvhDesc, CameraDesc, MaterialDesc, MediaDesc, MediumDesc, TextureDesc,
-    GuideConfig, GuideStats, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
+    GuideConfig, GuideStats, PhotonParams, RbError, RenderParams, RenderStats, SceneDesc, SceneGenParams, check, lib,
 )
 
 __all__ = ["Scene", "Context", "PathIntegrator", "generate_scene", "build_bvh", "RbError", "RAY_DTYPE", "HIT_DTYPE"]
@@ -232,6 +232,17 @@ class Context:
         img = out if out is not None else (np.zeros((camera.height, camera.width, 3), dtype=np.float32) if want_image else None)
         self._film_shape = (camera.width, camera.height)
         check(lib().rb_render(self._h, C.byref(p), img.ctypes.data if want_image else None), "rb_render")
+        return img
+
+    def render_photons(self, camera: CameraDesc, iterations: int = 64, max_depth: int = 5, photons: int = 0,
+                       radius: float = 1.0, seed: int = 0) -> np.ndarray:
+        """rb_render_photons: photon_mapping_integrator(iterations, max_depth, photons, radius)::render,
+        stochastic progressive photon mapping; returns the (height, width, 3) image."""
+        p = PhotonParams()
+        p.camera = camera
+        p.iterations, p.max_depth, p.photons, p.radius, p.seed = iterations, max_depth, photons, radius, seed
+        img = np.zeros((camera.height, camera.width, 3), dtype=np.float32)
+        check(lib().rb_render_photons(self._h, C.byref(p), img.ctypes.data), "rb_render_photons")
         return img
 
     def render_async(self, camera: CameraDesc, spp: int, first_sample: int = 0, max_depth: int = 5,

@@ -115,6 +115,11 @@ class RenderParams(C.Structure):
                 ("flags", C.c_uint32), ("paths_per_wave", C.c_uint32), ("direct_samples", C.c_uint32)]
 
 
+class PhotonParams(C.Structure):
+    _fields_ = [("camera", CameraDesc), ("iterations", C.c_uint32), ("max_depth", C.c_uint32),
+                ("photons", C.c_uint32), ("radius", C.c_float), ("seed", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("paths_per_wave", C.c_uint32), ("block_trace", C.c_uint32), ("block_shade", C.c_uint32),
                 ("grid_per_sm", C.c_uint32), ("sort", C.c_uint32), ("tail_bounce", C.c_uint32),
@@ -201,6 +206,7 @@ SIGNATURES = {
     "rb_scene_get": (C.c_int32, [C.c_void_p, C.POINTER(SceneDesc), C.POINTER(CameraDesc)]),
     "rb_scene_free": (None, [C.c_void_p]),
     "rb_abi_version": (C.c_int32, []),
+    "rb_render_photons": (C.c_int32, [C.c_void_p, C.POINTER(PhotonParams), C.c_void_p]),
     "rb_render_noalloc": (C.c_int32, [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rb_guide_init": (C.c_int32, [C.c_void_p, C.POINTER(GuideConfig)]),
     "rb_guide_get_params": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32]),

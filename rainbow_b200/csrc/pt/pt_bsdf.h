@@ -224,6 +224,7 @@ struct bsdf_t {
 	const material_rec* m;
 	float eta;     // collection eta (glass IOR, else 1)
 	uint32_t mix;  // a mixture: each lobe reads its own component record (lobe_ref)
+	uint32_t importance;  // transport_mode::important (photon paths): transmission without the (eta_i / eta_o)^2 of radiance
 };
 RB_HD uint32_t lobe_kind(const bsdf_t& b, uint32_t i) { return (b.kinds >> (4u * i)) & 15u; }
 RB_HD uint32_t lobe_type(const bsdf_t& b, uint32_t i) { return (b.types >> (5u * i)) & 31u; }
@@ -241,6 +242,7 @@ RB_HD bsdf_t make_bsdf(const material_rec* m) {
 	b.types = 0;
 	b.eta = 1.f;
 	b.mix = 0;
+	b.importance = 0;
 	switch (m->kind) {
 	case MAT_LAMBERT:
 		add_lobe(b, LOBE_LAMBERT, ST_DIFFUSE | ST_REFLECTION);
@@ -324,8 +326,8 @@ RB_HD float mf_reflect_pdf(const material_rec* m, vec3 wo, vec3 wi) {
 	return tr_pdf(m->alpha_x, m->alpha_y, wo, wh) / (4.f * dot(wo, wh));
 }
 // microfacet_transmission::evaluate (scatterings/transmission/microfacet_transmission.cpp:14-37),
-// radiance transport, eta (1, m->eta), scaled by T.
-RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi, spectrum T) {
+// eta (1, m->eta), scaled by T; importance transport drops the 1 / eta factor (:31).
+RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi, spectrum T, uint32_t importance = 0u) {
 	if (same_hemisphere(wo, wi)) return spectrum{0.f, 0.f, 0.f};
 	const float co = wo.z, ci = wi.z;
 	if (co == 0.f || ci == 0.f) return spectrum{0.f, 0.f, 0.f};
@@ -334,7 +336,7 @@ RB_HD spectrum mf_transmit_f(const material_rec* m, vec3 wo, vec3 wi, spectrum T
 	const vec3 wh = face_forward(normalize(wo + wi * eta), vec3{0.f, 0.f, 1.f});
 	const float F = fresnel_dielectric(dot(wo, wh), 1.f, m->eta);
 	const float denom = dot(wo, wh) + eta * dot(wi, wh);
-	const float factor = 1.f / eta;
+	const float factor = importance ? 1.f : 1.f / eta;
 	const float D = tr_d(m->alpha_x, m->alpha_y, wh);
 	const float G = tr_g(m->alpha_x, m->alpha_y, wo, wi);
 	const float v = fabs_ref(D * G * eta * eta * fabs_ref(dot(wi, wh)) * fabs_ref(dot(wo, wh) * factor * factor) /
@@ -430,20 +432,20 @@ RB_HD spectrum lobe_f(const bsdf_t& b, uint32_t i, vec3 wo, vec3 wi) {
 	else if constexpr (MAT == static_cast<int>(MAT_METAL)) return mf_reflect_f<MAT>(b.m, wo, wi, b.m->reflectance);
 	else if constexpr (MAT == static_cast<int>(MAT_GLASS_ROUGH))
 		return lobe_kind(b, i) == LOBE_MF_REFLECT ? mf_reflect_f<MAT>(b.m, wo, wi, b.m->reflectance)
-		                                          : mf_transmit_f(b.m, wo, wi, b.m->transmission);
+		                                          : mf_transmit_f(b.m, wo, wi, b.m->transmission, b.importance);
 	else {
 		const material_rec* m = lobe_rec(b, i);
 		switch (lobe_kind(b, i)) {
 		case LOBE_LAMBERT: return m->diffuse * kInvPi;
 		case LOBE_OREN_NAYAR: return oren_nayar_f(m, wo, wi);
 		case LOBE_MF_REFLECT: return mf_reflect_f<MAT_ANY>(m, wo, wi, m->reflectance);
-		case LOBE_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, m->transmission);
+		case LOBE_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, m->transmission, b.importance);
 		case LOBE_FRESNEL_BLEND: return fresnel_blend_f(m, wo, wi);
 		// lambertian_reflection / lambertian_transmission::evaluate: R / pi, T / pi
 		case LOBE_L_LAMBERT:
 		case LOBE_L_LAMBERT_TRANSMIT: return layered_r(b, i) * kInvPi;
 		case LOBE_L_MF_REFLECT: return mf_reflect_f<MAT_ANY>(m, wo, wi, layered_r(b, i));
-		case LOBE_L_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, layered_r(b, i));
+		case LOBE_L_MF_TRANSMIT: return mf_transmit_f(m, wo, wi, layered_r(b, i), b.importance);
 		case LOBE_SSS_EXIT: return splat3(sss_exit_f(m->eta, wi.z));
 		default: return spectrum{0.f, 0.f, 0.f};  // specular lobes evaluate to 0
 		}
@@ -507,10 +509,10 @@ RB_HD lobe_sample sample_mf_transmit(const bsdf_t& b, uint32_t i, vec3 wo, vec2 
 	const float eta = entering ? (1.f / m->eta) : (m->eta / 1.f);
 	const vec3 wi = refract(wo, wh, eta);
 	if (is_zero(wi)) return no_sample();
-	return lobe_sample{lobe_type(b, i), mf_transmit_f(m, wo, wi, T), wi, mf_transmit_pdf(m, wo, wi)};
+	return lobe_sample{lobe_type(b, i), mf_transmit_f(m, wo, wi, T, b.importance), wi, mf_transmit_pdf(m, wo, wi)};
 }
 // fresnel_specular::sample (rainbow-cpu/scatterings/mixture/fresnel_specular.cpp:25-54)
-RB_HD lobe_sample sample_fresnel_specular(const material_rec* m, vec3 wo, vec2 u) {
+RB_HD lobe_sample sample_fresnel_specular(const material_rec* m, vec3 wo, vec2 u, uint32_t importance) {
 	const float F = fresnel_dielectric(wo.z, 1.f, m->eta);
 	if (u.x < F) {
 		const vec3 wi{-wo.x, -wo.y, wo.z};
@@ -521,7 +523,7 @@ RB_HD lobe_sample sample_fresnel_specular(const material_rec* m, vec3 wo, vec2 u
 	const float eo = entering ? m->eta : 1.f;
 	const vec3 wi = refract(wo, face_forward(vec3{0.f, 0.f, 1.f}, wo), ei / eo);
 	if (is_zero(wi)) return no_sample();
-	const float factor = (ei * ei) / (eo * eo);
+	const float factor = importance ? 1.f : (ei * ei) / (eo * eo);
 	const spectrum v = m->transmission * (splat3(1.f) - splat3(F)) * factor / fabs_ref(wi.z);
 	return lobe_sample{ST_TRANSMISSION | ST_SPECULAR, v, wi, 1.f - F};
 }
@@ -565,7 +567,7 @@ RB_HD lobe_sample sample_specular_transmit(const bsdf_t& b, uint32_t i, vec3 wo)
 	const vec3 wi = refract(wo, face_forward(vec3{0.f, 0.f, 1.f}, wo), ei / eo);
 	if (is_zero(wi)) return no_sample();
 	const float F = fresnel_dielectric(wi.z, 1.f, lobe_eta);
-	const float factor = (ei * ei) / (eo * eo);
+	const float factor = b.importance ? 1.f : (ei * ei) / (eo * eo);
 	const spectrum v = layered_r(b, i) * (splat3(1.f) - splat3(F)) * factor / fabs_ref(wi.z);
 	return lobe_sample{ST_SPECULAR | ST_TRANSMISSION, v, wi, 1.f};
 }
@@ -589,7 +591,7 @@ RB_HD lobe_sample lobe_sample_dir(const bsdf_t& b, uint32_t i, vec3 wo, vec2 u) 
 		case LOBE_L_MF_REFLECT: return sample_mf_reflect<MAT_ANY>(b, i, wo, u, layered_r(b, i));
 		case LOBE_MF_TRANSMIT: return sample_mf_transmit<MAT_ANY>(b, i, wo, u, m->transmission);
 		case LOBE_L_MF_TRANSMIT: return sample_mf_transmit<MAT_ANY>(b, i, wo, u, layered_r(b, i));
-		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(m, wo, u);
+		case LOBE_FRESNEL_SPECULAR: return sample_fresnel_specular(m, wo, u, b.importance);
 		case LOBE_SPECULAR_REFLECT: return sample_specular_reflect(m, wo);
 		case LOBE_L_SPECULAR_REFLECT: return sample_layered_specular_reflect(b, i, wo);
 		case LOBE_L_SPECULAR_TRANSMIT: return sample_specular_transmit(b, i, wo);

@@ -33,6 +33,8 @@ product's seeded scene generator:
                  layered_scene, mixture_scene, textured_scene, subsurface_scene; --only
                  layered|mixture|textures|subsurface), with first_entity
   bsdf_uber_*, bsdf_translucent_*, bsdf_mixture_*  the BSDF tables of those materials
+  photons_box, photons_spheres, photons_materials  photon_mapping_integrator::render images
+                 (stochastic progressive photon mapping) of PHOTON_CASES (--only photons)
 
 The benchmark configurations themselves (--only baseline):
   config1_image  configuration 1 as specified (box room, 256 x 256, depth 5):
@@ -60,7 +62,7 @@ The reference's two-level tree (--only two_level):
                  sample) pairs, path_integrator, depth 5
 
 Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level|oren_nayar|layered|
-       mixture|textures|subsurface]
+       mixture|textures|subsurface|photons]
 """
 from __future__ import annotations
 
@@ -301,6 +303,29 @@ def subsurface_fixtures():
          first_entity=first_entity(R, px, sm))
 
 
+# photon_mapping_integrator::render cases: (name, scene params, scene variant,
+# iterations, max_depth, photons, radius)
+PHOTON_CASES = (
+    ("box", dict(BOX, width=32, height=32), None, 3, 5, 0, 0.1),
+    ("spheres", dict(SPHERES, width=48, height=40, num_spheres=12), None, 3, 5, 0, 0.5),
+    ("materials", dict(SPHERES, width=48, height=40, num_spheres=12), "extra_materials_scene", 4, 6, 3000, 0.3),
+)
+
+
+def photon_scene(params, variant):
+    import tests.helpers as H
+    sc = scene_of(params)
+    return getattr(H, variant)(sc) if variant else sc
+
+
+def photon_fixtures():
+    for name, params, variant, it, depth, photons, radius in PHOTON_CASES:
+        R = ref.RefScene(photon_scene(params, variant))
+        img, _ = R.render_photons(it, depth, photons, radius)
+        save(f"photons_{name}", params=params_array(params), image=img, iterations=np.array(it), max_depth=np.array(depth),
+             photons=np.array(photons), radius=np.array(radius, np.float32))
+
+
 def materials_fixtures():
     from tests.helpers import extra_materials_scene
     R = ref.RefScene(extra_materials_scene(scene_of(SPHERES)))
@@ -358,6 +383,8 @@ def main():
         return texture_fixtures()
     if only == "subsurface":
         return subsurface_fixtures()
+    if only == "photons":
+        return photon_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -410,6 +437,7 @@ def main():
     mixture_fixtures()
     texture_fixtures()
     subsurface_fixtures()
+    photon_fixtures()
 
 
 def material_desc(m):

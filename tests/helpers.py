@@ -129,6 +129,17 @@ class HostPaths:
                   seed, out.ctypes.data) == 0
         return out
 
+    def photon_render(self, camera, iterations, max_depth=5, photons=0, radius=1.0, streams=0, seed=0):
+        """photon_mapping_integrator::render through the photon stage functions: streams 0 in the
+        reference's order and streams (bit-equal to it), 1 with the kernels' per-pixel and
+        per-photon streams. Returns the (height, width, 3) image."""
+        self.L.hp_photon_render.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                            C.c_int, C.c_uint32, C.c_void_p]
+        out = np.zeros((camera.height, camera.width, 3), dtype=np.float32)
+        assert self.L.hp_photon_render(self.h, C.byref(camera), iterations, max_depth, photons, radius, streams, seed,
+                                       out.ctypes.data) == 0
+        return out
+
 
 def assert_hits_equal(got, want, what=""):
     assert np.array_equal(got["entity"], want["entity"]), f"{what}: entity ids differ at " \

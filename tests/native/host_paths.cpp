@@ -11,8 +11,11 @@
 #include "../../rainbow_b200/csrc/kernels.cuh"
 #include "../../rainbow_b200/csrc/pt/pt_path.h"
 #include "../../rainbow_b200/csrc/pt/pt_sss.h"
+#include "../../rainbow_b200/csrc/pt/pt_photon.h"
 
+#include <algorithm>
 #include <cmath>
+#include <limits>
 #include <new>
 #include <vector>
 
@@ -242,6 +245,125 @@ int hp_sss_table(float* table, uint32_t n, const float* du, float* r) {
 	for (uint32_t i = 0; i < kSssTableSize; i++) table[i] = t[i];
 	for (uint32_t i = 0; i < n; i++) r[i] = sss_sample_profile(t.data(), du[2 * i], du[2 * i + 1]);
 	return static_cast<int>(kSssTableSize);
+}
+
+// photon_mapping_integrator::render (photon_mapping_integrator.cpp:386-560)
+// through the photon stage functions. streams 0: the reference's own order and
+// streams (one pcg32 per 16 x 16 tile of pixels, seeded by the tile's index,
+// and one per chunk of 8192 photons, seeded by the chunk's index, each kept
+// across iterations; pixels and photons in order), so the image is the
+// reference's bit for bit; streams 1: the kernels' per-pixel and per-photon
+// streams (sppm_pixel_seed, sppm_photon_seed). The grid is built as the
+// reference builds it (a pixel appears in a bucket once per cell of its box
+// that hashes there). out: W * H * 3 floats, the film's set_pixel values.
+int hp_photon_render(void* hs, const rb_camera_desc* cam, uint32_t iterations, uint32_t max_depth, uint32_t photons,
+	float radius, int streams, uint32_t seed, float* out) {
+	const scene_view& view = static_cast<hp_scene*>(hs)->view;
+	const uint32_t W = static_cast<uint32_t>(cam->width), H = static_cast<uint32_t>(cam->height);
+	const uint32_t npix = W * H;
+	const uint64_t nphot = photons == 0 ? npix : photons;
+	std::vector<sppm_pixel> px(npix);
+	for (auto& q : px) {
+		q.tau = splat3(0.f);
+		q.L = splat3(0.f);
+		q.radius = radius;
+		q.n = 0.f;
+	}
+	std::vector<visible_point> vp(npix);
+	std::vector<spectrum> phi(npix);
+	std::vector<uint32_t> m(npix);
+	auto tracer = [&view](vec3 o, vec3 d, float& len, bool shadow) { return trace(view, o, d, len, shadow); };
+	// the reference's streams: tiles in row order, chunks in order
+	const uint32_t tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+	std::vector<pcg32> tile_rng(static_cast<size_t>(tiles_x) * tiles_y);
+	for (size_t t = 0; t < tile_rng.size(); t++) tile_rng[t] = pcg_seed(t);
+	const uint64_t chunks = (nphot + 8191) / 8192;
+	std::vector<pcg32> chunk_rng(chunks);
+	for (uint64_t c = 0; c < chunks; c++) chunk_rng[c] = pcg_seed(c);
+	for (uint32_t it = 0; it < iterations; it++) {
+		// visible points
+		for (uint32_t ty = 0; ty < tiles_y; ty++)
+			for (uint32_t tx = 0; tx < tiles_x; tx++)
+				for (uint32_t y = ty * 16; y < std::min(H, ty * 16 + 16); y++)
+					for (uint32_t x = tx * 16; x < std::min(W, tx * 16 + 16); x++) {
+						const uint32_t pixel = y * W + x;
+						path_state p;
+						pcg32& g = tile_rng[ty * tiles_x + tx];
+						p.rng = streams == 0 ? g : pcg_seed(sppm_pixel_seed(pixel, it, seed));
+						const ray_t r = camera_ray(cam->raster_to_camera, cam->camera_to_world, cam->lens_radius,
+							cam->focus_distance, x, y, p.rng);
+						p.o = r.o;
+						p.d = r.d;
+						p.len = r.len;
+						p.beta = splat3(1.f);
+						p.L = splat3(0.f);
+						p.eta = 1.f;
+						p.flags = 0u;
+						p.bounces = 0;
+						p.medium = -1;
+						sppm_visible(view, p, max_depth, tracer, vp[pixel]);
+						if (streams == 0) g = p.rng;
+						px[pixel].L = px[pixel].L + p.L;
+					}
+		// the grid (build_visible_point_grid)
+		sppm_grid g;
+		g.lo = splat3(std::numeric_limits<float>::max());
+		g.hi = splat3(std::numeric_limits<float>::min());
+		g.pool = npix;
+		float max_r = 0.f;
+		bool any = false;
+		for (uint32_t i = 0; i < npix; i++) {
+			if (!vp[i].valid) continue;
+			any = true;
+			const vec3 a = vp[i].p - splat3(px[i].radius), b = vp[i].p + splat3(px[i].radius);
+			g.lo = vec3{std::min(g.lo.x, a.x), std::min(g.lo.y, a.y), std::min(g.lo.z, a.z)};
+			g.hi = vec3{std::max(g.hi.x, b.x), std::max(g.hi.y, b.y), std::max(g.hi.z, b.z)};
+			max_r = std::max(max_r, px[i].radius);
+		}
+		std::vector<std::vector<uint32_t>> bucket(npix);
+		if (any) {
+			sppm_grid_size(g, max_r);
+			for (uint32_t i = 0; i < npix; i++) {
+				if (!vp[i].valid) continue;
+				int32_t x0, y0, z0, x1, y1, z1;
+				sppm_cell(g, vp[i].p - splat3(px[i].radius), x0, y0, z0);
+				sppm_cell(g, vp[i].p + splat3(px[i].radius), x1, y1, z1);
+				for (int32_t z = z0; z <= z1; z++)
+					for (int32_t y = y0; y <= y1; y++)
+						for (int32_t x = x0; x <= x1; x++) bucket[sppm_bucket(g, x, y, z)].push_back(i);
+			}
+		}
+		// photons
+		std::fill(phi.begin(), phi.end(), splat3(0.f));
+		std::fill(m.begin(), m.end(), 0u);
+		auto deposit = [&](const surface_t& si, const spectrum& beta, vec3 d) {
+			if (!any || !sppm_inside(g, si.p)) return;
+			int32_t x, y, z;
+			sppm_cell(g, si.p, x, y, z);
+			const auto& list = bucket[sppm_bucket(g, x, y, z)];
+			for (size_t k = list.size(); k-- > 0;) {  // the reference pushes at the list's head
+				const uint32_t i = list[k];
+				spectrum flux;
+				if (!sppm_flux(view, si, beta, d, vp[i], px[i].radius, flux)) continue;
+				phi[i] = phi[i] + flux;
+				m[i]++;
+			}
+		};
+		for (uint64_t j = 0; j < nphot; j++) {
+			pcg32& c = chunk_rng[j / 8192];
+			pcg32 rng = streams == 0 ? c : pcg_seed(sppm_photon_seed(static_cast<uint32_t>(j), it, seed));
+			sppm_photon(view, rng, max_depth, tracer, deposit);
+			if (streams == 0) c = rng;
+		}
+		for (uint32_t i = 0; i < npix; i++) sppm_update(px[i], vp[i].beta, phi[i], m[i]);
+	}
+	for (uint32_t i = 0; i < npix; i++) {
+		const spectrum v = sppm_value(px[i], iterations, nphot);
+		out[3 * i] = v.x;
+		out[3 * i + 1] = v.y;
+		out[3 * i + 2] = v.z;
+	}
+	return RB_OK;
 }
 
 int hp_trace(void* hs, const rb_ray* rays, uint32_t n, int shadow, rb_hit* hits) {

@@ -27,7 +27,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version_and_status_strings():
-    assert rb.lib().rb_abi_version() == 9
+    assert rb.lib().rb_abi_version() == 10
     for code in range(12):
         assert rb.lib().rb_status_string(code)
     assert rb.lib().rb_status_string(999) == b"unknown status"
