@@ -263,6 +263,21 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
             "guide": out.get("guide"), "timing": "sum of CUDA-event render times; training included in guided_s"}
 
 
+def photon_waves(res=512, iterations=2):
+    """One photon-mapping call (rb_render_photons, `iterations` iterations, one photon per pixel, depth 5,
+    radius 0.2) on the sphere field at res x res: the workload of the photon-mapping profile in profiles/."""
+    import rainbow_b200 as rb
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=res, height=res, num_spheres=200, subdivision=4)
+    ctx = rb.Context(0)
+    ctx.upload(scene)
+    t0 = time.perf_counter()
+    img = ctx.render_photons(scene.camera, iterations, 5, 0, 0.2, seed=1)
+    ms = (time.perf_counter() - t0) * 1e3
+    ctx.close()
+    print(json.dumps({"ms": ms, "image_mean": float(img.mean())}))
+    return 0
+
+
 def direct_waves(res=1024, spp=2):
     """One direct-lighting call (4 emitter + 4 BSDF samples, staged kernels) of `spp` samples on the sphere
     field: the workload of the direct-lighting profile in profiles/."""
@@ -377,6 +392,43 @@ def direct_leg(rb, device, threads, spp=4, rows=(384, 640)):
     return out
 
 
+def photons_leg(rb, device, iterations=4, radius=0.2, cpu_res=128, cpu_iterations=2):
+    """Stochastic progressive photon mapping (rb_render_photons; photon_mapping_integrator::render) on the
+    sphere field (1,024,010 triangles, 1024 x 1024): `iterations` iterations of a visible point per pixel
+    and one photon per pixel, max depth 5, initial radius `radius`; the call is synchronous, so its wall
+    time covers allocation, all iterations and the image's copy to the host. The reference's own
+    photon_mapping_integrator (its parallel loops run in order here: libstdc++'s serial backend) on the
+    same scene at cpu_res x cpu_res for cpu_iterations iterations, one host core."""
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=1024, height=1024, num_spheres=200, subdivision=4)
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    ctx.render_photons(scene.camera, 1, 5, 0, radius)  # warm-up (module loading)
+    best = None
+    for k in range(3):
+        t0 = time.perf_counter()
+        img = ctx.render_photons(scene.camera, iterations, 5, 0, radius, seed=1 + k)
+        ms = (time.perf_counter() - t0) * 1e3
+        best = ms if best is None else min(best, ms)
+    ctx.close()
+    items = 1024 * 1024 * iterations
+    out = {"workload": f"sphere field, {scene.num_triangles} triangles, 1024x1024, stochastic progressive photon "
+                       f"mapping, {iterations} iterations of 1,048,576 visible points and 1,048,576 photons, depth 5, "
+                       f"radius {radius}", "gpu_ms": best, "gpu_ms_per_iteration": best / iterations,
+           "gpu_mphotons_per_s": items / best / 1e3, "image_mean": float(img.mean())}
+    try:
+        from oracle import ref
+        if ref.available():
+            small = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=cpu_res, height=cpu_res, num_spheres=200,
+                                      subdivision=4)
+            _, sec = ref.RefScene(small).render_photons(cpu_iterations, 5, 0, radius)
+            n = cpu_res * cpu_res * cpu_iterations
+            out.update(cpu_reference_mphotons_per_s=n / sec / 1e6, cpu_reference_s=sec, cpu_cores=1,
+                       cpu_sample=f"{cpu_res}x{cpu_res}, {cpu_iterations} iterations ({n} visible points and photons)")
+    except Exception as e:  # reported, never required
+        out["cpu_reference_error"] = str(e)
+    return out
+
+
 def spheres_s5_leg(rb, device, spp=8):
     """The sphere field at icosphere subdivision 5 (200 spheres, 4,096,002 triangles): one call of `spp`
     samples per pixel with autotuned launch shapes."""
@@ -457,6 +509,7 @@ def summary_of(extra, batched, guided):
         return {k: (round(d[k], 4) if isinstance(d.get(k), float) else d.get(k)) for k in keys} if isinstance(d, dict) else d
     out = {name: pick(extra.get(name), "gpu_msamples_per_s", "msamples_per_s", "cpu_reference_msamples_per_s", "error")
            for name in ("config1", "direct", "spheres_s5", "config5_plain")}
+    out["photons"] = pick(extra.get("photons"), "gpu_mphotons_per_s", "cpu_reference_mphotons_per_s", "error")
     out = {k: {a: b for a, b in v.items() if b is not None} if isinstance(v, dict) else v for k, v in out.items()}
     if isinstance(batched, dict):
         out["batched"] = {k: v for k, v in pick(batched, "msamples_per_s", "error").items() if v is not None}
@@ -491,6 +544,8 @@ def main():
                     help="only render two 1-spp calls of the sphere field at 512x512 on one lane (profiling)")
     ap.add_argument("--direct-waves", action="store_true",
                     help="only render one 2-spp direct-lighting call on the sphere field (profiling)")
+    ap.add_argument("--photon-waves", action="store_true",
+                    help="only render one 2-iteration photon-mapping call on the sphere field at 512x512 (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tuning", default=None, help="launch shapes as JSON (skips the autotuner), e.g. "
                     "'{\"block_trace\": 256, \"grid_per_sm\": 16}'")
@@ -501,6 +556,8 @@ def main():
         return guided_waves()
     if args.direct_waves:
         return direct_waves()
+    if args.photon_waves:
+        return photon_waves()
     if args.trace_waves:
         return trace_waves()
 
@@ -685,7 +742,8 @@ def main():
         for name, leg in (("config1", lambda: config1_leg(rb, local, os.cpu_count() or 1)),
                           ("spheres_s5", lambda: spheres_s5_leg(rb, local)),
                           ("config5_plain", lambda: config5_leg(rb, local)),
-                          ("direct", lambda: direct_leg(rb, local, os.cpu_count() or 1))):
+                          ("direct", lambda: direct_leg(rb, local, os.cpu_count() or 1)),
+                          ("photons", lambda: photons_leg(rb, local))):
             try:
                 extra[name] = leg()
             except Exception as e:  # reported, never required for the throughput line

@@ -7,6 +7,7 @@
 // librbgpu.so. Only the tests load it.
 #include "../../rainbow_b200/adapter/scene_export.hpp"
 #include "../../rainbow_b200/adapter/wavefront_path_integrator.hpp"
+#include "../../rainbow_b200/adapter/wavefront_photon_mapping_integrator.hpp"
 
 #include "rainbow-cpu/cameras/perspective_camera.hpp"
 #include "rainbow-cpu/samplers/random_sampler.hpp"
@@ -56,6 +57,29 @@ int adp_render(orc_scene* s, uint32_t spp, uint32_t max_depth, float threshold, 
 // The adapter's export of a harness scene: the tree rb_bvh_build makes of it
 // (sizes first with NULL arrays) and, per entity, its material and emitter
 // descriptions (has[2 e] / has[2 e + 1]: 1 when present).
+// wavefront_photon_mapping_integrator(random_sampler2d(1), random_sampler1d(1),
+// iterations, max_depth, photons, radius).render(camera, scene) on a harness
+// scene; the result is in the camera's film. Returns 0, or -1 when render threw.
+int adp_render_photons(orc_scene* s, uint32_t iterations, uint32_t max_depth, uint32_t photons, float radius,
+	uint32_t seed, char* error, uint32_t error_size) {
+	std::shared_ptr<scenes::scene> world;
+	std::shared_ptr<cameras::camera> cam;
+	if (!objects(s, world, cam)) return RB_ERR_INVALID_ARGUMENT;
+	try {
+		integrators::wavefront_photon_mapping_integrator integrator(std::make_shared<samplers::random_sampler2d>(1),
+			std::make_shared<samplers::random_sampler1d>(1), iterations, max_depth, photons, radius);
+		integrator.set_seed(seed);
+		integrator.render(cam, world);
+	} catch (const std::exception& e) {
+		if (error != nullptr && error_size > 0) {
+			std::strncpy(error, e.what(), error_size - 1);
+			error[error_size - 1] = 0;
+		}
+		return -1;
+	}
+	return 0;
+}
+
 int adp_export(orc_scene* s, float* nodes, uint32_t* prim_entity, uint32_t* prim_index, uint32_t* num_nodes,
 	uint32_t* num_prims, rb_material_desc* materials, rb_emitter_desc* emitters, int32_t* has, rb_camera_desc* camera) {
 	std::shared_ptr<scenes::scene> world;

@@ -253,6 +253,8 @@ def adapter_lib():
         L = C.CDLL(ADAPTER_PATH)
         vp, u32, f32, i32 = C.c_void_p, C.c_uint32, C.c_float, C.c_int
         L.adp_render.restype, L.adp_render.argtypes = i32, [vp, u32, u32, f32, u32, C.c_char_p, u32]
+        L.adp_render_photons.restype = i32
+        L.adp_render_photons.argtypes = [vp, u32, u32, u32, f32, u32, C.c_char_p, u32]
         L.adp_export.restype = i32
         L.adp_export.argtypes = [vp, vp, vp, vp, C.POINTER(u32), C.POINTER(u32), vp, vp, vp, vp]
         L.adp_export_materials.restype = i32
@@ -270,6 +272,16 @@ def adapter_render(R, spp, max_depth=5, threshold=1.0, seed=0):
     st = adapter_lib().adp_render(R.h, spp, max_depth, threshold, seed, err, 512)
     if st != 0:
         raise RuntimeError(f"wavefront_path_integrator::render failed ({st}): {err.value.decode()}")
+    return R.film()
+
+
+def adapter_render_photons(R, iterations, max_depth=5, photons=0, radius=1.0, seed=0):
+    """wavefront_photon_mapping_integrator(random_sampler2d(1), random_sampler1d(1), iterations, max_depth,
+    photons, radius).render(camera, scene) on the reference scene of R; returns the camera's film (H, W, 3)."""
+    err = C.create_string_buffer(512)
+    st = adapter_lib().adp_render_photons(R.h, iterations, max_depth, photons, radius, seed, err, 512)
+    if st != 0:
+        raise RuntimeError(f"wavefront_photon_mapping_integrator::render failed ({st}): {err.value.decode()}")
     return R.film()
 
 

@@ -65,3 +65,25 @@ def test_adapter_two_level_scene_and_refusal():
     with pytest.raises(RuntimeError, match="invalid argument"):
         ref.adapter_render(R2, 4)
     np.testing.assert_array_equal(R2.film(), before)
+
+
+def test_photon_adapter_film_matches_rb_render_photons_and_the_reference():
+    """wavefront_photon_mapping_integrator::render on a reference scene writes what
+    rb_render_photons computes (up to the order of the photon flux sums), and over
+    several seeds estimates the image of photon_mapping_integrator::render as shipped."""
+    from tests.golden.make_golden import PHOTON_CASES, photon_scene
+    _, params, variant, it, depth, photons, radius = next(c for c in PHOTON_CASES if c[0] == "box")
+    scene = photon_scene(params, variant)
+    R = ref.RefScene(scene)
+    films = np.stack([ref.adapter_render_photons(R, it, depth, photons, radius, seed=s) for s in range(6)])
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        img = ctx.render_photons(scene.camera, it, depth, photons, radius, seed=0)
+    close = (np.abs(films[0] - img) <= 1e-3 * np.maximum(np.abs(img), 1e-2)).all(axis=2)
+    assert close.mean() >= 0.95, close.mean()
+    shipped = golden.load("photons_box")["image"]
+    blocks = films.reshape(6, 4, 8, 4, 8, 3).mean(axis=(2, 4))
+    want = shipped.reshape(4, 8, 4, 8, 3).mean(axis=(1, 3))
+    mean, sd = blocks.mean(axis=0), blocks.std(axis=0, ddof=1)
+    z = (mean - want) / np.maximum(sd * np.sqrt(1 + 1 / 6), 1e-3 * np.abs(want) + 1e-6)
+    assert np.abs(z).max() < 6.0, np.abs(z).max()
