@@ -677,6 +677,8 @@ def main():
         for ppw in (1 << 18, 1 << 19, 1 << 20):
             for lanes in (2, 4, 8):
                 cands.append(dict(t1.as_dict(), paths_per_wave=ppw, lanes=lanes))
+                # a one-sample call ends on its longest paths: the tail kernel takes the last bounces
+                cands.append(dict(t1.as_dict(), paths_per_wave=ppw, lanes=lanes, tail_bounce=5))
         best = None
         n_probe = min(8, args.steps)
         for c in cands:

@@ -316,9 +316,13 @@ rb_status prepare_volume(rb_context* c, const rb_render_params* prm) {
 
 // Wave lanes a render call can use: more than one for any render replayed
 // from graphs (not while profiling), with at least two waves.
-uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& cfg) {
+// async: calls that overlap on the GPU take their waves on the lanes in turn
+// across calls (a call of one wave runs beside the previous call's), so they
+// get every lane the tuning asks for.
+uint32_t lanes_for(const rb_context* c, uint64_t total, const gpu::launch_cfg& cfg, bool async = false) {
 	const uint32_t want = resolved_tuning(c->tuning).lanes;
 	if (want <= 1 || c->profiling || (c->has_invisible && c->drain_graph_failed)) return 1;
+	if (async) return want;
 	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
 	return static_cast<uint32_t>(waves < want ? waves : want);
 }
@@ -428,8 +432,10 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 	// a later async call of the same configuration: no clearing, no start
 	// barrier across the lanes; its counters add to the pending calls'
 	const bool continuing = async && c->async.pending > 0;
-	const uint32_t nlanes = lanes_for(c, total, cfg);
+	const uint32_t nlanes = lanes_for(c, total, cfg, async);
 	const uint64_t waves = (total + c->wave_capacity - 1) / c->wave_capacity;
+	// the lane of the call's first wave: the one after the previous async call's last wave
+	const uint32_t first_lane = continuing ? c->async.next_lane % nlanes : 0u;
 	if (record_waves || nlanes > 1) {
 		while (c->wave_events.size() < waves) {
 			cudaEvent_t e;
@@ -503,7 +509,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			RB_CUDA(gpu::launch_set_params(hp, l.params, l.stream));
 		}
 		for (uint64_t j = 0; j < waves; j++) {
-			const uint32_t lane = static_cast<uint32_t>(j % nlanes);
+			const uint32_t lane = static_cast<uint32_t>((first_lane + j) % nlanes);
 			const cudaStream_t s = lane == 0 ? c->stream : c->lanes[lane - 1].stream;
 			const gpu::wave_buffers& w = lane == 0 ? c->wave : c->lanes[lane - 1].wave;
 			const cudaGraphExec_t g = lane == 0 ? c->graph : c->lanes[lane - 1].graph;
@@ -516,9 +522,12 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 			if (training) RB_CUDA(guide::launch_snapshot(c->guide, c->lane_guides[lane], s));
 			if (training && cfg.guide_medium != nullptr)
 				RB_CUDA(guide::launch_snapshot(*cfg.guide_medium, c->lane_guides_medium[lane], s));
-			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
+			// the image slice this wave completes is read back before the wave's event, so that
+			// the next wave to resolve into the film (of this call or the next, on any lane)
+			// waits for the read
 			st = readback_after(c, readback, std::min<uint64_t>(total, (j + 1) * c->wave_capacity), s);
 			if (st != RB_OK) return st;
+			RB_CUDA(cudaEventRecord(c->wave_events[j], s));
 			launches += gpu::wave_launches(max_depth, cfg) + 1u + drain_begin;
 		}
 		for (uint32_t k = 0; k + 1 < nlanes; k++) {
@@ -564,6 +573,7 @@ rb_status run_waves(rb_context* c, uint64_t total, uint32_t max_depth, bool reco
 		c->async.pending++;
 		c->async.waves = waves;
 		c->async.lanes = nlanes;
+		c->async.next_lane = static_cast<uint32_t>((first_lane + waves) % nlanes);
 		c->async.samples += total;
 		c->async.launches += launches;
 		c->async.use_graph = use_graph;

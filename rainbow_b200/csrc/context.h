@@ -243,6 +243,7 @@ struct rb_context {
 		uint32_t pending = 0;
 		uint64_t waves = 0;
 		uint32_t lanes = 0;
+		uint32_t next_lane = 0;  // lane of the next continuing call's first wave
 		uint64_t samples = 0;
 		uint32_t launches = 0;
 		unsigned char signature[512];

@@ -20,8 +20,9 @@ def _scene():
     return rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=96, height=64, num_spheres=30, subdivision=3)
 
 
+# lanes=4 with one wave per call and lanes=3 with two: the calls' waves take the lanes in turn across calls
 @pytest.mark.parametrize("tuning", [dict(lanes=1, paths_per_wave=3000), dict(lanes=3, paths_per_wave=2048),
-                                    dict(lanes=4, paths_per_wave=6144)])
+                                    dict(lanes=4, paths_per_wave=6144), dict(lanes=3, paths_per_wave=4096)])
 def test_async_calls_equal_sync_calls(tuning):
     sc = _scene()
     W, H = sc.camera.width, sc.camera.height
