@@ -246,9 +246,12 @@ def guided_leg(rb, device, res, ref_spp, targets, chunk, max_spp, steps_per_wave
     for t in targets:
         p = out["plain"].get(t)
         runs = [g.get(t) for g in out["guided"]]
-        reached = [g for g in runs if g]
-        med_s = float(np.median([g["s"] for g in runs])) if len(reached) == len(runs) else None
-        med_spp = float(np.median([g["spp"] for g in runs])) if len(reached) == len(runs) else None
+        # a seed that never reaches the target within the sample budget counts as infinitely slow; the
+        # median exists while more than half of the seeds reach it
+        s_all = sorted(g["s"] if g else float("inf") for g in runs)
+        spp_all = sorted(g["spp"] if g else float("inf") for g in runs)
+        med_s = float(np.median(s_all)) if np.isfinite(np.median(s_all)) else None
+        med_spp = float(np.median(spp_all)) if np.isfinite(np.median(spp_all)) else None
         res_t[str(t)] = {"plain_s": p and p["s"], "plain_spp": p and p["spp"], "guided_s": med_s, "guided_spp": med_spp,
                          "speedup": (p["s"] / med_s) if (p and med_s) else None,
                          "guided_runs": [{"seed": k, "s": g and g["s"], "spp": g and g["spp"]}
