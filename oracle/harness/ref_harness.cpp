@@ -193,29 +193,29 @@ std::shared_ptr<material> make_material(const rb_material_desc* all, uint32_t co
 	const auto opacity = tex.spectrum_of(m.opacity, m.opacity_texture);
 	if (!diffuse || !reflectance || !transmission || !specular || !opacity) return nullptr;
 	switch (m.kind) {
-	case RB_MATERIAL_MATTE: return std::make_shared<matte_material>(diffuse, real_texture(m.sigma));
+	case RB_MATERIAL_MATTE: return std::make_shared<matte_material>(diffuse, tex.real_of(m.sigma, m.sigma_texture));
 	case RB_MATERIAL_METAL:
-		return std::make_shared<metal_material>(spectrum_texture(m.eta), spectrum_texture(m.k), real_texture(m.roughness_u),
-			real_texture(m.roughness_v), m.remap_roughness != 0);
+		return std::make_shared<metal_material>(spectrum_texture(m.eta), spectrum_texture(m.k), tex.real_of(m.roughness_u, m.roughness_u_texture),
+			tex.real_of(m.roughness_v, m.roughness_v_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_GLASS:
-		return std::make_shared<glass_material>(reflectance, transmission, real_texture(m.roughness_u),
-			real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
+		return std::make_shared<glass_material>(reflectance, transmission, tex.real_of(m.roughness_u, m.roughness_u_texture),
+			tex.real_of(m.roughness_v, m.roughness_v_texture), tex.real_of(m.ior, m.ior_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_PLASTIC:
-		return std::make_shared<plastic_material>(reflectance, diffuse, real_texture(m.roughness_u), real_texture(m.ior),
+		return std::make_shared<plastic_material>(reflectance, diffuse, tex.real_of(m.roughness_u, m.roughness_u_texture), tex.real_of(m.ior, m.ior_texture),
 			m.remap_roughness != 0);
 	case RB_MATERIAL_MIRROR: return std::make_shared<mirror_material>(reflectance);
 	case RB_MATERIAL_SUBSTRATE:
-		return std::make_shared<substrate_material>(reflectance, diffuse, real_texture(m.roughness_u),
-			real_texture(m.roughness_v), m.remap_roughness != 0);
+		return std::make_shared<substrate_material>(reflectance, diffuse, tex.real_of(m.roughness_u, m.roughness_u_texture),
+			tex.real_of(m.roughness_v, m.roughness_v_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_UBER:
 		return std::make_shared<uber_material>(transmission, reflectance, specular, diffuse, opacity,
-			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
+			tex.real_of(m.roughness_u, m.roughness_u_texture), tex.real_of(m.roughness_v, m.roughness_v_texture), tex.real_of(m.ior, m.ior_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_TRANSLUCENT:
 		return std::make_shared<translucent_material>(transmission, reflectance, specular, diffuse,
-			real_texture(m.roughness_u), m.remap_roughness != 0);
+			tex.real_of(m.roughness_u, m.roughness_u_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_SUBSURFACE:
 		return std::make_shared<subsurface_material>(transmission, reflectance, diffuse, spectrum_texture(m.mfp),
-			real_texture(m.roughness_u), real_texture(m.roughness_v), real_texture(m.ior), m.remap_roughness != 0);
+			tex.real_of(m.roughness_u, m.roughness_u_texture), tex.real_of(m.roughness_v, m.roughness_v_texture), tex.real_of(m.ior, m.ior_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_MIXTURE: {
 		if (m.components[0] < 0 || m.components[1] < 0) return nullptr;
 		const auto m0 = make_material(all, count, static_cast<uint32_t>(m.components[0]), tex, depth + 1);

@@ -64,7 +64,9 @@ class MaterialDesc(C.Structure):
                 ("roughness_u", C.c_float), ("roughness_v", C.c_float), ("specular", F3), ("opacity", F3),
                 ("components", C.c_int32 * 2), ("amount", F3), ("diffuse_texture", C.c_uint32),
                 ("reflectance_texture", C.c_uint32), ("transmission_texture", C.c_uint32),
-                ("specular_texture", C.c_uint32), ("opacity_texture", C.c_uint32), ("mfp", F3)]
+                ("specular_texture", C.c_uint32), ("opacity_texture", C.c_uint32), ("mfp", F3),
+                ("roughness_u_texture", C.c_uint32), ("roughness_v_texture", C.c_uint32), ("ior_texture", C.c_uint32),
+                ("sigma_texture", C.c_uint32)]
 
 
 class TextureDesc(C.Structure):

@@ -209,6 +209,16 @@ struct texture_registry {
 		ref_of.emplace(t.get(), ref);
 		return true;
 	}
+	// A real parameter: a constant texture's value in v (ref 0), or a real image
+	// texture exported as an RGB image whose channels all hold its values (the
+	// core reads channel 0); false for other textures.
+	bool real(const std::shared_ptr<textures::texture2d<rainbow::core::real>>& t, float& v, uint32_t& ref) {
+		ref = 0;
+		if (constant_real(t, v)) return true;
+		const auto img = std::dynamic_pointer_cast<textures::image_texture2d<rainbow::core::real>>(t);
+		return img != nullptr && add_image(img.get(), img->size().x, img->size().y,
+			[&](size_t i, float* c) { c[0] = c[1] = c[2] = img->value(i); }, ref);
+	}
 	// An RGB image texture, exported once.
 	bool image(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, uint32_t& ref) {
 		const auto img = std::dynamic_pointer_cast<textures::image_texture2d<shared::spectrums::spectrum>>(t);
@@ -248,25 +258,25 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 		uint32_t& ref) { return tex.spectrum(t, rgb, ref); };
 	if (const auto x = std::dynamic_pointer_cast<materials::matte_material>(m)) {
 		d.kind = RB_MATERIAL_MATTE;
-		ok = spec(read(*x, matte_diffuse{}), d.diffuse, d.diffuse_texture) && constant_real(read(*x, matte_sigma{}), d.sigma);
+		ok = spec(read(*x, matte_diffuse{}), d.diffuse, d.diffuse_texture) && tex.real(read(*x, matte_sigma{}), d.sigma, d.sigma_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::metal_material>(m)) {
 		d.kind = RB_MATERIAL_METAL;
 		d.remap_roughness = read(*x, metal_remap{}) ? 1 : 0;
 		ok = constant_rgb(read(*x, metal_eta{}), d.eta) && constant_rgb(read(*x, metal_k{}), d.k) &&
-			constant_real(read(*x, metal_ru{}), d.roughness_u) && constant_real(read(*x, metal_rv{}), d.roughness_v);
+			tex.real(read(*x, metal_ru{}), d.roughness_u, d.roughness_u_texture) && tex.real(read(*x, metal_rv{}), d.roughness_v, d.roughness_v_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::glass_material>(m)) {
 		d.kind = RB_MATERIAL_GLASS;
 		d.remap_roughness = read(*x, glass_remap{}) ? 1 : 0;
 		ok = spec(read(*x, glass_reflectance{}), d.reflectance, d.reflectance_texture) &&
 			spec(read(*x, glass_transmission{}), d.transmission, d.transmission_texture) &&
-			constant_real(read(*x, glass_ru{}), d.roughness_u) && constant_real(read(*x, glass_rv{}), d.roughness_v) &&
-			constant_real(read(*x, glass_eta{}), d.ior);
+			tex.real(read(*x, glass_ru{}), d.roughness_u, d.roughness_u_texture) && tex.real(read(*x, glass_rv{}), d.roughness_v, d.roughness_v_texture) &&
+			tex.real(read(*x, glass_eta{}), d.ior, d.ior_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::plastic_material>(m)) {
 		d.kind = RB_MATERIAL_PLASTIC;
 		d.remap_roughness = read(*x, plastic_remap{}) ? 1 : 0;
 		ok = spec(read(*x, plastic_specular{}), d.reflectance, d.reflectance_texture) &&
 			spec(read(*x, plastic_diffuse{}), d.diffuse, d.diffuse_texture) &&
-			constant_real(read(*x, plastic_roughness{}), d.roughness_u) && constant_real(read(*x, plastic_eta{}), d.ior);
+			tex.real(read(*x, plastic_roughness{}), d.roughness_u, d.roughness_u_texture) && tex.real(read(*x, plastic_eta{}), d.ior, d.ior_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::mirror_material>(m)) {
 		d.kind = RB_MATERIAL_MIRROR;
 		ok = spec(read(*x, mirror_reflectance{}), d.reflectance, d.reflectance_texture);
@@ -274,8 +284,8 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 		d.kind = RB_MATERIAL_SUBSTRATE;
 		d.remap_roughness = read(*x, substrate_remap{}) ? 1 : 0;
 		ok = spec(read(*x, substrate_specular{}), d.reflectance, d.reflectance_texture) &&
-			spec(read(*x, substrate_diffuse{}), d.diffuse, d.diffuse_texture) && constant_real(read(*x, substrate_ru{}), d.roughness_u) &&
-			constant_real(read(*x, substrate_rv{}), d.roughness_v);
+			spec(read(*x, substrate_diffuse{}), d.diffuse, d.diffuse_texture) && tex.real(read(*x, substrate_ru{}), d.roughness_u, d.roughness_u_texture) &&
+			tex.real(read(*x, substrate_rv{}), d.roughness_v, d.roughness_v_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::uber_material>(m)) {
 		d.kind = RB_MATERIAL_UBER;
 		d.remap_roughness = read(*x, uber_remap{}) ? 1 : 0;
@@ -283,8 +293,8 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 			spec(read(*x, uber_reflectance{}), d.reflectance, d.reflectance_texture) &&
 			spec(read(*x, uber_specular{}), d.specular, d.specular_texture) &&
 			spec(read(*x, uber_diffuse{}), d.diffuse, d.diffuse_texture) && spec(read(*x, uber_opacity{}), d.opacity, d.opacity_texture) &&
-			constant_real(read(*x, uber_ru{}), d.roughness_u) && constant_real(read(*x, uber_rv{}), d.roughness_v) &&
-			constant_real(read(*x, uber_eta{}), d.ior);
+			tex.real(read(*x, uber_ru{}), d.roughness_u, d.roughness_u_texture) && tex.real(read(*x, uber_rv{}), d.roughness_v, d.roughness_v_texture) &&
+			tex.real(read(*x, uber_eta{}), d.ior, d.ior_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::translucent_material>(m)) {
 		d.kind = RB_MATERIAL_TRANSLUCENT;
 		d.remap_roughness = read(*x, translucent_remap{}) ? 1 : 0;
@@ -292,7 +302,7 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 			spec(read(*x, translucent_reflectance{}), d.reflectance, d.reflectance_texture) &&
 			spec(read(*x, translucent_specular{}), d.specular, d.specular_texture) &&
 			spec(read(*x, translucent_diffuse{}), d.diffuse, d.diffuse_texture) &&
-			constant_real(read(*x, translucent_roughness{}), d.roughness_u);
+			tex.real(read(*x, translucent_roughness{}), d.roughness_u, d.roughness_u_texture);
 		d.roughness_v = d.roughness_u;
 	} else if (const auto x = std::dynamic_pointer_cast<materials::subsurface_material>(m)) {
 		d.kind = RB_MATERIAL_SUBSURFACE;
@@ -300,8 +310,8 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 		ok = spec(read(*x, subsurface_transmission{}), d.transmission, d.transmission_texture) &&
 			spec(read(*x, subsurface_reflectance{}), d.reflectance, d.reflectance_texture) &&
 			spec(read(*x, subsurface_diffuse{}), d.diffuse, d.diffuse_texture) &&
-			constant_rgb(read(*x, subsurface_mfp{}), d.mfp) && constant_real(read(*x, subsurface_ru{}), d.roughness_u) &&
-			constant_real(read(*x, subsurface_rv{}), d.roughness_v) && constant_real(read(*x, subsurface_eta{}), d.ior);
+			constant_rgb(read(*x, subsurface_mfp{}), d.mfp) && tex.real(read(*x, subsurface_ru{}), d.roughness_u, d.roughness_u_texture) &&
+			tex.real(read(*x, subsurface_rv{}), d.roughness_v, d.roughness_v_texture) && tex.real(read(*x, subsurface_eta{}), d.ior, d.ior_texture);
 	} else {
 		return RB_ERR_UNSUPPORTED;  // a material kind outside these (a mixture is exported by export_scene)
 	}

@@ -26,73 +26,57 @@ namespace {
 
 vec3 v3(const float* a, uint32_t i) { return vec3{a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
 
-// A material's parameters with what only the host computes applied:
-// trowbridge_reitz_distribution::roughness_to_alpha where the material maps
-// roughness (trowbridge_reitz_distribution.cpp:128-137), the sigma clamp and
-// oren_nayar_reflection's A and B (oren_nayar_reflection.cpp:5-16: radians in
-// float, then A and B in double, rounded to float). False for parameters the
-// reference material would not take (an IOR that is not positive).
+// A material's parameters with what derives from its reals applied
+// (pt::derive_src: roughness_to_alpha, the smooth-glass test, Oren-Nayar's A
+// and B). False for parameters the reference material would not take (a
+// constant IOR of a plastic or uber material that is not positive) and for
+// kinds it does not know.
 bool make_src(const rb_material_desc& md, pt::material_src& p) {
 	p = pt::material_src{};
 	p.kind = md.kind;
-	const auto alpha = [&](float r) { return md.remap_roughness ? pt::roughness_to_alpha(r) : r; };
 	p.diffuse = v3(md.diffuse, 0);
 	p.reflectance = v3(md.reflectance, 0);
 	p.transmission = v3(md.transmission, 0);
 	p.specular = v3(md.specular, 0);
 	p.opacity = v3(md.opacity, 0);
 	p.ior = md.ior;
+	p.roughness_u = md.roughness_u;
+	p.roughness_v = md.roughness_v;
+	p.sigma = md.sigma;
+	p.remap = md.remap_roughness ? 1u : 0u;
 	p.tex[pt::TEX_DIFFUSE] = md.diffuse_texture;
 	p.tex[pt::TEX_REFLECTANCE] = md.reflectance_texture;
 	p.tex[pt::TEX_TRANSMISSION] = md.transmission_texture;
 	p.tex[pt::TEX_SPECULAR] = md.specular_texture;
 	p.tex[pt::TEX_OPACITY] = md.opacity_texture;
+	p.tex[pt::TEX_ROUGHNESS_U] = md.roughness_u_texture;
+	p.tex[pt::TEX_ROUGHNESS_V] = md.roughness_v_texture;
+	p.tex[pt::TEX_IOR] = md.ior_texture;
+	p.tex[pt::TEX_SIGMA] = md.sigma_texture;
 	switch (md.kind) {
-	case RB_MATERIAL_MATTE: {
-		const float sigma = fclamp_ref(md.sigma, 0.f, 90.f);
-		if (sigma != 0.f) {
-			p.oren_nayar = 1u;
-			const float sr = sigma * 0.01745329251994329576923690768489f;
-			const float s2 = sr * sr;
-			p.on_a = static_cast<float>(1. - (s2 / (2 * (s2 + 0.33))));
-			p.on_b = static_cast<float>(0.45 * s2 / (s2 + 0.09));
-		}
-		return true;
-	}
 	case RB_MATERIAL_METAL:
-		p.alpha_x = alpha(md.roughness_u);
-		p.alpha_y = alpha(md.roughness_v);
 		p.cond_eta = v3(md.eta, 0);
 		p.cond_k = v3(md.k, 0);
-		return true;
+		break;
 	case RB_MATERIAL_GLASS:
-	case RB_MATERIAL_SUBSURFACE:
-		p.mfp = v3(md.mfp, 0);
-		p.smooth = (md.roughness_u == 0.f && md.roughness_v == 0.f) ? 1u : 0u;
-		if (!p.smooth) {
-			p.alpha_x = alpha(md.roughness_u);
-			p.alpha_y = alpha(md.roughness_v);
-		}
-		return true;
+	case RB_MATERIAL_SUBSURFACE: p.mfp = v3(md.mfp, 0); break;
 	case RB_MATERIAL_PLASTIC:
-	case RB_MATERIAL_TRANSLUCENT:
-		if (md.kind == RB_MATERIAL_PLASTIC && !(md.ior > 0.f)) return false;
-		p.alpha_x = p.alpha_y = alpha(md.roughness_u);
-		return true;
-	case RB_MATERIAL_SUBSTRATE:
 	case RB_MATERIAL_UBER:
-		if (md.kind == RB_MATERIAL_UBER && !(md.ior > 0.f)) return false;
-		p.alpha_x = alpha(md.roughness_u);
-		p.alpha_y = alpha(md.roughness_v);
-		return true;
-	case RB_MATERIAL_MIRROR: return true;
+		if (!md.ior_texture && !(md.ior > 0.f)) return false;
+		break;
+	case RB_MATERIAL_MATTE:
+	case RB_MATERIAL_TRANSLUCENT:
+	case RB_MATERIAL_SUBSTRATE:
+	case RB_MATERIAL_MIRROR: break;
 	default: return false;
 	}
+	pt::derive_src(p);
+	return true;
 }
 
 bool textured(const rb_material_desc& md) {
 	return md.diffuse_texture || md.reflectance_texture || md.transmission_texture || md.specular_texture ||
-		md.opacity_texture;
+		md.opacity_texture || md.roughness_u_texture || md.roughness_v_texture || md.ior_texture || md.sigma_texture;
 }
 
 // One material's record (pt::build_record), or with `scale` its scaled build.
@@ -158,6 +142,9 @@ rb_status pack_materials(const rb_scene_desc* desc, std::vector<pt::material_rec
 			if (!make_src(md, p)) return RB_ERR_INVALID_ARGUMENT;
 			for (uint32_t t = 0; t < pt::kNumTexSlots; t++)
 				if (p.tex[t] > desc->num_textures) return RB_ERR_INVALID_ARGUMENT;
+			// a real parameter reads channel 0 of an image (image_texture2d<real>); no composites
+			for (uint32_t t = pt::TEX_ROUGHNESS_U; t <= pt::TEX_SIGMA; t++)
+				if (p.tex[t] && desc->textures[p.tex[t] - 1].kind != RB_TEXTURE_IMAGE) return RB_ERR_UNSUPPORTED;
 			out[k] = pt::material_rec{};
 			out[k].kind = pt::MAT_TEXTURED;
 			out[k].src = static_cast<uint32_t>(srcs.size());

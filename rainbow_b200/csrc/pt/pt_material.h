@@ -85,6 +85,51 @@ RB_HD void build_layered(const material_src& p, const vec3* scale, material_rec&
 // metal's microfacet reflection takes the scale as its spectrum
 // (metal_material.cpp:39-59), the substrate's Fresnel-blend layer takes it as its
 // scale (substrate_material.cpp:38-58). False for a kind it does not build.
+// The fields of a material source that derive from its reals, as the
+// reference's materials derive them in build_surface_properties: the
+// Trowbridge-Reitz alphas (roughness_to_alpha when the material maps
+// roughness, trowbridge_reitz_distribution.cpp:128-137; plastic and
+// translucent take roughness u for both), glass and subsurface smooth when
+// both roughnesses are 0, and the matte's sigma clamped to [0, 90] with
+// oren_nayar_reflection's A and B (oren_nayar_reflection.cpp:5-16: radians in
+// float, then A and B in double, rounded to float). Called once on the host
+// for constant reals, at every hit for textured ones.
+RB_HD void derive_src(material_src& p) {
+	const auto alpha = [&](float v) { return p.remap ? roughness_to_alpha(v) : v; };
+	switch (p.kind) {
+	case RB_MATERIAL_MATTE: {
+		const float sigma = fclamp_ref(p.sigma, 0.f, 90.f);
+		p.oren_nayar = sigma != 0.f ? 1u : 0u;
+		if (p.oren_nayar) {
+			const float sr = sigma * 0.01745329251994329576923690768489f;
+			const float s2 = sr * sr;
+			p.on_a = static_cast<float>(1. - (s2 / (2 * (s2 + 0.33))));
+			p.on_b = static_cast<float>(0.45 * s2 / (s2 + 0.09));
+		}
+		return;
+	}
+	case RB_MATERIAL_METAL:
+	case RB_MATERIAL_SUBSTRATE:
+	case RB_MATERIAL_UBER:
+		p.alpha_x = alpha(p.roughness_u);
+		p.alpha_y = alpha(p.roughness_v);
+		return;
+	case RB_MATERIAL_GLASS:
+	case RB_MATERIAL_SUBSURFACE:
+		p.smooth = (p.roughness_u == 0.f && p.roughness_v == 0.f) ? 1u : 0u;
+		if (!p.smooth) {
+			p.alpha_x = alpha(p.roughness_u);
+			p.alpha_y = alpha(p.roughness_v);
+		}
+		return;
+	case RB_MATERIAL_PLASTIC:
+	case RB_MATERIAL_TRANSLUCENT:
+		p.alpha_x = p.alpha_y = alpha(p.roughness_u);
+		return;
+	default: return;
+	}
+}
+
 RB_HD bool build_record(const material_src& p, const vec3* scale, material_rec& r) {
 	r = material_rec{};
 	r.blend_scale = vec3{1.f, 1.f, 1.f};
@@ -243,6 +288,13 @@ RB_HD const material_rec* hit_material(const scene_view& s, uint32_t index, vec2
 	if (q.tex[TEX_TRANSMISSION]) q.transmission = sample_texture(s, q.tex[TEX_TRANSMISSION] - 1u, uv, p);
 	if (q.tex[TEX_SPECULAR]) q.specular = sample_texture(s, q.tex[TEX_SPECULAR] - 1u, uv, p);
 	if (q.tex[TEX_OPACITY]) q.opacity = sample_texture(s, q.tex[TEX_OPACITY] - 1u, uv, p);
+	// real parameters: channel 0 of their images (image_texture2d<real>)
+	const bool reals = q.tex[TEX_ROUGHNESS_U] | q.tex[TEX_ROUGHNESS_V] | q.tex[TEX_IOR] | q.tex[TEX_SIGMA];
+	if (q.tex[TEX_ROUGHNESS_U]) q.roughness_u = sample_texture(s, q.tex[TEX_ROUGHNESS_U] - 1u, uv, p).x;
+	if (q.tex[TEX_ROUGHNESS_V]) q.roughness_v = sample_texture(s, q.tex[TEX_ROUGHNESS_V] - 1u, uv, p).x;
+	if (q.tex[TEX_IOR]) q.ior = sample_texture(s, q.tex[TEX_IOR] - 1u, uv, p).x;
+	if (q.tex[TEX_SIGMA]) q.sigma = sample_texture(s, q.tex[TEX_SIGMA] - 1u, uv, p).x;
+	if (reals) derive_src(q);
 	build_record(q, nullptr, scratch);
 	return &scratch;
 }

@@ -159,9 +159,11 @@ struct material_rec {
 	spectrum sss_a, sss_d;
 };
 
-// Textured spectra of a material: diffuse, reflectance, transmission, specular, opacity.
+// Textured parameters of a material: the spectra diffuse, reflectance,
+// transmission, specular, opacity, then the reals roughness u and v, IOR and
+// Oren-Nayar sigma (channel 0 of an image).
 enum : uint32_t { TEX_DIFFUSE = 0, TEX_REFLECTANCE = 1, TEX_TRANSMISSION = 2, TEX_SPECULAR = 3, TEX_OPACITY = 4,
-	kNumTexSlots = 5 };
+	TEX_ROUGHNESS_U = 5, TEX_ROUGHNESS_V = 6, TEX_IOR = 7, TEX_SIGMA = 8, kNumTexSlots = 9 };
 
 // A material's parameters with what only the host computes already applied
 // (roughness_to_alpha, Oren-Nayar's A and B), from which its record is built
@@ -177,6 +179,8 @@ struct material_src {
 	spectrum diffuse, reflectance, transmission, specular, opacity;
 	spectrum cond_eta, cond_k;
 	spectrum mfp;             // subsurface: mean free path
+	float roughness_u, roughness_v, sigma;  // the description's reals, from which the fields above derive
+	uint32_t remap;           // roughness_to_alpha applies
 	uint32_t tex[kNumTexSlots];  // 0: the constant above; k > 0: texture k - 1 of the scene
 };
 

@@ -33,6 +33,8 @@ product's seeded scene generator:
                  layered_scene, mixture_scene, textured_scene, subsurface_scene; --only
                  layered|mixture|textures|subsurface), with first_entity
   bsdf_uber_*, bsdf_translucent_*, bsdf_mixture_*  the BSDF tables of those materials
+  real_texture_samples  the same on tests.helpers.real_textured_scene (roughness, IOR and
+                 sigma from image textures; --only real_textures)
   photons_box, photons_spheres, photons_materials  photon_mapping_integrator::render images
                  (stochastic progressive photon mapping) of PHOTON_CASES (--only photons)
 
@@ -62,7 +64,7 @@ The reference's two-level tree (--only two_level):
                  sample) pairs, path_integrator, depth 5
 
 Usage: python tests/golden/make_golden.py [--only fog|direct|materials|baseline|two_level|oren_nayar|layered|
-       mixture|textures|subsurface|photons]
+       mixture|textures|subsurface|photons|real_textures]
 """
 from __future__ import annotations
 
@@ -303,6 +305,17 @@ def subsurface_fixtures():
          first_entity=first_entity(R, px, sm))
 
 
+def real_texture_fixtures():
+    from tests.helpers import real_textured_scene
+    R = ref.RefScene(real_textured_scene(scene_of(SPHERES)))
+    rng = np.random.default_rng(59)
+    px = rng.integers(0, SPHERES["width"] * SPHERES["height"], 1024).astype(np.uint32)
+    sm = rng.integers(0, 4096, 1024).astype(np.uint32)
+    L = R.trace_samples(px, sm, max_depth=8, rr=1.0, seed=0)
+    save("real_texture_samples", params=params_array(SPHERES), pixels=px, samples=sm, radiance=L,
+         max_depth=np.array(8), first_entity=first_entity(R, px, sm))
+
+
 # photon_mapping_integrator::render cases: (name, scene params, scene variant,
 # iterations, max_depth, photons, radius)
 PHOTON_CASES = (
@@ -385,6 +398,8 @@ def main():
         return subsurface_fixtures()
     if only == "photons":
         return photon_fixtures()
+    if only == "real_textures":
+        return real_texture_fixtures()
     seeds = np.array([0, 1, 2, 3, 0xDEADBEEF, (1 << 48) | 12345], dtype=np.uint64)
     u32 = np.zeros((len(seeds), 64), np.uint32)
     reals = np.zeros((len(seeds), 64), np.float32)
@@ -437,6 +452,7 @@ def main():
     mixture_fixtures()
     texture_fixtures()
     subsurface_fixtures()
+    real_texture_fixtures()
     photon_fixtures()
 
 

@@ -549,6 +549,67 @@ def textured_scene(scene: rb.Scene) -> rb.Scene:
     return scene.with_materials(mats).with_textures(scene_textures())
 
 
+def real_texture_images():
+    """Images for real parameters (channel 0 read; all three channels equal): roughness 0.02-0.5 (7 x 5),
+    IOR 1.2-1.8 (4 x 6), Oren-Nayar sigma 0-60 degrees with zeros (5 x 5), and a checker of roughness
+    0 and 0.3 (3 x 2: glass is Fresnel-specular where both roughnesses are 0)."""
+    rng = np.random.default_rng(29)
+
+    def grey(v):
+        return np.repeat(v[..., None], 3, axis=2).astype(np.float32)
+    rough = grey(0.02 + 0.48 * rng.random((5, 7)))
+    ior = grey(1.2 + 0.6 * rng.random((6, 4)))
+    sigma = 60.0 * rng.random((5, 5))
+    sigma[rng.random((5, 5)) < 0.3] = 0.0
+    yy, xx = np.mgrid[0:2, 0:3]
+    checker = np.where((xx + yy) % 2 == 0, 0.0, 0.3)
+    return [rough, ior, grey(sigma), grey(checker)]
+
+
+def real_textured_scene(scene: rb.Scene) -> rb.Scene:
+    """The scene with textured real parameters (real_texture_images as textures 5-8 after
+    scene_textures): every matte material's sigma from the sigma image; every third material (from
+    the second, the floor's) in turn a metal with both roughnesses from the roughness image, a glass
+    whose roughnesses follow the 0 / 0.3 checker and whose IOR follows the IOR image, and a plastic
+    with textured roughness, IOR and diffuse; every third (from the third) in turn an uber with a
+    textured IOR and roughness u, a substrate with textured roughness v, and a subsurface material
+    with textured roughnesses and IOR."""
+    mats = []
+    for k in range(scene.desc.num_materials):
+        m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
+        if k % 3 == 1:
+            variant = (k // 3) % 3
+            if variant == 0:
+                m = _desc(rb.RB_MATERIAL_METAL, remap_roughness=1, eta=(0.200438, 0.924033, 1.102212),
+                          k=(3.912949, 2.452848, 2.142188), roughness_u=0.2, roughness_v=0.3, roughness_u_texture=5,
+                          roughness_v_texture=5)
+            elif variant == 1:
+                m = _desc(rb.RB_MATERIAL_GLASS, remap_roughness=1, reflectance=(1.0, 1.0, 1.0),
+                          transmission=(1.0, 1.0, 1.0), ior=1.5, roughness_u_texture=8, roughness_v_texture=8,
+                          ior_texture=6)
+            else:
+                m = _desc(rb.RB_MATERIAL_PLASTIC, remap_roughness=1, diffuse=(0.5, 0.5, 0.5),
+                          reflectance=(0.3, 0.3, 0.3), roughness_u=0.15, ior=1.49, diffuse_texture=1,
+                          roughness_u_texture=5, ior_texture=6)
+        elif k % 3 == 2:
+            variant = (k // 3) % 3
+            if variant == 0:
+                m = _desc(rb.RB_MATERIAL_UBER, remap_roughness=1, diffuse=(0.5, 0.3, 0.2), specular=(0.3, 0.3, 0.25),
+                          reflectance=(0.1, 0.1, 0.1), opacity=(1.0, 1.0, 1.0), roughness_u=0.15, roughness_v=0.2,
+                          ior=1.5, ior_texture=6, roughness_u_texture=5)
+            elif variant == 1:
+                m = _desc(rb.RB_MATERIAL_SUBSTRATE, remap_roughness=1, diffuse=(0.5, 0.35, 0.2),
+                          reflectance=(0.05, 0.05, 0.05), roughness_u=0.1, roughness_v=0.25, roughness_v_texture=5)
+            else:
+                m = _desc(rb.RB_MATERIAL_SUBSURFACE, remap_roughness=1, reflectance=(1.0, 1.0, 1.0),
+                          transmission=(1.0, 1.0, 1.0), diffuse=(0.8, 0.5, 0.3), mfp=(0.4, 0.2, 0.05), ior=1.33,
+                          roughness_u_texture=8, roughness_v_texture=8, ior_texture=6)
+        elif m.kind == rb.RB_MATERIAL_MATTE:
+            m.sigma_texture = 7
+        mats.append(m)
+    return scene.with_materials(mats).with_textures(scene_textures() + real_texture_images())
+
+
 def subsurface_scene(scene: rb.Scene) -> rb.Scene:
     """The scene with every third material (from the second, the floor's) a
     subsurface material (subsurface_material.cpp: glass lobes over a

@@ -10,8 +10,8 @@ import pytest
 
 import rainbow_b200 as rb
 from oracle import ref
-from tests.helpers import (extra_materials_scene, layered_scene, mixture_scene, subsurface_scene, textured_scene,
-                           two_level_scene)
+from tests.helpers import (extra_materials_scene, layered_scene, mixture_scene, real_textured_scene, subsurface_scene,
+                           textured_scene, two_level_scene)
 
 pytestmark = pytest.mark.skipif(not ref.adapter_available(), reason="oracle/_ref/libadapter_check.so not built")
 
@@ -106,12 +106,16 @@ def _resolve_texture(descs, texels, ref, channel0=False):
     return tuple(out)
 
 
-def test_export_keeps_image_textures():
-    """Image, scale and mixture textures of material spectra are exported with
-    the same texels, inputs and constants, each texture once, and the
-    material's other parameters kept."""
-    scene = textured_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12,
-                                             subdivision=2))
+_REAL_FIELDS = ("roughness_u_texture", "roughness_v_texture", "ior_texture", "sigma_texture")
+
+
+@pytest.mark.parametrize("make", [textured_scene, real_textured_scene])
+def test_export_keeps_image_textures(make):
+    """Image, scale and mixture textures of material spectra, and image textures
+    of real parameters (roughness, IOR, sigma: image_texture2d<real>, exported as
+    RGB images read at channel 0), are exported with the same texels, inputs and
+    constants, each texture once, and the material's other parameters kept."""
+    scene = make(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=48, height=40, num_spheres=12, subdivision=2))
     R = ref.RefScene(scene)
     mats, ent = ref.adapter_export_materials(R, rb.MaterialDesc)
     exported = ref.adapter_export_textures(R, rb.TextureDesc)
@@ -141,6 +145,21 @@ def test_export_keeps_image_textures():
                 getattr(b, value)[:] = (0.0, 0.0, 0.0)
             setattr(a, f, 0)
             setattr(b, f, 0)
+        for f in _REAL_FIELDS:
+            ra, rb_ = getattr(a, f), getattr(b, f)
+            assert (ra == 0) == (rb_ == 0), (e, f)
+            if ra:
+                assert _resolve_texture(exp_descs, lambda t: exported[t][1], ra, channel0=True) == \
+                    _resolve_texture(src_descs, src_texels, rb_, channel0=True), (e, f)
+                used += 1
+                setattr(a, f[:-len("_texture")], 0.0)  # the constant the texture replaces is not read
+                setattr(b, f[:-len("_texture")], 0.0)
+            setattr(a, f, 0)
+            setattr(b, f, 0)
+        if a.kind == rb.RB_MATERIAL_TRANSLUCENT:  # one roughness, exported as both
+            a.roughness_v = b.roughness_v
         assert bytes(a) == bytes(b), f"entity {e}"
     kinds = {dd.kind for dd in exp_descs}
-    assert used > 0 and kinds == {rb.RB_TEXTURE_IMAGE, rb.RB_TEXTURE_SCALE, rb.RB_TEXTURE_MIXTURE}
+    assert used > 0
+    if make is textured_scene:
+        assert kinds == {rb.RB_TEXTURE_IMAGE, rb.RB_TEXTURE_SCALE, rb.RB_TEXTURE_MIXTURE}

@@ -9,8 +9,8 @@ import pytest
 import rainbow_b200 as rb
 from tests import golden
 from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, layered_scene,
-                           mixture_scene, oren_nayar_scene, per_sample_radiance, scene_from_params, subsurface_scene,
-                           textured_scene)
+                           mixture_scene, oren_nayar_scene, per_sample_radiance, real_textured_scene, scene_from_params,
+                           subsurface_scene, textured_scene)
 
 pytestmark = pytest.mark.gpu
 
@@ -49,7 +49,8 @@ def test_oren_nayar_samples_match_reference():
 
 
 @pytest.mark.parametrize("name,make", [("layered_samples", layered_scene), ("mixture_samples", mixture_scene),
-                                       ("texture_samples", textured_scene), ("subsurface_samples", subsurface_scene)])
+                                       ("texture_samples", textured_scene), ("subsurface_samples", subsurface_scene),
+                                       ("real_texture_samples", real_textured_scene)])
 def test_layered_samples_match_reference(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))
@@ -63,7 +64,8 @@ def test_layered_samples_match_reference(name, make):
 
 
 @pytest.mark.parametrize("name,make", [("layered_samples", layered_scene), ("mixture_samples", mixture_scene),
-                                       ("texture_samples", textured_scene), ("subsurface_samples", subsurface_scene)])
+                                       ("texture_samples", textured_scene), ("subsurface_samples", subsurface_scene),
+                                       ("real_texture_samples", real_textured_scene)])
 def test_layered_direct_matches_host_build(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))

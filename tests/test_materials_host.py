@@ -2,7 +2,7 @@
 materials (plastic_material.cpp, mirror_material.cpp, substrate_material.cpp,
 matte_material.cpp with sigma != 0, uber_material.cpp, translucent_material.cpp,
 mixture_material.cpp, subsurface_material.cpp with the normalized-diffusion BSSRDF), and
-image textures (textures/detail/image_texture.hpp), in
+image textures (textures/detail/image_texture.hpp) of spectra and of real parameters, in
 the path integrator's stages and in direct lighting, compiled for the host,
 against the reference (fixture from the compiled reference, and the reference
 itself where it is built): bit-equal radiance per (pixel, sample)."""
@@ -16,8 +16,8 @@ import ctypes as C
 from oracle import ref
 from tests import golden
 from tests.helpers import (HOSTPATHS, _LOBE_NAMES, HostPaths, _desc, extra_materials_scene, layered_scene, material_lobes,
-                           mixture_scene, oren_nayar_scene, scene_from_params, subsurface_scene, texture_images,
-                           textured_scene)
+                           mixture_scene, oren_nayar_scene, real_textured_scene, scene_from_params, subsurface_scene,
+                           texture_images, textured_scene)
 
 
 def test_host_stages_extra_materials_match_fixture():
@@ -91,7 +91,8 @@ def test_layered_lobe_lists():
 
 
 @pytest.mark.parametrize("name,make", [("mixture_samples", mixture_scene), ("texture_samples", textured_scene),
-                                       ("subsurface_samples", subsurface_scene)])
+                                       ("subsurface_samples", subsurface_scene),
+                                       ("real_texture_samples", real_textured_scene)])
 def test_host_stages_mixture_match_fixture(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))
@@ -101,7 +102,8 @@ def test_host_stages_mixture_match_fixture(name, make):
 
 @pytest.mark.skipif(not ref.available(), reason="reference oracle not built")
 @pytest.mark.parametrize("name,make", [("mixture_samples", mixture_scene), ("texture_samples", textured_scene),
-                                       ("subsurface_samples", subsurface_scene)])
+                                       ("subsurface_samples", subsurface_scene),
+                                       ("real_texture_samples", real_textured_scene)])
 def test_host_direct_mixture_against_reference(name, make):
     fx = golden.load(name)
     scene = make(scene_from_params(fx["params"]))

@@ -4,7 +4,7 @@ own order and streams: bit-equal to the compiled reference's render (golden fixt
 and the reference itself where it is built), on the box room, the sphere scene and the
 sphere scene with plastic, mirror and substrate materials; more scenes (layered,
 mixture, textured and subsurface materials, invisible medium boundaries) against the
-reference directly."""
+reference directly; with real parameters from textures too."""
 import numpy as np
 import pytest
 
@@ -12,7 +12,8 @@ import rainbow_b200 as rb
 from oracle import ref
 from tests import golden
 from tests.golden.make_golden import PHOTON_CASES, photon_scene
-from tests.helpers import HostPaths, layered_scene, mixture_scene, scene_from_params, subsurface_scene, textured_scene
+from tests.helpers import (HostPaths, layered_scene, mixture_scene, real_textured_scene, scene_from_params, subsurface_scene,
+                           textured_scene)
 
 
 @pytest.mark.parametrize("case", PHOTON_CASES, ids=[c[0] for c in PHOTON_CASES])
@@ -28,11 +29,12 @@ def test_host_photon_render_matches_fixture(case):
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference oracle not built")
-@pytest.mark.parametrize("variant", ["layered", "mixture", "textured", "subsurface", "fog"])
+@pytest.mark.parametrize("variant", ["layered", "mixture", "textured", "real_textured", "subsurface", "fog"])
 def test_host_photon_render_against_reference(variant):
     base = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=3, width=40, height=32, num_spheres=10, subdivision=2)
     scene = {"layered": lambda: layered_scene(base), "mixture": lambda: mixture_scene(base),
-             "textured": lambda: textured_scene(base), "subsurface": lambda: subsurface_scene(base),
+             "textured": lambda: textured_scene(base), "real_textured": lambda: real_textured_scene(base),
+             "subsurface": lambda: subsurface_scene(base),
              "fog": lambda: rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=40, height=30, num_spheres=6,
                                               subdivision=2)}[variant]()
     want, _ = ref.RefScene(scene).render_photons(4, 6, 2500, 0.3)
