@@ -432,6 +432,69 @@ def photons_leg(rb, device, iterations=4, radius=0.2, cpu_res=128, cpu_iteration
     return out
 
 
+def subsurface_sphere_field(rb, res):
+    """The sphere field (1,024,010 triangles) at res x res with every third material a subsurface material
+    (glass lobes over the normalized-diffusion BSSRDF, mean free paths 0.05-0.4, smooth and rough in turn)."""
+    scene = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=1, width=res, height=res, num_spheres=200, subdivision=4)
+    mats = [rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k])) for k in range(scene.desc.num_materials)]
+    for k in range(1, len(mats), 3):
+        m = rb.MaterialDesc()
+        m.kind, m.remap_roughness, m.ior = rb.RB_MATERIAL_SUBSURFACE, 1, 1.33
+        m.reflectance[:], m.transmission[:] = (1.0, 1.0, 1.0), (1.0, 1.0, 1.0)
+        m.diffuse[:], m.mfp[:] = (0.8, 0.5, 0.3), (0.4, 0.2, 0.05)
+        m.roughness_u = m.roughness_v = 0.0 if (k // 3) % 2 == 0 else 0.2
+        mats[k] = m
+    return scene.with_materials(mats)
+
+
+def subsurface_waves(res=512):
+    """One 1-spp call of depth 8 on the subsurface sphere field at res x res (waves of res * res paths): the
+    workload of the subsurface profile in profiles/."""
+    import rainbow_b200 as rb
+    scene = subsurface_sphere_field(rb, res)
+    ctx = rb.Context(0)
+    ctx.upload(scene)
+    ctx.render(scene.camera, 1, max_depth=8, seed=3, want_image=False, paths_per_wave=res * res)
+    st = ctx.stats()
+    ctx.close()
+    print(json.dumps({"ms": st.elapsed_ms, "rays": st.extend_rays + st.shadow_rays + st.mis_rays,
+                      "launches": st.kernel_launches}))
+    return 0
+
+
+def subsurface_leg(rb, device, threads, spp=4, rows=(448, 576)):
+    """Path tracing with subsurface materials: the sphere field (1,024,010 triangles, 1024 x 1024, depth 8)
+    with every third material a subsurface material (glass lobes over the normalized-diffusion BSSRDF, mean
+    free paths 0.05-0.4, smooth and rough in turn), so a share of the paths takes the k_subsurface stage:
+    one call of `spp` samples per pixel with autotuned launch shapes; the reference's own path_integrator on
+    `rows` of the image at 1 spp on all host cores."""
+    scene = subsurface_sphere_field(rb, 1024)
+    ctx = rb.Context(device)
+    ctx.upload(scene)
+    t, _ = ctx.tune_render(scene.camera, probe_spp=1, max_depth=8, seed=90)
+    best, rays = None, 0
+    for k in range(2):
+        ctx.render(scene.camera, spp, max_depth=8, seed=3 + k, want_image=False)
+        st = ctx.stats()
+        if best is None or st.elapsed_ms < best:
+            best, rays = st.elapsed_ms, st.extend_rays + st.shadow_rays + st.mis_rays
+    ctx.close()
+    out = {"workload": f"sphere field, {scene.num_triangles} triangles, 1024x1024, {spp} spp, depth 8, every third "
+                       "material subsurface (normalized-diffusion BSSRDF)",
+           "gpu_msamples_per_s": 1024 * 1024 * spp / best / 1e3, "gpu_ms": best, "gpu_mrays_per_s": rays / best / 1e3,
+           "tuning": t.as_dict()}
+    try:
+        from oracle import ref
+        if ref.available():
+            _, _, sec = ref.RefScene(scene).render(1, 0, 8, 1.0, 0, threads, rows=rows)
+            n = 1024 * (rows[1] - rows[0])
+            out.update(cpu_reference_msamples_per_s=n / sec / 1e6, cpu_reference_s=sec, cpu_cores=threads,
+                       cpu_sample=f"rows {rows[0]}-{rows[1] - 1} at 1 spp ({n} samples)")
+    except Exception as e:  # reported, never required
+        out["cpu_reference_error"] = str(e)
+    return out
+
+
 def spheres_s5_leg(rb, device, spp=8):
     """The sphere field at icosphere subdivision 5 (200 spheres, 4,096,002 triangles): one call of `spp`
     samples per pixel with autotuned launch shapes."""
@@ -513,6 +576,7 @@ def summary_of(extra, batched, guided):
     out = {name: pick(extra.get(name), "gpu_msamples_per_s", "msamples_per_s", "cpu_reference_msamples_per_s", "error")
            for name in ("config1", "direct", "spheres_s5", "config5_plain")}
     out["photons"] = pick(extra.get("photons"), "gpu_mphotons_per_s", "cpu_reference_mphotons_per_s", "error")
+    out["subsurface"] = pick(extra.get("subsurface"), "gpu_msamples_per_s", "cpu_reference_msamples_per_s", "error")
     out = {k: {a: b for a, b in v.items() if b is not None} if isinstance(v, dict) else v for k, v in out.items()}
     if isinstance(batched, dict):
         out["batched"] = {k: v for k, v in pick(batched, "msamples_per_s", "error").items() if v is not None}
@@ -549,6 +613,8 @@ def main():
                     help="only render one 2-spp direct-lighting call on the sphere field (profiling)")
     ap.add_argument("--photon-waves", action="store_true",
                     help="only render one 2-iteration photon-mapping call on the sphere field at 512x512 (profiling)")
+    ap.add_argument("--subsurface-waves", action="store_true",
+                    help="only render one 1-spp call of the subsurface sphere field at 512x512 (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--tuning", default=None, help="launch shapes as JSON (skips the autotuner), e.g. "
                     "'{\"block_trace\": 256, \"grid_per_sm\": 16}'")
@@ -561,6 +627,8 @@ def main():
         return direct_waves()
     if args.photon_waves:
         return photon_waves()
+    if args.subsurface_waves:
+        return subsurface_waves()
     if args.trace_waves:
         return trace_waves()
 
@@ -748,7 +816,8 @@ def main():
                           ("spheres_s5", lambda: spheres_s5_leg(rb, local)),
                           ("config5_plain", lambda: config5_leg(rb, local)),
                           ("direct", lambda: direct_leg(rb, local, os.cpu_count() or 1)),
-                          ("photons", lambda: photons_leg(rb, local))):
+                          ("photons", lambda: photons_leg(rb, local)),
+                          ("subsurface", lambda: subsurface_leg(rb, local, os.cpu_count() or 1))):
             try:
                 extra[name] = leg()
             except Exception as e:  # reported, never required for the throughput line
