@@ -83,6 +83,13 @@ RB_HD vec3 world_dpdu(const scene_view& s, int32_t slot, float b1, float b2) {
 }
 
 constexpr int kSssMaxProbeHits = 64;  // probe-ray steps of one walk (the reference does not bound them)
+constexpr uint32_t kSssProbeCache = 8;  // hits the first walk keeps, so that the second walk is needed only beyond them
+
+// The hits of the subsurface material that a probe walk found, with their rays.
+struct sss_probe_cache {
+	hit_t hit[kSssProbeCache];
+	vec3 o[kSssProbeCache], d[kSssProbeCache];
+};
 
 // The probe of a BSSRDF sample: walks from `from` toward `to` as the
 // reference's loop does (scattering_surface_function.cpp:103-121): spawn_ray_to
@@ -90,9 +97,10 @@ constexpr int kSssMaxProbeHits = 64;  // probe-ray steps of one walk (the refere
 // repeat; hits on entities with `material` count. Returns their number (all
 // of them when want < 0, else want + 1 once the want-th one, counted from 0,
 // is reached) and that hit and its ray in hit_out / o_out / d_out.
+// cache (not null, want < 0): receives the first kSssProbeCache hits counted.
 template <typename Trace>
 RB_HD uint32_t sss_probe(const scene_view& s, uint32_t material, vec3 from, vec3 to, int32_t want, Trace&& trace,
-	hit_t& hit_out, vec3& o_out, vec3& d_out) {
+	hit_t& hit_out, vec3& o_out, vec3& d_out, sss_probe_cache* cache = nullptr) {
 	vec3 bp = from, bn{0.f, 0.f, 0.f};
 	uint32_t found = 0;
 	for (int step = 0; step < kSssMaxProbeHits; step++) {
@@ -109,6 +117,11 @@ RB_HD uint32_t sss_probe(const scene_view& s, uint32_t material, vec3 from, vec3
 				o_out = r.o;
 				d_out = r.d;
 				return found + 1;
+			}
+			if (cache != nullptr && found < kSssProbeCache) {
+				cache->hit[found] = h;
+				cache->o[found] = r.o;
+				cache->d[found] = r.d;
 			}
 			found++;
 		}
@@ -166,11 +179,19 @@ RB_HD bool subsurface_walk(const scene_view& s, path_state& p, const shade_recor
 	const vec3 to = from + l * pz;
 	hit_t h{};
 	vec3 o{}, dir{};
-	const uint32_t count = sss_probe(s, rec.material, from, to, -1, trace, h, o, dir);
+	sss_probe_cache cache;
+	const uint32_t count = sss_probe(s, rec.material, from, to, -1, trace, h, o, dir, &cache);
 	if (count == 0u) return false;
 	uint32_t which = static_cast<uint32_t>(u * static_cast<float>(count));
 	if (which > count - 1u) which = count - 1u;
-	sss_probe(s, rec.material, from, to, static_cast<int32_t>(which), trace, h, o, dir);
+	// the chosen hit (the reference walks the segment again up to it; the walk is deterministic)
+	if (which < kSssProbeCache) {
+		h = cache.hit[which];
+		o = cache.o[which];
+		dir = cache.d[which];
+	} else {
+		sss_probe(s, rec.material, from, to, static_cast<int32_t>(which), trace, h, o, dir);
+	}
 	surface_t sx = make_surface(s, h.slot, h.b1, h.b2, o, dir);
 	sx.wo = sx.sz;
 	const spectrum value = sss_eval_profile(m->sss_a, m->sss_d, length(si.p - sx.p));

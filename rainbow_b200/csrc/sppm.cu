@@ -7,9 +7,9 @@
 //                    bound of the search spheres and the largest radius by
 //                    warp reductions and atomics on order-preserving keys
 //   k_sppm_grid      one thread: the grid's cell counts from that bound
-//   k_sppm_count     one thread per visible point: entries per hash bucket
+//   k_sppm_cells<0>  one thread per visible point: entries per hash bucket
 //   k_scan_*         exclusive prefix sum of the bucket counts (bucket offsets)
-//   k_sppm_fill      the bucket entries (pixel indices), a pixel once per cell
+//   k_sppm_cells<1>  the bucket entries (pixel indices), a pixel once per cell
 //                    of its sphere's box that hashes to the bucket, as the
 //                    reference's lists hold it
 //   k_sppm_photons   one thread per photon: its path with importance
