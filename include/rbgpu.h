@@ -163,13 +163,18 @@ typedef struct rb_material_desc {
 	uint32_t opacity_texture;
 	float mfp[3];               /* subsurface: mean free path (RGB) */
 	/* real parameters from textures: 0 the constant above; k > 0: channel 0 of
-	 * image texture rb_scene_desc.textures[k - 1] (image_texture2d<real>; not
-	 * inside a mixture); roughness_to_alpha, the smooth-glass test and Oren-Nayar's
-	 * A and B then follow the texel at every hit */
+	 * texture rb_scene_desc.textures[k - 1] (an image_texture2d<real>, or a scale /
+	 * mixture texture of real images and constants; not inside a mixture);
+	 * roughness_to_alpha, the smooth-glass test and Oren-Nayar's A and B then
+	 * follow the texel at every hit */
 	uint32_t roughness_u_texture;
 	uint32_t roughness_v_texture;
 	uint32_t ior_texture;
 	uint32_t sigma_texture;
+	/* spectra from textures, as the *_texture fields above: metal eta and k, subsurface mfp */
+	uint32_t eta_texture;
+	uint32_t k_texture;
+	uint32_t mfp_texture;
 } rb_material_desc;
 
 enum {

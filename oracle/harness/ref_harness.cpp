@@ -170,10 +170,18 @@ struct texture_set {
 		}
 		return t;
 	}
-	// a real texture: a constant, or channel 0 of image ref - 1
-	std::shared_ptr<texture2d<real>> real_of(float v, uint32_t ref) {
-		if (ref == 0 || ref > count || descs[ref - 1].kind != RB_TEXTURE_IMAGE) return real_texture(v);
+	// a real texture: a constant, or with ref > 0 texture ref - 1 read at channel
+	// 0: an image_texture2d<real>, or a scale / mixture texture of real images
+	// and constants
+	std::shared_ptr<texture2d<real>> real_of(float v, uint32_t ref, int depth = 0) {
+		if (ref == 0 || ref > count || depth > 1) return real_texture(v);
 		const rb_texture_desc& d = descs[ref - 1];
+		if (d.kind == RB_TEXTURE_SCALE)
+			return std::make_shared<scale_texture_t<2, real>>(real_of(d.constants[0][0], d.inputs[0], depth + 1),
+				real_of(d.constants[1][0], d.inputs[1], depth + 1));
+		if (d.kind == RB_TEXTURE_MIXTURE)
+			return std::make_shared<mixture_texture_t<2, real>>(real_of(d.constants[0][0], d.inputs[0], depth + 1),
+				real_of(d.constants[1][0], d.inputs[1], depth + 1), real_of(d.constants[2][0], d.inputs[2], depth + 1));
 		std::vector<real> values;
 		for (size_t i = 0; i < static_cast<size_t>(d.width) * d.height; i++) values.push_back(d.rgb[3 * i]);
 		return std::make_shared<image_texture2d<real>>(rainbow::core::math::vector_t<2, size_t>(d.width, d.height), values);
@@ -195,7 +203,8 @@ std::shared_ptr<material> make_material(const rb_material_desc* all, uint32_t co
 	switch (m.kind) {
 	case RB_MATERIAL_MATTE: return std::make_shared<matte_material>(diffuse, tex.real_of(m.sigma, m.sigma_texture));
 	case RB_MATERIAL_METAL:
-		return std::make_shared<metal_material>(spectrum_texture(m.eta), spectrum_texture(m.k), tex.real_of(m.roughness_u, m.roughness_u_texture),
+		return std::make_shared<metal_material>(tex.spectrum_of(m.eta, m.eta_texture), tex.spectrum_of(m.k, m.k_texture),
+			tex.real_of(m.roughness_u, m.roughness_u_texture),
 			tex.real_of(m.roughness_v, m.roughness_v_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_GLASS:
 		return std::make_shared<glass_material>(reflectance, transmission, tex.real_of(m.roughness_u, m.roughness_u_texture),
@@ -214,7 +223,7 @@ std::shared_ptr<material> make_material(const rb_material_desc* all, uint32_t co
 		return std::make_shared<translucent_material>(transmission, reflectance, specular, diffuse,
 			tex.real_of(m.roughness_u, m.roughness_u_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_SUBSURFACE:
-		return std::make_shared<subsurface_material>(transmission, reflectance, diffuse, spectrum_texture(m.mfp),
+		return std::make_shared<subsurface_material>(transmission, reflectance, diffuse, tex.spectrum_of(m.mfp, m.mfp_texture),
 			tex.real_of(m.roughness_u, m.roughness_u_texture), tex.real_of(m.roughness_v, m.roughness_v_texture), tex.real_of(m.ior, m.ior_texture), m.remap_roughness != 0);
 	case RB_MATERIAL_MIXTURE: {
 		if (m.components[0] < 0 || m.components[1] < 0) return nullptr;

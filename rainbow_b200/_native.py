@@ -66,7 +66,8 @@ class MaterialDesc(C.Structure):
                 ("reflectance_texture", C.c_uint32), ("transmission_texture", C.c_uint32),
                 ("specular_texture", C.c_uint32), ("opacity_texture", C.c_uint32), ("mfp", F3),
                 ("roughness_u_texture", C.c_uint32), ("roughness_v_texture", C.c_uint32), ("ior_texture", C.c_uint32),
-                ("sigma_texture", C.c_uint32)]
+                ("sigma_texture", C.c_uint32), ("eta_texture", C.c_uint32), ("k_texture", C.c_uint32),
+                ("mfp_texture", C.c_uint32)]
 
 
 class TextureDesc(C.Structure):

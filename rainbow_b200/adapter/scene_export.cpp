@@ -119,6 +119,11 @@ RB_PRIVATE_MEMBER(scale_base, textures::scale_texture_t<2 COMMA shared::spectrum
 RB_PRIVATE_MEMBER(mixture_t0, textures::mixture_texture_t<2 COMMA shared::spectrums::spectrum>::mTexture0);
 RB_PRIVATE_MEMBER(mixture_t1, textures::mixture_texture_t<2 COMMA shared::spectrums::spectrum>::mTexture1);
 RB_PRIVATE_MEMBER(mixture_alpha_texture, textures::mixture_texture_t<2 COMMA shared::spectrums::spectrum>::mAlpha);
+RB_PRIVATE_MEMBER(real_scale_scale, textures::scale_texture_t<2 COMMA rainbow::core::real>::mScale);
+RB_PRIVATE_MEMBER(real_scale_base, textures::scale_texture_t<2 COMMA rainbow::core::real>::mBase);
+RB_PRIVATE_MEMBER(real_mixture_t0, textures::mixture_texture_t<2 COMMA rainbow::core::real>::mTexture0);
+RB_PRIVATE_MEMBER(real_mixture_t1, textures::mixture_texture_t<2 COMMA rainbow::core::real>::mTexture1);
+RB_PRIVATE_MEMBER(real_mixture_alpha, textures::mixture_texture_t<2 COMMA rainbow::core::real>::mAlpha);
 RB_PRIVATE_MEMBER(surface_radiance, emitters::surface_light::mRadiance);
 RB_PRIVATE_MEMBER(environment_map, emitters::environment_light::mEnvironmentMap);
 RB_PRIVATE_MEMBER(environment_intensity, emitters::environment_light::mIntensity);
@@ -215,9 +220,48 @@ struct texture_registry {
 	bool real(const std::shared_ptr<textures::texture2d<rainbow::core::real>>& t, float& v, uint32_t& ref) {
 		ref = 0;
 		if (constant_real(t, v)) return true;
+		if (real_image(t, ref)) return true;
+		return real_composite(t, ref);
+	}
+	bool real_image(const std::shared_ptr<textures::texture2d<rainbow::core::real>>& t, uint32_t& ref) {
 		const auto img = std::dynamic_pointer_cast<textures::image_texture2d<rainbow::core::real>>(t);
 		return img != nullptr && add_image(img.get(), img->size().x, img->size().y,
 			[&](size_t i, float* c) { c[0] = c[1] = c[2] = img->value(i); }, ref);
+	}
+	// A scale or mixture texture of reals whose inputs are real images or
+	// constants (constants in every channel; the core reads channel 0).
+	bool real_composite(const std::shared_ptr<textures::texture2d<rainbow::core::real>>& t, uint32_t& ref) {
+		using R = rainbow::core::real;
+		const auto it = ref_of.find(t.get());
+		if (it != ref_of.end()) {
+			ref = it->second;
+			return true;
+		}
+		rb_texture_desc td{};
+		const auto input = [&](const std::shared_ptr<textures::texture2d<R>>& in, uint32_t i) {
+			float v = 0.f;
+			if (constant_real(in, v)) {
+				td.constants[i][0] = td.constants[i][1] = td.constants[i][2] = v;
+				return true;
+			}
+			return real_image(in, td.inputs[i]);
+		};
+		if (const auto x = std::dynamic_pointer_cast<textures::scale_texture_t<2, R>>(t)) {
+			td.kind = RB_TEXTURE_SCALE;
+			if (!input(read(*x, real_scale_scale{}), 0) || !input(read(*x, real_scale_base{}), 1)) return false;
+		} else if (const auto x = std::dynamic_pointer_cast<textures::mixture_texture_t<2, R>>(t)) {
+			td.kind = RB_TEXTURE_MIXTURE;
+			if (!input(read(*x, real_mixture_t0{}), 0) || !input(read(*x, real_mixture_t1{}), 1) ||
+				!input(read(*x, real_mixture_alpha{}), 2))
+				return false;
+		} else {
+			return false;
+		}
+		out.texels.emplace_back();
+		out.textures.push_back(td);
+		ref = static_cast<uint32_t>(out.textures.size());
+		ref_of.emplace(t.get(), ref);
+		return true;
 	}
 	// An RGB image texture, exported once.
 	bool image(const std::shared_ptr<textures::texture2d<shared::spectrums::spectrum>>& t, uint32_t& ref) {
@@ -262,7 +306,7 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 	} else if (const auto x = std::dynamic_pointer_cast<materials::metal_material>(m)) {
 		d.kind = RB_MATERIAL_METAL;
 		d.remap_roughness = read(*x, metal_remap{}) ? 1 : 0;
-		ok = constant_rgb(read(*x, metal_eta{}), d.eta) && constant_rgb(read(*x, metal_k{}), d.k) &&
+		ok = spec(read(*x, metal_eta{}), d.eta, d.eta_texture) && spec(read(*x, metal_k{}), d.k, d.k_texture) &&
 			tex.real(read(*x, metal_ru{}), d.roughness_u, d.roughness_u_texture) && tex.real(read(*x, metal_rv{}), d.roughness_v, d.roughness_v_texture);
 	} else if (const auto x = std::dynamic_pointer_cast<materials::glass_material>(m)) {
 		d.kind = RB_MATERIAL_GLASS;
@@ -310,7 +354,7 @@ rb_status export_material(const std::shared_ptr<materials::material>& m, rb_mate
 		ok = spec(read(*x, subsurface_transmission{}), d.transmission, d.transmission_texture) &&
 			spec(read(*x, subsurface_reflectance{}), d.reflectance, d.reflectance_texture) &&
 			spec(read(*x, subsurface_diffuse{}), d.diffuse, d.diffuse_texture) &&
-			constant_rgb(read(*x, subsurface_mfp{}), d.mfp) && tex.real(read(*x, subsurface_ru{}), d.roughness_u, d.roughness_u_texture) &&
+			spec(read(*x, subsurface_mfp{}), d.mfp, d.mfp_texture) && tex.real(read(*x, subsurface_ru{}), d.roughness_u, d.roughness_u_texture) &&
 			tex.real(read(*x, subsurface_rv{}), d.roughness_v, d.roughness_v_texture) && tex.real(read(*x, subsurface_eta{}), d.ior, d.ior_texture);
 	} else {
 		return RB_ERR_UNSUPPORTED;  // a material kind outside these (a mixture is exported by export_scene)

@@ -53,6 +53,9 @@ bool make_src(const rb_material_desc& md, pt::material_src& p) {
 	p.tex[pt::TEX_ROUGHNESS_V] = md.roughness_v_texture;
 	p.tex[pt::TEX_IOR] = md.ior_texture;
 	p.tex[pt::TEX_SIGMA] = md.sigma_texture;
+	p.tex[pt::TEX_ETA] = md.eta_texture;
+	p.tex[pt::TEX_K] = md.k_texture;
+	p.tex[pt::TEX_MFP] = md.mfp_texture;
 	switch (md.kind) {
 	case RB_MATERIAL_METAL:
 		p.cond_eta = v3(md.eta, 0);
@@ -76,7 +79,8 @@ bool make_src(const rb_material_desc& md, pt::material_src& p) {
 
 bool textured(const rb_material_desc& md) {
 	return md.diffuse_texture || md.reflectance_texture || md.transmission_texture || md.specular_texture ||
-		md.opacity_texture || md.roughness_u_texture || md.roughness_v_texture || md.ior_texture || md.sigma_texture;
+		md.opacity_texture || md.roughness_u_texture || md.roughness_v_texture || md.ior_texture || md.sigma_texture ||
+		md.eta_texture || md.k_texture || md.mfp_texture;
 }
 
 // One material's record (pt::build_record), or with `scale` its scaled build.
@@ -142,9 +146,6 @@ rb_status pack_materials(const rb_scene_desc* desc, std::vector<pt::material_rec
 			if (!make_src(md, p)) return RB_ERR_INVALID_ARGUMENT;
 			for (uint32_t t = 0; t < pt::kNumTexSlots; t++)
 				if (p.tex[t] > desc->num_textures) return RB_ERR_INVALID_ARGUMENT;
-			// a real parameter reads channel 0 of an image (image_texture2d<real>); no composites
-			for (uint32_t t = pt::TEX_ROUGHNESS_U; t <= pt::TEX_SIGMA; t++)
-				if (p.tex[t] && desc->textures[p.tex[t] - 1].kind != RB_TEXTURE_IMAGE) return RB_ERR_UNSUPPORTED;
 			out[k] = pt::material_rec{};
 			out[k].kind = pt::MAT_TEXTURED;
 			out[k].src = static_cast<uint32_t>(srcs.size());

@@ -288,13 +288,16 @@ RB_HD const material_rec* hit_material(const scene_view& s, uint32_t index, vec2
 	if (q.tex[TEX_TRANSMISSION]) q.transmission = sample_texture(s, q.tex[TEX_TRANSMISSION] - 1u, uv, p);
 	if (q.tex[TEX_SPECULAR]) q.specular = sample_texture(s, q.tex[TEX_SPECULAR] - 1u, uv, p);
 	if (q.tex[TEX_OPACITY]) q.opacity = sample_texture(s, q.tex[TEX_OPACITY] - 1u, uv, p);
-	// real parameters: channel 0 of their images (image_texture2d<real>)
+	// real parameters: channel 0 of their textures (texture2d<real>)
 	const bool reals = q.tex[TEX_ROUGHNESS_U] | q.tex[TEX_ROUGHNESS_V] | q.tex[TEX_IOR] | q.tex[TEX_SIGMA];
 	if (q.tex[TEX_ROUGHNESS_U]) q.roughness_u = sample_texture(s, q.tex[TEX_ROUGHNESS_U] - 1u, uv, p).x;
 	if (q.tex[TEX_ROUGHNESS_V]) q.roughness_v = sample_texture(s, q.tex[TEX_ROUGHNESS_V] - 1u, uv, p).x;
 	if (q.tex[TEX_IOR]) q.ior = sample_texture(s, q.tex[TEX_IOR] - 1u, uv, p).x;
 	if (q.tex[TEX_SIGMA]) q.sigma = sample_texture(s, q.tex[TEX_SIGMA] - 1u, uv, p).x;
 	if (reals) derive_src(q);
+	if (q.tex[TEX_ETA]) q.cond_eta = sample_texture(s, q.tex[TEX_ETA] - 1u, uv, p);
+	if (q.tex[TEX_K]) q.cond_k = sample_texture(s, q.tex[TEX_K] - 1u, uv, p);
+	if (q.tex[TEX_MFP]) q.mfp = sample_texture(s, q.tex[TEX_MFP] - 1u, uv, p);
 	build_record(q, nullptr, scratch);
 	return &scratch;
 }

@@ -160,10 +160,12 @@ struct material_rec {
 };
 
 // Textured parameters of a material: the spectra diffuse, reflectance,
-// transmission, specular, opacity, then the reals roughness u and v, IOR and
-// Oren-Nayar sigma (channel 0 of an image).
+// transmission, specular, opacity, the reals roughness u and v, IOR and
+// Oren-Nayar sigma (channel 0 of a texture), then the spectra conductor eta
+// and k and the subsurface mean free path.
 enum : uint32_t { TEX_DIFFUSE = 0, TEX_REFLECTANCE = 1, TEX_TRANSMISSION = 2, TEX_SPECULAR = 3, TEX_OPACITY = 4,
-	TEX_ROUGHNESS_U = 5, TEX_ROUGHNESS_V = 6, TEX_IOR = 7, TEX_SIGMA = 8, kNumTexSlots = 9 };
+	TEX_ROUGHNESS_U = 5, TEX_ROUGHNESS_V = 6, TEX_IOR = 7, TEX_SIGMA = 8, TEX_ETA = 9, TEX_K = 10, TEX_MFP = 11,
+	kNumTexSlots = 12 };
 
 // A material's parameters with what only the host computes already applied
 // (roughness_to_alpha, Oren-Nayar's A and B), from which its record is built

@@ -550,9 +550,11 @@ def textured_scene(scene: rb.Scene) -> rb.Scene:
 
 
 def real_texture_images():
-    """Images for real parameters (channel 0 read; all three channels equal): roughness 0.02-0.5 (7 x 5),
-    IOR 1.2-1.8 (4 x 6), Oren-Nayar sigma 0-60 degrees with zeros (5 x 5), and a checker of roughness
-    0 and 0.3 (3 x 2: glass is Fresnel-specular where both roughnesses are 0)."""
+    """Textures 5-13 after scene_textures: images for real parameters (channel 0 read; all three channels
+    equal): roughness 0.02-0.5 (7 x 5), IOR 1.2-1.8 (4 x 6), Oren-Nayar sigma 0-60 degrees with zeros
+    (5 x 5), a checker of roughness 0 and 0.3 (3 x 2: glass is Fresnel-specular where both roughnesses
+    are 0); RGB images of conductor eta, k and mean free paths; a scale texture (the roughness image
+    times 0.5) and a mixture texture (the roughness image and 0.05, mixed by the checker) of reals."""
     rng = np.random.default_rng(29)
 
     def grey(v):
@@ -563,17 +565,23 @@ def real_texture_images():
     sigma[rng.random((5, 5)) < 0.3] = 0.0
     yy, xx = np.mgrid[0:2, 0:3]
     checker = np.where((xx + yy) % 2 == 0, 0.0, 0.3)
-    return [rough, ior, grey(sigma), grey(checker)]
+    eta = (0.2 + rng.random((4, 4, 3))).astype(np.float32)
+    k = (2.0 + 2.0 * rng.random((3, 5, 3))).astype(np.float32)
+    mfp = (0.05 + 0.35 * rng.random((4, 3, 3))).astype(np.float32)
+    return [rough, ior, grey(sigma), grey(checker), eta, k, mfp,
+            dict(kind=rb.RB_TEXTURE_SCALE, inputs=[5, 0], constants=[(0.0, 0.0, 0.0), (0.5, 0.5, 0.5)]),
+            dict(kind=rb.RB_TEXTURE_MIXTURE, inputs=[5, 0, 8], constants=[(0.0, 0.0, 0.0), (0.05, 0.05, 0.05)])]
 
 
 def real_textured_scene(scene: rb.Scene) -> rb.Scene:
-    """The scene with textured real parameters (real_texture_images as textures 5-8 after
+    """The scene with textured real parameters (real_texture_images as textures 5-13 after
     scene_textures): every matte material's sigma from the sigma image; every third material (from
-    the second, the floor's) in turn a metal with both roughnesses from the roughness image, a glass
+    the second, the floor's) in turn a metal with its roughnesses from the real scale and mixture
+    textures and its eta and k from images, a glass
     whose roughnesses follow the 0 / 0.3 checker and whose IOR follows the IOR image, and a plastic
     with textured roughness, IOR and diffuse; every third (from the third) in turn an uber with a
     textured IOR and roughness u, a substrate with textured roughness v, and a subsurface material
-    with textured roughnesses and IOR."""
+    with textured roughnesses, IOR and mean free path."""
     mats = []
     for k in range(scene.desc.num_materials):
         m = rb.MaterialDesc.from_buffer_copy(bytes(scene.desc.materials[k]))
@@ -581,8 +589,8 @@ def real_textured_scene(scene: rb.Scene) -> rb.Scene:
             variant = (k // 3) % 3
             if variant == 0:
                 m = _desc(rb.RB_MATERIAL_METAL, remap_roughness=1, eta=(0.200438, 0.924033, 1.102212),
-                          k=(3.912949, 2.452848, 2.142188), roughness_u=0.2, roughness_v=0.3, roughness_u_texture=5,
-                          roughness_v_texture=5)
+                          k=(3.912949, 2.452848, 2.142188), roughness_u=0.2, roughness_v=0.3, roughness_u_texture=12,
+                          roughness_v_texture=13, eta_texture=9, k_texture=10)
             elif variant == 1:
                 m = _desc(rb.RB_MATERIAL_GLASS, remap_roughness=1, reflectance=(1.0, 1.0, 1.0),
                           transmission=(1.0, 1.0, 1.0), ior=1.5, roughness_u_texture=8, roughness_v_texture=8,
@@ -603,7 +611,7 @@ def real_textured_scene(scene: rb.Scene) -> rb.Scene:
             else:
                 m = _desc(rb.RB_MATERIAL_SUBSURFACE, remap_roughness=1, reflectance=(1.0, 1.0, 1.0),
                           transmission=(1.0, 1.0, 1.0), diffuse=(0.8, 0.5, 0.3), mfp=(0.4, 0.2, 0.05), ior=1.33,
-                          roughness_u_texture=8, roughness_v_texture=8, ior_texture=6)
+                          roughness_u_texture=8, roughness_v_texture=8, ior_texture=6, mfp_texture=11)
         elif m.kind == rb.RB_MATERIAL_MATTE:
             m.sigma_texture = 7
         mats.append(m)

@@ -85,7 +85,8 @@ def test_export_keeps_mixtures():
     assert seen > 0
 
 
-_TEX_FIELDS = ("diffuse_texture", "reflectance_texture", "transmission_texture", "specular_texture", "opacity_texture")
+_TEX_FIELDS = ("diffuse_texture", "reflectance_texture", "transmission_texture", "specular_texture", "opacity_texture",
+               "eta_texture", "k_texture", "mfp_texture")
 
 
 def _resolve_texture(descs, texels, ref, channel0=False):
