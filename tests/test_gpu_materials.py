@@ -10,7 +10,7 @@ import rainbow_b200 as rb
 from tests import golden
 from tests.helpers import (HostPaths, assert_disagreements_unbiased, extra_materials_scene, layered_scene,
                            mixture_scene, oren_nayar_scene, per_sample_radiance, real_textured_scene, scene_from_params,
-                           subsurface_scene, textured_scene)
+                           subsurface_scene, textured_scene, two_level_scene)
 
 pytestmark = pytest.mark.gpu
 
@@ -131,3 +131,20 @@ def test_subsurface_refuses_guided_and_volume_renders():
             assert e.value.status == 7, kw  # RB_ERR_UNSUPPORTED
         ctx.render(scene.camera, spp=1, max_depth=8, want_image=False)  # the context stays usable
         assert ctx.stats().device_error == 0
+
+
+def test_subsurface_two_level_image_matches_host_build():
+    """The subsurface stage on a scene with the two-level tree (instance slots: a shared mesh and a
+    327,680-triangle mesh, every third material subsurface): whole 1-spp image against the host build."""
+    scene = subsurface_scene(two_level_scene(48, 40))
+    W, H = scene.camera.width, scene.camera.height
+    px = np.arange(W * H, dtype=np.uint32)
+    want = HostPaths(scene).samples(scene.camera, px, np.full_like(px, 4), 8)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        ctx.render(scene.camera, spp=1, first_sample=4, max_depth=8, want_image=False)
+        sums, _, cnt = ctx.film()
+        assert ctx.stats().device_error == 0
+    assert (cnt == 1).all()
+    agree = _agreement(sums.reshape(-1, 3).astype(np.float32), want)
+    assert agree >= 0.97, f"only {agree:.4f} of pixels agree"

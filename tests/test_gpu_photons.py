@@ -9,7 +9,7 @@ import pytest
 import rainbow_b200 as rb
 from tests import golden
 from tests.golden.make_golden import PHOTON_CASES, photon_scene
-from tests.helpers import HostPaths
+from tests.helpers import HostPaths, two_level_scene
 
 pytestmark = pytest.mark.gpu
 
@@ -68,3 +68,16 @@ def test_photon_render_arguments():
         assert np.isfinite(img).all() and img.mean() > 0.0
         ctx.render(scene.camera, 1, max_depth=5)  # the context stays usable for path tracing
         assert ctx.stats().device_error == 0
+
+
+def test_photon_render_two_level_scene_matches_host_build():
+    """A scene with the two-level tree (a shared mesh and a 327,680-triangle mesh): the photon kernels'
+    instance-slot traversal against the host build with the same streams."""
+    scene = two_level_scene(48, 40)
+    want = HostPaths(scene).photon_render(scene.camera, 3, 5, 0, 0.3, streams=1, seed=3)
+    with rb.Context(0) as ctx:
+        ctx.upload(scene)
+        got = ctx.render_photons(scene.camera, 3, 5, 0, 0.3, seed=3)
+    close = (np.abs(got - want) <= PIXEL_RTOL * np.maximum(np.abs(want), 1e-2)).all(axis=2)
+    assert close.mean() >= 0.95, f"only {close.mean():.4f} of pixels agree"
+    assert want.mean() > 0.0 and abs(got.mean() / want.mean() - 1.0) < 2e-3

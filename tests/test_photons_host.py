@@ -13,7 +13,7 @@ from oracle import ref
 from tests import golden
 from tests.golden.make_golden import PHOTON_CASES, photon_scene
 from tests.helpers import (HostPaths, layered_scene, mixture_scene, real_textured_scene, scene_from_params, subsurface_scene,
-                           textured_scene)
+                           textured_scene, two_level_scene)
 
 
 @pytest.mark.parametrize("case", PHOTON_CASES, ids=[c[0] for c in PHOTON_CASES])
@@ -29,14 +29,15 @@ def test_host_photon_render_matches_fixture(case):
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference oracle not built")
-@pytest.mark.parametrize("variant", ["layered", "mixture", "textured", "real_textured", "subsurface", "fog"])
+@pytest.mark.parametrize("variant", ["layered", "mixture", "textured", "real_textured", "subsurface", "fog", "two_level"])
 def test_host_photon_render_against_reference(variant):
     base = rb.generate_scene(rb.RB_SCENE_SPHERES, seed=3, width=40, height=32, num_spheres=10, subdivision=2)
     scene = {"layered": lambda: layered_scene(base), "mixture": lambda: mixture_scene(base),
              "textured": lambda: textured_scene(base), "real_textured": lambda: real_textured_scene(base),
              "subsurface": lambda: subsurface_scene(base),
              "fog": lambda: rb.generate_scene(rb.RB_SCENE_FOG, seed=4, width=40, height=30, num_spheres=6,
-                                              subdivision=2)}[variant]()
+                                              subdivision=2),
+             "two_level": lambda: two_level_scene(40, 30)}[variant]()
     want, _ = ref.RefScene(scene).render_photons(4, 6, 2500, 0.3)
     got = HostPaths(scene).photon_render(scene.camera, 4, 6, 2500, 0.3, streams=0)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
