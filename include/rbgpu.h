@@ -369,8 +369,9 @@ rb_status rb_render(rb_context* ctx, const rb_render_params* params, float* rgb_
 
 /* rb_render without waiting: returns once the call's work is enqueued, so that
  * consecutive calls overlap on the GPU (the late bounces of one call with the
- * first waves of the next, on the wave lanes) while the film still adds their
- * samples in call order. No counterpart in the reference, whose render() is
+ * first waves of the next: the calls' waves take the wave lanes in turn, so a
+ * call of one wave runs beside the previous call) while the film still adds
+ * their samples in call order. No counterpart in the reference, whose render() is
  * synchronous. Plain path tracing only: flags other than RB_RENDER_RESET return
  * RB_ERR_UNSUPPORTED. rgb_out, if not NULL, must be page-locked; its slices are
  * written as the call's pixels complete, and it must not be read or reused
