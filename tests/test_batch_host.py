@@ -5,15 +5,18 @@ for bit the hits and radiance of the same scene uploaded alone."""
 import numpy as np
 
 import rainbow_b200 as rb
-from tests.helpers import HostBatch, HostPaths, assert_hits_equal, mixture_scene, random_rays, textured_scene
+from tests.helpers import (HostBatch, HostPaths, assert_hits_equal, mixture_scene, random_rays, subsurface_scene,
+                           textured_scene)
 
 
 def batch_scenes():
     """Four scenes; the first and the last with image textures (the last's texture references and texels are
-    relocated by the merge), the third with mixtures (component records relocated)."""
+    relocated by the merge), the second with a subsurface material (the merged scene takes its profile table,
+    and every scene's bounces then run staged with the subsurface stage), the third with mixtures (component
+    records relocated)."""
     return [
         textured_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=5, width=40, height=30, num_spheres=12, subdivision=2)),
-        rb.generate_scene(rb.RB_SCENE_BOX, seed=0, width=32, height=32),
+        subsurface_scene(rb.generate_scene(rb.RB_SCENE_BOX, seed=0, width=32, height=32)),
         mixture_scene(rb.generate_scene(rb.RB_SCENE_SLIT_ROOM, seed=3, width=36, height=36, num_spheres=6, subdivision=2)),
         textured_scene(rb.generate_scene(rb.RB_SCENE_SPHERES, seed=9, width=24, height=24, num_spheres=3, subdivision=1)),
     ]
