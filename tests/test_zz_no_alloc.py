@@ -63,8 +63,13 @@ def _assert_equal_films(acc, want, w, h):
     np.testing.assert_allclose(d_sq.cpu().numpy().reshape(h, w, 3), want_sq, rtol=1e-12, atol=1e-12)
 
 
-def test_noalloc_render_matches_allocating_render_on_two_calls():
+@pytest.mark.parametrize("subsurface", [False, True])
+def test_noalloc_render_matches_allocating_render_on_two_calls(subsurface):
+    """Also on the box room with a subsurface material (the subsurface stage's queue lives in the scratch)."""
     scene = rb.generate_scene(rb.RB_SCENE_BOX, width=W, height=H)
+    if subsurface:
+        from tests.helpers import subsurface_scene
+        scene = subsurface_scene(scene)
     with rb.Context(0) as ctx:
         ctx.upload(scene)
         # the existing entry point: two calls, accumulating
